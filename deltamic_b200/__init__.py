@@ -1,0 +1,25 @@
+"""deltamic_b200: the deltaMic render-and-fit hot path on NVIDIA B200 (sm_100a).
+
+Drop-in names of the reference package (``from deltamic import ...``):
+``Fourier3dMesh``, ``generate_gaussian_psf``, ``generate_gaussian_psf_from_sigma``,
+``render_image_from_ftmesh``, ``normalize_tensor``, ``compute_box_size``,
+``compute_spatial_frequency_grid``, ``center_verts_in_box``.
+
+Beyond the reference: ``MeshRenderer`` (fused render + loss + adjoint),
+``fit_mesh`` / ``FitStep`` (Adam fitting loop, CUDA-graph captured), and the
+synthetic mesh generators in ``deltamic_b200.mesh``.
+
+All compute runs in hand-written CUDA kernels of ``lib/libdeltamic_b200.so``
+behind a C ABI (``include/deltamic_b200.h``); there is no CPU fallback.
+"""
+from .psf import generate_gaussian_psf, generate_gaussian_psf_from_sigma
+from .render import (Fourier3dMesh, center_verts_in_box, compute_box_size,
+                     compute_spatial_frequency_grid, normalize_tensor,
+                     render_image_from_ftmesh)
+from .pipeline import MeshRenderer
+
+__all__ = [
+    "Fourier3dMesh", "generate_gaussian_psf", "generate_gaussian_psf_from_sigma",
+    "render_image_from_ftmesh", "normalize_tensor", "compute_box_size",
+    "compute_spatial_frequency_grid", "center_verts_in_box", "MeshRenderer",
+]

@@ -1,0 +1,152 @@
+"""ctypes binding of ``lib/libdeltamic_b200.so`` (the C ABI in include/deltamic_b200.h).
+
+The library is required: there is no CPU or PyTorch fallback.  ``lib()`` raises
+``RuntimeError`` when the shared object is missing or fails to load.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libdeltamic_b200.so")
+
+DM_OK = 0
+DM_ERR_INVALID_ARG = 1
+DM_ERR_BAD_INDEX = 2
+DM_ERR_SIZE = 4
+DM_ERR_WORKSPACE = 8
+DM_ERR_CUDA = 16
+DM_ERR_TIMEOUT = 32
+DM_ERR_UNSUPPORTED = 64
+
+ABI_VERSION = 1
+
+# Entry points and their (restype, argtypes); every symbol of the public header.
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_SZ = ctypes.c_size_t
+_F = ctypes.c_float
+_INT = ctypes.c_int
+
+
+class DmBox(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3),
+                ("shape", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32)]
+
+
+_BOXP = ctypes.POINTER(DmBox)
+
+SIGNATURES = {
+    "dm_abi_version": (_INT, []),
+    "dm_status_string": (ctypes.c_char_p, [_INT]),
+    "dm_device_error": (_INT, [_P, ctypes.POINTER(_INT), _P]),
+    "dm_narrowband_workspace_size": (_SZ, [_I64]),
+    "dm_narrowband_compact": (_INT, [_P, _I64, _F, _P, _P, _P, _SZ, _P]),
+    "dm_topology_size": (_SZ, [_I64, _I64]),
+    "dm_topology_build": (_INT, [_P, _I64, _I64, _P, _SZ, _P]),
+    "dm_meshft_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft_forward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _P, _SZ,
+                                 _P]),
+    "dm_meshft_backward_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft_backward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _F, _P,
+                                  _P, _P, _P, _P, _P, _SZ, _P]),
+    "dm_gaussian_otf": (_INT, [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
+                               _P, _P]),
+    "dm_gaussian_otf_grad_workspace_size": (_SZ, [_I64]),
+    "dm_gaussian_otf_sigma_grad": (_INT, [_P, _P, _I64, _P, _P, ctypes.c_int32, _P,
+                                          ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),
+    "dm_image_loss_workspace_size": (_SZ, [_I64]),
+    "dm_image_loss": (_INT, [_P, _I64, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
+    "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """The loaded library (loads it on first use; raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"deltamic_b200 native library not found at {LIB_PATH}; build it with "
+                "`python -m deltamic_b200.build` (nvcc, sm_100a). There is no CPU fallback.")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        if handle.dm_abi_version() != ABI_VERSION:
+            raise RuntimeError("libdeltamic_b200.so ABI version mismatch; rebuild it")
+        _lib = handle
+    return _lib
+
+
+class DeltaMicError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib().dm_status_string(status).decode()
+        super().__init__(f"{where}: {msg} (status {status})")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != DM_OK:
+        raise DeltaMicError(status, where)
+
+
+def ptr(t) -> int | None:
+    """Device address of a tensor (None for None)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_ptr(device=None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def make_box(box_size, box_shape) -> DmBox:
+    b = DmBox()
+    for d in range(3):
+        b.lo[d] = float(box_size[d][0])
+        b.hi[d] = float(box_size[d][1])
+        b.shape[d] = int(box_shape[d])
+    b.reserved = 0
+    return b
+
+
+def require_cuda(t: torch.Tensor, name: str, dtype=None) -> None:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor (deltamic_b200 has no CPU path)")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise RuntimeError(f"{name} must be contiguous")
+
+
+class Workspace:
+    """Grow-only device scratch buffer per (device, purpose)."""
+
+    def __init__(self):
+        self._bufs: dict = {}
+
+    def get(self, key, nbytes: int, device) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        k = (key, str(device))
+        buf = self._bufs.get(k)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.zeros(nbytes, dtype=torch.uint8, device=device)
+            self._bufs[k] = buf
+        return buf
+
+
+WORKSPACES = Workspace()

@@ -1,0 +1,349 @@
+// extern "C" entry points of libdeltamic_b200.so (declared in
+// include/deltamic_b200.h): argument checks, workspace carving, launches.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "band_internal.h"
+#include "dm_common.cuh"
+#include "meshft_internal.h"
+
+using namespace dm;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// Sequential carving of a workspace into aligned pieces.
+struct Carve {
+  char* base;
+  size_t off;
+  explicit Carve(void* p) : base((char*)p), off(0) {}
+  template <typename T>
+  T* take(size_t count) {
+    T* p = base ? (T*)(base + off) : nullptr;
+    off += up(sizeof(T) * std::max<size_t>(count, 1));
+    return p;
+  }
+};
+
+bool box_ok(const dm_box* b) {
+  if (!b) return false;
+  for (int d = 0; d < 3; ++d) {
+    if (b->shape[d] <= 0) return false;
+    if (!(b->hi[d] > b->lo[d])) return false;
+  }
+  const int64_t n = (int64_t)b->shape[0] * b->shape[1] * b->shape[2];
+  return n <= (int64_t)INT32_MAX;
+}
+
+CellDesc single_cell(const dm_box* b, int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
+  CellDesc d;
+  memset(&d, 0, sizeof(d));
+  for (int k = 0; k < 3; ++k) {
+    d.lo[k] = b ? b->lo[k] : 0.0;
+    d.len[k] = b ? b->hi[k] - b->lo[k] : 1.0;
+    d.n[k] = b ? b->shape[k] : 1;
+  }
+  d.nv = (int32_t)nv;
+  d.nt = (int32_t)nt;
+  d.nband = (int32_t)nband;
+  d.grid_off = 0;
+  plan_offsets(&d, 1, t);
+  return d;
+}
+
+Cells one_cell(const CellDesc& d) {
+  Cells c;
+  c.p = nullptr;
+  c.n = 1;
+  c.one = d;
+  return c;
+}
+
+bool sizes_ok(int64_t nv, int64_t nt, int64_t nband) {
+  return nv >= 0 && nt >= 0 && nband >= 0 && nv < (int64_t)INT32_MAX / 3 &&
+         nt < (int64_t)INT32_MAX / 9 && nband < (int64_t)INT32_MAX;
+}
+
+// Forward workspace layout.
+struct FwdWs {
+  int* err;
+  double* area_part;
+  FaceRec* recs;
+  float2* fpart;
+};
+size_t fwd_layout(void* ws, const PlanTotals& t, FwdWs* out) {
+  Carve c(ws);
+  FwdWs w;
+  w.err = c.take<int>(4);
+  w.area_part = c.take<double>(t.face_blks);
+  w.recs = c.take<FaceRec>(t.nt);
+  w.fpart = c.take<float2>(t.fpart);
+  if (out) *out = w;
+  return c.off;
+}
+
+// Topology layout: off[nv+1], ent[3nt], count[nv+1], cursor[nv+1].
+struct TopoWs {
+  int* err;
+  int32_t* off;
+  int32_t* ent;
+  int32_t* count;
+  int32_t* cursor;
+};
+size_t topo_layout(void* p, int64_t nv, int64_t nt, TopoWs* out) {
+  Carve c(p);
+  TopoWs w;
+  w.err = c.take<int>(4);
+  w.off = c.take<int32_t>(nv + 1);
+  w.ent = c.take<int32_t>(3 * nt);
+  w.count = c.take<int32_t>(nv + 1);
+  w.cursor = c.take<int32_t>(nv + 1);
+  if (out) *out = w;
+  return c.off;
+}
+
+struct BwdWs {
+  int* err;
+  double* area_part;
+  double* s_part;
+  FaceRec* recs;
+  XiRec* xrec;
+  float* bpart;
+  float* contrib;
+  void* topo;
+};
+size_t bwd_layout(void* ws, const PlanTotals& t, BwdWs* out) {
+  Carve c(ws);
+  BwdWs w;
+  w.err = c.take<int>(4);
+  w.area_part = c.take<double>(t.face_blks);
+  w.s_part = c.take<double>(t.band_blks);
+  w.recs = c.take<FaceRec>(t.nt);
+  w.xrec = c.take<XiRec>(t.nband);
+  w.bpart = c.take<float>(t.bpart);
+  w.contrib = c.take<float>(9 * t.nt);
+  w.topo = c.base ? (void*)(c.base + c.off) : nullptr;
+  c.off += topo_layout(nullptr, t.nv, t.nt, nullptr);
+  if (out) *out = w;
+  return c.off;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dm_abi_version(void) { return 1; }
+
+const char* dm_status_string(int status) {
+  if (status == DM_OK) return "ok";
+  if (status & DM_ERR_INVALID_ARG) return "invalid argument";
+  if (status & DM_ERR_BAD_INDEX) return "face index out of range";
+  if (status & DM_ERR_SIZE) return "size out of range";
+  if (status & DM_ERR_WORKSPACE) return "workspace too small";
+  if (status & DM_ERR_CUDA) return "CUDA error";
+  if (status & DM_ERR_TIMEOUT) return "bounded device wait timed out";
+  if (status & DM_ERR_UNSUPPORTED) return "unsupported";
+  return "unknown status";
+}
+
+int dm_device_error(void* workspace, int* out_flags, dm_stream_t stream) {
+  if (!workspace || !out_flags) return DM_ERR_INVALID_ARG;
+  int v = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&v, workspace, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return DM_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return DM_ERR_CUDA;
+  if (cudaMemsetAsync(workspace, 0, sizeof(int), st) != cudaSuccess) return DM_ERR_CUDA;
+  *out_flags = v;
+  return DM_OK;
+}
+
+// ---------------------------------------------------------------------------
+size_t dm_narrowband_workspace_size(int64_t n_voxels) {
+  if (n_voxels < 0) return 0;
+  const int64_t nb = band_blocks(n_voxels);
+  return up(sizeof(int) * 4) + 2 * up(sizeof(int32_t) * std::max<int64_t>(nb, 1));
+}
+
+int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh, int32_t* band_index,
+                          int64_t* band_count, void* workspace, size_t ws_bytes,
+                          dm_stream_t stream) {
+  if (n_voxels < 0 || !band_count || !workspace || (n_voxels > 0 && (!otf || !band_index)))
+    return DM_ERR_INVALID_ARG;
+  if (n_voxels > (int64_t)INT32_MAX) return DM_ERR_SIZE;
+  if (ws_bytes < dm_narrowband_workspace_size(n_voxels)) return DM_ERR_WORKSPACE;
+  const int64_t nb = std::max<int64_t>(band_blocks(n_voxels), 1);
+  Carve c(workspace);
+  c.take<int>(4);
+  int32_t* bc = c.take<int32_t>(nb);
+  int32_t* bo = c.take<int32_t>(nb);
+  return launch_narrowband(otf, n_voxels, thresh, band_index, band_count, bc, bo,
+                           (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+size_t dm_topology_size(int64_t nv, int64_t nt) {
+  if (nv < 0 || nt < 0) return 0;
+  return topo_layout(nullptr, nv, nt, nullptr);
+}
+
+int dm_topology_build(const int64_t* faces, int64_t nt, int64_t nv, void* topology,
+                      size_t topo_bytes, dm_stream_t stream) {
+  if (!topology || (nt > 0 && !faces) || !sizes_ok(nv, nt, 0)) return DM_ERR_INVALID_ARG;
+  if (topo_bytes < dm_topology_size(nv, nt)) return DM_ERR_WORKSPACE;
+  PlanTotals t;
+  CellDesc d = single_cell(nullptr, nv, nt, 0, t);
+  TopoWs w;
+  topo_layout(topology, nv, nt, &w);
+  return launch_topology(one_cell(d), t, faces, w.count, w.off, w.cursor, w.ent, w.err,
+                         (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+size_t dm_meshft_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
+  if (!sizes_ok(nv, nt, n_band)) return 0;
+  PlanTotals t;
+  single_cell(nullptr, nv, nt, n_band, t);
+  return fwd_layout(nullptr, t, nullptr);
+}
+
+int dm_meshft_forward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                      const float* faces_coeff, const dm_box* box, const int32_t* band_index,
+                      int64_t n_band, const float* otf, float* ft_list, float* grid,
+                      void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_band)) return DM_ERR_SIZE;
+  if (!box_ok(box) || !workspace) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (n_band > 0 && (!band_index || !ft_list)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_forward_workspace_size(nv, nt, n_band)) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PlanTotals t;
+  CellDesc d = single_cell(box, nv, nt, n_band, t);
+  FwdWs w;
+  fwd_layout(workspace, t, &w);
+  const Cells c = one_cell(d);
+  int s = launch_face_prep(c, t, verts, faces, faces_coeff, w.recs, w.area_part, w.err, st);
+  if (s) return s;
+  return launch_forward(c, t, w.recs, band_index, w.area_part, otf, w.fpart, (float2*)ft_list,
+                        (float2*)grid, w.err, st);
+}
+
+// ---------------------------------------------------------------------------
+size_t dm_meshft_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
+  if (!sizes_ok(nv, nt, n_band)) return 0;
+  PlanTotals t;
+  single_cell(nullptr, nv, nt, n_band, t);
+  return bwd_layout(nullptr, t, nullptr);
+}
+
+int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                       const float* faces_coeff, const dm_box* box, const int32_t* band_index,
+                       int64_t n_band, const float* grad_list, const float* grad_grid,
+                       const float* otf, float grad_scale, const float* ft_list,
+                       const void* topology, float* grad_verts, float* grad_coeff,
+                       float* grad_otf_band, void* workspace, size_t ws_bytes,
+                       dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_band)) return DM_ERR_SIZE;
+  if (!box_ok(box) || !workspace) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (nv > 0 && !grad_verts) return DM_ERR_INVALID_ARG;
+  if (n_band > 0 && (!band_index || !ft_list || (!grad_list && !grad_grid)))
+    return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_backward_workspace_size(nv, nt, n_band)) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PlanTotals t;
+  CellDesc d = single_cell(box, nv, nt, n_band, t);
+  BwdWs w;
+  bwd_layout(workspace, t, &w);
+  const Cells c = one_cell(d);
+  const void* topo = topology;
+  if (!topo) {
+    TopoWs tw;
+    topo_layout(w.topo, nv, nt, &tw);
+    int s = launch_topology(c, t, faces, tw.count, tw.off, tw.cursor, tw.ent, w.err, st);
+    if (s) return s;
+    topo = w.topo;
+  }
+  TopoWs tw;
+  topo_layout(const_cast<void*>(topo), nv, nt, &tw);
+  int s = launch_face_prep(c, t, verts, faces, faces_coeff, w.recs, w.area_part, w.err, st);
+  if (s) return s;
+  return launch_backward(c, t, verts, faces, faces_coeff, w.recs, w.area_part, band_index,
+                         (const float2*)grad_list, (const float2*)grad_grid, otf, grad_scale,
+                         (const float2*)ft_list, w.xrec, w.s_part, w.bpart, w.contrib, tw.off,
+                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.err, st);
+}
+
+// ---------------------------------------------------------------------------
+static bool axes_ok(const float* x0, int32_t n0, const float* x1, int32_t n1, const float* x2,
+                    int32_t n2) {
+  return x0 && x1 && x2 && n0 > 0 && n1 > 0 && n2 > 0 &&
+         (int64_t)n0 * n1 * n2 <= (int64_t)INT32_MAX;
+}
+
+int dm_gaussian_otf(const float* sigma, const float* xi0, int32_t n0, const float* xi1,
+                    int32_t n1, const float* xi2, int32_t n2, float* otf, dm_stream_t stream) {
+  if (!sigma || !otf || !axes_ok(xi0, n0, xi1, n1, xi2, n2)) return DM_ERR_INVALID_ARG;
+  const float* xi[3] = {xi0, xi1, xi2};
+  const int32_t n[3] = {n0, n1, n2};
+  return launch_gaussian_otf(sigma, xi, n, otf, (cudaStream_t)stream);
+}
+
+size_t dm_gaussian_otf_grad_workspace_size(int64_t n) {
+  if (n < 0) return 0;
+  return up(sizeof(int) * 4) + up(sizeof(double) * 6 * (size_t)otf_grad_blocks(n));
+}
+
+int dm_gaussian_otf_sigma_grad(const float* grad_otf, const int32_t* band_index, int64_t n_band,
+                               const float* otf, const float* xi0, int32_t n0, const float* xi1,
+                               int32_t n1, const float* xi2, int32_t n2, float* grad_sigma,
+                               void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!otf || !grad_sigma || !workspace || !axes_ok(xi0, n0, xi1, n1, xi2, n2))
+    return DM_ERR_INVALID_ARG;
+  const int64_t nvox = (int64_t)n0 * n1 * n2;
+  const int64_t n = band_index ? n_band : nvox;
+  if (n < 0 || (n > 0 && !grad_otf)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_gaussian_otf_grad_workspace_size(n)) return DM_ERR_WORKSPACE;
+  Carve c(workspace);
+  c.take<int>(4);
+  double* part = c.take<double>(6 * (size_t)otf_grad_blocks(n));
+  const float* xi[3] = {xi0, xi1, xi2};
+  const int32_t nax[3] = {n0, n1, n2};
+  return launch_otf_sigma_grad(grad_otf, band_index, n, otf, xi, nax, grad_sigma, part,
+                               (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+size_t dm_image_loss_workspace_size(int64_t n) {
+  if (n < 0) return 0;
+  return image_ws_bytes(n);
+}
+
+int dm_image_loss(const float* z, int64_t n, int kind, const float* target, float contrast,
+                  float* image, float* loss, float* grad_z, void* workspace, size_t ws_bytes,
+                  dm_stream_t stream) {
+  if (!z || n <= 0 || !loss || !workspace) return DM_ERR_INVALID_ARG;
+  if (kind != 0 && kind != 1) return DM_ERR_INVALID_ARG;
+  if (kind == 1 && !target) return DM_ERR_INVALID_ARG;
+  if (n > (int64_t)INT32_MAX) return DM_ERR_SIZE;
+  if (ws_bytes < dm_image_loss_workspace_size(n)) return DM_ERR_WORKSPACE;
+  return launch_image_loss((const float2*)z, n, kind, target, contrast, image, loss,
+                           (float2*)grad_z, workspace, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
+                 float lr, float beta1, float beta2, float eps, int64_t* step,
+                 dm_stream_t stream) {
+  if (n < 0 || !step || (n > 0 && (!param || !grad || !exp_avg || !exp_avg_sq)))
+    return DM_ERR_INVALID_ARG;
+  return launch_adam(param, grad, exp_avg, exp_avg_sq, n, lr, beta1, beta2, eps, step,
+                     (cudaStream_t)stream);
+}
+
+}  // extern "C"

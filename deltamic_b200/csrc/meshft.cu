@@ -1,0 +1,798 @@
+// meshFT forward / backward kernels for sm_100a.
+//
+// Work decomposition (see the launch plans at the end of this file):
+//  * forward: item = (cell, frequency tile of NT*R, face split).  Each thread
+//    owns R band frequencies and loops over the faces of its split; face records
+//    are staged in shared memory by the bulk-copy engine in a ring of NS tiles
+//    and read as broadcasts.  Partial sums per (split, frequency) go to HBM and
+//    the epilogue adds them in a fixed order -> deterministic, no atomics.
+//  * backward: item = (cell, face block of NT*F, frequency chunk).  Each thread
+//    owns F faces (geometry and 10 accumulators in registers) and loops over the
+//    frequencies of its chunk, staged in shared memory the same way.  Per-face
+//    partials go to HBM; the face epilogue reduces chunks in a fixed order and a
+//    CSR gather sums face contributions per vertex in a fixed order.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "dm_common.cuh"
+#include "meshft_internal.h"
+#include "pair_math.cuh"
+
+namespace dm {
+
+constexpr int kBlk = 256;  // threads of the element-wise kernels
+
+// ---------------------------------------------------------------------------
+// helpers
+
+__device__ __forceinline__ void band_to_m(int32_t idx, const CellDesc& d, int32_t mi[3]) {
+  const int32_t n12 = d.n[1] * d.n[2];
+  const int32_t k0 = idx / n12;
+  const int32_t rem = idx - k0 * n12;
+  const int32_t k1 = rem / d.n[2];
+  const int32_t k2 = rem - k1 * d.n[2];
+  mi[0] = 2 * k0 - (d.n[0] - 1);
+  mi[1] = 2 * k1 - (d.n[1] - 1);
+  mi[2] = 2 * k2 - (d.n[2] - 1);
+}
+
+__device__ __forceinline__ FaceGeom geom_from_rec(const FaceRec& r) {
+  FaceGeom g;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    g.Ua[d] = r.Ua[d];
+    g.Ub[d] = r.Ub[d];
+    g.Uc[d] = r.Uc[d];
+    g.hab[d] = r.hab[d];
+    g.hbc[d] = r.hbc[d];
+  }
+  return g;
+}
+
+__device__ __forceinline__ void load_rec_shared(const FaceRec* p, FaceRec& r) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4* o = reinterpret_cast<uint4*>(&r);
+  o[0] = q[0];
+  o[1] = q[1];
+  o[2] = q[2];
+  o[3] = q[3];
+}
+
+// Block-wide sum in double (fixed order), result valid in thread 0.
+__device__ double block_sum_d(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < nw; ++i) r += sh[i];
+  }
+  __syncthreads();
+  return r;
+}
+
+// Sum of ``n`` doubles (fixed order), broadcast to the whole block.
+__device__ double block_sum_list(const double* p, int n, double* sh) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
+  double r = block_sum_d(v, sh);
+  if (threadIdx.x == 0) sh[32] = r;
+  __syncthreads();
+  r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Face records and per-block sums of area * coeff (replaces the host loops of
+// fourier3d_cuda_kernel.cu:16-51).
+
+__global__ void k_face_prep(Cells cells, const float* __restrict__ verts,
+                            const int64_t* __restrict__ faces, const float* __restrict__ coeff,
+                            FaceRec* __restrict__ recs, double* __restrict__ area_part, int* err) {
+  __shared__ double sh[40];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  double ac = 0.0;
+  if (f < d.nt) {
+    const int64_t gf = d.f_off + f;
+    int64_t iv[3];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      iv[k] = faces[3 * gf + k];
+      if (iv[k] < 0 || iv[k] >= d.nv) {
+        ok = false;
+        iv[k] = 0;
+      }
+    }
+    if (!ok) set_error(err, DM_ERR_BAD_INDEX);
+    double p[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) p[k][j] = (double)verts[3 * (d.v_off + iv[k]) + j];
+    FaceRec r;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double sc = 2147483648.0 / d.len[j];
+      r.Ua[j] = (uint32_t)(long long)llrint((p[0][j] - d.lo[j]) * sc);
+      r.Ub[j] = (uint32_t)(long long)llrint((p[1][j] - d.lo[j]) * sc);
+      r.Uc[j] = (uint32_t)(long long)llrint((p[2][j] - d.lo[j]) * sc);
+      const double hs = 1.5707963267948966 / d.len[j];
+      r.hab[j] = (float)((p[1][j] - p[0][j]) * hs);
+      r.hbc[j] = (float)((p[2][j] - p[1][j]) * hs);
+    }
+    const double e1[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+    const double e2[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+    const double cx = e1[1] * e2[2] - e1[2] * e2[1];
+    const double cy = e1[2] * e2[0] - e1[0] * e2[2];
+    const double cz = e1[0] * e2[1] - e1[1] * e2[0];
+    ac = 0.5 * sqrt(cx * cx + cy * cy + cz * cz) * (double)coeff[gf];
+    r.area_coeff = (float)ac;
+    recs[gf] = r;
+  }
+  const double s = block_sum_d(ac, sh);
+  if (threadIdx.x == 0) area_part[blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Forward main kernel.
+
+template <int R>
+__device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const XiVal (&xv)[R],
+                                         float2 (&acc)[R]) {
+  uint32_t spm = 0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    c32 E, G, Gu, Gw;
+    int piv;
+    const bool sp = pair_fast<false>(xv[r], g, E, G, Gu, Gw, piv);
+    const c32 F = cmul(E, G);
+    acc[r].x += sp ? 0.0f : ac * F.x;
+    acc[r].y += sp ? 0.0f : ac * F.y;
+    spm |= (sp ? 1u : 0u) << r;
+  }
+  if (spm) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if ((spm >> r) & 1u) {
+        c32 F;
+        pair_general<false>(xv[r], g, F, nullptr);
+        acc[r].x += ac * F.x;
+        acc[r].y += ac * F.y;
+      }
+    }
+  }
+}
+
+template <int R, int NT, int TF, int NS>
+__global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* __restrict__ recs,
+                                                  const int32_t* __restrict__ band_index,
+                                                  float2* __restrict__ fpart, int* err) {
+  __shared__ __align__(128) FaceRec sf[NS][TF];
+  __shared__ __align__(8) uint64_t bar[NS];
+  const int item = blockIdx.x;
+  const int ci = cell_find(cells, item, [](const CellDesc& d) { return d.fwd_item0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int local = item - d.fwd_item0;
+  const int xt = local % d.xtiles;
+  const int split = local / d.xtiles;
+  const int f0 = split * d.fchunk;
+  const int nf = min(d.nt, f0 + d.fchunk) - f0;
+  if (d.nband <= 0) return;
+  if (nf <= 0) {  // no faces: the partial sums are zero
+    for (int r = 0; r < R; ++r) {
+      const int m = xt * NT * R + r * NT + threadIdx.x;
+      if (m < d.nband) fpart[d.fpart_off + (int64_t)split * d.nband + m] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+
+  XiVal xv[R];
+  int mloc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int m = xt * NT * R + r * NT + threadIdx.x;
+    mloc[r] = m;
+    // lanes past the band evaluate a real frequency so every lane takes the
+    // same branches; their sums are never stored
+    const int mm = min(m, d.nband - 1);
+    band_to_m(band_index[d.b_off + mm], d, xv[r].mi);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) xv[r].mf[k] = (float)xv[r].mi[k];
+  }
+
+  const int ntiles = (nf + TF - 1) / TF;
+  const FaceRec* src0 = recs + d.f_off + f0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS && s < ntiles; ++s) {
+      const uint32_t bytes = (uint32_t)min(TF, nf - s * TF) * (uint32_t)sizeof(FaceRec);
+      mbar_expect_tx(&bar[s], bytes);
+      bulk_g2s(&sf[s][0], src0 + s * TF, bytes, &bar[s]);
+    }
+  }
+
+  float2 acc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = make_float2(0.f, 0.f);
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t % NS;
+    if (!mbar_wait_bounded(&bar[s], (uint32_t)((t / NS) & 1), err)) return;
+    const int nft = min(TF, nf - t * TF);
+    float2 tacc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) tacc[r] = make_float2(0.f, 0.f);
+    for (int j = 0; j < nft; ++j) {
+      FaceRec fr;
+      load_rec_shared(&sf[s][j], fr);
+      fwd_face<R>(geom_from_rec(fr), fr.area_coeff, xv, tacc);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      acc[r].x += tacc[r].x;
+      acc[r].y += tacc[r].y;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && t + NS < ntiles) {
+      fence_proxy_async();
+      const int tn = t + NS;
+      const uint32_t bytes = (uint32_t)min(TF, nf - tn * TF) * (uint32_t)sizeof(FaceRec);
+      mbar_expect_tx(&bar[s], bytes);
+      bulk_g2s(&sf[s][0], src0 + tn * TF, bytes, &bar[s]);
+    }
+  }
+  float2* out = fpart + d.fpart_off + (int64_t)split * d.nband;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (mloc[r] < d.nband) out[mloc[r]] = acc[r];
+}
+
+// ft_list = (2/M) * sum over splits; optional scatter of ft * OTF into the grid.
+__global__ void k_meshft_fwd_epi(Cells cells, const int32_t* __restrict__ band_index,
+                                 const float2* __restrict__ fpart,
+                                 const double* __restrict__ area_part,
+                                 const float* __restrict__ otf, float2* __restrict__ ft_list,
+                                 float2* __restrict__ grid, int* err) {
+  __shared__ double sh[40];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.band_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const double M = block_sum_list(area_part + d.face_blk0, (d.nt + kBlk - 1) / kBlk, sh);
+  const int m = (blockIdx.x - d.band_blk0) * kBlk + threadIdx.x;
+  if (m >= d.nband) return;
+  double sx = 0.0, sy = 0.0;
+  const float2* p = fpart + d.fpart_off + m;
+  for (int s = 0; s < d.fsplit; ++s) {
+    const float2 v = p[(int64_t)s * d.nband];
+    sx += v.x;
+    sy += v.y;
+  }
+  const double sc = d.nt > 0 ? 2.0 / M : 0.0;  // no faces: ft = 0 as in the reference
+  const float2 ft = make_float2((float)(sx * sc), (float)(sy * sc));
+  ft_list[d.b_off + m] = ft;
+  if (grid) {
+    const int32_t idx = band_index[d.b_off + m];
+    if (idx < 0 || (int64_t)idx >= (int64_t)d.n[0] * d.n[1] * d.n[2]) {
+      set_error(err, DM_ERR_BAD_INDEX);
+      return;
+    }
+    const float o = otf ? otf[d.grid_off + idx] : 1.0f;
+    grid[d.grid_off + idx] = make_float2(ft.x * o, ft.y * o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Backward: band records with the cotangent, and per-block sums of
+// s = sum Re(conj(g) ft).
+
+__global__ void k_bwd_band_prep(Cells cells, const int32_t* __restrict__ band_index,
+                                const float2* __restrict__ grad_list,
+                                const float2* __restrict__ grad_grid,
+                                const float* __restrict__ otf, float grad_scale,
+                                const float2* __restrict__ ft_list, XiRec* __restrict__ xrec,
+                                float* __restrict__ grad_otf_band, double* __restrict__ s_part,
+                                int* err) {
+  __shared__ double sh[40];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.band_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int m = (blockIdx.x - d.band_blk0) * kBlk + threadIdx.x;
+  double s = 0.0;
+  if (m < d.nband) {
+    const int64_t gm = d.b_off + m;
+    int32_t idx = band_index[gm];
+    const bool ok = idx >= 0 && (int64_t)idx < (int64_t)d.n[0] * d.n[1] * d.n[2];
+    if (!ok) {
+      set_error(err, DM_ERR_BAD_INDEX);
+      idx = 0;
+    }
+    float2 G = grad_list ? grad_list[gm] : grad_grid[d.grid_off + idx];
+    if (!ok) G = make_float2(0.f, 0.f);
+    const float o = otf ? otf[d.grid_off + idx] : 1.0f;
+    const float gs = grad_scale * o;
+    const float2 g = make_float2(gs * G.x, gs * G.y);
+    const float2 ft = ft_list[gm];
+    if (grad_otf_band) grad_otf_band[gm] = grad_scale * (G.x * ft.x + G.y * ft.y);
+    s = (double)g.x * ft.x + (double)g.y * ft.y;
+    XiRec r;
+    band_to_m(idx, d, r.mi);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r.mf[k] = (float)r.mi[k];
+    r.g_re = g.x;
+    r.g_im = g.y;
+    xrec[gm] = r;
+  }
+  const double t = block_sum_d(s, sh);
+  if (threadIdx.x == 0) s_part[blockIdx.x] = t;
+}
+
+// Backward main kernel.
+struct BwdAcc {
+  float q[10];  // q[3v+j] = sum z_v m_j (v = a,b,c), q[9] = sum Re(conj(g) F)
+};
+
+__device__ __forceinline__ void bwd_pair(const XiVal& xv, const FaceGeom& g, float gre, float gim,
+                                         BwdAcc& a, bool& special) {
+  c32 E, G, Gu, Gw;
+  int piv;
+  const bool sp = pair_fast<true>(xv, g, E, G, Gu, Gw, piv);
+  // h = conj(g) E
+  const float hx = gre * E.x + gim * E.y;
+  const float hy = gre * E.y - gim * E.x;
+  const float r = hx * G.x - hy * G.y;    // Re(h G) = Re(conj(g) F)
+  const float zt = hx * G.y + hy * G.x;   // Im(h G): Re(conj(g) (-i F))
+  const float zu = hx * Gu.x - hy * Gu.y;
+  const float zw = hx * Gw.x - hy * Gw.y;
+  const float zp = zt - zu - zw;
+  float za = piv == 0 ? zp : (piv == 1 ? zw : zu);
+  float zb = piv == 0 ? zu : (piv == 1 ? zp : zw);
+  float zc = piv == 0 ? zw : (piv == 1 ? zu : zp);
+  za = sp ? 0.f : za;
+  zb = sp ? 0.f : zb;
+  zc = sp ? 0.f : zc;
+  a.q[0] += za * xv.mf[0];
+  a.q[1] += za * xv.mf[1];
+  a.q[2] += za * xv.mf[2];
+  a.q[3] += zb * xv.mf[0];
+  a.q[4] += zb * xv.mf[1];
+  a.q[5] += zb * xv.mf[2];
+  a.q[6] += zc * xv.mf[0];
+  a.q[7] += zc * xv.mf[1];
+  a.q[8] += zc * xv.mf[2];
+  a.q[9] += sp ? 0.f : r;
+  special = sp;
+}
+
+__device__ __noinline__ void bwd_pair_general(const XiVal& xv, const FaceGeom& g, float gre,
+                                              float gim, BwdAcc& a) {
+  c32 F, dF[3];
+  pair_general<true>(xv, g, F, dF);
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    const float z = gre * dF[v].x + gim * dF[v].y;
+    a.q[3 * v + 0] += z * xv.mf[0];
+    a.q[3 * v + 1] += z * xv.mf[1];
+    a.q[3 * v + 2] += z * xv.mf[2];
+  }
+  a.q[9] += gre * F.x + gim * F.y;
+}
+
+template <int F, int NT, int TX, int NS>
+__global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
+                                                  const XiRec* __restrict__ xrec,
+                                                  float* __restrict__ bpart, int* err) {
+  __shared__ __align__(128) XiRec sx[NS][TX];
+  __shared__ __align__(8) uint64_t bar[NS];
+  const int item = blockIdx.x;
+  const int ci = cell_find(cells, item, [](const CellDesc& d) { return d.bwd_item0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int local = item - d.bwd_item0;
+  const int fb = local % d.fblocks;
+  const int chunk = local / d.fblocks;
+  const int x0 = chunk * d.bxchunk;
+  const int nx = min(d.nband, x0 + d.bxchunk) - x0;
+  if (nx <= 0 || d.nt <= 0) return;
+
+  FaceGeom geom[F];
+  int fidx[F];
+#pragma unroll
+  for (int k = 0; k < F; ++k) {
+    const int f = fb * NT * F + k * NT + threadIdx.x;
+    fidx[k] = f;
+    // lanes past the last face evaluate a real face (never stored)
+    geom[k] = geom_from_rec(recs[d.f_off + min(f, d.nt - 1)]);
+  }
+
+  const int ntiles = (nx + TX - 1) / TX;
+  const XiRec* src0 = xrec + d.b_off + x0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS && s < ntiles; ++s) {
+      const uint32_t bytes = (uint32_t)min(TX, nx - s * TX) * (uint32_t)sizeof(XiRec);
+      mbar_expect_tx(&bar[s], bytes);
+      bulk_g2s(&sx[s][0], src0 + s * TX, bytes, &bar[s]);
+    }
+  }
+
+  BwdAcc acc[F];
+#pragma unroll
+  for (int k = 0; k < F; ++k)
+#pragma unroll
+    for (int i = 0; i < 10; ++i) acc[k].q[i] = 0.f;
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t % NS;
+    if (!mbar_wait_bounded(&bar[s], (uint32_t)((t / NS) & 1), err)) return;
+    const int nxt = min(TX, nx - t * TX);
+    BwdAcc tacc[F];
+#pragma unroll
+    for (int k = 0; k < F; ++k)
+#pragma unroll
+      for (int i = 0; i < 10; ++i) tacc[k].q[i] = 0.f;
+    for (int j = 0; j < nxt; ++j) {
+      const uint4* q = reinterpret_cast<const uint4*>(&sx[s][j]);
+      const uint4 w0 = q[0], w1 = q[1];
+      XiVal xv;
+      xv.mi[0] = (int32_t)w0.x;
+      xv.mi[1] = (int32_t)w0.y;
+      xv.mi[2] = (int32_t)w0.z;
+      const float gre = __uint_as_float(w0.w);
+      xv.mf[0] = __uint_as_float(w1.x);
+      xv.mf[1] = __uint_as_float(w1.y);
+      xv.mf[2] = __uint_as_float(w1.z);
+      const float gim = __uint_as_float(w1.w);
+      uint32_t spm = 0;
+#pragma unroll
+      for (int k = 0; k < F; ++k) {
+        bool sp;
+        bwd_pair(xv, geom[k], gre, gim, tacc[k], sp);
+        spm |= (sp ? 1u : 0u) << k;
+      }
+      if (spm) {
+#pragma unroll
+        for (int k = 0; k < F; ++k)
+          if ((spm >> k) & 1u) bwd_pair_general(xv, geom[k], gre, gim, tacc[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < F; ++k)
+#pragma unroll
+      for (int i = 0; i < 10; ++i) acc[k].q[i] += tacc[k].q[i];
+    __syncthreads();
+    if (threadIdx.x == 0 && t + NS < ntiles) {
+      fence_proxy_async();
+      const int tn = t + NS;
+      const uint32_t bytes = (uint32_t)min(TX, nx - tn * TX) * (uint32_t)sizeof(XiRec);
+      mbar_expect_tx(&bar[s], bytes);
+      bulk_g2s(&sx[s][0], src0 + tn * TX, bytes, &bar[s]);
+    }
+  }
+  float* out = bpart + d.bpart_off + (int64_t)chunk * 10 * d.nt;
+#pragma unroll
+  for (int k = 0; k < F; ++k) {
+    if (fidx[k] < d.nt) {
+#pragma unroll
+      for (int i = 0; i < 10; ++i) out[(int64_t)i * d.nt + fidx[k]] = acc[k].q[i];
+    }
+  }
+}
+
+// Per-face epilogue: reduce chunks, then
+//   contrib[f][v][j] = trisar * (pi/L_j) * Q[v][j] + (c/M)(2r - s) dA/dv_j
+//   grad_coeff[f]    = (A/M)(2r - s)
+// (vertex adjoint of fourier3d_cuda_kernel.cu:365-394 with w and gradmeshar of
+// .cu:26-32 folded per face; Faces_coeff gradient from trisar = 2Ac/M).
+__global__ void k_bwd_face_epi(Cells cells, const float* __restrict__ verts,
+                               const int64_t* __restrict__ faces,
+                               const float* __restrict__ coeff,
+                               const double* __restrict__ area_part,
+                               const double* __restrict__ s_part,
+                               const float* __restrict__ bpart, float* __restrict__ contrib,
+                               float* __restrict__ grad_coeff) {
+  __shared__ double sh[40];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const double M = block_sum_list(area_part + d.face_blk0, (d.nt + kBlk - 1) / kBlk, sh);
+  const double S = block_sum_list(s_part + d.band_blk0, (d.nband + kBlk - 1) / kBlk, sh);
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  if (f >= d.nt) return;
+  const int64_t gf = d.f_off + f;
+  double q[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) q[i] = 0.0;
+  const float* p = bpart + d.bpart_off + f;
+  for (int c = 0; c < d.bchunks; ++c) {
+#pragma unroll
+    for (int i = 0; i < 10; ++i) q[i] += p[((int64_t)c * 10 + i) * d.nt];
+  }
+  int64_t iv[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    iv[k] = faces[3 * gf + k];
+    if (iv[k] < 0 || iv[k] >= d.nv) iv[k] = 0;
+  }
+  double P[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) P[k][j] = (double)verts[3 * (d.v_off + iv[k]) + j];
+  const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+  const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+  double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                 e1[0] * e2[1] - e1[1] * e2[0]};
+  const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  const double A = 0.5 * nn;
+  n[0] /= nn;
+  n[1] /= nn;
+  n[2] /= nn;
+  const double c = (double)coeff[gf];
+  const double trisar = 2.0 * A * c / M;
+  const double k2 = 2.0 * q[9] - S;
+  const double kk = (c / M) * k2;
+  if (grad_coeff) grad_coeff[gf] = (float)((A / M) * k2);
+  // dA/dv = n x (opposite edge, taken cyclically) / 2
+  const int nxt[3] = {1, 2, 0}, prv[3] = {2, 0, 1};
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    const double* pn = P[nxt[v]];
+    const double* pp = P[prv[v]];
+    const double e[3] = {pp[0] - pn[0], pp[1] - pn[1], pp[2] - pn[2]};  // for a: c - b
+    const double dA[3] = {0.5 * (n[1] * e[2] - n[2] * e[1]), 0.5 * (n[2] * e[0] - n[0] * e[2]),
+                          0.5 * (n[0] * e[1] - n[1] * e[0])};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double xs = 3.141592653589793 / d.len[j];
+      contrib[9 * gf + 3 * v + j] = (float)(trisar * xs * q[3 * v + j] + kk * dA[j]);
+    }
+  }
+}
+
+// grad_verts[v] = sum over the CSR entries of v (fixed order) of contrib.
+__global__ void k_vertex_gather(int64_t nv_total, const int32_t* __restrict__ off,
+                                const int32_t* __restrict__ ent,
+                                const float* __restrict__ contrib, float* __restrict__ grad_verts) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv_total) return;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+  const int32_t b = off[v], e = off[v + 1];
+  for (int32_t i = b; i < e; ++i) {
+    const int32_t x = ent[i];
+    const float* c = contrib + 9 * (int64_t)(x / 3) + 3 * (x % 3);
+    g0 += c[0];
+    g1 += c[1];
+    g2 += c[2];
+  }
+  grad_verts[3 * v + 0] = g0;
+  grad_verts[3 * v + 1] = g1;
+  grad_verts[3 * v + 2] = g2;
+}
+
+// ---------------------------------------------------------------------------
+// Topology: vertex <- face CSR over the concatenated mesh of a launch.
+
+__global__ void k_csr_count(Cells cells, const int64_t* __restrict__ faces,
+                            int32_t* __restrict__ count, int* err) {
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  if (f >= d.nt) return;
+  const int64_t gf = d.f_off + f;
+  for (int k = 0; k < 3; ++k) {
+    const int64_t v = faces[3 * gf + k];
+    if (v < 0 || v >= d.nv) {
+      set_error(err, DM_ERR_BAD_INDEX);
+      continue;
+    }
+    atomicAdd(&count[d.v_off + v], 1);
+  }
+}
+
+// Exclusive scan of count[0..n) into off[0..n] by one block.
+__global__ void k_csr_scan(const int32_t* __restrict__ count, int32_t* __restrict__ off,
+                           int64_t n) {
+  __shared__ int32_t sh[1024];
+  const int T = blockDim.x;
+  const int64_t per = (n + T - 1) / T;
+  const int64_t b = threadIdx.x * per, e = (b + per < n) ? b + per : n;
+  int32_t s = 0;
+  for (int64_t i = b; i < e; ++i) s += count[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    int32_t v = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int32_t run = sh[threadIdx.x] - s;
+  for (int64_t i = b; i < e; ++i) {
+    off[i] = run;
+    run += count[i];
+  }
+  if (threadIdx.x == T - 1) off[n] = sh[T - 1];
+}
+
+__global__ void k_csr_fill(Cells cells, const int64_t* __restrict__ faces,
+                           const int32_t* __restrict__ off, int32_t* __restrict__ cursor,
+                           int32_t* __restrict__ ent) {
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  if (f >= d.nt) return;
+  const int64_t gf = d.f_off + f;
+  for (int k = 0; k < 3; ++k) {
+    const int64_t v = faces[3 * gf + k];
+    if (v < 0 || v >= d.nv) continue;
+    const int64_t gv = d.v_off + v;
+    const int32_t pos = off[gv] + atomicAdd(&cursor[gv], 1);
+    ent[pos] = (int32_t)(3 * gf + k);
+  }
+}
+
+// Insertion-sort each vertex's entries: a fixed summation order per vertex.
+__global__ void k_csr_sort(int64_t nv_total, const int32_t* __restrict__ off,
+                           int32_t* __restrict__ ent) {
+  const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv_total) return;
+  const int32_t b = off[v], e = off[v + 1];
+  for (int32_t i = b + 1; i < e; ++i) {
+    const int32_t x = ent[i];
+    int32_t j = i - 1;
+    while (j >= b && ent[j] > x) {
+      ent[j + 1] = ent[j];
+      --j;
+    }
+    ent[j + 1] = x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: launch plans and launchers.
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Items per launch that fill the GPU in about two waves of FwdCfg/BwdCfg CTAs.
+static int64_t target_items() { return (int64_t)num_sms() * 8; }
+
+void plan_cell_tiles(CellDesc& d) {
+  const int64_t xtile = (int64_t)FwdCfg::NT * FwdCfg::R;
+  d.xtiles = (int32_t)std::max<int64_t>(1, cdiv(d.nband, xtile));
+  int64_t fsplit = std::max<int64_t>(1, cdiv(target_items(), d.xtiles));
+  fsplit = std::min<int64_t>(fsplit, std::max<int64_t>(1, cdiv(d.nt, FwdCfg::TF)));
+  int64_t fchunk = cdiv(std::max<int64_t>(d.nt, 1), fsplit);
+  fchunk = cdiv(fchunk, FwdCfg::TF) * FwdCfg::TF;
+  d.fchunk = (int32_t)fchunk;
+  d.fsplit = (int32_t)std::max<int64_t>(1, cdiv(d.nt, fchunk));
+
+  const int64_t fblock = (int64_t)BwdCfg::NT * BwdCfg::F;
+  d.fblocks = (int32_t)std::max<int64_t>(1, cdiv(d.nt, fblock));
+  int64_t bch = std::max<int64_t>(1, cdiv(target_items(), d.fblocks));
+  bch = std::min<int64_t>(bch, std::max<int64_t>(1, cdiv(d.nband, BwdCfg::TX)));
+  int64_t bx = cdiv(std::max<int64_t>(d.nband, 1), bch);
+  bx = cdiv(bx, BwdCfg::TX) * BwdCfg::TX;
+  d.bxchunk = (int32_t)bx;
+  d.bchunks = (int32_t)std::max<int64_t>(1, cdiv(d.nband, bx));
+}
+
+void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t) {
+  t = PlanTotals{};
+  for (int i = 0; i < ncells; ++i) {
+    CellDesc& d = cells[i];
+    plan_cell_tiles(d);
+    d.v_off = t.nv;
+    d.f_off = t.nt;
+    d.b_off = t.nband;
+    d.fpart_off = t.fpart;
+    d.bpart_off = t.bpart;
+    d.face_blk0 = (int32_t)t.face_blks;
+    d.band_blk0 = (int32_t)t.band_blks;
+    d.fwd_item0 = (int32_t)t.fwd_items;
+    d.bwd_item0 = (int32_t)t.bwd_items;
+    t.nv += d.nv;
+    t.nt += d.nt;
+    t.nband += d.nband;
+    t.fpart += (int64_t)d.fsplit * d.nband;
+    t.bpart += (int64_t)d.bchunks * 10 * d.nt;
+    t.face_blks += std::max<int64_t>(1, cdiv(d.nt, kBlk));
+    t.band_blks += std::max<int64_t>(1, cdiv(d.nband, kBlk));
+    t.fwd_items += (int64_t)d.xtiles * d.fsplit;
+    t.bwd_items += (int64_t)d.fblocks * d.bchunks;
+  }
+}
+
+static int launch_status() {
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int launch_face_prep(const Cells& c, const PlanTotals& t, const float* verts, const int64_t* faces,
+                     const float* coeff, FaceRec* recs, double* area_part, int* err,
+                     cudaStream_t st) {
+  k_face_prep<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, recs, area_part, err);
+  return launch_status();
+}
+
+int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
+                   const int32_t* band_index, const double* area_part, const float* otf,
+                   float2* fpart, float2* ft_list, float2* grid, int* err, cudaStream_t st) {
+  if (t.fwd_items > 0 && t.nband > 0) {
+    k_meshft_fwd<FwdCfg::R, FwdCfg::NT, FwdCfg::TF, FwdCfg::NS>
+        <<<(unsigned)t.fwd_items, FwdCfg::NT, 0, st>>>(c, recs, band_index, fpart, err);
+    if (launch_status()) return DM_ERR_CUDA;
+  }
+  if (t.nband > 0) {
+    k_meshft_fwd_epi<<<(unsigned)t.band_blks, kBlk, 0, st>>>(c, band_index, fpart, area_part, otf,
+                                                            ft_list, grid, err);
+  }
+  return launch_status();
+}
+
+int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, const int64_t* faces,
+                    const float* coeff, const FaceRec* recs, const double* area_part,
+                    const int32_t* band_index, const float2* grad_list, const float2* grad_grid,
+                    const float* otf, float grad_scale, const float2* ft_list, XiRec* xrec,
+                    double* s_part, float* bpart, float* contrib, const int32_t* csr_off,
+                    const int32_t* csr_ent, float* grad_verts, float* grad_coeff,
+                    float* grad_otf_band, int* err, cudaStream_t st) {
+  k_bwd_band_prep<<<(unsigned)t.band_blks, kBlk, 0, st>>>(c, band_index, grad_list, grad_grid, otf,
+                                                         grad_scale, ft_list, xrec, grad_otf_band,
+                                                         s_part, err);
+  if (launch_status()) return DM_ERR_CUDA;
+  if (t.bwd_items > 0 && t.nband > 0 && t.nt > 0) {
+    cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
+    k_meshft_bwd<BwdCfg::F, BwdCfg::NT, BwdCfg::TX, BwdCfg::NS>
+        <<<(unsigned)t.bwd_items, BwdCfg::NT, 0, st>>>(c, recs, xrec, bpart, err);
+    if (launch_status()) return DM_ERR_CUDA;
+  } else if (t.bpart > 0) {
+    cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)t.bpart, st);
+  }
+  k_bwd_face_epi<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, area_part, s_part,
+                                                        bpart, contrib, grad_coeff);
+  if (launch_status()) return DM_ERR_CUDA;
+  if (t.nv > 0)
+    k_vertex_gather<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, csr_off, csr_ent, contrib,
+                                                                grad_verts);
+  return launch_status();
+}
+
+int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, int32_t* count,
+                    int32_t* off, int32_t* cursor, int32_t* ent, int* err, cudaStream_t st) {
+  cudaMemsetAsync(count, 0, sizeof(int32_t) * (size_t)(t.nv + 1), st);
+  cudaMemsetAsync(cursor, 0, sizeof(int32_t) * (size_t)(t.nv + 1), st);
+  if (t.nt > 0) k_csr_count<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, faces, count, err);
+  k_csr_scan<<<1, 1024, 0, st>>>(count, off, t.nv);
+  if (t.nt > 0) k_csr_fill<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, faces, off, cursor, ent);
+  if (t.nv > 0) k_csr_sort<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, off, ent);
+  return launch_status();
+}
+
+}  // namespace dm

@@ -1,0 +1,44 @@
+// Internal launch interface between the C ABI (capi.cu) and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dm_common.cuh"
+
+namespace dm {
+
+// Forward: R frequencies per thread, NT threads, TF faces per staged tile, NS stages.
+struct FwdCfg {
+  static constexpr int R = 4, NT = 128, TF = 64, NS = 3;
+};
+// Backward: F faces per thread, NT threads, TX frequencies per staged tile, NS stages.
+struct BwdCfg {
+  static constexpr int F = 2, NT = 128, TX = 128, NS = 3;
+};
+
+// Totals of a batched plan (sums over cells).
+struct PlanTotals {
+  int64_t nv, nt, nband, fpart, bpart, face_blks, band_blks, fwd_items, bwd_items;
+};
+
+int num_sms();
+void plan_cell_tiles(CellDesc& d);
+void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t);
+
+int launch_face_prep(const Cells& c, const PlanTotals& t, const float* verts, const int64_t* faces,
+                     const float* coeff, FaceRec* recs, double* area_part, int* err,
+                     cudaStream_t st);
+int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
+                   const int32_t* band_index, const double* area_part, const float* otf,
+                   float2* fpart, float2* ft_list, float2* grid, int* err, cudaStream_t st);
+int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, const int64_t* faces,
+                    const float* coeff, const FaceRec* recs, const double* area_part,
+                    const int32_t* band_index, const float2* grad_list, const float2* grad_grid,
+                    const float* otf, float grad_scale, const float2* ft_list, XiRec* xrec,
+                    double* s_part, float* bpart, float* contrib, const int32_t* csr_off,
+                    const int32_t* csr_ent, float* grad_verts, float* grad_coeff,
+                    float* grad_otf_band, int* err, cudaStream_t st);
+int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, int32_t* count,
+                    int32_t* off, int32_t* cursor, int32_t* ent, int* err, cudaStream_t st);
+
+}  // namespace dm

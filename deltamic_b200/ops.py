@@ -1,0 +1,244 @@
+"""Autograd operators over the C ABI: narrow band, meshFT, Gaussian OTF, image loss.
+
+Every operator here launches the kernels of ``libdeltamic_b200.so`` on the current
+CUDA stream; none has a CPU or PyTorch fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+__all__ = ["FreqGrid", "narrowband", "topology", "meshft", "meshft_list",
+           "meshft_backward_list", "gaussian_otf", "image_loss", "adam_step"]
+
+
+class FreqGrid:
+    """Box and shape of a centred frequency grid (render.py:153-172).
+
+    ``box_size`` is a [3,2] array-like (lower, upper corner per axis); it is kept
+    in float64 for the kernels' phase arithmetic.
+    """
+
+    def __init__(self, box_size, box_shape):
+        b = np.asarray(torch.as_tensor(box_size).detach().cpu().double().numpy(), np.float64)
+        if b.shape != (3, 2):
+            raise ValueError("box_size must have shape [3, 2]")
+        self.box_size = b
+        self.shape = tuple(int(s) for s in box_shape)
+        if len(self.shape) != 3 or min(self.shape) <= 0:
+            raise ValueError("box_shape must be 3 positive integers")
+        self.numel = int(np.prod(self.shape))
+        self.cbox = N.make_box(b, self.shape)
+
+    def axes(self, dtype=torch.float32, device="cuda"):
+        """xi0, xi1, xi2 as Fourier3dMesh computes them (in ``dtype``)."""
+        bs = torch.tensor(self.box_size, dtype=dtype, device=device)
+        out = []
+        for d in range(3):
+            n = self.shape[d]
+            s = np.pi / (bs[d, 1] - bs[d, 0])
+            k = torch.arange(n, dtype=dtype, device=device)
+            out.append((2 * k - (n - 1)) * s)
+        return tuple(out)
+
+
+# ---------------------------------------------------------------------------
+# narrow band
+
+def narrowband(otf: torch.Tensor, thresh: float) -> torch.Tensor:
+    """Flat C-order indices (int32) of ``otf > thresh``; synchronises to learn the count."""
+    otf = otf.detach()
+    N.require_cuda(otf, "OTF", torch.float32)
+    otf = otf.contiguous()
+    n = otf.numel()
+    lib = N.lib()
+    idx = torch.empty(max(n, 1), dtype=torch.int32, device=otf.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=otf.device)
+    ws = N.WORKSPACES.get("band", lib.dm_narrowband_workspace_size(n), otf.device)
+    N.check(lib.dm_narrowband_compact(N.ptr(otf), n, float(thresh), N.ptr(idx), N.ptr(cnt),
+                                      N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
+            "dm_narrowband_compact")
+    c = int(cnt.item())
+    return idx[:c].clone()
+
+
+# ---------------------------------------------------------------------------
+# topology cache (vertex <- face CSR), keyed by the faces tensor
+
+_TOPO: "weakref.WeakKeyDictionary[torch.Tensor, tuple]" = weakref.WeakKeyDictionary()
+
+
+def topology(faces: torch.Tensor, nv: int) -> torch.Tensor:
+    """CSR incidence buffer for ``faces`` (built once; face indices validated)."""
+    key = (faces._version, int(nv), faces.data_ptr())
+    hit = _TOPO.get(faces)
+    if hit is not None and hit[0] == key:
+        return hit[1]
+    lib = N.lib()
+    nt = faces.shape[0]
+    if nt:
+        lo, hi = int(faces.min()), int(faces.max())
+        if lo < 0 or hi >= nv:
+            raise IndexError(f"face index out of range [0, {nv}): min {lo}, max {hi}")
+    buf = torch.zeros(lib.dm_topology_size(nv, nt), dtype=torch.uint8, device=faces.device)
+    N.check(lib.dm_topology_build(N.ptr(faces), nt, nv, N.ptr(buf), buf.numel(),
+                                  N.stream_ptr(faces.device)), "dm_topology_build")
+    _TOPO[faces] = (key, buf)
+    return buf
+
+
+def _check_mesh(verts, faces, coeff):
+    N.require_cuda(verts, "Verts", torch.float32)
+    N.require_cuda(faces, "Faces", torch.int64)
+    N.require_cuda(coeff, "Faces_coeff", torch.float32)
+    if verts.dim() != 2 or verts.shape[1] != 3:
+        raise ValueError("Verts must have shape [nv, 3]")
+    if faces.dim() != 2 or faces.shape[1] != 3:
+        raise ValueError("Faces must have shape [nt, 3]")
+    if coeff.shape != (faces.shape[0],):
+        raise ValueError("Faces_coeff must have shape [nt]")
+
+
+def meshft_list(verts, faces, coeff, grid: FreqGrid, band, otf=None, spectrum=None):
+    """Forward only: ft_list[n_band] (complex64); optionally scatter ft*otf into ``spectrum``."""
+    lib = N.lib()
+    nv, nt, nb = verts.shape[0], faces.shape[0], band.numel()
+    ft = torch.empty(nb, dtype=torch.complex64, device=verts.device)
+    ws = N.WORKSPACES.get("fwd", lib.dm_meshft_forward_workspace_size(nv, nt, nb), verts.device)
+    N.check(lib.dm_meshft_forward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(grid.cbox), N.ptr(band),
+        nb, N.ptr(otf), N.ptr(ft), N.ptr(spectrum), N.ptr(ws), ws.numel(),
+        N.stream_ptr(verts.device)), "dm_meshft_forward")
+    return ft
+
+
+def meshft_backward_list(verts, faces, coeff, grid: FreqGrid, band, ft, grad_list=None,
+                         grad_grid=None, otf=None, scale=1.0, want_coeff=True, want_otf=False):
+    """Backward only: (grad_verts, grad_coeff | None, grad_otf_band | None)."""
+    lib = N.lib()
+    nv, nt, nb = verts.shape[0], faces.shape[0], band.numel()
+    gv = torch.empty_like(verts)
+    gc = torch.empty_like(coeff) if want_coeff else None
+    go = torch.empty(nb, dtype=torch.float32, device=verts.device) if want_otf else None
+    topo = topology(faces, nv)
+    ws = N.WORKSPACES.get("bwd", lib.dm_meshft_backward_workspace_size(nv, nt, nb), verts.device)
+    N.check(lib.dm_meshft_backward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(grid.cbox), N.ptr(band), nb,
+        N.ptr(grad_list), N.ptr(grad_grid), N.ptr(otf), float(scale), N.ptr(ft), N.ptr(topo),
+        N.ptr(gv), N.ptr(gc), N.ptr(go), N.ptr(ws), ws.numel(), N.stream_ptr(verts.device)),
+        "dm_meshft_backward")
+    return gv, gc, go
+
+
+class _MeshFT(torch.autograd.Function):
+    """Dense meshFT: complex64 grid, ft on the band and 0 elsewhere (cuda_class.py:16-41)."""
+
+    @staticmethod
+    def forward(ctx, verts, faces, coeff, grid, band):
+        out = torch.zeros(grid.shape, dtype=torch.complex64, device=verts.device)
+        ft = meshft_list(verts, faces, coeff, grid, band, spectrum=out)
+        ctx.save_for_backward(verts, faces, coeff, band, ft)
+        ctx.grid = grid
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        verts, faces, coeff, band, ft = ctx.saved_tensors
+        g = g.contiguous()
+        if g.dtype != torch.complex64:
+            g = g.to(torch.complex64)
+        gv, gc, _ = meshft_backward_list(verts, faces, coeff, ctx.grid, band, ft, grad_grid=g,
+                                         want_coeff=ctx.needs_input_grad[2])
+        return gv, None, gc, None, None
+
+
+def meshft(verts, faces, coeff, grid: FreqGrid, band) -> torch.Tensor:
+    """Differentiable dense meshFT (gradients for verts and coeff)."""
+    _check_mesh(verts, faces, coeff)
+    return _MeshFT.apply(verts.contiguous(), faces.contiguous(), coeff.contiguous(), grid, band)
+
+
+# ---------------------------------------------------------------------------
+# Gaussian OTF
+
+class _GaussianOTF(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, sigma, x0, x1, x2):
+        lib = N.lib()
+        n = (x0.numel(), x1.numel(), x2.numel())
+        otf = torch.empty(n, dtype=torch.float32, device=sigma.device)
+        N.check(lib.dm_gaussian_otf(N.ptr(sigma), N.ptr(x0), n[0], N.ptr(x1), n[1], N.ptr(x2),
+                                    n[2], N.ptr(otf), N.stream_ptr(sigma.device)),
+                "dm_gaussian_otf")
+        ctx.save_for_backward(otf, x0, x1, x2)
+        return otf
+
+    @staticmethod
+    def backward(ctx, g):
+        otf, x0, x1, x2 = ctx.saved_tensors
+        if not ctx.needs_input_grad[0]:
+            return None, None, None, None
+        return sigma_grad_dense(g.contiguous().float(), otf, x0, x1, x2), None, None, None
+
+
+def sigma_grad_dense(gotf, otf, x0, x1, x2, band=None):
+    """d loss/d sigma from an OTF gradient (dense, or on ``band`` indices)."""
+    lib = N.lib()
+    n = band.numel() if band is not None else otf.numel()
+    gs = torch.empty(3, 3, dtype=torch.float32, device=otf.device)
+    ws = N.WORKSPACES.get("otfgrad", lib.dm_gaussian_otf_grad_workspace_size(n), otf.device)
+    N.check(lib.dm_gaussian_otf_sigma_grad(
+        N.ptr(gotf), N.ptr(band), n, N.ptr(otf), N.ptr(x0), x0.numel(), N.ptr(x1), x1.numel(),
+        N.ptr(x2), x2.numel(), N.ptr(gs), N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
+        "dm_gaussian_otf_sigma_grad")
+    return gs
+
+
+def gaussian_otf(sigma, xi0, xi1, xi2) -> torch.Tensor:
+    N.require_cuda(sigma, "sigma")
+    sigma = sigma.float().contiguous()
+    if sigma.shape != (3, 3):
+        raise ValueError("sigma must be a 3x3 matrix")
+    axes = []
+    for name, x in (("xi0", xi0), ("xi1", xi1), ("xi2", xi2)):
+        N.require_cuda(x, name)
+        axes.append(x.detach().float().contiguous())
+    return _GaussianOTF.apply(sigma, *axes)
+
+
+# ---------------------------------------------------------------------------
+# fused image stage and Adam
+
+LOSS_KINDS = {"sum": 0, "mse": 1}
+
+
+def image_loss(z, kind="sum", target=None, contrast=0.0, want_grad=True, want_image=False):
+    """(loss[1], image | None, dL/dz | None) for z = ifftn(ftmesh*OTF), complex64."""
+    lib = N.lib()
+    N.require_cuda(z, "z", torch.complex64)
+    n = z.numel()
+    k = LOSS_KINDS[kind]
+    if k == 1:
+        N.require_cuda(target, "target", torch.float32)
+        if target.numel() != n:
+            raise ValueError("target must have the image's shape")
+    loss = torch.empty(1, dtype=torch.float32, device=z.device)
+    img = torch.empty(z.shape, dtype=torch.float32, device=z.device) if want_image else None
+    gz = torch.empty_like(z) if want_grad else None
+    ws = N.WORKSPACES.get("img", lib.dm_image_loss_workspace_size(n), z.device)
+    N.check(lib.dm_image_loss(N.ptr(z), n, k, N.ptr(target), float(contrast), N.ptr(img),
+                              N.ptr(loss), N.ptr(gz), N.ptr(ws), ws.numel(),
+                              N.stream_ptr(z.device)), "dm_image_loss")
+    return loss, img, gz
+
+
+def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+    lib = N.lib()
+    N.check(lib.dm_adam_step(N.ptr(param), N.ptr(grad), N.ptr(exp_avg), N.ptr(exp_avg_sq),
+                             param.numel(), float(lr), float(beta1), float(beta2), float(eps),
+                             N.ptr(step), N.stream_ptr(param.device)), "dm_adam_step")

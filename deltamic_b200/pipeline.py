@@ -1,0 +1,116 @@
+"""Fused render-and-loss path: meshFT (with the OTF multiply in its epilogue) ->
+inverse FFT (cuFFT) -> |.| / normalize_tensor / loss and dL/dz in one pass ->
+forward FFT of dL/dz -> meshFT adjoint.
+
+This is the chain ``normalize_tensor(render_image_from_ftmesh(meshFT(V,F,c), OTF))``
+of the reference fitting loop (``Examples/Gradient_Descent.ipynb`` cell 2) with
+the dense complex spectrum kept resident: only band voxels of the spectrum are
+ever written, so it is zeroed once per narrow band, not per step.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import ops
+
+__all__ = ["MeshRenderer"]
+
+
+class MeshRenderer:
+    """Renderer for one box: holds the frequency grid, the OTF and its narrow band."""
+
+    def __init__(self, box_size, box_shape, narrowband_thresh=1e-5, device="cuda"):
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise RuntimeError("MeshRenderer runs on CUDA devices only")
+        self.grid = ops.FreqGrid(box_size, box_shape)
+        self.shape = self.grid.shape
+        self.thresh = float(narrowband_thresh)
+        self.xi = self.grid.axes(torch.float32, self.device)
+        c64 = dict(dtype=torch.complex64, device=self.device)
+        self.spec = torch.zeros(self.shape, **c64)     # ft * OTF on the band, 0 elsewhere
+        self.z = torch.empty(self.shape, **c64)        # ifftn(spec)
+        self.G = torch.empty(self.shape, **c64)        # fftn(dL/dz)
+        self.otf = None
+        self.band = None
+        self._sigma_key = None
+
+    @property
+    def numel(self) -> int:
+        return self.grid.numel
+
+    # -- PSF / band -----------------------------------------------------------
+    def set_otf(self, otf: torch.Tensor) -> None:
+        """Use ``otf`` (float32, box_shape) and recompute the narrow band."""
+        self.otf = otf.detach().float().contiguous()
+        self.band = ops.narrowband(self.otf, self.thresh)
+        self.spec.zero_()
+        self._sigma_key = None
+
+    def set_sigma(self, sigma: torch.Tensor) -> None:
+        """Gaussian OTF of ``sigma`` (psf.py:15-20) and its narrow band."""
+        s = sigma.detach().float().contiguous()
+        key = (s.data_ptr(), s._version)
+        if key == self._sigma_key and self.otf is not None:
+            return
+        with torch.no_grad():
+            otf = ops.gaussian_otf(s, *self.xi)
+        self.set_otf(otf)
+        self._sigma_key = key
+
+    @property
+    def n_band(self) -> int:
+        return 0 if self.band is None else int(self.band.numel())
+
+    # -- forward only ----------------------------------------------------------
+    @torch.no_grad()
+    def render(self, verts, faces, coeff) -> torch.Tensor:
+        """|ifftn(meshFT * OTF)| as a new float32 tensor (no normalisation)."""
+        self._require_band()
+        ops.meshft_list(verts, faces, coeff, self.grid, self.band, otf=self.otf,
+                        spectrum=self.spec)
+        torch.fft.ifftn(self.spec, out=self.z)
+        return self.z.abs()
+
+    def loss(self, verts, faces, coeff, kind="sum", target=None, contrast=0.0, sigma=None):
+        """Differentiable loss of the normalised render (grads: verts, coeff, sigma)."""
+        if sigma is not None:
+            self.set_sigma(sigma)
+        else:
+            sigma = torch.zeros(0, device=self.device)
+        self._require_band()
+        ops._check_mesh(verts, faces, coeff)
+        return _RenderLoss.apply(verts.contiguous(), coeff.contiguous(), sigma, self,
+                                 faces.contiguous(), kind, target, float(contrast))
+
+    def _require_band(self):
+        if self.band is None:
+            raise RuntimeError("call set_otf() or set_sigma() first")
+
+
+class _RenderLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, verts, coeff, sigma, r: MeshRenderer, faces, kind, target, contrast):
+        ft = ops.meshft_list(verts, faces, coeff, r.grid, r.band, otf=r.otf, spectrum=r.spec)
+        torch.fft.ifftn(r.spec, out=r.z)
+        loss, _, gz = ops.image_loss(r.z, kind, target, contrast, want_grad=True)
+        ctx.save_for_backward(verts, coeff, faces, ft, gz)
+        ctx.r = r
+        ctx.sigma_grad = sigma.numel() == 9 and ctx.needs_input_grad[2]
+        return loss.view(())
+
+    @staticmethod
+    def backward(ctx, gl):
+        verts, coeff, faces, ft, gz = ctx.saved_tensors
+        r = ctx.r
+        torch.fft.fftn(gz, out=r.G)
+        gv, gc, go = ops.meshft_backward_list(
+            verts, faces, coeff, r.grid, r.band, ft, grad_grid=r.G, otf=r.otf,
+            scale=1.0 / r.numel, want_coeff=ctx.needs_input_grad[1], want_otf=ctx.sigma_grad)
+        gv = gv * gl
+        if gc is not None:
+            gc = gc * gl
+        gs = None
+        if ctx.sigma_grad:
+            gs = ops.sigma_grad_dense(go, r.otf, *r.xi, band=r.band) * gl
+        return gv, gc, gs, None, None, None, None, None

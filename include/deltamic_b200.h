@@ -1,0 +1,163 @@
+/*
+ * deltamic_b200 -- C ABI of the B200 (sm_100a) mesh Fourier transform,
+ * narrow-band, OTF and image-loss kernels.
+ *
+ * Conventions for every entry point:
+ *  - all array arguments are DEVICE pointers (caller-owned, borrowed for the
+ *    duration of the stream work), row-major and contiguous;
+ *  - complex arrays are interleaved float pairs (re, im), i.e. complex64;
+ *  - work is enqueued on ``stream`` and nothing synchronises, except the calls
+ *    documented as synchronous (dm_device_error);
+ *  - scratch memory is passed in as ``workspace`` / ``ws_bytes``; sizes come
+ *    from the matching *_workspace_size query; nothing allocates device memory;
+ *  - the return value is a status: 0 (DM_OK) or an OR of DM_ERR_* bits.  Host
+ *    side argument checks return before anything is enqueued.  Faults detected
+ *    on the device (out-of-range face indices, a bounded wait that ran out) set
+ *    bits in a status word inside the workspace, read with dm_device_error.
+ *
+ * Frequencies are the centred grid of Fourier3dMesh (deltamic/render.py:153-172):
+ *   xi_d[k] = (2k - (n_d - 1)) * pi / (box.hi[d] - box.lo[d]),  k = 0..n_d-1,
+ * and a narrow band is a list of flat C-order voxel indices into that grid.
+ */
+#ifndef DELTAMIC_B200_H_
+#define DELTAMIC_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dm_stream_t; /* == cudaStream_t */
+
+#define DM_OK 0
+#define DM_ERR_INVALID_ARG 1   /* null pointer, negative size, bad dtype ... */
+#define DM_ERR_BAD_INDEX 2     /* a face index outside [0, nv) */
+#define DM_ERR_SIZE 4          /* a size beyond what the kernels index (int32 voxels) */
+#define DM_ERR_WORKSPACE 8     /* workspace smaller than the query returned */
+#define DM_ERR_CUDA 16         /* a CUDA launch or copy failed */
+#define DM_ERR_TIMEOUT 32      /* a bounded device wait gave up */
+#define DM_ERR_UNSUPPORTED 64  /* valid request this build does not serve */
+
+/* Box of a meshFT grid: box_size (render.py:116-123) and box_shape. */
+typedef struct dm_box {
+  double lo[3];     /* box_size[:,0] */
+  double hi[3];     /* box_size[:,1] */
+  int32_t shape[3]; /* box_shape */
+  int32_t reserved;
+} dm_box;
+
+/* ABI version of this header (bumped on any signature change). */
+int dm_abi_version(void);
+
+/* Human-readable name of the lowest set error bit of ``status``. */
+const char* dm_status_string(int status);
+
+/* Synchronous: waits for ``stream``, then returns the device status word held in
+ * a workspace of any of the calls below (and clears it).  *out_flags receives
+ * the DM_ERR_* bits raised on the device. */
+int dm_device_error(void* workspace, int* out_flags, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Narrow band.  Replaces the selection in MeshFTCUDA.forward
+ * (deltamic/cuda_class.py:21-24): bool_filter = Filter > thresh, then the
+ * frequency list gathered in C order.
+ * band_index[0..count) receives the flat indices of voxels with otf > thresh in
+ * ascending order (capacity n_voxels); *band_count (DEVICE int64) the count. */
+size_t dm_narrowband_workspace_size(int64_t n_voxels);
+int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh,
+                          int32_t* band_index, int64_t* band_count, void* workspace,
+                          size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Vertex <- face incidence (CSR), built once per topology.  Replaces the host
+ * loop that fills triangles_belonging_to_vertex_map / index_of_vertex_in_triangles
+ * (deltamic/cpp/fourier3d_cuda_kernel.cu:487-501) without its 30-faces-per-vertex
+ * cap.  Entries of a vertex are sorted by (face, corner), so the backward's
+ * per-vertex sums run in a fixed order. */
+size_t dm_topology_size(int64_t nv, int64_t nt);
+int dm_topology_build(const int64_t* faces, int64_t nt, int64_t nv, void* topology,
+                      size_t topo_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * meshFT forward.  Replaces forward_fourier3d_cpp
+ * (deltamic/cpp/fourier3d_cuda.cpp:27-42, :112-113; kernel .cu:281-311, host
+ * prep .cu:42-51, :421-462) for frequencies on the grid of ``box``.
+ *   verts[nv,3] float32 (unshifted: the box.lo shift of Fourier3dMesh.forward,
+ *   render.py:144/148, is applied inside), faces[nt,3] int64, faces_coeff[nt],
+ *   band_index[n_band] from dm_narrowband_compact.
+ * Writes ft_list[n_band] (complex64).  If ``grid`` is not NULL it also writes
+ * grid[band_index[m]] = ft_list[m] * (otf ? otf[band_index[m]] : 1); other grid
+ * elements are left untouched (the caller zeroes the grid once). */
+size_t dm_meshft_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band);
+int dm_meshft_forward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                      const float* faces_coeff, const dm_box* box, const int32_t* band_index,
+                      int64_t n_band, const float* otf, float* ft_list, float* grid,
+                      void* workspace, size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * meshFT backward.  Replaces backward_fourier3d_cpp
+ * (deltamic/cpp/fourier3d_cuda.cpp:44-65, :114; kernels .cu:314-416, host prep
+ * .cu:16-36, :466-539) and adds the Faces_coeff and OTF gradients the reference
+ * gets only from CPU autograd.
+ * The cotangent on the band (PyTorch convention, dL/dRe + i dL/dIm) is
+ *   g[m] = grad_scale * G[m] * (otf ? otf[band_index[m]] : 1),
+ * with G[m] = grad_list[m] if grad_list != NULL, else grad_grid[band_index[m]].
+ * ft_list is the forward's output.  topology from dm_topology_build (NULL: built
+ * in the workspace on every call).
+ * Writes grad_verts[nv,3]; optionally grad_coeff[nt] and
+ * grad_otf_band[m] = grad_scale * Re(conj(G[m]) ft_list[m]). */
+size_t dm_meshft_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band);
+int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                       const float* faces_coeff, const dm_box* box, const int32_t* band_index,
+                       int64_t n_band, const float* grad_list, const float* grad_grid,
+                       const float* otf, float grad_scale, const float* ft_list,
+                       const void* topology, float* grad_verts, float* grad_coeff,
+                       float* grad_otf_band, void* workspace, size_t ws_bytes,
+                       dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Gaussian OTF.  Replaces generate_gaussian_psf (deltamic/psf.py:15-20):
+ *   otf[i,j,k] = exp(-(x^T S x)/2),  x = (xi0[i], xi1[j], xi2[k]),
+ * S = sigma[3,3] (DEVICE float32, row-major, as the torch parameter), on the
+ * outer grid of the three DEVICE float32 axes (Fourier3dMesh.xi0/xi1/xi2),
+ * evaluated with the reference expression's float32 operation order. */
+int dm_gaussian_otf(const float* sigma, const float* xi0, int32_t n0, const float* xi1,
+                    int32_t n1, const float* xi2, int32_t n2, float* otf, dm_stream_t stream);
+
+/* d loss / d sigma for that OTF: grad_sigma[i*3+j] = sum over voxels of
+ * grad_otf * otf * (-x_i x_j / 2).  Dense form (band_index NULL: grad_otf[n0 n1 n2])
+ * or band form (grad_otf[n_band] holds the values at voxels band_index[m]). */
+size_t dm_gaussian_otf_grad_workspace_size(int64_t n);
+int dm_gaussian_otf_sigma_grad(const float* grad_otf, const int32_t* band_index, int64_t n_band,
+                               const float* otf, const float* xi0, int32_t n0, const float* xi1,
+                               int32_t n1, const float* xi2, int32_t n2, float* grad_sigma,
+                               void* workspace, size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Fused image stage on the inverse FFT z = ifftn(ftmesh * OTF) (complex64[n]):
+ * image = |z| (render_image_from_ftmesh, render.py:177-180), normalised by
+ * normalize_tensor (render.py:5-6) with ``contrast``, then the loss
+ *   kind 0: sum(normalised image)
+ *   kind 1: mean((normalised image - target)^2)
+ * Writes *loss (DEVICE float), optionally image[n] = |z|, and, if grad_z is not
+ * NULL, dL/dz in PyTorch's complex convention (ties of the min / max share
+ * their gradient evenly, as torch's full min/max reductions do). */
+size_t dm_image_loss_workspace_size(int64_t n);
+int dm_image_loss(const float* z, int64_t n, int kind, const float* target, float contrast,
+                  float* image, float* loss, float* grad_z, void* workspace, size_t ws_bytes,
+                  dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Adam step (torch.optim.Adam semantics, no weight decay) on a float32 array;
+ * ``step`` is a DEVICE int64 counter that the call increments (1-based after). */
+int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
+                 float lr, float beta1, float beta2, float eps, int64_t* step,
+                 dm_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DELTAMIC_B200_H_ */

@@ -1,0 +1,208 @@
+"""CUDA meshFT forward / adjoint against the float64 oracle and the reference's
+golden vectors.  Tolerances (rel-L2, float32 kernels vs float64):
+  ft_list 1e-5, vertex gradient 1e-4, Faces_coeff gradient 1e-5."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import load_golden, rel_l2
+from deltamic_b200 import ops
+from deltamic_b200.mesh import icosphere, jitter, random_sh_shape
+
+pytestmark = pytest.mark.gpu
+
+TOL_FT = 1e-5
+TOL_GV = 1e-4
+TOL_GC = 1e-5
+
+DEV = "cuda:0"
+
+
+def _t(a, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+def _setup(v, f, c, box, shape, sigma, thresh):
+    grid = ops.FreqGrid(box, shape)
+    xi = grid.axes(torch.float32, DEV)
+    otf = ops.gaussian_otf(_t(sigma), *xi)
+    band = ops.narrowband(otf, thresh)
+    return grid, xi, otf, band
+
+
+def _oracle_xi(grid, band):
+    axes = oracle.frequency_axes(grid.box_size, grid.shape)
+    return oracle.xi_list_from_band(band.cpu().numpy().astype(np.int64), axes)
+
+
+def _case(level=2, shape=(24, 24, 24), seed=0, sigma=None, thresh=1e-5):
+    v, f = random_sh_shape(level, 0.3, 4, 0.08, seed)
+    rng = np.random.default_rng(seed + 100)
+    c = rng.uniform(0.5, 1.5, len(f))
+    box = oracle.compute_box_size(v, 0.2)
+    sigma = np.diag([1e-3, 1e-3, 4e-3]) if sigma is None else sigma
+    return v, f, c, box, shape, sigma, thresh
+
+
+@pytest.mark.parametrize("level,shape", [(1, (16, 16, 16)), (2, (24, 20, 18)), (3, (33, 33, 33))])
+def test_forward_matches_oracle(level, shape):
+    v, f, c, box, shape, sigma, thresh = _case(level, shape)
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    ft = ops.meshft_list(_t(v), _t(f, torch.int64), _t(c), grid, band)
+    xil = _oracle_xi(grid, band)
+    ref = oracle.meshft_forward(v - box[:, 0], f, c, xil)
+    assert rel_l2(ft.cpu().numpy(), ref) < TOL_FT
+
+
+@pytest.mark.parametrize("level,shape", [(1, (16, 16, 16)), (2, (24, 20, 18)), (3, (25, 25, 25))])
+def test_backward_matches_oracle(level, shape):
+    v, f, c, box, shape, sigma, thresh = _case(level, shape, seed=1)
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    ft = ops.meshft_list(V, F, C, grid, band)
+    rng = np.random.default_rng(7)
+    g = (rng.normal(size=band.numel()) + 1j * rng.normal(size=band.numel()))
+    g = g * np.exp(-0.5 * np.linalg.norm(_oracle_xi(grid, band), axis=1) ** 2 * 1e-4)
+    gv, gc, _ = ops.meshft_backward_list(V, F, C, grid, band, ft,
+                                         grad_list=_t(g, torch.complex64))
+    xil = _oracle_xi(grid, band)
+    ft64 = oracle.meshft_forward(v - box[:, 0], f, c, xil)
+    rv, rc = oracle.meshft_backward(v - box[:, 0], f, c, xil, g.astype(np.complex64), ft64)
+    assert rel_l2(gv.cpu().numpy(), rv) < TOL_GV
+    assert rel_l2(gc.cpu().numpy(), rc) < TOL_GC
+
+
+def test_drop_in_chain_matches_reference_golden(golden):
+    """Fourier3dMesh -> render_image_from_ftmesh -> normalize_tensor -> loss ->
+    backward, against the reference's float64 autograd (golden vectors)."""
+    import deltamic_b200 as dm
+    name, d = golden
+    shape = tuple(int(s) for s in d["box_shape"])
+    V = _t(d["verts"]).requires_grad_(True)
+    F = _t(d["faces"], torch.int64)
+    C = _t(d["coeff"]).requires_grad_(True)
+    S = _t(d["sigma"]).requires_grad_(True)
+    mft = dm.Fourier3dMesh(torch.tensor(d["box_size"]), shape, device=DEV,
+                           narrowband_thresh=float(d["thresh"]))
+    otf = dm.generate_gaussian_psf(S, mft.xi0, mft.xi1, mft.xi2)
+    mft.OTF = otf.detach()
+    ft = mft(V, F, C)
+    img = dm.render_image_from_ftmesh(ft, otf, shape)
+    nimg = dm.normalize_tensor(img)
+    if str(d["loss_kind"]) == "sum":
+        loss = nimg.sum()
+    else:
+        loss = torch.mean((nimg - _t(d["target"])) ** 2)
+    loss.backward()
+    band = mft.band().cpu().numpy()
+    common, ia, ib = np.intersect1d(band, d["idx"], return_indices=True)
+    assert len(common) >= 0.999 * len(d["idx"])
+    ftb = ft.detach().reshape(-1).cpu().numpy()[common]
+    assert rel_l2(ftb, d["ft"][ib]) < TOL_FT, name
+    assert rel_l2(img.detach().cpu().numpy(), d["image"]) < TOL_FT, name
+    assert abs(float(loss) - float(d["loss"])) < 1e-4 * abs(float(d["loss"])), name
+    assert rel_l2(V.grad.cpu().numpy(), d["grad_verts"]) < 2e-4, name
+    assert rel_l2(C.grad.cpu().numpy(), d["grad_coeff"]) < 1e-4, name
+    assert rel_l2(S.grad.cpu().numpy(), d["grad_sigma"]) < 1e-4, name
+    # the reference's own float32 path is much further away on the vertex gradient
+    print(name, "vertex grad rel-L2: ours %.2e, reference f32 %.2e" % (
+        rel_l2(V.grad.cpu().numpy(), d["grad_verts"]),
+        rel_l2(d["grad_verts_f32"], d["grad_verts"])))
+
+
+def test_deterministic_bitwise():
+    v, f, c, box, shape, sigma, thresh = _case(3, (32, 32, 32), seed=4)
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    g = torch.randn(band.numel(), dtype=torch.complex64, device=DEV)
+    outs = []
+    for _ in range(2):
+        ft = ops.meshft_list(V, F, C, grid, band)
+        gv, gc, _ = ops.meshft_backward_list(V, F, C, grid, band, ft, grad_list=g)
+        outs.append((ft.clone(), gv.clone(), gc.clone()))
+    for a, b in zip(outs[0], outs[1]):
+        assert torch.equal(a, b)
+
+
+def test_empty_band_and_tiny_meshes():
+    v, f, c, box, shape, sigma, thresh = _case(1, (12, 12, 12))
+    grid, xi, otf, _ = _setup(v, f, c, box, shape, sigma, thresh)
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    empty = ops.narrowband(otf, 2.0)
+    assert empty.numel() == 0
+    ft = ops.meshft_list(V, F, C, grid, empty)
+    assert ft.numel() == 0
+    gv, gc, _ = ops.meshft_backward_list(V, F, C, grid, empty, ft,
+                                         grad_list=torch.zeros(0, dtype=torch.complex64,
+                                                               device=DEV))
+    assert torch.count_nonzero(gv) == 0 and torch.count_nonzero(gc) == 0
+    # a single face
+    band = ops.narrowband(otf, 1e-5)
+    ft1 = ops.meshft_list(V, F[:1].contiguous(), C[:1].contiguous(), grid, band)
+    xil = _oracle_xi(grid, band)
+    ref = oracle.meshft_forward(v - box[:, 0], f[:1], c[:1], xil)
+    assert rel_l2(ft1.cpu().numpy(), ref) < TOL_FT
+
+
+def test_bad_face_index_raises():
+    v, f, c, box, shape, sigma, thresh = _case(1, (12, 12, 12))
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    V, C = _t(v), _t(c)
+    fbad = f.copy()
+    fbad[3, 1] = len(v) + 5
+    F = _t(fbad, torch.int64)
+    ft = ops.meshft_list(V, F, C, grid, band)  # forward clamps and flags
+    with pytest.raises(IndexError):
+        ops.meshft_backward_list(V, F, C, grid, band, ft,
+                                 grad_list=torch.ones(band.numel(), dtype=torch.complex64,
+                                                      device=DEV))
+
+
+def test_degenerate_cube_on_odd_grid():
+    d = load_golden("cube_degenerate")
+    shape = tuple(int(s) for s in d["box_shape"])
+    grid, xi, otf, band = _setup(d["verts"], d["faces"], d["coeff"], d["box_size"], shape,
+                                 d["sigma"], float(d["thresh"]))
+    V, F, C = _t(d["verts"]), _t(d["faces"], torch.int64), _t(d["coeff"])
+    ft = ops.meshft_list(V, F, C, grid, band)
+    xil = _oracle_xi(grid, band)
+    vs = d["verts"] - d["box_size"][:, 0]
+    ref = oracle.meshft_forward(vs, d["faces"], d["coeff"], xil)
+    assert rel_l2(ft.cpu().numpy(), ref) < TOL_FT
+    # xi = 0 is on the odd grid: ft(0) = 1
+    k0 = np.ravel_multi_index(tuple(s // 2 for s in shape), shape)
+    pos = np.searchsorted(band.cpu().numpy(), k0)
+    assert abs(complex(ft[pos].cpu()) - 1.0) < 1e-6
+    g = np.exp(1j * np.arange(band.numel()) * 0.1) * otf.reshape(-1)[band.long()].cpu().numpy()
+    gv, gc, _ = ops.meshft_backward_list(V, F, C, grid, band, ft,
+                                         grad_list=_t(g, torch.complex64))
+    rv, rc = oracle.meshft_backward(vs, d["faces"], d["coeff"], xil, g, ref)
+    assert rel_l2(gv.cpu().numpy(), rv) < TOL_GV
+    assert rel_l2(gc.cpu().numpy(), rc) < TOL_GC
+
+
+def test_full_size_properties_200cube_20480_faces():
+    """Size-independent checks at the fit configuration (200^3, level-5 SH shape):
+    translation -> phase, Faces_coeff scale invariance, and oracle agreement on a
+    random subsample of the band."""
+    v, f = random_sh_shape(5, 0.3, 6, 0.08, seed=11)
+    box = oracle.compute_box_size(v, 0.2)
+    shape = (200, 200, 200)
+    grid, xi, otf, band = _setup(v, f, np.ones(len(f)), box, shape,
+                                 np.diag([1e-3, 1e-3, 4e-3]), 1e-5)
+    assert 10000 < band.numel() < 20000
+    V, F = _t(v), _t(f, torch.int64)
+    C = torch.ones(len(f), device=DEV)
+    ft = ops.meshft_list(V, F, C, grid, band)
+    ft2 = ops.meshft_list(V, F, C * 3.7, grid, band)
+    assert rel_l2(ft2.cpu().numpy(), ft.cpu().numpy()) < 2e-6
+    t = np.array([0.011, -0.007, 0.003])
+    ftt = ops.meshft_list(_t(v + t), F, C, grid, band)
+    xil = _oracle_xi(grid, band)
+    pred = ft.cpu().numpy() * np.exp(-1j * xil @ t)
+    assert rel_l2(ftt.cpu().numpy(), pred) < 1e-5
+    rng = np.random.default_rng(0)
+    sub = np.sort(rng.choice(band.numel(), 256, replace=False))
+    ref = oracle.meshft_forward(v - box[:, 0], f, np.ones(len(f)), xil[sub])
+    assert rel_l2(ft.cpu().numpy()[sub], ref) < TOL_FT

@@ -1,0 +1,81 @@
+"""The C-ABI library: builds, loads without a GPU, exports every declared symbol,
+and rejects bad arguments on the host before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "deltamic_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(dm_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from deltamic_b200 import _native
+    if not os.path.exists(_native.LIB_PATH):
+        from deltamic_b200 import build
+        build.build()
+    return _native.lib()
+
+
+def test_every_declared_symbol_is_exported_and_bound(lib):
+    from deltamic_b200 import _native
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _native.SIGNATURES, n
+    assert set(_native.SIGNATURES) == set(names)
+
+
+def test_abi_version_and_status_strings(lib):
+    assert lib.dm_abi_version() == 1
+    assert lib.dm_status_string(0) == b"ok"
+    assert b"index" in lib.dm_status_string(2)
+
+
+def test_host_side_argument_checks(lib):
+    from deltamic_b200 import _native as N
+    box = N.make_box([[0, 1], [0, 1], [0, 1]], (8, 8, 8))
+    bad = N.make_box([[0, 1], [0, 1], [1, 0]], (8, 8, 8))
+    # null workspace / bad box / negative sizes: rejected before any launch
+    assert lib.dm_meshft_forward(None, 3, None, 1, None, ctypes.byref(box), None, 0, None, None,
+                                 None, None, 0, None) & N.DM_ERR_INVALID_ARG
+    assert lib.dm_meshft_forward(None, 0, None, 0, None, ctypes.byref(bad), None, 0, None, None,
+                                 None, ctypes.c_void_p(16), 1 << 20, None) == N.DM_ERR_INVALID_ARG
+    assert lib.dm_meshft_backward(None, -1, None, 0, None, ctypes.byref(box), None, 0, None, None,
+                                  None, 1.0, None, None, None, None, None, None, 0,
+                                  None) == N.DM_ERR_SIZE
+    assert lib.dm_image_loss(None, 10, 0, None, 0.0, None, None, None, None, 0,
+                             None) == N.DM_ERR_INVALID_ARG
+    assert lib.dm_narrowband_compact(None, -1, 0.0, None, None, None, 0,
+                                     None) == N.DM_ERR_INVALID_ARG
+    # workspace smaller than the query
+    need = lib.dm_meshft_forward_workspace_size(10, 16, 100)
+    assert need > 0
+    assert lib.dm_meshft_forward(ctypes.c_void_p(16), 10, ctypes.c_void_p(16), 16,
+                                 ctypes.c_void_p(16), ctypes.byref(box), ctypes.c_void_p(16),
+                                 100, None, ctypes.c_void_p(16), None, ctypes.c_void_p(16),
+                                 need - 1, None) == N.DM_ERR_WORKSPACE
+
+
+def test_workspace_sizes_grow_with_problem(lib):
+    a = lib.dm_meshft_backward_workspace_size(642, 1280, 24464)
+    b = lib.dm_meshft_backward_workspace_size(10242, 20480, 14064)
+    assert 0 < a < b
+    assert lib.dm_topology_size(10242, 20480) > 4 * 3 * 20480
+
+
+def test_product_path_refuses_cpu():
+    import torch
+    import deltamic_b200 as dm
+    with pytest.raises(RuntimeError):
+        dm.Fourier3dMesh(torch.tensor([[0.0, 1.0]] * 3), (8, 8, 8), device="cpu")
