@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark: meshFT face*xi pairs per second in the 200^3 mesh-fitting step.
+
+Workload (one replica per GPU, weak scaling): a level-5 spherical-harmonic shape
+(10,242 vertices, 20,480 faces) rendered at 200^3 with the anisotropic Gaussian
+PSF diag(1e-3, 1e-3, 4e-3) and narrow band OTF > 1e-5; target = that render
+scaled to 200 photons with Poisson + N(0, 2^2) noise, normalised.  A step is one
+Adam iteration of the fit from the r = 0.3 level-5 icosphere: meshFT forward with
+the OTF multiply, inverse FFT, |.| + normalize + image L2 and its gradient, FFT,
+meshFT adjoint, Adam -- captured as one CUDA graph.  value = face*xi pairs of
+the step (n_faces * n_band) per second over all GPUs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the reference
+algorithm's CPU path (the float64 numpy restatement in oracle/) on this host.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (200, 200, 200)
+LEVEL = 5
+SIGMA = (1e-3, 1e-3, 4e-3)
+THRESH = 1e-5
+LR = 1e-3
+# Algorithmic work per (face, xi) pair of the meshFT kernels (frozen constants):
+# forward 32 FP32 + 7 MUFU, adjoint with recompute 80 FP32 + 9 MUFU.
+FWD_FP32, FWD_MUFU = 32, 7
+BWD_FP32, BWD_MUFU = 80, 9
+METRIC = "meshFT face*xi pairs/s (fit step: fwd+bwd, 200^3, 20,480 faces)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--no-graph", action="store_true")
+    p.add_argument("--small", action="store_true",
+                   help="level-3 mesh at 64^3 (for profiler captures)")
+    p.add_argument("--skip-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def make_workload(rank, small=False):
+    """Ground truth, initial mesh and box for replica ``rank`` (numpy float64)."""
+    from deltamic_b200.mesh import icosphere, random_sh_shape
+    import oracle
+    level = 3 if small else LEVEL
+    gt_v, faces = random_sh_shape(level, 0.3, 6, 0.08, seed=1234 + rank)
+    init_v, _ = icosphere(level, 0.3)
+    box = oracle.compute_box_size(np.concatenate([gt_v, init_v]), 0.2)
+    return gt_v, init_v, faces, box
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=96, threads=None):
+    """Oracle (reference algorithm restated in numpy) forward+adjoint on a sample."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    sub = np.sort(rng.choice(len(band_xi), min(sample_xi, len(band_xi)), replace=False))
+    xi = band_xi[sub]
+    vs = gt_v - box[:, 0]
+    coeff = np.ones(len(faces))
+    g = np.ones(len(xi), np.complex128)
+    chunk = max(len(faces), len(xi) * len(faces) // (4 * threads))
+    t0 = time.perf_counter()
+    ft = oracle.meshft_forward(vs, faces, coeff, xi, threads=threads, chunk_pairs=chunk)
+    oracle.meshft_backward(vs, faces, coeff, xi, g, ft, threads=threads, chunk_pairs=chunk)
+    dt = time.perf_counter() - t0
+    pairs = len(xi) * len(faces)
+    return {"value": pairs / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
+            "sample": f"{len(xi)} band frequencies x {len(faces)} faces, forward+adjoint, "
+                      f"float64 numpy ({dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm (rank 0 only): the oracle port on a sample per step."""
+    if rank != 0:
+        return
+    import oracle
+    gt_v, init_v, faces, box = make_workload(0, args.small)
+    axes = oracle.frequency_axes(box, SHAPE)
+    otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
+    idx = oracle.band_indices(otf, THRESH)
+    band_xi = oracle.xi_list_from_band(idx, axes)
+    threads = os.cpu_count() or 1
+    per_step = 48
+    vals = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_baseline(gt_v, faces, box, band_xi[k * per_step % len(band_xi):], per_step,
+                         threads)
+        if k >= args.warmup:
+            vals.append(r["value"])
+    value = float(np.mean(vals))
+    full_pairs = len(idx) * len(faces)
+    out = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": full_pairs / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "fit200: level-5 SH mesh, 200^3, OTF>1e-5 band",
+                   "n_faces": int(len(faces)), "n_band": int(len(idx)),
+                   "pairs_per_step": int(full_pairs), "parallelism": "replicas only"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_step} band frequencies x {len(faces)} faces per step"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from deltamic_b200 import MeshRenderer, normalize_tensor, _native as N
+    from deltamic_b200.fit import FitStep
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.lib()
+    gt_v, init_v, faces_np, box = make_workload(rank, args.small)
+    shape = (64, 64, 64) if args.small else SHAPE
+    r = MeshRenderer(box, shape, THRESH, dev)
+    r.set_sigma(torch.diag(torch.tensor(SIGMA, device=dev)))
+    F = torch.tensor(faces_np, device=dev)
+    C = torch.ones(len(faces_np), device=dev)
+    gen = torch.Generator(device=dev).manual_seed(99 + rank)
+    img = r.render(torch.tensor(gt_v, dtype=torch.float32, device=dev), F, C)
+    photons = img / img.max() * 200.0
+    noisy = torch.poisson(photons, generator=gen) + 2.0 * torch.randn(
+        shape, device=dev, generator=gen)
+    target = normalize_tensor(noisy).contiguous()
+    V = torch.tensor(init_v, dtype=torch.float32, device=dev)
+    nt, nb = len(faces_np), r.n_band
+    pairs = nt * nb
+
+    step = FitStep(r, V, F, C, target, "mse", 0.0, LR, graph=not args.no_graph)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    loss_end = float(step.loss[0])
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+
+    # roofline: the meshFT kernels timed with events on their stream (eager steps)
+    eager = FitStep(r, V.clone(), F, C, target, "mse", 0.0, LR, graph=False)
+    eager()
+    torch.cuda.synchronize()
+    lib.dm_profile_enable(1)
+    nprof = 10
+    for _ in range(nprof):
+        eager()
+    torch.cuda.synchronize()
+    cnt, tot = N._INT(), N._F()
+    N.check(lib.dm_profile_read(1, cnt, tot), "dm_profile_read")
+    bwd_ms = tot.value / max(cnt.value, 1)
+    N.check(lib.dm_profile_read(0, cnt, tot), "dm_profile_read")
+    fwd_ms = tot.value / max(cnt.value, 1)
+    lib.dm_profile_enable(0)
+    peak_fma, peak_mufu = N.ctypes.c_double(), N.ctypes.c_double()
+    N.check(lib.dm_peak_probe(0, 4096, peak_fma, N.stream_ptr(dev)), "dm_peak_probe")
+    N.check(lib.dm_peak_probe(1, 2048, peak_mufu, N.stream_ptr(dev)), "dm_peak_probe")
+    mufu_bwd = pairs * BWD_MUFU / (bwd_ms * 1e-3)
+    fp32_bwd = pairs * BWD_FP32 / (bwd_ms * 1e-3)
+    mufu_fwd = pairs * FWD_MUFU / (fwd_ms * 1e-3)
+    fp32_fwd = pairs * FWD_FP32 / (fwd_ms * 1e-3)
+    frac_m, frac_f = mufu_bwd / peak_mufu.value, fp32_bwd / peak_fma.value
+    bound = "mufu" if frac_m >= frac_f else "fp32"
+    achieved = mufu_bwd if bound == "mufu" else fp32_bwd
+    peak = peak_mufu.value if bound == "mufu" else peak_fma.value
+
+    # end to end through the public API, host buffers: H2D verts, render + loss +
+    # backward, D2H loss and vertex gradient
+    host_v = torch.tensor(init_v, dtype=torch.float32).pin_memory()
+    host_g = torch.empty_like(host_v).pin_memory()
+    host_l = torch.empty(1).pin_memory()
+    Vd = torch.empty_like(V)
+
+    def e2e_step():
+        Vd.copy_(host_v, non_blocking=True)
+        Vp = Vd.requires_grad_(True)
+        loss = r.loss(Vp, F, C, "mse", target)
+        loss.backward()
+        host_g.copy_(Vp.grad, non_blocking=True)
+        host_l.copy_(loss.detach().view(1), non_blocking=True)
+        Vp.grad = None
+        Vd.requires_grad_(False)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t[0])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        axes = oracle.frequency_axes(box, shape)
+        band_xi = oracle.xi_list_from_band(r.band.cpu().numpy().astype(np.int64), axes)
+        cpu = cpu_baseline(gt_v, faces_np, box, band_xi)
+
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC,
+        "value": pairs * world / (ms * 1e-3),
+        "unit": "pairs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded SH shapes, Poisson + Gaussian noise)",
+        "config": {
+            "workload": ("fit64-small" if args.small else
+                         "fit200: Adam step fitting a level-5 sphere to a level-5 SH shape, "
+                         "200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5"),
+            "n_verts": int(len(init_v)), "n_faces": int(nt), "n_band": int(nb),
+            "pairs_per_step": int(pairs), "box_shape": list(shape),
+            "cuda_graph": not args.no_graph, "parallelism": "replicas only (one mesh per GPU)",
+            "l2_flush": "no: the step streams >256 MB of complex grids (> 126 MB L2)",
+            "loss_last_step": loss_end,
+        },
+        "gpu_launches": int((step.launches_per_step or 0) * args.steps),
+        "clocks": clk,
+        "e2e": {"value": pairs * world / (e2e_ms * 1e-3), "unit": "pairs/s",
+                "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(host_v.numel() * 4),
+                "d2h_bytes_per_step": int(host_g.numel() * 4 + 4)},
+        "roofline": {
+            "bound": bound, "kernel": "k_meshft_bwd (adjoint)",
+            "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
+            "frac": achieved / peak,
+            "peak_source": "measured in this run by dm_peak_probe (MUFU sin / FP32 FMA chains)",
+            "traffic": None,
+            "ops_per_pair": {"fp32": BWD_FP32, "mufu": BWD_MUFU},
+            "kernel_ms": bwd_ms,
+            "fp32_frac": frac_f, "mufu_frac": frac_m,
+            "forward": {"kernel": "k_meshft_fwd", "kernel_ms": fwd_ms,
+                        "mufu_frac": mufu_fwd / peak_mufu.value,
+                        "fp32_frac": fp32_fwd / peak_fma.value},
+        },
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

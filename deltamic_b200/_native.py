@@ -62,6 +62,10 @@ SIGNATURES = {
     "dm_image_loss_workspace_size": (_SZ, [_I64]),
     "dm_image_loss": (_INT, [_P, _I64, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
+    "dm_launch_count": (ctypes.c_longlong, []),
+    "dm_peak_probe": (_INT, [_INT, _INT, ctypes.POINTER(ctypes.c_double), _P]),
+    "dm_profile_enable": (_INT, [_INT]),
+    "dm_profile_read": (_INT, [_INT, ctypes.POINTER(_INT), ctypes.POINTER(_F)]),
 }
 
 _lib = None

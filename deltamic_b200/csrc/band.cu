@@ -104,6 +104,7 @@ int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, i
   }
   k_band_scan<<<1, 1024, 0, st>>>(blk_count, blk_off, nb, count);
   if (nb > 0) k_band_write<<<(unsigned)nb, kBandThreads, 0, st>>>(otf, n, thresh, blk_off, out);
+  count_launches(1 + (nb > 0 ? 2 : 0));
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -213,7 +214,10 @@ int launch_gaussian_otf(const float* sigma, const float* const xi[3], const int3
                         float* otf, cudaStream_t st) {
   const int64_t nv = (int64_t)n[0] * n[1] * n[2];
   const int64_t blocks = std::min<int64_t>((nv + 255) / 256, 148 * 32);
-  if (nv > 0) k_gaussian_otf<<<(unsigned)blocks, 256, 0, st>>>(sigma, make_axes(xi, n), nv, otf);
+  if (nv > 0) {
+    k_gaussian_otf<<<(unsigned)blocks, 256, 0, st>>>(sigma, make_axes(xi, n), nv, otf);
+    count_launches(1);
+  }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -229,6 +233,7 @@ int launch_otf_sigma_grad(const float* gotf, const int32_t* band, int64_t n, con
   k_otf_sigma_grad_part<<<nblk, kBandThreads, 0, st>>>(gotf, band, n, otf, make_axes(xi, nax),
                                                        part);
   k_otf_sigma_grad_final<<<1, 32, 0, st>>>(part, nblk, grad_sigma);
+  count_launches(2);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 

@@ -7,6 +7,8 @@
 
 namespace dm {
 
+void count_launches(int n);
+
 int64_t band_blocks(int64_t n);
 int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, int64_t* count,
                       int32_t* blk_count, int32_t* blk_off, cudaStream_t st);

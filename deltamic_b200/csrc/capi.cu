@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "band_internal.h"
 #include "dm_common.cuh"
@@ -135,7 +136,74 @@ size_t bwd_layout(void* ws, const PlanTotals& t, BwdWs* out) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Instrumentation state (process-wide, current device only).
+namespace dm {
+namespace {
+std::atomic<long long> g_launches{0};
+constexpr int kProfRing = 512;
+struct ProfRing {
+  cudaEvent_t ev[kProfRing][2];
+  int n = 0;        // pairs recorded since the last read
+  bool ready = false;
+};
+int g_profile_on = 0;
+ProfRing g_prof[2];
+int g_pending[2] = {-1, -1};
+}  // namespace
+
+void count_launches(int n) { g_launches += n; }
+
+void profile_begin(int kind, cudaStream_t st) {
+  if (!g_profile_on || kind < 0 || kind > 1) return;
+  ProfRing& r = g_prof[kind];
+  if (!r.ready) {
+    for (int i = 0; i < kProfRing; ++i) {
+      cudaEventCreate(&r.ev[i][0]);
+      cudaEventCreate(&r.ev[i][1]);
+    }
+    r.ready = true;
+  }
+  if (r.n >= kProfRing) return;
+  cudaEventRecord(r.ev[r.n][0], st);
+  g_pending[kind] = r.n;
+}
+
+void profile_end(int kind, cudaStream_t st) {
+  if (!g_profile_on || kind < 0 || kind > 1 || g_pending[kind] < 0) return;
+  ProfRing& r = g_prof[kind];
+  cudaEventRecord(r.ev[g_pending[kind]][1], st);
+  r.n += 1;
+  g_pending[kind] = -1;
+}
+}  // namespace dm
+
 extern "C" {
+
+int dm_profile_enable(int enable) {
+  dm::g_profile_on = enable ? 1 : 0;
+  for (int k = 0; k < 2; ++k) dm::g_prof[k].n = 0;
+  return DM_OK;
+}
+
+int dm_profile_read(int kernel, int* count, float* total_ms) {
+  if (kernel < 0 || kernel > 1 || !count || !total_ms) return DM_ERR_INVALID_ARG;
+  dm::ProfRing& r = dm::g_prof[kernel];
+  float tot = 0.f;
+  for (int i = 0; i < r.n; ++i) {
+    if (cudaEventSynchronize(r.ev[i][1]) != cudaSuccess) return DM_ERR_CUDA;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.ev[i][0], r.ev[i][1]) != cudaSuccess) return DM_ERR_CUDA;
+    tot += ms;
+  }
+  *count = r.n;
+  *total_ms = tot;
+  r.n = 0;
+  return DM_OK;
+}
+
+long long dm_launch_count(void) { return dm::g_launches.load(); }
+
 
 int dm_abi_version(void) { return 1; }
 

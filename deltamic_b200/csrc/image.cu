@@ -248,6 +248,7 @@ int launch_image_loss(const float2* z, int64_t n, int kind, const float* target,
   k_img_loss<<<nb, kImgThreads, 0, st>>>(z, n, kind, target, contrast, image, grad_z, ws, lp);
   k_img_final<<<1, 256, 0, st>>>(z, n, kind, contrast, lp, nb, ws, loss, grad_z);
   if (grad_z) k_img_ties_full<<<nb, kImgThreads, 0, st>>>(z, n, ws, grad_z);
+  count_launches(4 + (grad_z ? 1 : 0));
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -284,10 +285,12 @@ int launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float l
                 float b2, float eps, int64_t* step, cudaStream_t st) {
   if (n <= (1 << 20)) {
     k_adam<<<1, 1024, 0, st>>>(p, g, m, v, n, lr, b1, b2, eps, step, 1);
+    count_launches(1);
   } else {
     const int64_t nb = std::min<int64_t>((n + 255) / 256, 148 * 16);
     k_adam<<<(unsigned)nb, 256, 0, st>>>(p, g, m, v, n, lr, b1, b2, eps, step, 0);
     k_bump<<<1, 1, 0, st>>>(step);
+    count_launches(2);
   }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }

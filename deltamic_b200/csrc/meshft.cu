@@ -151,20 +151,19 @@ __device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const XiVa
   uint32_t spm = 0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    c32 E, G, Gu, Gw;
-    int piv;
-    const bool sp = pair_fast<false>(xv[r], g, E, G, Gu, Gw, piv);
-    const c32 F = cmul(E, G);
-    acc[r].x += sp ? 0.0f : ac * F.x;
-    acc[r].y += sp ? 0.0f : ac * F.y;
-    spm |= (sp ? 1u : 0u) << r;
+    c32 F;
+    if (pair_forward(xv[r], g, F)) {
+      acc[r].x += ac * F.x;
+      acc[r].y += ac * F.y;
+    } else {
+      spm |= 1u << r;
+    }
   }
   if (spm) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if ((spm >> r) & 1u) {
-        c32 F;
-        pair_general<false>(xv[r], g, F, nullptr);
+        const c32 F = pair_forward_degenerate(xv[r], g);
         acc[r].x += ac * F.x;
         acc[r].y += ac * F.y;
       }
@@ -343,50 +342,15 @@ struct BwdAcc {
   float q[10];  // q[3v+j] = sum z_v m_j (v = a,b,c), q[9] = sum Re(conj(g) F)
 };
 
-__device__ __forceinline__ void bwd_pair(const XiVal& xv, const FaceGeom& g, float gre, float gim,
-                                         BwdAcc& a, bool& special) {
-  c32 E, G, Gu, Gw;
-  int piv;
-  const bool sp = pair_fast<true>(xv, g, E, G, Gu, Gw, piv);
-  // h = conj(g) E
-  const float hx = gre * E.x + gim * E.y;
-  const float hy = gre * E.y - gim * E.x;
-  const float r = hx * G.x - hy * G.y;    // Re(h G) = Re(conj(g) F)
-  const float zt = hx * G.y + hy * G.x;   // Im(h G): Re(conj(g) (-i F))
-  const float zu = hx * Gu.x - hy * Gu.y;
-  const float zw = hx * Gw.x - hy * Gw.y;
-  const float zp = zt - zu - zw;
-  float za = piv == 0 ? zp : (piv == 1 ? zw : zu);
-  float zb = piv == 0 ? zu : (piv == 1 ? zp : zw);
-  float zc = piv == 0 ? zw : (piv == 1 ? zu : zp);
-  za = sp ? 0.f : za;
-  zb = sp ? 0.f : zb;
-  zc = sp ? 0.f : zc;
-  a.q[0] += za * xv.mf[0];
-  a.q[1] += za * xv.mf[1];
-  a.q[2] += za * xv.mf[2];
-  a.q[3] += zb * xv.mf[0];
-  a.q[4] += zb * xv.mf[1];
-  a.q[5] += zb * xv.mf[2];
-  a.q[6] += zc * xv.mf[0];
-  a.q[7] += zc * xv.mf[1];
-  a.q[8] += zc * xv.mf[2];
-  a.q[9] += sp ? 0.f : r;
-  special = sp;
-}
-
-__device__ __noinline__ void bwd_pair_general(const XiVal& xv, const FaceGeom& g, float gre,
-                                              float gim, BwdAcc& a) {
-  c32 F, dF[3];
-  pair_general<true>(xv, g, F, dF);
+__device__ __forceinline__ void bwd_accumulate(BwdAcc& a, const float z[3], float r,
+                                               const float mf[3]) {
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
-    const float z = gre * dF[v].x + gim * dF[v].y;
-    a.q[3 * v + 0] += z * xv.mf[0];
-    a.q[3 * v + 1] += z * xv.mf[1];
-    a.q[3 * v + 2] += z * xv.mf[2];
+    a.q[3 * v + 0] += z[v] * mf[0];
+    a.q[3 * v + 1] += z[v] * mf[1];
+    a.q[3 * v + 2] += z[v] * mf[2];
   }
-  a.q[9] += gre * F.x + gim * F.y;
+  a.q[9] += r;
 }
 
 template <int F, int NT, int TX, int NS>
@@ -461,14 +425,21 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
       uint32_t spm = 0;
 #pragma unroll
       for (int k = 0; k < F; ++k) {
-        bool sp;
-        bwd_pair(xv, geom[k], gre, gim, tacc[k], sp);
-        spm |= (sp ? 1u : 0u) << k;
+        float z[3], r;
+        if (pair_adjoint(xv, geom[k], gre, gim, z, r))
+          bwd_accumulate(tacc[k], z, r, xv.mf);
+        else
+          spm |= 1u << k;
       }
       if (spm) {
 #pragma unroll
-        for (int k = 0; k < F; ++k)
-          if ((spm >> k) & 1u) bwd_pair_general(xv, geom[k], gre, gim, tacc[k]);
+        for (int k = 0; k < F; ++k) {
+          if ((spm >> k) & 1u) {
+            float z[3], r;
+            pair_adjoint_degenerate(xv, geom[k], gre, gim, z, r);
+            bwd_accumulate(tacc[k], z, r, xv.mf);
+          }
+        }
       }
     }
 #pragma unroll
@@ -738,6 +709,7 @@ int launch_face_prep(const Cells& c, const PlanTotals& t, const float* verts, co
                      const float* coeff, FaceRec* recs, double* area_part, int* err,
                      cudaStream_t st) {
   k_face_prep<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, recs, area_part, err);
+  count_launches(1);
   return launch_status();
 }
 
@@ -745,13 +717,17 @@ int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
                    const int32_t* band_index, const double* area_part, const float* otf,
                    float2* fpart, float2* ft_list, float2* grid, int* err, cudaStream_t st) {
   if (t.fwd_items > 0 && t.nband > 0) {
+    profile_begin(0, st);
     k_meshft_fwd<FwdCfg::R, FwdCfg::NT, FwdCfg::TF, FwdCfg::NS>
         <<<(unsigned)t.fwd_items, FwdCfg::NT, 0, st>>>(c, recs, band_index, fpart, err);
+    profile_end(0, st);
+    count_launches(1);
     if (launch_status()) return DM_ERR_CUDA;
   }
   if (t.nband > 0) {
     k_meshft_fwd_epi<<<(unsigned)t.band_blks, kBlk, 0, st>>>(c, band_index, fpart, area_part, otf,
                                                             ft_list, grid, err);
+    count_launches(1);
   }
   return launch_status();
 }
@@ -766,21 +742,28 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
   k_bwd_band_prep<<<(unsigned)t.band_blks, kBlk, 0, st>>>(c, band_index, grad_list, grad_grid, otf,
                                                          grad_scale, ft_list, xrec, grad_otf_band,
                                                          s_part, err);
+  count_launches(1);
   if (launch_status()) return DM_ERR_CUDA;
   if (t.bwd_items > 0 && t.nband > 0 && t.nt > 0) {
     cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
+    profile_begin(1, st);
     k_meshft_bwd<BwdCfg::F, BwdCfg::NT, BwdCfg::TX, BwdCfg::NS>
         <<<(unsigned)t.bwd_items, BwdCfg::NT, 0, st>>>(c, recs, xrec, bpart, err);
+    profile_end(1, st);
+    count_launches(1);
     if (launch_status()) return DM_ERR_CUDA;
   } else if (t.bpart > 0) {
     cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)t.bpart, st);
   }
   k_bwd_face_epi<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, area_part, s_part,
                                                         bpart, contrib, grad_coeff);
+  count_launches(1);
   if (launch_status()) return DM_ERR_CUDA;
-  if (t.nv > 0)
+  if (t.nv > 0) {
     k_vertex_gather<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, csr_off, csr_ent, contrib,
                                                                 grad_verts);
+    count_launches(1);
+  }
   return launch_status();
 }
 
@@ -792,6 +775,7 @@ int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, i
   k_csr_scan<<<1, 1024, 0, st>>>(count, off, t.nv);
   if (t.nt > 0) k_csr_fill<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, faces, off, cursor, ent);
   if (t.nv > 0) k_csr_sort<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, off, ent);
+  count_launches(2 + (t.nt > 0 ? 2 : 0) + (t.nv > 0 ? 1 : 0));
   return launch_status();
 }
 

@@ -22,6 +22,12 @@ struct PlanTotals {
 };
 
 int num_sms();
+
+// Instrumentation: launches counted per process; optional CUDA events around the
+// main forward / backward kernels (kind 0 / 1).
+void count_launches(int n);
+void profile_begin(int kind, cudaStream_t st);
+void profile_end(int kind, cudaStream_t st);
 void plan_cell_tiles(CellDesc& d);
 void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t);
 

@@ -23,11 +23,14 @@
 //        G = -i (S(U) - S(W)) / (W - U),   S(t) = (1 - e^{-it})/(it)
 //          = e^{-it/2} sinc(t/2),
 //    sinc by Taylor polynomial for |t/2| < 1 and sin/rcp otherwise;
-//  * when |W - U| < 1 the divided difference is summed as its Taylor series
-//    G = sum_n (-i)^n h_n(U,W)/(n+2)!  (h_n complete homogeneous symmetric
-//    polynomials), which is exact to < 1e-7 there;
+//  * when the largest difference is below 3.5 the term is expanded about the
+//    centroid: F = e^{-i x_g} H(p2, p3) with d_v = x_v - x_g, p2 = sum d^2,
+//    p3 = sum d^3 and H = sum_n (-i)^n h_n(d)/(n+2)! (h_n complete homogeneous
+//    symmetric polynomials, reduced by the Newton identities to a polynomial in
+//    p2, p3; coefficients in series_coeffs.cuh), exact to < 1e-8 there;
 //  * the reference's branch selection (R1..R4 at Seps = sqrt(FLT_EPSILON)) is
-//    kept: in those branches the same merged-vertex / centroid values are formed.
+//    kept: in those branches the phases are merged exactly as the reference
+//    does (centroid, or midpoint of the close pair) and the same evaluators run.
 //
 // The header compiles for the host too (libm sin/cos instead of the MUFU
 // approximations) so the math can be checked on a machine without a GPU.
@@ -36,12 +39,12 @@
 #include <math.h>
 #include <string.h>
 
+#include "series_coeffs.cuh"
+
 #if defined(__CUDACC__)
 #define DM_HD __host__ __device__ __forceinline__
-#define DM_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define DM_HD static inline
-#define DM_HD_NOINLINE static
 #endif
 
 namespace dm {
@@ -49,8 +52,8 @@ namespace dm {
 // Seps/2: the reference compares |ab| <= sqrt(FLT_EPSILON); differences here are
 // held in half units.
 constexpr float kSepsHalf = 1.72633492e-4f;
-// Series for |W - U| < 1 (half units: largest |h| < 0.5).
-constexpr float kSeriesHalf = 0.5f;
+// Centroid series when the largest difference is below 3.5 (half units: 1.75).
+constexpr float kSeriesHalf = 1.75f;
 // Polynomial sinc / sinc' below this half-angle magnitude.
 constexpr float kPolyX = 1.0f;
 constexpr float kTwoPi = 6.28318530717958647692f;
@@ -162,49 +165,41 @@ DM_HD void g_sinc(float hu, float hw, c32& G, c32& Gu, c32& Gw) {
   }
 }
 
-// Taylor series of G = -g[0,U,W] for g = exp(-i t) in full units, |U|,|W| <= 1:
-//   G      = sum_n (-i)^n h_n(U,W)   / (n+2)!
-//   dG/dU  = -i sum_n (-i)^n h_n(U,U,W) / (n+3)!
-//   dG/dW  = -i sum_n (-i)^n h_n(U,W,W) / (n+3)!
-template <bool kGrad>
-DM_HD void g_series(float U, float W, c32& G, c32& Gu, c32& Gw) {
-  // 1/(n+2)! and 1/(n+3)! for n = 0..9
-  const float f2[10] = {1.0f / 2, 1.0f / 6, 1.0f / 24, 1.0f / 120, 1.0f / 720, 1.0f / 5040,
-                        1.0f / 40320, 1.0f / 362880, 1.0f / 3628800, 1.0f / 39916800};
-  const float f3[10] = {1.0f / 6, 1.0f / 24, 1.0f / 120, 1.0f / 720, 1.0f / 5040, 1.0f / 40320,
-                        1.0f / 362880, 1.0f / 3628800, 1.0f / 39916800, 1.0f / 479001600};
-  float A = 1.0f, B = 1.0f, C = 1.0f, wp = 1.0f;
-  float gr = 0.f, gi = 0.f, ur = 0.f, ui = 0.f, vr = 0.f, vi = 0.f;
+// ---------------------------------------------------------------------------
+// Centroid series: H(p2, p3) and its partials in p2 and p3.
+
+template <int N>
+DM_HD void horner(const float (&c)[N], float x, float& v, float& dv) {
+  v = c[N - 1];
+  dv = 0.f;
 #pragma unroll
-  for (int n = 0; n < 10; ++n) {
-    if (n > 0) {
-      wp *= W;
-      A = U * A + wp;          // h_n(U,W)
-      B = U * B + A;           // h_n(U,U,W)
-      C = W * C + A;           // h_n(U,W,W)
-    }
-    const float a = A * f2[n];
-    switch (n & 3) {  // (-i)^n = 1, -i, -1, i
-      case 0: gr += a; break;
-      case 1: gi -= a; break;
-      case 2: gr -= a; break;
-      default: gi += a; break;
-    }
-    if (kGrad) {
-      // -i (-i)^n = (-i)^{n+1}
-      const float b = B * f3[n], c = C * f3[n];
-      switch (n & 3) {
-        case 0: ui -= b; vi -= c; break;   // -i
-        case 1: ur -= b; vr -= c; break;   // -1
-        case 2: ui += b; vi += c; break;   // i
-        default: ur += b; vr += c; break;  // 1
-      }
-    }
+  for (int k = N - 2; k >= 0; --k) {
+    dv = dv * x + v;
+    v = v * x + c[k];
   }
-  G = c32{gr, gi};
+}
+
+template <bool kGrad>
+DM_HD void centroid_H(float p2, float p3, c32& H, c32& Hp2, c32& Hp3) {
+  constexpr float P0[DM_SERIES_P0_N] = DM_SERIES_P0;
+  constexpr float P2[DM_SERIES_P2_N] = DM_SERIES_P2;
+  constexpr float P4[DM_SERIES_P4_N] = DM_SERIES_P4;
+  constexpr float Q1[DM_SERIES_Q1_N] = DM_SERIES_Q1;
+  constexpr float Q3[DM_SERIES_Q3_N] = DM_SERIES_Q3;
+  float a0, a0d, a2, a2d, a4, a4d, b1, b1d, b3, b3d;
+  horner(P0, p2, a0, a0d);
+  horner(P2, p2, a2, a2d);
+  horner(P4, p2, a4, a4d);
+  horner(Q1, p2, b1, b1d);
+  horner(Q3, p2, b3, b3d);
+  const float q = p3 * p3;
+  H.x = a0 + q * (a2 + q * a4);
+  H.y = p3 * (b1 + q * b3);
   if (kGrad) {
-    Gu = c32{ur, ui};
-    Gw = c32{vr, vi};
+    Hp2.x = a0d + q * (a2d + q * a4d);
+    Hp2.y = p3 * (b1d + q * b3d);
+    Hp3.x = p3 * (2.0f * a2 + 4.0f * q * a4);
+    Hp3.y = b1 + 3.0f * q * b3;
   }
 }
 
@@ -215,19 +210,37 @@ DM_HD void half_diffs(const float mf[3], const FaceGeom& g, float& hab, float& h
   hca = -(hab + hbc);
 }
 
-// Fast path: generic branch (no difference within Seps, largest difference >= 1).
-// Returns true when the pair needs the general evaluator instead (outputs are
-// then meaningless).  On the fast path: E = exp(-i x_p), G and, if kGrad, dG/dU,
-// dG/dW; piv = 0/1/2 for pivot a/b/c.
+DM_HD c32 expmi(float angle) {
+  float s, c;
+  sincos_fast(angle, &s, &c);
+  return c32{c, -s};
+}
+
+// Centroid path.  Vertex phases x'_v = x_v + off[v] with half differences
+// (hab, hbc, hca) of the x'.  Outputs E = exp(-i x'_g), H and, if kGrad, the
+// centroid deviations d[3] and the partials Hp2, Hp3; F = E H.
 template <bool kGrad>
-DM_HD bool pair_fast(const XiVal& xv, const FaceGeom& g, c32& E, c32& G, c32& Gu, c32& Gw,
-                     int& piv) {
-  float hab, hbc, hca;
-  half_diffs(xv.mf, g, hab, hbc, hca);
+DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca, float off_a,
+                       c32& E, c32& H, c32& Hp2, c32& Hp3, float d[3], float& p2) {
+  const float ab = 2.0f * hab, ca = 2.0f * hca;
+  const float da = (ca - ab) * (1.0f / 3.0f);
+  const float db = da + ab;
+  const float dc = da - ca;
+  p2 = da * da + db * db + dc * dc;
+  const float p3 = 3.0f * da * db * dc;  // sum d^3 when sum d = 0
+  E = expmi(turns_to_angle(fixed_phase(xv.mi, g.Ua[0], g.Ua[1], g.Ua[2])) + (off_a - da));
+  centroid_H<kGrad>(p2, p3, H, Hp2, Hp3);
+  d[0] = da;
+  d[1] = db;
+  d[2] = dc;
+}
+
+// Pivot path (largest difference >= 3.5).  Outputs E = exp(-i x'_p), G and, if
+// kGrad, dG/dU and dG/dW; F = E G; piv = 0/1/2 for pivot a/b/c.
+template <bool kGrad>
+DM_HD void eval_pivot(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+                      const float off[3], c32& E, c32& G, c32& Gu, c32& Gw, int& piv) {
   const float aab = fabsf(hab), abc = fabsf(hbc), aca = fabsf(hca);
-  const float mn = fminf(aab, fminf(abc, aca));
-  const float mx = fmaxf(aab, fmaxf(abc, aca));
-  const bool special = (mn <= kSepsHalf) || (mx < kSeriesHalf);
   const bool pa = (abc >= aca) && (abc >= aab);
   const bool pb = !pa && (aca >= aab);
   piv = pa ? 0 : (pb ? 1 : 2);
@@ -236,79 +249,209 @@ DM_HD bool pair_fast(const XiVal& xv, const FaceGeom& g, c32& E, c32& G, c32& Gu
   const uint32_t P0 = pa ? g.Ua[0] : (pb ? g.Ub[0] : g.Uc[0]);
   const uint32_t P1 = pa ? g.Ua[1] : (pb ? g.Ub[1] : g.Uc[1]);
   const uint32_t P2 = pa ? g.Ua[2] : (pb ? g.Ub[2] : g.Uc[2]);
-  const float th = turns_to_angle(fixed_phase(xv.mi, P0, P1, P2));
-  float s, c;
-  sincos_fast(th, &s, &c);
-  E = c32{c, -s};
+  const float o = pa ? off[0] : (pb ? off[1] : off[2]);
+  E = expmi(turns_to_angle(fixed_phase(xv.mi, P0, P1, P2)) + o);
   g_sinc<kGrad>(hu, hw, G, Gu, Gw);
-  return special;
 }
 
-// General evaluator for any configuration, following the reference's branch
-// selection.  Returns F and the three partials dF/dx_a, dF/dx_b, dF/dx_c.
+// F and dF/dx_{a,b,c} for vertex phases x_v + off[v] (no degenerate branch).
 template <bool kGrad>
-DM_HD_NOINLINE void pair_general(const XiVal& xv, const FaceGeom& g, c32& F, c32* dF) {
+DM_HD void eval_any(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+                    const float off[3], c32& F, c32* dF) {
+  const float amax = fmaxf(fabsf(hab), fmaxf(fabsf(hbc), fabsf(hca)));
+  if (amax < kSeriesHalf) {
+    c32 E, H, Hp2, Hp3;
+    float d[3], p2;
+    eval_series<kGrad>(xv, g, hab, hca, off[0], E, H, Hp2, Hp3, d, p2);
+    F = cmul(E, H);
+    if (kGrad) {
+      const c32 EHp2 = cmul(E, Hp2), EHp3 = cmul(E, Hp3);
+      for (int v = 0; v < 3; ++v) {
+        const float a = 2.0f * d[v], b = 3.0f * d[v] * d[v] - p2;
+        dF[v] = c32{F.y * (1.0f / 3.0f) + a * EHp2.x + b * EHp3.x,
+                    -F.x * (1.0f / 3.0f) + a * EHp2.y + b * EHp3.y};
+      }
+    }
+  } else {
+    c32 E, G, Gu, Gw;
+    int piv;
+    eval_pivot<kGrad>(xv, g, hab, hbc, hca, off, E, G, Gu, Gw, piv);
+    F = cmul(E, G);
+    if (kGrad) {
+      const c32 EGu = cmul(E, Gu), EGw = cmul(E, Gw);
+      const int q = piv == 2 ? 0 : piv + 1;
+      const int r = q == 2 ? 0 : q + 1;
+      dF[piv] = c32{F.y - EGu.x - EGw.x, -F.x - EGu.y - EGw.y};
+      dF[q] = EGu;
+      dF[r] = EGw;
+    }
+  }
+}
+
+// Degenerate frequencies of the reference (a phase difference within Seps):
+// R1 collapses the three phases to their centroid, R2/R3/R4 merge the close pair
+// at its midpoint (fourier3d_cuda_kernel.cu:250-271, render.py:77-102); the
+// merged vertices share the derivative of the merged phase equally.
+template <bool kGrad>
+DM_HD void pair_degenerate(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+                           c32& F, c32* dF) {
+  const bool sab = fabsf(hab) <= kSepsHalf, sbc = fabsf(hbc) <= kSepsHalf,
+             sca = fabsf(hca) <= kSepsHalf;
+  const bool r1 = (sab && sbc) || (sbc && sca) || (sca && sab);
+  float off[3] = {0.f, 0.f, 0.f};
+  int mode;
+  if (r1) {
+    mode = 0;
+    off[0] = (2.0f * hab - 2.0f * hca) * (1.0f / 3.0f);
+    off[1] = off[0] - 2.0f * hab;
+    off[2] = off[0] + 2.0f * hca;
+    hab = hbc = hca = 0.f;
+  } else if (sab) {
+    mode = 1;
+    off[0] = hab;
+    off[1] = -hab;
+    hbc += 0.5f * hab;
+    hca += 0.5f * hab;
+    hab = 0.f;
+  } else if (sbc) {
+    mode = 2;
+    off[1] = hbc;
+    off[2] = -hbc;
+    hab += 0.5f * hbc;
+    hca += 0.5f * hbc;
+    hbc = 0.f;
+  } else {
+    mode = 3;
+    off[2] = hca;
+    off[0] = -hca;
+    hab += 0.5f * hca;
+    hbc += 0.5f * hca;
+    hca = 0.f;
+  }
+  c32 d3[3];
+  eval_any<kGrad>(xv, g, hab, hbc, hca, off, F, d3);
+  if (!kGrad) return;
+  if (mode == 0) {
+    const c32 m{(d3[0].x + d3[1].x + d3[2].x) * (1.0f / 3.0f),
+                (d3[0].y + d3[1].y + d3[2].y) * (1.0f / 3.0f)};
+    dF[0] = m; dF[1] = m; dF[2] = m;
+    return;
+  }
+  // merged pair (i, j), lone vertex o
+  const int i = mode == 1 ? 0 : (mode == 2 ? 1 : 2);
+  const int j = i == 2 ? 0 : i + 1;
+  const int o = j == 2 ? 0 : j + 1;
+  const c32 m{0.5f * (d3[i].x + d3[j].x), 0.5f * (d3[i].y + d3[j].y)};
+  dF[i] = m;
+  dF[j] = m;
+  dF[o] = d3[o];
+}
+
+// Classification shared by the kernels: 0 = centroid series, 1 = pivot,
+// 2 = reference-degenerate branch.
+DM_HD int pair_class(float hab, float hbc, float hca) {
+  const float aab = fabsf(hab), abc = fabsf(hbc), aca = fabsf(hca);
+  const float mn = fminf(aab, fminf(abc, aca));
+  const float mx = fmaxf(aab, fmaxf(abc, aca));
+  return mn <= kSepsHalf ? 2 : (mx < kSeriesHalf ? 0 : 1);
+}
+
+// Any pair: F and (if kGrad) dF/dx_{a,b,c}.
+template <bool kGrad>
+DM_HD void pair_general(const XiVal& xv, const FaceGeom& g, c32& F, c32* dF) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
-  const float aab = fabsf(hab), abc = fabsf(hbc), aca = fabsf(hca);
-  const bool sab = aab <= kSepsHalf, sbc = abc <= kSepsHalf, sca = aca <= kSepsHalf;
-  const bool r1 = (sab && sbc) || (sbc && sca) || (sca && sab);
-  int base;       // vertex whose fixed-point phase anchors E
-  float delta;    // extra phase (full units) added to that vertex
-  int mode;       // 0: R1, 1: R2, 2: R3, 3: R4, 4: R5
-  float U = 0.f, W = 0.f;
-  int piv = 0;
-  if (r1) {
-    mode = 0; base = 0; delta = (2.0f * hab - 2.0f * hca) * (1.0f / 3.0f);
-  } else if (sab) {
-    mode = 1; base = 0; delta = hab; W = -2.0f * hca - hab;      // x_c - (x_a+x_b)/2
-  } else if (sbc) {
-    mode = 2; base = 1; delta = hbc; W = -2.0f * hab - hbc;      // x_a - (x_b+x_c)/2
-  } else if (sca) {
-    mode = 3; base = 2; delta = hca; W = -2.0f * hbc - hca;      // x_b - (x_c+x_a)/2
+  if (pair_class(hab, hbc, hca) == 2) {
+    pair_degenerate<kGrad>(xv, g, hab, hbc, hca, F, dF);
   } else {
-    mode = 4; delta = 0.f;
-    const bool pa = (abc >= aca) && (abc >= aab);
-    const bool pb = !pa && (aca >= aab);
-    piv = pa ? 0 : (pb ? 1 : 2);
-    base = piv;
-    U = 2.0f * (pa ? hab : (pb ? hbc : hca));
-    W = 2.0f * (pa ? -hca : (pb ? -hab : -hbc));
+    const float off[3] = {0.f, 0.f, 0.f};
+    eval_any<kGrad>(xv, g, hab, hbc, hca, off, F, dF);
   }
-  const uint32_t* Ub = base == 0 ? g.Ua : (base == 1 ? g.Ub : g.Uc);
-  const float th = turns_to_angle(fixed_phase(xv.mi, Ub[0], Ub[1], Ub[2])) + delta;
-  float s, c;
-  sincos_fast(th, &s, &c);
-  const c32 E{c, -s};
-  c32 G, Gu{0.f, 0.f}, Gw{0.f, 0.f};
-  if (mode == 0) {
-    G = c32{0.5f, 0.f};
-  } else if (fabsf(W - U) < 2.0f * kSeriesHalf) {
-    g_series<kGrad>(U, W, G, Gu, Gw);
+}
+
+// ---------------------------------------------------------------------------
+// Per-pair work of the kernels (shared with the host test build).
+
+// Forward: F on the series / pivot paths; returns false for a degenerate pair
+// (F then undefined: the caller runs pair_degenerate for it).
+DM_HD bool pair_forward(const XiVal& xv, const FaceGeom& g, c32& F) {
+  float hab, hbc, hca;
+  half_diffs(xv.mf, g, hab, hbc, hca);
+  const int cls = pair_class(hab, hbc, hca);
+  if (cls == 2) return false;
+  const float off[3] = {0.f, 0.f, 0.f};
+  if (cls == 0) {
+    c32 E, H, Hp2, Hp3;
+    float d[3], p2;
+    eval_series<false>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    F = cmul(E, H);
   } else {
-    g_sinc<kGrad>(0.5f * U, 0.5f * W, G, Gu, Gw);
+    c32 E, G, Gu, Gw;
+    int piv;
+    eval_pivot<false>(xv, g, hab, hbc, hca, off, E, G, Gu, Gw, piv);
+    F = cmul(E, G);
   }
-  F = cmul(E, G);
-  if (!kGrad) return;
-  const c32 miF{F.y, -F.x};  // -i F
-  if (mode == 0) {
-    const c32 t{miF.x * (1.0f / 3.0f), miF.y * (1.0f / 3.0f)};
-    dF[0] = t; dF[1] = t; dF[2] = t;
-    return;
+  return true;
+}
+
+// Adjoint: z_v = Re(conj(g) dF/dx_v) and r = Re(conj(g) F) for cotangent g;
+// returns false for a degenerate pair (outputs undefined).
+DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
+                        float& r) {
+  float hab, hbc, hca;
+  half_diffs(xv.mf, g, hab, hbc, hca);
+  const int cls = pair_class(hab, hbc, hca);
+  if (cls == 2) return false;
+  if (cls == 0) {
+    c32 E, H, Hp2, Hp3;
+    float d[3], p2;
+    eval_series<true>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    const float hx = gre * E.x + gim * E.y;  // h = conj(g) E
+    const float hy = gre * E.y - gim * E.x;
+    r = hx * H.x - hy * H.y;
+    const float zt = (hx * H.y + hy * H.x) * (1.0f / 3.0f);
+    const float r1 = 2.0f * (hx * Hp2.x - hy * Hp2.y);
+    const float r2 = hx * Hp3.x - hy * Hp3.y;
+    z[0] = zt + r1 * d[0] + r2 * (3.0f * d[0] * d[0] - p2);
+    z[1] = zt + r1 * d[1] + r2 * (3.0f * d[1] * d[1] - p2);
+    z[2] = zt + r1 * d[2] + r2 * (3.0f * d[2] * d[2] - p2);
+  } else {
+    const float off[3] = {0.f, 0.f, 0.f};
+    c32 E, G, Gu, Gw;
+    int piv;
+    eval_pivot<true>(xv, g, hab, hbc, hca, off, E, G, Gu, Gw, piv);
+    const float hx = gre * E.x + gim * E.y;
+    const float hy = gre * E.y - gim * E.x;
+    r = hx * G.x - hy * G.y;
+    const float zt = hx * G.y + hy * G.x;  // Re(conj(g) (-i F))
+    const float zu = hx * Gu.x - hy * Gu.y;
+    const float zw = hx * Gw.x - hy * Gw.y;
+    const float zp = zt - zu - zw;
+    z[0] = piv == 0 ? zp : (piv == 1 ? zw : zu);
+    z[1] = piv == 0 ? zu : (piv == 1 ? zp : zw);
+    z[2] = piv == 0 ? zw : (piv == 1 ? zu : zp);
   }
-  const c32 EGw = cmul(E, Gw);
-  if (mode == 4) {
-    const c32 EGu = cmul(E, Gu);
-    const c32 dp{miF.x - EGu.x - EGw.x, miF.y - EGu.y - EGw.y};
-    const int q = piv == 2 ? 0 : piv + 1;
-    const int r = q == 2 ? 0 : q + 1;
-    dF[piv] = dp; dF[q] = EGu; dF[r] = EGw;
-    return;
-  }
-  // merged pair: the lone vertex o gets E dG/dW, each merged vertex half the rest
-  const c32 half{0.5f * (miF.x - EGw.x), 0.5f * (miF.y - EGw.y)};
-  const int o = mode == 1 ? 2 : (mode == 2 ? 0 : 1);
-  for (int v = 0; v < 3; ++v) dF[v] = (v == o) ? EGw : half;
+  return true;
+}
+
+// Adjoint of a degenerate pair.
+DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre, float gim,
+                                   float z[3], float& r) {
+  float hab, hbc, hca;
+  half_diffs(xv.mf, g, hab, hbc, hca);
+  c32 F, dF[3];
+  pair_degenerate<true>(xv, g, hab, hbc, hca, F, dF);
+  r = gre * F.x + gim * F.y;
+  for (int v = 0; v < 3; ++v) z[v] = gre * dF[v].x + gim * dF[v].y;
+}
+
+// Forward of a degenerate pair.
+DM_HD c32 pair_forward_degenerate(const XiVal& xv, const FaceGeom& g) {
+  float hab, hbc, hca;
+  half_diffs(xv.mf, g, hab, hbc, hca);
+  c32 F;
+  pair_degenerate<false>(xv, g, hab, hbc, hca, F, nullptr);
+  return F;
 }
 
 }  // namespace dm

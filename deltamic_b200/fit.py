@@ -1,0 +1,105 @@
+"""Gradient-descent fitting of a mesh to a 3D image (the loop of the reference's
+``Examples/Gradient_Descent.ipynb`` cell 2, with plain Adam on the vertices).
+
+``FitStep`` runs one iteration -- fused render + loss (``MeshRenderer``), adjoint,
+Adam -- entirely on the GPU and, by default, replays it as one captured CUDA graph.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _native as N
+from . import ops
+from .pipeline import MeshRenderer
+
+__all__ = ["FitStep", "fit_mesh"]
+
+
+class FitStep:
+    """One Adam step on ``verts`` minimising the loss of the normalised render.
+
+    ``verts`` is updated in place (it is the optimised parameter).  The loss of the
+    step (evaluated before the update, like ``loss.backward(); opt.step()``) is
+    left in ``self.loss`` on the device.
+    """
+
+    def __init__(self, renderer: MeshRenderer, verts, faces, coeff, target=None, kind="mse",
+                 contrast=0.0, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True):
+        ops._check_mesh(verts, faces, coeff)
+        if renderer.band is None:
+            raise RuntimeError("set the renderer's OTF first")
+        self.r = renderer
+        self.V = verts
+        self.F = faces.contiguous()
+        self.C = coeff.contiguous()
+        self.target = target
+        self.kind = kind
+        self.contrast = float(contrast)
+        self.lr, self.betas, self.eps = float(lr), betas, float(eps)
+        self.m = torch.zeros_like(verts)
+        self.v = torch.zeros_like(verts)
+        self.t = torch.zeros(1, dtype=torch.int64, device=verts.device)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=verts.device)
+        self.grad = torch.zeros_like(verts)
+        self.graph = None
+        self.launches_per_step = None
+        if graph:
+            self._capture()
+
+    def _body(self):
+        r = self.r
+        ft = ops.meshft_list(self.V, self.F, self.C, r.grid, r.band, otf=r.otf,
+                             spectrum=r.spec)
+        torch.fft.ifftn(r.spec, out=r.z)
+        loss, _, gz = ops.image_loss(r.z, self.kind, self.target, self.contrast,
+                                     want_grad=True)
+        self.loss.copy_(loss)
+        torch.fft.fftn(gz, out=r.G)
+        gv, _, _ = ops.meshft_backward_list(self.V, self.F, self.C, r.grid, r.band, ft,
+                                            grad_grid=r.G, otf=r.otf, scale=1.0 / r.numel,
+                                            want_coeff=False)
+        self.grad.copy_(gv)
+        ops.adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0],
+                      self.betas[1], self.eps)
+
+    def _capture(self):
+        state = [x.clone() for x in (self.V, self.m, self.v, self.t)]
+        side = torch.cuda.Stream(device=self.V.device)
+        side.wait_stream(torch.cuda.current_stream(self.V.device))
+        with torch.cuda.stream(side):
+            c0 = N.lib().dm_launch_count()
+            self._body()
+            self.launches_per_step = int(N.lib().dm_launch_count() - c0)
+            self._body()
+        torch.cuda.current_stream(self.V.device).wait_stream(side)
+        for dst, src in zip((self.V, self.m, self.v, self.t), state):
+            dst.copy_(src)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._body()
+
+    def __call__(self):
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            if self.launches_per_step is None:
+                c0 = N.lib().dm_launch_count()
+                self._body()
+                self.launches_per_step = int(N.lib().dm_launch_count() - c0)
+            else:
+                self._body()
+        return self.loss
+
+
+def fit_mesh(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr=1e-3,
+             kind="mse", contrast=0.0, graph=True, record_every=1):
+    """Fit ``verts0`` to ``target`` (already normalised) with ``steps`` Adam steps.
+
+    Returns ``(verts, losses)`` with the loss of every ``record_every``-th step."""
+    V = verts0.detach().clone().contiguous()
+    step = FitStep(renderer, V, faces, coeff, target, kind, contrast, lr, graph=graph)
+    losses = torch.zeros(steps, device=V.device)
+    for k in range(steps):
+        step()
+        losses[k] = step.loss[0]
+    return V, losses[::record_every].cpu()

@@ -70,15 +70,19 @@ def narrowband(otf: torch.Tensor, thresh: float) -> torch.Tensor:
 # ---------------------------------------------------------------------------
 # topology cache (vertex <- face CSR), keyed by the faces tensor
 
-_TOPO: "weakref.WeakKeyDictionary[torch.Tensor, tuple]" = weakref.WeakKeyDictionary()
+_TOPO: dict = {}
 
 
 def topology(faces: torch.Tensor, nv: int) -> torch.Tensor:
-    """CSR incidence buffer for ``faces`` (built once; face indices validated)."""
-    key = (faces._version, int(nv), faces.data_ptr())
-    hit = _TOPO.get(faces)
-    if hit is not None and hit[0] == key:
-        return hit[1]
+    """CSR incidence buffer for ``faces`` (built once; face indices validated).
+
+    Cached per faces tensor (by identity, held weakly) and its version counter."""
+    key = (faces._version, int(nv), faces.data_ptr(), tuple(faces.shape))
+    hit = _TOPO.get(id(faces))
+    if hit is not None and hit[0]() is faces and hit[1] == key:
+        return hit[2]
+    for k in [k for k, v in _TOPO.items() if v[0]() is None]:
+        del _TOPO[k]
     lib = N.lib()
     nt = faces.shape[0]
     if nt:
@@ -88,7 +92,7 @@ def topology(faces: torch.Tensor, nv: int) -> torch.Tensor:
     buf = torch.zeros(lib.dm_topology_size(nv, nt), dtype=torch.uint8, device=faces.device)
     N.check(lib.dm_topology_build(N.ptr(faces), nt, nv, N.ptr(buf), buf.numel(),
                                   N.stream_ptr(faces.device)), "dm_topology_build")
-    _TOPO[faces] = (key, buf)
+    _TOPO[id(faces)] = (weakref.ref(faces), key, buf)
     return buf
 
 

@@ -156,6 +156,25 @@ int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg
                  float lr, float beta1, float beta2, float eps, int64_t* step,
                  dm_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Instrumentation (no counterpart in the reference, which has no profiling).
+ * dm_launch_count: kernels this library has launched in the process (host-side
+ * count; graph replays are not counted).
+ * dm_profile_enable: when on, every launch of the main meshFT forward (kernel 0)
+ * or adjoint (kernel 1) kernel is bracketed by CUDA events on its stream (up to
+ * 512 per kernel between reads).  Not for use inside stream capture.
+ * dm_profile_read: synchronises those events and returns their count and total
+ * milliseconds, then clears them. */
+long long dm_launch_count(void);
+
+/* Throughput probe (no counterpart in the reference): times ``iters`` rounds of
+ * 8 independent FP32 FMA chains (kind 0) or MUFU sin.approx chains (kind 1) per
+ * thread over the whole GPU and returns instructions per second.  Synchronous;
+ * these are the roofline denominators for the FP32/MUFU-bound meshFT kernels. */
+int dm_peak_probe(int kind, int iters, double* ops_per_s, dm_stream_t stream);
+int dm_profile_enable(int enable);
+int dm_profile_read(int kernel, int* count, float* total_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,6 +1,7 @@
 // Host build of the kernel pair math (deltamic_b200/csrc/pair_math.cuh) for CPU
-// tests: the same formulas the CUDA kernels run, with libm sin/cos in place of
-// the MUFU approximations.  Built by tests/test_pairmath_host.py with g++.
+// tests: the same per-pair functions the CUDA kernels call (pair_forward,
+// pair_adjoint and their degenerate-branch variants), with libm sin/cos in place
+// of the MUFU approximations.  Built by tests/test_pairmath_host.py with g++.
 #include <cmath>
 #include <cstdint>
 
@@ -28,12 +29,13 @@ static FaceGeom make_geom(const double* va, const double* vb, const double* vc,
 
 extern "C" {
 
-// For each (face k, frequency m) pair: F and dF/dx_{a,b,c} (complex, interleaved
-// re/im) and whether the fast path flagged it special.
-// verts[nv*3] double, faces[nt*3] int64, m[nxi*3] int32; outputs sized nxi*nt.
+// For each (frequency i, face k): F (forward path), z[3] = Re(conj(g_i) dF/dx_v)
+// and r = Re(conj(g_i) F) (adjoint path), and the pair class (0 series, 1 pivot,
+// 2 degenerate).  verts[nv*3] double, faces[nt*3] int64, m[nxi*3] int32,
+// g[nxi*2] float (re, im); outputs sized nxi*nt (F: *2, z: *3).
 void dm_host_pairs(const double* verts, const int64_t* faces, int64_t nt, const int32_t* m,
-                   int64_t nxi, const double* lo, const double* len, float* F, float* dF,
-                   uint8_t* special, int use_fast) {
+                   int64_t nxi, const float* gc, const double* lo, const double* len, float* F,
+                   float* z, float* r, uint8_t* cls) {
   for (int64_t k = 0; k < nt; ++k) {
     const FaceGeom g = make_geom(verts + 3 * faces[3 * k], verts + 3 * faces[3 * k + 1],
                                  verts + 3 * faces[3 * k + 2], lo, len);
@@ -44,27 +46,18 @@ void dm_host_pairs(const double* verts, const int64_t* faces, int64_t nt, const 
         xv.mf[d] = (float)m[3 * i + d];
       }
       const int64_t o = i * nt + k;
-      c32 E, G, Gu, Gw, Fv, d3[3];
-      int piv;
-      bool sp = pair_fast<true>(xv, g, E, G, Gu, Gw, piv);
-      special[o] = sp ? 1 : 0;
-      if (use_fast && !sp) {
-        Fv = cmul(E, G);
-        const c32 miF{Fv.y, -Fv.x};
-        const c32 EGu = cmul(E, Gu), EGw = cmul(E, Gw);
-        const int q = piv == 2 ? 0 : piv + 1, r = q == 2 ? 0 : q + 1;
-        d3[piv] = c32{miF.x - EGu.x - EGw.x, miF.y - EGu.y - EGw.y};
-        d3[q] = EGu;
-        d3[r] = EGw;
-      } else {
-        pair_general<true>(xv, g, Fv, d3);
-      }
+      float hab, hbc, hca;
+      half_diffs(xv.mf, g, hab, hbc, hca);
+      cls[o] = (uint8_t)pair_class(hab, hbc, hca);
+      c32 Fv;
+      if (!pair_forward(xv, g, Fv)) Fv = pair_forward_degenerate(xv, g);
       F[2 * o] = Fv.x;
       F[2 * o + 1] = Fv.y;
-      for (int v = 0; v < 3; ++v) {
-        dF[6 * o + 2 * v] = d3[v].x;
-        dF[6 * o + 2 * v + 1] = d3[v].y;
-      }
+      float zz[3], rr;
+      if (!pair_adjoint(xv, g, gc[2 * i], gc[2 * i + 1], zz, rr))
+        pair_adjoint_degenerate(xv, g, gc[2 * i], gc[2 * i + 1], zz, rr);
+      for (int v = 0; v < 3; ++v) z[3 * o + v] = zz[v];
+      r[o] = rr;
     }
   }
 }

@@ -25,56 +25,70 @@ def hostlib(tmp_path_factory):
     return ctypes.CDLL(out)
 
 
-def _run(lib, v, f, m, lo, L, fast):
+def _run(lib, v, f, m, g, lo, L):
     n, nt = len(m), len(f)
     F = np.zeros((n, nt, 2), np.float32)
-    dF = np.zeros((n, nt, 3, 2), np.float32)
-    sp = np.zeros((n, nt), np.uint8)
+    z = np.zeros((n, nt, 3), np.float32)
+    r = np.zeros((n, nt), np.float32)
+    cls = np.zeros((n, nt), np.uint8)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     vv = np.ascontiguousarray(v, np.float64)
     ff = np.ascontiguousarray(f, np.int64)
     mm = np.ascontiguousarray(m, np.int32)
+    gg = np.ascontiguousarray(np.stack([g.real, g.imag], 1), np.float32)
     lo = np.ascontiguousarray(lo, np.float64)
     L = np.ascontiguousarray(L, np.float64)
-    lib.dm_host_pairs(P(vv), P(ff), ctypes.c_int64(nt), P(mm), ctypes.c_int64(n), P(lo), P(L),
-                      P(F), P(dF), P(sp), ctypes.c_int(fast))
-    return F[..., 0] + 1j * F[..., 1], dF[..., 0] + 1j * dF[..., 1], sp
+    lib.dm_host_pairs(P(vv), P(ff), ctypes.c_int64(nt), P(mm), ctypes.c_int64(n), P(gg), P(lo),
+                      P(L), P(F), P(z), P(r), P(cls))
+    return F[..., 0] + 1j * F[..., 1], z, r, cls
 
 
-def _reference(v, f, m, box, shape):
+def _reference(v, f, m, g, box, shape):
     axes = oracle.frequency_axes(box, shape)
     k = (m + (np.array(shape) - 1)) // 2
     xi = np.stack([axes[d][k[:, d]] for d in range(3)], 1)
     xiv = xi @ (v - box[:, 0]).T
-    return oracle.pair_F_and_grads(xiv[:, f[:, 0]], xiv[:, f[:, 1]], xiv[:, f[:, 2]])
+    F, dF = oracle.pair_F_and_grads(xiv[:, f[:, 0]], xiv[:, f[:, 1]], xiv[:, f[:, 2]])
+    cg = np.conj(g)[:, None]
+    z = np.stack([np.real(cg * d) for d in dF], axis=2)
+    return F, z, np.real(cg * F)
 
 
-@pytest.mark.parametrize("shape", [(21, 21, 21), (64, 64, 64)])
-@pytest.mark.parametrize("fast", [1, 0])
-def test_pair_math_matches_oracle(hostlib, shape, fast):
+def _check(hostlib, v, f, m, box, shape, tol_f, tol_z):
+    rng = np.random.default_rng(1)
+    g = rng.normal(size=len(m)) + 1j * rng.normal(size=len(m))
+    F, z, r, cls = _run(hostlib, v, f, m, g, box[:, 0], box[:, 1] - box[:, 0])
+    F0, z0, r0 = _reference(v, f, m, g, box, shape)
+    assert np.linalg.norm(F - F0) / np.linalg.norm(F0) < tol_f
+    assert np.linalg.norm(z - z0) / np.linalg.norm(z0) < tol_z
+    assert np.linalg.norm(r - r0) / np.linalg.norm(r0) < tol_f
+    for c in (0, 1):  # each path separately
+        sel = cls == c
+        if sel.sum() > 100:
+            assert np.linalg.norm((F - F0)[sel]) / np.linalg.norm(F0[sel]) < tol_f
+            assert np.linalg.norm((z - z0)[sel]) / np.linalg.norm(z0[sel]) < tol_z
+    return cls
+
+
+@pytest.mark.parametrize("level,shape", [(2, (21, 21, 21)), (2, (64, 64, 64)),
+                                         (4, (128, 128, 128))])
+def test_pair_math_matches_oracle(hostlib, level, shape):
     rng = np.random.default_rng(0)
-    v, f = icosphere(2, 0.3)
+    v, f = icosphere(level, 0.3)
     v, _ = sh_perturb(v, 4, 0.08, rng, radius=0.3)
     box = oracle.compute_box_size(v, 0.2)
-    k = np.stack([rng.integers(0, s, 1500) for s in shape], 1)
+    k = np.stack([rng.integers(0, s, 800) for s in shape], 1)
     m = (2 * k - (np.array(shape) - 1)).astype(np.int32)
-    F, dF, sp = _run(hostlib, v, f, m, box[:, 0], box[:, 1] - box[:, 0], fast)
-    F0, g0 = _reference(v, f, m, box, shape)
-    assert np.linalg.norm(F - F0) / np.linalg.norm(F0) < 2e-6
-    for i in range(3):
-        assert np.linalg.norm(dF[..., i] - g0[i]) / np.linalg.norm(g0[i]) < 2e-6
-    assert 0 < sp.mean() < 0.2
+    sub = rng.choice(len(f), min(len(f), 320), replace=False)
+    cls = _check(hostlib, v, f[sub], m, box, shape, 1e-6, 2e-6)
+    assert (cls == 0).any() and (cls == 1).any()
 
 
 def test_pair_math_degenerate_branches(hostlib):
     """Axis-aligned faces on an odd grid: exact zeros in the phase differences."""
     d = load_golden("cube_degenerate")
     box, shape = d["box_size"], tuple(int(s) for s in d["box_shape"])
-    axes_k = np.stack(np.unravel_index(d["idx"], shape), 1)
-    m = (2 * axes_k - (np.array(shape) - 1)).astype(np.int32)
-    F, dF, sp = _run(hostlib, d["verts"], d["faces"], m, box[:, 0], box[:, 1] - box[:, 0], 1)
-    F0, g0 = _reference(d["verts"], d["faces"], m, box, shape)
-    assert sp.mean() > 0.01
-    assert np.max(np.abs(F - F0)) < 2e-6
-    for i in range(3):
-        assert np.max(np.abs(dF[..., i] - g0[i])) < 1e-5 * max(1.0, np.abs(g0[i]).max())
+    k = np.stack(np.unravel_index(d["idx"], shape), 1)
+    m = (2 * k - (np.array(shape) - 1)).astype(np.int32)
+    cls = _check(hostlib, d["verts"], d["faces"], m, box, shape, 1e-6, 2e-6)
+    assert (cls == 2).mean() > 0.01
