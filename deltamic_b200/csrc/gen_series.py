@@ -9,7 +9,9 @@ d_v = x_v - x_g (sum d_v = 0), the triangle term is F = e^{-i x_g} H with
 divided difference of exp(-i x)).  With p2 = sum d^2, p3 = sum d^3 and e1 = 0 the
 Newton identities give h_n = (p2/2) h_{n-2} + (p3/3) h_{n-3}, h_0 = 1, h_1 = 0.
 Grouping by powers of p3:  Re H = P0(p2) + p3^2 P2(p2) + p3^4 P4(p2),
-Im H = p3 Q1(p2) + p3^3 Q3(p2).  Terms up to n = NMAX are kept.
+Im H = p3 Q1(p2) + p3^3 Q3(p2).  Terms up to n = NMAX are formed, then every
+monomial whose largest value over the series domain (largest phase difference
+D <= DMAX, so p2 <= 2 D^2/3 and |p3| <= 2 D^3/9) is below DROP is dropped.
 
     python deltamic_b200/csrc/gen_series.py > deltamic_b200/csrc/series_coeffs.cuh
 """
@@ -17,6 +19,8 @@ from fractions import Fraction
 from math import factorial
 
 NMAX = 14
+DMAX = 3.5
+DROP = 1e-9
 
 
 def h_polys(nmax):
@@ -46,8 +50,10 @@ def series(nmax=NMAX):
 
 
 def poly(d, k):
-    """Coefficients (ascending in p2) of the p3^k part."""
-    js = [j for (j, kk) in d if kk == k]
+    """Coefficients (ascending in p2) of the p3^k part, truncated by DROP."""
+    p2max, p3max = 2 * DMAX ** 2 / 3, 2 * DMAX ** 3 / 9
+    js = [j for (j, kk), c in d.items()
+          if kk == k and abs(float(c)) * p2max ** j * p3max ** k >= DROP]
     if not js:
         return []
     return [d.get((j, k), Fraction(0)) for j in range(max(js) + 1)]
@@ -56,11 +62,12 @@ def poly(d, k):
 def main():
     re, im = series()
     print("// Generated by gen_series.py (do not edit): centroid-series coefficients,")
-    print(f"// terms n <= {NMAX}.  Ascending powers of p2.")
+    print(f"// terms n <= {NMAX}, monomials below {DROP:g} for D <= {DMAX} dropped.")
+    print("// Ascending powers of p2.")
     print("#pragma once")
     for name, d, k in (("P0", re, 0), ("P2", re, 2), ("P4", re, 4), ("Q1", im, 1),
                        ("Q3", im, 3)):
-        c = poly(d, k)
+        c = poly(d, k) or [Fraction(0)]
         vals = ", ".join(f"{float(x):.9e}f" for x in c)
         print(f"#define DM_SERIES_{name}_N {len(c)}")
         print(f"#define DM_SERIES_{name} {{{vals}}}")

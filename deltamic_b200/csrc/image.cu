@@ -78,17 +78,27 @@ __global__ void k_img_minmax(const float2* __restrict__ z, int64_t n, MinMaxPart
   }
 }
 
+__device__ __forceinline__ void mm_merge(MinMaxPart& r, const MinMaxPart& o) {
+  if (o.mn < r.mn || (o.mn == r.mn && o.imn < r.imn)) { r.mn = o.mn; r.imn = o.imn; }
+  if (o.mx > r.mx || (o.mx == r.mx && o.imx < r.imx)) { r.mx = o.mx; r.imx = o.imx; }
+}
+
+// One block: each thread merges a fixed strided subset, then a fixed tree.
 __global__ void k_img_minmax_final(const MinMaxPart* __restrict__ part, int nb, ImgWs* ws) {
-  if (threadIdx.x != 0) return;
-  MinMaxPart r = part[0];
-  for (int b = 1; b < nb; ++b) {
-    const MinMaxPart o = part[b];
-    if (o.mn < r.mn || (o.mn == r.mn && o.imn < r.imn)) { r.mn = o.mn; r.imn = o.imn; }
-    if (o.mx > r.mx || (o.mx == r.mx && o.imx < r.imx)) { r.mx = o.mx; r.imx = o.imx; }
+  __shared__ MinMaxPart sh[kImgThreads];
+  MinMaxPart r{INFINITY, -INFINITY, INT64_MAX, INT64_MAX};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) mm_merge(r, part[b]);
+  sh[threadIdx.x] = r;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) mm_merge(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
   }
-  ws->stats = ImgStats{r.mn, r.mx, r.imn, r.imx};
-  ws->tie_count[0] = 0;
-  ws->tie_count[1] = 0;
+  if (threadIdx.x == 0) {
+    ws->stats = ImgStats{sh[0].mn, sh[0].mx, sh[0].imn, sh[0].imx};
+    ws->tie_count[0] = 0;
+    ws->tie_count[1] = 0;
+  }
 }
 
 // Per element: normalised value, loss term, dL/dimage without the min/max
@@ -172,15 +182,31 @@ __global__ void k_img_final(const float2* __restrict__ z, int64_t n, int kind, f
                             float* __restrict__ loss, float2* __restrict__ grad_z) {
   __shared__ double fin[3];
   __shared__ long long cnt[2];
-  if (threadIdx.x == 0) {
+  __shared__ LossPart sh[256];
+  {
     LossPart r{0, 0, 0, 0, 0};
-    for (int b = 0; b < nb; ++b) {
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
       r.loss += part[b].loss;
       r.dmn += part[b].dmn;
       r.dmx += part[b].dmx;
       r.cmn += part[b].cmn;
       r.cmx += part[b].cmx;
     }
+    sh[threadIdx.x] = r;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) {
+        sh[threadIdx.x].loss += sh[threadIdx.x + o].loss;
+        sh[threadIdx.x].dmn += sh[threadIdx.x + o].dmn;
+        sh[threadIdx.x].dmx += sh[threadIdx.x + o].dmx;
+        sh[threadIdx.x].cmn += sh[threadIdx.x + o].cmn;
+        sh[threadIdx.x].cmx += sh[threadIdx.x + o].cmx;
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    const LossPart r = sh[0];
     const double rng = (double)ws->stats.mx - (double)ws->stats.mn;
     const double inv = 1.0 / (rng * (1.0 + contrast));
     fin[0] = kind == 0 ? r.loss : r.loss / (double)n;
@@ -244,7 +270,7 @@ int launch_image_loss(const float2* z, int64_t n, int kind, const float* target,
   MinMaxPart* mm = (MinMaxPart*)(base + ((sizeof(ImgWs) + 255) / 256) * 256);
   LossPart* lp = (LossPart*)(mm + nb);
   k_img_minmax<<<nb, kImgThreads, 0, st>>>(z, n, mm);
-  k_img_minmax_final<<<1, 32, 0, st>>>(mm, nb, ws);
+  k_img_minmax_final<<<1, kImgThreads, 0, st>>>(mm, nb, ws);
   k_img_loss<<<nb, kImgThreads, 0, st>>>(z, n, kind, target, contrast, image, grad_z, ws, lp);
   k_img_final<<<1, 256, 0, st>>>(z, n, kind, contrast, lp, nb, ws, loss, grad_z);
   if (grad_z) k_img_ties_full<<<nb, kImgThreads, 0, st>>>(z, n, ws, grad_z);
@@ -283,7 +309,7 @@ __global__ void k_bump(int64_t* step) { *step += 1; }
 
 int launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
                 float b2, float eps, int64_t* step, cudaStream_t st) {
-  if (n <= (1 << 20)) {
+  if (n <= 4096) {
     k_adam<<<1, 1024, 0, st>>>(p, g, m, v, n, lr, b1, b2, eps, step, 1);
     count_launches(1);
   } else {

@@ -111,13 +111,15 @@ def image_loss_backward(img, kind="sum", target=None, c=0.0):
 
 def pipeline(verts, faces, coeff, box_size, box_shape, sigma, thresh,
              loss="sum", target=None, contrast=0.0, seps=SEPS_F32, threads=None,
-             grads=True):
+             grads=True, ft_perturb=None):
     """Full oracle pass: OTF -> band -> meshFT -> render -> normalise -> loss.
 
     ``verts`` are in the box frame of the caller (unshifted); they are shifted by
     ``box_size[:,0]`` as ``Fourier3dMesh.forward`` does.  Returns a dict with the
     band indices, ``ft_list``, image, loss and (if ``grads``) the gradients with
-    respect to verts, Faces_coeff and sigma.
+    respect to verts, Faces_coeff and sigma.  ``ft_perturb(ft) -> ft`` replaces the
+    spectrum before rendering (used to measure how strongly the gradients react
+    to rounding-level changes of the spectrum).
     """
     box_size = np.asarray(box_size, np.float64)
     axes = frequency_axes(box_size, box_shape)
@@ -126,6 +128,8 @@ def pipeline(verts, faces, coeff, box_size, box_shape, sigma, thresh,
     xi = xi_list_from_band(idx, axes)
     v = np.asarray(verts, np.float64) - box_size[:, 0]
     ft = meshft_forward(v, faces, coeff, xi, seps=seps, threads=threads)
+    if ft_perturb is not None:
+        ft = ft_perturb(ft)
     img, z = render_from_band(ft, idx, otf)
     out = dict(idx=idx, xi=xi, ft=ft, otf=otf, image=img,
                loss=image_loss(img, loss, target, contrast))
@@ -147,3 +151,27 @@ def pipeline(verts, faces, coeff, box_size, box_shape, sigma, thresh,
     out.update(grad_verts=gv, grad_coeff=gc, grad_sigma=gsig, grad_ft=g_ft,
                grad_otf_band=g_otf)
     return out
+
+
+def chain_floor(verts, faces, coeff, box_size, box_shape, sigma, thresh, loss="sum",
+                target=None, rel=3e-7, trials=2, seed=0):
+    """Conditioning floor of the render-chain gradients: the largest relative
+    change of the (verts, coeff, sigma) gradients when the spectrum is perturbed by
+    complex noise of relative size ``rel`` (float32 rounding level)."""
+    base = pipeline(verts, faces, coeff, box_size, box_shape, sigma, thresh, loss, target)
+    rng = np.random.default_rng(seed)
+    worst = np.zeros(3)
+
+    def rl(a, b):
+        return np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+    for _ in range(trials):
+        def pert(ft):
+            n = rng.normal(size=ft.shape) + 1j * rng.normal(size=ft.shape)
+            return ft + n * np.abs(ft) * rel
+        o = pipeline(verts, faces, coeff, box_size, box_shape, sigma, thresh, loss, target,
+                     ft_perturb=pert)
+        worst = np.maximum(worst, [rl(o["grad_verts"], base["grad_verts"]),
+                                   rl(o["grad_coeff"], base["grad_coeff"]),
+                                   rl(o["grad_sigma"], base["grad_sigma"])])
+    return dict(verts=float(worst[0]), coeff=float(worst[1]), sigma=float(worst[2]))

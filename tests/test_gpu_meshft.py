@@ -1,8 +1,9 @@
 """CUDA meshFT forward / adjoint against the float64 oracle and the reference's
 golden vectors.  Tolerances (rel-L2, float32 kernels vs float64):
   ft_list 1e-5, vertex gradient 1e-4, Faces_coeff gradient 1e-5 for the meshFT
-  adjoint with a given cotangent; 1e-3 (vertices) and 1e-4 (Faces_coeff, sigma)
-  through the whole float32 render chain (FFT, |.|, normalize, loss)."""
+  adjoint with a given cotangent; through the whole float32 render chain (FFT,
+  |.|, normalize, loss) 2e-4 (vertices) and 1e-4 (Faces_coeff, sigma), or twice
+  the chain's conditioning floor where that is larger (oracle.chain_floor)."""
 import numpy as np
 import pytest
 import torch
@@ -17,7 +18,7 @@ pytestmark = pytest.mark.gpu
 TOL_FT = 1e-5
 TOL_GV = 1e-4
 TOL_GC = 1e-5
-TOL_CHAIN_V = 1e-3
+TOL_CHAIN_V = 2e-4
 TOL_CHAIN = 1e-4
 
 DEV = "cuda:0"
@@ -115,11 +116,17 @@ def test_drop_in_chain_matches_reference_golden(golden):
               ec, rel_l2(d["grad_coeff_f32"], d["grad_coeff"]),
               es, rel_l2(d["grad_sigma_f32"], d["grad_sigma"])))
     assert abs(float(loss.detach()) - float(d["loss"])) < 1e-4 * abs(float(d["loss"])), name
-    # full-chain tolerances: float32 FFT noise in dark voxels (|z| ~ 0, where
-    # d|z|/dz = z/|z| is ill-conditioned) bounds the agreement of any float32 chain
-    assert ev < TOL_CHAIN_V, name
-    assert ec < TOL_CHAIN, name
-    assert es < TOL_CHAIN, name
+    # Through |.| and normalize_tensor the gradients can be ill-conditioned in the
+    # spectrum (d|z|/dz = z/|z| at near-zero voxels, the argmin voxel): the floor
+    # is how much the float64 gradients move under a 3e-7 relative perturbation
+    # of the spectrum; agreement is required to the larger of the fixed
+    # tolerance and twice that floor.
+    fl = oracle.chain_floor(d["verts"], d["faces"], d["coeff"], d["box_size"], shape,
+                            d["sigma"], float(d["thresh"]), str(d["loss_kind"]), d.get("target"))
+    print(name, "conditioning floor", fl)
+    assert ev < max(TOL_CHAIN_V, 2 * fl["verts"]), name
+    assert ec < max(TOL_CHAIN, 2 * fl["coeff"]), name
+    assert es < max(TOL_CHAIN, 2 * fl["sigma"]), name
 
 
 def test_deterministic_bitwise():

@@ -12,7 +12,7 @@ from deltamic_b200.mesh import random_sh_shape
 
 pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
-TOL_CHAIN_V = 1e-3
+TOL_CHAIN_V = 2e-4
 TOL_CHAIN = 1e-4
 
 
@@ -126,8 +126,11 @@ def test_fused_renderer_matches_oracle_pipeline():
     print("fused renderer vs oracle: loss %.2e verts %.2e coeff %.2e sigma %.2e" % (
         abs(float(loss) - o["loss"]) / abs(o["loss"]), ev, ec, es))
     assert abs(float(loss) - o["loss"]) < 1e-4 * abs(o["loss"])
-    # full-chain tolerance: float32 FFT noise in the dark voxels, where |z| ~ 0
-    # and d|z|/dz = z/|z| is ill-conditioned, bounds the achievable agreement
-    assert ev < TOL_CHAIN_V
-    assert ec < TOL_CHAIN
-    assert es < TOL_CHAIN
+    # chain tolerance: the larger of a fixed bound and twice the conditioning
+    # floor of the float64 gradients (see test_gpu_meshft)
+    fl = oracle.chain_floor(v, f, c, box, shape, S.detach().cpu().double().numpy(), 1e-5,
+                            "mse", T.cpu().double().numpy())
+    print("conditioning floor", fl)
+    assert ev < max(TOL_CHAIN_V, 2 * fl["verts"])
+    assert ec < max(TOL_CHAIN, 2 * fl["coeff"])
+    assert es < max(TOL_CHAIN, 2 * fl["sigma"])
