@@ -51,6 +51,8 @@ SIGNATURES = {
     "dm_meshft_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_forward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _P, _SZ,
                                  _P]),
+    "dm_meshft_forward_noalloc": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P,
+                                         _P]),
     "dm_meshft_backward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_backward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _F, _P,
                                   _P, _P, _P, _P, _P, _SZ, _P]),

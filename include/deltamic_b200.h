@@ -96,6 +96,18 @@ int dm_meshft_forward(const float* verts, int64_t nv, const int64_t* faces, int6
                       int64_t n_band, const float* otf, float* ft_list, float* grid,
                       void* workspace, size_t ws_bytes, dm_stream_t stream);
 
+/* meshFT forward for callers that cannot allocate device memory (no counterpart
+ * in the reference).  Same arguments and results as dm_meshft_forward minus the
+ * workspace: scratch is a fixed 8 MiB array inside this library (held on every
+ * GPU that loads it).  Requests needing more workspace than that return
+ * DM_ERR_SIZE before anything is enqueued.  The first call on a device looks up
+ * the array's address (make it before any stream capture); calls share the
+ * array, so calls that overlap on the GPU race. */
+int dm_meshft_forward_noalloc(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                              const float* faces_coeff, const dm_box* box,
+                              const int32_t* band_index, int64_t n_band, const float* otf,
+                              float* ft_list, float* grid, dm_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * meshFT backward.  Replaces backward_fourier3d_cpp
  * (deltamic/cpp/fourier3d_cuda.cpp:44-65, :114; kernels .cu:314-416, host prep
