@@ -41,6 +41,7 @@ LR = 1e-3
 FWD_FP32, FWD_MUFU = 32, 7
 BWD_FP32, BWD_MUFU = 80, 9
 METRIC = "meshFT face*xi pairs/s (fit step: fwd+bwd, 200^3, 20,480 faces)"
+METRIC_BATCH = "meshFT face*xi pairs/s (batched fit step: 64 cells, fwd+bwd)"
 
 
 def parse():
@@ -53,12 +54,26 @@ def parse():
     p.add_argument("--small", action="store_true",
                    help="level-3 mesh at 64^3 (for profiler captures)")
     p.add_argument("--skip-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["fit200", "batch64"], default="fit200",
+                   help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
+                        "cells of mixed sizes per step")
     return p.parse_args()
 
 
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value, device="cpu"):
+    """Largest ``value`` over all ranks (the value itself without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0])
 
 
 def make_workload(rank, small=False):
@@ -185,16 +200,21 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
-def run_ours(args, rank, world, local):
+def noisy_target(img, gen, shape_numel, dev):
+    """Render scaled to 200 photons, Poisson + N(0, 2^2) read noise, normalised."""
     import torch
-    import torch.distributed as dist
-    import oracle
-    from deltamic_b200 import MeshRenderer, normalize_tensor, _native as N
-    from deltamic_b200.fit import FitStep
+    from deltamic_b200 import normalize_tensor
+    photons = img / img.max() * 200.0
+    noisy = torch.poisson(photons, generator=gen) + 2.0 * torch.randn(
+        img.shape, device=dev, generator=gen)
+    return normalize_tensor(noisy).contiguous()
 
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    lib = N.lib()
+
+def setup_fit200(args, rank, dev):
+    """configs: 200^3 single-mesh fit (level-5 meshes, 20,480 faces)."""
+    import torch
+    from deltamic_b200 import MeshRenderer
+    from deltamic_b200.fit import FitStep
     gt_v, init_v, faces_np, box = make_workload(rank, args.small)
     shape = (64, 64, 64) if args.small else SHAPE
     r = MeshRenderer(box, shape, THRESH, dev)
@@ -203,15 +223,87 @@ def run_ours(args, rank, world, local):
     C = torch.ones(len(faces_np), device=dev)
     gen = torch.Generator(device=dev).manual_seed(99 + rank)
     img = r.render(torch.tensor(gt_v, dtype=torch.float32, device=dev), F, C)
-    photons = img / img.max() * 200.0
-    noisy = torch.poisson(photons, generator=gen) + 2.0 * torch.randn(
-        shape, device=dev, generator=gen)
-    target = normalize_tensor(noisy).contiguous()
+    target = noisy_target(img, gen, img.numel(), dev)
     V = torch.tensor(init_v, dtype=torch.float32, device=dev)
-    nt, nb = len(faces_np), r.n_band
-    pairs = nt * nb
+    pairs = len(faces_np) * r.n_band
 
-    step = FitStep(r, V, F, C, target, "mse", 0.0, LR, graph=not args.no_graph)
+    def make_step(graph):
+        return FitStep(r, V.clone(), F, C, target, "mse", 0.0, LR, graph=graph)
+
+    def e2e_call(Vd):
+        loss = r.loss(Vd, F, C, "mse", target)
+        loss.backward()
+        return loss
+
+    info = {"workload": ("fit64-small" if args.small else
+                         "fit200: Adam step fitting a level-5 sphere to a level-5 SH shape, "
+                         "200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5"),
+            "n_verts": int(len(init_v)), "n_faces": int(len(faces_np)),
+            "n_band": int(r.n_band), "box_shape": list(shape)}
+    cpu = dict(gt_v=gt_v, faces=faces_np, box=box, shape=shape, band=r.band)
+    return make_step, e2e_call, init_v, pairs, info, cpu
+
+
+def setup_batch64(args, rank, dev):
+    """configs: 64 cells (level 2-5, 64/96/128^3, per-cell PSF and coefficients)."""
+    import torch
+    import oracle
+    from deltamic_b200.batch import BatchFitStep, BatchRenderer
+    from deltamic_b200.mesh import icosphere, random_sh_shape
+    rng = np.random.default_rng(4242 + rank)
+    ncells = 8 if args.small else 64
+    gts, inits, faces, coeffs, boxes, shapes, sigmas = [], [], [], [], [], [], []
+    for i in range(ncells):
+        level = int(rng.integers(2, 6)) if not args.small else int(rng.integers(2, 4))
+        n = int(rng.choice([64, 96, 128])) if not args.small else 48
+        gt, f = random_sh_shape(level, 0.3, 6, 0.08, seed=int(rng.integers(1 << 30)))
+        init, _ = icosphere(level, 0.3)
+        gts.append(gt)
+        inits.append(init)
+        faces.append(f)
+        coeffs.append(rng.uniform(0.5, 1.5, len(f)))
+        boxes.append(oracle.compute_box_size(np.concatenate([gt, init]), 0.2))
+        shapes.append((n, n, n))
+        sigmas.append(np.diag(rng.uniform(5e-4, 4e-3, 3)))
+    br = BatchRenderer(boxes, shapes, THRESH, dev)
+    br.set_sigmas(sigmas)
+    br.set_meshes(gts, faces)
+    C = torch.tensor(np.concatenate(coeffs), dtype=torch.float32, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(77 + rank)
+    img = br.render(torch.tensor(np.concatenate(gts), dtype=torch.float32, device=dev), C)
+    target = torch.empty_like(img)
+    for i in range(ncells):
+        br.cell_view(target, i).copy_(noisy_target(br.cell_view(img, i), gen, 0, dev))
+    V = torch.tensor(np.concatenate(inits), dtype=torch.float32, device=dev)
+
+    def make_step(graph):
+        return BatchFitStep(br, V.clone(), C, target, "mse", 0.0, LR, graph=graph)
+
+    def e2e_call(Vd):
+        loss = br.loss(Vd, C, "mse", target)
+        loss.backward()
+        return loss
+
+    info = {"workload": f"batch{ncells}: {ncells} cells, levels 2-5, 64/96/128^3, sigma diag "
+                        "U[5e-4,4e-3], Faces_coeff U[0.5,1.5], summed per-cell image L2",
+            "n_cells": ncells, "n_verts": int(V.shape[0]), "n_faces": int(sum(br.nt)),
+            "n_band": int(br.band.numel())}
+    return make_step, e2e_call, np.concatenate(inits), br.pairs, info, None
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from deltamic_b200 import _native as N
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.lib()
+    setup = setup_batch64 if args.workload == "batch64" else setup_fit200
+    make_step, e2e_call, init_v, pairs, info, cpu_case = setup(args, rank, dev)
+
+    step = make_step(not args.no_graph)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -232,18 +324,14 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     loss_end = float(step.loss[0])
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0])
+    ms = max_over_ranks(ms, dev)
 
     # roofline: the meshFT kernels timed with events on their stream (eager steps)
-    eager = FitStep(r, V.clone(), F, C, target, "mse", 0.0, LR, graph=False)
+    eager = make_step(False)
     eager()
     torch.cuda.synchronize()
     lib.dm_profile_enable(1)
-    nprof = 10
-    for _ in range(nprof):
+    for _ in range(10):
         eager()
     torch.cuda.synchronize()
     cnt, tot = N._INT(), N._F()
@@ -269,13 +357,12 @@ def run_ours(args, rank, world, local):
     host_v = torch.tensor(init_v, dtype=torch.float32).pin_memory()
     host_g = torch.empty_like(host_v).pin_memory()
     host_l = torch.empty(1).pin_memory()
-    Vd = torch.empty_like(V)
+    Vd = torch.empty(host_v.shape, dtype=torch.float32, device=dev)
 
     def e2e_step():
         Vd.copy_(host_v, non_blocking=True)
         Vp = Vd.requires_grad_(True)
-        loss = r.loss(Vp, F, C, "mse", target)
-        loss.backward()
+        loss = e2e_call(Vp)
         host_g.copy_(Vp.grad, non_blocking=True)
         host_l.copy_(loss.detach().view(1), non_blocking=True)
         Vp.grad = None
@@ -291,22 +378,24 @@ def run_ours(args, rank, world, local):
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t[0])
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
-        axes = oracle.frequency_axes(box, shape)
-        band_xi = oracle.xi_list_from_band(r.band.cpu().numpy().astype(np.int64), axes)
-        cpu = cpu_baseline(gt_v, faces_np, box, band_xi)
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline and cpu_case is not None:
+        axes = oracle.frequency_axes(cpu_case["box"], cpu_case["shape"])
+        band_xi = oracle.xi_list_from_band(cpu_case["band"].cpu().numpy().astype(np.int64), axes)
+        cpu = cpu_baseline(cpu_case["gt_v"], cpu_case["faces"], cpu_case["box"], band_xi)
 
     if rank != 0:
         return
+    config = dict(info)
+    config.update({
+        "pairs_per_step": int(pairs), "cuda_graph": not args.no_graph,
+        "parallelism": "replicas only (one workload per GPU)",
+        "l2_flush": "no: the step streams >256 MB of complex grids (> 126 MB L2)",
+        "loss_last_step": loss_end})
     out = {
-        "metric": METRIC,
+        "metric": METRIC if args.workload == "fit200" else METRIC_BATCH,
         "value": pairs * world / (ms * 1e-3),
         "unit": "pairs/s",
         "n_gpus": world,
@@ -318,16 +407,7 @@ def run_ours(args, rank, world, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded SH shapes, Poisson + Gaussian noise)",
-        "config": {
-            "workload": ("fit64-small" if args.small else
-                         "fit200: Adam step fitting a level-5 sphere to a level-5 SH shape, "
-                         "200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5"),
-            "n_verts": int(len(init_v)), "n_faces": int(nt), "n_band": int(nb),
-            "pairs_per_step": int(pairs), "box_shape": list(shape),
-            "cuda_graph": not args.no_graph, "parallelism": "replicas only (one mesh per GPU)",
-            "l2_flush": "no: the step streams >256 MB of complex grids (> 126 MB L2)",
-            "loss_last_step": loss_end,
-        },
+        "config": config,
         "gpu_launches": int((step.launches_per_step or 0) * args.steps),
         "clocks": clk,
         "e2e": {"value": pairs * world / (e2e_ms * 1e-3), "unit": "pairs/s",

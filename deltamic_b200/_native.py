@@ -40,6 +40,23 @@ class DmBox(ctypes.Structure):
 
 _BOXP = ctypes.POINTER(DmBox)
 
+
+class DmCell(ctypes.Structure):
+    _fields_ = [("nv", ctypes.c_int64), ("nt", ctypes.c_int64), ("n_band", ctypes.c_int64),
+                ("grid_offset", ctypes.c_int64), ("box", DmBox)]
+
+
+class DmBatch(ctypes.Structure):
+    _fields_ = [("ncells", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("nv", ctypes.c_int64), ("nt", ctypes.c_int64), ("n_band", ctypes.c_int64),
+                ("grid_elems", ctypes.c_int64), ("fwd_workspace", ctypes.c_int64),
+                ("bwd_workspace", ctypes.c_int64), ("topology_bytes", ctypes.c_int64),
+                ("image_workspace", ctypes.c_int64), ("plan", ctypes.c_int64 * 12),
+                ("cells", ctypes.c_void_p)]
+
+
+_BATCHP = ctypes.POINTER(DmBatch)
+
 SIGNATURES = {
     "dm_abi_version": (_INT, []),
     "dm_status_string": (ctypes.c_char_p, [_INT]),
@@ -56,6 +73,13 @@ SIGNATURES = {
     "dm_meshft_backward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_backward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _F, _P,
                                   _P, _P, _P, _P, _P, _SZ, _P]),
+    "dm_batch_desc_size": (_SZ, [_INT]),
+    "dm_batch_plan": (_INT, [ctypes.POINTER(DmCell), _INT, _P, _SZ, _BATCHP, _P]),
+    "dm_batched_topology_build": (_INT, [_BATCHP, _P, _P, _SZ, _P]),
+    "dm_batched_meshft_forward": (_INT, [_BATCHP, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "dm_batched_meshft_backward": (_INT, [_BATCHP, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P, _P,
+                                          _P, _P, _P, _SZ, _P]),
+    "dm_batched_image_loss": (_INT, [_BATCHP, _P, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     "dm_gaussian_otf": (_INT, [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
                                _P, _P]),
     "dm_gaussian_otf_grad_workspace_size": (_SZ, [_I64]),

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include "../../include/deltamic_b200.h"
+#include "dm_common.cuh"
 
 namespace dm {
 
@@ -27,8 +28,12 @@ struct ImgStats {
 constexpr int kTieSlots = 1024;
 int image_blocks(int64_t n);
 size_t image_ws_bytes(int64_t n);
+size_t image_ws_bytes_segs(int64_t max_len, int nseg);
 int launch_image_loss(const float2* z, int64_t n, int kind, const float* target, float contrast,
                       float* image, float* loss, float2* grad_z, void* ws, cudaStream_t st);
+int launch_image_loss_cells(const CellDesc* cells, int ncells, int64_t max_len, const float2* z,
+                            int kind, const float* target, float contrast, float* image,
+                            float* loss, float2* grad_z, void* ws, cudaStream_t st);
 int launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
                 float b2, float eps, int64_t* step, cudaStream_t st);
 

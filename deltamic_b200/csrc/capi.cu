@@ -302,6 +302,163 @@ int dm_meshft_forward(const float* verts, int64_t nv, const int64_t* faces, int6
 }
 
 // ---------------------------------------------------------------------------
+// Batches
+
+static PlanTotals totals_of(const dm_batch* b) {
+  PlanTotals t;
+  t.nv = b->plan[0];
+  t.nt = b->plan[1];
+  t.nband = b->plan[2];
+  t.fpart = b->plan[3];
+  t.bpart = b->plan[4];
+  t.face_blks = b->plan[5];
+  t.band_blks = b->plan[6];
+  t.fwd_items = b->plan[7];
+  t.bwd_items = b->plan[8];
+  return t;
+}
+
+static Cells cells_of(const dm_batch* b) {
+  Cells c;
+  memset(&c, 0, sizeof(c));
+  c.p = (const CellDesc*)b->cells;
+  c.n = b->ncells;
+  return c;
+}
+
+static bool batch_ok(const dm_batch* b) { return b && b->ncells > 0 && b->cells; }
+
+size_t dm_batch_desc_size(int ncells) {
+  return ncells > 0 ? sizeof(CellDesc) * (size_t)ncells : 0;
+}
+
+int dm_batch_plan(const dm_cell* cells, int ncells, void* desc, size_t desc_bytes,
+                  dm_batch* out, dm_stream_t stream) {
+  if (!cells || ncells <= 0 || !desc || !out) return DM_ERR_INVALID_ARG;
+  if (desc_bytes < dm_batch_desc_size(ncells)) return DM_ERR_WORKSPACE;
+  CellDesc* d = new CellDesc[ncells];
+  int64_t grid_end = 0, max_grid = 0;
+  for (int i = 0; i < ncells; ++i) {
+    const dm_cell& c = cells[i];
+    if (!sizes_ok(c.nv, c.nt, c.n_band) || !box_ok(&c.box) || c.grid_offset < 0) {
+      delete[] d;
+      return DM_ERR_INVALID_ARG;
+    }
+    memset(&d[i], 0, sizeof(CellDesc));
+    for (int k = 0; k < 3; ++k) {
+      d[i].lo[k] = c.box.lo[k];
+      d[i].len[k] = c.box.hi[k] - c.box.lo[k];
+      d[i].n[k] = c.box.shape[k];
+    }
+    d[i].nv = (int32_t)c.nv;
+    d[i].nt = (int32_t)c.nt;
+    d[i].nband = (int32_t)c.n_band;
+    d[i].grid_off = c.grid_offset;
+    const int64_t g = (int64_t)c.box.shape[0] * c.box.shape[1] * c.box.shape[2];
+    grid_end = std::max(grid_end, c.grid_offset + g);
+    max_grid = std::max(max_grid, g);
+  }
+  PlanTotals t;
+  plan_offsets(d, ncells, t);
+  if (t.nv >= (int64_t)INT32_MAX / 3 || t.nt >= (int64_t)INT32_MAX / 9 ||
+      t.nband >= (int64_t)INT32_MAX || grid_end >= (int64_t)INT32_MAX ||
+      t.fwd_items >= (int64_t)INT32_MAX || t.bwd_items >= (int64_t)INT32_MAX) {
+    delete[] d;
+    return DM_ERR_SIZE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool ok = cudaMemcpyAsync(desc, d, sizeof(CellDesc) * ncells, cudaMemcpyHostToDevice,
+                                  st) == cudaSuccess &&
+                  cudaStreamSynchronize(st) == cudaSuccess;
+  delete[] d;
+  if (!ok) return DM_ERR_CUDA;
+  memset(out, 0, sizeof(*out));
+  out->ncells = ncells;
+  out->nv = t.nv;
+  out->nt = t.nt;
+  out->n_band = t.nband;
+  out->grid_elems = grid_end;
+  out->fwd_workspace = (int64_t)fwd_layout(nullptr, t, nullptr);
+  out->bwd_workspace = (int64_t)bwd_layout(nullptr, t, nullptr);
+  out->topology_bytes = (int64_t)topo_layout(nullptr, t.nv, t.nt, nullptr);
+  out->image_workspace = (int64_t)image_ws_bytes_segs(max_grid, ncells);
+  const int64_t p[9] = {t.nv, t.nt, t.nband, t.fpart, t.bpart,
+                        t.face_blks, t.band_blks, t.fwd_items, t.bwd_items};
+  for (int k = 0; k < 9; ++k) out->plan[k] = p[k];
+  out->plan[9] = max_grid;
+  out->cells = desc;
+  return DM_OK;
+}
+
+int dm_batched_topology_build(const dm_batch* batch, const int64_t* faces, void* topology,
+                              size_t topo_bytes, dm_stream_t stream) {
+  if (!batch_ok(batch) || !topology || (batch->nt > 0 && !faces)) return DM_ERR_INVALID_ARG;
+  if (topo_bytes < (size_t)batch->topology_bytes) return DM_ERR_WORKSPACE;
+  const PlanTotals t = totals_of(batch);
+  TopoWs w;
+  topo_layout(topology, t.nv, t.nt, &w);
+  return launch_topology(cells_of(batch), t, faces, w.count, w.off, w.cursor, w.ent, w.err,
+                         (cudaStream_t)stream);
+}
+
+int dm_batched_meshft_forward(const dm_batch* batch, const float* verts, const int64_t* faces,
+                              const float* faces_coeff, const int32_t* band_index,
+                              const float* otf, float* ft_list, float* grid, void* workspace,
+                              size_t ws_bytes, dm_stream_t stream) {
+  if (!batch_ok(batch) || !workspace) return DM_ERR_INVALID_ARG;
+  if (batch->nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (batch->n_band > 0 && (!band_index || !ft_list)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < (size_t)batch->fwd_workspace) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const PlanTotals t = totals_of(batch);
+  const Cells c = cells_of(batch);
+  FwdWs w;
+  fwd_layout(workspace, t, &w);
+  int s = launch_face_prep(c, t, verts, faces, faces_coeff, w.recs, w.area_part, w.err, st);
+  if (s) return s;
+  return launch_forward(c, t, w.recs, band_index, w.area_part, otf, w.fpart, (float2*)ft_list,
+                        (float2*)grid, w.err, st);
+}
+
+int dm_batched_meshft_backward(const dm_batch* batch, const float* verts, const int64_t* faces,
+                               const float* faces_coeff, const int32_t* band_index,
+                               const float* grad_list, const float* grad_grid, const float* otf,
+                               float grad_scale, const float* ft_list, const void* topology,
+                               float* grad_verts, float* grad_coeff, float* grad_otf_band,
+                               void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!batch_ok(batch) || !workspace || !topology) return DM_ERR_INVALID_ARG;
+  if (batch->nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (batch->nv > 0 && !grad_verts) return DM_ERR_INVALID_ARG;
+  if (batch->n_band > 0 && (!band_index || !ft_list || (!grad_list && !grad_grid)))
+    return DM_ERR_INVALID_ARG;
+  if (ws_bytes < (size_t)batch->bwd_workspace) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const PlanTotals t = totals_of(batch);
+  const Cells c = cells_of(batch);
+  BwdWs w;
+  bwd_layout(workspace, t, &w);
+  TopoWs tw;
+  topo_layout(const_cast<void*>(topology), t.nv, t.nt, &tw);
+  int s = launch_face_prep(c, t, verts, faces, faces_coeff, w.recs, w.area_part, w.err, st);
+  if (s) return s;
+  return launch_backward(c, t, verts, faces, faces_coeff, w.recs, w.area_part, band_index,
+                         (const float2*)grad_list, (const float2*)grad_grid, otf, grad_scale,
+                         (const float2*)ft_list, w.xrec, w.s_part, w.bpart, w.contrib, tw.off,
+                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.err, st);
+}
+
+int dm_batched_image_loss(const dm_batch* batch, const float* z, int kind, const float* target,
+                          float contrast, float* image, float* loss, float* grad_z,
+                          void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!batch_ok(batch) || !z || !loss || !workspace) return DM_ERR_INVALID_ARG;
+  if ((kind != 0 && kind != 1) || (kind == 1 && !target)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < (size_t)batch->image_workspace) return DM_ERR_WORKSPACE;
+  return launch_image_loss_cells((const CellDesc*)batch->cells, batch->ncells, batch->plan[9],
+                                 (const float2*)z, kind, target, contrast, image, loss,
+                                 (float2*)grad_z, workspace, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
 size_t dm_meshft_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
   if (!sizes_ok(nv, nt, n_band)) return 0;
   PlanTotals t;

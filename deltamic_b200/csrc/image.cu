@@ -24,7 +24,7 @@ struct LossPart {
   int64_t cmn, cmx;
 };
 
-// Workspace of dm_image_loss.
+// Per-image state of dm_image_loss (one per segment of a batched call).
 struct ImgWs {
   int err;
   int tie_count[2];   // recorded min / max ties (may exceed kTieSlots)
@@ -34,6 +34,27 @@ struct ImgWs {
   int64_t cnt[2];
   int32_t ties[2][kTieSlots];
 };
+constexpr size_t kImgWsStride = ((sizeof(ImgWs) + 255) / 256) * 256;
+
+// Segments of a launch: the images of the cells of a batch (CellDesc::grid_off
+// and box shape), or one image [0, n0).  Each segment gets ``bps`` blocks.
+struct Segs {
+  const CellDesc* cells;
+  int32_t nseg;
+  int32_t bps;
+  int64_t n0;
+};
+
+__device__ __forceinline__ void seg_range(const Segs& s, int seg, int64_t& b, int64_t& e) {
+  if (s.cells) {
+    const CellDesc& d = s.cells[seg];
+    b = d.grid_off;
+    e = b + (int64_t)d.n[0] * d.n[1] * d.n[2];
+  } else {
+    b = 0;
+    e = s.n0;
+  }
+}
 
 __device__ __forceinline__ float cabs(float2 z) { return sqrtf(fmaf(z.x, z.x, z.y * z.y)); }
 
@@ -42,52 +63,61 @@ int image_blocks(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
 }
 
-size_t image_ws_bytes(int64_t n) {
-  const size_t nb = (size_t)image_blocks(n);
-  return 256 + ((sizeof(ImgWs) + 255) / 256) * 256 + nb * sizeof(MinMaxPart) + nb * sizeof(LossPart);
+static int blocks_per_segment(int64_t max_len, int nseg) {
+  const int64_t b = (max_len + kImgThreads - 1) / kImgThreads;
+  const int64_t cap = std::max<int64_t>(1, (int64_t)148 * 16 / std::max(nseg, 1));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
 }
 
-__global__ void k_img_minmax(const float2* __restrict__ z, int64_t n, MinMaxPart* __restrict__ part) {
-  __shared__ MinMaxPart sh[kImgThreads / 32];
-  float mn = INFINITY, mx = -INFINITY;
-  int64_t imn = INT64_MAX, imx = INT64_MAX;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const float a = cabs(z[i]);
-    if (a < mn) { mn = a; imn = i; }
-    if (a > mx) { mx = a; imx = i; }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    const float omn = __shfl_down_sync(0xffffffffu, mn, o);
-    const float omx = __shfl_down_sync(0xffffffffu, mx, o);
-    const int64_t oimn = __shfl_down_sync(0xffffffffu, imn, o);
-    const int64_t oimx = __shfl_down_sync(0xffffffffu, imx, o);
-    if (omn < mn || (omn == mn && oimn < imn)) { mn = omn; imn = oimn; }
-    if (omx > mx || (omx == mx && oimx < imx)) { mx = omx; imx = oimx; }
-  }
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = MinMaxPart{mn, mx, imn, imx};
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    MinMaxPart r = sh[0];
-    for (int w = 1; w < kImgThreads / 32; ++w) {
-      const MinMaxPart o = sh[w];
-      if (o.mn < r.mn || (o.mn == r.mn && o.imn < r.imn)) { r.mn = o.mn; r.imn = o.imn; }
-      if (o.mx > r.mx || (o.mx == r.mx && o.imx < r.imx)) { r.mx = o.mx; r.imx = o.imx; }
-    }
-    part[blockIdx.x] = r;
-  }
+size_t image_ws_bytes_segs(int64_t max_len, int nseg) {
+  const size_t nb = (size_t)blocks_per_segment(max_len, nseg) * (size_t)std::max(nseg, 1);
+  return 256 + kImgWsStride * (size_t)std::max(nseg, 1) + nb * sizeof(MinMaxPart) +
+         nb * sizeof(LossPart);
 }
+
+size_t image_ws_bytes(int64_t n) { return image_ws_bytes_segs(n, 1); }
 
 __device__ __forceinline__ void mm_merge(MinMaxPart& r, const MinMaxPart& o) {
   if (o.mn < r.mn || (o.mn == r.mn && o.imn < r.imn)) { r.mn = o.mn; r.imn = o.imn; }
   if (o.mx > r.mx || (o.mx == r.mx && o.imx < r.imx)) { r.mx = o.mx; r.imx = o.imx; }
 }
 
-// One block: each thread merges a fixed strided subset, then a fixed tree.
-__global__ void k_img_minmax_final(const MinMaxPart* __restrict__ part, int nb, ImgWs* ws) {
-  __shared__ MinMaxPart sh[kImgThreads];
+__global__ void k_img_minmax(const float2* __restrict__ z, Segs sg, MinMaxPart* __restrict__ part) {
+  __shared__ MinMaxPart sh[kImgThreads / 32];
+  const int seg = blockIdx.x / sg.bps, loc = blockIdx.x % sg.bps;
+  int64_t b, e;
+  seg_range(sg, seg, b, e);
   MinMaxPart r{INFINITY, -INFINITY, INT64_MAX, INT64_MAX};
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) mm_merge(r, part[b]);
+  for (int64_t i = b + (int64_t)loc * blockDim.x + threadIdx.x; i < e;
+       i += (int64_t)sg.bps * blockDim.x) {
+    const float a = cabs(z[i]);
+    if (a < r.mn) { r.mn = a; r.imn = i; }
+    if (a > r.mx) { r.mx = a; r.imx = i; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    MinMaxPart q;
+    q.mn = __shfl_down_sync(0xffffffffu, r.mn, o);
+    q.mx = __shfl_down_sync(0xffffffffu, r.mx, o);
+    q.imn = __shfl_down_sync(0xffffffffu, r.imn, o);
+    q.imx = __shfl_down_sync(0xffffffffu, r.imx, o);
+    mm_merge(r, q);
+  }
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    MinMaxPart t = sh[0];
+    for (int w = 1; w < kImgThreads / 32; ++w) mm_merge(t, sh[w]);
+    part[blockIdx.x] = t;
+  }
+}
+
+// One block per segment: fixed strided subsets, then a fixed tree.
+__global__ void k_img_minmax_final(const MinMaxPart* __restrict__ part, Segs sg, char* wsb) {
+  __shared__ MinMaxPart sh[kImgThreads];
+  const int seg = blockIdx.x;
+  ImgWs* ws = (ImgWs*)(wsb + kImgWsStride * seg);
+  MinMaxPart r{INFINITY, -INFINITY, INT64_MAX, INT64_MAX};
+  for (int b = threadIdx.x; b < sg.bps; b += blockDim.x) mm_merge(r, part[seg * sg.bps + b]);
   sh[threadIdx.x] = r;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -103,19 +133,24 @@ __global__ void k_img_minmax_final(const MinMaxPart* __restrict__ part, int nb, 
 
 // Per element: normalised value, loss term, dL/dimage without the min/max
 // terms, dL/dz = g z/|z|; partial sums of the loss and of the min/max terms.
-__global__ void k_img_loss(const float2* __restrict__ z, int64_t n, int kind,
+__global__ void k_img_loss(const float2* __restrict__ z, Segs sg, int kind,
                            const float* __restrict__ target, float contrast,
-                           float* __restrict__ image, float2* __restrict__ grad_z, ImgWs* ws,
+                           float* __restrict__ image, float2* __restrict__ grad_z, char* wsb,
                            LossPart* __restrict__ part) {
   __shared__ double sh[3][kImgThreads / 32];
   __shared__ long long shc[2][kImgThreads / 32];
+  const int seg = blockIdx.x / sg.bps, loc = blockIdx.x % sg.bps;
+  int64_t b, e;
+  seg_range(sg, seg, b, e);
+  ImgWs* ws = (ImgWs*)(wsb + kImgWsStride * seg);
   const float mn = ws->stats.mn, mx = ws->stats.mx;
   const float rng = mx - mn;
   const float inv = 1.0f / (rng * (1.0f + contrast));
+  const float nseg_inv = 1.0f / (float)(e - b);
   double L = 0.0, dmn = 0.0, dmx = 0.0;
   long long cmn = 0, cmx = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = b + (int64_t)loc * blockDim.x + threadIdx.x; i < e;
+       i += (int64_t)sg.bps * blockDim.x) {
     const float2 zi = z[i];
     const float a = cabs(zi);
     const float u = (a - mn) / rng;
@@ -127,25 +162,25 @@ __global__ void k_img_loss(const float2* __restrict__ z, int64_t n, int kind,
     } else {
       const float dlt = nv - target[i];
       L += (double)dlt * dlt;
-      gn = 2.0f * dlt / (float)n;
+      gn = 2.0f * dlt * nseg_inv;
     }
     dmn += (double)gn * (-(1.0 - (double)u));
     dmx += (double)gn * (-(double)u);
     if (image) image[i] = a;
     if (grad_z) {
       const float g = gn * inv;
-      const float s = a > 0.f ? g / a : 0.f;
-      grad_z[i] = make_float2(s * zi.x, s * zi.y);
+      const float sc = a > 0.f ? g / a : 0.f;
+      grad_z[i] = make_float2(sc * zi.x, sc * zi.y);
     }
     if (a == mn) {
       ++cmn;
       const int slot = atomicAdd(&ws->tie_count[0], 1);
-      if (slot < kTieSlots) ws->ties[0][slot] = (int32_t)i;
+      if (slot < kTieSlots) ws->ties[0][slot] = (int32_t)(i - b);
     }
     if (a == mx) {
       ++cmx;
       const int slot = atomicAdd(&ws->tie_count[1], 1);
-      if (slot < kTieSlots) ws->ties[1][slot] = (int32_t)i;
+      if (slot < kTieSlots) ws->ties[1][slot] = (int32_t)(i - b);
     }
   }
   double v[3] = {L, dmn, dmx};
@@ -176,21 +211,27 @@ __global__ void k_img_loss(const float2* __restrict__ z, int64_t n, int kind,
   }
 }
 
-// Loss value, then the min/max gradient shared evenly by tied elements.
-__global__ void k_img_final(const float2* __restrict__ z, int64_t n, int kind, float contrast,
-                            const LossPart* __restrict__ part, int nb, ImgWs* ws,
+// One block per segment: loss value, then the min/max gradient shared evenly by
+// tied elements.
+__global__ void k_img_final(const float2* __restrict__ z, Segs sg, int kind, float contrast,
+                            const LossPart* __restrict__ part, char* wsb,
                             float* __restrict__ loss, float2* __restrict__ grad_z) {
   __shared__ double fin[3];
   __shared__ long long cnt[2];
   __shared__ LossPart sh[256];
+  const int seg = blockIdx.x;
+  int64_t b, e;
+  seg_range(sg, seg, b, e);
+  ImgWs* ws = (ImgWs*)(wsb + kImgWsStride * seg);
   {
     LossPart r{0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      r.loss += part[b].loss;
-      r.dmn += part[b].dmn;
-      r.dmx += part[b].dmx;
-      r.cmn += part[b].cmn;
-      r.cmx += part[b].cmx;
+    for (int k = threadIdx.x; k < sg.bps; k += blockDim.x) {
+      const LossPart& q = part[seg * sg.bps + k];
+      r.loss += q.loss;
+      r.dmn += q.dmn;
+      r.dmx += q.dmx;
+      r.cmn += q.cmn;
+      r.cmx += q.cmx;
     }
     sh[threadIdx.x] = r;
     __syncthreads();
@@ -209,12 +250,12 @@ __global__ void k_img_final(const float2* __restrict__ z, int64_t n, int kind, f
     const LossPart r = sh[0];
     const double rng = (double)ws->stats.mx - (double)ws->stats.mn;
     const double inv = 1.0 / (rng * (1.0 + contrast));
-    fin[0] = kind == 0 ? r.loss : r.loss / (double)n;
+    fin[0] = kind == 0 ? r.loss : r.loss / (double)(e - b);
     fin[1] = r.dmn * inv;
     fin[2] = r.dmx * inv;
     cnt[0] = r.cmn;
     cnt[1] = r.cmx;
-    *loss = (float)fin[0];
+    loss[seg] = (float)fin[0];
     ws->final_[0] = fin[0];
     ws->final_[1] = fin[1];
     ws->final_[2] = fin[2];
@@ -228,28 +269,32 @@ __global__ void k_img_final(const float2* __restrict__ z, int64_t n, int kind, f
     if (c <= 0 || c > kTieSlots) continue;  // overflow handled by k_img_ties_full
     const float add = (float)(fin[1 + k] / (double)c);
     for (int t = threadIdx.x; t < c; t += blockDim.x) {
-      const int32_t i = ws->ties[k][t];
+      const int64_t i = b + ws->ties[k][t];
       const float2 zi = z[i];
       const float a = cabs(zi);
-      const float s = a > 0.f ? add / a : 0.f;
-      grad_z[i].x += s * zi.x;
-      grad_z[i].y += s * zi.y;
+      const float sc = a > 0.f ? add / a : 0.f;
+      grad_z[i].x += sc * zi.x;
+      grad_z[i].y += sc * zi.y;
     }
     __syncthreads();
   }
 }
 
-// Only when more than kTieSlots elements tie at the min or max: distribute over
-// the whole image (the kernel returns at once otherwise).
-__global__ void k_img_ties_full(const float2* __restrict__ z, int64_t n, const ImgWs* ws,
+// Only when more than kTieSlots elements tie at a segment's min or max:
+// distribute over that whole image (blocks of other segments return at once).
+__global__ void k_img_ties_full(const float2* __restrict__ z, Segs sg, const char* wsb,
                                 float2* __restrict__ grad_z) {
+  const int seg = blockIdx.x / sg.bps, loc = blockIdx.x % sg.bps;
+  const ImgWs* ws = (const ImgWs*)(wsb + kImgWsStride * seg);
   const bool over0 = ws->cnt[0] > kTieSlots, over1 = ws->cnt[1] > kTieSlots;
   if (!over0 && !over1) return;
+  int64_t b, e;
+  seg_range(sg, seg, b, e);
   const float mn = ws->stats.mn, mx = ws->stats.mx;
   const float add0 = over0 ? (float)(ws->final_[1] / (double)ws->cnt[0]) : 0.f;
   const float add1 = over1 ? (float)(ws->final_[2] / (double)ws->cnt[1]) : 0.f;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = b + (int64_t)loc * blockDim.x + threadIdx.x; i < e;
+       i += (int64_t)sg.bps * blockDim.x) {
     const float2 zi = z[i];
     const float a = cabs(zi);
     float add = 0.f;
@@ -262,20 +307,33 @@ __global__ void k_img_ties_full(const float2* __restrict__ z, int64_t n, const I
   }
 }
 
-int launch_image_loss(const float2* z, int64_t n, int kind, const float* target, float contrast,
-                      float* image, float* loss, float2* grad_z, void* wsv, cudaStream_t st) {
-  const int nb = image_blocks(n);
-  char* base = (char*)wsv + 256;
-  ImgWs* ws = (ImgWs*)base;
-  MinMaxPart* mm = (MinMaxPart*)(base + ((sizeof(ImgWs) + 255) / 256) * 256);
+static int launch_image_loss_segs(const float2* z, const Segs& sg, int kind, const float* target,
+                                  float contrast, float* image, float* loss, float2* grad_z,
+                                  void* wsv, cudaStream_t st) {
+  const int nb = sg.nseg * sg.bps;
+  char* wsb = (char*)wsv + 256;
+  MinMaxPart* mm = (MinMaxPart*)(wsb + kImgWsStride * sg.nseg);
   LossPart* lp = (LossPart*)(mm + nb);
-  k_img_minmax<<<nb, kImgThreads, 0, st>>>(z, n, mm);
-  k_img_minmax_final<<<1, kImgThreads, 0, st>>>(mm, nb, ws);
-  k_img_loss<<<nb, kImgThreads, 0, st>>>(z, n, kind, target, contrast, image, grad_z, ws, lp);
-  k_img_final<<<1, 256, 0, st>>>(z, n, kind, contrast, lp, nb, ws, loss, grad_z);
-  if (grad_z) k_img_ties_full<<<nb, kImgThreads, 0, st>>>(z, n, ws, grad_z);
+  k_img_minmax<<<nb, kImgThreads, 0, st>>>(z, sg, mm);
+  k_img_minmax_final<<<sg.nseg, kImgThreads, 0, st>>>(mm, sg, wsb);
+  k_img_loss<<<nb, kImgThreads, 0, st>>>(z, sg, kind, target, contrast, image, grad_z, wsb, lp);
+  k_img_final<<<sg.nseg, 256, 0, st>>>(z, sg, kind, contrast, lp, wsb, loss, grad_z);
+  if (grad_z) k_img_ties_full<<<nb, kImgThreads, 0, st>>>(z, sg, wsb, grad_z);
   count_launches(4 + (grad_z ? 1 : 0));
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int launch_image_loss(const float2* z, int64_t n, int kind, const float* target, float contrast,
+                      float* image, float* loss, float2* grad_z, void* wsv, cudaStream_t st) {
+  Segs sg{nullptr, 1, blocks_per_segment(n, 1), n};
+  return launch_image_loss_segs(z, sg, kind, target, contrast, image, loss, grad_z, wsv, st);
+}
+
+int launch_image_loss_cells(const CellDesc* cells, int ncells, int64_t max_len, const float2* z,
+                            int kind, const float* target, float contrast, float* image,
+                            float* loss, float2* grad_z, void* wsv, cudaStream_t st) {
+  Segs sg{cells, ncells, blocks_per_segment(max_len, ncells), 0};
+  return launch_image_loss_segs(z, sg, kind, target, contrast, image, loss, grad_z, wsv, st);
 }
 
 // ---------------------------------------------------------------------------

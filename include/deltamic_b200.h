@@ -130,6 +130,55 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
                        dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Batches: many meshes ("cells"), each with its own box, grid shape and narrow
+ * band, in one launch per stage.  There is no batched counterpart in the
+ * reference (one mesh per Fourier3dMesh call, render.py:136-150); the per-cell
+ * results equal the single-cell calls above.
+ * Concatenation: verts[sum nv,3], faces[sum nt,3] with indices LOCAL to each
+ * cell's vertices, faces_coeff[sum nt], band_index[sum n_band] with indices LOCAL
+ * to each cell's grid, ft_list[sum n_band]; per-cell grids (otf, spectrum,
+ * image) live at grid_offset of one concatenated array. */
+typedef struct dm_cell {
+  int64_t nv, nt, n_band; /* this cell's mesh and band sizes */
+  int64_t grid_offset;    /* first element of its grid in the concatenated grids */
+  dm_box box;
+} dm_cell;
+
+typedef struct dm_batch {
+  int32_t ncells;
+  int32_t reserved;
+  int64_t nv, nt, n_band, grid_elems;           /* totals */
+  int64_t fwd_workspace, bwd_workspace;         /* workspace bytes for the calls below */
+  int64_t topology_bytes, image_workspace;
+  int64_t plan[12];                             /* launch sizes (opaque) */
+  const void* cells;                            /* device copy of the cell plan */
+} dm_batch;
+
+/* Bytes of the device buffer that holds the plan of ``ncells`` cells. */
+size_t dm_batch_desc_size(int ncells);
+/* Plans the batch, uploads the cell plan into ``desc`` (device, desc_bytes) and
+ * fills *out.  Synchronous (waits for the upload): call it outside stream capture,
+ * once per set of meshes and bands. */
+int dm_batch_plan(const dm_cell* cells, int ncells, void* desc, size_t desc_bytes,
+                  dm_batch* out, dm_stream_t stream);
+int dm_batched_topology_build(const dm_batch* batch, const int64_t* faces, void* topology,
+                              size_t topo_bytes, dm_stream_t stream);
+int dm_batched_meshft_forward(const dm_batch* batch, const float* verts, const int64_t* faces,
+                              const float* faces_coeff, const int32_t* band_index,
+                              const float* otf, float* ft_list, float* grid, void* workspace,
+                              size_t ws_bytes, dm_stream_t stream);
+int dm_batched_meshft_backward(const dm_batch* batch, const float* verts, const int64_t* faces,
+                               const float* faces_coeff, const int32_t* band_index,
+                               const float* grad_list, const float* grad_grid, const float* otf,
+                               float grad_scale, const float* ft_list, const void* topology,
+                               float* grad_verts, float* grad_coeff, float* grad_otf_band,
+                               void* workspace, size_t ws_bytes, dm_stream_t stream);
+/* dm_image_loss per cell image (loss[ncells], each normalised by its own min/max). */
+int dm_batched_image_loss(const dm_batch* batch, const float* z, int kind, const float* target,
+                          float contrast, float* image, float* loss, float* grad_z,
+                          void* workspace, size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Gaussian OTF.  Replaces generate_gaussian_psf (deltamic/psf.py:15-20):
  *   otf[i,j,k] = exp(-(x^T S x)/2),  x = (xi0[i], xi1[j], xi2[k]),
  * S = sigma[3,3] (DEVICE float32, row-major, as the torch parameter), on the
