@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--small", action="store_true",
                    help="level-3 mesh at 64^3 (for profiler captures)")
     p.add_argument("--skip-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["fit200", "batch64"], default="fit200",
+    p.add_argument("--workload", choices=["fit200", "batch64", "fit300"], default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
                         "cells of mixed sizes per step")
     return p.parse_args()
@@ -291,6 +291,43 @@ def setup_batch64(args, rank, dev):
     return make_step, e2e_call, np.concatenate(inits), br.pairs, info, None
 
 
+def run_fit300(args, rank, world, local):
+    """Time-to-fit of the plain sphere-initialised fit: 300 Adam steps (lr 1e-3) on
+    image L2 at 200^3, final image L2 and volumetric IoU against the ground truth."""
+    import torch
+    from deltamic_b200 import MeshRenderer
+    from deltamic_b200.fit import mesh_iou, run_fit
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    gt_v, init_v, faces_np, box = make_workload(rank, args.small)
+    shape = (64, 64, 64) if args.small else SHAPE
+    r = MeshRenderer(box, shape, THRESH, dev)
+    r.set_sigma(torch.diag(torch.tensor(SIGMA, device=dev)))
+    F = torch.tensor(faces_np, device=dev)
+    C = torch.ones(len(faces_np), device=dev)
+    gen = torch.Generator(device=dev).manual_seed(99 + rank)
+    G = torch.tensor(gt_v, dtype=torch.float32, device=dev)
+    target = noisy_target(r.render(G, F, C), gen, 0, dev)
+    V0 = torch.tensor(init_v, dtype=torch.float32, device=dev)
+    run_fit(r, V0, F, C, target, steps=3, lr=LR)  # warm-up: graph capture, plans
+    res = run_fit(r, V0, F, C, target, steps=300, lr=LR)
+    iou0 = mesh_iou(V0, G, F, r.grid)
+    iou1 = mesh_iou(res["verts"], G, F, r.grid)
+    ms = max_over_ranks(res["ms_total"], dev)
+    if rank != 0:
+        return
+    out = {"metric": "time-to-fit: plain sphere-init fit, 300 Adam steps at 200^3",
+           "value": ms, "unit": "ms", "n_gpus": world, "steps": 300, "warmup": 3,
+           "ms_per_step": ms / 300, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "fit300: level-5 sphere -> level-5 SH shape, 200^3, "
+                                  "sigma diag(1e-3,1e-3,4e-3), Poisson+read noise target",
+                      "image_l2_first": float(res["losses"][0]),
+                      "image_l2_final": float(res["losses"][-1]),
+                      "iou_init": iou0, "iou_final": iou1}}
+    print(json.dumps(out), flush=True)
+
+
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -445,7 +482,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     try:
-        run_ours(args, rank, world, local)
+        if args.workload == "fit300":
+            run_fit300(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
     finally:
         if world > 1:
             dist.destroy_process_group()

@@ -34,6 +34,8 @@ int launch_image_loss(const float2* z, int64_t n, int kind, const float* target,
 int launch_image_loss_cells(const CellDesc* cells, int ncells, int64_t max_len, const float2* z,
                             int kind, const float* target, float contrast, float* image,
                             float* loss, float2* grad_z, void* ws, cudaStream_t st);
+int launch_voxelize(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                    const dm_box& box, uint8_t* occ, int* err, cudaStream_t st);
 int launch_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
                 float b2, float eps, int64_t* step, cudaStream_t st);
 

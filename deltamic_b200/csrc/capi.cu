@@ -562,6 +562,14 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
 }
 
 // ---------------------------------------------------------------------------
+int dm_voxelize(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                const dm_box* box, uint8_t* occupancy, int* status, dm_stream_t stream) {
+  if (!box_ok(box) || !occupancy || nv < 0 || nt < 0 || (nt > 0 && (!verts || !faces)))
+    return DM_ERR_INVALID_ARG;
+  return launch_voxelize(verts, nv, faces, nt, *box, occupancy, status, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
 int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
                  float lr, float beta1, float beta2, float eps, int64_t* step,
                  dm_stream_t stream) {

@@ -12,7 +12,7 @@ from . import _native as N
 from . import ops
 from .pipeline import MeshRenderer
 
-__all__ = ["FitStep", "fit_mesh"]
+__all__ = ["FitStep", "fit_mesh", "run_fit", "mesh_iou"]
 
 
 class FitStep:
@@ -103,3 +103,37 @@ def fit_mesh(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr
         step()
         losses[k] = step.loss[0]
     return V, losses[::record_every].cpu()
+
+
+def run_fit(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr=1e-3,
+            kind="mse", contrast=0.0, stop_at=None, graph=True):
+    """Adam fit with per-step losses and device timing.
+
+    Returns ``dict(verts, losses[steps_run], ms_total, steps_run, reached)``; with
+    ``stop_at`` the fit stops at the first step whose loss is <= stop_at (checked
+    on the host every step, so the timing includes one small read per step).
+    """
+    V = verts0.detach().clone().contiguous()
+    step = FitStep(renderer, V, faces, coeff, target, kind, contrast, lr, graph=graph)
+    losses = torch.zeros(steps, device=V.device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    k, reached = 0, False
+    for k in range(steps):
+        step()
+        losses[k] = step.loss[0]
+        if stop_at is not None and float(step.loss[0]) <= stop_at:
+            reached = True
+            break
+    e1.record()
+    torch.cuda.synchronize()
+    n = k + 1
+    return dict(verts=V, losses=losses[:n].cpu(), ms_total=e0.elapsed_time(e1), steps_run=n,
+                reached=reached)
+
+
+def mesh_iou(verts_a, verts_b, faces, grid) -> float:
+    """Volumetric IoU of two meshes with the same faces on ``grid``."""
+    return ops.iou(ops.voxelize(verts_a.contiguous(), faces, grid),
+                   ops.voxelize(verts_b.contiguous(), faces, grid))

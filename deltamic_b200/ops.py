@@ -246,3 +246,27 @@ def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, beta1=0.9, beta2=0.999
     N.check(lib.dm_adam_step(N.ptr(param), N.ptr(grad), N.ptr(exp_avg), N.ptr(exp_avg_sq),
                              param.numel(), float(lr), float(beta1), float(beta2), float(eps),
                              N.ptr(step), N.stream_ptr(param.device)), "dm_adam_step")
+
+
+# ---------------------------------------------------------------------------
+# occupancy and volumetric IoU (evaluation of fits)
+
+def voxelize(verts, faces, grid: FreqGrid) -> torch.Tensor:
+    """uint8 occupancy of the closed mesh at the image sample positions of ``grid``."""
+    N.require_cuda(verts, "verts", torch.float32)
+    N.require_cuda(faces, "faces", torch.int64)
+    lib = N.lib()
+    occ = torch.empty(grid.shape, dtype=torch.uint8, device=verts.device)
+    st = torch.zeros(1, dtype=torch.int32, device=verts.device)
+    N.check(lib.dm_voxelize(N.ptr(verts), verts.shape[0], N.ptr(faces), faces.shape[0],
+                            ctypes.byref(grid.cbox), N.ptr(occ), N.ptr(st),
+                            N.stream_ptr(verts.device)), "dm_voxelize")
+    return occ
+
+
+def iou(a: torch.Tensor, b: torch.Tensor) -> float:
+    """Intersection over union of two occupancy grids."""
+    a, b = a.bool(), b.bool()
+    inter = torch.logical_and(a, b).sum()
+    union = torch.logical_or(a, b).sum()
+    return float(inter) / max(float(union), 1.0)

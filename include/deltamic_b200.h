@@ -211,6 +211,16 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
                   dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Occupancy of a closed mesh (for the volumetric IoU of a fit; no counterpart in
+ * the reference, whose label tooling uses a KD-tree on the host,
+ * mask_creation.py:210-224).  occupancy[n0,n1,n2] (uint8 0/1) at the image sample
+ * positions lo + (i,j,k) L/n, by ray parity along the third axis.  ``status``
+ * (DEVICE int, may be NULL) receives DM_ERR_BAD_INDEX for face indices outside
+ * [0, nv) and DM_ERR_SIZE for a column with more than 64 crossings. */
+int dm_voxelize(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                const dm_box* box, uint8_t* occupancy, int* status, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Adam step (torch.optim.Adam semantics, no weight decay) on a float32 array;
  * ``step`` is a DEVICE int64 counter that the call increments (1-based after). */
 int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
