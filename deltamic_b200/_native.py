@@ -87,6 +87,10 @@ SIGNATURES = {
                                           ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),
     "dm_image_loss_workspace_size": (_SZ, [_I64]),
     "dm_image_loss": (_INT, [_P, _I64, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
+    "dm_conv3d_s2_workspace_size": (_SZ, [_INT] * 6),
+    "dm_conv3d_s2_forward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _P, _INT, _P, _P, _P]),
+    "dm_conv3d_s2_backward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P, _P, _P,
+                                     _P, _P, _SZ, _P]),
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
     "dm_launch_count": (ctypes.c_longlong, []),

@@ -211,6 +211,24 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
                   dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * 3x3x3 stride-2 padding-1 3D convolution with bias and GELU, for the learned
+ * initialiser's encoder (no counterpart in the reference).  Channels-last BF16
+ * tensors (uint16 storage): x[B,D,H,W,Ci], w[Kp,Co] with row k = ((kd*3+kh)*3+kw)*Ci
+ * + ci and Kp = 27*Ci rounded up to 32 (padding rows zero); Co in {16,32,64,128},
+ * Ci <= 128; output (D+1)/2 x (H+1)/2 x (W+1)/2.  Tensor-core products with FP32
+ * accumulation.  Forward writes pre[.., Co] (FP32 pre-activation) and act = GELU(pre)
+ * (BF16).  Backward takes dact = dL/dact (FP32) and writes dw[Kp,Co], db[Co] and,
+ * if dx != NULL, dx = dL/dx (FP32); deterministic (no atomics). */
+size_t dm_conv3d_s2_workspace_size(int B, int D, int H, int W, int Ci, int Co);
+int dm_conv3d_s2_forward(const uint16_t* x, int B, int D, int H, int W, int Ci, const uint16_t* w,
+                         const float* bias, int Co, float* pre, uint16_t* act,
+                         dm_stream_t stream);
+int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,
+                          const uint16_t* w, int Co, const float* pre, const float* dact,
+                          float* dx, float* dw, float* db, void* workspace, size_t ws_bytes,
+                          dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Occupancy of a closed mesh (for the volumetric IoU of a fit; no counterpart in
  * the reference, whose label tooling uses a KD-tree on the host,
  * mask_creation.py:210-224).  occupancy[n0,n1,n2] (uint8 0/1) at the image sample
