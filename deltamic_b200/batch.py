@@ -214,6 +214,7 @@ class BatchFitStep:
         self.v = torch.zeros_like(verts)
         self.t = torch.zeros(1, dtype=torch.int64, device=verts.device)
         self.loss = torch.zeros(1, dtype=torch.float32, device=verts.device)
+        self.cell_losses = torch.zeros(r.ncells, dtype=torch.float32, device=verts.device)
         self.graph = None
         self.launches_per_step = None
         if graph:
@@ -224,6 +225,7 @@ class BatchFitStep:
         ft = r.forward_spectrum(self.V, self.C)
         r.inverse_fft()
         losses, _, gz = r.image_loss(self.kind, self.target, self.contrast)
+        self.cell_losses.copy_(losses)
         torch.sum(losses, dim=0, keepdim=True, out=self.loss)
         r.adjoint_fft(gz)
         gv, _ = r.backward(self.V, self.C, ft, want_coeff=False)

@@ -134,7 +134,11 @@ class ShapeSampler:
 
 def render_batch(verts, sig, faces, rng_seed, device, thresh=1e-5, photons=200.0,
                  read_noise=2.0):
-    """Noisy normalised 64^3 images of ``verts[n, nv, 3]`` (one BatchRenderer launch set)."""
+    """Noisy 64^3 images of ``verts[n, nv, 3]`` (one BatchRenderer launch set).
+
+    Returns ``(inputs, targets)``: the min/max-normalised noisy images (network
+    input) and the noisy images divided by the ``photons`` exposure (fit target,
+    unbiased against the min/max-normalised render)."""
     n = len(verts)
     br = BatchRenderer([BOX] * n, [(IMAGE,) * 3] * n, thresh, device)
     br.set_sigmas([np.diag(s) for s in sig])
@@ -149,13 +153,14 @@ def render_batch(verts, sig, faces, rng_seed, device, thresh=1e-5, photons=200.0
         img.shape, device=device, generator=gen)
     lo = noisy.amin(dim=(1, 2, 3), keepdim=True)
     hi = noisy.amax(dim=(1, 2, 3), keepdim=True)
-    return (noisy - lo) / (hi - lo)
+    return (noisy - lo) / (hi - lo), noisy / photons
 
 
 def train_learned_init(n_train, epochs, batch=64, lr=1e-3, seed=0, device="cuda",
                        model=None, log=None):
-    """Render ``n_train`` pairs with the package's renderer, then train with Adam on
-    the vertex-position MSE.  Returns (model, sampler, per-epoch losses)."""
+    """Render ``n_train`` pairs with the package's renderer, then train with Adam
+    (cosine-decayed learning rate) on the vertex-position MSE.  Returns (model,
+    sampler, per-epoch losses)."""
     rng = np.random.default_rng(seed)
     sampler = ShapeSampler()
     imgs, disps = [], []
@@ -163,13 +168,16 @@ def train_learned_init(n_train, epochs, batch=64, lr=1e-3, seed=0, device="cuda"
     for s in range(0, n_train, batch):
         k = min(batch, n_train - s)
         v, sig = sampler.sample(k, rng)
-        imgs.append(render_batch(v, sig, sampler.faces, rng.integers(1 << 30), device)
+        imgs.append(render_batch(v, sig, sampler.faces, rng.integers(1 << 30), device)[0]
                     .to(torch.bfloat16))
         disps.append(torch.tensor(v, dtype=torch.float32, device=device) - tmpl)
     imgs = torch.cat(imgs)
     disps = torch.cat(disps)
     model = (model or LearnedInit(len(sampler.template), seed=seed)).to(device)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
+    iters = epochs * ((n_train + batch - 1) // batch)
+    sched = torch.optim.lr_scheduler.LambdaLR(
+        opt, lambda it: 0.5 * (1.0 + math.cos(math.pi * min(it, iters) / max(iters, 1))))
     g = torch.Generator(device=device).manual_seed(seed)
     hist = []
     for ep in range(epochs):
@@ -182,8 +190,99 @@ def train_learned_init(n_train, epochs, batch=64, lr=1e-3, seed=0, device="cuda"
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
+            sched.step()
             tot += loss.detach() * len(idx)
         hist.append(float(tot) / n_train)
         if log:
             log(f"epoch {ep}: vertex MSE {hist[-1]:.3e}")
     return model, sampler, hist
+
+
+def evaluate_learned_init(model, sampler, n_eval=256, steps=300, lr=1e-3, seed=12345,
+                          device="cuda", chunk=64, tol=0.01):
+    """Held-out comparison of learned-init + GD against sphere-init GD.
+
+    For every shape both fits run ``steps`` Adam steps on the image L2 (cells of a
+    chunk are fitted together, each with its own loss).  The plain fit's final
+    loss L_p is the target; the learned fit's time to reach (1 + tol) L_p counts
+    the network inference plus its steps.  Returns per-shape arrays and timings.
+    """
+    from .batch import BatchFitStep
+    from .ops import FreqGrid, iou, voxelize
+    rng = np.random.default_rng(seed)
+    tmpl = torch.tensor(sampler.template, dtype=torch.float32, device=device)
+    faces_t = torch.tensor(sampler.faces, device=device)
+    grid = FreqGrid(BOX, (IMAGE,) * 3)
+    out = {k: [] for k in ("plain_final", "learned_first", "learned_steps", "reached",
+                           "iou_plain", "iou_learned", "iou_learned_init", "iou_sphere",
+                           "iou_learned_at_target")}
+    t_step = t_infer = 0.0
+    n_steps_timed = n_infer = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for s0 in range(0, n_eval, chunk):
+        k = min(chunk, n_eval - s0)
+        v, sig = sampler.sample(k, rng)
+        net_in, target = render_batch(v, sig, sampler.faces, rng.integers(1 << 30), device)
+        br = BatchRenderer([BOX] * k, [(IMAGE,) * 3] * k, 1e-5, device)
+        br.set_sigmas([np.diag(x) for x in sig])
+        br.set_meshes([sampler.template] * k, [sampler.faces] * k)
+        C = torch.ones(k * len(sampler.faces), device=device)
+        tgt = target.reshape(-1).contiguous()
+        # learned initial meshes (inference timed)
+        torch.cuda.synchronize()
+        e0.record()
+        with torch.no_grad():
+            init_l = (model(net_in) + tmpl).reshape(-1, 3).contiguous()
+        e1.record()
+        torch.cuda.synchronize()
+        t_infer += e0.elapsed_time(e1)
+        n_infer += k
+        curves = {}
+        snaps = {}
+        for name, V0 in (("plain", tmpl.repeat(k, 1)), ("learned", init_l)):
+            st = BatchFitStep(br, V0.clone(), C, tgt, "mse", 0.0, lr, graph=True)
+            losses = torch.zeros(steps, k, device=device)
+            hist = [] if name == "learned" else None
+            torch.cuda.synchronize()
+            e0.record()
+            for i in range(steps):
+                st()
+                losses[i] = st.cell_losses
+                if hist is not None and i % 10 == 9:
+                    hist.append(st.V.detach().clone())
+            e1.record()
+            torch.cuda.synchronize()
+            t_step += e0.elapsed_time(e1)
+            n_steps_timed += steps * k
+            curves[name] = (losses.cpu().numpy(), st.V.view(k, -1, 3))
+            snaps[name] = hist
+        lp, Vp = curves["plain"]
+        ll, Vl = curves["learned"]
+        target_l2 = lp[-1] * (1 + tol)
+        gt = torch.tensor(v, dtype=torch.float32, device=device)
+        V0l = init_l.view(k, -1, 3)
+        for c in range(k):
+            hit = np.flatnonzero(ll[:, c] <= target_l2[c])
+            out["plain_final"].append(float(lp[-1, c]))
+            out["learned_first"].append(float(ll[0, c]))
+            n_hit = int(hit[0]) + 1 if len(hit) else steps
+            out["learned_steps"].append(n_hit)
+            out["reached"].append(bool(len(hit)))
+            occ_gt = voxelize(gt[c].contiguous(), faces_t, grid)
+            occ = lambda VV: iou(voxelize(VV.contiguous(), faces_t, grid), occ_gt)
+            out["iou_plain"].append(occ(Vp[c]))
+            out["iou_learned"].append(occ(Vl[c]))
+            out["iou_learned_init"].append(occ(V0l[c]))
+            out["iou_sphere"].append(occ(tmpl))
+            # mesh at the reach step, from the snapshots taken every 10 steps
+            j = min(max((n_hit + 9) // 10 - 1, 0), len(snaps["learned"]) - 1)
+            Vs = snaps["learned"][j].view(k, -1, 3)[c] if n_hit > 1 else V0l[c]
+            out["iou_learned_at_target"].append(occ(Vs))
+    res = {k: np.array(v) for k, v in out.items() if v}
+    ms_step = t_step / n_steps_timed      # per shape per step
+    ms_infer = t_infer / n_infer          # per shape
+    t_plain = steps * ms_step
+    t_learned = res["learned_steps"] * ms_step + ms_infer
+    res.update(ms_step_per_shape=ms_step, ms_infer_per_shape=ms_infer,
+               time_ratio=t_learned / t_plain, steps=steps)
+    return res

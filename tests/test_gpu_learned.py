@@ -85,7 +85,7 @@ def test_trained_network_beats_sphere_initialisation():
     assert hist[-1] < 0.5 * hist[0]
     rng = np.random.default_rng(999)
     v, sig = sampler.sample(32, rng)
-    img = render_batch(v, sig, sampler.faces, 7, DEV)
+    img, _ = render_batch(v, sig, sampler.faces, 7, DEV)
     with torch.no_grad():
         pred = model(img) + torch.tensor(sampler.template, dtype=torch.float32, device=DEV)
     gt = torch.tensor(v, dtype=torch.float32, device=DEV)
