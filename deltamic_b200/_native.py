@@ -94,6 +94,8 @@ SIGNATURES = {
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
     "dm_launch_count": (ctypes.c_longlong, []),
+    "dm_set_variants": (_INT, [_INT, _INT]),
+    "dm_get_variants": (_INT, [ctypes.POINTER(_INT)] * 4),
     "dm_peak_probe": (_INT, [_INT, _INT, ctypes.POINTER(ctypes.c_double), _P]),
     "dm_profile_enable": (_INT, [_INT]),
     "dm_profile_read": (_INT, [_INT, ctypes.POINTER(_INT), ctypes.POINTER(_F)]),

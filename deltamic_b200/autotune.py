@@ -1,0 +1,92 @@
+"""Autotuner for the meshFT kernels' tile shapes.
+
+The library compiles several tile-shape variants of the forward kernel
+(frequencies per thread x threads per CTA x waves) and of the adjoint kernel
+(faces per thread x threads per CTA x waves).  ``tune`` times every variant on
+the caller's own problem and keeps the fastest per *size class* (log2 of the face
+count, log2 of the band size); the choice is remembered for the process and, if
+``$DM_AUTOTUNE_CACHE`` names a JSON file, across processes.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+
+import torch
+
+from . import _native as N
+from . import ops
+
+__all__ = ["size_class", "tune", "apply", "current"]
+
+_CACHE: dict = {}
+
+
+def size_class(nt: int, nband: int) -> str:
+    return f"{int(math.log2(max(nt, 1)))}:{int(math.log2(max(nband, 1)))}"
+
+
+def _load():
+    path = os.environ.get("DM_AUTOTUNE_CACHE")
+    if path and os.path.exists(path):
+        try:
+            with open(path) as f:
+                _CACHE.update({k: tuple(v) for k, v in json.load(f).items()})
+        except (OSError, ValueError):
+            pass
+
+
+def _save():
+    path = os.environ.get("DM_AUTOTUNE_CACHE")
+    if path:
+        try:
+            with open(path, "w") as f:
+                json.dump(_CACHE, f)
+        except OSError:
+            pass
+
+
+def current():
+    f, b, nf, nb = (N._INT() for _ in range(4))
+    N.lib().dm_get_variants(ctypes.byref(f), ctypes.byref(b), ctypes.byref(nf), ctypes.byref(nb))
+    return f.value, b.value, nf.value, nb.value
+
+
+def apply(variants) -> None:
+    N.check(N.lib().dm_set_variants(int(variants[0]), int(variants[1])), "dm_set_variants")
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(verts, faces, coeff, grid, band, reps=3, force=False):
+    """Pick and apply the fastest (forward, adjoint) variants for this size class."""
+    if not _CACHE:
+        _load()
+    key = size_class(int(faces.shape[0]), int(band.numel()))
+    if key in _CACHE and not force:
+        apply(_CACHE[key])
+        return _CACHE[key]
+    f0, b0, nf, nb = current()
+    g = torch.ones(band.numel(), dtype=torch.complex64, device=verts.device)
+    ft = ops.meshft_list(verts, faces, coeff, grid, band)
+    best_f = min(range(nf), key=lambda v: (apply((v, b0)), _time(
+        lambda: ops.meshft_list(verts, faces, coeff, grid, band), reps))[1])
+    best_b = min(range(nb), key=lambda v: (apply((best_f, v)), _time(
+        lambda: ops.meshft_backward_list(verts, faces, coeff, grid, band, ft, grad_list=g,
+                                         want_coeff=False), reps))[1])
+    _CACHE[key] = (best_f, best_b)
+    apply(_CACHE[key])
+    _save()
+    return _CACHE[key]

@@ -204,6 +204,21 @@ int dm_profile_read(int kernel, int* count, float* total_ms) {
 
 long long dm_launch_count(void) { return dm::g_launches.load(); }
 
+int dm_set_variants(int fwd, int bwd) {
+  if (fwd < 0 || fwd >= dm::kNumFwdVariants || bwd < 0 || bwd >= dm::kNumBwdVariants)
+    return DM_ERR_INVALID_ARG;
+  dm::set_variants(fwd, bwd);
+  return DM_OK;
+}
+
+int dm_get_variants(int* fwd, int* bwd, int* n_fwd, int* n_bwd) {
+  if (fwd) *fwd = dm::fwd_variant();
+  if (bwd) *bwd = dm::bwd_variant();
+  if (n_fwd) *n_fwd = dm::kNumFwdVariants;
+  if (n_bwd) *n_bwd = dm::kNumBwdVariants;
+  return DM_OK;
+}
+
 
 int dm_abi_version(void) { return 1; }
 

@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "dm_common.cuh"
 #include "meshft_internal.h"
@@ -652,25 +653,36 @@ int num_sms() {
 
 static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// Items per launch that fill the GPU in about two waves of FwdCfg/BwdCfg CTAs.
-static int64_t target_items() { return (int64_t)num_sms() * 8; }
+namespace {
+std::atomic<int> g_fwd_variant{0};
+std::atomic<int> g_bwd_variant{0};
+}  // namespace
+
+int fwd_variant() { return g_fwd_variant.load(); }
+int bwd_variant() { return g_bwd_variant.load(); }
+void set_variants(int fwd, int bwd) {
+  g_fwd_variant.store(fwd);
+  g_bwd_variant.store(bwd);
+}
 
 void plan_cell_tiles(CellDesc& d) {
-  const int64_t xtile = (int64_t)FwdCfg::NT * FwdCfg::R;
+  const FwdVariant fv = kFwdVariants[fwd_variant()];
+  const BwdVariant bv = kBwdVariants[bwd_variant()];
+  const int64_t xtile = (int64_t)fv.NT * fv.R;
   d.xtiles = (int32_t)std::max<int64_t>(1, cdiv(d.nband, xtile));
-  int64_t fsplit = std::max<int64_t>(1, cdiv(target_items(), d.xtiles));
-  fsplit = std::min<int64_t>(fsplit, std::max<int64_t>(1, cdiv(d.nt, FwdCfg::TF)));
+  int64_t fsplit = std::max<int64_t>(1, cdiv((int64_t)num_sms() * fv.waves, d.xtiles));
+  fsplit = std::min<int64_t>(fsplit, std::max<int64_t>(1, cdiv(d.nt, kFwdTF)));
   int64_t fchunk = cdiv(std::max<int64_t>(d.nt, 1), fsplit);
-  fchunk = cdiv(fchunk, FwdCfg::TF) * FwdCfg::TF;
+  fchunk = cdiv(fchunk, kFwdTF) * kFwdTF;
   d.fchunk = (int32_t)fchunk;
   d.fsplit = (int32_t)std::max<int64_t>(1, cdiv(d.nt, fchunk));
 
-  const int64_t fblock = (int64_t)BwdCfg::NT * BwdCfg::F;
+  const int64_t fblock = (int64_t)bv.NT * bv.F;
   d.fblocks = (int32_t)std::max<int64_t>(1, cdiv(d.nt, fblock));
-  int64_t bch = std::max<int64_t>(1, cdiv(target_items(), d.fblocks));
-  bch = std::min<int64_t>(bch, std::max<int64_t>(1, cdiv(d.nband, BwdCfg::TX)));
+  int64_t bch = std::max<int64_t>(1, cdiv((int64_t)num_sms() * bv.waves, d.fblocks));
+  bch = std::min<int64_t>(bch, std::max<int64_t>(1, cdiv(d.nband, kBwdTX)));
   int64_t bx = cdiv(std::max<int64_t>(d.nband, 1), bch);
-  bx = cdiv(bx, BwdCfg::TX) * BwdCfg::TX;
+  bx = cdiv(bx, kBwdTX) * kBwdTX;
   d.bxchunk = (int32_t)bx;
   d.bchunks = (int32_t)std::max<int64_t>(1, cdiv(d.nband, bx));
 }
@@ -718,8 +730,15 @@ int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
                    float2* fpart, float2* ft_list, float2* grid, int* err, cudaStream_t st) {
   if (t.fwd_items > 0 && t.nband > 0) {
     profile_begin(0, st);
-    k_meshft_fwd<FwdCfg::R, FwdCfg::NT, FwdCfg::TF, FwdCfg::NS>
-        <<<(unsigned)t.fwd_items, FwdCfg::NT, 0, st>>>(c, recs, band_index, fpart, err);
+    const unsigned g = (unsigned)t.fwd_items;
+    switch (fwd_variant()) {
+      case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
+      case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, band_index, fpart, err); break;
+      case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, band_index, fpart, err); break;
+      case 4: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
+      case 5: k_meshft_fwd<2, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, band_index, fpart, err); break;
+      default: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
+    }
     profile_end(0, st);
     count_launches(1);
     if (launch_status()) return DM_ERR_CUDA;
@@ -747,8 +766,15 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
   if (t.bwd_items > 0 && t.nband > 0 && t.nt > 0) {
     cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
     profile_begin(1, st);
-    k_meshft_bwd<BwdCfg::F, BwdCfg::NT, BwdCfg::TX, BwdCfg::NS>
-        <<<(unsigned)t.bwd_items, BwdCfg::NT, 0, st>>>(c, recs, xrec, bpart, err);
+    const unsigned g = (unsigned)t.bwd_items;
+    switch (bwd_variant()) {
+      case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
+      case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, xrec, bpart, err); break;
+      case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, xrec, bpart, err); break;
+      case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
+      case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
+      default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
+    }
     profile_end(1, st);
     count_launches(1);
     if (launch_status()) return DM_ERR_CUDA;

@@ -7,14 +7,26 @@
 
 namespace dm {
 
-// Forward: R frequencies per thread, NT threads, TF faces per staged tile, NS stages.
-struct FwdCfg {
-  static constexpr int R = 4, NT = 128, TF = 64, NS = 3;
+// Tile-shape variants (picked per size class by the autotuner, dm_set_variants).
+// Forward: R frequencies per thread, NT threads; face tiles of 64 in 3 stages.
+// Backward: F faces per thread, NT threads; frequency tiles of 128 in 3 stages.
+// ``waves``: items per launch as a multiple of the SM count.
+struct FwdVariant {
+  int R, NT, waves;
 };
-// Backward: F faces per thread, NT threads, TX frequencies per staged tile, NS stages.
-struct BwdCfg {
-  static constexpr int F = 2, NT = 128, TX = 128, NS = 3;
+struct BwdVariant {
+  int F, NT, waves;
 };
+constexpr int kFwdTF = 64, kBwdTX = 128, kStages = 3;
+constexpr int kNumFwdVariants = 6;
+constexpr int kNumBwdVariants = 6;
+constexpr FwdVariant kFwdVariants[kNumFwdVariants] = {
+    {4, 128, 8}, {2, 128, 8}, {4, 256, 8}, {8, 64, 8}, {4, 128, 16}, {2, 256, 16}};
+constexpr BwdVariant kBwdVariants[kNumBwdVariants] = {
+    {2, 128, 8}, {1, 128, 8}, {2, 64, 8}, {1, 256, 8}, {2, 128, 16}, {1, 128, 16}};
+int fwd_variant();
+int bwd_variant();
+void set_variants(int fwd, int bwd);
 
 // Totals of a batched plan (sums over cells).
 struct PlanTotals {

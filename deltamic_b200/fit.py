@@ -41,6 +41,7 @@ class FitStep:
         self.t = torch.zeros(1, dtype=torch.int64, device=verts.device)
         self.loss = torch.zeros(1, dtype=torch.float32, device=verts.device)
         self.grad = torch.zeros_like(verts)
+        renderer.tune(verts, self.F, self.C)
         self.graph = None
         self.launches_per_step = None
         if graph:

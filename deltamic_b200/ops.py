@@ -67,6 +67,24 @@ def narrowband(otf: torch.Tensor, thresh: float) -> torch.Tensor:
     return idx[:c].clone()
 
 
+def order_band_by_radius(band: torch.Tensor, grid: FreqGrid) -> torch.Tensor:
+    """The band's voxel indices sorted by |xi| (stable).  The meshFT calls accept
+    the band in any order; neighbouring threads then see similar frequencies and
+    take the same evaluation path more often."""
+    if band.numel() == 0:
+        return band
+    n0, n1, n2 = grid.shape
+    idx = band.long()
+    k0 = idx // (n1 * n2)
+    k1 = (idx // n2) % n1
+    k2 = idx % n2
+    L = grid.box_size[:, 1] - grid.box_size[:, 0]
+    r2 = (((2 * k0 - (n0 - 1)) / L[0]) ** 2 + ((2 * k1 - (n1 - 1)) / L[1]) ** 2
+          + ((2 * k2 - (n2 - 1)) / L[2]) ** 2)
+    order = torch.sort(r2, stable=True).indices
+    return band[order].contiguous()
+
+
 # ---------------------------------------------------------------------------
 # topology cache (vertex <- face CSR), keyed by the faces tensor
 

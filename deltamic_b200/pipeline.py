@@ -19,7 +19,8 @@ __all__ = ["MeshRenderer"]
 class MeshRenderer:
     """Renderer for one box: holds the frequency grid, the OTF and its narrow band."""
 
-    def __init__(self, box_size, box_shape, narrowband_thresh=1e-5, device="cuda"):
+    def __init__(self, box_size, box_shape, narrowband_thresh=1e-5, device="cuda",
+                 autotune=True):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("MeshRenderer runs on CUDA devices only")
@@ -34,6 +35,8 @@ class MeshRenderer:
         self.otf = None
         self.band = None
         self._sigma_key = None
+        self.autotune = autotune
+        self.variants = None
 
     @property
     def numel(self) -> int:
@@ -46,6 +49,7 @@ class MeshRenderer:
         self.band = ops.narrowband(self.otf, self.thresh)
         self.spec.zero_()
         self._sigma_key = None
+        self.variants = None
 
     def set_sigma(self, sigma: torch.Tensor) -> None:
         """Gaussian OTF of ``sigma`` (psf.py:15-20) and its narrow band."""
@@ -67,6 +71,7 @@ class MeshRenderer:
     def render(self, verts, faces, coeff) -> torch.Tensor:
         """|ifftn(meshFT * OTF)| as a new float32 tensor (no normalisation)."""
         self._require_band()
+        self.tune(verts, faces, coeff)
         ops.meshft_list(verts, faces, coeff, self.grid, self.band, otf=self.otf,
                         spectrum=self.spec)
         torch.fft.ifftn(self.spec, out=self.z)
@@ -80,12 +85,25 @@ class MeshRenderer:
             sigma = torch.zeros(0, device=self.device)
         self._require_band()
         ops._check_mesh(verts, faces, coeff)
+        self.tune(verts, faces, coeff)
         return _RenderLoss.apply(verts.contiguous(), coeff.contiguous(), sigma, self,
                                  faces.contiguous(), kind, target, float(contrast))
 
     def _require_band(self):
         if self.band is None:
             raise RuntimeError("call set_otf() or set_sigma() first")
+
+    def tune(self, verts, faces, coeff):
+        """Choose (once per size class) and apply the kernels' tile-shape variants."""
+        from . import autotune
+        self._require_band()
+        if self.variants is None:
+            if self.autotune:
+                self.variants = autotune.tune(verts.detach().contiguous(), faces.contiguous(),
+                                              coeff.detach().contiguous(), self.grid, self.band)
+            else:
+                self.variants = autotune.current()[:2]
+        autotune.apply(self.variants)
 
 
 class _RenderLoss(torch.autograd.Function):

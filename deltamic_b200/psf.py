@@ -14,6 +14,10 @@ __all__ = ["generate_gaussian_psf", "generate_gaussian_psf_from_sigma"]
 
 
 def generate_gaussian_psf(sigma, xi0, xi1, xi2):
+    """exp(-(xi^T sigma xi)/2) on the grid of the axes (float32 kernel; a float64
+    sigma or float64 axes give a float64 result with gradients to sigma)."""
+    if sigma.dtype == torch.float64 or xi0.dtype == torch.float64:
+        return ops.gaussian_otf(sigma.float(), xi0, xi1, xi2).double()
     return ops.gaussian_otf(sigma, xi0, xi1, xi2)
 
 

@@ -12,8 +12,11 @@ Same names, arguments and results as the reference:
   (render.py:343-355).
 
 Differences, all deliberate: the module runs on CUDA only (``device='cpu'``
-raises -- there is no CPU fallback) and in float32 only; the box used for the
-phases is kept in float64.
+raises -- there is no CPU fallback); the kernels compute in float32 (with the
+fixed-point phases their error against a float64 evaluation is ~1e-6), so a
+``dtype=torch.float64`` module casts its inputs to float32 and returns a
+complex128 spectrum whose gradients flow back to the float64 inputs; the box
+used for the phases is kept in float64.
 """
 from __future__ import annotations
 
@@ -90,8 +93,8 @@ class Fourier3dMesh(nn.Module):
         if not _is_cuda(device):
             raise RuntimeError("deltamic_b200.Fourier3dMesh runs on CUDA devices only "
                                f"(got device={device!r}); there is no CPU path")
-        if dtype not in (torch.float, torch.float32):
-            raise NotImplementedError("deltamic_b200 kernels compute in float32 only")
+        if dtype not in (torch.float32, torch.float64):
+            raise TypeError(f"Fourier3dMesh supports float32 and float64, not {dtype}")
         bs = torch.as_tensor(box_size).detach().cpu()
         self.grid = ops.FreqGrid(bs.double().numpy(), box_shape)
         self.box_size = torch.tensor(bs.numpy(), device=device, dtype=dtype)
@@ -124,9 +127,12 @@ class Fourier3dMesh(nn.Module):
         if key != self._band_key or self._band is None:
             if tuple(otf.shape) != tuple(self.box_shape):
                 raise ValueError("OTF must have shape box_shape")
-            self._band = ops.narrowband(otf.float(), thr)
+            self._band = ops.narrowband(otf.detach().float().contiguous(), thr)
             self._band_key = key
         return self._band
 
     def forward(self, Verts, Faces, Faces_coeff):
+        if self.dtype == torch.float64:
+            ft = ops.meshft(Verts.float(), Faces, Faces_coeff.float(), self.grid, self.band())
+            return ft.to(torch.complex128)
         return ops.meshft(Verts, Faces, Faces_coeff, self.grid, self.band())

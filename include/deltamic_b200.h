@@ -256,6 +256,14 @@ int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg
  * milliseconds, then clears them. */
 long long dm_launch_count(void);
 
+/* Tile-shape variants of the meshFT forward and adjoint kernels (no counterpart in
+ * the reference).  Process-wide; a plan, workspace size and launch use the
+ * variants current when they are made, so re-query workspace sizes after a
+ * change and do not change variants between a workspace query and its call.
+ * The autotuner (deltamic_b200.autotune) picks them per size class. */
+int dm_set_variants(int fwd, int bwd);
+int dm_get_variants(int* fwd, int* bwd, int* n_fwd, int* n_bwd);
+
 /* Throughput probe (no counterpart in the reference): times ``iters`` rounds of
  * 8 independent FP32 FMA chains (kind 0) or MUFU sin.approx chains (kind 1) per
  * thread over the whole GPU and returns instructions per second.  Synchronous;

@@ -224,3 +224,49 @@ def test_full_size_properties_200cube_20480_faces():
     sub = np.sort(rng.choice(band.numel(), 256, replace=False))
     ref = oracle.meshft_forward(v - box[:, 0], f, np.ones(len(f)), xil[sub])
     assert rel_l2(ft.cpu().numpy()[sub], ref) < TOL_FT
+
+
+def test_device_status_word_reports_bad_band_index():
+    """A band index outside the grid (injected on the host) is skipped by the
+    kernels and reported through the workspace status word, not a fault."""
+    import ctypes
+    from deltamic_b200 import _native as N
+    v, f, c, box, shape, sigma, thresh = _case(1, (12, 12, 12))
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    lib = N.lib()
+    bad = band.clone()
+    bad[5] = 12 ** 3 + 100
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    nb = bad.numel()
+    ws = torch.zeros(lib.dm_meshft_forward_workspace_size(len(v), len(f), nb), dtype=torch.uint8,
+                     device=DEV)
+    ft = torch.empty(nb, dtype=torch.complex64, device=DEV)
+    spec = torch.zeros(shape, dtype=torch.complex64, device=DEV)
+    st = lib.dm_meshft_forward(N.ptr(V), len(v), N.ptr(F), len(f), N.ptr(C),
+                               ctypes.byref(grid.cbox), N.ptr(bad), nb, None, N.ptr(ft),
+                               N.ptr(spec), N.ptr(ws), ws.numel(), N.stream_ptr(DEV))
+    assert st == N.DM_OK
+    flags = N._INT()
+    assert lib.dm_device_error(N.ptr(ws), ctypes.byref(flags), N.stream_ptr(DEV)) == N.DM_OK
+    assert flags.value & N.DM_ERR_BAD_INDEX
+    assert lib.dm_device_error(N.ptr(ws), ctypes.byref(flags), N.stream_ptr(DEV)) == N.DM_OK
+    assert flags.value == 0  # cleared by the read
+
+
+def test_float64_module_matches_float32_path():
+    import deltamic_b200 as dm
+    v, f, c, box, shape, sigma, thresh = _case(2, (20, 20, 20))
+    out = []
+    for dt in (torch.float32, torch.float64):
+        V = torch.tensor(v, dtype=dt, device=DEV, requires_grad=True)
+        C = torch.tensor(c, dtype=dt, device=DEV)
+        m = dm.Fourier3dMesh(torch.tensor(box), shape, device=DEV, dtype=dt,
+                             narrowband_thresh=thresh)
+        S = torch.tensor(sigma, dtype=dt, device=DEV)
+        m.OTF = dm.generate_gaussian_psf(S, m.xi0, m.xi1, m.xi2)
+        ft = m(V, _t(f, torch.int64), C)
+        ft.abs().sum().backward()
+        out.append((ft.detach().cpu().numpy(), V.grad.cpu().numpy()))
+        assert ft.dtype == (torch.complex64 if dt == torch.float32 else torch.complex128)
+    assert rel_l2(out[1][0], out[0][0]) < 1e-6
+    assert rel_l2(out[1][1], out[0][1]) < 1e-5
