@@ -15,6 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libdeltamic_b200.so")
 
 DM_OK = 0
+DM_BAND_HERMITIAN = 1
 DM_ERR_INVALID_ARG = 1
 DM_ERR_BAD_INDEX = 2
 DM_ERR_SIZE = 4
@@ -23,7 +24,7 @@ DM_ERR_CUDA = 16
 DM_ERR_TIMEOUT = 32
 DM_ERR_UNSUPPORTED = 64
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # Entry points and their (restype, argtypes); every symbol of the public header.
 _P = ctypes.c_void_p
@@ -35,7 +36,7 @@ _INT = ctypes.c_int
 
 class DmBox(ctypes.Structure):
     _fields_ = [("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3),
-                ("shape", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32)]
+                ("shape", ctypes.c_int32 * 3), ("band_flags", ctypes.c_int32)]
 
 
 _BOXP = ctypes.POINTER(DmBox)
@@ -63,6 +64,7 @@ SIGNATURES = {
     "dm_device_error": (_INT, [_P, ctypes.POINTER(_INT), _P]),
     "dm_narrowband_workspace_size": (_SZ, [_I64]),
     "dm_narrowband_compact": (_INT, [_P, _I64, _F, _P, _P, _P, _SZ, _P]),
+    "dm_narrowband_hermitian": (_INT, [_P, _I64, _I64, _P, _P]),
     "dm_topology_size": (_SZ, [_I64, _I64]),
     "dm_topology_build": (_INT, [_P, _I64, _I64, _P, _SZ, _P]),
     "dm_meshft_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
@@ -157,7 +159,7 @@ def make_box(box_size, box_shape) -> DmBox:
         b.lo[d] = float(box_size[d][0])
         b.hi[d] = float(box_size[d][1])
         b.shape[d] = int(box_shape[d])
-    b.reserved = 0
+    b.band_flags = 0
     return b
 
 

@@ -78,6 +78,7 @@ class BatchRenderer:
                 self.cell_view(self.otf, i).copy_(o)
                 bands.append(ops.narrowband(o, self.thresh))
         self.band_sizes = [int(b.numel()) for b in bands]
+        self.band_herm = [ops.band_is_hermitian(b) for b in bands]
         self.band = torch.cat(bands).contiguous()
         self.spec.zero_()
         self.batch = None
@@ -99,7 +100,7 @@ class BatchRenderer:
         for i in range(self.ncells):
             cells[i].nv, cells[i].nt, cells[i].n_band = nvs[i], nts[i], self.band_sizes[i]
             cells[i].grid_offset = self.grid_offset[i]
-            cells[i].box = self.grids[i].cbox
+            cells[i].box = ops.band_box(self.grids[i], self.band_herm[i])
         lib = N.lib()
         self._desc = torch.empty(lib.dm_batch_desc_size(self.ncells), dtype=torch.uint8,
                                  device=self.device)
@@ -116,6 +117,9 @@ class BatchRenderer:
         self.faces = faces
         self.nv, self.nt = nvs, nts
         self.pairs = sum(nt * nb for nt, nb in zip(nts, self.band_sizes))
+        # face*xi pairs the kernels evaluate (half of each mirror-symmetric band)
+        self.eval_pairs = sum(nt * ((nb + 1) // 2 if h else nb)
+                              for nt, nb, h in zip(nts, self.band_sizes, self.band_herm))
         self._ws = {k: torch.zeros(max(int(getattr(self.batch, k)), 256), dtype=torch.uint8,
                                    device=self.device)
                     for k in ("fwd_workspace", "bwd_workspace", "image_workspace")}

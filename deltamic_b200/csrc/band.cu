@@ -108,6 +108,23 @@ int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, i
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
+// Mirror test of a band (DM_BAND_HERMITIAN): one block, fixed result.
+__global__ void k_band_mirror(const int32_t* __restrict__ band, int64_t nb, int64_t nvox,
+                              int32_t* __restrict__ flag) {
+  int ok = 1;
+  for (int64_t m = threadIdx.x; m < nb; m += blockDim.x)
+    ok &= (int64_t)band[nb - 1 - m] == nvox - 1 - (int64_t)band[m];
+  ok = __syncthreads_and(ok);
+  if (threadIdx.x == 0) *flag = ok;
+}
+
+int launch_band_mirror(const int32_t* band, int64_t nb, int64_t nvox, int32_t* flag,
+                       cudaStream_t st) {
+  k_band_mirror<<<1, 1024, 0, st>>>(band, nb, nvox, flag);
+  count_launches(1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
 // ---------------------------------------------------------------------------
 // Gaussian OTF exp(-(xi^T S xi)/2) (generate_gaussian_psf, psf.py:15-20) on the
 // outer grid of three frequency axes, with the float32 operation order of the

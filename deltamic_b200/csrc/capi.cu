@@ -33,6 +33,7 @@ struct Carve {
 
 bool box_ok(const dm_box* b) {
   if (!b) return false;
+  if (b->band_flags & ~DM_BAND_HERMITIAN) return false;
   for (int d = 0; d < 3; ++d) {
     if (b->shape[d] <= 0) return false;
     if (!(b->hi[d] > b->lo[d])) return false;
@@ -52,9 +53,28 @@ CellDesc single_cell(const dm_box* b, int64_t nv, int64_t nt, int64_t nband, Pla
   d.nv = (int32_t)nv;
   d.nt = (int32_t)nt;
   d.nband = (int32_t)nband;
+  set_band_half(d, b && (b->band_flags & DM_BAND_HERMITIAN));
   d.grid_off = 0;
   plan_offsets(&d, 1, t);
   return d;
+}
+
+// Totals of the larger of the full-band and half-band plans: the workspace
+// queries see no box, so their sizes cover either.
+void plan_any(int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
+  PlanTotals a, h;
+  dm_box b;
+  memset(&b, 0, sizeof(b));
+  for (int k = 0; k < 3; ++k) {
+    b.hi[k] = 1.0;
+    b.shape[k] = 1;
+  }
+  single_cell(&b, nv, nt, nband, a);
+  b.band_flags = DM_BAND_HERMITIAN;
+  single_cell(&b, nv, nt, nband, h);
+  t = a;
+  t.fpart = std::max(a.fpart, h.fpart);
+  t.bpart = std::max(a.bpart, h.bpart);
 }
 
 Cells one_cell(const CellDesc& d) {
@@ -220,7 +240,7 @@ int dm_get_variants(int* fwd, int* bwd, int* n_fwd, int* n_bwd) {
 }
 
 
-int dm_abi_version(void) { return 1; }
+int dm_abi_version(void) { return 2; }
 
 const char* dm_status_string(int status) {
   if (status == DM_OK) return "ok";
@@ -269,6 +289,14 @@ int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh, int3
                            (cudaStream_t)stream);
 }
 
+int dm_narrowband_hermitian(const int32_t* band_index, int64_t n_band, int64_t n_voxels,
+                            int32_t* is_hermitian, dm_stream_t stream) {
+  if (!is_hermitian || n_band < 0 || n_voxels < 0 || n_band > n_voxels ||
+      (n_band > 0 && !band_index))
+    return DM_ERR_INVALID_ARG;
+  return launch_band_mirror(band_index, n_band, n_voxels, is_hermitian, (cudaStream_t)stream);
+}
+
 // ---------------------------------------------------------------------------
 size_t dm_topology_size(int64_t nv, int64_t nt) {
   if (nv < 0 || nt < 0) return 0;
@@ -291,7 +319,7 @@ int dm_topology_build(const int64_t* faces, int64_t nt, int64_t nv, void* topolo
 size_t dm_meshft_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
   if (!sizes_ok(nv, nt, n_band)) return 0;
   PlanTotals t;
-  single_cell(nullptr, nv, nt, n_band, t);
+  plan_any(nv, nt, n_band, t);
   return fwd_layout(nullptr, t, nullptr);
 }
 
@@ -368,6 +396,7 @@ int dm_batch_plan(const dm_cell* cells, int ncells, void* desc, size_t desc_byte
     d[i].nv = (int32_t)c.nv;
     d[i].nt = (int32_t)c.nt;
     d[i].nband = (int32_t)c.n_band;
+    set_band_half(d[i], (c.box.band_flags & DM_BAND_HERMITIAN) != 0);
     d[i].grid_off = c.grid_offset;
     const int64_t g = (int64_t)c.box.shape[0] * c.box.shape[1] * c.box.shape[2];
     grid_end = std::max(grid_end, c.grid_offset + g);
@@ -477,7 +506,7 @@ int dm_batched_image_loss(const dm_batch* batch, const float* z, int kind, const
 size_t dm_meshft_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
   if (!sizes_ok(nv, nt, n_band)) return 0;
   PlanTotals t;
-  single_cell(nullptr, nv, nt, n_band, t);
+  plan_any(nv, nt, n_band, t);
   return bwd_layout(nullptr, t, nullptr);
 }
 

@@ -35,6 +35,8 @@ struct CellDesc {
   double len[3];      // box extents
   int32_t n[3];       // box_shape
   int32_t nv, nt, nband;
+  int32_t ne;         // frequencies evaluated: band[0, ne) (half the band if herm)
+  int32_t herm;       // band closed under xi -> -xi (DM_BAND_HERMITIAN)
   int64_t v_off;      // first vertex in the concatenated vertex array
   int64_t f_off;      // first face in the concatenated face arrays
   int64_t b_off;      // first band entry in the concatenated band arrays

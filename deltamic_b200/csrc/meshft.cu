@@ -186,11 +186,11 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
   const int split = local / d.xtiles;
   const int f0 = split * d.fchunk;
   const int nf = min(d.nt, f0 + d.fchunk) - f0;
-  if (d.nband <= 0) return;
+  if (d.ne <= 0) return;
   if (nf <= 0) {  // no faces: the partial sums are zero
     for (int r = 0; r < R; ++r) {
       const int m = xt * NT * R + r * NT + threadIdx.x;
-      if (m < d.nband) fpart[d.fpart_off + (int64_t)split * d.nband + m] = make_float2(0.f, 0.f);
+      if (m < d.ne) fpart[d.fpart_off + (int64_t)split * d.ne + m] = make_float2(0.f, 0.f);
     }
     return;
   }
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
     mloc[r] = m;
     // lanes past the band evaluate a real frequency so every lane takes the
     // same branches; their sums are never stored
-    const int mm = min(m, d.nband - 1);
+    const int mm = min(m, d.ne - 1);
     band_to_m(band_index[d.b_off + mm], d, xv[r].mi);
 #pragma unroll
     for (int k = 0; k < 3; ++k) xv[r].mf[k] = (float)xv[r].mi[k];
@@ -255,13 +255,14 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
       bulk_g2s(&sf[s][0], src0 + tn * TF, bytes, &bar[s]);
     }
   }
-  float2* out = fpart + d.fpart_off + (int64_t)split * d.nband;
+  float2* out = fpart + d.fpart_off + (int64_t)split * d.ne;
 #pragma unroll
   for (int r = 0; r < R; ++r)
-    if (mloc[r] < d.nband) out[mloc[r]] = acc[r];
+    if (mloc[r] < d.ne) out[mloc[r]] = acc[r];
 }
 
 // ft_list = (2/M) * sum over splits; optional scatter of ft * OTF into the grid.
+// With a mirrored band (herm) the entries past ne are conj of their mirrors.
 __global__ void k_meshft_fwd_epi(Cells cells, const int32_t* __restrict__ band_index,
                                  const float2* __restrict__ fpart,
                                  const double* __restrict__ area_part,
@@ -272,31 +273,71 @@ __global__ void k_meshft_fwd_epi(Cells cells, const int32_t* __restrict__ band_i
   const CellDesc d = cell_get(cells, ci);
   const double M = block_sum_list(area_part + d.face_blk0, (d.nt + kBlk - 1) / kBlk, sh);
   const int m = (blockIdx.x - d.band_blk0) * kBlk + threadIdx.x;
-  if (m >= d.nband) return;
+  if (m >= d.ne) return;
   double sx = 0.0, sy = 0.0;
   const float2* p = fpart + d.fpart_off + m;
-  for (int s = 0; s < d.fsplit; ++s) {
-    const float2 v = p[(int64_t)s * d.nband];
+  // eight loads in flight, summed in split order (fixed result)
+  int s = 0;
+  for (; s + 8 <= d.fsplit; s += 8) {
+    float2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = p[(int64_t)(s + u) * d.ne];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      sx += v[u].x;
+      sy += v[u].y;
+    }
+  }
+  for (; s < d.fsplit; ++s) {
+    const float2 v = p[(int64_t)s * d.ne];
     sx += v.x;
     sy += v.y;
   }
   const double sc = d.nt > 0 ? 2.0 / M : 0.0;  // no faces: ft = 0 as in the reference
   const float2 ft = make_float2((float)(sx * sc), (float)(sy * sc));
+  const int64_t nvox = (int64_t)d.n[0] * d.n[1] * d.n[2];
+  const int mr = d.nband - 1 - m;  // mirror entry
+  const bool mirror = d.herm && mr != m;
   ft_list[d.b_off + m] = ft;
+  if (mirror) ft_list[d.b_off + mr] = make_float2(ft.x, -ft.y);
+  const int32_t idx = band_index[d.b_off + m];
+  const int32_t idr = mirror ? band_index[d.b_off + mr] : idx;
+  const bool ok = idx >= 0 && (int64_t)idx < nvox &&
+                  (!mirror || (int64_t)idr == nvox - 1 - (int64_t)idx);
+  if (!ok) {
+    set_error(err, DM_ERR_BAD_INDEX);
+    return;
+  }
   if (grid) {
-    const int32_t idx = band_index[d.b_off + m];
-    if (idx < 0 || (int64_t)idx >= (int64_t)d.n[0] * d.n[1] * d.n[2]) {
-      set_error(err, DM_ERR_BAD_INDEX);
-      return;
-    }
     const float o = otf ? otf[d.grid_off + idx] : 1.0f;
     grid[d.grid_off + idx] = make_float2(ft.x * o, ft.y * o);
+    if (mirror) {
+      const float orr = otf ? otf[d.grid_off + idr] : 1.0f;
+      grid[d.grid_off + idr] = make_float2(ft.x * orr, -ft.y * orr);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Backward: band records with the cotangent, and per-block sums of
-// s = sum Re(conj(g) ft).
+// s = sum Re(conj(g) ft) over the whole band.  With a mirrored band (herm) the
+// record of entry m < ne carries g(xi) + conj(g(-xi)): the adjoint of
+// ft(-xi) = conj(ft(xi)).
+
+// Cotangent of band entry gm (0 for an invalid voxel index).
+__device__ __forceinline__ float2 band_cotangent(const CellDesc& d, int64_t gm, int32_t idx,
+                                                 bool ok, const float2* __restrict__ grad_list,
+                                                 const float2* __restrict__ grad_grid,
+                                                 const float* __restrict__ otf,
+                                                 float grad_scale, float2& G) {
+  if (!ok) {
+    G = make_float2(0.f, 0.f);
+    return G;
+  }
+  G = grad_list ? grad_list[gm] : grad_grid[d.grid_off + idx];
+  const float gs = grad_scale * (otf ? otf[d.grid_off + idx] : 1.0f);
+  return make_float2(gs * G.x, gs * G.y);
+}
 
 __global__ void k_bwd_band_prep(Cells cells, const int32_t* __restrict__ band_index,
                                 const float2* __restrict__ grad_list,
@@ -309,30 +350,45 @@ __global__ void k_bwd_band_prep(Cells cells, const int32_t* __restrict__ band_in
   const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.band_blk0; });
   const CellDesc d = cell_get(cells, ci);
   const int m = (blockIdx.x - d.band_blk0) * kBlk + threadIdx.x;
+  const int64_t nvox = (int64_t)d.n[0] * d.n[1] * d.n[2];
   double s = 0.0;
   if (m < d.nband) {
     const int64_t gm = d.b_off + m;
     int32_t idx = band_index[gm];
-    const bool ok = idx >= 0 && (int64_t)idx < (int64_t)d.n[0] * d.n[1] * d.n[2];
+    const bool ok = idx >= 0 && (int64_t)idx < nvox;
     if (!ok) {
       set_error(err, DM_ERR_BAD_INDEX);
       idx = 0;
     }
-    float2 G = grad_list ? grad_list[gm] : grad_grid[d.grid_off + idx];
-    if (!ok) G = make_float2(0.f, 0.f);
-    const float o = otf ? otf[d.grid_off + idx] : 1.0f;
-    const float gs = grad_scale * o;
-    const float2 g = make_float2(gs * G.x, gs * G.y);
+    float2 G;
+    float2 g = band_cotangent(d, gm, idx, ok, grad_list, grad_grid, otf, grad_scale, G);
     const float2 ft = ft_list[gm];
     if (grad_otf_band) grad_otf_band[gm] = grad_scale * (G.x * ft.x + G.y * ft.y);
     s = (double)g.x * ft.x + (double)g.y * ft.y;
-    XiRec r;
-    band_to_m(idx, d, r.mi);
+    if (m < d.ne) {
+      const int mr = d.nband - 1 - m;
+      if (d.herm && mr != m) {
+        const int64_t gr = d.b_off + mr;
+        int32_t idr = band_index[gr];
+        const bool okr = ok && (int64_t)idr == nvox - 1 - (int64_t)idx;
+        if (!okr) {
+          set_error(err, DM_ERR_BAD_INDEX);
+          idr = 0;
+        }
+        float2 Gr;
+        const float2 gr_ = band_cotangent(d, gr, idr, okr, grad_list, grad_grid, otf,
+                                          grad_scale, Gr);
+        g.x += gr_.x;
+        g.y -= gr_.y;
+      }
+      XiRec r;
+      band_to_m(idx, d, r.mi);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) r.mf[k] = (float)r.mi[k];
-    r.g_re = g.x;
-    r.g_im = g.y;
-    xrec[gm] = r;
+      for (int k = 0; k < 3; ++k) r.mf[k] = (float)r.mi[k];
+      r.g_re = g.x;
+      r.g_im = g.y;
+      xrec[gm] = r;
+    }
   }
   const double t = block_sum_d(s, sh);
   if (threadIdx.x == 0) s_part[blockIdx.x] = t;
@@ -367,7 +423,7 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
   const int fb = local % d.fblocks;
   const int chunk = local / d.fblocks;
   const int x0 = chunk * d.bxchunk;
-  const int nx = min(d.nband, x0 + d.bxchunk) - x0;
+  const int nx = min(d.ne, x0 + d.bxchunk) - x0;
   if (nx <= 0 || d.nt <= 0) return;
 
   FaceGeom geom[F];
@@ -665,11 +721,16 @@ void set_variants(int fwd, int bwd) {
   g_bwd_variant.store(bwd);
 }
 
+void set_band_half(CellDesc& d, bool herm) {
+  d.herm = herm ? 1 : 0;
+  d.ne = herm ? (d.nband + 1) / 2 : d.nband;
+}
+
 void plan_cell_tiles(CellDesc& d) {
   const FwdVariant fv = kFwdVariants[fwd_variant()];
   const BwdVariant bv = kBwdVariants[bwd_variant()];
   const int64_t xtile = (int64_t)fv.NT * fv.R;
-  d.xtiles = (int32_t)std::max<int64_t>(1, cdiv(d.nband, xtile));
+  d.xtiles = (int32_t)std::max<int64_t>(1, cdiv(d.ne, xtile));
   int64_t fsplit = std::max<int64_t>(1, cdiv((int64_t)num_sms() * fv.waves, d.xtiles));
   fsplit = std::min<int64_t>(fsplit, std::max<int64_t>(1, cdiv(d.nt, kFwdTF)));
   int64_t fchunk = cdiv(std::max<int64_t>(d.nt, 1), fsplit);
@@ -680,11 +741,11 @@ void plan_cell_tiles(CellDesc& d) {
   const int64_t fblock = (int64_t)bv.NT * bv.F;
   d.fblocks = (int32_t)std::max<int64_t>(1, cdiv(d.nt, fblock));
   int64_t bch = std::max<int64_t>(1, cdiv((int64_t)num_sms() * bv.waves, d.fblocks));
-  bch = std::min<int64_t>(bch, std::max<int64_t>(1, cdiv(d.nband, kBwdTX)));
-  int64_t bx = cdiv(std::max<int64_t>(d.nband, 1), bch);
+  bch = std::min<int64_t>(bch, std::max<int64_t>(1, cdiv(d.ne, kBwdTX)));
+  int64_t bx = cdiv(std::max<int64_t>(d.ne, 1), bch);
   bx = cdiv(bx, kBwdTX) * kBwdTX;
   d.bxchunk = (int32_t)bx;
-  d.bchunks = (int32_t)std::max<int64_t>(1, cdiv(d.nband, bx));
+  d.bchunks = (int32_t)std::max<int64_t>(1, cdiv(d.ne, bx));
 }
 
 void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t) {
@@ -704,7 +765,7 @@ void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t) {
     t.nv += d.nv;
     t.nt += d.nt;
     t.nband += d.nband;
-    t.fpart += (int64_t)d.fsplit * d.nband;
+    t.fpart += (int64_t)d.fsplit * d.ne;
     t.bpart += (int64_t)d.bchunks * 10 * d.nt;
     t.face_blks += std::max<int64_t>(1, cdiv(d.nt, kBlk));
     t.band_blks += std::max<int64_t>(1, cdiv(d.nband, kBlk));

@@ -40,6 +40,7 @@ int num_sms();
 void count_launches(int n);
 void profile_begin(int kind, cudaStream_t st);
 void profile_end(int kind, cudaStream_t st);
+void set_band_half(CellDesc& d, bool herm);
 void plan_cell_tiles(CellDesc& d);
 void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t);
 

@@ -13,7 +13,8 @@ import torch
 
 from . import _native as N
 
-__all__ = ["FreqGrid", "narrowband", "topology", "meshft", "meshft_list",
+__all__ = ["FreqGrid", "narrowband", "band_is_hermitian", "band_eval_count", "band_box",
+           "topology", "meshft", "meshft_list",
            "meshft_backward_list", "gaussian_otf", "image_loss", "adam_step"]
 
 
@@ -64,7 +65,42 @@ def narrowband(otf: torch.Tensor, thresh: float) -> torch.Tensor:
                                       N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
             "dm_narrowband_compact")
     c = int(cnt.item())
-    return idx[:c].clone()
+    band = idx[:c].clone()
+    flag = torch.zeros(1, dtype=torch.int32, device=otf.device)
+    N.check(lib.dm_narrowband_hermitian(N.ptr(band), c, n, N.ptr(flag),
+                                        N.stream_ptr(otf.device)), "dm_narrowband_hermitian")
+    _HERM[id(band)] = (weakref.ref(band), bool(flag.item()))
+    return band
+
+
+# Bands from narrowband() that are closed under xi -> -xi (the meshFT calls then
+# evaluate half of them); keyed by id with a weak reference to the tensor.
+_HERM: dict = {}
+
+
+def band_is_hermitian(band: torch.Tensor) -> bool:
+    """True for a band made by narrowband() whose voxel set is symmetric about the
+    grid centre (every Gaussian OTF gives one)."""
+    e = _HERM.get(id(band))
+    if e is None or e[0]() is not band:
+        return False
+    return e[1]
+
+
+def band_eval_count(band: torch.Tensor) -> int:
+    """Frequencies the meshFT kernels evaluate for ``band``: half (rounded up)
+    of a mirror-symmetric band, else all of it."""
+    n = int(band.numel())
+    return (n + 1) // 2 if band_is_hermitian(band) else n
+
+
+def band_box(grid: FreqGrid, band) -> N.DmBox:
+    """The C box of ``grid`` with the DM_BAND_* flags of ``band`` (a tensor from
+    narrowband(), or a bool: the band is known to be mirror-symmetric)."""
+    herm = band if isinstance(band, bool) else band_is_hermitian(band)
+    b = N.DmBox.from_buffer_copy(grid.cbox)
+    b.band_flags = N.DM_BAND_HERMITIAN if herm else 0
+    return b
 
 
 def order_band_by_radius(band: torch.Tensor, grid: FreqGrid) -> torch.Tensor:
@@ -133,8 +169,8 @@ def meshft_list(verts, faces, coeff, grid: FreqGrid, band, otf=None, spectrum=No
     ft = torch.empty(nb, dtype=torch.complex64, device=verts.device)
     ws = N.WORKSPACES.get("fwd", lib.dm_meshft_forward_workspace_size(nv, nt, nb), verts.device)
     N.check(lib.dm_meshft_forward(
-        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(grid.cbox), N.ptr(band),
-        nb, N.ptr(otf), N.ptr(ft), N.ptr(spectrum), N.ptr(ws), ws.numel(),
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(band_box(grid, band)),
+        N.ptr(band), nb, N.ptr(otf), N.ptr(ft), N.ptr(spectrum), N.ptr(ws), ws.numel(),
         N.stream_ptr(verts.device)), "dm_meshft_forward")
     return ft
 
@@ -150,8 +186,8 @@ def meshft_backward_list(verts, faces, coeff, grid: FreqGrid, band, ft, grad_lis
     topo = topology(faces, nv)
     ws = N.WORKSPACES.get("bwd", lib.dm_meshft_backward_workspace_size(nv, nt, nb), verts.device)
     N.check(lib.dm_meshft_backward(
-        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(grid.cbox), N.ptr(band), nb,
-        N.ptr(grad_list), N.ptr(grad_grid), N.ptr(otf), float(scale), N.ptr(ft), N.ptr(topo),
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), ctypes.byref(band_box(grid, band)),
+        N.ptr(band), nb, N.ptr(grad_list), N.ptr(grad_grid), N.ptr(otf), float(scale), N.ptr(ft), N.ptr(topo),
         N.ptr(gv), N.ptr(gc), N.ptr(go), N.ptr(ws), ws.numel(), N.stream_ptr(verts.device)),
         "dm_meshft_backward")
     return gv, gc, go

@@ -66,6 +66,11 @@ class MeshRenderer:
     def n_band(self) -> int:
         return 0 if self.band is None else int(self.band.numel())
 
+    @property
+    def n_eval(self) -> int:
+        """Band frequencies the meshFT kernels evaluate (half of a symmetric band)."""
+        return 0 if self.band is None else ops.band_eval_count(self.band)
+
     # -- forward only ----------------------------------------------------------
     @torch.no_grad()
     def render(self, verts, faces, coeff) -> torch.Tensor:

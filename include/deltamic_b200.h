@@ -33,20 +33,32 @@ typedef struct CUstream_st* dm_stream_t; /* == cudaStream_t */
 
 #define DM_OK 0
 #define DM_ERR_INVALID_ARG 1   /* null pointer, negative size, bad dtype ... */
-#define DM_ERR_BAD_INDEX 2     /* a face index outside [0, nv) */
+#define DM_ERR_BAD_INDEX 2     /* a face or band index out of range, or a broken band mirror */
 #define DM_ERR_SIZE 4          /* a size beyond what the kernels index (int32 voxels) */
 #define DM_ERR_WORKSPACE 8     /* workspace smaller than the query returned */
 #define DM_ERR_CUDA 16         /* a CUDA launch or copy failed */
 #define DM_ERR_TIMEOUT 32      /* a bounded device wait gave up */
 #define DM_ERR_UNSUPPORTED 64  /* valid request this build does not serve */
 
-/* Box of a meshFT grid: box_size (render.py:116-123) and box_shape. */
+/* Box of a meshFT grid: box_size (render.py:116-123) and box_shape, plus the
+ * properties of the narrow band passed with it. */
 typedef struct dm_box {
-  double lo[3];     /* box_size[:,0] */
-  double hi[3];     /* box_size[:,1] */
-  int32_t shape[3]; /* box_shape */
-  int32_t reserved;
+  double lo[3];       /* box_size[:,0] */
+  double hi[3];       /* box_size[:,1] */
+  int32_t shape[3];   /* box_shape */
+  int32_t band_flags; /* DM_BAND_* bits of the band passed with this box */
 } dm_box;
+
+/* The band is closed under xi -> -xi: with N voxels and the band in ascending
+ * order, band_index[n_band-1-m] == N-1-band_index[m] for every m (the voxel of
+ * -xi on the centred grid is N-1-idx).  Every OTF with OTF(-xi) == OTF(xi), the
+ * Gaussian OTFs among them, gives such a band (dm_narrowband_hermitian tests
+ * it).  The meshFT calls then evaluate the first (n_band+1)/2 frequencies only
+ * and take the others from ft(-xi) = conj(ft(xi)) (the transform of a real
+ * indicator); the backward folds the cotangent of -xi into xi the same way.
+ * The kernels check the mirror relation and raise DM_ERR_BAD_INDEX where it
+ * fails.  Without the bit every frequency is evaluated. */
+#define DM_BAND_HERMITIAN 1
 
 /* ABI version of this header (bumped on any signature change). */
 int dm_abi_version(void);
@@ -69,6 +81,12 @@ size_t dm_narrowband_workspace_size(int64_t n_voxels);
 int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh,
                           int32_t* band_index, int64_t* band_count, void* workspace,
                           size_t ws_bytes, dm_stream_t stream);
+
+/* Asynchronous: *is_hermitian (DEVICE int32) = 1 if band_index[0..n_band) (of a
+ * grid of n_voxels) is closed under xi -> -xi in the sense of DM_BAND_HERMITIAN,
+ * else 0.  No counterpart in the reference, which evaluates every frequency. */
+int dm_narrowband_hermitian(const int32_t* band_index, int64_t n_band, int64_t n_voxels,
+                            int32_t* is_hermitian, dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Vertex <- face incidence (CSR), built once per topology.  Replaces the host

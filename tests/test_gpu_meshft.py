@@ -270,3 +270,73 @@ def test_float64_module_matches_float32_path():
         assert ft.dtype == (torch.complex64 if dt == torch.float32 else torch.complex128)
     assert rel_l2(out[1][0], out[0][0]) < 1e-6
     assert rel_l2(out[1][1], out[0][1]) < 1e-5
+
+
+@pytest.mark.parametrize("level,shape", [(2, (24, 20, 18)), (2, (15, 17, 13)), (3, (32, 31, 30))])
+def test_half_band_matches_full_band(level, shape):
+    """A band from a Gaussian OTF is mirror-symmetric, so the kernels evaluate
+    half of it; the results equal the every-frequency path (a clone of the band
+    carries no symmetry flag) and the oracle.  Odd shapes hold xi = 0 itself."""
+    v, f, c, box, shape, sigma, thresh = _case(level, shape, sigma=np.array(
+        [[2e-3, 4e-4, 0.0], [4e-4, 1e-3, -3e-4], [0.0, -3e-4, 4e-3]]))
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    assert ops.band_is_hermitian(band)
+    full = band.clone()
+    assert not ops.band_is_hermitian(full)
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    ft_h = ops.meshft_list(V, F, C, grid, band)
+    ft_g = ops.meshft_list(V, F, C, grid, full)
+    h = ft_h.cpu().numpy()
+    assert np.array_equal(h[::-1], np.conj(h))
+    assert rel_l2(h, ft_g.cpu().numpy()) < 1e-6
+    ref = oracle.meshft_forward(v - box[:, 0], f, c, _oracle_xi(grid, band))
+    assert rel_l2(h, ref) < TOL_FT
+    rng = np.random.default_rng(5)
+    G = _t(rng.normal(size=(band.numel(), 2))).view(torch.complex64).view(-1).contiguous()
+    oh = ops.meshft_backward_list(V, F, C, grid, band, ft_h, grad_list=G, otf=otf.view(-1),
+                                  want_otf=True)
+    og = ops.meshft_backward_list(V, F, C, grid, full, ft_g, grad_list=G, otf=otf.view(-1),
+                                  want_otf=True)
+    for a, b in zip(oh, og):
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+    gv_ref, gc_ref = oracle.meshft_backward(
+        v - box[:, 0], f, c, _oracle_xi(grid, band),
+        (G * otf.view(-1)[band.long()]).cpu().numpy().astype(np.complex128), ref)
+    assert rel_l2(oh[0].cpu().numpy(), gv_ref) < TOL_GV
+    assert rel_l2(oh[1].cpu().numpy(), gc_ref) < TOL_GC
+
+
+def test_asymmetric_band_takes_the_full_path():
+    v, f, c, box, shape, sigma, thresh = _case(2, (20, 20, 20))
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    o2 = otf.clone().view(-1)
+    o2[band[:3].long()] = 0.0  # drop three voxels on one side only
+    b2 = ops.narrowband(o2.view(otf.shape), thresh)
+    assert not ops.band_is_hermitian(b2)
+    ft = ops.meshft_list(_t(v), _t(f, torch.int64), _t(c), grid, b2)
+    ref = oracle.meshft_forward(v - box[:, 0], f, c, _oracle_xi(grid, b2))
+    assert rel_l2(ft.cpu().numpy(), ref) < TOL_FT
+
+
+def test_symmetry_flag_on_asymmetric_band_is_reported():
+    """DM_BAND_HERMITIAN on a band that is not mirror-symmetric is caught by the
+    kernels' mirror check (status word), with every access in bounds."""
+    import ctypes
+    from deltamic_b200 import _native as N
+    v, f, c, box, shape, sigma, thresh = _case(1, (12, 12, 12))
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    bad = band[1:].contiguous()  # one entry short: the mirror relation breaks
+    lib = N.lib()
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    nb = bad.numel()
+    ws = torch.zeros(lib.dm_meshft_forward_workspace_size(len(v), len(f), nb), dtype=torch.uint8,
+                     device=DEV)
+    ft = torch.empty(nb, dtype=torch.complex64, device=DEV)
+    box_h = ops.band_box(grid, True)
+    st = lib.dm_meshft_forward(N.ptr(V), len(v), N.ptr(F), len(f), N.ptr(C), ctypes.byref(box_h),
+                               N.ptr(bad), nb, None, N.ptr(ft), None, N.ptr(ws), ws.numel(),
+                               N.stream_ptr(DEV))
+    assert st == N.DM_OK
+    flags = N._INT()
+    assert lib.dm_device_error(N.ptr(ws), ctypes.byref(flags), N.stream_ptr(DEV)) == N.DM_OK
+    assert flags.value & N.DM_ERR_BAD_INDEX

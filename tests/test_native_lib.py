@@ -37,7 +37,7 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
 
 
 def test_abi_version_and_status_strings(lib):
-    assert lib.dm_abi_version() == 1
+    assert lib.dm_abi_version() == 2
     assert lib.dm_status_string(0) == b"ok"
     assert b"index" in lib.dm_status_string(2)
 

@@ -33,6 +33,24 @@ def test_translation_is_a_phase():
     assert np.allclose(ft1, ft0 * np.exp(-1j * xi @ t), rtol=1e-10, atol=1e-12)
 
 
+@pytest.mark.parametrize("shape", [(15, 15, 15), (16, 13, 12)])
+def test_hermitian_band_and_spectrum(shape):
+    """The two facts behind evaluating half of a symmetric band: a Gaussian OTF's
+    band is closed under xi -> -xi, which on the centred grid maps flat voxel
+    index i to N-1-i, and the mesh transform obeys ft(-xi) = conj(ft(xi))."""
+    v, f, c, box, _ = _small_case(seed=3)
+    axes = oracle.frequency_axes(box, shape)
+    sigma = np.array([[2e-3, 4e-4, 0.0], [4e-4, 1e-3, -3e-4], [0.0, -3e-4, 4e-3]])
+    otf = oracle.gaussian_otf(sigma, *axes)
+    band = oracle.band_indices(otf, 1e-5)
+    n = int(np.prod(shape))
+    assert np.array_equal(band[::-1], n - 1 - band)
+    xi = oracle.xi_list_from_band(band, axes)
+    assert np.array_equal(xi[::-1], -xi)
+    ft = oracle.meshft_forward(v - box[:, 0], f, c, xi)
+    assert np.allclose(ft[::-1], np.conj(ft), rtol=0, atol=1e-13)
+
+
 def test_coefficient_scale_invariance():
     v, f, c, box, shape = _small_case()
     o = oracle.pipeline(v, f, c, box, shape, 1e-3 * np.eye(3), 1e-5, loss="sum")
