@@ -89,6 +89,11 @@ SIGNATURES = {
                                           ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),
     "dm_image_loss_workspace_size": (_SZ, [_I64]),
     "dm_image_loss": (_INT, [_P, _I64, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
+    "dm_band_bounds": (_INT, [_P, _I64, _BOXP, _P, _P]),
+    "dm_render_loss_bandbox_supported": (_INT, [_BOXP, ctypes.POINTER(ctypes.c_int32)]),
+    "dm_render_loss_bandbox_workspace_size": (_SZ, [_BOXP, ctypes.POINTER(ctypes.c_int32)]),
+    "dm_render_loss_bandbox": (_INT, [_P, _P, _I64, _BOXP, ctypes.POINTER(ctypes.c_int32), _P,
+                                      _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     "dm_conv3d_s2_workspace_size": (_SZ, [_INT] * 6),
     "dm_conv3d_s2_forward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _P, _INT, _P, _P, _P]),
     "dm_conv3d_s2_backward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P, _P, _P,

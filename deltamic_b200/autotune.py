@@ -58,19 +58,24 @@ def apply(variants) -> None:
     N.check(N.lib().dm_set_variants(int(variants[0]), int(variants[1])), "dm_set_variants")
 
 
-def _time(fn, reps):
+def _time(fn, reps, trials=3):
+    """Fastest of ``trials`` event-timed runs of ``reps`` calls each (after one
+    untimed call): variants a few percent apart are told apart reliably."""
     fn()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        fn()
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+    best = float("inf")
+    for _ in range(trials):
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / reps)
+    return best
 
 
-def tune(verts, faces, coeff, grid, band, reps=3, force=False):
+def tune(verts, faces, coeff, grid, band, reps=4, force=False):
     """Pick and apply the fastest (forward, adjoint) variants for this size class."""
     if not _CACHE:
         _load()

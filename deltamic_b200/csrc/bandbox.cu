@@ -1,0 +1,1034 @@
+// Render + image loss + adjoint for a spectrum that is zero outside the narrow
+// band: separable inverse / forward DFTs pruned to the band's bounding box.
+//
+// The reference renders with torch.fft.ifftn of the dense spectrum
+// (render.py:177-180) and its fitting loop back-propagates through it with a
+// dense fftn.  The spectrum S = ft * OTF is non-zero only on the band, whose
+// voxels lie in the index box [lo_d, lo_d + ext_d) (at 200^3 with the
+// anisotropic PSF: 44 x 44 x 22 of 200^3).  With w_d = e^{2 pi i / n_d}:
+//
+//   T1[x0][j1][j2] = sum_j0 S[lo0+j0][lo1+j1][lo2+j2] w0^{(lo0+j0) x0}     (axis 0)
+//   T2[x0][x1][j2] = sum_j1 T1[x0][j1][j2] w1^{(lo1+j1) x1}                (axis 1)
+//   z[x0][x1][x2]  = 1/N sum_j2 T2[x0][x1][j2] w2^{(lo2+j2) x2}            (axis 2, lines)
+//
+// which is ifftn(S) exactly (the DFT is separable; only zero terms are left out).
+// The axis-2 pass is the only one over the whole grid.  It also forms |z| and
+// its min / max.  A second line pass forms the normalised image, the loss and
+// g = dL/dz (normalize_tensor, render.py:5-6, and the loss of the fitting loop),
+// and contracts each line with conj(w2) at once; two small pruned passes and a
+// gather at the band voxels then give G = fftn(dL/dz) on the band -- the
+// cotangent the meshFT adjoint takes.  Full-grid traffic per step: z written
+// once and read once, the target read once.
+//
+// Every sum has a fixed order (no atomics on values): results are bitwise
+// reproducible.  The min / max gradient is shared evenly by tied voxels as
+// torch's min/max backward does (a single voxel is the common case, added in
+// the gather; several are folded into the line contractions by k_bb_ties).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "band_internal.h"
+#include "dm_common.cuh"
+
+namespace dm {
+namespace {
+
+constexpr int kLines = 32;         // grid lines (x0, x1) per CTA of the line passes
+constexpr int kLineThreads = 256;  // 8 warps; warp w owns lines 4w..4w+3 (z pass)
+constexpr int kMaxExt2 = 32;       // band extent along axis 2 served by the line passes
+constexpr int kGemmThreads = 256;
+constexpr int kSmemLimit = 220 * 1024;
+
+struct BBShape {
+  int32_t n[3];    // box shape
+  int32_t lo[3];   // band box lower index per axis
+  int32_t ext[3];  // band box extent per axis
+  int32_t ldj;     // row length of the transposed axis-2 table: ext2 rounded up to 8
+  int32_t zc;      // z pass: columns per thread (column block of 32 zc)
+  int32_t ldw2;    // row length of the axis-2 table: n2 rounded up to whole column blocks
+  int32_t q1split; // K split of the axis-1 forward contraction (partials summed by the next)
+  int32_t q1chunk; // positions x1 per split (a multiple of 16)
+  int32_t g0split; // K split of the axis-0 forward contraction (partials summed in the gather)
+  int32_t g0chunk; // positions x0 per split
+  int64_t nlines;  // n0 * n1
+  int64_t nvox;
+};
+
+// min / max of |z| with the first flat index of each and the number of ties
+// (box sizes stay below 2^31 voxels)
+struct MMC {
+  float mn, mx;
+  int32_t imn, imx;
+  int32_t cmn, cmx;
+};
+
+struct LP {
+  double loss, dmn, dmx;
+};
+
+// Per-call state in the workspace header.
+struct BBHdr {
+  int err;
+  int ties_full;      // several voxels tie at the min or max: k_bb_ties folds them in
+  unsigned int done[2];  // CTAs finished in the z / gradient pass (last one reduces)
+  float mn, mx;
+  int64_t imn, imx, cmn, cmx;
+  float add_mn, add_mx;  // d loss / d min (max) per tied voxel
+  double fin[3];         // loss, d loss / d min, d loss / d max
+};
+
+__device__ __forceinline__ float cabs2(float2 z) { return sqrtf(fmaf(z.x, z.x, z.y * z.y)); }
+
+__device__ __forceinline__ float2 cmac(float2 acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+  return acc;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// e^{2 pi i (k x mod n) / n}, exact index arithmetic, double-precision angle.
+__device__ __forceinline__ float2 unit_root(int32_t k, int32_t x, int32_t n) {
+  const int64_t r = ((int64_t)k * (int64_t)x) % (int64_t)n;
+  double s, c;
+  sincospi(2.0 * (double)r / (double)n, &s, &c);
+  return make_float2((float)c, (float)s);
+}
+
+__device__ __forceinline__ void mmc_add(MMC& r, float a, int32_t i) {
+  if (a < r.mn) {
+    r.mn = a;
+    r.imn = i;
+    r.cmn = 1;
+  } else if (a == r.mn) {
+    r.cmn += 1;
+    if (i < r.imn) r.imn = i;
+  }
+  if (a > r.mx) {
+    r.mx = a;
+    r.imx = i;
+    r.cmx = 1;
+  } else if (a == r.mx) {
+    r.cmx += 1;
+    if (i < r.imx) r.imx = i;
+  }
+}
+
+__device__ __forceinline__ void mmc_merge(MMC& r, const MMC& o) {
+  if (o.mn < r.mn) {
+    r.mn = o.mn;
+    r.imn = o.imn;
+    r.cmn = o.cmn;
+  } else if (o.mn == r.mn) {
+    r.cmn += o.cmn;
+    r.imn = min(r.imn, o.imn);
+  }
+  if (o.mx > r.mx) {
+    r.mx = o.mx;
+    r.imx = o.imx;
+    r.cmx = o.cmx;
+  } else if (o.mx == r.mx) {
+    r.cmx += o.cmx;
+    r.imx = min(r.imx, o.imx);
+  }
+}
+
+__device__ __forceinline__ MMC mmc_shfl(const MMC& r, int o) {
+  MMC q;
+  q.mn = __shfl_down_sync(0xffffffffu, r.mn, o);
+  q.mx = __shfl_down_sync(0xffffffffu, r.mx, o);
+  q.imn = __shfl_down_sync(0xffffffffu, r.imn, o);
+  q.imx = __shfl_down_sync(0xffffffffu, r.imx, o);
+  q.cmn = __shfl_down_sync(0xffffffffu, r.cmn, o);
+  q.cmx = __shfl_down_sync(0xffffffffu, r.cmx, o);
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// Root tables: W_d[j][x] = w_d^{(lo_d + j) x} (rows j < ext_d, columns x < n_d;
+// the axis-2 rows padded with zeros to ldw2), and the conjugate axis-2 table
+// transposed, W2T[x][j] (rows padded to ldj).  Also clears the CTA counters.
+
+__global__ void k_bb_tables(BBShape s, float2* __restrict__ w0, float2* __restrict__ w1,
+                            float2* __restrict__ w2, float2* __restrict__ w2t, BBHdr* hdr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    hdr->done[0] = 0u;
+    hdr->done[1] = 0u;
+  }
+  const int64_t e0 = (int64_t)s.ext[0] * s.n[0];
+  const int64_t e1 = (int64_t)s.ext[1] * s.n[1];
+  const int64_t e2 = (int64_t)s.ext[2] * s.ldw2;
+  const int64_t e3 = (int64_t)s.n[2] * s.ldj;
+  const int64_t tot = e0 + e1 + e2 + e3;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < e0) {
+      const int j = (int)(i / s.n[0]), x = (int)(i % s.n[0]);
+      w0[i] = unit_root(s.lo[0] + j, x, s.n[0]);
+    } else if (i < e0 + e1) {
+      const int64_t r = i - e0;
+      const int j = (int)(r / s.n[1]), x = (int)(r % s.n[1]);
+      w1[r] = unit_root(s.lo[1] + j, x, s.n[1]);
+    } else if (i < e0 + e1 + e2) {
+      const int64_t r = i - e0 - e1;
+      const int j = (int)(r / s.ldw2), x = (int)(r % s.ldw2);
+      w2[r] = x < s.n[2] ? unit_root(s.lo[2] + j, x, s.n[2]) : make_float2(0.f, 0.f);
+    } else {
+      const int64_t r = i - e0 - e1 - e2;
+      const int x = (int)(r / s.ldj), j = (int)(r % s.ldj);
+      float2 v = make_float2(0.f, 0.f);
+      if (j < s.ext[2]) {
+        v = unit_root(s.lo[2] + j, x, s.n[2]);
+        v.y = -v.y;
+      }
+      w2t[r] = v;
+    }
+  }
+}
+
+// S = ft * OTF at the band voxels, written into the (zeroed) band box T0.
+__global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_t nb,
+                             const float2* __restrict__ ft, const float* __restrict__ otf,
+                             float2* __restrict__ t0, int* err) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nb) return;
+  const int32_t idx = band[m];
+  if (idx < 0 || (int64_t)idx >= s.nvox) {
+    set_error(err, DM_ERR_BAD_INDEX);
+    return;
+  }
+  const int32_t n12 = s.n[1] * s.n[2];
+  const int32_t k0 = idx / n12, rem = idx - k0 * n12;
+  const int32_t k1 = rem / s.n[2], k2 = rem - k1 * s.n[2];
+  const int32_t j0 = k0 - s.lo[0], j1 = k1 - s.lo[1], j2 = k2 - s.lo[2];
+  if (j0 < 0 || j0 >= s.ext[0] || j1 < 0 || j1 >= s.ext[1] || j2 < 0 || j2 >= s.ext[2]) {
+    set_error(err, DM_ERR_BAD_INDEX);
+    return;
+  }
+  const float o = otf ? otf[idx] : 1.0f;
+  const float2 f = ft[m];
+  t0[((int64_t)j0 * s.ext[1] + j1) * s.ext[2] + j2] = make_float2(f.x * o, f.y * o);
+}
+
+// ---------------------------------------------------------------------------
+// Small batched complex GEMM with a root table on the left:
+//   C[kp][b][m][n] = sum_{k in split kp} A(m, k) X[b][k][n],
+//   X = the sum (in order) of ``xparts`` arrays sxp elements apart,
+//   kInv:  A(m, k) = W[k * ldw + m]        (inverse pass: m = position, k = band offset)
+//   else:  A(m, k) = conj(W[m * ldw + k])  (forward pass: m = band offset, k = position)
+// blockIdx.z = kp * batch + b; split kp covers k in [kp kc, (kp+1) kc) and writes its
+// partial sums at C + kp * scp.  Tile 64 (m) x 32 (n), k in steps of 16 through
+// shared memory with the next step's tiles loaded into registers while the current
+// one is used; each thread owns 4 x 2 outputs.
+
+template <bool kInv>
+__global__ void __launch_bounds__(kGemmThreads)
+    k_bb_gemm(const float2* __restrict__ W, int ldw, int M, int N, int K, int batch, int kc,
+              const float2* __restrict__ X, int64_t sxb, int64_t sxk, int xparts, int64_t sxp,
+              float2* __restrict__ C, int64_t scb, int64_t scm, int64_t scp) {
+  __shared__ __align__(16) float2 As[16][64];
+  __shared__ __align__(16) float2 Bs[16][32];
+  const int t = threadIdx.x;
+  const int tm = t >> 4, tn = t & 15;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 32;
+  const int64_t b = blockIdx.z % batch;
+  const int kp = blockIdx.z / batch;
+  const int kb = kp * kc, ke = min(K, kb + kc);
+  const float2* Xb = X + b * sxb;
+  float2 ra[4], rb[2];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int e = t + kGemmThreads * r;
+      const int m = kInv ? (e & 63) : (e >> 4);
+      const int k = kInv ? (e >> 6) : (e & 15);
+      float2 v = make_float2(0.f, 0.f);
+      if (m0 + m < M && k0 + k < ke) {
+        if (kInv) {
+          v = W[(int64_t)(k0 + k) * ldw + m0 + m];
+        } else {
+          v = W[(int64_t)(m0 + m) * ldw + k0 + k];
+          v.y = -v.y;
+        }
+      }
+      ra[r] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int e = t + kGemmThreads * r;
+      const int n = e & 31, k = e >> 5;
+      float2 v = make_float2(0.f, 0.f);
+      if (n0 + n < N && k0 + k < ke) {
+        const float2* px = Xb + (int64_t)(k0 + k) * sxk + n0 + n;
+        v = px[0];
+        for (int p = 1; p < xparts; ++p) {
+          const float2 q = px[p * sxp];
+          v.x += q.x;
+          v.y += q.y;
+        }
+      }
+      rb[r] = v;
+    }
+  };
+  float2 acc[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+  if (kb < ke) fetch(kb);
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int e = t + kGemmThreads * r;
+      const int m = kInv ? (e & 63) : (e >> 4);
+      const int k = kInv ? (e >> 6) : (e & 15);
+      As[k][m] = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int e = t + kGemmThreads * r;
+      Bs[e >> 5][e & 31] = rb[r];
+    }
+    __syncthreads();
+    if (k0 + 16 < ke) fetch(k0 + 16);
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      const float4 a01 = *reinterpret_cast<const float4*>(&As[kk][tm * 4]);
+      const float4 a23 = *reinterpret_cast<const float4*>(&As[kk][tm * 4 + 2]);
+      const float4 bb = *reinterpret_cast<const float4*>(&Bs[kk][tn * 2]);
+      const float2 a[4] = {make_float2(a01.x, a01.y), make_float2(a01.z, a01.w),
+                           make_float2(a23.x, a23.y), make_float2(a23.z, a23.w)};
+      const float2 bv[2] = {make_float2(bb.x, bb.y), make_float2(bb.z, bb.w)};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j] = cmac(acc[i][j], a[i], bv[j]);
+    }
+    __syncthreads();
+  }
+  float2* Cb = C + kp * scp + b * scb;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = m0 + tm * 4 + i;
+    if (m >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int n = n0 + tn * 2 + j;
+      if (n < N) Cb[(int64_t)m * scm + n] = acc[i][j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions by the last CTA of a pass: every CTA stores its partial, the CTA
+// that finishes last (counter in the header) combines all partials in a fixed
+// order, so the result does not depend on which CTA that is.
+
+__device__ __forceinline__ MMC mmc_empty() {
+  return MMC{INFINITY, -INFINITY, INT32_MAX, INT32_MAX, 0, 0};
+}
+
+__device__ __forceinline__ MMC mmc_load(const MMC* p) {
+  MMC q;
+  q.mn = __ldcg(&p->mn);
+  q.mx = __ldcg(&p->mx);
+  q.imn = __ldcg(&p->imn);
+  q.imx = __ldcg(&p->imx);
+  q.cmn = __ldcg(&p->cmn);
+  q.cmx = __ldcg(&p->cmx);
+  return q;
+}
+
+// Merge of one MMC per thread over the block; the result is valid in thread 0.
+__device__ MMC block_mmc(MMC r, MMC* sh) {
+  for (int o = 16; o > 0; o >>= 1) mmc_merge(r, mmc_shfl(r, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mmc_merge(r, sh[w]);
+  __syncthreads();
+  return r;
+}
+
+// True in every thread of the CTA that finished last (after its partial is out).
+__device__ bool last_cta(unsigned int* counter, unsigned int total, int* flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(counter, 1u);
+    *flag = prev == total - 1u;
+  }
+  __syncthreads();
+  const bool last = *flag != 0;
+  if (last) __threadfence();
+  return last;
+}
+
+// ---------------------------------------------------------------------------
+// z pass: 32 lines per CTA, columns x2 in blocks of 32*C (blockIdx.y).
+//   z[line][x2] = 1/N sum_j T2[line][j] W2[j][x2];  |z|, min / max.
+// The CTA's T2 rows and W2 column block are staged by bulk copies.  Thread (warp
+// w, lane l): lines 4w..4w+3, columns l + 32c.  The last CTA writes the min /
+// max (first index, tie count) to the header.
+
+template <int C>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bb_zlines(BBShape s, const float2* __restrict__ t2, const float2* __restrict__ w2,
+                float inv_n, float2* __restrict__ z, float* __restrict__ image,
+                MMC* __restrict__ part, BBHdr* hdr) {
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ MMC shm[kLineThreads / 32];
+  __shared__ int last;
+  const int ext = s.ext[2], n2 = s.n[2];
+  constexpr int Wc = 32 * C;
+  float2* xs = sm;                 // [kLines][ext]
+  float2* ws = sm + kLines * ext;  // [ext][Wc]
+  const int64_t line0 = (int64_t)blockIdx.x * kLines;
+  const int col0 = blockIdx.y * Wc;
+  const int64_t nl = min((int64_t)kLines, s.nlines - line0);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t xb = (uint32_t)((nl * ext * (int64_t)sizeof(float2) + 15) & ~(int64_t)15);
+    const uint32_t wb = (uint32_t)(Wc * sizeof(float2));
+    mbar_expect_tx(&bar, xb + (uint32_t)ext * wb);
+    bulk_g2s(xs, t2 + line0 * ext, xb, &bar);
+    for (int j = 0; j < ext; ++j)
+      bulk_g2s(ws + j * Wc, w2 + (int64_t)j * s.ldw2 + col0, wb, &bar);
+  }
+  const bool ok = mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
+  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  MMC r = mmc_empty();
+  if (ok) {
+    float2 acc[4][C];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[i][c] = make_float2(0.f, 0.f);
+    for (int j = 0; j < ext; ++j) {
+      float2 xv[4], wv[C];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xv[i] = xs[(ty * 4 + i) * ext + j];
+#pragma unroll
+      for (int c = 0; c < C; ++c) wv[c] = ws[j * Wc + tx + 32 * c];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[i][c] = cmac(acc[i][c], xv[i], wv[c]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t line = line0 + ty * 4 + i;
+      if (line >= s.nlines) continue;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int x = col0 + tx + 32 * c;
+        if (x >= n2) continue;
+        const float2 v = make_float2(acc[i][c].x * inv_n, acc[i][c].y * inv_n);
+        const int32_t idx = (int32_t)(line * n2 + x);
+        z[idx] = v;
+        const float a = cabs2(v);
+        if (image) image[idx] = a;
+        mmc_add(r, a, idx);
+      }
+    }
+  }
+  r = block_mmc(r, shm);
+  const unsigned int total = gridDim.x * gridDim.y;
+  if (threadIdx.x == 0) part[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = r;
+  if (!last_cta(&hdr->done[0], total, &last)) return;
+  MMC q = mmc_empty();
+  for (unsigned int b = threadIdx.x; b < total; b += blockDim.x) mmc_merge(q, mmc_load(part + b));
+  q = block_mmc(q, shm);
+  if (threadIdx.x == 0) {
+    hdr->mn = q.mn;
+    hdr->mx = q.mx;
+    hdr->imn = q.imn;
+    hdr->imx = q.imx;
+    hdr->cmn = q.cmn;
+    hdr->cmx = q.cmx;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient pass: per voxel of 32 lines the normalised image, the loss term and
+// g = dL/dz without the min / max terms (the same float arithmetic as
+// dm_image_loss), staged transposed in shared memory; then
+//   Q2[line][j] = sum_x2 g[line][x2] conj(W2[j][x2])
+// with warp w summing x2 in [w n2/8, (w+1) n2/8) for 4 lines x 2JC band offsets
+// per thread, and the eight warp partials added in warp order.  The conjugate
+// table arrives by a bulk copy while the voxels are processed.  Voxels go to the
+// warps in tiles of 4 lines x 8 positions (coalesced 64-byte row pieces), read
+// kAhead tiles ahead.  The transposed tile gT[x2][line] swaps groups of 4 lines
+// by x2 mod 8 and the partial sums swap 16-byte units by line, so neither the
+// stores nor the reads of either meet bank conflicts.  The last CTA forms the
+// loss and the min / max gradient per tied voxel.
+
+constexpr int kAhead = 8;  // voxel tiles per warp loaded before use
+
+__host__ __device__ inline int red_units(int ldj) {  // 16-byte units per partial-sum row
+  const int u = ldj / 2;
+  return u <= 8 ? 8 : 16;
+}
+
+size_t gradlines_smem(int n2, int ldj) {
+  const size_t a = (size_t)n2 * (kLines + ldj) * sizeof(float2);
+  const size_t b = (size_t)8 * kLines * red_units(ldj) * 16;
+  return std::max(a, b);
+}
+
+template <int JC>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bb_gradlines(BBShape s, const float2* __restrict__ z, const float* __restrict__ target,
+                   int kind, float contrast, BBHdr* hdr, const float2* __restrict__ w2t,
+                   float2* __restrict__ q2, LP* __restrict__ part, float* __restrict__ loss) {
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ double shl[3][kLineThreads / 32];
+  __shared__ LP shp[kLineThreads];
+  __shared__ int last;
+  const int n2 = s.n[2], ext = s.ext[2], ldj = s.ldj;
+  float2* gzt = sm;                // [n2][kLines], line groups swizzled by x2 mod 8
+  float2* wt = sm + n2 * kLines;   // [n2][ldj]
+  float4* red = reinterpret_cast<float4*>(sm);  // [8][kLines][RU] 16-byte units, after the contraction
+  const int RU = red_units(ldj);
+  const int64_t line0 = (int64_t)blockIdx.x * kLines;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t bytes = (uint32_t)((size_t)n2 * ldj * sizeof(float2));
+    mbar_expect_tx(&bar, bytes);
+    bulk_g2s(wt, w2t, bytes, &bar);
+  }
+  const float mn = hdr->mn, mx = hdr->mx;
+  const float rng = mx - mn;
+  const float inv = 1.0f / (rng * (1.0f + contrast));
+  const float nseg_inv = 1.0f / (float)s.nvox;
+  double L = 0.0, dmn = 0.0, dmx = 0.0;
+  // warp w: lines 4w..4w+3; lane = 8 li + xi: line 4w+li, position 8k+xi of tile k
+  const int li = lane >> 3, xi = lane & 7;
+  const int l = 4 * w + li;
+  const int64_t line = line0 + l;
+  const bool live_line = line < s.nlines;
+  const int ntile = (n2 + 7) / 8;
+  const int col = (l ^ (xi << 2));  // gT column of this lane's line (x2 mod 8 == xi)
+  for (int k0 = 0; k0 < ntile; k0 += kAhead) {
+    float2 zv[kAhead];
+    float tv[kAhead];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const int x = 8 * (k0 + u) + xi;
+      const bool live = live_line && x < n2;
+      const int64_t i = line * n2 + x;
+      zv[u] = live ? z[i] : make_float2(0.f, 0.f);
+      tv[u] = (live && kind != 0) ? target[i] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const int x = 8 * (k0 + u) + xi;
+      if (x >= n2) continue;
+      float2 g = make_float2(0.f, 0.f);
+      if (live_line) {
+        const float2 zi = zv[u];
+        const float a = cabs2(zi);
+        const float uu = (a - mn) / rng;
+        const float nv = (uu + contrast) / (1.0f + contrast);
+        float gn;
+        if (kind == 0) {
+          L += nv;
+          gn = 1.0f;
+        } else {
+          const float dlt = nv - tv[u];
+          L += (double)dlt * dlt;
+          gn = 2.0f * dlt * nseg_inv;
+        }
+        dmn += (double)gn * (-(1.0 - (double)uu));
+        dmx += (double)gn * (-(double)uu);
+        const float gg = gn * inv;
+        const float sc = a > 0.f ? gg / a : 0.f;
+        g = make_float2(sc * zi.x, sc * zi.y);
+      }
+      gzt[x * kLines + col] = g;
+    }
+  }
+  const bool ok = mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
+  __syncthreads();
+  const int lg = lane & 7, jg = lane >> 3;
+  float2 acc[4][JC][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
+  const int xb = w * n2 / 8, xe = ok ? (w + 1) * n2 / 8 : xb;
+  for (int x = xb; x < xe; ++x) {
+    const float2* row = gzt + x * kLines + 4 * (lg ^ (x & 7));  // lines 4lg..4lg+3
+    const float4 g01 = *reinterpret_cast<const float4*>(row);
+    const float4 g23 = *reinterpret_cast<const float4*>(row + 2);
+    const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
+                          make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
+#pragma unroll
+    for (int c = 0; c < JC; ++c) {
+      const float4 wv = *reinterpret_cast<const float4*>(&wt[x * ldj + c * 8 + jg * 2]);
+      const float2 w0 = make_float2(wv.x, wv.y), w1 = make_float2(wv.z, wv.w);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc[i][c][0] = cmac(acc[i][c][0], gv[i], w0);
+        acc[i][c][1] = cmac(acc[i][c][1], gv[i], w1);
+      }
+    }
+  }
+  __syncthreads();
+  // partial sums: row (warp, line), 16-byte unit (c*4 + jg) ^ (line >> 2)
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int ln = lg * 4 + i;
+#pragma unroll
+    for (int c = 0; c < JC; ++c)
+      red[(w * kLines + ln) * RU + ((c * 4 + jg) ^ lg)] =
+          make_float4(acc[i][c][0].x, acc[i][c][0].y, acc[i][c][1].x, acc[i][c][1].y);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kLines * ext; e += kLineThreads) {
+    const int ln = e / ext, j = e - ln * ext;
+    const int64_t lq = line0 + ln;
+    if (lq >= s.nlines) continue;
+    const int unit = (j >> 1) ^ (ln >> 2);
+    const float* base = reinterpret_cast<const float*>(red) + 4 * unit + 2 * (j & 1);
+    float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float* p = base + 4 * (k * kLines + ln) * RU;
+      v.x += p[0];
+      v.y += p[1];
+    }
+    q2[lq * ext + j] = v;
+  }
+  // loss partials (fixed order)
+  double v[3] = {L, dmn, dmx};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double x = v[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) shl[k][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    LP r{0.0, 0.0, 0.0};
+    for (int k = 0; k < kLineThreads / 32; ++k) {
+      r.loss += shl[0][k];
+      r.dmn += shl[1][k];
+      r.dmx += shl[2][k];
+    }
+    part[blockIdx.x] = r;
+  }
+  if (!last_cta(&hdr->done[1], gridDim.x, &last)) return;
+  LP r{0.0, 0.0, 0.0};
+  for (unsigned int k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    r.loss += __ldcg(&part[k].loss);
+    r.dmn += __ldcg(&part[k].dmn);
+    r.dmx += __ldcg(&part[k].dmx);
+  }
+  shp[threadIdx.x] = r;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      shp[threadIdx.x].loss += shp[threadIdx.x + o].loss;
+      shp[threadIdx.x].dmn += shp[threadIdx.x + o].dmn;
+      shp[threadIdx.x].dmx += shp[threadIdx.x + o].dmx;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const LP q = shp[0];
+    const double drng = (double)hdr->mx - (double)hdr->mn;
+    const double dinv = 1.0 / (drng * (1.0 + contrast));
+    const double f0 = kind == 0 ? q.loss : q.loss / (double)s.nvox;
+    const double f1 = q.dmn * dinv, f2 = q.dmx * dinv;
+    hdr->fin[0] = f0;
+    hdr->fin[1] = f1;
+    hdr->fin[2] = f2;
+    hdr->add_mn = hdr->cmn > 0 ? (float)(f1 / (double)hdr->cmn) : 0.f;
+    hdr->add_mx = hdr->cmx > 0 ? (float)(f2 / (double)hdr->cmx) : 0.f;
+    hdr->ties_full = (hdr->cmn >= 2 || hdr->cmx >= 2) ? 1 : 0;
+    if (loss) loss[0] = (float)f0;
+  }
+}
+
+// Several voxels at the min (max): add their share of the min (max) gradient to
+// the line contractions, one thread per line in x2 order.  Returns at once in the
+// usual case of a single voxel (added in the gather instead).
+__global__ void k_bb_ties(BBShape s, const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
+                          const float2* __restrict__ w2t, float2* __restrict__ q2) {
+  if (!hdr->ties_full) return;
+  const int64_t line = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= s.nlines) return;
+  const bool t0 = hdr->cmn >= 2, t1 = hdr->cmx >= 2;
+  const float mn = hdr->mn, mx = hdr->mx, a0 = hdr->add_mn, a1 = hdr->add_mx;
+  const int n2 = s.n[2], ext = s.ext[2];
+  for (int x = 0; x < n2; ++x) {
+    const float2 zi = z[line * n2 + x];
+    const float a = cabs2(zi);
+    const bool h0 = t0 && a == mn, h1 = t1 && a == mx;
+    if (!(h0 || h1) || !(a > 0.f)) continue;
+    for (int k = 0; k < 2; ++k) {
+      if (!(k == 0 ? h0 : h1)) continue;
+      const float sc = (k == 0 ? a0 : a1) / a;
+      const float2 v = make_float2(sc * zi.x, sc * zi.y);
+      for (int j = 0; j < ext; ++j)
+        q2[line * ext + j] = cmac(q2[line * ext + j], v, w2t[(int64_t)x * s.ldj + j]);
+    }
+  }
+}
+
+// G at the band voxels: the K-split partials of the axis-0 contraction G0[j0][j1][j2]
+// added in order, plus the min / max gradient of a single extreme voxel.
+__global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t nb,
+                            const float2* __restrict__ g0p, const float2* __restrict__ w0,
+                            const float2* __restrict__ w1, const float2* __restrict__ w2,
+                            const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
+                            float2* __restrict__ grad_list) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nb) return;
+  int32_t idx = band[m];
+  if (idx < 0 || (int64_t)idx >= s.nvox) idx = 0;  // reported by the scatter
+  const int32_t n12 = s.n[1] * s.n[2];
+  const int32_t k0 = idx / n12, rem = idx - k0 * n12;
+  const int32_t k1 = rem / s.n[2], k2 = rem - k1 * s.n[2];
+  const int32_t j0 = min(max(k0 - s.lo[0], 0), s.ext[0] - 1);
+  const int32_t j1 = min(max(k1 - s.lo[1], 0), s.ext[1] - 1);
+  const int32_t j2 = min(max(k2 - s.lo[2], 0), s.ext[2] - 1);
+  const int64_t box = (int64_t)s.ext[0] * s.ext[1] * s.ext[2];
+  const float2* p = g0p + ((int64_t)j0 * s.ext[1] + j1) * s.ext[2] + j2;
+  float2 g = p[0];
+  for (int kp = 1; kp < s.g0split; ++kp) {
+    const float2 q = p[kp * box];
+    g.x += q.x;
+    g.y += q.y;
+  }
+  if (!hdr->ties_full) {
+    for (int k = 0; k < 2; ++k) {
+      const int64_t c = k == 0 ? hdr->cmn : hdr->cmx;
+      if (c != 1) continue;
+      const int64_t i = k == 0 ? hdr->imn : hdr->imx;
+      const float2 zi = z[i];
+      const float a = cabs2(zi);
+      const float sc = a > 0.f ? (k == 0 ? hdr->add_mn : hdr->add_mx) / a : 0.f;
+      const float2 v = make_float2(sc * zi.x, sc * zi.y);
+      const int64_t nn12 = (int64_t)s.n[1] * s.n[2];
+      const int x0 = (int)(i / nn12), x1 = (int)((i / s.n[2]) % s.n[1]), x2 = (int)(i % s.n[2]);
+      float2 e = cmulf(cmulf(w0[(int64_t)j0 * s.n[0] + x0], w1[(int64_t)j1 * s.n[1] + x1]),
+                       w2[(int64_t)j2 * s.ldw2 + x2]);
+      e.y = -e.y;
+      g = cmac(g, v, e);
+    }
+  }
+  grad_list[m] = g;
+}
+
+// Band bounding box: per axis the smallest and largest index of the band
+// (integer atomics: order-independent).
+__global__ void k_bb_bounds(const int32_t* __restrict__ band, int64_t nb, int32_t n1, int32_t n2,
+                            int32_t* __restrict__ out) {
+  int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {-1, -1, -1};
+  for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < nb;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t idx = band[m];
+    if (idx < 0) continue;
+    const int32_t n12 = n1 * n2;
+    const int32_t k[3] = {idx / n12, (idx / n2) % n1, idx % n2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = min(lo[d], k[d]);
+      hi[d] = max(hi[d], k[d]);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = min(lo[d], __shfl_down_sync(0xffffffffu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_down_sync(0xffffffffu, hi[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&out[d], lo[d]);
+      atomicMax(&out[3 + d], hi[d]);
+    }
+  }
+}
+
+__global__ void k_bb_bounds_init(int32_t* out) {
+  if (threadIdx.x < 3) {
+    out[threadIdx.x] = INT32_MAX;
+    out[3 + threadIdx.x] = -1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Workspace layout.
+
+size_t up256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct BBWs {
+  BBHdr* hdr;
+  float2 *w0, *w1, *w2, *w2t;
+  float2 *t0, *t1, *t2;  // band box, after axis 0, after axis 1 (Q2 reuses t2)
+  float2* q1p;           // K-split partials of the axis-1 forward contraction
+  float2* g0p;           // K-split partials of the axis-0 forward contraction (band box)
+  float2* z;
+  MMC* mm;
+  LP* lp;
+};
+
+int z_col_chunk(int n2) { return std::min(8, (n2 + 31) / 32); }
+
+size_t bb_layout(const BBShape& s, char* base, BBWs* w) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char* {
+    char* p = base ? base + off : nullptr;
+    off += up256(std::max<size_t>(bytes, 1) + 16);  // 16 bytes of slack: rounded bulk copies
+    return p;
+  };
+  const size_t c8 = sizeof(float2);
+  const int64_t e0 = s.ext[0], e1 = s.ext[1], e2 = s.ext[2];
+  const int64_t nlb = (s.nlines + kLines - 1) / kLines;
+  const int64_t cb = s.ldw2 / (32 * s.zc);
+  BBWs r;
+  r.hdr = (BBHdr*)take(sizeof(BBHdr));
+  r.w0 = (float2*)take(c8 * e0 * s.n[0]);
+  r.w1 = (float2*)take(c8 * e1 * s.n[1]);
+  r.w2 = (float2*)take(c8 * e2 * s.ldw2);
+  r.w2t = (float2*)take(c8 * (size_t)s.n[2] * s.ldj);
+  r.t0 = (float2*)take(c8 * e0 * e1 * e2);
+  r.t1 = (float2*)take(c8 * (size_t)s.n[0] * e1 * e2);
+  r.t2 = (float2*)take(c8 * (size_t)s.nlines * e2);
+  r.q1p = (float2*)take(c8 * (size_t)s.q1split * s.n[0] * e1 * e2);
+  r.g0p = (float2*)take(c8 * (size_t)s.g0split * e0 * e1 * e2);
+  r.z = (float2*)take(c8 * (size_t)s.nvox);
+  r.mm = (MMC*)take(sizeof(MMC) * (size_t)(nlb * cb));
+  r.lp = (LP*)take(sizeof(LP) * (size_t)nlb);
+  if (w) *w = r;
+  return off;
+}
+
+// K split of a forward contraction over n positions: (chunk, splits), chunk a
+// multiple of 16.
+void ksplit(int n, int& chunk, int& splits) {
+  const int want = std::max(1, std::min(8, n / 48));
+  chunk = ((n + want - 1) / want + 15) / 16 * 16;
+  splits = (n + chunk - 1) / chunk;
+}
+
+bool make_shape(const int32_t n[3], const int32_t lo[3], const int32_t ext[3], BBShape& s) {
+  for (int d = 0; d < 3; ++d) {
+    if (n[d] <= 0 || ext[d] <= 0 || lo[d] < 0 || (int64_t)lo[d] + ext[d] > n[d]) return false;
+    s.n[d] = n[d];
+    s.lo[d] = lo[d];
+    s.ext[d] = ext[d];
+  }
+  s.ldj = (ext[2] + 7) / 8 * 8;
+  s.zc = z_col_chunk(n[2]);
+  s.ldw2 = (n[2] + 32 * s.zc - 1) / (32 * s.zc) * (32 * s.zc);
+  ksplit(n[1], s.q1chunk, s.q1split);
+  ksplit(n[0], s.g0chunk, s.g0split);
+  s.nlines = (int64_t)n[0] * n[1];
+  s.nvox = s.nlines * n[2];
+  return s.nvox <= (int64_t)INT32_MAX && (int64_t)n[0] * s.q1split <= 65535 &&
+         s.nlines / kLines < (int64_t)INT32_MAX;
+}
+
+template <bool kInv>
+void gemm(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X, int64_t sxb,
+          int64_t sxk, int xparts, int64_t sxp, float2* C, int64_t scb, int64_t scm,
+          int64_t scp, int batch, cudaStream_t st) {
+  const int splits = (K + kc - 1) / kc;
+  dim3 grid((N + 31) / 32, (M + 63) / 64, batch * splits);
+  k_bb_gemm<kInv><<<grid, kGemmThreads, 0, st>>>(W, ldw, M, N, K, batch, kc, X, sxb, sxk,
+                                                  xparts, sxp, C, scb, scm, scp);
+}
+
+
+// Raises a kernel's dynamic shared-memory limit to kSmemLimit, once per device
+// (a host-side attribute, set on the first call, before any stream capture).
+template <typename Kern>
+cudaError_t smem_limit_once(Kern k, bool* done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  return e;
+}
+
+template <int C>
+cudaError_t zlines(const BBShape& s, const BBWs& w, float inv_n, float* image, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * ((size_t)kLines * s.ext[2] + (size_t)s.ext[2] * 32 * C);
+  auto k = k_bb_zlines<C>;
+  static bool done[64] = {};
+  cudaError_t e = smem_limit_once(k, done);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((s.nlines + kLines - 1) / kLines), s.ldw2 / (32 * C));
+  k<<<grid, kLineThreads, smem, st>>>(s, w.t2, w.w2, inv_n, w.z, image, w.mm, w.hdr);
+  return cudaGetLastError();
+}
+
+template <int JC>
+cudaError_t gradlines(const BBShape& s, const BBWs& w, int kind, const float* target,
+                      float contrast, float* loss, cudaStream_t st) {
+  const size_t smem = gradlines_smem(s.n[2], s.ldj);
+  auto k = k_bb_gradlines<JC>;
+  static bool done[64] = {};
+  cudaError_t e = smem_limit_once(k, done);
+  if (e != cudaSuccess) return e;
+  const unsigned nlb = (unsigned)((s.nlines + kLines - 1) / kLines);
+  k<<<nlb, kLineThreads, smem, st>>>(s, w.z, target, kind, contrast, w.hdr, w.w2t, w.t2, w.lp,
+                                     loss);
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace dm
+
+using namespace dm;
+
+extern "C" {
+
+int dm_band_bounds(const int32_t* band_index, int64_t n_band, const dm_box* box,
+                   int32_t* bounds, dm_stream_t stream) {
+  if (!box || !bounds || n_band < 0 || (n_band > 0 && !band_index)) return DM_ERR_INVALID_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (box->shape[d] <= 0) return DM_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_bb_bounds_init<<<1, 32, 0, st>>>(bounds);
+  if (n_band > 0) {
+    const int64_t nb = std::min<int64_t>((n_band + 255) / 256, 1024);
+    k_bb_bounds<<<(unsigned)nb, 256, 0, st>>>(band_index, n_band, box->shape[1], box->shape[2],
+                                              bounds);
+  }
+  count_launches(n_band > 0 ? 2 : 1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+size_t dm_render_loss_bandbox_workspace_size(const dm_box* box, const int32_t bounds[6]) {
+  if (!box || !bounds) return 0;
+  int32_t lo[3], ext[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = bounds[d];
+    ext[d] = bounds[3 + d] - bounds[d] + 1;
+  }
+  BBShape s;
+  if (!make_shape(box->shape, lo, ext, s)) return 0;
+  return bb_layout(s, nullptr, nullptr);
+}
+
+int dm_render_loss_bandbox_supported(const dm_box* box, const int32_t bounds[6]) {
+  if (!box || !bounds) return 0;
+  int32_t lo[3], ext[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = bounds[d];
+    ext[d] = bounds[3 + d] - bounds[d] + 1;
+  }
+  BBShape s;
+  if (!make_shape(box->shape, lo, ext, s)) return 0;
+  if (s.ext[2] > kMaxExt2) return 0;
+  if (gradlines_smem(s.n[2], s.ldj) > (size_t)kSmemLimit) return 0;
+  return 1;
+}
+
+int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int64_t n_band,
+                           const dm_box* box, const int32_t bounds[6], const float* otf,
+                           int kind, const float* target, float contrast, float* loss,
+                           float* grad_list, float* image, void* workspace, size_t ws_bytes,
+                           dm_stream_t stream) {
+  if (!box || !bounds || !workspace || !loss || n_band <= 0 || !band_index || !ft_list)
+    return DM_ERR_INVALID_ARG;
+  if ((kind != 0 && kind != 1) || (kind == 1 && !target)) return DM_ERR_INVALID_ARG;
+  if (!dm_render_loss_bandbox_supported(box, bounds)) return DM_ERR_UNSUPPORTED;
+  if (n_band > (int64_t)INT32_MAX) return DM_ERR_SIZE;
+  const size_t need = dm_render_loss_bandbox_workspace_size(box, bounds);
+  if (need == 0) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < need) return DM_ERR_WORKSPACE;
+  int32_t lo[3], ext[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = bounds[d];
+    ext[d] = bounds[3 + d] - bounds[d] + 1;
+  }
+  BBShape s;
+  make_shape(box->shape, lo, ext, s);
+  BBWs w;
+  bb_layout(s, (char*)workspace, &w);
+  cudaStream_t st = (cudaStream_t)stream;
+  int launches = 0;
+  cudaError_t e = cudaSuccess;
+  {
+    const int64_t tot = (int64_t)s.ext[0] * s.n[0] + (int64_t)s.ext[1] * s.n[1] +
+                        (int64_t)s.ext[2] * s.ldw2 + (int64_t)s.n[2] * s.ldj;
+    const unsigned nb = (unsigned)std::min<int64_t>((tot + 255) / 256, 1024);
+    k_bb_tables<<<nb, 256, 0, st>>>(s, w.w0, w.w1, w.w2, w.w2t, w.hdr);
+    ++launches;
+  }
+  if (cudaMemsetAsync(w.t0, 0, sizeof(float2) * (size_t)s.ext[0] * s.ext[1] * s.ext[2], st) !=
+      cudaSuccess)
+    return DM_ERR_CUDA;
+  k_bb_scatter<<<(unsigned)((n_band + 255) / 256), 256, 0, st>>>(
+      s, band_index, n_band, (const float2*)ft_list, otf, w.t0, &w.hdr->err);
+  ++launches;
+  const int64_t e12 = (int64_t)s.ext[1] * s.ext[2];
+  // axis 0: T1[x0][j1 j2] = sum_j0 W0[j0][x0] T0[j0][j1 j2]
+  gemm<true>(w.w0, s.n[0], s.n[0], (int)e12, s.ext[0], s.ext[0], w.t0, 0, e12, 1, 0, w.t1, 0,
+             e12, 0, 1, st);
+  // axis 1: T2[x0][x1][j2] = sum_j1 W1[j1][x1] T1[x0][j1][j2]
+  gemm<true>(w.w1, s.n[1], s.n[1], s.ext[2], s.ext[1], s.ext[1], w.t1, e12, s.ext[2], 1, 0,
+             w.t2, (int64_t)s.n[1] * s.ext[2], s.ext[2], 0, s.n[0], st);
+  launches += 2;
+  const float inv_n = (float)(1.0 / (double)s.nvox);
+  switch (s.zc) {
+    case 1: e = zlines<1>(s, w, inv_n, image, st); break;
+    case 2: e = zlines<2>(s, w, inv_n, image, st); break;
+    case 3: e = zlines<3>(s, w, inv_n, image, st); break;
+    case 4: e = zlines<4>(s, w, inv_n, image, st); break;
+    case 5: e = zlines<5>(s, w, inv_n, image, st); break;
+    case 6: e = zlines<6>(s, w, inv_n, image, st); break;
+    case 7: e = zlines<7>(s, w, inv_n, image, st); break;
+    default: e = zlines<8>(s, w, inv_n, image, st); break;
+  }
+  if (e != cudaSuccess) return DM_ERR_CUDA;
+  switch (s.ldj / 8) {
+    case 1: e = gradlines<1>(s, w, kind, target, contrast, loss, st); break;
+    case 2: e = gradlines<2>(s, w, kind, target, contrast, loss, st); break;
+    case 3: e = gradlines<3>(s, w, kind, target, contrast, loss, st); break;
+    default: e = gradlines<4>(s, w, kind, target, contrast, loss, st); break;
+  }
+  if (e != cudaSuccess) return DM_ERR_CUDA;
+  launches += 2;
+  if (grad_list) {
+    k_bb_ties<<<(unsigned)((s.nlines + 127) / 128), 128, 0, st>>>(s, w.z, w.hdr, w.w2t, w.t2);
+    // axis 1 (forward): Q1[kp][x0][j1][j2] = sum_{x1 in split kp} conj(W1[j1][x1]) Q2[x0][x1][j2]
+    gemm<false>(w.w1, s.n[1], s.ext[1], s.ext[2], s.n[1], s.q1chunk, w.t2,
+                (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, w.q1p, e12, s.ext[2],
+                (int64_t)s.n[0] * e12, s.n[0], st);
+    // axis 0 (forward): G0[kp][j0][j1 j2] = sum_{x0 in split kp} conj(W0[j0][x0]) sum_q Q1[q][x0][j1 j2]
+    gemm<false>(w.w0, s.n[0], s.ext[0], (int)e12, s.n[0], s.g0chunk, w.q1p, 0, e12,
+                s.q1split, (int64_t)s.n[0] * e12, w.g0p, 0, e12,
+                (int64_t)s.ext[0] * e12, 1, st);
+    k_bb_gather<<<(unsigned)((n_band + 255) / 256), 256, 0, st>>>(
+        s, band_index, n_band, w.g0p, w.w0, w.w1, w.w2, w.z, w.hdr, (float2*)grad_list);
+    launches += 4;
+  }
+  count_launches(launches);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+}  // extern "C"

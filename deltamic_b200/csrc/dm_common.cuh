@@ -132,6 +132,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait: gives up after ``kWaitLimit`` polls, records DM_ERR_TIMEOUT and
 // returns false so the kernel can leave instead of hanging the GPU.
+// try_wait with a suspend-time hint: the thread may sleep up to ``ns`` nanoseconds
+// for the phase to complete instead of spinning on issue slots.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded sleeping wait for a copy issued just before: at most kSleepTries tries
+// of up to kSleepNs each (about 1.3 s in all), then DM_ERR_TIMEOUT and false.
+constexpr uint32_t kSleepTries = 1u << 16;
+constexpr uint32_t kSleepNs = 20000;
+__device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t* bar, uint32_t parity,
+                                                        int* err) {
+  for (uint32_t i = 0; i < kSleepTries; ++i)
+    if (mbar_try_wait_sleep(bar, parity, kSleepNs)) return true;
+  set_error(err, DM_ERR_TIMEOUT);
+  return false;
+}
+
 constexpr uint32_t kWaitLimit = 1u << 22;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
   for (uint32_t i = 0; i < kWaitLimit; ++i)

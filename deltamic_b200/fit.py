@@ -49,16 +49,22 @@ class FitStep:
 
     def _body(self):
         r = self.r
-        ft = ops.meshft_list(self.V, self.F, self.C, r.grid, r.band, otf=r.otf,
-                             spectrum=r.spec)
-        torch.fft.ifftn(r.spec, out=r.z)
-        loss, _, gz = ops.image_loss(r.z, self.kind, self.target, self.contrast,
-                                     want_grad=True)
+        if r.use_bandbox:
+            ft = ops.meshft_list(self.V, self.F, self.C, r.grid, r.band)
+            loss, G = r.render_loss(ft, self.kind, self.target, self.contrast)
+            cot = dict(grad_list=G)
+        else:
+            ft = ops.meshft_list(self.V, self.F, self.C, r.grid, r.band, otf=r.otf,
+                                 spectrum=r.spec)
+            torch.fft.ifftn(r.spec, out=r.z)
+            loss, _, gz = ops.image_loss(r.z, self.kind, self.target, self.contrast,
+                                         want_grad=True)
+            torch.fft.fftn(gz, out=r.G)
+            cot = dict(grad_grid=r.G)
         self.loss.copy_(loss)
-        torch.fft.fftn(gz, out=r.G)
         gv, _, _ = ops.meshft_backward_list(self.V, self.F, self.C, r.grid, r.band, ft,
-                                            grad_grid=r.G, otf=r.otf, scale=1.0 / r.numel,
-                                            want_coeff=False)
+                                            otf=r.otf, scale=1.0 / r.numel, want_coeff=False,
+                                            **cot)
         self.grad.copy_(gv)
         ops.adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0],
                       self.betas[1], self.eps)

@@ -295,6 +295,66 @@ def image_loss(z, kind="sum", target=None, contrast=0.0, want_grad=True, want_im
     return loss, img, gz
 
 
+def band_bounds(band: torch.Tensor, grid: FreqGrid) -> tuple:
+    """(lo0, lo1, lo2, hi0, hi1, hi2): per-axis smallest and largest voxel index of
+    the band (synchronises to read them)."""
+    N.require_cuda(band, "band", torch.int32)
+    out = torch.empty(6, dtype=torch.int32, device=band.device)
+    N.check(N.lib().dm_band_bounds(N.ptr(band), band.numel(), ctypes.byref(grid.cbox),
+                                   N.ptr(out), N.stream_ptr(band.device)), "dm_band_bounds")
+    return tuple(int(v) for v in out.cpu().tolist())
+
+
+class BandBox:
+    """Plan of the band-box render of ``band`` on ``grid``: the band's bounding box
+    (host copy) and whether the library serves it."""
+
+    def __init__(self, grid: FreqGrid, band: torch.Tensor):
+        self.grid = grid
+        self.bounds_tuple = band_bounds(band, grid) if band.numel() else (0, 0, 0, -1, -1, -1)
+        self.bounds = (ctypes.c_int32 * 6)(*self.bounds_tuple)
+        self.box = band_box(grid, band)
+        lib = N.lib()
+        self.supported = band.numel() > 0 and bool(
+            lib.dm_render_loss_bandbox_supported(ctypes.byref(self.box), self.bounds))
+        self.ws_bytes = (int(lib.dm_render_loss_bandbox_workspace_size(ctypes.byref(self.box),
+                                                                       self.bounds))
+                         if self.supported else 0)
+
+    @property
+    def extent(self) -> tuple:
+        b = self.bounds_tuple
+        return tuple(b[3 + d] - b[d] + 1 for d in range(3))
+
+
+def render_loss_bandbox(ft, band, plan: BandBox, otf, kind="sum", target=None, contrast=0.0,
+                        want_grad=True, want_image=False):
+    """(loss[1], image | None, G | None) for S = ft * otf on the band: the loss of
+    normalize(|ifftn(S)|) as image_loss computes it, and G = fftn(dL/dz) on the band
+    (the grad_list of meshft_backward_list with otf and scale = 1/numel)."""
+    lib = N.lib()
+    if not plan.supported:
+        raise N.DeltaMicError(N.DM_ERR_UNSUPPORTED, "render_loss_bandbox")
+    N.require_cuda(ft, "ft", torch.complex64)
+    N.require_cuda(otf, "OTF", torch.float32)
+    k = LOSS_KINDS[kind]
+    n = plan.grid.numel
+    if k == 1:
+        N.require_cuda(target, "target", torch.float32)
+        if target.numel() != n:
+            raise ValueError("target must have the image's shape")
+    dev = ft.device
+    loss = torch.empty(1, dtype=torch.float32, device=dev)
+    G = torch.empty_like(ft) if want_grad else None
+    img = torch.empty(plan.grid.shape, dtype=torch.float32, device=dev) if want_image else None
+    ws = N.WORKSPACES.get("bandbox", plan.ws_bytes, dev)
+    N.check(lib.dm_render_loss_bandbox(
+        N.ptr(ft), N.ptr(band), band.numel(), ctypes.byref(plan.box), plan.bounds, N.ptr(otf), k,
+        N.ptr(target), float(contrast), N.ptr(loss), N.ptr(G), N.ptr(img), N.ptr(ws), ws.numel(),
+        N.stream_ptr(dev)), "dm_render_loss_bandbox")
+    return loss, img, G
+
+
 def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
     lib = N.lib()
     N.check(lib.dm_adam_step(N.ptr(param), N.ptr(grad), N.ptr(exp_avg), N.ptr(exp_avg_sq),

@@ -1,6 +1,11 @@
-"""Fused render-and-loss path: meshFT (with the OTF multiply in its epilogue) ->
-inverse FFT (cuFFT) -> |.| / normalize_tensor / loss and dL/dz in one pass ->
-forward FFT of dL/dz -> meshFT adjoint.
+"""Fused render-and-loss path: meshFT -> ifftn of ft * OTF -> |.| / normalize_tensor
+/ loss and dL/dz -> fftn of dL/dz on the band -> meshFT adjoint.
+
+Two implementations of the middle part, both on the GPU: the band-box render
+(``ops.render_loss_bandbox``: separable DFTs pruned to the band's bounding box,
+fused with the image loss; the default wherever the library serves the box) and
+the dense one (the OTF multiply in the meshFT epilogue, cuFFT on the whole grid,
+the fused image-loss kernels, cuFFT again).
 
 This is the chain ``normalize_tensor(render_image_from_ftmesh(meshFT(V,F,c), OTF))``
 of the reference fitting loop (``Examples/Gradient_Descent.ipynb`` cell 2) with
@@ -20,7 +25,7 @@ class MeshRenderer:
     """Renderer for one box: holds the frequency grid, the OTF and its narrow band."""
 
     def __init__(self, box_size, box_shape, narrowband_thresh=1e-5, device="cuda",
-                 autotune=True):
+                 autotune=True, render_path="auto"):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("MeshRenderer runs on CUDA devices only")
@@ -37,6 +42,10 @@ class MeshRenderer:
         self._sigma_key = None
         self.autotune = autotune
         self.variants = None
+        if render_path not in ("auto", "bandbox", "dense"):
+            raise ValueError("render_path must be 'auto', 'bandbox' or 'dense'")
+        self.render_path = render_path
+        self.bbox = None
 
     @property
     def numel(self) -> int:
@@ -50,6 +59,10 @@ class MeshRenderer:
         self.spec.zero_()
         self._sigma_key = None
         self.variants = None
+        self.bbox = ops.BandBox(self.grid, self.band)
+        if self.render_path == "bandbox" and not self.bbox.supported:
+            raise RuntimeError(f"band box extent {self.bbox.extent} is not served by the "
+                               "band-box render (axis-2 extent above 32 or tiles too large)")
 
     def set_sigma(self, sigma: torch.Tensor) -> None:
         """Gaussian OTF of ``sigma`` (psf.py:15-20) and its narrow band."""
@@ -61,6 +74,20 @@ class MeshRenderer:
             otf = ops.gaussian_otf(s, *self.xi)
         self.set_otf(otf)
         self._sigma_key = key
+
+    @property
+    def use_bandbox(self) -> bool:
+        """True when the render + loss go through the band-box kernels."""
+        return (self.render_path != "dense" and self.bbox is not None
+                and self.bbox.supported)
+
+    def render_loss(self, ft, kind, target, contrast):
+        """(loss[1], G) from the band's meshFT ``ft``: the loss of the normalised render
+        and G = fftn(dL/dz) on the band, the cotangent of meshft_backward_list
+        (grad_list with otf and scale = 1/numel)."""
+        loss, _, G = ops.render_loss_bandbox(ft, self.band, self.bbox, self.otf, kind, target,
+                                             contrast, want_grad=True)
+        return loss, G
 
     @property
     def n_band(self) -> int:
@@ -114,22 +141,31 @@ class MeshRenderer:
 class _RenderLoss(torch.autograd.Function):
     @staticmethod
     def forward(ctx, verts, coeff, sigma, r: MeshRenderer, faces, kind, target, contrast):
-        ft = ops.meshft_list(verts, faces, coeff, r.grid, r.band, otf=r.otf, spectrum=r.spec)
-        torch.fft.ifftn(r.spec, out=r.z)
-        loss, _, gz = ops.image_loss(r.z, kind, target, contrast, want_grad=True)
-        ctx.save_for_backward(verts, coeff, faces, ft, gz)
+        ctx.bandbox = r.use_bandbox
+        if ctx.bandbox:
+            ft = ops.meshft_list(verts, faces, coeff, r.grid, r.band)
+            loss, g = r.render_loss(ft, kind, target, contrast)
+        else:
+            ft = ops.meshft_list(verts, faces, coeff, r.grid, r.band, otf=r.otf, spectrum=r.spec)
+            torch.fft.ifftn(r.spec, out=r.z)
+            loss, _, g = ops.image_loss(r.z, kind, target, contrast, want_grad=True)
+        ctx.save_for_backward(verts, coeff, faces, ft, g)
         ctx.r = r
         ctx.sigma_grad = sigma.numel() == 9 and ctx.needs_input_grad[2]
         return loss.view(())
 
     @staticmethod
     def backward(ctx, gl):
-        verts, coeff, faces, ft, gz = ctx.saved_tensors
+        verts, coeff, faces, ft, g = ctx.saved_tensors
         r = ctx.r
-        torch.fft.fftn(gz, out=r.G)
+        if ctx.bandbox:
+            cot = dict(grad_list=g)
+        else:
+            torch.fft.fftn(g, out=r.G)
+            cot = dict(grad_grid=r.G)
         gv, gc, go = ops.meshft_backward_list(
-            verts, faces, coeff, r.grid, r.band, ft, grad_grid=r.G, otf=r.otf,
-            scale=1.0 / r.numel, want_coeff=ctx.needs_input_grad[1], want_otf=ctx.sigma_grad)
+            verts, faces, coeff, r.grid, r.band, ft, otf=r.otf, scale=1.0 / r.numel,
+            want_coeff=ctx.needs_input_grad[1], want_otf=ctx.sigma_grad, **cot)
         gv = gv * gl
         if gc is not None:
             gc = gc * gl

@@ -229,6 +229,37 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
                   dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Band-box render: the chain render_image_from_ftmesh -> normalize_tensor ->
+ * loss of the reference fitting loop (render.py:177-180, render.py:5-6,
+ * Examples/Gradient_Descent.ipynb cell 2) and its backward to the spectrum,
+ * for a spectrum that is zero outside the narrow band.  Replaces the dense
+ * ifftn / image loss / fftn sequence (torch.fft on the dense grid of
+ * cuda_class.py:28-29) by separable DFTs pruned to the band's bounding box.
+ *
+ * dm_band_bounds writes bounds[6] (DEVICE int32) = per-axis smallest band index
+ * (lo0, lo1, lo2) then largest (hi0, hi1, hi2); the other calls take the same six
+ * numbers from HOST memory.  dm_render_loss_bandbox_supported says whether this
+ * build serves a box (band extent along axis 2 at most 32 and the line tiles
+ * within shared memory); otherwise the call returns DM_ERR_UNSUPPORTED and the
+ * dense path applies.
+ * dm_render_loss_bandbox takes ft_list[n_band] (complex64, the band's meshFT as
+ * dm_meshft_forward returns it) and the OTF, forms S = ft * OTF on the band and
+ * z = ifftn(S) over the whole box, then the loss of dm_image_loss (same kinds,
+ * contrast and min / max tie rule).  Writes *loss (DEVICE float), optionally
+ * image[n] = |z|, and, if grad_list is not NULL, grad_list[n_band] = fftn(dL/dz)
+ * at the band voxels (complex64): the cotangent dm_meshft_backward takes as
+ * grad_list with otf and grad_scale = 1/n.  Deterministic. */
+int dm_band_bounds(const int32_t* band_index, int64_t n_band, const dm_box* box,
+                   int32_t* bounds, dm_stream_t stream);
+int dm_render_loss_bandbox_supported(const dm_box* box, const int32_t bounds[6]);
+size_t dm_render_loss_bandbox_workspace_size(const dm_box* box, const int32_t bounds[6]);
+int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int64_t n_band,
+                           const dm_box* box, const int32_t bounds[6], const float* otf,
+                           int kind, const float* target, float contrast, float* loss,
+                           float* grad_list, float* image, void* workspace, size_t ws_bytes,
+                           dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * 3x3x3 stride-2 padding-1 3D convolution with bias and GELU, for the learned
  * initialiser's encoder (no counterpart in the reference).  Channels-last BF16
  * tensors (uint16 storage): x[B,D,H,W,Ci], w[Kp,Co] with row k = ((kd*3+kh)*3+kw)*Ci

@@ -46,7 +46,8 @@ def test_batch_matches_single_cells():
     fo = np.cumsum([0] + [len(c[1]) for c in cells])
     total = 0.0
     for i, (v, f, c, box, shape, sig) in enumerate(cells):
-        r = MeshRenderer(box, shape, 1e-5, DEV)
+        # the batch renders through cuFFT: compare with the single cell's dense path
+        r = MeshRenderer(box, shape, 1e-5, DEV, render_path="dense")
         r.set_sigma(torch.tensor(sig, dtype=torch.float32, device=DEV))
         assert r.n_band == br.band_sizes[i]
         Vi = torch.tensor(v, dtype=torch.float32, device=DEV, requires_grad=True)

@@ -79,3 +79,27 @@ def test_product_path_refuses_cpu():
     import deltamic_b200 as dm
     with pytest.raises(RuntimeError):
         dm.Fourier3dMesh(torch.tensor([[0.0, 1.0]] * 3), (8, 8, 8), device="cpu")
+
+
+def test_bandbox_render_host_checks(lib):
+    """Band boxes the line kernels do not serve are refused before any launch."""
+    from deltamic_b200 import _native as N
+    box = N.make_box([[0, 1], [0, 1], [0, 1]], (64, 64, 64))
+    wide = (ctypes.c_int32 * 6)(0, 0, 0, 63, 63, 63)  # axis-2 extent 64 > 32
+    narrow = (ctypes.c_int32 * 6)(10, 12, 20, 50, 52, 41)
+    outside = (ctypes.c_int32 * 6)(10, 12, 20, 50, 52, 64)
+    assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), wide) == 0
+    assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), narrow) == 1
+    assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), outside) == 0
+    assert lib.dm_render_loss_bandbox_workspace_size(ctypes.byref(box), narrow) > 64 ** 3 * 8
+    fake = ctypes.c_void_p(16)
+    st = lib.dm_render_loss_bandbox(fake, fake, 1, ctypes.byref(box), wide, None, 0, None, 0.0,
+                                    fake, None, None, fake, 1 << 30, None)
+    assert st == N.DM_ERR_UNSUPPORTED
+    # mse without a target, and a workspace below the query
+    assert lib.dm_render_loss_bandbox(fake, fake, 1, ctypes.byref(box), narrow, None, 1, None,
+                                      0.0, fake, None, None, fake, 1 << 30,
+                                      None) == N.DM_ERR_INVALID_ARG
+    assert lib.dm_render_loss_bandbox(fake, fake, 1, ctypes.byref(box), narrow, None, 0, None,
+                                      0.0, fake, None, None, fake, 1024,
+                                      None) == N.DM_ERR_WORKSPACE
