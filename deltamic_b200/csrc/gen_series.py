@@ -13,6 +13,11 @@ Im H = p3 Q1(p2) + p3^3 Q3(p2).  Terms up to n = NMAX are formed, then every
 monomial whose largest value over the series domain (largest phase difference
 D <= DMAX, so p2 <= 2 D^2/3 and |p3| <= 2 D^3/9) is below DROP is dropped.
 
+Two sets are written: DM_SERIES_* for the whole series domain (D <= 3.5) and
+DM_SERIES_LO_* for D <= 1.5, where fewer terms reach the same truncation error
+(the kernels pick the short set when every lane of a warp qualifies).  A part
+with no term left has length 0.
+
     python deltamic_b200/csrc/gen_series.py > deltamic_b200/csrc/series_coeffs.cuh
 """
 from fractions import Fraction
@@ -49,9 +54,10 @@ def series(nmax=NMAX):
     return re, im
 
 
-def poly(d, k):
+def poly(d, k, dmax=None):
     """Coefficients (ascending in p2) of the p3^k part, truncated by DROP."""
-    p2max, p3max = 2 * DMAX ** 2 / 3, 2 * DMAX ** 3 / 9
+    dmax = DMAX if dmax is None else dmax
+    p2max, p3max = 2 * dmax ** 2 / 3, 2 * dmax ** 3 / 9
     js = [j for (j, kk), c in d.items()
           if kk == k and abs(float(c)) * p2max ** j * p3max ** k >= DROP]
     if not js:
@@ -59,18 +65,22 @@ def poly(d, k):
     return [d.get((j, k), Fraction(0)) for j in range(max(js) + 1)]
 
 
+DMAX_LO = 1.5
+
+
 def main():
     re, im = series()
     print("// Generated by gen_series.py (do not edit): centroid-series coefficients,")
-    print(f"// terms n <= {NMAX}, monomials below {DROP:g} for D <= {DMAX} dropped.")
-    print("// Ascending powers of p2.")
+    print(f"// terms n <= {NMAX}, monomials below {DROP:g} dropped: DM_SERIES_* for")
+    print(f"// D <= {DMAX}, DM_SERIES_LO_* for D <= {DMAX_LO}.  Ascending powers of p2.")
     print("#pragma once")
-    for name, d, k in (("P0", re, 0), ("P2", re, 2), ("P4", re, 4), ("Q1", im, 1),
-                       ("Q3", im, 3)):
-        c = poly(d, k) or [Fraction(0)]
-        vals = ", ".join(f"{float(x):.9e}f" for x in c)
-        print(f"#define DM_SERIES_{name}_N {len(c)}")
-        print(f"#define DM_SERIES_{name} {{{vals}}}")
+    for tag, dmax in (("", DMAX), ("LO_", DMAX_LO)):
+        for name, d, k in (("P0", re, 0), ("P2", re, 2), ("P4", re, 4), ("Q1", im, 1),
+                           ("Q3", im, 3)):
+            c = poly(d, k, dmax)
+            vals = ", ".join(f"{float(x):.9e}f" for x in (c or [Fraction(0)]))
+            print(f"#define DM_SERIES_{tag}{name}_N {len(c)}")
+            print(f"#define DM_SERIES_{tag}{name} {{{vals}}}")
 
 
 if __name__ == "__main__":

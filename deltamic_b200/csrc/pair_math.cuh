@@ -52,8 +52,10 @@ namespace dm {
 // Seps/2: the reference compares |ab| <= sqrt(FLT_EPSILON); differences here are
 // held in half units.
 constexpr float kSepsHalf = 1.72633492e-4f;
-// Centroid series when the largest difference is below 3.5 (half units: 1.75).
+// Centroid series when the largest difference is below 3.5 (half units: 1.75);
+// its short coefficient set when it is at most 1.5 (half units: 0.75).
 constexpr float kSeriesHalf = 1.75f;
+constexpr float kSeriesLoHalf = 0.75f;
 // Polynomial sinc / sinc' below this half-angle magnitude.
 constexpr float kPolyX = 1.0f;
 constexpr float kTwoPi = 6.28318530717958647692f;
@@ -168,38 +170,83 @@ DM_HD void g_sinc(float hu, float hw, c32& G, c32& Gu, c32& Gw) {
 // ---------------------------------------------------------------------------
 // Centroid series: H(p2, p3) and its partials in p2 and p3.
 
+// First N coefficients of c (ascending) at x, and the derivative; N == 0 gives 0.
 template <int N>
-DM_HD void horner(const float (&c)[N], float x, float& v, float& dv) {
-  v = c[N - 1];
-  dv = 0.f;
+DM_HD void horner(const float* c, float x, float& v, float& dv) {
+  if constexpr (N == 0) {
+    v = 0.f;
+    dv = 0.f;
+  } else {
+    v = c[N - 1];
+    dv = 0.f;
 #pragma unroll
-  for (int k = N - 2; k >= 0; --k) {
-    dv = dv * x + v;
-    v = v * x + c[k];
+    for (int k = N - 2; k >= 0; --k) {
+      dv = dv * x + v;
+      v = v * x + c[k];
+    }
   }
 }
 
-template <bool kGrad>
-DM_HD void centroid_H(float p2, float p3, c32& H, c32& Hp2, c32& Hp3) {
-  constexpr float P0[DM_SERIES_P0_N] = DM_SERIES_P0;
-  constexpr float P2[DM_SERIES_P2_N] = DM_SERIES_P2;
-  constexpr float P4[DM_SERIES_P4_N] = DM_SERIES_P4;
-  constexpr float Q1[DM_SERIES_Q1_N] = DM_SERIES_Q1;
-  constexpr float Q3[DM_SERIES_Q3_N] = DM_SERIES_Q3;
+// H = P0 + p3^2 P2 + p3^4 P4 + i p3 (Q1 + p3^2 Q3) (polynomials in p2) and, if
+// kGrad, its partials in p2 and p3; parts of length 0 are left out.
+template <bool kGrad, int N0, int N2, int N4, int M1, int M3>
+DM_HD void centroid_H_set(const float* P0, const float* P2, const float* P4, const float* Q1,
+                          const float* Q3, float p2, float p3, c32& H, c32& Hp2, c32& Hp3) {
   float a0, a0d, a2, a2d, a4, a4d, b1, b1d, b3, b3d;
-  horner(P0, p2, a0, a0d);
-  horner(P2, p2, a2, a2d);
-  horner(P4, p2, a4, a4d);
-  horner(Q1, p2, b1, b1d);
-  horner(Q3, p2, b3, b3d);
+  horner<N0>(P0, p2, a0, a0d);
+  horner<N2>(P2, p2, a2, a2d);
+  horner<N4>(P4, p2, a4, a4d);
+  horner<M1>(Q1, p2, b1, b1d);
+  horner<M3>(Q3, p2, b3, b3d);
   const float q = p3 * p3;
-  H.x = a0 + q * (a2 + q * a4);
-  H.y = p3 * (b1 + q * b3);
+  if constexpr (N4 > 0) {
+    H.x = a0 + q * (a2 + q * a4);
+  } else {
+    H.x = a0 + q * a2;
+  }
+  if constexpr (M3 > 0) {
+    H.y = p3 * (b1 + q * b3);
+  } else {
+    H.y = p3 * b1;
+  }
   if (kGrad) {
-    Hp2.x = a0d + q * (a2d + q * a4d);
-    Hp2.y = p3 * (b1d + q * b3d);
-    Hp3.x = p3 * (2.0f * a2 + 4.0f * q * a4);
-    Hp3.y = b1 + 3.0f * q * b3;
+    if constexpr (N4 > 0) {
+      Hp2.x = a0d + q * (a2d + q * a4d);
+      Hp3.x = p3 * (2.0f * a2 + 4.0f * q * a4);
+    } else {
+      Hp2.x = a0d + q * a2d;
+      Hp3.x = p3 * (2.0f * a2);
+    }
+    if constexpr (M3 > 0) {
+      Hp2.y = p3 * (b1d + q * b3d);
+      Hp3.y = b1 + 3.0f * q * b3;
+    } else {
+      Hp2.y = p3 * b1d;
+      Hp3.y = b1;
+    }
+  }
+}
+
+// The whole series domain (kLo false: largest phase difference below 3.5), or the
+// short set for largest differences up to 1.5 (same truncation error there).
+template <bool kGrad, bool kLo = false>
+DM_HD void centroid_H(float p2, float p3, c32& H, c32& Hp2, c32& Hp3) {
+  if constexpr (kLo) {
+    constexpr float P0[] = DM_SERIES_LO_P0;
+    constexpr float P2[] = DM_SERIES_LO_P2;
+    constexpr float P4[] = DM_SERIES_LO_P4;
+    constexpr float Q1[] = DM_SERIES_LO_Q1;
+    constexpr float Q3[] = DM_SERIES_LO_Q3;
+    centroid_H_set<kGrad, DM_SERIES_LO_P0_N, DM_SERIES_LO_P2_N, DM_SERIES_LO_P4_N,
+                   DM_SERIES_LO_Q1_N, DM_SERIES_LO_Q3_N>(P0, P2, P4, Q1, Q3, p2, p3, H, Hp2, Hp3);
+  } else {
+    constexpr float P0[] = DM_SERIES_P0;
+    constexpr float P2[] = DM_SERIES_P2;
+    constexpr float P4[] = DM_SERIES_P4;
+    constexpr float Q1[] = DM_SERIES_Q1;
+    constexpr float Q3[] = DM_SERIES_Q3;
+    centroid_H_set<kGrad, DM_SERIES_P0_N, DM_SERIES_P2_N, DM_SERIES_P4_N, DM_SERIES_Q1_N,
+                   DM_SERIES_Q3_N>(P0, P2, P4, Q1, Q3, p2, p3, H, Hp2, Hp3);
   }
 }
 
@@ -219,7 +266,7 @@ DM_HD c32 expmi(float angle) {
 // Centroid path.  Vertex phases x'_v = x_v + off[v] with half differences
 // (hab, hbc, hca) of the x'.  Outputs E = exp(-i x'_g), H and, if kGrad, the
 // centroid deviations d[3] and the partials Hp2, Hp3; F = E H.
-template <bool kGrad>
+template <bool kGrad, bool kLo = false>
 DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca, float off_a,
                        c32& E, c32& H, c32& Hp2, c32& Hp3, float d[3], float& p2) {
   const float ab = 2.0f * hab, ca = 2.0f * hca;
@@ -229,7 +276,7 @@ DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca,
   p2 = da * da + db * db + dc * dc;
   const float p3 = 3.0f * da * db * dc;  // sum d^3 when sum d = 0
   E = expmi(turns_to_angle(fixed_phase(xv.mi, g.Ua[0], g.Ua[1], g.Ua[2])) + (off_a - da));
-  centroid_H<kGrad>(p2, p3, H, Hp2, Hp3);
+  centroid_H<kGrad, kLo>(p2, p3, H, Hp2, Hp3);
   d[0] = da;
   d[1] = db;
   d[2] = dc;
@@ -369,6 +416,19 @@ DM_HD void pair_general(const XiVal& xv, const FaceGeom& g, c32& F, c32* dF) {
   }
 }
 
+// Short series set for a pair whose largest half difference is at most
+// kSeriesLoHalf.  On the GPU the choice is made for the converged lanes of the
+// warp together (short set only if every one of them qualifies), so a warp does
+// not run both sets.
+DM_HD bool series_short(float hab, float hbc, float hca) {
+  const bool lo = fmaxf(fabsf(hab), fmaxf(fabsf(hbc), fabsf(hca))) <= kSeriesLoHalf;
+#if defined(__CUDA_ARCH__)
+  return __all_sync(__activemask(), lo);
+#else
+  return lo;
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // Per-pair work of the kernels (shared with the host test build).
 
@@ -383,7 +443,10 @@ DM_HD bool pair_forward(const XiVal& xv, const FaceGeom& g, c32& F) {
   if (cls == 0) {
     c32 E, H, Hp2, Hp3;
     float d[3], p2;
-    eval_series<false>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    if (series_short(hab, hbc, hca))
+      eval_series<false, true>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    else
+      eval_series<false, false>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
     F = cmul(E, H);
   } else {
     c32 E, G, Gu, Gw;
@@ -405,7 +468,10 @@ DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim
   if (cls == 0) {
     c32 E, H, Hp2, Hp3;
     float d[3], p2;
-    eval_series<true>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    if (series_short(hab, hbc, hca))
+      eval_series<true, true>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
+    else
+      eval_series<true, false>(xv, g, hab, hca, 0.f, E, H, Hp2, Hp3, d, p2);
     const float hx = gre * E.x + gim * E.y;  // h = conj(g) E
     const float hy = gre * E.y - gim * E.x;
     r = hx * H.x - hy * H.y;
