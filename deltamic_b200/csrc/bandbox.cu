@@ -32,6 +32,7 @@
 
 #include "band_internal.h"
 #include "dm_common.cuh"
+#include "meshft_internal.h"
 
 namespace dm {
 namespace {
@@ -51,8 +52,6 @@ struct BBShape {
   int32_t ldw2;    // row length of the axis-2 table: n2 rounded up to whole column blocks
   int32_t q1split; // K split of the axis-1 forward contraction (partials summed by the next)
   int32_t q1chunk; // positions x1 per split (a multiple of 16)
-  int32_t g0split; // K split of the axis-0 forward contraction (partials summed in the gather)
-  int32_t g0chunk; // positions x0 per split
   int64_t nlines;  // n0 * n1
   int64_t nvox;
 };
@@ -219,7 +218,7 @@ __global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_
 
 // ---------------------------------------------------------------------------
 // Small batched complex GEMM with a root table on the left:
-//   C[kp][b][m][n] = sum_{k in split kp} A(m, k) X[b][k][n],
+//   C[kp][b][m][n] = sum_{k in split kp} A(m, k) X[b][k][n]  (C strides scp, scb, scm, scn),
 //   X = the sum (in order) of ``xparts`` arrays sxp elements apart,
 //   kInv:  A(m, k) = W[k * ldw + m]        (inverse pass: m = position, k = band offset)
 //   else:  A(m, k) = conj(W[m * ldw + k])  (forward pass: m = band offset, k = position)
@@ -232,8 +231,9 @@ template <bool kInv>
 __global__ void __launch_bounds__(kGemmThreads)
     k_bb_gemm(const float2* __restrict__ W, int ldw, int M, int N, int K, int batch, int kc,
               const float2* __restrict__ X, int64_t sxb, int64_t sxk, int xparts, int64_t sxp,
-              float2* __restrict__ C, int64_t scb, int64_t scm, int64_t scp) {
-  __shared__ __align__(16) float2 As[16][64];
+              float2* __restrict__ C, int64_t scb, int64_t scm, int64_t scn, int64_t scp) {
+  // rows padded by 16 bytes: the forward pass stores A with k across the lanes
+  __shared__ __align__(16) float2 As[16][66];
   __shared__ __align__(16) float2 Bs[16][32];
   const int t = threadIdx.x;
   const int tm = t >> 4, tn = t & 15;
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int n = n0 + tn * 2 + j;
-      if (n < N) Cb[(int64_t)m * scm + n] = acc[i][j];
+      if (n < N) Cb[(int64_t)m * scm + (int64_t)n * scn] = acc[i][j];
     }
   }
 }
@@ -370,11 +370,19 @@ __device__ bool last_cta(unsigned int* counter, unsigned int total, int* flag) {
 }
 
 // ---------------------------------------------------------------------------
-// z pass: 32 lines per CTA, columns x2 in blocks of 32*C (blockIdx.y).
+// z pass: persistent CTAs, each with one column block of 32*C positions x2
+// (blockIdx.y) and the line tiles blockIdx.x, blockIdx.x + gridDim.x, ... of 32
+// lines (x0, x1) each:
 //   z[line][x2] = 1/N sum_j T2[line][j] W2[j][x2];  |z|, min / max.
-// The CTA's T2 rows and W2 column block are staged by bulk copies.  Thread (warp
-// w, lane l): lines 4w..4w+3, columns l + 32c.  The last CTA writes the min /
-// max (first index, tie count) to the header.
+// The W2 column block is staged once by bulk copies; the T2 rows of a tile arrive
+// by bulk copy into one of two buffers while the previous tile is computed.
+// Thread (warp w, lane l): lines 4w..4w+3, positions l + 32c.  The last CTA
+// writes the min / max (first index, tie count) to the header.
+
+__device__ __forceinline__ uint32_t zl_tile_bytes(const BBShape& s, int64_t tile) {
+  const int64_t nl = min((int64_t)kLines, s.nlines - tile * kLines);
+  return (uint32_t)((nl * s.ext[2] * (int64_t)sizeof(float2) + 15) & ~(int64_t)15);
+}
 
 template <int C>
 __global__ void __launch_bounds__(kLineThreads)
@@ -382,33 +390,50 @@ __global__ void __launch_bounds__(kLineThreads)
                 float inv_n, float2* __restrict__ z, float* __restrict__ image,
                 MMC* __restrict__ part, BBHdr* hdr) {
   extern __shared__ __align__(16) float2 sm[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[3];  // W2 block, T2 buffers 0 / 1
   __shared__ MMC shm[kLineThreads / 32];
   __shared__ int last;
   const int ext = s.ext[2], n2 = s.n[2];
   constexpr int Wc = 32 * C;
-  float2* xs = sm;                 // [kLines][ext]
-  float2* ws = sm + kLines * ext;  // [ext][Wc]
-  const int64_t line0 = (int64_t)blockIdx.x * kLines;
+  float2* ws = sm;                        // [ext][Wc]
+  float2* xs0 = sm + ext * Wc;            // [2][kLines][ext]
+  const int64_t ntiles = (s.nlines + kLines - 1) / kLines;
+  const int64_t G = gridDim.x;
   const int col0 = blockIdx.y * Wc;
-  const int64_t nl = min((int64_t)kLines, s.nlines - line0);
   if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
+    for (int b = 0; b < 3; ++b) mbar_init(&bar[b], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  // copies issued into each barrier and copies waited for (thread 0 drains the
+  // difference if a wait gives up, before the CTA leaves)
+  int iss_w = 0, iss_0 = 0, iss_1 = 0, got_w = 0, got_0 = 0, got_1 = 0;
   if (threadIdx.x == 0) {
-    const uint32_t xb = (uint32_t)((nl * ext * (int64_t)sizeof(float2) + 15) & ~(int64_t)15);
     const uint32_t wb = (uint32_t)(Wc * sizeof(float2));
-    mbar_expect_tx(&bar, xb + (uint32_t)ext * wb);
-    bulk_g2s(xs, t2 + line0 * ext, xb, &bar);
+    mbar_expect_tx(&bar[0], (uint32_t)ext * wb);
     for (int j = 0; j < ext; ++j)
-      bulk_g2s(ws + j * Wc, w2 + (int64_t)j * s.ldw2 + col0, wb, &bar);
+      bulk_g2s(ws + j * Wc, w2 + (int64_t)j * s.ldw2 + col0, wb, &bar[0]);
+    iss_w = 1;
+    for (int b = 0; b < 2; ++b) {
+      const int64_t tile = blockIdx.x + b * G;
+      if (tile >= ntiles) break;
+      const uint32_t xb = zl_tile_bytes(s, tile);
+      mbar_expect_tx(&bar[1 + b], xb);
+      bulk_g2s(xs0 + b * kLines * ext, t2 + tile * kLines * ext, xb, &bar[1 + b]);
+      if (b == 0) iss_0 = 1; else iss_1 = 1;
+    }
   }
-  const bool ok = mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
+  bool ok = __syncthreads_and(mbar_wait_sleep_bounded(&bar[0], 0, &hdr->err));
+  got_w = ok ? 1 : 0;
   const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
   MMC r = mmc_empty();
-  if (ok) {
+  int it = 0;
+  for (int64_t tile = blockIdx.x; ok && tile < ntiles; tile += G, ++it) {
+    const int buf = it & 1;
+    ok = __syncthreads_and(mbar_wait_sleep_bounded(&bar[1 + buf], (it >> 1) & 1, &hdr->err));
+    if (!ok) break;
+    if (buf == 0) ++got_0; else ++got_1;
+    const float2* xs = xs0 + buf * kLines * ext;
     float2 acc[4][C];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -425,6 +450,15 @@ __global__ void __launch_bounds__(kLineThreads)
 #pragma unroll
         for (int c = 0; c < C; ++c) acc[i][c] = cmac(acc[i][c], xv[i], wv[c]);
     }
+    __syncthreads();  // every read of this buffer is done: refill it
+    if (threadIdx.x == 0 && tile + 2 * G < ntiles) {
+      fence_proxy_async();
+      const uint32_t xb = zl_tile_bytes(s, tile + 2 * G);
+      mbar_expect_tx(&bar[1 + buf], xb);
+      bulk_g2s(xs0 + buf * kLines * ext, t2 + (tile + 2 * G) * kLines * ext, xb, &bar[1 + buf]);
+      if (buf == 0) ++iss_0; else ++iss_1;
+    }
+    const int64_t line0 = tile * kLines;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int64_t line = line0 + ty * 4 + i;
@@ -441,6 +475,11 @@ __global__ void __launch_bounds__(kLineThreads)
         mmc_add(r, a, idx);
       }
     }
+  }
+  if (!ok && threadIdx.x == 0) {  // a wait gave up: let the copies in flight land first
+    if (iss_w > got_w) mbar_wait_sleep_bounded(&bar[0], 0, &hdr->err);
+    if (iss_0 > got_0) mbar_wait_sleep_bounded(&bar[1], (iss_0 - 1) & 1, &hdr->err);
+    if (iss_1 > got_1) mbar_wait_sleep_bounded(&bar[2], (iss_1 - 1) & 1, &hdr->err);
   }
   r = block_mmc(r, shm);
   const unsigned int total = gridDim.x * gridDim.y;
@@ -481,9 +520,9 @@ __host__ __device__ inline int red_units(int ldj) {  // 16-byte units per partia
 }
 
 size_t gradlines_smem(int n2, int ldj) {
-  const size_t a = (size_t)n2 * (kLines + ldj) * sizeof(float2);
-  const size_t b = (size_t)8 * kLines * red_units(ldj) * 16;
-  return std::max(a, b);
+  const size_t tile = std::max((size_t)n2 * kLines * sizeof(float2),
+                               (size_t)8 * kLines * red_units(ldj) * 16);
+  return (size_t)n2 * ldj * sizeof(float2) + tile;
 }
 
 template <int JC>
@@ -497,11 +536,11 @@ __global__ void __launch_bounds__(kLineThreads)
   __shared__ LP shp[kLineThreads];
   __shared__ int last;
   const int n2 = s.n[2], ext = s.ext[2], ldj = s.ldj;
-  float2* gzt = sm;                // [n2][kLines], line groups swizzled by x2 mod 8
-  float2* wt = sm + n2 * kLines;   // [n2][ldj]
-  float4* red = reinterpret_cast<float4*>(sm);  // [8][kLines][RU] 16-byte units, after the contraction
+  float2* wt = sm;                 // [n2][ldj], staged once
+  float2* gzt = sm + n2 * ldj;     // [n2][kLines], line groups swizzled by x2 mod 8
+  float4* red = reinterpret_cast<float4*>(gzt);  // [8][kLines][RU] 16-byte units, after the contraction
   const int RU = red_units(ldj);
-  const int64_t line0 = (int64_t)blockIdx.x * kLines;
+  const int64_t ntiles = (s.nlines + kLines - 1) / kLines;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -518,104 +557,116 @@ __global__ void __launch_bounds__(kLineThreads)
   const float inv = 1.0f / (rng * (1.0f + contrast));
   const float nseg_inv = 1.0f / (float)s.nvox;
   double L = 0.0, dmn = 0.0, dmx = 0.0;
-  // warp w: lines 4w..4w+3; lane = 8 li + xi: line 4w+li, position 8k+xi of tile k
+  // phase 1 mapping: warp w, lines 4w..4w+3; lane = 8 li + xi: line 4w+li, position
+  // 8k+xi of position tile k.  GEMM mapping: lane = lg + 8 jg.
   const int li = lane >> 3, xi = lane & 7;
   const int l = 4 * w + li;
-  const int64_t line = line0 + l;
-  const bool live_line = line < s.nlines;
-  const int ntile = (n2 + 7) / 8;
   const int col = (l ^ (xi << 2));  // gT column of this lane's line (x2 mod 8 == xi)
-  for (int k0 = 0; k0 < ntile; k0 += kAhead) {
-    float2 zv[kAhead];
-    float tv[kAhead];
-#pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const int x = 8 * (k0 + u) + xi;
-      const bool live = live_line && x < n2;
-      const int64_t i = line * n2 + x;
-      zv[u] = live ? z[i] : make_float2(0.f, 0.f);
-      tv[u] = (live && kind != 0) ? target[i] : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const int x = 8 * (k0 + u) + xi;
-      if (x >= n2) continue;
-      float2 g = make_float2(0.f, 0.f);
-      if (live_line) {
-        const float2 zi = zv[u];
-        const float a = cabs2(zi);
-        const float uu = (a - mn) / rng;
-        const float nv = (uu + contrast) / (1.0f + contrast);
-        float gn;
-        if (kind == 0) {
-          L += nv;
-          gn = 1.0f;
-        } else {
-          const float dlt = nv - tv[u];
-          L += (double)dlt * dlt;
-          gn = 2.0f * dlt * nseg_inv;
-        }
-        dmn += (double)gn * (-(1.0 - (double)uu));
-        dmx += (double)gn * (-(double)uu);
-        const float gg = gn * inv;
-        const float sc = a > 0.f ? gg / a : 0.f;
-        g = make_float2(sc * zi.x, sc * zi.y);
-      }
-      gzt[x * kLines + col] = g;
-    }
-  }
-  const bool ok = mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
-  __syncthreads();
+  const int ntile = (n2 + 7) / 8;
   const int lg = lane & 7, jg = lane >> 3;
-  float2 acc[4][JC][2];
+  bool ok = true, staged = false;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t line0 = tile * kLines;
+    const int64_t line = line0 + l;
+    const bool live_line = line < s.nlines;
+    for (int k0 = 0; k0 < ntile; k0 += kAhead) {
+      float2 zv[kAhead];
+      float tv[kAhead];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+      for (int u = 0; u < kAhead; ++u) {
+        const int x = 8 * (k0 + u) + xi;
+        const bool live = live_line && x < n2;
+        const int64_t i = line * n2 + x;
+        zv[u] = live ? z[i] : make_float2(0.f, 0.f);
+        tv[u] = (live && kind != 0) ? target[i] : 0.f;
+      }
 #pragma unroll
-    for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
-  const int xb = w * n2 / 8, xe = ok ? (w + 1) * n2 / 8 : xb;
-  for (int x = xb; x < xe; ++x) {
-    const float2* row = gzt + x * kLines + 4 * (lg ^ (x & 7));  // lines 4lg..4lg+3
-    const float4 g01 = *reinterpret_cast<const float4*>(row);
-    const float4 g23 = *reinterpret_cast<const float4*>(row + 2);
-    const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
-                          make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
-#pragma unroll
-    for (int c = 0; c < JC; ++c) {
-      const float4 wv = *reinterpret_cast<const float4*>(&wt[x * ldj + c * 8 + jg * 2]);
-      const float2 w0 = make_float2(wv.x, wv.y), w1 = make_float2(wv.z, wv.w);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        acc[i][c][0] = cmac(acc[i][c][0], gv[i], w0);
-        acc[i][c][1] = cmac(acc[i][c][1], gv[i], w1);
+      for (int u = 0; u < kAhead; ++u) {
+        const int x = 8 * (k0 + u) + xi;
+        if (x >= n2) continue;
+        float2 g = make_float2(0.f, 0.f);
+        if (live_line) {
+          const float2 zi = zv[u];
+          const float a = cabs2(zi);
+          const float uu = (a - mn) / rng;
+          const float nv = (uu + contrast) / (1.0f + contrast);
+          float gn;
+          if (kind == 0) {
+            L += nv;
+            gn = 1.0f;
+          } else {
+            const float dlt = nv - tv[u];
+            L += (double)dlt * dlt;
+            gn = 2.0f * dlt * nseg_inv;
+          }
+          dmn += (double)gn * (-(1.0 - (double)uu));
+          dmx += (double)gn * (-(double)uu);
+          const float gg = gn * inv;
+          const float sc = a > 0.f ? gg / a : 0.f;
+          g = make_float2(sc * zi.x, sc * zi.y);
+        }
+        gzt[x * kLines + col] = g;
       }
     }
-  }
-  __syncthreads();
-  // partial sums: row (warp, line), 16-byte unit (c*4 + jg) ^ (line >> 2)
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int ln = lg * 4 + i;
-#pragma unroll
-    for (int c = 0; c < JC; ++c)
-      red[(w * kLines + ln) * RU + ((c * 4 + jg) ^ lg)] =
-          make_float4(acc[i][c][0].x, acc[i][c][0].y, acc[i][c][1].x, acc[i][c][1].y);
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < kLines * ext; e += kLineThreads) {
-    const int ln = e / ext, j = e - ln * ext;
-    const int64_t lq = line0 + ln;
-    if (lq >= s.nlines) continue;
-    const int unit = (j >> 1) ^ (ln >> 2);
-    const float* base = reinterpret_cast<const float*>(red) + 4 * unit + 2 * (j & 1);
-    float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const float* p = base + 4 * (k * kLines + ln) * RU;
-      v.x += p[0];
-      v.y += p[1];
+    if (!staged) {
+      ok = __syncthreads_and(mbar_wait_sleep_bounded(&bar, 0, &hdr->err));
+      staged = true;
+      if (!ok) break;
     }
-    q2[lq * ext + j] = v;
+    __syncthreads();
+    float2 acc[4][JC][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
+    const int xb = w * n2 / 8, xe = (w + 1) * n2 / 8;
+    for (int x = xb; x < xe; ++x) {
+      const float2* row = gzt + x * kLines + 4 * (lg ^ (x & 7));  // lines 4lg..4lg+3
+      const float4 g01 = *reinterpret_cast<const float4*>(row);
+      const float4 g23 = *reinterpret_cast<const float4*>(row + 2);
+      const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
+                            make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
+#pragma unroll
+      for (int c = 0; c < JC; ++c) {
+        const float4 wv = *reinterpret_cast<const float4*>(&wt[x * ldj + c * 8 + jg * 2]);
+        const float2 w0 = make_float2(wv.x, wv.y), w1 = make_float2(wv.z, wv.w);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          acc[i][c][0] = cmac(acc[i][c][0], gv[i], w0);
+          acc[i][c][1] = cmac(acc[i][c][1], gv[i], w1);
+        }
+      }
+    }
+    __syncthreads();
+    // partial sums: row (warp, line), 16-byte unit (c*4 + jg) ^ (line >> 2)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int ln = lg * 4 + i;
+#pragma unroll
+      for (int c = 0; c < JC; ++c)
+        red[(w * kLines + ln) * RU + ((c * 4 + jg) ^ lg)] =
+            make_float4(acc[i][c][0].x, acc[i][c][0].y, acc[i][c][1].x, acc[i][c][1].y);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kLines * ext; e += kLineThreads) {
+      const int ln = e / ext, j = e - ln * ext;
+      const int64_t lq = line0 + ln;
+      if (lq >= s.nlines) continue;
+      const int unit = (j >> 1) ^ (ln >> 2);
+      const float* base = reinterpret_cast<const float*>(red) + 4 * unit + 2 * (j & 1);
+      float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float* p = base + 4 * (k * kLines + ln) * RU;
+        v.x += p[0];
+        v.y += p[1];
+      }
+      q2[lq * ext + j] = v;
+    }
+    __syncthreads();  // the tile region is written again by the next tile
   }
+  if (!staged && threadIdx.x == 0) mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
+  if (!ok && threadIdx.x == 0) mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
   // loss partials (fixed order)
   double v[3] = {L, dmn, dmx};
 #pragma unroll
@@ -693,10 +744,55 @@ __global__ void k_bb_ties(BBShape s, const float2* __restrict__ z, const BBHdr* 
   }
 }
 
-// G at the band voxels: the K-split partials of the axis-0 contraction G0[j0][j1][j2]
-// added in order, plus the min / max gradient of a single extreme voxel.
+// Axis-0 forward contraction into the band box, one CTA per column (j1, j2):
+//   G0[j0][j1 j2] = sum_x0 conj(W0[j0][x0]) Q1[j1 j2][x0]
+// with Q1 the sum (in order) of its K-split partials, staged in shared memory
+// from its column-major layout; eight lanes per output, fixed shuffle tree.
+constexpr int kColThreads = 128;
+
+__global__ void __launch_bounds__(kColThreads)
+    k_bb_columns(BBShape s, const float2* __restrict__ q1t, const float2* __restrict__ w0,
+                 float2* __restrict__ g0) {
+  extern __shared__ __align__(16) float2 colv[];  // [n0]
+  const int64_t c = blockIdx.x;                    // j1 * ext2 + j2
+  const int64_t ncol = (int64_t)s.ext[1] * s.ext[2];
+  const int n0 = s.n[0];
+  for (int x0 = threadIdx.x; x0 < n0; x0 += kColThreads) {
+    const float2* p = q1t + c * n0 + x0;
+    float2 q = p[0];
+    for (int kp = 1; kp < s.q1split; ++kp) {
+      const float2 r = p[kp * ncol * n0];
+      q.x += r.x;
+      q.y += r.y;
+    }
+    colv[x0] = q;
+  }
+  __syncthreads();
+  const int sub = threadIdx.x & 7, grp = threadIdx.x >> 3;
+  const int rounds = (s.ext[0] + kColThreads / 8 - 1) / (kColThreads / 8);
+  for (int it = 0; it < rounds; ++it) {  // the same rounds for every lane (shuffles)
+    const int j0 = grp + it * (kColThreads / 8);
+    float2 g = make_float2(0.f, 0.f);
+    if (j0 < s.ext[0]) {
+      const float2* wr = w0 + (int64_t)j0 * n0;
+#pragma unroll 5
+      for (int x0 = sub; x0 < n0; x0 += 8) {
+        float2 w = wr[x0];
+        w.y = -w.y;
+        g = cmac(g, colv[x0], w);
+      }
+    }
+    for (int o = 4; o > 0; o >>= 1) {
+      g.x += __shfl_down_sync(0xffffffffu, g.x, o, 8);
+      g.y += __shfl_down_sync(0xffffffffu, g.y, o, 8);
+    }
+    if (sub == 0 && j0 < s.ext[0]) g0[(int64_t)j0 * ncol + c] = g;
+  }
+}
+
+// G at the band voxels: G0 plus the min / max gradient of a single extreme voxel.
 __global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t nb,
-                            const float2* __restrict__ g0p, const float2* __restrict__ w0,
+                            const float2* __restrict__ g0, const float2* __restrict__ w0,
                             const float2* __restrict__ w1, const float2* __restrict__ w2,
                             const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
                             float2* __restrict__ grad_list) {
@@ -710,14 +806,7 @@ __global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t
   const int32_t j0 = min(max(k0 - s.lo[0], 0), s.ext[0] - 1);
   const int32_t j1 = min(max(k1 - s.lo[1], 0), s.ext[1] - 1);
   const int32_t j2 = min(max(k2 - s.lo[2], 0), s.ext[2] - 1);
-  const int64_t box = (int64_t)s.ext[0] * s.ext[1] * s.ext[2];
-  const float2* p = g0p + ((int64_t)j0 * s.ext[1] + j1) * s.ext[2] + j2;
-  float2 g = p[0];
-  for (int kp = 1; kp < s.g0split; ++kp) {
-    const float2 q = p[kp * box];
-    g.x += q.x;
-    g.y += q.y;
-  }
+  float2 g = g0[((int64_t)j0 * s.ext[1] + j1) * s.ext[2] + j2];
   if (!hdr->ties_full) {
     for (int k = 0; k < 2; ++k) {
       const int64_t c = k == 0 ? hdr->cmn : hdr->cmx;
@@ -785,7 +874,7 @@ struct BBWs {
   float2 *w0, *w1, *w2, *w2t;
   float2 *t0, *t1, *t2;  // band box, after axis 0, after axis 1 (Q2 reuses t2)
   float2* q1p;           // K-split partials of the axis-1 forward contraction
-  float2* g0p;           // K-split partials of the axis-0 forward contraction (band box)
+  float2* g0;            // axis-0 forward contraction over the band box
   float2* z;
   MMC* mm;
   LP* lp;
@@ -814,7 +903,7 @@ size_t bb_layout(const BBShape& s, char* base, BBWs* w) {
   r.t1 = (float2*)take(c8 * (size_t)s.n[0] * e1 * e2);
   r.t2 = (float2*)take(c8 * (size_t)s.nlines * e2);
   r.q1p = (float2*)take(c8 * (size_t)s.q1split * s.n[0] * e1 * e2);
-  r.g0p = (float2*)take(c8 * (size_t)s.g0split * e0 * e1 * e2);
+  r.g0 = (float2*)take(c8 * e0 * e1 * e2);
   r.z = (float2*)take(c8 * (size_t)s.nvox);
   r.mm = (MMC*)take(sizeof(MMC) * (size_t)(nlb * cb));
   r.lp = (LP*)take(sizeof(LP) * (size_t)nlb);
@@ -841,21 +930,20 @@ bool make_shape(const int32_t n[3], const int32_t lo[3], const int32_t ext[3], B
   s.zc = z_col_chunk(n[2]);
   s.ldw2 = (n[2] + 32 * s.zc - 1) / (32 * s.zc) * (32 * s.zc);
   ksplit(n[1], s.q1chunk, s.q1split);
-  ksplit(n[0], s.g0chunk, s.g0split);
   s.nlines = (int64_t)n[0] * n[1];
   s.nvox = s.nlines * n[2];
-  return s.nvox <= (int64_t)INT32_MAX && (int64_t)n[0] * s.q1split <= 65535 &&
+  return s.nvox <= (int64_t)INT32_MAX && (int64_t)n[0] * s.q1split <= 65535 && n[0] <= 4096 &&
          s.nlines / kLines < (int64_t)INT32_MAX;
 }
 
 template <bool kInv>
 void gemm(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X, int64_t sxb,
           int64_t sxk, int xparts, int64_t sxp, float2* C, int64_t scb, int64_t scm,
-          int64_t scp, int batch, cudaStream_t st) {
+          int64_t scn, int64_t scp, int batch, cudaStream_t st) {
   const int splits = (K + kc - 1) / kc;
   dim3 grid((N + 31) / 32, (M + 63) / 64, batch * splits);
   k_bb_gemm<kInv><<<grid, kGemmThreads, 0, st>>>(W, ldw, M, N, K, batch, kc, X, sxb, sxk,
-                                                  xparts, sxp, C, scb, scm, scp);
+                                                  xparts, sxp, C, scb, scm, scn, scp);
 }
 
 
@@ -872,14 +960,17 @@ cudaError_t smem_limit_once(Kern k, bool* done) {
   return e;
 }
 
+// Persistent CTAs of the line passes: two per SM, never more than the tiles.
+int line_ctas(int64_t tiles) { return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 2 * num_sms())); }
+
 template <int C>
 cudaError_t zlines(const BBShape& s, const BBWs& w, float inv_n, float* image, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * ((size_t)kLines * s.ext[2] + (size_t)s.ext[2] * 32 * C);
+  const size_t smem = sizeof(float2) * ((size_t)s.ext[2] * 32 * C + 2 * (size_t)kLines * s.ext[2]);
   auto k = k_bb_zlines<C>;
   static bool done[64] = {};
   cudaError_t e = smem_limit_once(k, done);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((s.nlines + kLines - 1) / kLines), s.ldw2 / (32 * C));
+  dim3 grid((unsigned)line_ctas((s.nlines + kLines - 1) / kLines), s.ldw2 / (32 * C));
   k<<<grid, kLineThreads, smem, st>>>(s, w.t2, w.w2, inv_n, w.z, image, w.mm, w.hdr);
   return cudaGetLastError();
 }
@@ -892,9 +983,9 @@ cudaError_t gradlines(const BBShape& s, const BBWs& w, int kind, const float* ta
   static bool done[64] = {};
   cudaError_t e = smem_limit_once(k, done);
   if (e != cudaSuccess) return e;
-  const unsigned nlb = (unsigned)((s.nlines + kLines - 1) / kLines);
-  k<<<nlb, kLineThreads, smem, st>>>(s, w.z, target, kind, contrast, w.hdr, w.w2t, w.t2, w.lp,
-                                     loss);
+  const unsigned nb = (unsigned)line_ctas((s.nlines + kLines - 1) / kLines);
+  k<<<nb, kLineThreads, smem, st>>>(s, w.z, target, kind, contrast, w.hdr, w.w2t, w.t2, w.lp,
+                                    loss);
   return cudaGetLastError();
 }
 
@@ -988,10 +1079,10 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
   const int64_t e12 = (int64_t)s.ext[1] * s.ext[2];
   // axis 0: T1[x0][j1 j2] = sum_j0 W0[j0][x0] T0[j0][j1 j2]
   gemm<true>(w.w0, s.n[0], s.n[0], (int)e12, s.ext[0], s.ext[0], w.t0, 0, e12, 1, 0, w.t1, 0,
-             e12, 0, 1, st);
+             e12, 1, 0, 1, st);
   // axis 1: T2[x0][x1][j2] = sum_j1 W1[j1][x1] T1[x0][j1][j2]
   gemm<true>(w.w1, s.n[1], s.n[1], s.ext[2], s.ext[1], s.ext[1], w.t1, e12, s.ext[2], 1, 0,
-             w.t2, (int64_t)s.n[1] * s.ext[2], s.ext[2], 0, s.n[0], st);
+             w.t2, (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, s.n[0], st);
   launches += 2;
   const float inv_n = (float)(1.0 / (double)s.nvox);
   switch (s.zc) {
@@ -1015,16 +1106,15 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
   launches += 2;
   if (grad_list) {
     k_bb_ties<<<(unsigned)((s.nlines + 127) / 128), 128, 0, st>>>(s, w.z, w.hdr, w.w2t, w.t2);
-    // axis 1 (forward): Q1[kp][x0][j1][j2] = sum_{x1 in split kp} conj(W1[j1][x1]) Q2[x0][x1][j2]
+    // axis 1 (forward), column-major: Q1[kp][j1 j2][x0] = sum_{x1 in split kp} conj(W1[j1][x1]) Q2[x0][x1][j2]
     gemm<false>(w.w1, s.n[1], s.ext[1], s.ext[2], s.n[1], s.q1chunk, w.t2,
-                (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, w.q1p, e12, s.ext[2],
-                (int64_t)s.n[0] * e12, s.n[0], st);
-    // axis 0 (forward): G0[kp][j0][j1 j2] = sum_{x0 in split kp} conj(W0[j0][x0]) sum_q Q1[q][x0][j1 j2]
-    gemm<false>(w.w0, s.n[0], s.ext[0], (int)e12, s.n[0], s.g0chunk, w.q1p, 0, e12,
-                s.q1split, (int64_t)s.n[0] * e12, w.g0p, 0, e12,
-                (int64_t)s.ext[0] * e12, 1, st);
+                (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, w.q1p, 1,
+                (int64_t)s.ext[2] * s.n[0], s.n[0], e12 * s.n[0], s.n[0], st);
+    // axis 0 (forward) over the band box, then the band entries
+    k_bb_columns<<<(unsigned)e12, kColThreads, sizeof(float2) * (size_t)s.n[0], st>>>(
+        s, w.q1p, w.w0, w.g0);
     k_bb_gather<<<(unsigned)((n_band + 255) / 256), 256, 0, st>>>(
-        s, band_index, n_band, w.g0p, w.w0, w.w1, w.w2, w.z, w.hdr, (float2*)grad_list);
+        s, band_index, n_band, w.g0, w.w0, w.w1, w.w2, w.z, w.hdr, (float2*)grad_list);
     launches += 4;
   }
   count_launches(launches);
