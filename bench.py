@@ -43,6 +43,11 @@ LR = 1e-3
 # forward 32 FP32 + 7 MUFU, adjoint with recompute 80 FP32 + 9 MUFU.
 FWD_FP32, FWD_MUFU = 32, 7
 BWD_FP32, BWD_MUFU = 80, 9
+# DRAM bytes (read + write) per launch of the adjoint kernel in this workload, from
+# one ncu capture of the fit step (dram__bytes_read.sum + dram__bytes_write.sum,
+# profiles/k_meshft_fit200.md): the kernel streams face records and frequency
+# tiles, far below its compute time at HBM speed.
+NCU_TRAFFIC_BWD = 3061248 + 577024
 METRIC = "meshFT face*xi pairs/s (fit step: fwd+bwd, 200^3, 20,480 faces)"
 METRIC_BATCH = "meshFT face*xi pairs/s (batched fit step: 64 cells, fwd+bwd)"
 
@@ -61,6 +66,10 @@ def parse():
     p.add_argument("--train", type=int, default=50000, help="learned: training pairs")
     p.add_argument("--epochs", type=int, default=8, help="learned: training epochs")
     p.add_argument("--eval", type=int, default=256, help="learned: held-out shapes")
+    p.add_argument("--precond-lambda", type=float, default=0.0,
+                   help="fit300: precondition the vertex gradient with (M M)^-1, M = I + lambda L, "
+                        "and step with VectorAdam (0: plain Adam, the configured fit)")
+    p.add_argument("--precond-lr", type=float, default=5e-3)
     p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned"],
                    default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
@@ -320,14 +329,25 @@ def run_fit300(args, rank, world, local):
     G = torch.tensor(gt_v, dtype=torch.float32, device=dev)
     target = noisy_target(r.render(G, F, C), gen, 0, dev)
     V0 = torch.tensor(init_v, dtype=torch.float32, device=dev)
-    run_fit(r, V0, F, C, target, steps=3, lr=LR)  # warm-up: graph capture, plans
-    res = run_fit(r, V0, F, C, target, steps=300, lr=LR)
+    kw = dict(lr=LR)
+    label = "plain sphere-init fit, 300 Adam steps"
+    if args.precond_lambda > 0:
+        from deltamic_b200.precond import LargeStepsPreconditioner
+        t0 = time.perf_counter()
+        pc = LargeStepsPreconditioner(F, len(init_v), args.precond_lambda, dev)
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        kw = dict(lr=args.precond_lr, precond=pc, optimizer="vector_adam")
+        label = (f"preconditioned sphere-init fit ((M M)^-1, lambda {args.precond_lambda:g}, "
+                 f"VectorAdam lr {args.precond_lr:g}), 300 steps")
+    run_fit(r, V0, F, C, target, steps=3, **kw)  # warm-up: graph capture, plans
+    res = run_fit(r, V0, F, C, target, steps=300, **kw)
     iou0 = mesh_iou(V0, G, F, r.grid)
     iou1 = mesh_iou(res["verts"], G, F, r.grid)
     ms = max_over_ranks(res["ms_total"], dev)
     if rank != 0:
         return
-    out = {"metric": "time-to-fit: plain sphere-init fit, 300 Adam steps at 200^3",
+    out = {"metric": f"time-to-fit: {label} at 200^3",
            "value": ms, "unit": "ms", "n_gpus": world, "steps": 300, "warmup": 3,
            "ms_per_step": ms / 300, "higher_is_better": False, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -336,6 +356,8 @@ def run_fit300(args, rank, world, local):
                       "image_l2_first": float(res["losses"][0]),
                       "image_l2_final": float(res["losses"][-1]),
                       "iou_init": iou0, "iou_final": iou1}}
+    if args.precond_lambda > 0:
+        out["config"]["precond_setup_s"] = t_setup
     print(json.dumps(out), flush=True)
 
 
@@ -513,7 +535,8 @@ def run_ours(args, rank, world, local):
             "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
             "frac": achieved / peak,
             "peak_source": "measured in this run by dm_peak_probe (MUFU sin / FP32 FMA chains)",
-            "traffic": None,
+            "traffic": NCU_TRAFFIC_BWD if args.workload == "fit200" and not args.small else None,
+            "traffic_unit": "bytes per launch (ncu capture)",
             "ops_per_pair": {"fp32": BWD_FP32, "mufu": BWD_MUFU},
             "kernel_ms": bwd_ms,
             "fp32_frac": frac_f, "mufu_frac": frac_m,

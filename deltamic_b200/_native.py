@@ -100,6 +100,8 @@ SIGNATURES = {
                                      _P, _P, _SZ, _P]),
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
+    "dm_precond_apply": (_INT, [_P, _I64, _I64, _P, _P, _P]),
+    "dm_vector_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
     "dm_launch_count": (ctypes.c_longlong, []),
     "dm_set_variants": (_INT, [_INT, _INT]),
     "dm_get_variants": (_INT, [ctypes.POINTER(_INT)] * 4),

@@ -75,6 +75,21 @@ def _time(fn, reps, trials=3):
     return best
 
 
+def _pick(n_variants, set_variant, fn, reps, trials=4):
+    """Index of the fastest variant: every trial times each variant once, in
+    turn, so clock changes during tuning fall on all variants alike; a variant
+    keeps its fastest trial."""
+    best = [float("inf")] * n_variants
+    for v in range(n_variants):  # warm-up: first launch of each variant
+        set_variant(v)
+        fn()
+    for _ in range(trials):
+        for v in range(n_variants):
+            set_variant(v)
+            best[v] = min(best[v], _time(fn, reps, trials=1))
+    return min(range(n_variants), key=lambda v: best[v])
+
+
 def tune(verts, faces, coeff, grid, band, reps=4, force=False):
     """Pick and apply the fastest (forward, adjoint) variants for this size class."""
     if not _CACHE:
@@ -86,11 +101,11 @@ def tune(verts, faces, coeff, grid, band, reps=4, force=False):
     f0, b0, nf, nb = current()
     g = torch.ones(band.numel(), dtype=torch.complex64, device=verts.device)
     ft = ops.meshft_list(verts, faces, coeff, grid, band)
-    best_f = min(range(nf), key=lambda v: (apply((v, b0)), _time(
-        lambda: ops.meshft_list(verts, faces, coeff, grid, band), reps))[1])
-    best_b = min(range(nb), key=lambda v: (apply((best_f, v)), _time(
-        lambda: ops.meshft_backward_list(verts, faces, coeff, grid, band, ft, grad_list=g,
-                                         want_coeff=False), reps))[1])
+    best_f = _pick(nf, lambda v: apply((v, b0)),
+                   lambda: ops.meshft_list(verts, faces, coeff, grid, band), reps)
+    best_b = _pick(nb, lambda v: apply((best_f, v)),
+                   lambda: ops.meshft_backward_list(verts, faces, coeff, grid, band, ft,
+                                                    grad_list=g, want_coeff=False), reps)
     _CACHE[key] = (best_f, best_b)
     apply(_CACHE[key])
     _save()

@@ -1,0 +1,155 @@
+// Gradient preconditioning and the vector Adam step of the preconditioned fit.
+//
+// The reference's fitting notebook replaces the vertex gradient g by
+// (M^2)^-1 g with M = I + lambda L (L the uniform mesh Laplacian; largesteps'
+// compute_matrix + CholeskySolver(M@M), Examples/Gradient_Descent.ipynb cell 2),
+// and its optimize.py:207-212 forms the same operator densely as
+// inv(M) @ inv(M).  Here the dense operator P (nv x nv, float32, rows padded to a
+// multiple of 4) is built once per topology and applied every step by an
+// HBM-bound product: each warp streams four rows of P with 16-byte loads and
+// multiplies them with the matching 4 x 3 block of g, read through L1.
+// The optimizer is VectorAdam of optimize.py:215-258 (axis -1): the second
+// moment of each vertex is the squared norm of its 3-vector gradient.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "band_internal.h"
+#include "dm_common.cuh"
+
+namespace dm {
+namespace {
+
+constexpr int kRowsPerWarp = 4;
+constexpr int kGemvThreads = 256;
+
+// out[r][d] = sum_c P[r][c] g[c][d] for d < 3; P row stride ldp (multiple of 4),
+// g and out [nv][3] (g read through the read-only cache).
+__global__ void __launch_bounds__(kGemvThreads)
+    k_precond_gemv(const float* __restrict__ P, int64_t nv, int64_t ldp,
+                   const float* __restrict__ g, float* __restrict__ out) {
+  const int64_t warp = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t r0 = warp * kRowsPerWarp;
+  if (r0 >= nv) return;
+  float acc[kRowsPerWarp][3];
+#pragma unroll
+  for (int i = 0; i < kRowsPerWarp; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
+  const int64_t nq = ldp / 4;  // 16-byte column groups per row
+  for (int64_t q = lane; q < nq; q += 32) {
+    const int64_t c = 4 * q;
+    float gv[12];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const bool live = c + k < nv;
+      gv[3 * k + 0] = live ? __ldg(g + 3 * (c + k) + 0) : 0.f;
+      gv[3 * k + 1] = live ? __ldg(g + 3 * (c + k) + 1) : 0.f;
+      gv[3 * k + 2] = live ? __ldg(g + 3 * (c + k) + 2) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kRowsPerWarp; ++i) {
+      if (r0 + i >= nv) break;
+      const float4 p = __ldcs(reinterpret_cast<const float4*>(P + (r0 + i) * ldp) + q);
+      const float pv[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        acc[i][0] = fmaf(pv[k], gv[3 * k + 0], acc[i][0]);
+        acc[i][1] = fmaf(pv[k], gv[3 * k + 1], acc[i][1]);
+        acc[i][2] = fmaf(pv[k], gv[3 * k + 2], acc[i][2]);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kRowsPerWarp; ++i)
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int o = 16; o > 0; o >>= 1) acc[i][d] += __shfl_xor_sync(0xffffffffu, acc[i][d], o);
+  if (lane < kRowsPerWarp * 3) {
+    const int i = lane / 3, d = lane % 3;
+    if (r0 + i < nv) {
+      float v = 0.f;
+#pragma unroll
+      for (int ii = 0; ii < kRowsPerWarp; ++ii)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd)
+          if (ii == i && dd == d) v = acc[ii][dd];
+      out[3 * (r0 + i) + d] = v;
+    }
+  }
+}
+
+// VectorAdam (optimize.py:215-258, axis -1) on nv 3-vectors; ``step`` is a device
+// counter, incremented by the single-block launch or by k_bump afterwards.
+__global__ void k_vector_adam(float* __restrict__ p, const float* __restrict__ g,
+                              float* __restrict__ m, float* __restrict__ v, int64_t nv, float lr,
+                              float b1, float b2, float eps, int64_t* step, int bump) {
+  const int64_t t = *step + 1;
+  const double bc1 = 1.0 - pow((double)b1, (double)t);
+  const double bc2 = 1.0 - pow((double)b2, (double)t);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float g0 = g[3 * i], g1 = g[3 * i + 1], g2 = g[3 * i + 2];
+    const float nrm = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+    const float vi = b2 * v[i] + (1.0f - b2) * (nrm * nrm);
+    v[i] = vi;
+    const float den = eps + sqrtf((float)(vi / bc2));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float mi = b1 * m[3 * i + d] + (1.0f - b1) * g[3 * i + d];
+      m[3 * i + d] = mi;
+      p[3 * i + d] -= lr * ((float)(mi / bc1) / den);
+    }
+  }
+  if (bump) {
+    __syncthreads();
+    if (threadIdx.x == 0) *step = t;
+  }
+}
+
+__global__ void k_step_bump(int64_t* step) { *step += 1; }
+
+}  // namespace
+}  // namespace dm
+
+using namespace dm;
+
+extern "C" {
+
+int dm_precond_apply(const float* P, int64_t nv, int64_t ldp, const float* grad, float* out,
+                     dm_stream_t stream) {
+  if (nv < 0 || ldp < nv || (ldp & 3) != 0) return DM_ERR_INVALID_ARG;
+  if (nv == 0) return DM_OK;
+  if (!P || !grad || !out || grad == out) return DM_ERR_INVALID_ARG;
+  if (((uintptr_t)P & 15) != 0) return DM_ERR_INVALID_ARG;
+  const int64_t warps = (nv + kRowsPerWarp - 1) / kRowsPerWarp;
+  const int64_t blocks = (warps * 32 + kGemvThreads - 1) / kGemvThreads;
+  if (blocks > INT32_MAX) return DM_ERR_SIZE;
+  k_precond_gemv<<<(unsigned)blocks, kGemvThreads, 0, (cudaStream_t)stream>>>(P, nv, ldp, grad,
+                                                                             out);
+  count_launches(1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int dm_vector_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_norm_sq,
+                        int64_t nv, float lr, float beta1, float beta2, float eps, int64_t* step,
+                        dm_stream_t stream) {
+  if (nv < 0 || !step || (nv > 0 && (!param || !grad || !exp_avg || !exp_avg_norm_sq)))
+    return DM_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nv <= 4096) {
+    k_vector_adam<<<1, 1024, 0, st>>>(param, grad, exp_avg, exp_avg_norm_sq, nv, lr, beta1, beta2,
+                                      eps, step, 1);
+    count_launches(1);
+  } else {
+    const int64_t nb = std::min<int64_t>((nv + 255) / 256, 148 * 16);
+    k_vector_adam<<<(unsigned)nb, 256, 0, st>>>(param, grad, exp_avg, exp_avg_norm_sq, nv, lr,
+                                                beta1, beta2, eps, step, 0);
+    k_step_bump<<<1, 1, 0, st>>>(step);
+    count_launches(2);
+  }
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+}  // extern "C"

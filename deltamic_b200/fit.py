@@ -24,7 +24,8 @@ class FitStep:
     """
 
     def __init__(self, renderer: MeshRenderer, verts, faces, coeff, target=None, kind="mse",
-                 contrast=0.0, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True):
+                 contrast=0.0, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True,
+                 precond=None, optimizer="adam"):
         ops._check_mesh(verts, faces, coeff)
         if renderer.band is None:
             raise RuntimeError("set the renderer's OTF first")
@@ -36,8 +37,14 @@ class FitStep:
         self.kind = kind
         self.contrast = float(contrast)
         self.lr, self.betas, self.eps = float(lr), betas, float(eps)
+        if optimizer not in ("adam", "vector_adam"):
+            raise ValueError("optimizer must be 'adam' or 'vector_adam'")
+        self.optimizer = optimizer
+        self.precond = precond  # e.g. precond.LargeStepsPreconditioner: g <- (M M)^-1 g
         self.m = torch.zeros_like(verts)
-        self.v = torch.zeros_like(verts)
+        self.v = (torch.zeros_like(verts) if optimizer == "adam"
+                  else torch.zeros(verts.shape[0], dtype=verts.dtype, device=verts.device))
+        self.gpre = torch.zeros_like(verts) if precond is not None else None
         self.t = torch.zeros(1, dtype=torch.int64, device=verts.device)
         self.loss = torch.zeros(1, dtype=torch.float32, device=verts.device)
         self.grad = torch.zeros_like(verts)
@@ -66,8 +73,15 @@ class FitStep:
                                             otf=r.otf, scale=1.0 / r.numel, want_coeff=False,
                                             **cot)
         self.grad.copy_(gv)
-        ops.adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0],
-                      self.betas[1], self.eps)
+        if self.precond is not None:
+            gv = self.precond.apply(gv, out=self.gpre)
+        if self.optimizer == "adam":
+            ops.adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0],
+                          self.betas[1], self.eps)
+        else:
+            from .precond import vector_adam_step
+            vector_adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0],
+                             self.betas[1], self.eps)
 
     def _capture(self):
         state = [x.clone() for x in (self.V, self.m, self.v, self.t)]
@@ -113,7 +127,8 @@ def fit_mesh(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr
 
 
 def run_fit(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr=1e-3,
-            kind="mse", contrast=0.0, stop_at=None, graph=True):
+            kind="mse", contrast=0.0, stop_at=None, graph=True, precond=None,
+            optimizer="adam"):
     """Adam fit with per-step losses and device timing.
 
     Returns ``dict(verts, losses[steps_run], ms_total, steps_run, reached)``; with
@@ -121,7 +136,8 @@ def run_fit(renderer: MeshRenderer, verts0, faces, coeff, target, steps=300, lr=
     on the host every step, so the timing includes one small read per step).
     """
     V = verts0.detach().clone().contiguous()
-    step = FitStep(renderer, V, faces, coeff, target, kind, contrast, lr, graph=graph)
+    step = FitStep(renderer, V, faces, coeff, target, kind, contrast, lr, graph=graph,
+                   precond=precond, optimizer=optimizer)
     losses = torch.zeros(steps, device=V.device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()

@@ -295,6 +295,23 @@ int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg
                  dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Preconditioned fit (the reference notebook's gradient preconditioning,
+ * Examples/Gradient_Descent.ipynb cell 2: Verts.grad = solve(M@M, Verts.grad),
+ * M = I + lambda L from largesteps' compute_matrix; optimize.py:207-212 forms the
+ * same operator densely as inv(M) @ inv(M)).
+ * dm_precond_apply: out[nv,3] = P grad[nv,3] for a dense P[nv, ldp] (float32,
+ * row-major, ldp a multiple of 4 with zero padding, 16-byte aligned); out must
+ * not alias grad.
+ * dm_vector_adam_step: VectorAdam of optimize.py:215-258 (axis -1): per-vertex
+ * second moment exp_avg_norm_sq[nv] of the squared gradient norm; ``step`` is a
+ * DEVICE int64 counter that the call increments. */
+int dm_precond_apply(const float* P, int64_t nv, int64_t ldp, const float* grad, float* out,
+                     dm_stream_t stream);
+int dm_vector_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_norm_sq,
+                        int64_t nv, float lr, float beta1, float beta2, float eps, int64_t* step,
+                        dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Instrumentation (no counterpart in the reference, which has no profiling).
  * dm_launch_count: kernels this library has launched in the process (host-side
  * count; graph replays are not counted).
