@@ -621,9 +621,14 @@ __global__ void __launch_bounds__(kLineThreads)
       for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
     const int xb = w * n2 / 8, xe = (w + 1) * n2 / 8;
     for (int x = xb; x < xe; ++x) {
-      const float2* row = gzt + x * kLines + 4 * (lg ^ (x & 7));  // lines 4lg..4lg+3
-      const float4 g01 = *reinterpret_cast<const float4*>(row);
-      const float4 g23 = *reinterpret_cast<const float4*>(row + 2);
+      const int grp = lg ^ (x & 7);
+      const float2* row = gzt + x * kLines + 4 * grp;  // lines 4lg..4lg+3
+      // groups 4..7 read their second half first: the eight lanes of a quarter
+      // warp then cover all 32 banks in each of the two 16-byte loads
+      const int h = (grp >> 2) & 1;
+      const float4 ga = *reinterpret_cast<const float4*>(row + 2 * h);
+      const float4 gb = *reinterpret_cast<const float4*>(row + 2 - 2 * h);
+      const float4 g01 = h ? gb : ga, g23 = h ? ga : gb;
       const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
                             make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
 #pragma unroll

@@ -38,26 +38,39 @@ __global__ void __launch_bounds__(kGemvThreads)
 #pragma unroll
   for (int i = 0; i < kRowsPerWarp; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
   const int64_t nq = ldp / 4;  // 16-byte column groups per row
-  for (int64_t q = lane; q < nq; q += 32) {
-    const int64_t c = 4 * q;
-    float gv[12];
+  const int nrow = (int)min((int64_t)kRowsPerWarp, nv - r0);
+  // two column groups per lane and round: eight 16-byte row loads in flight
+  for (int64_t q0 = lane; q0 < nq; q0 += 64) {
+    float4 pr[2][kRowsPerWarp];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const bool live = c + k < nv;
-      gv[3 * k + 0] = live ? __ldg(g + 3 * (c + k) + 0) : 0.f;
-      gv[3 * k + 1] = live ? __ldg(g + 3 * (c + k) + 1) : 0.f;
-      gv[3 * k + 2] = live ? __ldg(g + 3 * (c + k) + 2) : 0.f;
-    }
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
-    for (int i = 0; i < kRowsPerWarp; ++i) {
-      if (r0 + i >= nv) break;
-      const float4 p = __ldcs(reinterpret_cast<const float4*>(P + (r0 + i) * ldp) + q);
-      const float pv[4] = {p.x, p.y, p.z, p.w};
+      for (int i = 0; i < kRowsPerWarp; ++i) {
+        const int64_t q = q0 + 32 * u;
+        pr[u][i] = (q < nq && i < nrow)
+                       ? __ldcs(reinterpret_cast<const float4*>(P + (r0 + i) * ldp) + q)
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int64_t c = 4 * (q0 + 32 * u);
+      float gv[12];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        acc[i][0] = fmaf(pv[k], gv[3 * k + 0], acc[i][0]);
-        acc[i][1] = fmaf(pv[k], gv[3 * k + 1], acc[i][1]);
-        acc[i][2] = fmaf(pv[k], gv[3 * k + 2], acc[i][2]);
+        const bool live = c + k < nv;
+        gv[3 * k + 0] = live ? __ldg(g + 3 * (c + k) + 0) : 0.f;
+        gv[3 * k + 1] = live ? __ldg(g + 3 * (c + k) + 1) : 0.f;
+        gv[3 * k + 2] = live ? __ldg(g + 3 * (c + k) + 2) : 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < kRowsPerWarp; ++i) {
+        const float pv[4] = {pr[u][i].x, pr[u][i].y, pr[u][i].z, pr[u][i].w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          acc[i][0] = fmaf(pv[k], gv[3 * k + 0], acc[i][0]);
+          acc[i][1] = fmaf(pv[k], gv[3 * k + 1], acc[i][1]);
+          acc[i][2] = fmaf(pv[k], gv[3 * k + 2], acc[i][2]);
+        }
       }
     }
   }
@@ -81,7 +94,7 @@ __global__ void __launch_bounds__(kGemvThreads)
 }
 
 // VectorAdam (optimize.py:215-258, axis -1) on nv 3-vectors; ``step`` is a device
-// counter, incremented by the single-block launch or by k_bump afterwards.
+// counter, incremented by the single-block launch or by k_step_bump afterwards.
 __global__ void k_vector_adam(float* __restrict__ p, const float* __restrict__ g,
                               float* __restrict__ m, float* __restrict__ v, int64_t nv, float lr,
                               float b1, float b2, float eps, int64_t* step, int bump) {
