@@ -12,7 +12,8 @@ synthetic mesh generators in ``deltamic_b200.mesh``.
 All compute runs in hand-written CUDA kernels of ``lib/libdeltamic_b200.so``
 behind a C ABI (``include/deltamic_b200.h``); there is no CPU fallback.
 """
-from .psf import generate_gaussian_psf, generate_gaussian_psf_from_sigma
+from .psf import (Gaussian_psf, generate_gaussian_psf, generate_gaussian_psf_from_sigma,
+                  otf_from_psf)
 from .render import (Fourier3dMesh, center_verts_in_box, compute_box_size,
                      compute_spatial_frequency_grid, normalize_tensor,
                      render_image_from_ftmesh)
@@ -21,5 +22,6 @@ from .pipeline import MeshRenderer
 __all__ = [
     "Fourier3dMesh", "generate_gaussian_psf", "generate_gaussian_psf_from_sigma",
     "render_image_from_ftmesh", "normalize_tensor", "compute_box_size",
-    "compute_spatial_frequency_grid", "center_verts_in_box", "MeshRenderer",
+    "compute_spatial_frequency_grid", "center_verts_in_box", "MeshRenderer", "Gaussian_psf",
+    "otf_from_psf",
 ]

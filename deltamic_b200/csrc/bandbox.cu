@@ -555,6 +555,7 @@ __global__ void __launch_bounds__(kLineThreads)
   const float mn = hdr->mn, mx = hdr->mx;
   const float rng = mx - mn;
   const float inv = 1.0f / (rng * (1.0f + contrast));
+  const float inv_rng = 1.0f / rng, inv_1c = 1.0f / (1.0f + contrast);
   const float nseg_inv = 1.0f / (float)s.nvox;
   double L = 0.0, dmn = 0.0, dmx = 0.0;
   // phase 1 mapping: warp w, lines 4w..4w+3; lane = 8 li + xi: line 4w+li, position
@@ -588,8 +589,10 @@ __global__ void __launch_bounds__(kLineThreads)
         if (live_line) {
           const float2 zi = zv[u];
           const float a = cabs2(zi);
-          const float uu = (a - mn) / rng;
-          const float nv = (uu + contrast) / (1.0f + contrast);
+          // reciprocals of the per-image constants instead of divisions (ulp-level
+          // differences from dm_image_loss)
+          const float uu = (a - mn) * inv_rng;
+          const float nv = contrast == 0.0f ? uu : (uu + contrast) * inv_1c;
           float gn;
           if (kind == 0) {
             L += nv;
@@ -602,7 +605,7 @@ __global__ void __launch_bounds__(kLineThreads)
           dmn += (double)gn * (-(1.0 - (double)uu));
           dmx += (double)gn * (-(double)uu);
           const float gg = gn * inv;
-          const float sc = a > 0.f ? gg / a : 0.f;
+          const float sc = a > 0.f ? __fdividef(gg, a) : 0.f;
           g = make_float2(sc * zi.x, sc * zi.y);
         }
         gzt[x * kLines + col] = g;

@@ -109,16 +109,34 @@ class MeshRenderer:
         torch.fft.ifftn(self.spec, out=self.z)
         return self.z.abs()
 
-    def loss(self, verts, faces, coeff, kind="sum", target=None, contrast=0.0, sigma=None):
-        """Differentiable loss of the normalised render (grads: verts, coeff, sigma)."""
+    def loss(self, verts, faces, coeff, kind="sum", target=None, contrast=0.0, sigma=None,
+             otf=None):
+        """Differentiable loss of the normalised render.
+
+        Gradients flow to verts, coeff, and either ``sigma`` (the renderer's OTF is
+        then the Gaussian OTF of sigma) or ``otf`` (any OTF tensor of box_shape,
+        e.g. ``psf.otf_from_psf(Gaussian_psf(...)())`` as in the reference notebook;
+        the narrow band follows it)."""
+        if sigma is not None and otf is not None:
+            raise ValueError("pass sigma or otf, not both")
         if sigma is not None:
             self.set_sigma(sigma)
         else:
             sigma = torch.zeros(0, device=self.device)
+        if otf is not None:
+            if tuple(otf.shape) != tuple(self.shape):
+                raise ValueError("otf must have shape box_shape")
+            key = (otf.data_ptr(), otf._version)
+            if key != getattr(self, "_otf_key", None) or self.otf is None:
+                self.set_otf(otf)
+                self._otf_key = key
+            otf_in = otf
+        else:
+            otf_in = torch.zeros(0, device=self.device)
         self._require_band()
         ops._check_mesh(verts, faces, coeff)
         self.tune(verts, faces, coeff)
-        return _RenderLoss.apply(verts.contiguous(), coeff.contiguous(), sigma, self,
+        return _RenderLoss.apply(verts.contiguous(), coeff.contiguous(), sigma, otf_in, self,
                                  faces.contiguous(), kind, target, float(contrast))
 
     def _require_band(self):
@@ -140,7 +158,8 @@ class MeshRenderer:
 
 class _RenderLoss(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, verts, coeff, sigma, r: MeshRenderer, faces, kind, target, contrast):
+    def forward(ctx, verts, coeff, sigma, otf_in, r: MeshRenderer, faces, kind, target,
+                contrast):
         ctx.bandbox = r.use_bandbox
         if ctx.bandbox:
             ft = ops.meshft_list(verts, faces, coeff, r.grid, r.band)
@@ -152,6 +171,7 @@ class _RenderLoss(torch.autograd.Function):
         ctx.save_for_backward(verts, coeff, faces, ft, g)
         ctx.r = r
         ctx.sigma_grad = sigma.numel() == 9 and ctx.needs_input_grad[2]
+        ctx.otf_grad = otf_in.numel() > 0 and ctx.needs_input_grad[3]
         return loss.view(())
 
     @staticmethod
@@ -165,11 +185,15 @@ class _RenderLoss(torch.autograd.Function):
             cot = dict(grad_grid=r.G)
         gv, gc, go = ops.meshft_backward_list(
             verts, faces, coeff, r.grid, r.band, ft, otf=r.otf, scale=1.0 / r.numel,
-            want_coeff=ctx.needs_input_grad[1], want_otf=ctx.sigma_grad, **cot)
+            want_coeff=ctx.needs_input_grad[1], want_otf=ctx.sigma_grad or ctx.otf_grad,
+            **cot)
         gv = gv * gl
         if gc is not None:
             gc = gc * gl
-        gs = None
+        gs = go_dense = None
         if ctx.sigma_grad:
             gs = ops.sigma_grad_dense(go, r.otf, *r.xi, band=r.band) * gl
-        return gv, gc, gs, None, None, None, None, None
+        if ctx.otf_grad:  # the OTF enters the render on the band only
+            go_dense = torch.zeros(r.shape, dtype=torch.float32, device=go.device)
+            go_dense.view(-1)[r.band.long()] = go * gl
+        return gv, gc, gs, go_dense, None, None, None, None, None

@@ -295,6 +295,19 @@ int dm_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg
                  dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * OTF of a spatial PSF (the notebook's OTF = |fftshift(fftn(PSF))|,
+ * Examples/Gradient_Descent.ipynb cell 2, PSF from psf.py:551-587), around the
+ * caller's 3-D FFT: dm_otf_from_spectrum writes otf[k] = |spectrum[k - n/2 mod n]|
+ * (fftshift and |.| fused); dm_otf_from_spectrum_backward writes
+ * grad_spectrum[j] = grad_otf[j + n/2 mod n] * spectrum[j] / |spectrum[j]|
+ * (0 where the spectrum is 0).  spectrum / grad_spectrum complex64 [n0,n1,n2]. */
+int dm_otf_from_spectrum(const float* spectrum, int32_t n0, int32_t n1, int32_t n2, float* otf,
+                         dm_stream_t stream);
+int dm_otf_from_spectrum_backward(const float* spectrum, const float* grad_otf, int32_t n0,
+                                  int32_t n1, int32_t n2, float* grad_spectrum,
+                                  dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Preconditioned fit (the reference notebook's gradient preconditioning,
  * Examples/Gradient_Descent.ipynb cell 2: Verts.grad = solve(M@M, Verts.grad),
  * M = I + lambda L from largesteps' compute_matrix; optimize.py:207-212 forms the
