@@ -136,6 +136,10 @@ struct BwdWs {
   XiRec* xrec;
   float* bpart;
   float* contrib;
+  int32_t* key_hist;    // [face_blks][256]
+  int32_t* key_first;   // [face_blks][256]
+  int32_t* face_order;  // [nt]
+  int32_t* face_slot;   // [nt]
   void* topo;
 };
 size_t bwd_layout(void* ws, const PlanTotals& t, BwdWs* out) {
@@ -148,6 +152,10 @@ size_t bwd_layout(void* ws, const PlanTotals& t, BwdWs* out) {
   w.xrec = c.take<XiRec>(t.nband);
   w.bpart = c.take<float>(t.bpart);
   w.contrib = c.take<float>(9 * t.nt);
+  w.key_hist = c.take<int32_t>(256 * t.face_blks);
+  w.key_first = c.take<int32_t>(256 * t.face_blks);
+  w.face_order = c.take<int32_t>(t.nt);
+  w.face_slot = c.take<int32_t>(t.nt);
   w.topo = c.base ? (void*)(c.base + c.off) : nullptr;
   c.off += topo_layout(nullptr, t.nv, t.nt, nullptr);
   if (out) *out = w;
@@ -488,7 +496,8 @@ int dm_batched_meshft_backward(const dm_batch* batch, const float* verts, const 
   return launch_backward(c, t, verts, faces, faces_coeff, w.recs, w.area_part, band_index,
                          (const float2*)grad_list, (const float2*)grad_grid, otf, grad_scale,
                          (const float2*)ft_list, w.xrec, w.s_part, w.bpart, w.contrib, tw.off,
-                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.err, st);
+                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.key_hist,
+                         w.key_first, w.face_order, w.face_slot, w.err, st);
 }
 
 int dm_batched_image_loss(const dm_batch* batch, const float* z, int kind, const float* target,
@@ -545,7 +554,8 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
   return launch_backward(c, t, verts, faces, faces_coeff, w.recs, w.area_part, band_index,
                          (const float2*)grad_list, (const float2*)grad_grid, otf, grad_scale,
                          (const float2*)ft_list, w.xrec, w.s_part, w.bpart, w.contrib, tw.off,
-                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.err, st);
+                         tw.ent, grad_verts, grad_coeff, grad_otf_band, w.key_hist,
+                         w.key_first, w.face_order, w.face_slot, w.err, st);
 }
 
 // ---------------------------------------------------------------------------

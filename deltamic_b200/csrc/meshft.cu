@@ -25,6 +25,7 @@
 namespace dm {
 
 constexpr int kBlk = 256;  // threads of the element-wise kernels
+constexpr int64_t kSortMinFaces = 1024;  // adjoint face order by size from this many faces
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -413,6 +414,7 @@ __device__ __forceinline__ void bwd_accumulate(BwdAcc& a, const float z[3], floa
 template <int F, int NT, int TX, int NS>
 __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
                                                   const XiRec* __restrict__ xrec,
+                                                  const int32_t* __restrict__ order,
                                                   float* __restrict__ bpart, int* err) {
   __shared__ __align__(128) XiRec sx[NS][TX];
   __shared__ __align__(8) uint64_t bar[NS];
@@ -432,8 +434,10 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
   for (int k = 0; k < F; ++k) {
     const int f = fb * NT * F + k * NT + threadIdx.x;
     fidx[k] = f;
-    // lanes past the last face evaluate a real face (never stored)
-    geom[k] = geom_from_rec(recs[d.f_off + min(f, d.nt - 1)]);
+    // lanes past the last face evaluate a real face (never stored); with a face
+    // order, slot f holds face order[f] (faces of similar size share a warp)
+    const int64_t slot = d.f_off + min(f, d.nt - 1);
+    geom[k] = geom_from_rec(recs[order ? (int64_t)order[slot] : slot]);
   }
 
   const int ntiles = (nx + TX - 1) / TX;
@@ -532,8 +536,8 @@ __global__ void k_bwd_face_epi(Cells cells, const float* __restrict__ verts,
                                const float* __restrict__ coeff,
                                const double* __restrict__ area_part,
                                const double* __restrict__ s_part,
-                               const float* __restrict__ bpart, float* __restrict__ contrib,
-                               float* __restrict__ grad_coeff) {
+                               const float* __restrict__ bpart, const int32_t* __restrict__ slot_of,
+                               float* __restrict__ contrib, float* __restrict__ grad_coeff) {
   __shared__ double sh[40];
   const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
   const CellDesc d = cell_get(cells, ci);
@@ -545,7 +549,7 @@ __global__ void k_bwd_face_epi(Cells cells, const float* __restrict__ verts,
   double q[10];
 #pragma unroll
   for (int i = 0; i < 10; ++i) q[i] = 0.0;
-  const float* p = bpart + d.bpart_off + f;
+  const float* p = bpart + d.bpart_off + (slot_of ? (int64_t)slot_of[gf] - d.f_off : f);
   for (int c = 0; c < d.bchunks; ++c) {
 #pragma unroll
     for (int i = 0; i < 10; ++i) q[i] += p[((int64_t)c * 10 + i) * d.nt];
@@ -610,6 +614,99 @@ __global__ void k_vertex_gather(int64_t nv_total, const int32_t* __restrict__ of
   grad_verts[3 * v + 0] = g0;
   grad_verts[3 * v + 1] = g1;
   grad_verts[3 * v + 2] = g2;
+}
+
+// ---------------------------------------------------------------------------
+// Face order for the adjoint: faces of each cell sorted by size (a stable
+// counting sort on 8 buckets per octave of the longest edge, in phase units).
+// In the adjoint a warp's lanes are faces at the same frequency; whether a pair
+// takes the series or the pivot path depends on the face's size, so a mesh whose
+// face sizes spread (a fit that crumples the surface) splits most warps over
+// both paths unless similar faces share a warp.  Slot f of a cell then holds face
+// order[f]; slot_of is the inverse.  Per-face sums keep their order, so only the
+// warp-uniform choice of the series coefficient set can change (both sets agree
+// to their truncation error).
+
+constexpr int kKeyBins = 256;
+
+__device__ __forceinline__ int face_size_key(const FaceRec& r) {
+  const float ab = r.hab[0] * r.hab[0] + r.hab[1] * r.hab[1] + r.hab[2] * r.hab[2];
+  const float bc = r.hbc[0] * r.hbc[0] + r.hbc[1] * r.hbc[1] + r.hbc[2] * r.hbc[2];
+  const float c0 = r.hab[0] + r.hbc[0], c1 = r.hab[1] + r.hbc[1], c2 = r.hab[2] + r.hbc[2];
+  const float ca = c0 * c0 + c1 * c1 + c2 * c2;
+  const float m = fmaxf(ab, fmaxf(bc, ca));
+  if (!(m > 0.f)) return 0;
+  const int k = (int)floorf(4.0f * log2f(m)) + kKeyBins / 2;  // 8 bins per octave of length
+  return min(max(k, 0), kKeyBins - 1);
+}
+
+// Per face block (the 256-face blocks of k_face_prep): key histogram.
+__global__ void k_face_key_hist(Cells cells, const FaceRec* __restrict__ recs,
+                                int32_t* __restrict__ hist) {
+  __shared__ int32_t h[kKeyBins];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  if (f < d.nt) atomicAdd(&h[face_size_key(recs[d.f_off + f])], 1);
+  __syncthreads();
+  hist[(int64_t)blockIdx.x * kKeyBins + threadIdx.x] = h[threadIdx.x];
+}
+
+// One CTA per cell (thread = bin): first slot of every (block, bin).
+__global__ void k_face_key_scan(Cells cells, const int32_t* __restrict__ hist,
+                                int32_t* __restrict__ first) {
+  __shared__ int32_t tot[kKeyBins];
+  const CellDesc d = cell_get(cells, blockIdx.x);
+  const int nblk = (d.nt + kBlk - 1) / kBlk;
+  const int k = threadIdx.x;
+  int32_t sum = 0;
+  for (int b = 0; b < nblk; ++b) sum += hist[(int64_t)(d.face_blk0 + b) * kKeyBins + k];
+  tot[k] = sum;
+  __syncthreads();
+  if (k == 0) {  // exclusive scan over the bins, in order
+    int32_t run = 0;
+    for (int i = 0; i < kKeyBins; ++i) {
+      const int32_t v = tot[i];
+      tot[i] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  int32_t run = (int32_t)d.f_off + tot[k];
+  for (int b = 0; b < nblk; ++b) {
+    const int64_t o = (int64_t)(d.face_blk0 + b) * kKeyBins + k;
+    first[o] = run;
+    run += hist[o];
+  }
+}
+
+// Per face block: stable slots (warps in order, lanes in order within a key).
+__global__ void k_face_key_scatter(Cells cells, const FaceRec* __restrict__ recs,
+                                   const int32_t* __restrict__ first, int32_t* __restrict__ order,
+                                   int32_t* __restrict__ slot_of) {
+  __shared__ int32_t base[kKeyBins];
+  const int ci = cell_find(cells, blockIdx.x, [](const CellDesc& d) { return d.face_blk0; });
+  const CellDesc d = cell_get(cells, ci);
+  base[threadIdx.x] = first[(int64_t)blockIdx.x * kKeyBins + threadIdx.x];
+  __syncthreads();
+  const int f = (blockIdx.x - d.face_blk0) * kBlk + threadIdx.x;
+  const bool live = f < d.nt;
+  const int key = live ? face_size_key(recs[d.f_off + f]) : -1 - (int)(threadIdx.x & 31);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned same = __match_any_sync(0xffffffffu, key);
+  const int rank = __popc(same & ((1u << lane) - 1u));
+  for (int w = 0; w < kBlk / 32; ++w) {
+    if (warp == w && live) {
+      const int32_t slot = base[key] + rank;
+      order[slot] = (int32_t)(d.f_off + f);
+      slot_of[d.f_off + f] = slot;
+    }
+    __syncthreads();
+    if (warp == w && live && rank == 0) base[key] += __popc(same);
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -818,7 +915,20 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
                     const float* otf, float grad_scale, const float2* ft_list, XiRec* xrec,
                     double* s_part, float* bpart, float* contrib, const int32_t* csr_off,
                     const int32_t* csr_ent, float* grad_verts, float* grad_coeff,
-                    float* grad_otf_band, int* err, cudaStream_t st) {
+                    float* grad_otf_band, int32_t* key_hist, int32_t* key_first,
+                    int32_t* face_order, int32_t* face_slot, int* err, cudaStream_t st) {
+  // face order by size (see k_face_key_hist); skipped for small meshes
+  const bool sort = face_order && t.nt >= kSortMinFaces;
+  if (sort) {
+    k_face_key_hist<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, recs, key_hist);
+    k_face_key_scan<<<(unsigned)std::max(c.n, 1), kKeyBins, 0, st>>>(c, key_hist, key_first);
+    k_face_key_scatter<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, recs, key_first, face_order,
+                                                               face_slot);
+    count_launches(3);
+    if (launch_status()) return DM_ERR_CUDA;
+  }
+  const int32_t* order = sort ? face_order : nullptr;
+  const int32_t* slot_of = sort ? face_slot : nullptr;
   k_bwd_band_prep<<<(unsigned)t.band_blks, kBlk, 0, st>>>(c, band_index, grad_list, grad_grid, otf,
                                                          grad_scale, ft_list, xrec, grad_otf_band,
                                                          s_part, err);
@@ -829,12 +939,12 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
     profile_begin(1, st);
     const unsigned g = (unsigned)t.bwd_items;
     switch (bwd_variant()) {
-      case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
-      case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, xrec, bpart, err); break;
-      case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, xrec, bpart, err); break;
-      case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
-      case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
-      default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, bpart, err); break;
+      case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
     }
     profile_end(1, st);
     count_launches(1);
@@ -843,7 +953,7 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
     cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)t.bpart, st);
   }
   k_bwd_face_epi<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, area_part, s_part,
-                                                        bpart, contrib, grad_coeff);
+                                                        bpart, slot_of, contrib, grad_coeff);
   count_launches(1);
   if (launch_status()) return DM_ERR_CUDA;
   if (t.nv > 0) {

@@ -56,7 +56,8 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
                     const float* otf, float grad_scale, const float2* ft_list, XiRec* xrec,
                     double* s_part, float* bpart, float* contrib, const int32_t* csr_off,
                     const int32_t* csr_ent, float* grad_verts, float* grad_coeff,
-                    float* grad_otf_band, int* err, cudaStream_t st);
+                    float* grad_otf_band, int32_t* key_hist, int32_t* key_first,
+                    int32_t* face_order, int32_t* face_slot, int* err, cudaStream_t st);
 int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, int32_t* count,
                     int32_t* off, int32_t* cursor, int32_t* ent, int* err, cudaStream_t st);
 
