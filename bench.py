@@ -48,7 +48,14 @@ BWD_FP32, BWD_MUFU = 80, 9
 # profiles/k_meshft_fit200.md): the kernel streams face records and frequency
 # tiles, far below its compute time at HBM speed.
 NCU_TRAFFIC_BWD = 3061248 + 577024
+# Surface + enclosed-volume transform (render.py:228-318): the complex weight
+# a_k + i beta xi.nor_k/|xi|^2 adds 5 FP32 ops per pair to the forward (the
+# normal's dot product and a second complex accumulate) and 18 to the adjoint
+# (weighted cotangent, F, and the three normal sums).
+VOL_FWD_FP32, VOL_BWD_FP32 = FWD_FP32 + 5, BWD_FP32 + 18
 METRIC = "meshFT face*xi pairs/s (fit step: fwd+bwd, 200^3, 20,480 faces)"
+METRIC_VOLUME = ("meshFT face*xi pairs/s (autofluorescence surface+volume transform: fwd+bwd, "
+                 "200^3, 20,480 faces)")
 METRIC_BATCH = "meshFT face*xi pairs/s (batched fit step: 64 cells, fwd+bwd)"
 
 
@@ -70,10 +77,12 @@ def parse():
                    help="fit300: precondition the vertex gradient with (M M)^-1, M = I + lambda L, "
                         "and step with VectorAdam (0: plain Adam, the configured fit)")
     p.add_argument("--precond-lr", type=float, default=5e-3)
-    p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned"],
+    p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned",
+                                           "volume200"],
                    default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
-                        "cells of mixed sizes per step")
+                        "cells of mixed sizes per step; volume200: forward + adjoint of "
+                        "the autofluorescence transform on the fit200 mesh and band")
     return p.parse_args()
 
 
@@ -180,11 +189,33 @@ def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=96, threads=None):
                       f"float64 numpy ({dt:.1f} s)"}
 
 
+def volume_cpu_baseline(gt_v, faces, band_xi, sample_xi=96, threads=None, regint=0.5):
+    """Oracle of the autofluorescence transform, forward + adjoint, on a sample of
+    the band (frequency chunks on a thread pool)."""
+    import oracle.volume as ov
+    threads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    sub = np.sort(rng.choice(len(band_xi), min(sample_xi, len(band_xi)), replace=False))
+    xi = band_xi[sub]
+    g = np.ones(len(xi), np.complex128)
+    chunk = max(len(faces), len(xi) * len(faces) // (4 * threads))
+    t0 = time.perf_counter()
+    ov.volume_forward(gt_v, faces, regint, xi, chunk_pairs=chunk, threads=threads)
+    ov.volume_backward(gt_v, faces, regint, xi, g, chunk_pairs=chunk, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": len(xi) * len(faces) / dt, "unit": "pairs/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{len(xi)} band frequencies x {len(faces)} faces, forward+adjoint, "
+                      f"float64 numpy ({dt:.1f} s)"}
+
+
 def run_reference(args, rank, world):
     """CPU reference arm (rank 0 only): the oracle port on a sample per step."""
     if rank != 0:
         return
     import oracle
+    if args.workload == "volume200":
+        return run_reference_volume(args)
     gt_v, init_v, faces, box = make_workload(0, args.small)
     axes = oracle.frequency_axes(box, SHAPE)
     otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
@@ -214,6 +245,188 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_volume(args):
+    """Reference arm of volume200: the oracle's restatement of the reference's
+    torch function (render.py:228-318) on a band sample per step."""
+    import oracle
+    gt_v, _, faces, box = make_workload(0, args.small)
+    L = box[:, 1] - box[:, 0]
+    axes = oracle.frequency_axes(np.stack([np.zeros(3), L], axis=1), SHAPE)
+    otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
+    idx = oracle.band_indices(otf, THRESH)
+    band_xi = oracle.xi_list_from_band(idx, axes)
+    per_step = 48
+    threads = os.cpu_count() or 1
+    vals = []
+    for k in range(args.warmup + args.steps):
+        r = volume_cpu_baseline(gt_v, faces, band_xi[k * per_step % len(band_xi):], per_step,
+                                threads)
+        if k >= args.warmup:
+            vals.append(r["value"])
+    value = float(np.mean(vals))
+    full_pairs = len(idx) * len(faces)
+    print(json.dumps({
+        "metric": METRIC_VOLUME, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_pairs / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "volume200: level-5 SH mesh, 200^3, OTF>1e-5 band",
+                   "n_faces": int(len(faces)), "n_band": int(len(idx)),
+                   "pairs_per_step": int(full_pairs), "parallelism": "replicas only"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_step} band frequencies x {len(faces)} faces per step"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def run_volume(args, rank, world, local):
+    """volume200: forward + adjoint of the autofluorescence transform on the fit200
+    mesh (20,480 faces) and band (200^3, OTF > 1e-5), regint 0.5, with a fixed
+    cotangent on the band (the adjoint of L = sum Re(conj(w) ft)).  value = face*xi
+    pairs per second; e2e runs fourier_from_mesh_narrowband_autofluorescence with
+    torch autograd from pinned host vertices to the host gradient."""
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from deltamic_b200 import (_native as N, compute_spatial_frequency_grid,
+                               fourier_from_mesh_narrowband_autofluorescence, generate_gaussian_psf,
+                               ops)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.lib()
+    gt_v, _, faces_np, box = make_workload(rank, args.small)
+    shape = (64, 64, 64) if args.small else SHAPE
+    L = box[:, 1] - box[:, 0]
+    xi = compute_spatial_frequency_grid(shape, L, device=dev, dtype=torch.float32)
+    otf = generate_gaussian_psf(torch.diag(torch.tensor(SIGMA, device=dev)), *xi).contiguous()
+    grid = ops.FreqGrid(np.stack([np.zeros(3), L], axis=1), shape)
+    band = ops.narrowband(otf, THRESH)
+    V = torch.tensor(gt_v, dtype=torch.float32, device=dev)
+    F = torch.tensor(faces_np, device=dev)
+    R = torch.tensor([0.5], device=dev)
+    gen = torch.Generator(device=dev).manual_seed(5 + rank)
+    w = torch.randn(band.numel(), 2, device=dev, generator=gen)
+    w = torch.view_as_complex(w.contiguous())
+    pairs = len(faces_np) * band.numel()
+    epairs = len(faces_np) * ops.band_eval_count(band)
+
+    def step():
+        ft, vol = ops.volume_list(V, F, R, grid, band)
+        return ops.volume_backward_list(V, F, R, grid, band, ft, vol, grad_list=w)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = lib.dm_launch_count()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = lib.dm_launch_count() - n0
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+
+    lib.dm_profile_enable(1)
+    for _ in range(10):
+        step()
+    torch.cuda.synchronize()
+    cnt, tot = N._INT(), N._F()
+    N.check(lib.dm_profile_read(1, cnt, tot), "dm_profile_read")
+    bwd_ms = tot.value / max(cnt.value, 1)
+    N.check(lib.dm_profile_read(0, cnt, tot), "dm_profile_read")
+    fwd_ms = tot.value / max(cnt.value, 1)
+    lib.dm_profile_enable(0)
+    peak_fma, peak_mufu = N.ctypes.c_double(), N.ctypes.c_double()
+    N.check(lib.dm_peak_probe(0, 4096, peak_fma, N.stream_ptr(dev)), "dm_peak_probe")
+    N.check(lib.dm_peak_probe(1, 2048, peak_mufu, N.stream_ptr(dev)), "dm_peak_probe")
+    fp32_bwd = epairs * VOL_BWD_FP32 / (bwd_ms * 1e-3)
+    mufu_bwd = epairs * BWD_MUFU / (bwd_ms * 1e-3)
+    frac_f, frac_m = fp32_bwd / peak_fma.value, mufu_bwd / peak_mufu.value
+    bound = "mufu" if frac_m >= frac_f else "fp32"
+    achieved = mufu_bwd if bound == "mufu" else fp32_bwd
+    peak = peak_mufu.value if bound == "mufu" else peak_fma.value
+
+    # end to end through the reference-facing function, host buffers in and out
+    host_v = torch.tensor(gt_v, dtype=torch.float32).pin_memory()
+    host_g = torch.empty_like(host_v).pin_memory()
+    host_l = torch.empty(1).pin_memory()
+    wd = torch.zeros(shape, dtype=torch.complex64, device=dev).reshape(-1)
+    wd[band.long()] = w
+    wd = wd.reshape(shape)
+    Vd = torch.empty(host_v.shape, dtype=torch.float32, device=dev)
+
+    def e2e_step():
+        Vd.copy_(host_v, non_blocking=True)
+        Vp = Vd.requires_grad_(True)
+        out = fourier_from_mesh_narrowband_autofluorescence(otf, THRESH, R[0], *xi, Vp, F)
+        loss = torch.sum(torch.real(torch.conj(wd) * out))
+        loss.backward()
+        host_g.copy_(Vp.grad, non_blocking=True)
+        host_l.copy_(loss.detach().view(1), non_blocking=True)
+        Vp.grad = None
+        Vd.requires_grad_(False)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        axes = oracle.frequency_axes(np.stack([np.zeros(3), L], axis=1), shape)
+        band_xi = oracle.xi_list_from_band(band.cpu().numpy().astype(np.int64), axes)
+        cpu = volume_cpu_baseline(gt_v, faces_np, band_xi)
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC_VOLUME, "value": pairs * world / (ms * 1e-3), "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded SH shape, seeded cotangent)",
+        "config": {"workload": "volume200: autofluorescence transform forward + adjoint, "
+                               "level-5 SH mesh, 200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5, "
+                               "regint 0.5",
+                   "n_verts": int(len(gt_v)), "n_faces": int(len(faces_np)),
+                   "n_band": int(band.numel()), "box_shape": list(shape),
+                   "pairs_per_step": int(pairs), "eval_pairs_per_step": int(epairs),
+                   "cuda_graph": False, "parallelism": "replicas only (one workload per GPU)",
+                   "l2_flush": "no: inputs are ~1 MB; the kernels are compute bound and "
+                               "read their face and frequency tiles once per launch"},
+        "gpu_launches": int(launches), "clocks": clk,
+        "e2e": {"value": pairs * world / (e2e_ms * 1e-3), "unit": "pairs/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(host_v.numel() * 4),
+                "d2h_bytes_per_step": int(host_g.numel() * 4 + 4)},
+        "roofline": {
+            "bound": bound, "kernel": "k_meshft_bwd<kVol> (adjoint)",
+            "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
+            "frac": achieved / peak,
+            "peak_source": "measured in this run by dm_peak_probe (MUFU sin / FP32 FMA chains)",
+            "traffic": None, "ops_per_pair": {"fp32": VOL_BWD_FP32, "mufu": BWD_MUFU},
+            "kernel_ms": bwd_ms, "fp32_frac": frac_f, "mufu_frac": frac_m,
+            "forward": {"kernel": "k_meshft_fwd<kVol>", "kernel_ms": fwd_ms,
+                        "fp32_frac": epairs * VOL_FWD_FP32 / (fwd_ms * 1e-3) / peak_fma.value,
+                        "mufu_frac": epairs * FWD_MUFU / (fwd_ms * 1e-3) / peak_mufu.value}},
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)
 
 
@@ -566,6 +779,8 @@ def main():
             run_fit300(args, rank, world, local)
         elif args.workload == "learned":
             run_learned(args, rank, world, local)
+        elif args.workload == "volume200":
+            run_volume(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

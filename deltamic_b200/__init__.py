@@ -3,7 +3,8 @@
 Drop-in names of the reference package (``from deltamic import ...``):
 ``Fourier3dMesh``, ``generate_gaussian_psf``, ``generate_gaussian_psf_from_sigma``,
 ``render_image_from_ftmesh``, ``normalize_tensor``, ``compute_box_size``,
-``compute_spatial_frequency_grid``, ``center_verts_in_box``.
+``compute_spatial_frequency_grid``, ``center_verts_in_box``,
+``fourier_from_mesh_narrowband_autofluorescence``.
 
 Beyond the reference: ``MeshRenderer`` (fused render + loss + adjoint),
 ``fit_mesh`` / ``FitStep`` (Adam fitting loop, CUDA-graph captured), and the
@@ -15,7 +16,10 @@ behind a C ABI (``include/deltamic_b200.h``); there is no CPU fallback.
 from .psf import (Gaussian_psf, generate_gaussian_psf, generate_gaussian_psf_from_sigma,
                   otf_from_psf)
 from .render import (Fourier3dMesh, center_verts_in_box, compute_box_size,
-                     compute_spatial_frequency_grid, normalize_tensor,
+                     compute_spatial_frequency_grid, compute_volume_manifold,
+                     fourier_from_mesh_narrowband_autofluorescence,
+                     get_internal_triangle_and_mesh_areas,
+                     get_internal_triangle_and_mesh_areas_and_normals, normalize_tensor,
                      render_image_from_ftmesh)
 from .pipeline import MeshRenderer
 
@@ -23,5 +27,7 @@ __all__ = [
     "Fourier3dMesh", "generate_gaussian_psf", "generate_gaussian_psf_from_sigma",
     "render_image_from_ftmesh", "normalize_tensor", "compute_box_size",
     "compute_spatial_frequency_grid", "center_verts_in_box", "MeshRenderer", "Gaussian_psf",
-    "otf_from_psf",
+    "otf_from_psf", "fourier_from_mesh_narrowband_autofluorescence",
+    "get_internal_triangle_and_mesh_areas", "get_internal_triangle_and_mesh_areas_and_normals",
+    "compute_volume_manifold",
 ]

@@ -206,6 +206,89 @@ void profile_end(int kind, cudaStream_t st) {
 }
 }  // namespace dm
 
+// Workspace plans of the surface + enclosed-volume transform (volume.cu).
+namespace {
+
+CellDesc volume_cell(const dm_box* b, int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
+  CellDesc d = single_cell(b, nv, nt, nband, t);
+  plan_volume(d, t);
+  return d;
+}
+
+// Part sizes of the larger of the full-band and half-band plans (no box).
+void volume_plan_any(int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
+  dm_box b;
+  memset(&b, 0, sizeof(b));
+  for (int k = 0; k < 3; ++k) {
+    b.hi[k] = 1.0;
+    b.shape[k] = 1;
+  }
+  PlanTotals a, h;
+  volume_cell(&b, nv, nt, nband, a);
+  b.band_flags = DM_BAND_HERMITIAN;
+  volume_cell(&b, nv, nt, nband, h);
+  t = a;
+  t.fpart = std::max(a.fpart, h.fpart);
+  t.bpart = std::max(a.bpart, h.bpart);
+}
+
+struct VolFwdWs {
+  int* err;
+  double* area_part;
+  double* det_part;
+  FaceRec* recs;
+  float4* vrec;
+  float2* fpart;
+};
+size_t vol_fwd_layout(void* ws, const PlanTotals& t, VolFwdWs* out) {
+  Carve c(ws);
+  VolFwdWs w;
+  w.err = c.take<int>(4);
+  w.area_part = c.take<double>(t.face_blks);
+  w.det_part = c.take<double>(t.face_blks);
+  w.recs = c.take<FaceRec>(t.nt);
+  w.vrec = c.take<float4>(t.nt);
+  w.fpart = c.take<float2>(t.fpart);
+  if (out) *out = w;
+  return c.off;
+}
+
+struct VolBwdWs {
+  int* err;
+  double* area_part;
+  double* det_part;
+  double* s_part;  // [3][band_blks]
+  FaceRec* recs;
+  float4* vrec;
+  float4* fw;
+  XiRec* xrec;
+  float4* xg;
+  float* bpart;
+  float* contrib;
+  void* topo;
+};
+size_t vol_bwd_layout(void* ws, const PlanTotals& t, VolBwdWs* out) {
+  Carve c(ws);
+  VolBwdWs w;
+  w.err = c.take<int>(4);
+  w.area_part = c.take<double>(t.face_blks);
+  w.det_part = c.take<double>(t.face_blks);
+  w.s_part = c.take<double>(3 * t.band_blks);
+  w.recs = c.take<FaceRec>(t.nt);
+  w.vrec = c.take<float4>(t.nt);
+  w.fw = c.take<float4>(t.nt);
+  w.xrec = c.take<XiRec>(t.nband);
+  w.xg = c.take<float4>(t.nband);
+  w.bpart = c.take<float>(t.bpart);
+  w.contrib = c.take<float>(9 * t.nt);
+  w.topo = c.base ? (void*)(c.base + c.off) : nullptr;
+  c.off += topo_layout(nullptr, t.nv, t.nt, nullptr);
+  if (out) *out = w;
+  return c.off;
+}
+
+}  // namespace
+
 extern "C" {
 
 int dm_profile_enable(int enable) {
@@ -556,6 +639,81 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
                          (const float2*)ft_list, w.xrec, w.s_part, w.bpart, w.contrib, tw.off,
                          tw.ent, grad_verts, grad_coeff, grad_otf_band, w.key_hist,
                          w.key_first, w.face_order, w.face_slot, w.err, st);
+}
+
+// ---------------------------------------------------------------------------
+// Surface + enclosed-volume transform (volume.cu).
+
+size_t dm_meshft_volume_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
+  if (!sizes_ok(nv, nt, n_band)) return 0;
+  PlanTotals t;
+  volume_plan_any(nv, nt, n_band, t);
+  return vol_fwd_layout(nullptr, t, nullptr);
+}
+
+int dm_meshft_volume_forward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                             const float* regint, const dm_box* box, const int32_t* band_index,
+                             int64_t n_band, const float* otf, float* ft_list, float* vol_list,
+                             float* grid, void* workspace, size_t ws_bytes,
+                             dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_band)) return DM_ERR_SIZE;
+  if (!box_ok(box) || !workspace || !regint) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces)) return DM_ERR_INVALID_ARG;
+  if (n_band > 0 && (!band_index || !ft_list || !vol_list)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_volume_forward_workspace_size(nv, nt, n_band)) return DM_ERR_WORKSPACE;
+  PlanTotals t;
+  const CellDesc d = volume_cell(box, nv, nt, n_band, t);
+  VolFwdWs w;
+  vol_fwd_layout(workspace, t, &w);
+  return launch_volume_forward(d, t, verts, faces, regint, band_index, otf, w.area_part,
+                               w.det_part, w.recs, w.vrec, w.fpart, (float2*)ft_list,
+                               (float2*)vol_list, (float2*)grid, w.err, (cudaStream_t)stream);
+}
+
+size_t dm_meshft_volume_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
+  if (!sizes_ok(nv, nt, n_band)) return 0;
+  PlanTotals t;
+  volume_plan_any(nv, nt, n_band, t);
+  return vol_bwd_layout(nullptr, t, nullptr);
+}
+
+int dm_meshft_volume_backward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                              const float* regint, const dm_box* box, const int32_t* band_index,
+                              int64_t n_band, const float* grad_list, const float* grad_grid,
+                              const float* otf, float grad_scale, const float* ft_list,
+                              const float* vol_list, const void* topology, float* grad_verts,
+                              float* grad_regint, void* workspace, size_t ws_bytes,
+                              dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_band)) return DM_ERR_SIZE;
+  if (!box_ok(box) || !workspace || !regint) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces)) return DM_ERR_INVALID_ARG;
+  if (nv > 0 && !grad_verts) return DM_ERR_INVALID_ARG;
+  if (n_band > 0 && (!band_index || !ft_list || !vol_list || (!grad_list && !grad_grid)))
+    return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_volume_backward_workspace_size(nv, nt, n_band))
+    return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PlanTotals t;
+  const CellDesc d = volume_cell(box, nv, nt, n_band, t);
+  VolBwdWs w;
+  vol_bwd_layout(workspace, t, &w);
+  const void* topo = topology;
+  if (!topo) {
+    TopoWs tw;
+    topo_layout(w.topo, nv, nt, &tw);
+    int s = launch_topology(one_cell(d), t, faces, tw.count, tw.off, tw.cursor, tw.ent, w.err,
+                            st);
+    if (s) return s;
+    topo = w.topo;
+  }
+  TopoWs tw;
+  topo_layout(const_cast<void*>(topo), nv, nt, &tw);
+  return launch_volume_backward(d, t, verts, faces, regint, band_index,
+                                (const float2*)grad_list, (const float2*)grad_grid, otf,
+                                grad_scale, (const float2*)ft_list, (const float2*)vol_list,
+                                w.area_part, w.det_part, w.s_part, w.recs, w.vrec, w.fw, w.xrec,
+                                w.xg, w.bpart, w.contrib, tw.off, tw.ent, grad_verts,
+                                grad_regint, w.err, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,16 +1,9 @@
-// meshFT forward / backward kernels for sm_100a.
-//
-// Work decomposition (see the launch plans at the end of this file):
-//  * forward: item = (cell, frequency tile of NT*R, face split).  Each thread
-//    owns R band frequencies and loops over the faces of its split; face records
-//    are staged in shared memory by the bulk-copy engine in a ring of NS tiles
-//    and read as broadcasts.  Partial sums per (split, frequency) go to HBM and
-//    the epilogue adds them in a fixed order -> deterministic, no atomics.
-//  * backward: item = (cell, face block of NT*F, frequency chunk).  Each thread
-//    owns F faces (geometry and 10 accumulators in registers) and loops over the
-//    frequencies of its chunk, staged in shared memory the same way.  Per-face
-//    partials go to HBM; the face epilogue reduces chunks in a fixed order and a
-//    CSR gather sums face contributions per vertex in a fixed order.
+// meshFT forward / backward for sm_100a: face records, epilogues, the adjoint's
+// face order, the vertex <- face CSR, and the launch plans.  The main kernels
+// (k_meshft_fwd, k_meshft_bwd) and their work decomposition are in
+// meshft_kernels.cuh.  Partial sums go to HBM and are reduced in a fixed order
+// (deterministic, no atomics); a CSR gather sums face contributions per vertex
+// in a fixed order.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -20,75 +13,12 @@
 
 #include "dm_common.cuh"
 #include "meshft_internal.h"
+#include "meshft_kernels.cuh"
 #include "pair_math.cuh"
 
 namespace dm {
 
-constexpr int kBlk = 256;  // threads of the element-wise kernels
 constexpr int64_t kSortMinFaces = 1024;  // adjoint face order by size from this many faces
-
-// ---------------------------------------------------------------------------
-// helpers
-
-__device__ __forceinline__ void band_to_m(int32_t idx, const CellDesc& d, int32_t mi[3]) {
-  const int32_t n12 = d.n[1] * d.n[2];
-  const int32_t k0 = idx / n12;
-  const int32_t rem = idx - k0 * n12;
-  const int32_t k1 = rem / d.n[2];
-  const int32_t k2 = rem - k1 * d.n[2];
-  mi[0] = 2 * k0 - (d.n[0] - 1);
-  mi[1] = 2 * k1 - (d.n[1] - 1);
-  mi[2] = 2 * k2 - (d.n[2] - 1);
-}
-
-__device__ __forceinline__ FaceGeom geom_from_rec(const FaceRec& r) {
-  FaceGeom g;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    g.Ua[d] = r.Ua[d];
-    g.Ub[d] = r.Ub[d];
-    g.Uc[d] = r.Uc[d];
-    g.hab[d] = r.hab[d];
-    g.hbc[d] = r.hbc[d];
-  }
-  return g;
-}
-
-__device__ __forceinline__ void load_rec_shared(const FaceRec* p, FaceRec& r) {
-  const uint4* q = reinterpret_cast<const uint4*>(p);
-  uint4* o = reinterpret_cast<uint4*>(&r);
-  o[0] = q[0];
-  o[1] = q[1];
-  o[2] = q[2];
-  o[3] = q[3];
-}
-
-// Block-wide sum in double (fixed order), result valid in thread 0.
-__device__ double block_sum_d(double v, double* sh) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-    for (int i = 0; i < nw; ++i) r += sh[i];
-  }
-  __syncthreads();
-  return r;
-}
-
-// Sum of ``n`` doubles (fixed order), broadcast to the whole block.
-__device__ double block_sum_list(const double* p, int n, double* sh) {
-  double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
-  double r = block_sum_d(v, sh);
-  if (threadIdx.x == 0) sh[32] = r;
-  __syncthreads();
-  r = sh[32];
-  __syncthreads();
-  return r;
-}
 
 // ---------------------------------------------------------------------------
 // Face records and per-block sums of area * coeff (replaces the host loops of
@@ -136,7 +66,7 @@ __global__ void k_face_prep(Cells cells, const float* __restrict__ verts,
     const double cx = e1[1] * e2[2] - e1[2] * e2[1];
     const double cy = e1[2] * e2[0] - e1[0] * e2[2];
     const double cz = e1[0] * e2[1] - e1[1] * e2[0];
-    ac = 0.5 * sqrt(cx * cx + cy * cy + cz * cz) * (double)coeff[gf];
+    ac = 0.5 * sqrt(cx * cx + cy * cy + cz * cz) * (coeff ? (double)coeff[gf] : 1.0);
     r.area_coeff = (float)ac;
     recs[gf] = r;
   }
@@ -144,123 +74,6 @@ __global__ void k_face_prep(Cells cells, const float* __restrict__ verts,
   if (threadIdx.x == 0) area_part[blockIdx.x] = s;
 }
 
-// ---------------------------------------------------------------------------
-// Forward main kernel.
-
-template <int R>
-__device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const XiVal (&xv)[R],
-                                         float2 (&acc)[R]) {
-  uint32_t spm = 0;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    c32 F;
-    if (pair_forward(xv[r], g, F)) {
-      acc[r].x += ac * F.x;
-      acc[r].y += ac * F.y;
-    } else {
-      spm |= 1u << r;
-    }
-  }
-  if (spm) {
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if ((spm >> r) & 1u) {
-        const c32 F = pair_forward_degenerate(xv[r], g);
-        acc[r].x += ac * F.x;
-        acc[r].y += ac * F.y;
-      }
-    }
-  }
-}
-
-template <int R, int NT, int TF, int NS>
-__global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* __restrict__ recs,
-                                                  const int32_t* __restrict__ band_index,
-                                                  float2* __restrict__ fpart, int* err) {
-  __shared__ __align__(128) FaceRec sf[NS][TF];
-  __shared__ __align__(8) uint64_t bar[NS];
-  const int item = blockIdx.x;
-  const int ci = cell_find(cells, item, [](const CellDesc& d) { return d.fwd_item0; });
-  const CellDesc d = cell_get(cells, ci);
-  const int local = item - d.fwd_item0;
-  const int xt = local % d.xtiles;
-  const int split = local / d.xtiles;
-  const int f0 = split * d.fchunk;
-  const int nf = min(d.nt, f0 + d.fchunk) - f0;
-  if (d.ne <= 0) return;
-  if (nf <= 0) {  // no faces: the partial sums are zero
-    for (int r = 0; r < R; ++r) {
-      const int m = xt * NT * R + r * NT + threadIdx.x;
-      if (m < d.ne) fpart[d.fpart_off + (int64_t)split * d.ne + m] = make_float2(0.f, 0.f);
-    }
-    return;
-  }
-
-  XiVal xv[R];
-  int mloc[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int m = xt * NT * R + r * NT + threadIdx.x;
-    mloc[r] = m;
-    // lanes past the band evaluate a real frequency so every lane takes the
-    // same branches; their sums are never stored
-    const int mm = min(m, d.ne - 1);
-    band_to_m(band_index[d.b_off + mm], d, xv[r].mi);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) xv[r].mf[k] = (float)xv[r].mi[k];
-  }
-
-  const int ntiles = (nf + TF - 1) / TF;
-  const FaceRec* src0 = recs + d.f_off + f0;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < NS && s < ntiles; ++s) {
-      const uint32_t bytes = (uint32_t)min(TF, nf - s * TF) * (uint32_t)sizeof(FaceRec);
-      mbar_expect_tx(&bar[s], bytes);
-      bulk_g2s(&sf[s][0], src0 + s * TF, bytes, &bar[s]);
-    }
-  }
-
-  float2 acc[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r] = make_float2(0.f, 0.f);
-
-  for (int t = 0; t < ntiles; ++t) {
-    const int s = t % NS;
-    if (!mbar_wait_bounded(&bar[s], (uint32_t)((t / NS) & 1), err)) return;
-    const int nft = min(TF, nf - t * TF);
-    float2 tacc[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) tacc[r] = make_float2(0.f, 0.f);
-    for (int j = 0; j < nft; ++j) {
-      FaceRec fr;
-      load_rec_shared(&sf[s][j], fr);
-      fwd_face<R>(geom_from_rec(fr), fr.area_coeff, xv, tacc);
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      acc[r].x += tacc[r].x;
-      acc[r].y += tacc[r].y;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && t + NS < ntiles) {
-      fence_proxy_async();
-      const int tn = t + NS;
-      const uint32_t bytes = (uint32_t)min(TF, nf - tn * TF) * (uint32_t)sizeof(FaceRec);
-      mbar_expect_tx(&bar[s], bytes);
-      bulk_g2s(&sf[s][0], src0 + tn * TF, bytes, &bar[s]);
-    }
-  }
-  float2* out = fpart + d.fpart_off + (int64_t)split * d.ne;
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-    if (mloc[r] < d.ne) out[mloc[r]] = acc[r];
-}
 
 // ft_list = (2/M) * sum over splits; optional scatter of ft * OTF into the grid.
 // With a mirrored band (herm) the entries past ne are conj of their mirrors.
@@ -325,21 +138,6 @@ __global__ void k_meshft_fwd_epi(Cells cells, const int32_t* __restrict__ band_i
 // record of entry m < ne carries g(xi) + conj(g(-xi)): the adjoint of
 // ft(-xi) = conj(ft(xi)).
 
-// Cotangent of band entry gm (0 for an invalid voxel index).
-__device__ __forceinline__ float2 band_cotangent(const CellDesc& d, int64_t gm, int32_t idx,
-                                                 bool ok, const float2* __restrict__ grad_list,
-                                                 const float2* __restrict__ grad_grid,
-                                                 const float* __restrict__ otf,
-                                                 float grad_scale, float2& G) {
-  if (!ok) {
-    G = make_float2(0.f, 0.f);
-    return G;
-  }
-  G = grad_list ? grad_list[gm] : grad_grid[d.grid_off + idx];
-  const float gs = grad_scale * (otf ? otf[d.grid_off + idx] : 1.0f);
-  return make_float2(gs * G.x, gs * G.y);
-}
-
 __global__ void k_bwd_band_prep(Cells cells, const int32_t* __restrict__ band_index,
                                 const float2* __restrict__ grad_list,
                                 const float2* __restrict__ grad_grid,
@@ -395,136 +193,6 @@ __global__ void k_bwd_band_prep(Cells cells, const int32_t* __restrict__ band_in
   if (threadIdx.x == 0) s_part[blockIdx.x] = t;
 }
 
-// Backward main kernel.
-struct BwdAcc {
-  float q[10];  // q[3v+j] = sum z_v m_j (v = a,b,c), q[9] = sum Re(conj(g) F)
-};
-
-__device__ __forceinline__ void bwd_accumulate(BwdAcc& a, const float z[3], float r,
-                                               const float mf[3]) {
-#pragma unroll
-  for (int v = 0; v < 3; ++v) {
-    a.q[3 * v + 0] += z[v] * mf[0];
-    a.q[3 * v + 1] += z[v] * mf[1];
-    a.q[3 * v + 2] += z[v] * mf[2];
-  }
-  a.q[9] += r;
-}
-
-template <int F, int NT, int TX, int NS>
-__global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
-                                                  const XiRec* __restrict__ xrec,
-                                                  const int32_t* __restrict__ order,
-                                                  float* __restrict__ bpart, int* err) {
-  __shared__ __align__(128) XiRec sx[NS][TX];
-  __shared__ __align__(8) uint64_t bar[NS];
-  const int item = blockIdx.x;
-  const int ci = cell_find(cells, item, [](const CellDesc& d) { return d.bwd_item0; });
-  const CellDesc d = cell_get(cells, ci);
-  const int local = item - d.bwd_item0;
-  const int fb = local % d.fblocks;
-  const int chunk = local / d.fblocks;
-  const int x0 = chunk * d.bxchunk;
-  const int nx = min(d.ne, x0 + d.bxchunk) - x0;
-  if (nx <= 0 || d.nt <= 0) return;
-
-  FaceGeom geom[F];
-  int fidx[F];
-#pragma unroll
-  for (int k = 0; k < F; ++k) {
-    const int f = fb * NT * F + k * NT + threadIdx.x;
-    fidx[k] = f;
-    // lanes past the last face evaluate a real face (never stored); with a face
-    // order, slot f holds face order[f] (faces of similar size share a warp)
-    const int64_t slot = d.f_off + min(f, d.nt - 1);
-    geom[k] = geom_from_rec(recs[order ? (int64_t)order[slot] : slot]);
-  }
-
-  const int ntiles = (nx + TX - 1) / TX;
-  const XiRec* src0 = xrec + d.b_off + x0;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < NS && s < ntiles; ++s) {
-      const uint32_t bytes = (uint32_t)min(TX, nx - s * TX) * (uint32_t)sizeof(XiRec);
-      mbar_expect_tx(&bar[s], bytes);
-      bulk_g2s(&sx[s][0], src0 + s * TX, bytes, &bar[s]);
-    }
-  }
-
-  BwdAcc acc[F];
-#pragma unroll
-  for (int k = 0; k < F; ++k)
-#pragma unroll
-    for (int i = 0; i < 10; ++i) acc[k].q[i] = 0.f;
-
-  for (int t = 0; t < ntiles; ++t) {
-    const int s = t % NS;
-    if (!mbar_wait_bounded(&bar[s], (uint32_t)((t / NS) & 1), err)) return;
-    const int nxt = min(TX, nx - t * TX);
-    BwdAcc tacc[F];
-#pragma unroll
-    for (int k = 0; k < F; ++k)
-#pragma unroll
-      for (int i = 0; i < 10; ++i) tacc[k].q[i] = 0.f;
-    for (int j = 0; j < nxt; ++j) {
-      const uint4* q = reinterpret_cast<const uint4*>(&sx[s][j]);
-      const uint4 w0 = q[0], w1 = q[1];
-      XiVal xv;
-      xv.mi[0] = (int32_t)w0.x;
-      xv.mi[1] = (int32_t)w0.y;
-      xv.mi[2] = (int32_t)w0.z;
-      const float gre = __uint_as_float(w0.w);
-      xv.mf[0] = __uint_as_float(w1.x);
-      xv.mf[1] = __uint_as_float(w1.y);
-      xv.mf[2] = __uint_as_float(w1.z);
-      const float gim = __uint_as_float(w1.w);
-      uint32_t spm = 0;
-#pragma unroll
-      for (int k = 0; k < F; ++k) {
-        float z[3], r;
-        if (pair_adjoint(xv, geom[k], gre, gim, z, r))
-          bwd_accumulate(tacc[k], z, r, xv.mf);
-        else
-          spm |= 1u << k;
-      }
-      if (spm) {
-#pragma unroll
-        for (int k = 0; k < F; ++k) {
-          if ((spm >> k) & 1u) {
-            float z[3], r;
-            pair_adjoint_degenerate(xv, geom[k], gre, gim, z, r);
-            bwd_accumulate(tacc[k], z, r, xv.mf);
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < F; ++k)
-#pragma unroll
-      for (int i = 0; i < 10; ++i) acc[k].q[i] += tacc[k].q[i];
-    __syncthreads();
-    if (threadIdx.x == 0 && t + NS < ntiles) {
-      fence_proxy_async();
-      const int tn = t + NS;
-      const uint32_t bytes = (uint32_t)min(TX, nx - tn * TX) * (uint32_t)sizeof(XiRec);
-      mbar_expect_tx(&bar[s], bytes);
-      bulk_g2s(&sx[s][0], src0 + tn * TX, bytes, &bar[s]);
-    }
-  }
-  float* out = bpart + d.bpart_off + (int64_t)chunk * 10 * d.nt;
-#pragma unroll
-  for (int k = 0; k < F; ++k) {
-    if (fidx[k] < d.nt) {
-#pragma unroll
-      for (int i = 0; i < 10; ++i) out[(int64_t)i * d.nt + fidx[k]] = acc[k].q[i];
-    }
-  }
-}
 
 // Per-face epilogue: reduce chunks, then
 //   contrib[f][v][j] = trisar * (pi/L_j) * Q[v][j] + (c/M)(2r - s) dA/dv_j
@@ -824,8 +492,10 @@ void set_band_half(CellDesc& d, bool herm) {
 }
 
 void plan_cell_tiles(CellDesc& d) {
-  const FwdVariant fv = kFwdVariants[fwd_variant()];
-  const BwdVariant bv = kBwdVariants[bwd_variant()];
+  plan_cell_tiles_for(d, kFwdVariants[fwd_variant()], kBwdVariants[bwd_variant()]);
+}
+
+void plan_cell_tiles_for(CellDesc& d, const FwdVariant& fv, const BwdVariant& bv) {
   const int64_t xtile = (int64_t)fv.NT * fv.R;
   d.xtiles = (int32_t)std::max<int64_t>(1, cdiv(d.ne, xtile));
   int64_t fsplit = std::max<int64_t>(1, cdiv((int64_t)num_sms() * fv.waves, d.xtiles));
@@ -890,12 +560,12 @@ int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
     profile_begin(0, st);
     const unsigned g = (unsigned)t.fwd_items;
     switch (fwd_variant()) {
-      case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
-      case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, band_index, fpart, err); break;
-      case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, band_index, fpart, err); break;
-      case 4: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
-      case 5: k_meshft_fwd<2, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, band_index, fpart, err); break;
-      default: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, band_index, fpart, err); break;
+      case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      case 4: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      case 5: k_meshft_fwd<2, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      default: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
     }
     profile_end(0, st);
     count_launches(1);
@@ -939,12 +609,12 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
     profile_begin(1, st);
     const unsigned g = (unsigned)t.bwd_items;
     switch (bwd_variant()) {
-      case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
-      case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, xrec, order, bpart, err); break;
-      case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, xrec, order, bpart, err); break;
-      case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
-      case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
-      default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, xrec, order, bpart, err); break;
+      case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
     }
     profile_end(1, st);
     count_launches(1);
@@ -959,6 +629,16 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
   if (t.nv > 0) {
     k_vertex_gather<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, csr_off, csr_ent, contrib,
                                                                 grad_verts);
+    count_launches(1);
+  }
+  return launch_status();
+}
+
+int launch_vertex_gather(int64_t nv, const int32_t* csr_off, const int32_t* csr_ent,
+                         const float* contrib, float* grad_verts, cudaStream_t st) {
+  if (nv > 0) {
+    k_vertex_gather<<<(unsigned)cdiv(nv, kBlk), kBlk, 0, st>>>(nv, csr_off, csr_ent, contrib,
+                                                              grad_verts);
     count_launches(1);
   }
   return launch_status();

@@ -42,6 +42,7 @@ void profile_begin(int kind, cudaStream_t st);
 void profile_end(int kind, cudaStream_t st);
 void set_band_half(CellDesc& d, bool herm);
 void plan_cell_tiles(CellDesc& d);
+void plan_cell_tiles_for(CellDesc& d, const FwdVariant& fv, const BwdVariant& bv);
 void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t);
 
 int launch_face_prep(const Cells& c, const PlanTotals& t, const float* verts, const int64_t* faces,
@@ -58,6 +59,25 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
                     const int32_t* csr_ent, float* grad_verts, float* grad_coeff,
                     float* grad_otf_band, int32_t* key_hist, int32_t* key_first,
                     int32_t* face_order, int32_t* face_slot, int* err, cudaStream_t st);
+int launch_vertex_gather(int64_t nv, const int32_t* csr_off, const int32_t* csr_ent,
+                         const float* contrib, float* grad_verts, cudaStream_t st);
+
+// Surface + enclosed-volume transform (volume.cu): fixed tile shapes; plan_volume
+// re-plans a single cell and sets t's part sizes and item counts for them.
+void plan_volume(CellDesc& d, PlanTotals& t);
+int launch_volume_forward(const CellDesc& d, const PlanTotals& t, const float* verts,
+                          const int64_t* faces, const float* regint, const int32_t* band_index,
+                          const float* otf, double* area_part, double* det_part, FaceRec* recs,
+                          float4* vrec, float2* fpart, float2* ft_list, float2* vol_list,
+                          float2* grid, int* err, cudaStream_t st);
+int launch_volume_backward(const CellDesc& d, const PlanTotals& t, const float* verts,
+                           const int64_t* faces, const float* regint, const int32_t* band_index,
+                           const float2* grad_list, const float2* grad_grid, const float* otf,
+                           float grad_scale, const float2* ft_list, const float2* vol_list,
+                           double* area_part, double* det_part, double* s_part, FaceRec* recs,
+                           float4* vrec, float4* fw, XiRec* xrec, float4* xg, float* bpart,
+                           float* contrib, const int32_t* csr_off, const int32_t* csr_ent,
+                           float* grad_verts, float* grad_regint, int* err, cudaStream_t st);
 int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, int32_t* count,
                     int32_t* off, int32_t* cursor, int32_t* ent, int* err, cudaStream_t st);
 

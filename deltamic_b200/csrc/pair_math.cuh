@@ -457,10 +457,11 @@ DM_HD bool pair_forward(const XiVal& xv, const FaceGeom& g, c32& F) {
   return true;
 }
 
-// Adjoint: z_v = Re(conj(g) dF/dx_v) and r = Re(conj(g) F) for cotangent g;
-// returns false for a degenerate pair (outputs undefined).
-DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
-                        float& r) {
+// Adjoint: z_v = Re(conj(g) dF/dx_v) and r = Re(conj(g) F) for cotangent g, and
+// F itself if kF; returns false for a degenerate pair (outputs undefined).
+template <bool kF>
+DM_HD bool pair_adjoint_t(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
+                          float& r, c32& Fo) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
   const int cls = pair_class(hab, hbc, hca);
@@ -475,6 +476,7 @@ DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim
     const float hx = gre * E.x + gim * E.y;  // h = conj(g) E
     const float hy = gre * E.y - gim * E.x;
     r = hx * H.x - hy * H.y;
+    if (kF) Fo = cmul(E, H);
     const float zt = (hx * H.y + hy * H.x) * (1.0f / 3.0f);
     const float r1 = 2.0f * (hx * Hp2.x - hy * Hp2.y);
     const float r2 = hx * Hp3.x - hy * Hp3.y;
@@ -489,6 +491,7 @@ DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim
     const float hx = gre * E.x + gim * E.y;
     const float hy = gre * E.y - gim * E.x;
     r = hx * G.x - hy * G.y;
+    if (kF) Fo = cmul(E, G);
     const float zt = hx * G.y + hy * G.x;  // Re(conj(g) (-i F))
     const float zu = hx * Gu.x - hy * Gu.y;
     const float zw = hx * Gw.x - hy * Gw.y;
@@ -500,15 +503,26 @@ DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim
   return true;
 }
 
-// Adjoint of a degenerate pair.
+DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
+                        float& r) {
+  c32 unused;
+  return pair_adjoint_t<false>(xv, g, gre, gim, z, r, unused);
+}
+
+// Adjoint of a degenerate pair (F returned as well).
 DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre, float gim,
-                                   float z[3], float& r) {
+                                   float z[3], float& r, c32& F) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
-  c32 F, dF[3];
+  c32 dF[3];
   pair_degenerate<true>(xv, g, hab, hbc, hca, F, dF);
   r = gre * F.x + gim * F.y;
   for (int v = 0; v < 3; ++v) z[v] = gre * dF[v].x + gim * dF[v].y;
+}
+DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre, float gim,
+                                   float z[3], float& r) {
+  c32 F;
+  pair_adjoint_degenerate(xv, g, gre, gim, z, r, F);
 }
 
 // Forward of a degenerate pair.

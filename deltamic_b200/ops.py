@@ -15,7 +15,8 @@ from . import _native as N
 
 __all__ = ["FreqGrid", "narrowband", "band_is_hermitian", "band_eval_count", "band_box",
            "topology", "meshft", "meshft_list",
-           "meshft_backward_list", "gaussian_otf", "image_loss", "adam_step"]
+           "meshft_backward_list", "volume_list", "volume_backward_list", "volume_ft",
+           "gaussian_otf", "image_loss", "adam_step"]
 
 
 class FreqGrid:
@@ -219,6 +220,87 @@ def meshft(verts, faces, coeff, grid: FreqGrid, band) -> torch.Tensor:
     """Differentiable dense meshFT (gradients for verts and coeff)."""
     _check_mesh(verts, faces, coeff)
     return _MeshFT.apply(verts.contiguous(), faces.contiguous(), coeff.contiguous(), grid, band)
+
+
+# ---------------------------------------------------------------------------
+# surface + enclosed-volume transform (render.py:228-318)
+
+def volume_list(verts, faces, regint, grid: FreqGrid, band, otf=None, spectrum=None):
+    """Forward of the surface + enclosed-volume transform: ``(ft_list, vol_list)``
+    (complex64 on the band); optionally scatters ft*otf into ``spectrum``.
+    ``regint`` is a one-element float32 CUDA tensor; ``grid`` has lower corner 0."""
+    lib = N.lib()
+    nv, nt, nb = verts.shape[0], faces.shape[0], band.numel()
+    ft = torch.empty(nb, dtype=torch.complex64, device=verts.device)
+    vol = torch.empty(nb, dtype=torch.complex64, device=verts.device)
+    ws = N.WORKSPACES.get("vol_fwd", lib.dm_meshft_volume_forward_workspace_size(nv, nt, nb),
+                          verts.device)
+    N.check(lib.dm_meshft_volume_forward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(regint), ctypes.byref(band_box(grid, band)),
+        N.ptr(band), nb, N.ptr(otf), N.ptr(ft), N.ptr(vol), N.ptr(spectrum), N.ptr(ws),
+        ws.numel(), N.stream_ptr(verts.device)), "dm_meshft_volume_forward")
+    return ft, vol
+
+
+def volume_backward_list(verts, faces, regint, grid: FreqGrid, band, ft, vol, grad_list=None,
+                         grad_grid=None, otf=None, scale=1.0, want_regint=True):
+    """Backward of :func:`volume_list`: ``(grad_verts, grad_regint[1] | None)``."""
+    lib = N.lib()
+    nv, nt, nb = verts.shape[0], faces.shape[0], band.numel()
+    gv = torch.empty_like(verts)
+    gr = torch.zeros(1, dtype=torch.float32, device=verts.device) if want_regint else None
+    topo = topology(faces, nv)
+    ws = N.WORKSPACES.get("vol_bwd", lib.dm_meshft_volume_backward_workspace_size(nv, nt, nb),
+                          verts.device)
+    N.check(lib.dm_meshft_volume_backward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(regint), ctypes.byref(band_box(grid, band)),
+        N.ptr(band), nb, N.ptr(grad_list), N.ptr(grad_grid), N.ptr(otf), float(scale),
+        N.ptr(ft), N.ptr(vol), N.ptr(topo), N.ptr(gv), N.ptr(gr), N.ptr(ws), ws.numel(),
+        N.stream_ptr(verts.device)), "dm_meshft_volume_backward")
+    return gv, gr
+
+
+class _VolumeFT(torch.autograd.Function):
+    """Dense surface + enclosed-volume transform: complex64 grid, ft on the band and
+    0 elsewhere (render.py:228-318); gradients for verts and regint."""
+
+    @staticmethod
+    def forward(ctx, verts, regint, faces, grid, band):
+        out = torch.zeros(grid.shape, dtype=torch.complex64, device=verts.device)
+        ft, vol = volume_list(verts, faces, regint, grid, band, spectrum=out)
+        ctx.save_for_backward(verts, regint, faces, band, ft, vol)
+        ctx.grid = grid
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        verts, regint, faces, band, ft, vol = ctx.saved_tensors
+        g = g.contiguous()
+        if g.dtype != torch.complex64:
+            g = g.to(torch.complex64)
+        gv, gr = volume_backward_list(verts, faces, regint, ctx.grid, band, ft, vol, grad_grid=g,
+                                      want_regint=ctx.needs_input_grad[1])
+        return gv, gr, None, None, None
+
+
+def volume_ft(verts, faces, regint, grid: FreqGrid, band) -> torch.Tensor:
+    """Differentiable dense surface + enclosed-volume transform (gradients for
+    ``verts`` and a tensor ``regint``).  ``grid`` must have lower corner 0: the
+    vertex coordinates enter as given."""
+    N.require_cuda(verts, "Verts", torch.float32)
+    N.require_cuda(faces, "Faces", torch.int64)
+    if verts.dim() != 2 or verts.shape[1] != 3:
+        raise ValueError("Verts must have shape [nv, 3]")
+    if faces.dim() != 2 or faces.shape[1] != 3:
+        raise ValueError("Faces must have shape [nt, 3]")
+    if np.any(grid.box_size[:, 0] != 0.0):
+        raise ValueError("the volume transform takes vertex coordinates as given: "
+                         "grid.box_size[:, 0] must be 0")
+    r = regint if isinstance(regint, torch.Tensor) else torch.tensor(float(regint))
+    if r.numel() != 1:
+        raise ValueError("regint must be a scalar")
+    r = r.to(device=verts.device, dtype=torch.float32).reshape(1)
+    return _VolumeFT.apply(verts.contiguous(), r, faces.contiguous(), grid, band)
 
 
 # ---------------------------------------------------------------------------

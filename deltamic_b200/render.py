@@ -9,14 +9,22 @@ Same names, arguments and results as the reference:
 * ``render_image_from_ftmesh`` (render.py:177-180), ``normalize_tensor``
   (render.py:5-6), ``compute_box_size`` (render.py:9-18),
   ``compute_spatial_frequency_grid`` (render.py:321-340), ``center_verts_in_box``
-  (render.py:343-355).
+  (render.py:343-355);
+* ``fourier_from_mesh_narrowband_autofluorescence`` (render.py:228-318): surface
+  plus enclosed-volume transform on the kernels of volume.cu, gradients for
+  Verts and regint; its helpers ``get_internal_triangle_and_mesh_areas``,
+  ``get_internal_triangle_and_mesh_areas_and_normals`` and
+  ``compute_volume_manifold`` (render.py:184-226) are plain torch as in the
+  reference.
 
 Differences, all deliberate: the module runs on CUDA only (``device='cpu'``
 raises -- there is no CPU fallback); the kernels compute in float32 (with the
 fixed-point phases their error against a float64 evaluation is ~1e-6), so a
 ``dtype=torch.float64`` module casts its inputs to float32 and returns a
 complex128 spectrum whose gradients flow back to the float64 inputs; the box
-used for the phases is kept in float64.
+used for the phases is kept in float64.  In the autofluorescence transform the
+reference's value at xi = 0 (grids with every axis odd) is 0/0 = NaN; here it is
+the limit of its volume term, ``1 - regint`` in all.
 """
 from __future__ import annotations
 
@@ -27,7 +35,10 @@ from torch import nn
 from . import ops
 
 __all__ = ["Fourier3dMesh", "render_image_from_ftmesh", "normalize_tensor",
-           "compute_box_size", "compute_spatial_frequency_grid", "center_verts_in_box"]
+           "compute_box_size", "compute_spatial_frequency_grid", "center_verts_in_box",
+           "get_internal_triangle_and_mesh_areas",
+           "get_internal_triangle_and_mesh_areas_and_normals", "compute_volume_manifold",
+           "fourier_from_mesh_narrowband_autofluorescence"]
 
 
 def normalize_tensor(t, contrast_variable=0):
@@ -136,3 +147,83 @@ class Fourier3dMesh(nn.Module):
             ft = ops.meshft(Verts.float(), Faces, Faces_coeff.float(), self.grid, self.band())
             return ft.to(torch.complex128)
         return ops.meshft(Verts, Faces, Faces_coeff, self.grid, self.band())
+
+
+# ---------------------------------------------------------------------------
+# Surface + enclosed-volume ("autofluorescence") transform
+
+def _heron(Verts, Faces):
+    pos = Verts[Faces]
+    ls = torch.norm(pos - pos[:, [2, 0, 1]], dim=2)
+    hp = ls.sum(dim=1) / 2
+    return pos, (hp * (hp - ls[:, 0]) * (hp - ls[:, 1]) * (hp - ls[:, 2])) ** 0.5
+
+
+def get_internal_triangle_and_mesh_areas(Verts, Faces):
+    """Heron areas of the faces and their sum (render.py:184-199)."""
+    _, trisar = _heron(Verts, Faces)
+    return trisar, trisar.sum()
+
+
+def get_internal_triangle_and_mesh_areas_and_normals(Verts, Faces):
+    """Heron areas, their sum and the unnormalised normals
+    ``p0 x p1 + p1 x p2 + p2 x p0`` (render.py:202-218)."""
+    pos, trisar = _heron(Verts, Faces)
+    nor = (torch.cross(pos[:, 0], pos[:, 1], dim=1) + torch.cross(pos[:, 1], pos[:, 2], dim=1)
+           + torch.cross(pos[:, 2], pos[:, 0], dim=1))
+    return trisar, trisar.sum(), nor
+
+
+def compute_volume_manifold(Verts, Faces):
+    """``-sum p0 . (p1 x p2) / 6`` (render.py:221-226)."""
+    c = Verts[Faces]
+    return -torch.sum(torch.sum(torch.cross(c[:, 1], c[:, 2], dim=1) * c[:, 0], dim=1)) / 6
+
+
+def _axis_length(x: torch.Tensor) -> float:
+    """Box length L of a centred axis ``(2k - (n-1)) pi / L`` (render.py:321-340)."""
+    v = x.detach().double().cpu().numpy().reshape(-1)
+    n = v.size
+    if n == 0:
+        raise ValueError("empty frequency axis")
+    if n == 1:
+        if v[0] != 0.0:
+            raise ValueError("a one-point frequency axis must be [0]")
+        return 1.0
+    s = (v[-1] - v[0]) / (2 * (n - 1))
+    k = 2 * np.arange(n) - (n - 1)
+    if not s > 0 or np.max(np.abs(v - k * s)) > 1e-5 * np.max(np.abs(v)):
+        raise ValueError("frequency axes must be centred grids (2k - (n-1)) pi / L, as "
+                         "compute_spatial_frequency_grid makes them")
+    return float(np.pi / s)
+
+
+_AUTO_BANDS: dict = {}
+
+
+def fourier_from_mesh_narrowband_autofluorescence(OTF, narrowband_thresh, regint, xi0, xi1,
+                                                  xi2, Verts, Faces):
+    """Dense surface + enclosed-volume spectrum (render.py:228-318): zero outside
+    ``OTF > narrowband_thresh``, and on the band
+    ``sum_k F_k (2 A_k / sum A + i (regint / regvol) xi . nor_k / |xi|^2)``.
+
+    Vertex coordinates enter as given.  Gradients flow to ``Verts`` and to
+    ``regint`` when it is a tensor.  A float64 ``Verts`` is evaluated in float32
+    and returns complex128, as ``Fourier3dMesh(dtype=float64)`` does."""
+    shape = (int(xi0.numel()), int(xi1.numel()), int(xi2.numel()))
+    if tuple(OTF.shape) != shape:
+        raise ValueError(f"OTF shape {tuple(OTF.shape)} does not match the axes {shape}")
+    L = [_axis_length(x) for x in (xi0, xi1, xi2)]
+    grid = ops.FreqGrid(np.array([[0.0, L[0]], [0.0, L[1]], [0.0, L[2]]]), shape)
+    thr = float(narrowband_thresh)
+    key = (OTF.data_ptr(), OTF._version, shape, thr)
+    hit = _AUTO_BANDS.get(id(OTF))
+    if hit is not None and hit[0] == key:
+        band = hit[1]
+    else:
+        band = ops.narrowband(OTF.detach().float().contiguous(), thr)
+        _AUTO_BANDS.clear()
+        _AUTO_BANDS[id(OTF)] = (key, band)
+    f64 = Verts.dtype == torch.float64
+    out = ops.volume_ft(Verts.float() if f64 else Verts, Faces, regint, grid, band)
+    return out.to(torch.complex128) if f64 else out

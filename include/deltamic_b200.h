@@ -148,6 +148,37 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
                        dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Surface + enclosed-volume ("autofluorescence") transform.  Replaces
+ * fourier_from_mesh_narrowband_autofluorescence (deltamic/render.py:228-318,
+ * pure torch in the reference, differentiated by its autograd):
+ *   ft(xi) = sum_k F_k(xi) (2 A_k / sum A + i (regint / regvol) xi.nor_k / |xi|^2)
+ * with Heron-equal areas A_k, nor_k = p0 x p1 + p1 x p2 + p2 x p0 and
+ * regvol = -sum_k p0 . (p1 x p2) / 6, vertex coordinates AS GIVEN (pass a box
+ * with lo = 0 and hi = the box lengths: the reference does not shift the mesh).
+ * regint is a DEVICE float.  At xi = 0 (every axis of the grid odd) the
+ * reference returns 0/0 = NaN; here the volume term there is its limit -regint.
+ * The forward writes ft_list[n_band] and vol_list[n_band] (complex64),
+ * vol = i sum_k F_k xi.nor_k / |xi|^2 (-regvol at xi = 0), so that
+ * ft = surface part + (regint / regvol) vol; the backward needs both.  The
+ * cotangent convention, grad_scale, otf, topology and mirror-symmetric bands are
+ * as for dm_meshft_backward; it writes grad_verts[nv,3] and, if not NULL,
+ * *grad_regint (DEVICE float). */
+size_t dm_meshft_volume_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band);
+int dm_meshft_volume_forward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                             const float* regint, const dm_box* box, const int32_t* band_index,
+                             int64_t n_band, const float* otf, float* ft_list, float* vol_list,
+                             float* grid, void* workspace, size_t ws_bytes,
+                             dm_stream_t stream);
+size_t dm_meshft_volume_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_band);
+int dm_meshft_volume_backward(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                              const float* regint, const dm_box* box, const int32_t* band_index,
+                              int64_t n_band, const float* grad_list, const float* grad_grid,
+                              const float* otf, float grad_scale, const float* ft_list,
+                              const float* vol_list, const void* topology, float* grad_verts,
+                              float* grad_regint, void* workspace, size_t ws_bytes,
+                              dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Batches: many meshes ("cells"), each with its own box, grid shape and narrow
  * band, in one launch per stage.  There is no batched counterpart in the
  * reference (one mesh per Fourier3dMesh call, render.py:136-150); the per-cell

@@ -17,8 +17,13 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
-def golden_cases():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+def golden_cases(prefix=""):
+    """Fixture names under tests/golden: the surface-transform cases (no prefix:
+    every file not starting with ``volume_``) or those starting with ``prefix``."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    if prefix:
+        return [n for n in names if n.startswith(prefix)]
+    return [n for n in names if not n.startswith("volume_")]
 
 
 def load_golden(name):
@@ -36,3 +41,16 @@ def rel_l2(a, b):
 @pytest.fixture(params=golden_cases())
 def golden(request):
     return request.param, load_golden(request.param)
+
+
+@pytest.fixture(params=golden_cases("volume_"))
+def golden_volume(request):
+    return request.param, load_golden(request.param)
+
+
+def band_xi(shape, lengths, idx):
+    """xi[len(idx), 3] of the band's voxel indices on the centred grid of a box
+    with the given lengths (render.py:321-340)."""
+    axes = [(2 * np.arange(n) - (n - 1)) * np.pi / lengths[d] for d, n in enumerate(shape)]
+    k = np.unravel_index(np.asarray(idx), tuple(shape))
+    return np.stack([axes[d][k[d]] for d in range(3)], axis=1)
