@@ -31,8 +31,11 @@
 namespace dm {
 namespace {
 
-constexpr int kVolR = 2, kVolFwdNT = 128;  // forward: frequencies per thread, threads
+// Tile shapes of the fit step's tuned surface kernels at 200^3 (forward {2, 256},
+// adjoint {1, 128}, 16 items per SM).
+constexpr int kVolR = 2, kVolFwdNT = 256;  // forward: frequencies per thread, threads
 constexpr int kVolF = 1, kVolBwdNT = 128;  // adjoint: faces per thread, threads
+constexpr int kVolWaves = 16;
 constexpr int kVolQ = 13;                  // adjoint accumulators per face
 constexpr double kPi = 3.141592653589793;
 
@@ -130,9 +133,26 @@ __global__ void k_vol_fwd_epi(CellDesc d, const int32_t* __restrict__ band_index
   const int m = blockIdx.x * kBlk + threadIdx.x;
   if (m >= d.ne) return;
   double sx = 0.0, sy = 0.0, vx = 0.0, vy = 0.0;
-  for (int s = 0; s < d.fsplit; ++s) {
-    const float2 a = fpart[(int64_t)s * d.ne + m];
-    const float2 b = fpart[(int64_t)(d.fsplit + s) * d.ne + m];
+  const float2* pa = fpart + m;
+  const float2* pb = fpart + (int64_t)d.fsplit * d.ne + m;
+  int s = 0;
+  for (; s + 4 <= d.fsplit; s += 4) {  // eight loads in flight, summed in split order
+    float2 a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = pa[(int64_t)(s + u) * d.ne];
+      b[u] = pb[(int64_t)(s + u) * d.ne];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      sx += a[u].x;
+      sy += a[u].y;
+      vx += b[u].x;
+      vy += b[u].y;
+    }
+  }
+  for (; s < d.fsplit; ++s) {
+    const float2 a = pa[(int64_t)s * d.ne], b = pb[(int64_t)s * d.ne];
     sx += a.x;
     sy += a.y;
     vx += b.x;
@@ -291,7 +311,19 @@ __global__ void k_vol_face_epi(CellDesc d, const float* __restrict__ verts,
   double q[kVolQ];
 #pragma unroll
   for (int i = 0; i < kVolQ; ++i) q[i] = 0.0;
-  for (int c = 0; c < d.bchunks; ++c) {
+  int c = 0;
+  for (; c + 2 <= d.bchunks; c += 2) {  // 26 loads in flight, summed in chunk order
+    float v[2][kVolQ];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int i = 0; i < kVolQ; ++i) v[u][i] = bpart[((int64_t)(c + u) * kVolQ + i) * d.nt + f];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int i = 0; i < kVolQ; ++i) q[i] += v[u][i];
+  }
+  for (; c < d.bchunks; ++c) {
 #pragma unroll
     for (int i = 0; i < kVolQ; ++i) q[i] += bpart[((int64_t)c * kVolQ + i) * d.nt + f];
   }
@@ -336,7 +368,8 @@ int64_t cdiv64(int64_t a, int64_t b) { return (a + b - 1) / b; }
 }  // namespace
 
 void plan_volume(CellDesc& d, PlanTotals& t) {
-  plan_cell_tiles_for(d, FwdVariant{kVolR, kVolFwdNT, 8}, BwdVariant{kVolF, kVolBwdNT, 8});
+  plan_cell_tiles_for(d, FwdVariant{kVolR, kVolFwdNT, kVolWaves},
+                      BwdVariant{kVolF, kVolBwdNT, kVolWaves});
   t.fpart = 2 * (int64_t)d.fsplit * d.ne;
   t.bpart = (int64_t)kVolQ * d.bchunks * d.nt;
   t.fwd_items = (int64_t)d.xtiles * d.fsplit;

@@ -248,7 +248,7 @@ def volume_backward_list(verts, faces, regint, grid: FreqGrid, band, ft, vol, gr
     lib = N.lib()
     nv, nt, nb = verts.shape[0], faces.shape[0], band.numel()
     gv = torch.empty_like(verts)
-    gr = torch.zeros(1, dtype=torch.float32, device=verts.device) if want_regint else None
+    gr = torch.empty(1, dtype=torch.float32, device=verts.device) if want_regint else None
     topo = topology(faces, nv)
     ws = N.WORKSPACES.get("vol_bwd", lib.dm_meshft_volume_backward_workspace_size(nv, nt, nb),
                           verts.device)
