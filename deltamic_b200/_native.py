@@ -32,6 +32,7 @@ _I64 = ctypes.c_int64
 _SZ = ctypes.c_size_t
 _F = ctypes.c_float
 _INT = ctypes.c_int
+_I32 = ctypes.c_int32
 
 
 class DmBox(ctypes.Structure):
@@ -81,6 +82,29 @@ SIGNATURES = {
     "dm_meshft_backward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_backward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P, _F, _P,
                                   _P, _P, _P, _P, _P, _SZ, _P]),
+    "dm_aniso_gaussian_psf": (_INT, [_P, _P, _I32, _P, _I32, _P, _I32, _P, _P]),
+    "dm_aniso_gaussian_psf_grad_workspace_size": (_SZ, [_I64]),
+    "dm_aniso_gaussian_psf_grad": (_INT, [_P, _P, _P, _P, _I32, _P, _I32, _P, _I32, _P, _P,
+                                          _SZ, _P]),
+    "dm_radial_basis": (_INT, [_P, _I32, _P, _P, _I64, _P, _P, _P, _P]),
+    "dm_radial_basis_grad_workspace_size": (_SZ, [_I64, _I32]),
+    "dm_radial_basis_grad": (_INT, [_P, _P, _I32, _P, _P, _I64, _P, _P, _I32, _P, _P, _P, _P,
+                                    _SZ, _P]),
+    "dm_radial_intensity_workspace_size": (_SZ, [_I64, _I32]),
+    "dm_radial_intensity": (_INT, [_P, _I64, _I32, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
+    "dm_radial_intensity_backward": (_INT, [_P, _P, _P, _P, _I64, _I32, _P, _P, _P, _P, _SZ,
+                                            _P]),
+    "dm_pupil_defocus": (_INT, [_P, _P, _P, _I32, _I32, _I32, _P, _P]),
+    "dm_pupil_defocus_grad_workspace_size": (_SZ, [_I32, _I32, _I32]),
+    "dm_pupil_defocus_backward": (_INT, [_P, _P, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _SZ,
+                                         _P]),
+    "dm_shifted_intensity": (_INT, [_P, _I32, _I32, _I32, _P, _P]),
+    "dm_shifted_intensity_backward": (_INT, [_P, _P, _I32, _I32, _I32, _P, _P]),
+    "dm_zernike": (_INT, [_P, _P, _I64, _P, _I32, _P, _P]),
+    "dm_mask_workspace_size": (_SZ, [_I64, _I32]),
+    "dm_membrane_mask": (_INT, [_P, _I64, _P, _I64, _I32, _BOXP, ctypes.c_double, _I32, _P, _P,
+                                _SZ, _P]),
+    "dm_instance_mask": (_INT, [_P, _I64, _P, _I64, _BOXP, _I32, _P, _P, _SZ, _P]),
     "dm_batch_desc_size": (_SZ, [_INT]),
     "dm_batch_plan": (_INT, [ctypes.POINTER(DmCell), _INT, _P, _SZ, _BATCHP, _P]),
     "dm_batched_topology_build": (_INT, [_BATCHP, _P, _P, _SZ, _P]),

@@ -179,6 +179,109 @@ int dm_meshft_volume_backward(const float* verts, int64_t nv, const int64_t* fac
                               dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Spatial PSF models of deltamic/psf.py: the volume-sized stages (the small
+ * per-parameter maps stay with the caller).  All pointers are DEVICE memory.
+ *
+ * Anisotropic_gaussian_psf (psf.py:628-665): psf[i][j][k] =
+ *   exp(-u^T S u / (2 D)) / D, u = (x[i], y[j]), D = eps + (|z[k]| sigma_z)^2,
+ * params = {S00, S01, S10, S11, sigma_z, eps} (float32, the reference's operation
+ * order); the gradient call writes d loss / d params[6] for grad_psf. */
+int dm_aniso_gaussian_psf(const float* params, const float* x, int32_t nx, const float* y,
+                          int32_t ny, const float* z, int32_t nz, float* psf, dm_stream_t stream);
+size_t dm_aniso_gaussian_psf_grad_workspace_size(int64_t n);
+int dm_aniso_gaussian_psf_grad(const float* grad_psf, const float* psf, const float* params,
+                               const float* x, int32_t nx, const float* y, int32_t ny,
+                               const float* z, int32_t nz, float* grad_params, void* workspace,
+                               size_t ws_bytes, dm_stream_t stream);
+
+/* Gibson_Lanni_psf (psf.py:23-154), float64.  The PSF depends on the pixel only
+ * through its distance from the lateral centre, so the Fourier-Bessel basis of
+ * psf.py:141-143 is formed for the distinct radii u:
+ *   basis[u][k] = (s J1(s rm) J0(b rm) rm - b J0(s rm) J1(b rm) rm) / (s s - b b),
+ *   s = scaling[k], b = b[u] (= 2 pi radius_u res_lateral NA / wavelength),
+ *   rm = *rhomax,
+ * with the Bessel values given as tables bessel_s = {J0(s rm)} ++ {J1(s rm)} [2K]
+ * and bessel_b = {J0(b rm)} ++ {J1(b rm)} [2U] (the caller's Bessel functions: the
+ * amplitude basis @ C cancels large terms of an ill-conditioned least-squares fit,
+ * so the basis must use the values the fit used).  dm_radial_basis_grad returns
+ * d loss / d scaling[K], d loss / d rhomax[1] and d loss / d b[U]; exact == 0 holds
+ * the Bessel values constant, as the reference's autograd does (torch's
+ * bessel_j0/j1 have no derivative), exact != 0 differentiates them as well.
+ * With the amplitude amp[u][z] = (basis @ C)[u][z] (complex128, interleaved),
+ * dm_radial_intensity writes profile[u][z] = |amp|^2, *peak = its maximum and
+ * psf[p][z] = profile[pixel_radius[p]][z] / peak for every pixel p = x ny + y; its
+ * backward returns d loss / d amp (PyTorch's complex convention), the maximum's
+ * gradient shared by every voxel tied with it, as torch's max() does.
+ * radius_off[n_radii + 1] / radius_pixels[n_pixels] list the pixels of each
+ * radius (CSR, ascending). */
+int dm_radial_basis(const double* scaling, int32_t n_basis, const double* rhomax,
+                    const double* b, int64_t n_radii, const double* bessel_s,
+                    const double* bessel_b, double* basis, dm_stream_t stream);
+size_t dm_radial_basis_grad_workspace_size(int64_t n_radii, int32_t n_basis);
+int dm_radial_basis_grad(const double* grad_basis, const double* scaling, int32_t n_basis,
+                         const double* rhomax, const double* b, int64_t n_radii,
+                         const double* bessel_s, const double* bessel_b, int32_t exact,
+                         double* grad_scaling, double* grad_rhomax, double* grad_b,
+                         void* workspace, size_t ws_bytes, dm_stream_t stream);
+size_t dm_radial_intensity_workspace_size(int64_t n_radii, int32_t nz);
+int dm_radial_intensity(const double* amp, int64_t n_radii, int32_t nz, const int32_t* pixel_radius,
+                        int64_t n_pixels, double* psf, double* profile, double* peak,
+                        void* workspace, size_t ws_bytes, dm_stream_t stream);
+int dm_radial_intensity_backward(const double* grad_psf, const double* amp, const double* profile,
+                                 const double* peak, int64_t n_radii, int32_t nz,
+                                 const int32_t* radius_off, const int32_t* radius_pixels,
+                                 double* grad_amp, void* workspace, size_t ws_bytes,
+                                 dm_stream_t stream);
+
+/* Hanser_psf (psf.py:157-371), float32 / complex64 interleaved.
+ * dm_pupil_defocus: pupil[z][x][y] = pupil0[x][y] exp(2 pi i kz[x][y] zr[z])
+ * (psf.py:310-314, 336); its backward returns the gradients to pupil0, kz, zr.
+ * dm_shifted_intensity: out[x][y][z] = |field[z][x'][y']|^2 with x' = (x - nx/2)
+ * mod nx (fftshift over x and y, then the (z, x, y) -> (x, y, z) permutation of
+ * psf.py:262-266); its backward returns d loss / d field.  The batched 2-D
+ * inverse FFT between them is the caller's (cuFFT).
+ * dm_zernike: out[j][i] = Z_{n_j}^{m_j}(r[i], theta[i]), degrees = {n_j, m_j}
+ * pairs in HOST memory (n_j <= 10), Noll-normalised, 0 for r > 1 (psf.py:373-548). */
+int dm_pupil_defocus(const float* pupil0, const float* kz, const float* zr, int32_t nx,
+                     int32_t ny, int32_t nz, float* pupil, dm_stream_t stream);
+size_t dm_pupil_defocus_grad_workspace_size(int32_t nx, int32_t ny, int32_t nz);
+int dm_pupil_defocus_backward(const float* grad_pupil, const float* pupil0, const float* kz,
+                              const float* zr, int32_t nx, int32_t ny, int32_t nz,
+                              float* grad_pupil0, float* grad_kz, float* grad_zr,
+                              void* workspace, size_t ws_bytes, dm_stream_t stream);
+int dm_shifted_intensity(const float* field, int32_t nx, int32_t ny, int32_t nz, float* out,
+                         dm_stream_t stream);
+int dm_shifted_intensity_backward(const float* field, const float* grad_out, int32_t nx,
+                                  int32_t ny, int32_t nz, float* grad_field, dm_stream_t stream);
+int dm_zernike(const float* r, const float* theta, int64_t n_points, const int32_t* degrees,
+               int32_t n_modes, float* out, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Segmentation masks of deltamic/mask_creation.py (float64 vertices [nv,3] and
+ * grid; the grid points are numpy.linspace(box.lo[d], box.hi[d], box.shape[d]) per
+ * axis, create_coords, mask_creation.py:195-205).
+ * dm_membrane_mask (create_semantic_segmentation_mask, :208-222): faces read with
+ * face_stride int64 per face (first three = vertex indices) are refined until every
+ * edge is at most max_edge (trimesh's subdivide_to_size: four-way splits at the
+ * edge midpoints, at most max_depth <= 24 levels, else DM_ERR_SIZE in the
+ * workspace's status word), and mask[(ix ny + iy) nz + iz] = 1 at the grid point
+ * nearest to each vertex of the refined faces (0 elsewhere).
+ * dm_instance_mask (create_instance_segmentation_mask, :225-266): faces [nt,5]
+ * (indices, then the labels on either side; a face whose first label is the smaller
+ * is flipped, reorder_faces :49-53) split four ways `levels` times
+ * (subdivide_with_materials, :60-176); mask[p] = 1 + the label, on grid point p's
+ * side of the normal, of the child face whose centroid is nearest to p (ties: the
+ * lower child index).  Exhaustive nearest search: cost grid points x nt 4^levels.
+ * Workspace from dm_mask_workspace_size(nt, levels); status via dm_device_error. */
+size_t dm_mask_workspace_size(int64_t nt, int32_t levels);
+int dm_membrane_mask(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                     int32_t face_stride, const dm_box* box, double max_edge, int32_t max_depth,
+                     double* mask, void* workspace, size_t ws_bytes, dm_stream_t stream);
+int dm_instance_mask(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                     const dm_box* box, int32_t levels, double* mask, void* workspace,
+                     size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Batches: many meshes ("cells"), each with its own box, grid shape and narrow
  * band, in one launch per stage.  There is no batched counterpart in the
  * reference (one mesh per Fourier3dMesh call, render.py:136-150); the per-cell

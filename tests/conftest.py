@@ -19,11 +19,12 @@ def pytest_configure(config):
 
 def golden_cases(prefix=""):
     """Fixture names under tests/golden: the surface-transform cases (no prefix:
-    every file not starting with ``volume_``) or those starting with ``prefix``."""
+    every file not starting with ``volume_`` or ``psf_``) or those starting with
+    ``prefix``."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
     if prefix:
         return [n for n in names if n.startswith(prefix)]
-    return [n for n in names if not n.startswith("volume_")]
+    return [n for n in names if not n.startswith(("volume_", "psf_"))]
 
 
 def load_golden(name):
