@@ -78,7 +78,7 @@ def parse():
                         "and step with VectorAdam (0: plain Adam, the configured fit)")
     p.add_argument("--precond-lr", type=float, default=5e-3)
     p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned",
-                                           "volume200"],
+                                           "volume200", "psf200", "masks64"],
                    default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
                         "cells of mixed sizes per step; volume200: forward + adjoint of "
@@ -216,6 +216,8 @@ def run_reference(args, rank, world):
     import oracle
     if args.workload == "volume200":
         return run_reference_volume(args)
+    if args.workload in ("psf200", "masks64"):
+        return run_reference_host(args)
     gt_v, init_v, faces, box = make_workload(0, args.small)
     axes = oracle.frequency_axes(box, SHAPE)
     otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
@@ -246,6 +248,53 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
+
+
+def run_reference_host(args):
+    """Reference arm of psf200 / masks64: the oracles' restatements of the
+    reference's host code (torch / numpy / scipy) on a bounded sample per step."""
+    if args.workload == "psf200":
+        import oracle.psf as op
+        metric = ("spatial PSF models fwd+bwd at 200^3 (Gibson-Lanni, Hanser, anisotropic "
+                  "Gaussian per step)")
+        unit, sample = "PSF sets/s", "Gibson-Lanni + Hanser forward at 64 x 64 x 32"
+
+        def one():
+            op.gibson_lanni_radial((64, 64, 32))
+            op.hanser_psf((64, 64, 32), np.linspace(-0.2, 0.2, 21), np.zeros(21))
+    else:
+        import oracle.masks as om
+        from deltamic_b200.mesh import random_sh_shape
+        metric = "segmentation masks (membrane + labels) per second, two level-4 cells, 64^3"
+        unit, sample = "mask pairs/s", "the masks64 pair, scipy KDTree"
+        v1, f1 = random_sh_shape(4, 0.25, 4, 0.08, seed=1)
+        v2, f2 = random_sh_shape(4, 0.2, 4, 0.08, seed=2)
+        V = np.concatenate([v1, v2 + np.array([0.5, 0.05, 0.0])])
+        F = np.concatenate([np.hstack([f1, np.full((len(f1), 1), 1), np.zeros((len(f1), 1), int)]),
+                            np.hstack([f2 + len(v1), np.full((len(f2), 1), 2),
+                                       np.zeros((len(f2), 1), int)])])
+        box = np.stack([V.min(0) - 0.1, V.max(0) + 0.1], axis=1)
+
+        def one():
+            om.semantic_mask(V, F, np.array([64, 64, 64]), box)
+            om.instance_mask(V, F, np.array([64, 64, 64]), box)
+    vals = []
+    for k in range(min(args.warmup, 1) + min(args.steps, 3)):
+        t0 = time.perf_counter()
+        one()
+        if k >= min(args.warmup, 1):
+            vals.append(1.0 / (time.perf_counter() - t0))
+    value = float(np.mean(vals))
+    print(json.dumps({
+        "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": len(vals), "warmup": min(args.warmup, 1), "ms_per_step": 1e3 / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "parallelism": "replicas only"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": os.cpu_count() or 1,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}), flush=True)
 
 
 def run_reference_volume(args):
@@ -280,6 +329,134 @@ def run_reference_volume(args):
                          "sample": f"{per_step} band frequencies x {len(faces)} faces per step"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def _event_ms(fn, steps, warmup):
+    """Device time per call of ``fn`` (CUDA events, after ``warmup`` calls)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_psf(args, rank, world, local):
+    """psf200: the spatial PSF models on a 200 x 200 x 200 volume, forward plus the
+    gradient of sum(w * psf) to every parameter: Gibson-Lanni (float64), Hanser
+    (21 Zernike modes), the anisotropic Gaussian.  value = PSF volumes per second
+    (all three models per step); the Gibson-Lanni and Hanser oracles (torch / numpy
+    on the host) are timed on a 64 x 64 x 32 sample for the CPU baseline."""
+    import torch
+    import oracle.psf as op
+    from deltamic_b200 import Anisotropic_gaussian_psf, Gibson_Lanni_psf, Hanser_psf
+    from deltamic_b200 import _native as N
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.lib()
+    shape = (64, 64, 32) if args.small else (200, 200, 200)
+    gl = Gibson_Lanni_psf(shape, device=dev)
+    xi = [torch.zeros(n, device=dev) for n in shape]
+    hs = Hanser_psf(shape, *xi, device=dev)
+    with torch.no_grad():
+        hs.pcoefs.copy_(torch.linspace(-0.2, 0.2, 21, device=dev))
+    an = Anisotropic_gaussian_psf(shape, (20.0, 20.0, 20.0), sigma=0.5, sigma_z=0.3, device=dev)
+    w64 = torch.randn(shape, dtype=torch.float64, device=dev)
+    w32 = w64.float()
+
+    def step_gl():
+        (gl() * w64).sum().backward()
+
+    def step_hs():
+        (hs() * w32).sum().backward()
+
+    def step_an():
+        (an() * w32).sum().backward()
+
+    n0 = lib.dm_launch_count()
+    ms = {k: max_over_ranks(_event_ms(f, args.steps, args.warmup), dev)
+          for k, f in (("gibson_lanni", step_gl), ("hanser", step_hs), ("anisotropic", step_an))}
+    launches = lib.dm_launch_count() - n0
+    total = sum(ms.values())
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        t0 = time.perf_counter()
+        op.gibson_lanni_radial((64, 64, 32))
+        op.hanser_psf((64, 64, 32), np.linspace(-0.2, 0.2, 21), np.zeros(21))
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / dt, "unit": "PSF sets/s", "cores": os.cpu_count() or 1,
+               "kind": "port", "sample": f"Gibson-Lanni + Hanser forward at 64 x 64 x 32 "
+                                         f"({dt:.2f} s)"}
+    if rank != 0:
+        return
+    out = {"metric": "spatial PSF models fwd+bwd at 200^3 (Gibson-Lanni, Hanser, anisotropic "
+                     "Gaussian per step)",
+           "value": world * 1e3 / total, "unit": "PSF sets/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 (Gibson-Lanni), f32", "data": "synthetic",
+           "config": {"workload": "psf200: " + " x ".join(map(str, shape)),
+                      "ms_per_model": ms, "parallelism": "replicas only"},
+           "gpu_launches": int(launches)}
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
+def run_masks(args, rank, world, local):
+    """masks64: membrane and label masks of two SH cells (level 4, 2 x 5,120 faces
+    with region labels) on a 64^3 grid.  value = mask pairs per second; the oracle
+    (scipy KDTree) is the CPU baseline."""
+    import torch
+    import oracle.masks as om
+    from deltamic_b200 import create_instance_segmentation_mask, create_semantic_segmentation_mask
+    from deltamic_b200.mesh import random_sh_shape
+    from deltamic_b200.mesh_io import combine_all_verts_faces_mm
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    v1, f1 = random_sh_shape(4, 0.25, 4, 0.08, seed=1 + rank)
+    v2, f2 = random_sh_shape(4, 0.2, 4, 0.08, seed=2 + rank)
+    v2 = v2 + np.array([0.5, 0.05, 0.0])
+    mm = [np.hstack([f1, np.full((len(f1), 1), 1), np.zeros((len(f1), 1), int)]),
+          np.hstack([f2, np.full((len(f2), 1), 2), np.zeros((len(f2), 1), int)])]
+    V, F = combine_all_verts_faces_mm([v1, v2], mm)
+    F = F.astype(np.int64)
+    box = np.stack([V.min(0) - 0.1, V.max(0) + 0.1], axis=1)
+    shape = np.array([64, 64, 64])
+    Vd = torch.tensor(V, dtype=torch.float64, device=dev)
+    Fd = torch.tensor(F, device=dev)
+
+    def step():
+        create_semantic_segmentation_mask(Vd, Fd, shape, box, device=dev)
+        create_instance_segmentation_mask(Vd, Fd, shape, box, device=dev)
+
+    ms = max_over_ranks(_event_ms(step, args.steps, args.warmup), dev)
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        t0 = time.perf_counter()
+        om.semantic_mask(V, F, shape, box)
+        om.instance_mask(V, F, shape, box)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / dt, "unit": "mask pairs/s", "cores": 1, "kind": "port",
+               "sample": f"the same two masks ({dt:.2f} s)"}
+    if rank != 0:
+        return
+    out = {"metric": "segmentation masks (membrane + labels) per second, two level-4 cells, 64^3",
+           "value": world * 1e3 / ms, "unit": "mask pairs/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": "masks64: 2 x 5,120 faces, 64^3",
+                      "note": "includes the status read-back of each call (one sync)",
+                      "parallelism": "replicas only"}}
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
 
 
 def run_volume(args, rank, world, local):
@@ -781,6 +958,10 @@ def main():
             run_learned(args, rank, world, local)
         elif args.workload == "volume200":
             run_volume(args, rank, world, local)
+        elif args.workload == "psf200":
+            run_psf(args, rank, world, local)
+        elif args.workload == "masks64":
+            run_masks(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

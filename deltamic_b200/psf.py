@@ -219,27 +219,18 @@ def _radial_tables(nx, ny, device):
     return t
 
 
-def _host_bessel(fn, x):
-    """torch's CPU Bessel function of a device tensor, returned on its device.  The
-    reference evaluates the fit's Bessel values with torch on the CPU; torch's CUDA
-    versions differ from them in the last digits, and the ill-conditioned pupil fit
-    (cond(J) ~ 4e12) and the cancelling sum basis @ C magnify that to 1e-5 of the
-    PSF.  These are O(K * samples + K + radii) values (~1e5), not volume-sized."""
-    return fn(x.detach().cpu()).to(x.device)
-
-
 class _BesselJ0(torch.autograd.Function):
     """J0 of the pupil fit with its derivative -J1 (torch's bessel_j0 has none)."""
 
     @staticmethod
     def forward(ctx, x):
         ctx.save_for_backward(x)
-        return _host_bessel(torch.special.bessel_j0, x)
+        return torch.special.bessel_j0(x)
 
     @staticmethod
     def backward(ctx, g):
         (x,) = ctx.saved_tensors
-        return -_host_bessel(torch.special.bessel_j1, x) * g
+        return -torch.special.bessel_j1(x) * g
 
 
 class _RadialBasis(torch.autograd.Function):
@@ -357,16 +348,14 @@ class Gibson_Lanni_psf(nn.Module):
         phase = torch.cos(W) + 1j * torch.sin(W)
         x = scaling.reshape(-1, 1) * rho
         J = (_BesselJ0.apply(x) if self.exact_bessel_grad
-             else _host_bessel(torch.special.bessel_j0, x)).type(torch.complex128)
+             else torch.special.bessel_j0(x)).type(torch.complex128)
         C = torch.linalg.lstsq(J.T, phase.T).solution                  # [K, nz]
         radii, pix, off, pixels = _radial_tables(self.size_x, self.size_y, dev)
         b = 2 * np.pi * (radii * self.res_lateral) * NA / lam          # per distinct radius
-        with torch.no_grad():
+        with torch.no_grad():  # the Bessel values the fit and the basis share
             sr, br = scaling * rhomax, b * rhomax
-            bess_s = torch.cat([_host_bessel(torch.special.bessel_j0, sr),
-                                _host_bessel(torch.special.bessel_j1, sr)])
-            bess_b = torch.cat([_host_bessel(torch.special.bessel_j0, br),
-                                _host_bessel(torch.special.bessel_j1, br)])
+            bess_s = torch.cat([torch.special.bessel_j0(sr), torch.special.bessel_j1(sr)])
+            bess_b = torch.cat([torch.special.bessel_j0(br), torch.special.bessel_j1(br)])
         R = _RadialBasis.apply(scaling.contiguous(), rhomax.reshape(1).contiguous(),
                                b.contiguous(), bess_s, bess_b, self.exact_bessel_grad)
         amp = (R.type(torch.complex128) @ C).contiguous()             # cuBLAS

@@ -49,45 +49,60 @@ def zernike_explicit(r, theta, n, m):
     return np.where(r <= 1.0, R * ang * norm, 0.0)
 
 
-def gibson_lanni_radial(shape, NA=1.4, wavelength=0.610, res_lateral=0.1, res_axial=0.1,
-                        ns=1.33, ng0=1.499, ng=1.5, ni0=1.499, ni=1.5, ti0=150, tg0=170,
-                        tg=169.99, pZ=2.0, min_wavelength=0.436, num_basis=100):
-    """The pupil-phase fit is restated with torch CPU tensors of the reference's
-    dtypes: the pupil radius is a float32 linspace and the parameters 0-d float64
-    tensors, so by torch's promotion rules OPDs, OPDg, ``ti0 * sqrt(...)`` and the
-    axial positions are float32 quantities (psf.py:86, 106-118) -- part of the
-    reference's result at the 1e-4 level."""
+GL_DEFAULTS = dict(NA=1.4, wavelength=0.610, res_lateral=0.1, res_axial=0.1, ns=1.33,
+                   ng0=1.499, ng=1.5, ni0=1.499, ni=1.5, ti0=150.0, tg0=170.0, tg=169.99,
+                   pZ=2.0)
+
+
+def gibson_lanni_torch(shape, P, min_wavelength=0.436, num_basis=100):
+    """The reference's expressions (psf.py:77-151) as torch ops on the device of the
+    0-d float64 tensors ``P`` (keys of ``GL_DEFAULTS``), differentiable by torch's
+    autograd as the reference is, with the amplitude formed once per distinct pixel
+    radius and scattered.  Its pupil radius is a float32 linspace, so by torch's
+    promotion rules OPDs, OPDg, ``ti0 * sqrt(...)`` and the axial positions are
+    float32 quantities (psf.py:86, 106-118); its Bessel functions are torch's.  On the
+    CPU this is the reference's own computation; on a GPU it is what the reference
+    gives there -- torch's CUDA float32 arithmetic and Bessel functions differ from
+    its CPU ones in the last digits, which the ill-conditioned fit (cond(J) ~ 4e12)
+    carries to 1e-5 of the PSF."""
     nx, ny, nz = shape
-    t = lambda v: torch.tensor(v, dtype=torch.double)
-    NA_, wl_, ra_ = t(NA), t(wavelength), t(res_axial)
-    sf = (NA_ * (3 * torch.arange(1, num_basis + 1, dtype=torch.double) - 2)
-          * min_wavelength / wl_)
-    rhomax_t = min([NA_, t(ns), t(ni), t(ni0), t(ng), t(ng0)]) / NA_
-    rho = torch.linspace(0, rhomax_t.item(), 1000)
+    dev = P["NA"].device
+    NA, wl = P["NA"], P["wavelength"]
+    sf = NA * (3 * torch.arange(1, num_basis + 1, dtype=torch.double, device=dev) - 2) \
+        * min_wavelength / wl
+    rhomax = min([NA, P["ns"], P["ni"], P["ni0"], P["ng"], P["ng0"]]) / NA
+    rho = torch.linspace(0, rhomax.item(), 1000).to(dev)
     seps = np.sqrt(2.22045e-16)
-    sq = lambda n_: torch.sqrt((t(n_) * t(n_) - NA_ * NA_ * rho * rho).clamp(seps))
-    zv = (ra_ * torch.arange(-nz / 2, nz / 2) + ra_ / 2).type(torch.double)
-    W = 2 * np.pi / wl_ * (t(pZ) * sq(ns) + ((zv.reshape(-1, 1) + t(ti0)) * sq(ni)
-                                             - t(ti0) * sq(ni0))
-                           + (t(tg) * sq(ng) - t(tg0) * sq(ng0)))
-    phase = (torch.cos(W) + 1j * torch.sin(W)).numpy()
-    # torch's Bessel functions, as the reference: they differ from scipy's by up to
-    # 4e-7, and the least-squares fit below is ill-conditioned (cond(J) ~ 4e12)
-    tj0 = lambda x: torch.special.bessel_j0(torch.as_tensor(x)).numpy()
-    tj1 = lambda x: torch.special.bessel_j1(torch.as_tensor(x)).numpy()
-    J = torch.special.bessel_j0(sf.reshape(-1, 1) * rho).numpy().astype(np.complex128)
-    C = np.linalg.lstsq(J.T, phase.T, rcond=None)[0]                 # [K, nz]
-    sf, rhomax = sf.numpy(), float(rhomax_t)
+    sq = lambda n_: torch.sqrt((n_ * n_ - NA * NA * rho * rho).clamp(seps))
+    zv = (P["res_axial"] * torch.arange(-nz / 2, nz / 2, device=dev)
+          + P["res_axial"] / 2).type(torch.double)
+    W = 2 * np.pi / wl * (P["pZ"] * sq(P["ns"])
+                          + ((zv.reshape(-1, 1) + P["ti0"]) * sq(P["ni"])
+                             - P["ti0"] * sq(P["ni0"]))
+                          + (P["tg"] * sq(P["ng"]) - P["tg0"] * sq(P["ng0"])))
+    phase = torch.cos(W) + 1j * torch.sin(W)
+    J = torch.special.bessel_j0(sf.reshape(-1, 1) * rho).type(torch.complex128)
+    C = torch.linalg.lstsq(J.T, phase.T).solution                    # [K, nz]
     dx = np.arange(nx) - (nx - 1) / 2
     dy = np.arange(ny) - (ny - 1) / 2
     r2 = (dx[:, None] ** 2 + dy[None, :] ** 2).reshape(-1)
     u2, inv = np.unique(r2, return_inverse=True)
-    b = 2 * np.pi * np.sqrt(u2) * res_lateral * NA / wavelength
-    R = ((sf * tj1(sf * rhomax) * tj0(b[:, None] * rhomax) * rhomax
-          - b[:, None] * tj0(sf * rhomax) * tj1(b[:, None] * rhomax) * rhomax)
-         / (sf * sf - b[:, None] ** 2))
-    prof = np.abs(R @ C) ** 2                                         # [U, nz]
-    return (prof[inv] / prof.max()).reshape(nx, ny, nz)
+    r_pix = torch.tensor(np.sqrt(u2), dtype=torch.double, device=dev) * P["res_lateral"]
+    b = (2 * np.pi * r_pix * NA / wl).reshape(-1, 1)
+    j0, j1 = torch.special.bessel_j0, torch.special.bessel_j1
+    R = ((sf * j1(sf * rhomax) * j0(b * rhomax) * rhomax
+          - b * j0(sf * rhomax) * j1(b * rhomax) * rhomax) / (sf * sf - b * b))
+    prof = torch.abs(R.type(torch.complex128) @ C) ** 2                # [U, nz]
+    idx = torch.as_tensor(inv.reshape(-1), device=dev)
+    return (prof[idx] / torch.max(prof)).reshape(nx, ny, nz)
+
+
+def gibson_lanni_radial(shape, device="cpu", min_wavelength=0.436, num_basis=100, **kw):
+    """Numpy result of :func:`gibson_lanni_torch` for float parameters (defaults of
+    the reference module)."""
+    P = {k: torch.tensor(float(kw.get(k, v)), dtype=torch.double, device=device)
+         for k, v in GL_DEFAULTS.items()}
+    return gibson_lanni_torch(shape, P, min_wavelength, num_basis).cpu().numpy()
 
 
 def _noll(j):
