@@ -183,14 +183,16 @@ __device__ __forceinline__ void basis_partials(double s, double b, double rm, do
   dr = dnr / den;
 }
 
-// gb[u] = sum_k gR dR/db and per-block sums of gR dR/d rm (u in blocks, k in order).
+// gb[u] = sum_k gR dR/db, ds[u][k] = gR dR/ds, and per-block sums of gR dR/d rm
+// (u in blocks, k in order).
 __global__ void k_radial_basis_grad_u(const double* __restrict__ gR,
                                       const double* __restrict__ scaling, int K,
                                       const double* __restrict__ rhomax,
                                       const double* __restrict__ b, int64_t U,
                                       const double* __restrict__ bs,
                                       const double* __restrict__ bb, int exact,
-                                      double* __restrict__ gb, double* __restrict__ part) {
+                                      double* __restrict__ gb, double* __restrict__ ds_out,
+                                      double* __restrict__ part) {
   const double rm = rhomax[0];
   const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
@@ -203,30 +205,28 @@ __global__ void k_radial_basis_grad_u(const double* __restrict__ gR,
       const double g = gR[u * K + k];
       sb += g * db;
       acc[0] += g * dr;
+      ds_out[u * K + k] = g * ds;
     }
     gb[u] = sb;
   }
   block_partials<1>(acc, part);
 }
 
-// gscaling[k] = sum_u gR dR/ds (u in order).
-__global__ void k_radial_basis_grad_k(const double* __restrict__ gR,
-                                      const double* __restrict__ scaling, int K,
-                                      const double* __restrict__ rhomax,
-                                      const double* __restrict__ b, int64_t U,
-                                      const double* __restrict__ bs,
-                                      const double* __restrict__ bb, int exact,
+// gscaling[k] = sum_u ds[u][k]: one block per k, a fixed-order tree over u.
+__global__ void k_radial_basis_grad_k(const double* __restrict__ ds, int K, int64_t U,
                                       double* __restrict__ gscaling) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K) return;
-  const double rm = rhomax[0];
-  double acc = 0.0;
-  for (int64_t u = 0; u < U; ++u) {
-    double ds, db, dr;
-    basis_partials(scaling[k], b[u], rm, bs[k], bs[K + k], bb[u], bb[U + u], exact, ds, db, dr);
-    acc += gR[u * K + k] * ds;
+  __shared__ double sh[kThreads / 32];
+  const int k = blockIdx.x;
+  double x = 0.0;
+  for (int64_t u = threadIdx.x; u < U; u += blockDim.x) x += ds[u * K + k];
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+    gscaling[k] = t;
   }
-  gscaling[k] = acc;
 }
 
 // prof[u][z] = |A[u][z]|^2 and per-block maxima.
@@ -533,7 +533,7 @@ int dm_radial_basis(const double* scaling, int32_t n_basis, const double* rhomax
 
 size_t dm_radial_basis_grad_workspace_size(int64_t n_radii, int32_t n_basis) {
   if (n_radii <= 0 || n_basis <= 0) return 0;
-  return sizeof(double) * (size_t)cdiv(n_radii, kThreads) + 256;
+  return sizeof(double) * ((size_t)cdiv(n_radii, kThreads) + (size_t)n_radii * n_basis) + 512;
 }
 
 int dm_radial_basis_grad(const double* grad_basis, const double* scaling, int32_t n_basis,
@@ -548,11 +548,12 @@ int dm_radial_basis_grad(const double* grad_basis, const double* scaling, int32_
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned nb = (unsigned)cdiv(n_radii, kThreads);
   double* part = (double*)workspace;
+  double* ds = part + nb;
   k_radial_basis_grad_u<<<nb, kThreads, 0, st>>>(grad_basis, scaling, n_basis, rhomax, b,
-                                                n_radii, bessel_s, bessel_b, exact, grad_b,
+                                                n_radii, bessel_s, bessel_b, exact, grad_b, ds,
                                                 part);
-  k_radial_basis_grad_k<<<(unsigned)cdiv(n_basis, 128), 128, 0, st>>>(
-      grad_basis, scaling, n_basis, rhomax, b, n_radii, bessel_s, bessel_b, exact, grad_scaling);
+  k_radial_basis_grad_k<<<(unsigned)n_basis, kThreads, 0, st>>>(ds, n_basis, n_radii,
+                                                                grad_scaling);
   k_sum_partials<1, double><<<1, 32, 0, st>>>(part, (int)nb, grad_rhomax);
   count_launches(3);
   return status();

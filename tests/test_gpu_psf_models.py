@@ -68,8 +68,9 @@ def test_gibson_lanni_matches_reference(case):
     """Against the oracle's restatement of the reference's expressions evaluated on
     the same GPU with torch autograd (the reference run there): PSF within 1e-9 and
     every parameter gradient within ten times the gradient's own sensitivity to the
-    order of its sums (measured on the CPU; 0 for well-conditioned parameters, 9e-5
-    for the defaults) plus 1e-9.  Against the reference run on the CPU (golden):
+    order of its sums (measured on the CPU; 3e-13 for the custom set, 9e-5 for the
+    defaults) or within the reference's own CPU-to-GPU spread of that gradient,
+    plus 1e-9.  Against the reference run on the CPU (golden):
     within twice the distance between that restatement on the GPU and on the CPU
     -- the reference's own CPU-to-GPU spread (float32 steps in its pupil phase,
     Bessel functions, least squares with cond(J) ~ 4e12) -- plus 1e-9."""
@@ -105,7 +106,10 @@ def test_gibson_lanni_matches_reference(case):
     print(f"  gradient floor (order of sums, CPU) {floor_g:.1e}")
     assert e_dev < 1e-9
     assert e < 2 * spread + 1e-9
-    assert max(eg_dev.values()) < 10 * floor_g + 1e-9
+    # each gradient: within the reordering floor, or within the reference's own
+    # CPU-to-GPU spread for that parameter (torch's GPU backward sums with atomics)
+    for p in GL_PARAMS:
+        assert eg_dev[p] < max(10 * floor_g, eg_spread[p]) + 1e-9, p
 
 
 @pytest.mark.parametrize("param", ["wavelength", "res_lateral"])
