@@ -77,6 +77,8 @@ def parse():
                    help="fit300: precondition the vertex gradient with (M M)^-1, M = I + lambda L, "
                         "and step with VectorAdam (0: plain Adam, the configured fit)")
     p.add_argument("--precond-lr", type=float, default=5e-3)
+    p.add_argument("--mask-grid", type=int, default=64,
+                   help="masks64: grid points per axis of the masks (64: the workload's grid)")
     p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned",
                                            "volume200", "psf200", "masks64"],
                    default="fit200",
@@ -427,7 +429,7 @@ def run_masks(args, rank, world, local):
     V, F = combine_all_verts_faces_mm([v1, v2], mm)
     F = F.astype(np.int64)
     box = np.stack([V.min(0) - 0.1, V.max(0) + 0.1], axis=1)
-    shape = np.array([64, 64, 64])
+    shape = np.array([args.mask_grid] * 3)
     Vd = torch.tensor(V, dtype=torch.float64, device=dev)
     Fd = torch.tensor(F, device=dev)
 
@@ -446,12 +448,13 @@ def run_masks(args, rank, world, local):
                "sample": f"the same two masks ({dt:.2f} s)"}
     if rank != 0:
         return
-    out = {"metric": "segmentation masks (membrane + labels) per second, two level-4 cells, 64^3",
+    out = {"metric": "segmentation masks (membrane + labels) per second, two level-4 cells, "
+                     f"{args.mask_grid}^3",
            "value": world * 1e3 / ms, "unit": "mask pairs/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
-           "config": {"workload": "masks64: 2 x 5,120 faces, 64^3",
+           "config": {"workload": f"masks64: 2 x 5,120 faces, {args.mask_grid}^3",
                       "note": "includes the status read-back of each call (one sync)",
                       "parallelism": "replicas only"}}
     if cpu is not None:

@@ -101,7 +101,7 @@ SIGNATURES = {
     "dm_shifted_intensity": (_INT, [_P, _I32, _I32, _I32, _P, _P]),
     "dm_shifted_intensity_backward": (_INT, [_P, _P, _I32, _I32, _I32, _P, _P]),
     "dm_zernike": (_INT, [_P, _P, _I64, _P, _I32, _P, _P]),
-    "dm_mask_workspace_size": (_SZ, [_I64, _I32]),
+    "dm_mask_workspace_size": (_SZ, [_I64, _I32, _BOXP]),
     "dm_membrane_mask": (_INT, [_P, _I64, _P, _I64, _I32, _BOXP, ctypes.c_double, _I32, _P, _P,
                                 _SZ, _P]),
     "dm_instance_mask": (_INT, [_P, _I64, _P, _I64, _BOXP, _I32, _P, _P, _SZ, _P]),

@@ -12,9 +12,11 @@
 //    carry the labels of the regions on either side; every face is split four ways
 //    `levels` times (subdivide_with_materials, :60-176), and every grid point takes
 //    the label on its side of the nearest child face (nearest centroid, side by the
-//    sign of (centroid - point) . normal), plus one.  The nearest centroid is an
-//    exhaustive search over centroid tiles staged in shared memory (exact; ties go
-//    to the lower child index).
+//    sign of (centroid - point) . normal), plus one.  The nearest centroid is exact
+//    (ties go to the lower child index): the centroids are counting-sorted into a
+//    uniform grid of buckets with tight bounding boxes; each point first bounds its
+//    nearest distance by the farthest corner of every non-empty bucket, then reads
+//    the centroids of the buckets whose nearest corner is within that bound.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -30,7 +32,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxDepth = 24;     // refinement levels of the membrane mask
-constexpr int kTile = 256;        // centroids per shared-memory tile
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 int status() { return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA; }
@@ -219,16 +220,112 @@ __global__ void k_children(const double* __restrict__ verts, int64_t nv,
   lab[2 * i + 1] = (double)l2;
 }
 
-// One thread per grid point: nearest centroid over all children (tiles in shared
-// memory, lower index on ties), then the label on the point's side of its normal.
+// Uniform bucket grid over the query box (centroids outside it go to the border
+// buckets; every bucket's box is the tight box of its own centroids).
+struct Buckets {
+  double lo[3], inv[3];
+  int32_t n[3];
+};
+
+__device__ __forceinline__ int64_t bucket_of(const Buckets& g, const double* c) {
+  int64_t idx = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double t = (c[d] - g.lo[d]) * g.inv[d];
+    const int i = isfinite(t) ? (int)fmin(fmax(floor(t), 0.0), (double)(g.n[d] - 1)) : 0;
+    idx = idx * g.n[d] + i;
+  }
+  return idx;
+}
+
+__global__ void k_bucket_count(const double* __restrict__ cen, int64_t nc, Buckets g,
+                               int32_t* __restrict__ count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nc) atomicAdd(&count[bucket_of(g, cen + 3 * i)], 1);
+}
+
+// Exclusive scan of cnt[0..n) into off[0..n] by one block of 1024 threads
+// (flags: the counts are turned into 0/1 first).
+__global__ void k_scan(const int32_t* __restrict__ cnt, int64_t n, int flags,
+                       int32_t* __restrict__ off) {
+  __shared__ int32_t sh[1024];
+  const int T = blockDim.x;
+  const int64_t per = (n + T - 1) / T;
+  const int64_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+  int32_t s = 0;
+  for (int64_t i = b; i < e; ++i) s += flags ? (cnt[i] > 0) : cnt[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    const int32_t v = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int32_t run = sh[threadIdx.x] - s;
+  for (int64_t i = b; i < e; ++i) {
+    off[i] = run;
+    run += flags ? (cnt[i] > 0) : cnt[i];
+  }
+  if (threadIdx.x == T - 1) off[n] = sh[T - 1];
+}
+
+__global__ void k_bucket_fill(const double* __restrict__ cen, int64_t nc, Buckets g,
+                              const int32_t* __restrict__ off, int32_t* __restrict__ cursor,
+                              int32_t* __restrict__ slot) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const int64_t b = bucket_of(g, cen + 3 * i);
+  slot[off[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
+}
+
+// Non-empty buckets, in bucket order: tight box, first slot and count.
+struct BucketRec {
+  double lo[3], hi[3];
+  int32_t first, count;
+};
+
+__global__ void k_bucket_boxes(const int32_t* __restrict__ off, const int32_t* __restrict__ nz_off,
+                               const int32_t* __restrict__ slot, const double* __restrict__ cen,
+                               int64_t nb, BucketRec* __restrict__ rec) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int32_t s0 = off[b], s1 = off[b + 1];
+  if (s1 == s0) return;
+  BucketRec r;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r.lo[d] = INFINITY;
+    r.hi[d] = -INFINITY;
+  }
+  for (int32_t s = s0; s < s1; ++s) {
+    const double* c = cen + 3 * (int64_t)slot[s];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      r.lo[d] = fmin(r.lo[d], c[d]);
+      r.hi[d] = fmax(r.hi[d], c[d]);
+    }
+  }
+  r.first = s0;
+  r.count = s1 - s0;
+  rec[nz_off[b]] = r;
+}
+
+// One thread per grid point.  Pass 1: U = the smallest farthest-corner distance
+// over the non-empty buckets (some centroid lies within it).  Pass 2: the
+// centroids of every bucket whose nearest corner is within min(U, best), the
+// nearest by (distance, child index).  Then the label on the point's side.
+constexpr int kRecTile = 64;
 __global__ void __launch_bounds__(kThreads)
     k_nearest_label(const double* __restrict__ cen, const double* __restrict__ nrm,
-                    const double* __restrict__ lab, int64_t nc, Axes a,
-                    double* __restrict__ out) {
-  __shared__ double sc[kTile][3];
+                    const double* __restrict__ lab, const int32_t* __restrict__ slot,
+                    const BucketRec* __restrict__ rec, const int32_t* __restrict__ n_rec_p,
+                    Axes a, double* __restrict__ out) {
+  __shared__ BucketRec sr[kRecTile];
   const int64_t npts = (int64_t)a.n[0] * a.n[1] * a.n[2];
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = p < npts;
+  const int32_t n_rec = *n_rec_p;
   double q[3] = {0.0, 0.0, 0.0};
   if (live) {
     const int64_t nyz = (int64_t)a.n[1] * a.n[2];
@@ -237,19 +334,48 @@ __global__ void __launch_bounds__(kThreads)
     q[1] = grid_value(a, 1, iy);
     q[2] = grid_value(a, 2, iz);
   }
-  double best = INFINITY;
-  int64_t bi = 0;
-  for (int64_t t0 = 0; t0 < nc; t0 += kTile) {
-    const int cnt = (int)(nc - t0 < kTile ? nc - t0 : kTile);
+  constexpr double kSlack = 1.0 + 1e-12;  // rounding of the box distances
+  double U = INFINITY;
+  for (int t0 = 0; t0 < n_rec; t0 += kRecTile) {
+    const int cnt = min(kRecTile, n_rec - t0);
     __syncthreads();
-    for (int k = threadIdx.x; k < cnt * 3; k += blockDim.x) sc[k / 3][k % 3] = cen[3 * t0 + k];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sr[k] = rec[t0 + k];
     __syncthreads();
     for (int k = 0; k < cnt; ++k) {
-      const double dx = sc[k][0] - q[0], dy = sc[k][1] - q[1], dz = sc[k][2] - q[2];
-      const double d = dx * dx + dy * dy + dz * dz;
-      if (d < best) {
-        best = d;
-        bi = t0 + k;
+      double far2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double f = fmax(fabs(q[d] - sr[k].lo[d]), fabs(q[d] - sr[k].hi[d]));
+        far2 += f * f;
+      }
+      U = fmin(U, far2);
+    }
+  }
+  double best = INFINITY;
+  int64_t bi = 0;
+  for (int t0 = 0; t0 < n_rec; t0 += kRecTile) {
+    const int cnt = min(kRecTile, n_rec - t0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sr[k] = rec[t0 + k];
+    __syncthreads();
+    if (!live) continue;
+    for (int k = 0; k < cnt; ++k) {
+      double near2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double e = fmax(fmax(sr[k].lo[d] - q[d], q[d] - sr[k].hi[d]), 0.0);
+        near2 += e * e;
+      }
+      if (near2 > fmin(U, best) * kSlack) continue;
+      for (int32_t s = sr[k].first; s < sr[k].first + sr[k].count; ++s) {
+        const int64_t c = slot[s];
+        const double dx = cen[3 * c] - q[0], dy = cen[3 * c + 1] - q[1],
+                     dz = cen[3 * c + 2] - q[2];
+        const double dd = dx * dx + dy * dy + dz * dz;
+        if (dd < best || (dd == best && c < bi)) {
+          best = dd;
+          bi = c;
+        }
       }
     }
   }
@@ -258,6 +384,24 @@ __global__ void __launch_bounds__(kThreads)
   const double dot = __dadd_rn(__dadd_rn(__dmul_rn(vx, nrm[3 * bi]), __dmul_rn(vy, nrm[3 * bi + 1])),
                                __dmul_rn(vz, nrm[3 * bi + 2]));
   out[p] = lab[2 * bi + (dot < 0.0 ? 1 : 0)] + 1.0;
+}
+
+// Bucket grid of about nc / 16 buckets over the query box (at most 2^21).
+Buckets bucket_grid(const dm_box* b, int64_t nc) {
+  Buckets g;
+  double L[3], vol = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    L[d] = b->hi[d] > b->lo[d] ? b->hi[d] - b->lo[d] : 1.0;
+    vol *= L[d];
+  }
+  const double target = std::max<double>(1.0, std::min<double>((double)nc / 16.0, 1 << 21));
+  const double h = cbrt(vol / target);
+  for (int d = 0; d < 3; ++d) {
+    g.n[d] = (int32_t)std::max(1.0, std::min(128.0, ceil(L[d] / h)));
+    g.lo[d] = b->lo[d];
+    g.inv[d] = g.n[d] / L[d];
+  }
+  return g;
 }
 
 bool box_fine(const dm_box* b) {
@@ -272,12 +416,50 @@ bool box_fine(const dm_box* b) {
 
 using namespace dm;
 
+namespace {
+// Instance-mask workspace: status word, children (centroid, normal, labels: 8
+// doubles), bucket counts / offsets / cursors and non-empty offsets (4 int32 per
+// bucket), slots (1 int32 per child), bucket records.
+size_t instance_layout(int64_t nc, int64_t nb, char* base, double** cen, int32_t** cnt,
+                              int32_t** off, int32_t** cur, int32_t** nzo, int32_t** slot,
+                              BucketRec** rec) {
+  size_t o = 256;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o += (bytes + 255) / 256 * 256;
+    return base ? base + at : nullptr;
+  };
+  char* c0 = take(sizeof(double) * 8 * (size_t)nc);
+  char* c1 = take(sizeof(int32_t) * (size_t)(nb + 1));
+  char* c2 = take(sizeof(int32_t) * (size_t)(nb + 1));
+  char* c3 = take(sizeof(int32_t) * (size_t)(nb + 1));
+  char* c4 = take(sizeof(int32_t) * (size_t)(nb + 1));
+  char* c5 = take(sizeof(int32_t) * (size_t)nc);
+  char* c6 = take(sizeof(BucketRec) * (size_t)nb);
+  if (base) {
+    *cen = (double*)c0;
+    *cnt = (int32_t*)c1;
+    *off = (int32_t*)c2;
+    *cur = (int32_t*)c3;
+    *nzo = (int32_t*)c4;
+    *slot = (int32_t*)c5;
+    *rec = (BucketRec*)c6;
+  }
+  return o;
+}
+
+}  // namespace
+
 extern "C" {
 
-size_t dm_mask_workspace_size(int64_t nt, int32_t levels) {
+size_t dm_mask_workspace_size(int64_t nt, int32_t levels, const dm_box* box) {
   if (nt < 0 || levels < 0 || levels > 8) return 0;
-  const int64_t nc = nt << (2 * levels);
-  return 256 + sizeof(double) * 8 * (size_t)std::max<int64_t>(nc, 1);
+  if (!box) return 256;
+  const int64_t nc = std::max<int64_t>(nt << (2 * levels), 1);
+  const Buckets g = bucket_grid(box, nc);
+  const int64_t nb = (int64_t)g.n[0] * g.n[1] * g.n[2];
+  return instance_layout(nc, nb, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         nullptr);
 }
 
 int dm_membrane_mask(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
@@ -306,20 +488,35 @@ int dm_instance_mask(const double* verts, int64_t nv, const int64_t* faces, int6
   if (!box_fine(box) || !mask || !workspace || nv < 0 || nt <= 0 || !verts || !faces ||
       levels < 0 || levels > 8)
     return DM_ERR_INVALID_ARG;
-  if (ws_bytes < dm_mask_workspace_size(nt, levels)) return DM_ERR_WORKSPACE;
+  if (ws_bytes < dm_mask_workspace_size(nt, levels, box)) return DM_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t nc = nt << (2 * levels);
+  if (nc >= (int64_t)INT32_MAX) return DM_ERR_SIZE;
+  const Buckets g = bucket_grid(box, nc);
+  const int64_t nb = (int64_t)g.n[0] * g.n[1] * g.n[2];
   char* w = (char*)workspace;
   int* err = (int*)w;
-  double* cen = (double*)(w + 256);
+  double* cen;
+  int32_t *cnt, *off, *cur, *nzo, *slot;
+  BucketRec* rec;
+  instance_layout(nc, nb, w, &cen, &cnt, &off, &cur, &nzo, &slot, &rec);
   double* nrm = cen + 3 * nc;
   double* lab = nrm + 3 * nc;
   k_children<<<(unsigned)cdiv(nc, kThreads), kThreads, 0, st>>>(verts, nv, faces, nt, levels,
                                                                  cen, nrm, lab, err);
+  if (cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nb + 1), st) != cudaSuccess ||
+      cudaMemsetAsync(cur, 0, sizeof(int32_t) * (size_t)(nb + 1), st) != cudaSuccess)
+    return DM_ERR_CUDA;
+  const unsigned gc = (unsigned)cdiv(nc, kThreads), gb = (unsigned)cdiv(nb, kThreads);
+  k_bucket_count<<<gc, kThreads, 0, st>>>(cen, nc, g, cnt);
+  k_scan<<<1, 1024, 0, st>>>(cnt, nb, 0, off);
+  k_scan<<<1, 1024, 0, st>>>(cnt, nb, 1, nzo);  // nzo[nb] = non-empty buckets
+  k_bucket_fill<<<gc, kThreads, 0, st>>>(cen, nc, g, off, cur, slot);
+  k_bucket_boxes<<<gb, kThreads, 0, st>>>(off, nzo, slot, cen, nb, rec);
   const int64_t npts = (int64_t)box->shape[0] * box->shape[1] * box->shape[2];
-  k_nearest_label<<<(unsigned)cdiv(npts, kThreads), kThreads, 0, st>>>(cen, nrm, lab, nc,
-                                                                        make_axes(box), mask);
-  count_launches(2);
+  k_nearest_label<<<(unsigned)cdiv(npts, kThreads), kThreads, 0, st>>>(
+      cen, nrm, lab, slot, rec, nzo + nb, make_axes(box), mask);
+  count_launches(7);
   return status();
 }
 

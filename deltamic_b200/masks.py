@@ -12,7 +12,9 @@
   norm of the stacked edge vectors b-a, c-b, c-b), ``reorder_faces``,
   ``create_voxel_centroids``.
 
-Numpy inputs give numpy results (drop-in); the work runs on ``device``.  The
+Numpy inputs give numpy results (drop-in); the work runs on ``device``.  The label
+mask's nearest-centroid search buckets the child faces' centroids on a uniform grid
+(exact; ties to the lower child index).  The
 refinement (trimesh's ``subdivide_to_size`` / the reference's
 ``subdivide_with_materials``) happens inside the kernels, face by face.
 """
@@ -132,7 +134,7 @@ def create_instance_segmentation_mask(verts, faces, box_shape, box_size, device=
     V = _dev(vz, torch.float64, device)
     F = _dev(fz.astype(np.int64), torch.int64, device)
     lib = N.lib()
-    nbytes = lib.dm_mask_workspace_size(F.shape[0], levels)
+    nbytes = lib.dm_mask_workspace_size(F.shape[0], levels, ctypes.byref(cbox))
     ws = torch.zeros(max(nbytes, 256), dtype=torch.uint8, device=V.device)
     out = torch.empty(tuple(int(s) for s in shape), dtype=torch.float64, device=V.device)
     N.check(lib.dm_instance_mask(N.ptr(V), V.shape[0], N.ptr(F), F.shape[0], ctypes.byref(cbox),

@@ -271,9 +271,10 @@ int dm_zernike(const float* r, const float* theta, int64_t n_points, const int32
  * is flipped, reorder_faces :49-53) split four ways `levels` times
  * (subdivide_with_materials, :60-176); mask[p] = 1 + the label, on grid point p's
  * side of the normal, of the child face whose centroid is nearest to p (ties: the
- * lower child index).  Exhaustive nearest search: cost grid points x nt 4^levels.
- * Workspace from dm_mask_workspace_size(nt, levels); status via dm_device_error. */
-size_t dm_mask_workspace_size(int64_t nt, int32_t levels);
+ * lower child index); the nearest search buckets the child centroids on a uniform
+ * grid over the box.  Workspace from dm_mask_workspace_size(nt, levels, box) (box
+ * NULL: the membrane mask's 256 bytes); status via dm_device_error. */
+size_t dm_mask_workspace_size(int64_t nt, int32_t levels, const dm_box* box);
 int dm_membrane_mask(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
                      int32_t face_stride, const dm_box* box, double max_edge, int32_t max_depth,
                      double* mask, void* workspace, size_t ws_bytes, dm_stream_t stream);

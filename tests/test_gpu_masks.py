@@ -42,7 +42,7 @@ def _two_cells():
     return combine_all_verts_faces_mm([v1, v2], mm)
 
 
-@pytest.mark.parametrize("shape", [(12, 10, 9), (24, 20, 18), (64, 48, 48)])
+@pytest.mark.parametrize("shape", [(12, 10, 9), (24, 20, 18), (64, 48, 48), (96, 80, 72)])
 def test_instance_mask_matches_oracle(shape):
     V, F = _two_cells()
     box = _box(V, 0.1)
