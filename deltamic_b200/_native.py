@@ -126,6 +126,7 @@ SIGNATURES = {
                                       _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     "dm_conv3d_s2_workspace_size": (_SZ, [_INT] * 6),
     "dm_conv3d_s2_forward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _P, _INT, _P, _P, _P]),
+    "dm_conv3d_s2_device_error": (_INT, [ctypes.POINTER(_INT), _P]),
     "dm_conv3d_s2_backward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P, _P, _P,
                                      _P, _P, _SZ, _P]),
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),

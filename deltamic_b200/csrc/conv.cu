@@ -1,6 +1,6 @@
 // 3x3x3 stride-2 padding-1 3D convolutions (channels-last, BF16 operands, FP32
-// accumulation on the tensor cores) with a fused bias + GELU epilogue, and their
-// adjoints.  They run the learned initialiser's encoder (no counterpart in the
+// accumulation in tensor memory by tcgen05 MMAs) with a fused bias + GELU epilogue,
+// and their adjoints.  They run the learned initialiser's encoder (no counterpart in the
 // reference).  All three products are implicit GEMMs over one generic tiled
 // kernel with gather loaders:
 //   forward  C[m, n]  = sum_k  A[m, k] W[k, n]       (A = im2col of x, on the fly)
@@ -11,20 +11,21 @@
 // zero padding up to a multiple of 32), P = pre-activation, dP = dL/dP.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
-#include <mma.h>
 #include <stdint.h>
 
 #include <algorithm>
 
 #include "../../include/deltamic_b200.h"
 #include "band_internal.h"
+#include "tcgen05.cuh"
 
 namespace dm {
 
 using bf16 = __nv_bfloat16;
-using namespace nvcuda;
 
-constexpr int kBM = 64, kBK = 32, kConvThreads = 128;
+// Tile: 128 output rows (the MMA's M, one TMEM lane each) x BN columns, reduction
+// staged 32 elements at a time (two K = 16 MMAs) through two shared-memory stages.
+constexpr int kBM = 128, kBK = 32, kConvThreads = 128;
 
 struct ConvShape {
   int B, D, H, W, Ci;      // input
@@ -39,71 +40,182 @@ __device__ __forceinline__ float gelu_grad(float x) {
          x * expf(-0.5f * x * x) * 0.39894228040143268f;
 }
 
+// Output voxel m -> (b, od, oh, ow).
+__device__ __forceinline__ void out_voxel(const ConvShape& s, int64_t m, int& b, int& od, int& oh,
+                                          int& ow) {
+  int64_t t = m;
+  ow = (int)(t % s.Wo); t /= s.Wo;
+  oh = (int)(t % s.Ho); t /= s.Ho;
+  od = (int)(t % s.Do);
+  b = (int)(t / s.Do);
+}
+
+// Offset of x[b, d, h, w, 0] for the tap (kd, kh, kw) of output voxel m, or -1 in
+// the zero padding.
+__device__ __forceinline__ int64_t tap_offset(const ConvShape& s, int64_t m, int tap) {
+  const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+  int b, od, oh, ow;
+  out_voxel(s, m, b, od, oh, ow);
+  const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
+  if (d < 0 || d >= s.D || h < 0 || h >= s.H || w < 0 || w >= s.W) return -1;
+  return ((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci;
+}
+
 // im2col element A[m, k] of x (zero outside the volume and in the K padding).
 __device__ __forceinline__ bf16 im2col(const bf16* __restrict__ x, const ConvShape& s, int64_t m,
                                        int k) {
   if (k >= s.K) return __float2bfloat16(0.f);
-  const int ci = k % s.Ci;
-  const int tap = k / s.Ci;
-  const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
-  int64_t t = m;
-  const int ow = (int)(t % s.Wo); t /= s.Wo;
-  const int oh = (int)(t % s.Ho); t /= s.Ho;
-  const int od = (int)(t % s.Do);
-  const int b = (int)(t / s.Do);
-  const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
-  if (d < 0 || d >= s.D || h < 0 || h >= s.H || w < 0 || w >= s.W) return __float2bfloat16(0.f);
-  return x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + ci];
+  const int64_t o = tap_offset(s, m, k / s.Ci);
+  return o < 0 ? __float2bfloat16(0.f) : x[o + k % s.Ci];
 }
 
-// Generic tile: C[rows x BN] over a reduction [r_begin, r_end) split by blockIdx.y.
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// Eight consecutive reduction elements red0..red0+7 of row ``row`` of A (zero past
+// ``rows`` and ``r_end``): one 16-byte load where the loader offers it, else
+// element by element.
+template <class LA>
+__device__ __forceinline__ uint4 gather8_a(const LA& la, int64_t row, int64_t rows, int64_t red0,
+                                           int64_t r_end) {
+  uint4 v = make_uint4(0u, 0u, 0u, 0u);
+  if (row >= rows || red0 >= r_end) return v;
+  if (red0 + 8 <= r_end && la.load8(row, red0, v)) return v;
+  const bf16 z = __float2bfloat16(0.f);
+  bf16 e[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) e[j] = red0 + j < r_end ? la(row, red0 + j) : z;
+  return make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
+}
+
+// B[red0..red0+7, col] (zero past r_end).
+template <class LB>
+__device__ __forceinline__ uint4 gather8_b(const LB& lb, int col, int64_t red0, int64_t r_end) {
+  uint4 v = make_uint4(0u, 0u, 0u, 0u);
+  if (red0 >= r_end) return v;
+  if (red0 + 8 <= r_end && lb.load8(red0, col, v)) return v;
+  const bf16 z = __float2bfloat16(0.f);
+  bf16 e[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) e[j] = red0 + j < r_end ? lb(red0 + j, col) : z;
+  return make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
+}
+
+// Shared memory of one tile: two stages of A [128 x 32] and B [BN x 32] in the
+// K-major no-swizzle layout, two mbarriers and the TMEM address slot.  The size is
+// padded so that the CTAs one SM can hold never ask for more than its 512 TMEM
+// columns together (228 KB of shared memory per SM; 16 CTAs of 128 threads at most).
+template <int BN>
+struct UmmaTile {
+  static constexpr int kCols = tc::tmem_cols<BN>();
+  static constexpr int kStageA = kBM * kBK;  // elements
+  static constexpr int kStageB = BN * kBK;
+  static constexpr int kStageBytes = (kStageA + kStageB) * 2;
+  static constexpr int kMaxCtas = 512 / kCols;
+  static constexpr int kMinSmem = kMaxCtas >= 16 ? 0 : 233472 / (kMaxCtas + 1) + 128;
+  static constexpr int kUsed = 2 * kStageBytes + 64;
+  static constexpr int kSmem = ((kUsed > kMinSmem ? kUsed : kMinSmem) + 127) / 128 * 128;
+  static_assert(kSmem <= 48 * 1024, "tile shared memory above the default 48 KB");
+  static_assert(kStageBytes % 16 == 0, "stage alignment");
+};
+
+// Generic tile: C[rows x BN] over a reduction [r_begin, r_end) split by blockIdx.y,
+// C = sum_k A[row, k] B[k, col] with A = la(row, k), B = lb(k, col), then ep(row,
+// col, split, C).  Every thread gathers its share of a stage into shared memory;
+// one thread issues the stage's two tcgen05 MMAs into the TMEM accumulator and
+// commits them to the stage's mbarrier, so the next stage's gather overlaps them.
+// Each warp reads its 32 accumulator rows back from TMEM for the epilogue.
 template <int BN, class LA, class LB, class EP>
-__global__ void __launch_bounds__(kConvThreads) k_conv_gemm(LA la, LB lb, EP ep, int64_t rows,
-                                                            int64_t red_total, int64_t red_split) {
-  __shared__ __align__(32) bf16 As[kBM][kBK + 8];
-  __shared__ __align__(32) bf16 Bs[kBK][BN + 8];
-  __shared__ __align__(32) float Cs[kBM][BN + 4];
+__global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la, LB lb, EP ep, int64_t rows,
+                                                            int64_t red_total, int64_t red_split,
+                                                            int* err) {
+  using T = UmmaTile<BN>;
+  extern __shared__ __align__(128) uint8_t smem[];
+  bf16* const As0 = (bf16*)smem;
+  bf16* const Bs0 = (bf16*)(smem + T::kStageA * 2);
+  uint64_t* const bar = (uint64_t*)(smem + 2 * T::kStageBytes);
+  uint32_t* const slot = (uint32_t*)(bar + 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row0 = (int64_t)blockIdx.x * kBM;
   const int64_t r_begin = (int64_t)blockIdx.y * red_split;
   const int64_t r_end = min(red_total, r_begin + red_split);
-  const int warp = threadIdx.x >> 5;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[BN / 16];
-#pragma unroll
-  for (int j = 0; j < BN / 16; ++j) wmma::fill_fragment(acc[j], 0.0f);
-  const bf16 zero = __float2bfloat16(0.f);
-  for (int64_t k0 = r_begin; k0 < r_end; k0 += kBK) {
-    for (int e = threadIdx.x; e < kBM * kBK; e += kConvThreads) {
-      const int r = e / kBK, c = e % kBK;
-      const int64_t row = row0 + r, red = k0 + c;
-      As[r][c] = (row < rows && red < r_end) ? la(row, red) : zero;
-    }
-    for (int e = threadIdx.x; e < kBK * BN; e += kConvThreads) {
-      const int r = e / BN, c = e % BN;
-      const int64_t red = k0 + r;
-      Bs[r][c] = red < r_end ? lb(red, c) : zero;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 16) {
-      wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
-      wmma::load_matrix_sync(a, &As[warp * 16][kk], kBK + 8);
-#pragma unroll
-      for (int j = 0; j < BN / 16; ++j) {
-        wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
-        wmma::load_matrix_sync(b, &Bs[kk][j * 16], BN + 8);
-        wmma::mma_sync(acc[j], a, b, acc[j]);
-      }
-    }
-    __syncthreads();
+  const int nk = r_end > r_begin ? (int)((r_end - r_begin + kBK - 1) / kBK) : 0;
+
+  if (warp == 0) tc::tmem_alloc(slot, T::kCols);
+  if (threadIdx.x == 32) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
   }
-#pragma unroll
-  for (int j = 0; j < BN / 16; ++j)
-    wmma::store_matrix_sync(&Cs[warp * 16][j * 16], acc[j], BN + 4, wmma::mem_row_major);
+  tc::fence_before_sync();
   __syncthreads();
-  for (int e = threadIdx.x; e < kBM * BN; e += kConvThreads) {
-    const int r = e / BN, c = e % BN;
-    const int64_t row = row0 + r;
-    if (row < rows) ep(row, c, (int)blockIdx.y, Cs[r][c]);
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+  constexpr uint32_t idesc = tc::idesc_bf16_f32<kBM, BN>();
+
+  bool ok = true;
+  int issued = 0;
+  for (int t = 0; t < nk; ++t) {
+    const int s = t & 1;
+    bf16* const As = As0 + s * (T::kStageBytes / 2);
+    bf16* const Bs = Bs0 + s * (T::kStageBytes / 2);
+    // the MMAs of stage t - 2 read this buffer: wait for their commit
+    if (t >= 2) ok = mbar_wait_bounded(&bar[s], (uint32_t)(((t - 2) >> 1) & 1), err);
+    const int64_t k0 = r_begin + (int64_t)t * kBK;
+    // chunk e: row (e & 7) + 8 (e >> 5), reduction chunk (e >> 3) & 3 -- eight lanes
+    // store one 128-byte core-matrix column (no bank conflicts), and tiles with at
+    // most 32 live rows still spread over every thread
+#pragma unroll
+    for (int i = 0; i < kBM * (kBK / 8) / kConvThreads; ++i) {
+      const int e = threadIdx.x + i * kConvThreads;
+      const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
+      if (row0 + r < rows)
+        *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) =
+            gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end);
+      else if (t < 2)  // dead rows: zero once per stage buffer
+        *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int e = threadIdx.x; e < BN * (kBK / 8); e += kConvThreads) {
+      const int n = e % BN, kc = e / BN;
+      *(uint4*)(Bs + tc::kmaj32_off(n, kc * 8)) = gather8_b(lb, n, k0 + kc * 8, r_end);
+    }
+    fence_proxy_async();  // generic-proxy stores -> the MMA's async-proxy reads
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    if (threadIdx.x == 0) {
+      tc::fence_after_sync();
+      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+#pragma unroll
+      for (int kk = 0; kk < kBK / 16; ++kk)
+        tc::mma_bf16(tmem, tc::smem_desc(a0 + kk * 256), tc::smem_desc(b0 + kk * 256), idesc,
+                     t > 0 || kk > 0);
+      tc::commit(&bar[s]);
+    }
+    issued = t + 1;
+  }
+  // the last commit of each stage not yet waited for: every MMA of the tile is
+  // done, and no commit arrives on a barrier after the block has left
+  for (int t = issued >= 2 ? issued - 2 : 0; t < issued; ++t)
+    ok = mbar_wait_bounded(&bar[t & 1], (uint32_t)((t >> 1) & 1), err) && ok;
+  tc::fence_after_sync();
+  const int64_t row = row0 + warp * 32 + lane;
+#pragma unroll
+  for (int c = 0; c < BN; c += 16) {
+    float v[16];
+    tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (row < rows) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) ep(row, c + j, (int)blockIdx.y, issued > 0 ? v[j] : 0.f);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, T::kCols);
   }
 }
 
@@ -113,12 +225,39 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_gemm(LA la, LB lb, EP ep,
 struct FwdA {
   const bf16* x;
   ConvShape s;
+  bool vec;  // Ci % 8 == 0 and x 16-byte aligned: eight channels of one tap per load
   __device__ bf16 operator()(int64_t m, int64_t k) const { return im2col(x, s, m, (int)k); }
+  __device__ bool load8(int64_t m, int64_t k, uint4& v) const {
+    v = make_uint4(0u, 0u, 0u, 0u);
+    if (k >= s.K) return true;
+    if (vec) {
+      const int64_t o = tap_offset(s, m, (int)(k / s.Ci));
+      if (o >= 0) v = *(const uint4*)(x + o + k % s.Ci);
+      return true;
+    }
+    // chunk across taps (Ci < 8): the output voxel decomposed once
+    int b, od, oh, ow;
+    out_voxel(s, m, b, od, oh, ow);
+    const bf16 z = __float2bfloat16(0.f);
+    bf16 e[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int kj = (int)k + j, tap = kj / s.Ci;
+      const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+      const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
+      e[j] = (kj < s.K && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+                 ? x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + kj % s.Ci]
+                 : z;
+    }
+    v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
+    return true;
+  }
 };
 struct WeightB {  // W[k, n], row-major [Kp, Co]
   const bf16* w;
   int Co;
   __device__ bf16 operator()(int64_t k, int n) const { return w[k * Co + n]; }
+  __device__ bool load8(int64_t, int, uint4&) const { return false; }
 };
 struct FwdEp {
   const float* bias;
@@ -146,11 +285,42 @@ struct WgradA {  // A^T[k, m]
   const bf16* x;
   ConvShape s;
   __device__ bf16 operator()(int64_t k, int64_t m) const { return im2col(x, s, m, (int)k); }
+  // eight consecutive output voxels m.. at one (tap, ci): decomposed once, then stepped
+  __device__ bool load8(int64_t k, int64_t m, uint4& v) const {
+    v = make_uint4(0u, 0u, 0u, 0u);
+    if (k >= s.K) return true;
+    const int ci = (int)(k % s.Ci), tap = (int)(k / s.Ci);
+    const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+    int b, od, oh, ow;
+    out_voxel(s, m, b, od, oh, ow);
+    const bf16 z = __float2bfloat16(0.f);
+    bf16 e[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
+      e[j] = (b < s.B && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+                 ? x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + ci]
+                 : z;
+      if (++ow == s.Wo) {
+        ow = 0;
+        if (++oh == s.Ho) {
+          oh = 0;
+          if (++od == s.Do) {
+            od = 0;
+            ++b;
+          }
+        }
+      }
+    }
+    v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
+    return true;
+  }
 };
 struct DpreB {  // dP[m, n]
   const bf16* dp;
   int Co;
   __device__ bf16 operator()(int64_t m, int n) const { return dp[m * Co + n]; }
+  __device__ bool load8(int64_t, int, uint4&) const { return false; }
 };
 struct WgradEp {  // partial[split][k][n]
   float* part;
@@ -207,10 +377,9 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
   const bf16* dp;
   ConvShape s;
   Cls c;
-  __device__ bf16 operator()(int64_t q, int64_t r) const {
-    const int co = (int)(r % s.Co);
-    const int t = (int)(r / s.Co);
-    if (t >= c.T) return __float2bfloat16(0.f);
+  bool vec;  // dp 16-byte aligned (Co is a multiple of 8): eight channels per load
+  // Offset of dP[voxel reached from input voxel q through tap t, 0], or -1 outside.
+  __device__ int64_t offset(int64_t q, int t) const {
     int kk[3];
     cls_tap(c, t, kk);
     int64_t u = q;
@@ -220,23 +389,48 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
     const int b = (int)(u / c.n[0]);
     const int d = 2 * id + c.p[0], h = 2 * ih + c.p[1], w = 2 * iw + c.p[2];
     const int od = (d + 1 - kk[0]) >> 1, oh = (h + 1 - kk[1]) >> 1, ow = (w + 1 - kk[2]) >> 1;
-    if (od < 0 || od >= s.Do || oh < 0 || oh >= s.Ho || ow < 0 || ow >= s.Wo)
-      return __float2bfloat16(0.f);
-    return dp[((((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow) * s.Co + co];
+    if (od < 0 || od >= s.Do || oh < 0 || oh >= s.Ho || ow < 0 || ow >= s.Wo) return -1;
+    return ((((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow) * s.Co;
+  }
+  __device__ bf16 operator()(int64_t q, int64_t r) const {
+    const int t = (int)(r / s.Co);
+    if (t >= c.T) return __float2bfloat16(0.f);
+    const int64_t o = offset(q, t);
+    return o < 0 ? __float2bfloat16(0.f) : dp[o + r % s.Co];
+  }
+  __device__ bool load8(int64_t q, int64_t r, uint4& v) const {
+    if (!vec) return false;
+    v = make_uint4(0u, 0u, 0u, 0u);
+    const int t = (int)(r / s.Co);
+    if (t >= c.T) return true;
+    const int64_t o = offset(q, t);
+    if (o >= 0) v = *(const uint4*)(dp + o + r % s.Co);
+    return true;
   }
 };
 struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
   const bf16* w;
   ConvShape s;
   Cls c;
-  __device__ bf16 operator()(int64_t r, int ci) const {
-    const int co = (int)(r % s.Co);
-    const int t = (int)(r / s.Co);
-    if (t >= c.T || ci >= s.Ci) return __float2bfloat16(0.f);
+  bool vec;  // w 16-byte aligned (Co is a multiple of 8): eight co per load
+  __device__ int64_t offset(int t, int ci) const {
     int kk[3];
     cls_tap(c, t, kk);
     const int tap = (kk[0] * 3 + kk[1]) * 3 + kk[2];
-    return w[((int64_t)tap * s.Ci + ci) * s.Co + co];
+    return ((int64_t)tap * s.Ci + ci) * s.Co;
+  }
+  __device__ bf16 operator()(int64_t r, int ci) const {
+    const int t = (int)(r / s.Co);
+    if (t >= c.T || ci >= s.Ci) return __float2bfloat16(0.f);
+    return w[offset(t, ci) + r % s.Co];
+  }
+  __device__ bool load8(int64_t r, int ci, uint4& v) const {
+    if (!vec) return false;
+    v = make_uint4(0u, 0u, 0u, 0u);
+    const int t = (int)(r / s.Co);
+    if (t >= c.T || ci >= s.Ci) return true;
+    v = *(const uint4*)(w + offset(t, ci) + r % s.Co);
+    return true;
   }
 };
 struct DgradEp {
@@ -258,18 +452,39 @@ struct DgradEp {
 // ---------------------------------------------------------------------------
 // launchers
 
+// Status word of the convolution kernels (bounded waits that gave up).
+__device__ int g_conv_status;
+
+static int* conv_status_ptr() {
+  static int* p = nullptr;
+  if (!p) {
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_conv_status) == cudaSuccess) p = (int*)a;
+  }
+  return p;
+}
+
+template <int BN, class LA, class LB, class EP>
+static void umma_launch(LA la, LB lb, EP ep, int64_t rows, int64_t red, int64_t red_split,
+                        int splits, cudaStream_t st) {
+  const dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)splits);
+  k_conv_umma<BN><<<grid, kConvThreads, UmmaTile<BN>::kSmem, st>>>(la, lb, ep, rows, red,
+                                                                    red_split, conv_status_ptr());
+}
+
 template <class LA, class LB, class EP>
 static void gemm_launch(int bn, LA la, LB lb, EP ep, int64_t rows, int64_t red, int64_t red_split,
                         int splits, cudaStream_t st) {
-  const dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)splits);
   switch (bn) {
-    case 16: k_conv_gemm<16><<<grid, kConvThreads, 0, st>>>(la, lb, ep, rows, red, red_split); break;
-    case 32: k_conv_gemm<32><<<grid, kConvThreads, 0, st>>>(la, lb, ep, rows, red, red_split); break;
-    case 64: k_conv_gemm<64><<<grid, kConvThreads, 0, st>>>(la, lb, ep, rows, red, red_split); break;
-    default: k_conv_gemm<128><<<grid, kConvThreads, 0, st>>>(la, lb, ep, rows, red, red_split); break;
+    case 16: umma_launch<16>(la, lb, ep, rows, red, red_split, splits, st); break;
+    case 32: umma_launch<32>(la, lb, ep, rows, red, red_split, splits, st); break;
+    case 64: umma_launch<64>(la, lb, ep, rows, red, red_split, splits, st); break;
+    default: umma_launch<128>(la, lb, ep, rows, red, red_split, splits, st); break;
   }
   count_launches(1);
 }
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 static int pad_cols(int c) { return c <= 16 ? 16 : (c <= 32 ? 32 : (c <= 64 ? 64 : 128)); }
 
@@ -300,8 +515,8 @@ size_t conv_ws_bytes(const ConvShape& s) {
 
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st) {
-  gemm_launch(s.Co, FwdA{x, s}, WeightB{w, s.Co}, FwdEp{bias, pre, act, s.Co}, s.M, s.Kp, s.Kp,
-              1, st);
+  gemm_launch(s.Co, FwdA{x, s, s.Ci % 8 == 0 && aligned16(x)}, WeightB{w, s.Co},
+              FwdEp{bias, pre, act, s.Co}, s.M, s.Kp, s.Kp, 1, st);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -343,8 +558,8 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
       if (empty) continue;
       const int64_t rows = (int64_t)s.B * c.n[0] * c.n[1] * c.n[2];
       const int64_t red = ((int64_t)c.T * s.Co + kBK - 1) / kBK * kBK;
-      gemm_launch(pad_cols(s.Ci), DgradA{dp, s, c}, DgradB{w, s, c}, DgradEp{dx, s, c}, rows, red,
-                  red, 1, st);
+      gemm_launch(pad_cols(s.Ci), DgradA{dp, s, c, aligned16(dp)}, DgradB{w, s, c, aligned16(w)},
+                  DgradEp{dx, s, c}, rows, red, red, 1, st);
     }
   }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
@@ -369,6 +584,20 @@ int dm_conv3d_s2_forward(const uint16_t* x, int B, int D, int H, int W, int Ci, 
   if (!x || !w || !pre || !act) return DM_ERR_INVALID_ARG;
   return dm::launch_conv_forward(s, (const dm::bf16*)x, (const dm::bf16*)w, bias, pre,
                                  (dm::bf16*)act, (cudaStream_t)stream);
+}
+
+int dm_conv3d_s2_device_error(int* out_flags, dm_stream_t stream) {
+  if (!out_flags) return DM_ERR_INVALID_ARG;
+  int* p = dm::conv_status_ptr();
+  if (!p) return DM_ERR_CUDA;
+  int v = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&v, p, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return DM_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return DM_ERR_CUDA;
+  if (cudaMemsetAsync(p, 0, sizeof(int), st) != cudaSuccess) return DM_ERR_CUDA;
+  *out_flags = v;
+  return DM_OK;
 }
 
 int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,

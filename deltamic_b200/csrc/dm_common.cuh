@@ -83,7 +83,8 @@ __device__ __forceinline__ void set_error(int* err, int code) {
 
 // ---------------------------------------------------------------------------
 // Bulk-copy (TMA) staging into shared memory with mbarrier completion.
-// Plain CTA-local copies: no cluster multicast anywhere in this library.
+// Plain CTA-local copies: every copy lands in the issuing block's own shared
+// memory, from this GPU's global memory.
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);

@@ -3,7 +3,8 @@ per-vertex displacements of a level-4 icosphere template, giving the fitting loo
 a starting mesh closer than the sphere (no counterpart in the reference).
 
 Network: four 3x3x3 stride-2 convolutions 1 -> 16 -> 32 -> 64 -> 128 with GELU
-(BF16 tensor-core implicit GEMMs of ``csrc/conv.cu``, FP32 accumulation), global
+(BF16 implicit GEMMs of ``csrc/conv.cu`` on tcgen05 tensor cores, FP32
+accumulators in tensor memory), global
 average pooling, then an MLP 128 -> 512 (GELU) -> 2,562 x 3.  Training pairs are
 rendered by this package's own renderer (``BatchRenderer``) from random
 spherical-harmonic shapes with random anisotropic Gaussian PSFs and
@@ -22,7 +23,8 @@ from . import _native as N
 from .batch import BatchRenderer
 from .mesh import icosphere, real_sph_harm
 
-__all__ = ["LearnedInit", "conv3d_s2", "ShapeSampler", "render_batch", "train_learned_init"]
+__all__ = ["LearnedInit", "conv3d_s2", "conv_status_check", "ShapeSampler", "render_batch",
+           "train_learned_init"]
 
 CHANNELS = (1, 16, 32, 64, 128)
 IMAGE = 64
@@ -68,6 +70,15 @@ class _ConvS2(torch.autograd.Function):
                                           N.ptr(ws), ws.numel(), N.stream_ptr(x.device)),
                 "dm_conv3d_s2_backward")
         return (dx.to(x.dtype) if dx is not None else None), dw, db
+
+
+def conv_status_check(device):
+    """Raise if a convolution kernel gave up a bounded wait since the last check
+    (reads and clears the kernels' status word; synchronises ``device``'s stream)."""
+    flags = ctypes.c_int(0)
+    N.check(N.lib().dm_conv3d_s2_device_error(ctypes.byref(flags), N.stream_ptr(device)),
+            "dm_conv3d_s2_device_error")
+    N.check(flags.value, "convolution kernels")
 
 
 def conv3d_s2(x, w32, b32):
@@ -193,6 +204,7 @@ def train_learned_init(n_train, epochs, batch=64, lr=1e-3, seed=0, device="cuda"
             sched.step()
             tot += loss.detach() * len(idx)
         hist.append(float(tot) / n_train)
+        conv_status_check(torch.device(device))
         if log:
             log(f"epoch {ep}: vertex MSE {hist[-1]:.3e}")
     return model, sampler, hist

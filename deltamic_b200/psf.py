@@ -333,10 +333,11 @@ class Gibson_Lanni_psf(nn.Module):
         rhomax = min([NA, self.ns, self.ni, self.ni0, self.ng, self.ng0]) / NA
         # the reference's float32 sample points (torch's CPU linspace), moved over
         rho = torch.linspace(0, rhomax.item(), self.num_samples).to(dev)
-        thresh = -self.Seps
-        for n_, r_ in ((self.ns, rhomax), (self.ni, rhomax), (self.ni0, rho), (self.ns, rho),
-                       (self.ng0, rho)):
-            assert float((n_ * n_ - NA * NA * r_ * r_).min()) >= thresh
+        with torch.no_grad():  # the reference's five domain asserts, read back once
+            lows = torch.stack([(n_ * n_ - NA * NA * r_ * r_).min() for n_, r_ in (
+                (self.ns, rhomax), (self.ni, rhomax), (self.ni0, rho), (self.ns, rho),
+                (self.ng0, rho))])
+            assert float(lows.min()) >= -self.Seps
         zv = (self.res_axial * torch.arange(-self.size_z / 2, self.size_z / 2, device=dev)
               + self.res_axial / 2).type(torch.double)
         na2r2 = NA * NA * rho * rho

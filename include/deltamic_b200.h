@@ -399,14 +399,18 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
  * initialiser's encoder (no counterpart in the reference).  Channels-last BF16
  * tensors (uint16 storage): x[B,D,H,W,Ci], w[Kp,Co] with row k = ((kd*3+kh)*3+kw)*Ci
  * + ci and Kp = 27*Ci rounded up to 32 (padding rows zero); Co in {16,32,64,128},
- * Ci <= 128; output (D+1)/2 x (H+1)/2 x (W+1)/2.  Tensor-core products with FP32
- * accumulation.  Forward writes pre[.., Co] (FP32 pre-activation) and act = GELU(pre)
- * (BF16).  Backward takes dact = dL/dact (FP32) and writes dw[Kp,Co], db[Co] and,
- * if dx != NULL, dx = dL/dx (FP32); deterministic (no atomics). */
+ * Ci <= 128; output (D+1)/2 x (H+1)/2 x (W+1)/2.  Implicit GEMMs on the fifth-
+ * generation tensor cores (tcgen05 MMAs, FP32 accumulators in tensor memory).
+ * Forward writes pre[.., Co] (FP32 pre-activation) and act = GELU(pre) (BF16).
+ * Backward takes dact = dL/dact (FP32) and writes dw[Kp,Co], db[Co] and, if
+ * dx != NULL, dx = dL/dx (FP32); deterministic (no atomics).
+ * dm_conv3d_s2_device_error reads and clears the kernels' status word
+ * (DM_ERR_TIMEOUT: a bounded wait for the tensor cores gave up); synchronous. */
 size_t dm_conv3d_s2_workspace_size(int B, int D, int H, int W, int Ci, int Co);
 int dm_conv3d_s2_forward(const uint16_t* x, int B, int D, int H, int W, int Ci, const uint16_t* w,
                          const float* bias, int Co, float* pre, uint16_t* act,
                          dm_stream_t stream);
+int dm_conv3d_s2_device_error(int* out_flags, dm_stream_t stream);
 int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,
                           const uint16_t* w, int Co, const float* pre, const float* dact,
                           float* dx, float* dw, float* db, void* workspace, size_t ws_bytes,

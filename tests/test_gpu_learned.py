@@ -17,9 +17,13 @@ def _bf(a):
 
 
 @pytest.mark.parametrize("shape", [(2, 16, 16, 16, 1, 16), (2, 12, 10, 14, 16, 32),
-                                   (1, 8, 8, 8, 32, 64), (2, 6, 6, 6, 64, 128)])
+                                   (1, 8, 8, 8, 32, 64), (2, 6, 6, 6, 64, 128),
+                                   (3, 17, 15, 19, 8, 32), (1, 9, 7, 5, 128, 16)])
 def test_conv_kernels_match_oracle(shape):
-    from deltamic_b200.learned import _kp, conv3d_s2
+    """Forward, weight, bias and data gradients of the tcgen05 implicit GEMMs
+    against the float64 oracle on the same BF16 inputs (odd extents: ragged row
+    tiles and parity classes; Ci = 8 and 128: the vector and element gathers)."""
+    from deltamic_b200.learned import _kp, conv3d_s2, conv_status_check
     B, D, H, W, Ci, Co = shape
     rng = np.random.default_rng(Ci)
     xb = _bf(rng.normal(size=(B, D, H, W, Ci)))
@@ -40,6 +44,7 @@ def test_conv_kernels_match_oracle(shape):
     assert rel_l2(w.grad[:27 * Ci].cpu().numpy(), dw) < 1e-2
     assert rel_l2(bt.grad.cpu().numpy(), db) < 1e-2
     assert rel_l2(x.grad.float().cpu().numpy(), dx) < 1e-2
+    conv_status_check(torch.device(DEV))
 
 
 def test_network_gradients_match_float32_reference():
