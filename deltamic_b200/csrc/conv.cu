@@ -4,7 +4,9 @@
 // reference).  All three products are implicit GEMMs over one generic tiled
 // kernel with gather loaders:
 //   forward  C[m, n]  = sum_k  A[m, k] W[k, n]       (A = im2col of x, on the fly)
-//   wgrad    dW[k, n] = sum_m  A[m, k] dP[m, n]      (split over m, fixed-order sum)
+//   wgrad    dW[k, n] = sum_m  A[m, k] dP[m, n]      (split over m, fixed-order sum;
+//                                                   a row of ones appended to A^T
+//                                                   gives db in the same product)
 //   dgrad    dX[q, c] = sum_t  dP[q(t)] W[t, c]      (one GEMM per stride parity
 //                                                   class of the input voxel)
 // with m = (b, od, oh, ow), k = ((kd*3 + kh)*3 + kw)*Ci + ci (rows past 27*Ci are
@@ -40,14 +42,15 @@ __device__ __forceinline__ float gelu_grad(float x) {
          x * expf(-0.5f * x * x) * 0.39894228040143268f;
 }
 
-// Output voxel m -> (b, od, oh, ow).
+// Output voxel m -> (b, od, oh, ow); 32-bit arithmetic (conv_shape keeps every
+// tensor below 2^31 elements).
 __device__ __forceinline__ void out_voxel(const ConvShape& s, int64_t m, int& b, int& od, int& oh,
                                           int& ow) {
-  int64_t t = m;
-  ow = (int)(t % s.Wo); t /= s.Wo;
-  oh = (int)(t % s.Ho); t /= s.Ho;
-  od = (int)(t % s.Do);
-  b = (int)(t / s.Do);
+  uint32_t t = (uint32_t)m;
+  ow = (int)(t % (uint32_t)s.Wo); t /= (uint32_t)s.Wo;
+  oh = (int)(t % (uint32_t)s.Ho); t /= (uint32_t)s.Ho;
+  od = (int)(t % (uint32_t)s.Do);
+  b = (int)(t / (uint32_t)s.Do);
 }
 
 // Offset of x[b, d, h, w, 0] for the tap (kd, kh, kw) of output voxel m, or -1 in
@@ -102,6 +105,33 @@ __device__ __forceinline__ uint4 gather8_b(const LB& lb, int col, int64_t red0, 
   return make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
 }
 
+// Transposed stage fill: unit (g, mc) supplies rows 8g..8g+7 of reduction column
+// mc as one uint4 (element e = row 8g + e), for operands whose contiguous global
+// direction runs along the rows.  Each thread stores its eight rows in an order
+// rotated by its lane group (lane >> 3 == mc >> 3), so the four lane groups of a
+// warp write four different rows of their core matrices: distinct banks.
+template <class F>
+__device__ __forceinline__ void fill_transposed(bf16* S, int ngroups, F unit) {
+  const int c = (threadIdx.x >> 3) & 3;
+  for (int u = threadIdx.x; u < ngroups * 32; u += kConvThreads) {
+    const int g = u >> 5, mc = u & 31;
+    uint4 v;
+    if (!unit(g, mc, v)) continue;
+    const uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
+    // rw[q] = w[(q + c) & 3]: element j of rw is element (j + 2c) & 7 of v
+    const uint32_t rw[4] = {c == 0 ? w0 : c == 1 ? w1 : c == 2 ? w2 : w3,
+                            c == 0 ? w1 : c == 1 ? w2 : c == 2 ? w3 : w0,
+                            c == 0 ? w2 : c == 1 ? w3 : c == 2 ? w0 : w1,
+                            c == 0 ? w3 : c == 1 ? w0 : c == 2 ? w1 : w2};
+    bf16* col = S + tc::kmaj32_off(g * 8, mc);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t word = rw[j >> 1];
+      col[((j + 2 * c) & 7) * 8] = __ushort_as_bfloat16((unsigned short)((j & 1) ? word >> 16 : word));
+    }
+  }
+}
+
 // Shared memory of one tile: two stages of A [128 x 32] and B [BN x 32] in the
 // K-major no-swizzle layout, two mbarriers and the TMEM address slot.  The size is
 // padded so that the CTAs one SM can hold never ask for more than its 512 TMEM
@@ -120,24 +150,59 @@ struct UmmaTile {
   static_assert(kStageBytes % 16 == 0, "stage alignment");
 };
 
+// Stage of A: the loader's own fill where it has one, else 8-element chunks along
+// the reduction.  Chunk e: row (e & 7) + 8 (e >> 5), reduction chunk (e >> 3) & 3 --
+// eight lanes store one 128-byte core-matrix column (no bank conflicts), and tiles
+// with at most 32 live rows still spread over every thread.  Rows past ``rows``
+// are left as they are: they only feed accumulator rows that are never read.
+template <class LA>
+__device__ __forceinline__ void fill_a(const LA& la, bf16* As, int64_t row0, int64_t rows,
+                                       int64_t k0, int64_t r_end) {
+  if (la.fill(As, row0, rows, k0, r_end)) return;
+#pragma unroll
+  for (int i = 0; i < kBM * (kBK / 8) / kConvThreads; ++i) {
+    const int e = threadIdx.x + i * kConvThreads;
+    const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
+    if (row0 + r < rows)
+      *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) =
+          gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end);
+  }
+}
+
+// Stage of B [BN x 32]: the loader's own fill, else chunks along the reduction.
+template <int BN, class LB>
+__device__ __forceinline__ void fill_b(const LB& lb, bf16* Bs, int64_t k0, int64_t r_end) {
+  if (lb.fill(Bs, BN, k0, r_end)) return;
+  for (int e = threadIdx.x; e < BN * (kBK / 8); e += kConvThreads) {
+    const int n = e % BN, kc = e / BN;
+    *(uint4*)(Bs + tc::kmaj32_off(n, kc * 8)) = gather8_b(lb, n, k0 + kc * 8, r_end);
+  }
+}
+
 // Generic tile: C[rows x BN] over a reduction [r_begin, r_end) split by blockIdx.y,
-// C = sum_k A[row, k] B[k, col] with A = la(row, k), B = lb(k, col), then ep(row,
-// col, split, C).  Every thread gathers its share of a stage into shared memory;
+// C = sum_k A[row, k] B[k, col] with A = la(row, k), B = lb(k, col), then
+// ep.put16(row, col, split, C[row, col..col+15]).  Every thread gathers its share of a stage into shared memory;
 // one thread issues the stage's two tcgen05 MMAs into the TMEM accumulator and
 // commits them to the stage's mbarrier, so the next stage's gather overlaps them.
 // Each warp reads its 32 accumulator rows back from TMEM for the epilogue.
 template <int BN, class LA, class LB, class EP>
-__global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la, LB lb, EP ep, int64_t rows,
-                                                            int64_t red_total, int64_t red_split,
+__global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la0, LB lb0, EP ep0, int64_t rows0,
+                                                            int64_t red_total0, int64_t red_split,
                                                             int* err) {
   using T = UmmaTile<BN>;
+  // blockIdx.z selects a column tile or a sub-problem (the loaders specialise)
+  const LA la = la0.at(blockIdx.z);
+  const LB lb = lb0.at(blockIdx.z, BN);
+  const EP ep = ep0.at(blockIdx.z, BN);
+  const int64_t rows = la.rows_at(rows0), red_total = la.red_at(red_total0);
+  const int64_t row0 = (int64_t)blockIdx.x * kBM;
+  if (row0 >= rows) return;  // whole block, before any TMEM or barrier is set up
   extern __shared__ __align__(128) uint8_t smem[];
   bf16* const As0 = (bf16*)smem;
   bf16* const Bs0 = (bf16*)(smem + T::kStageA * 2);
   uint64_t* const bar = (uint64_t*)(smem + 2 * T::kStageBytes);
   uint32_t* const slot = (uint32_t*)(bar + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row0 = (int64_t)blockIdx.x * kBM;
   const int64_t r_begin = (int64_t)blockIdx.y * red_split;
   const int64_t r_end = min(red_total, r_begin + red_split);
   const int nk = r_end > r_begin ? (int)((r_end - r_begin + kBK - 1) / kBK) : 0;
@@ -163,23 +228,8 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la, LB lb, EP ep,
     // the MMAs of stage t - 2 read this buffer: wait for their commit
     if (t >= 2) ok = mbar_wait_bounded(&bar[s], (uint32_t)(((t - 2) >> 1) & 1), err);
     const int64_t k0 = r_begin + (int64_t)t * kBK;
-    // chunk e: row (e & 7) + 8 (e >> 5), reduction chunk (e >> 3) & 3 -- eight lanes
-    // store one 128-byte core-matrix column (no bank conflicts), and tiles with at
-    // most 32 live rows still spread over every thread
-#pragma unroll
-    for (int i = 0; i < kBM * (kBK / 8) / kConvThreads; ++i) {
-      const int e = threadIdx.x + i * kConvThreads;
-      const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
-      if (row0 + r < rows)
-        *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) =
-            gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end);
-      else if (t < 2)  // dead rows: zero once per stage buffer
-        *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    for (int e = threadIdx.x; e < BN * (kBK / 8); e += kConvThreads) {
-      const int n = e % BN, kc = e / BN;
-      *(uint4*)(Bs + tc::kmaj32_off(n, kc * 8)) = gather8_b(lb, n, k0 + kc * 8, r_end);
-    }
+    fill_a(la, As, row0, rows, k0, r_end);
+    fill_b<BN>(lb, Bs, k0, r_end);
     fence_proxy_async();  // generic-proxy stores -> the MMA's async-proxy reads
     if (__syncthreads_or(!ok)) {
       ok = false;
@@ -206,10 +256,11 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la, LB lb, EP ep,
   for (int c = 0; c < BN; c += 16) {
     float v[16];
     tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-    if (row < rows) {
+    if (issued == 0) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) ep(row, c + j, (int)blockIdx.y, issued > 0 ? v[j] : 0.f);
+      for (int j = 0; j < 16; ++j) v[j] = 0.f;
     }
+    if (row < rows) ep.put16(row, c, (int)blockIdx.y, v);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -222,11 +273,17 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la, LB lb, EP ep,
 // ---------------------------------------------------------------------------
 // forward
 
+// Loader / epilogue protocol: at(z[, BN]) specialises for blockIdx.z; A loaders
+// also give the rows and reduction length of that sub-problem (rows_at, red_at).
 struct FwdA {
   const bf16* x;
   ConvShape s;
   bool vec;  // Ci % 8 == 0 and x 16-byte aligned: eight channels of one tap per load
+  __device__ FwdA at(int) const { return *this; }
+  __device__ int64_t rows_at(int64_t r) const { return r; }
+  __device__ int64_t red_at(int64_t r) const { return r; }
   __device__ bf16 operator()(int64_t m, int64_t k) const { return im2col(x, s, m, (int)k); }
+  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t) const { return false; }
   __device__ bool load8(int64_t m, int64_t k, uint4& v) const {
     v = make_uint4(0u, 0u, 0u, 0u);
     if (k >= s.K) return true;
@@ -253,21 +310,51 @@ struct FwdA {
     return true;
   }
 };
-struct WeightB {  // W[k, n], row-major [Kp, Co]
+struct WeightB {  // W[k, col0 + n], row-major [Kp, Co]; blockIdx.z = column tile
   const bf16* w;
   int Co;
-  __device__ bf16 operator()(int64_t k, int n) const { return w[k * Co + n]; }
+  int col0;
+  __device__ WeightB at(int z, int bn) const { return WeightB{w, Co, z * bn}; }
+  __device__ bf16 operator()(int64_t k, int n) const { return w[k * Co + col0 + n]; }
   __device__ bool load8(int64_t, int, uint4&) const { return false; }
+  __device__ bool fill(bf16*, int, int64_t, int64_t) const { return false; }
 };
 struct FwdEp {
   const float* bias;
   float* pre;
   bf16* act;
   int Co;
-  __device__ void operator()(int64_t m, int n, int, float v) const {
-    const float p = v + (bias ? bias[n] : 0.f);
-    pre[m * Co + n] = p;
-    act[m * Co + n] = __float2bfloat16(gelu(p));
+  int col0;
+  bool vec;  // pre and act 16-byte aligned
+  __device__ FwdEp at(int z, int bn) const {
+    FwdEp e = *this;
+    e.col0 = z * bn;
+    return e;
+  }
+  __device__ void put16(int64_t m, int c, int, const float (&v)[16]) const {
+    const int n0 = col0 + c;
+    float p[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) p[j] = v[j] + (bias ? bias[n0 + j] : 0.f);
+    float* pr = pre + m * Co + n0;
+    bf16* ar = act + m * Co + n0;
+    if (vec) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        *(float4*)(pr + 4 * q) = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+      uint32_t a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        a[q] = pack2(__float2bfloat16(gelu(p[2 * q])), __float2bfloat16(gelu(p[2 * q + 1])));
+      *(uint4*)ar = make_uint4(a[0], a[1], a[2], a[3]);
+      *(uint4*)(ar + 8) = make_uint4(a[4], a[5], a[6], a[7]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        pr[j] = p[j];
+        ar[j] = __float2bfloat16(gelu(p[j]));
+      }
+    }
   }
 };
 
@@ -281,12 +368,22 @@ __global__ void k_gelu_back(const float* __restrict__ pre, const float* __restri
     dpre[i] = __float2bfloat16(dact[i] * gelu_grad(pre[i]));
 }
 
-struct WgradA {  // A^T[k, m]
+struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
   const bf16* x;
   ConvShape s;
-  __device__ bf16 operator()(int64_t k, int64_t m) const { return im2col(x, s, m, (int)k); }
+  bool vec;  // Ci % 8 == 0 and x 16-byte aligned: transposed 16-byte gathers
+  __device__ WgradA at(int) const { return *this; }
+  __device__ int64_t rows_at(int64_t r) const { return r; }
+  __device__ int64_t red_at(int64_t r) const { return r; }
+  __device__ bf16 operator()(int64_t k, int64_t m) const {
+    return k == s.Kp ? __float2bfloat16(1.f) : im2col(x, s, m, (int)k);
+  }
   // eight consecutive output voxels m.. at one (tap, ci): decomposed once, then stepped
   __device__ bool load8(int64_t k, int64_t m, uint4& v) const {
+    if (k == s.Kp) {
+      v = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);  // BF16 ones
+      return true;
+    }
     v = make_uint4(0u, 0u, 0u, 0u);
     if (k >= s.K) return true;
     const int ci = (int)(k % s.Ci), tap = (int)(k / s.Ci);
@@ -315,56 +412,100 @@ struct WgradA {  // A^T[k, m]
     v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
     return true;
   }
+  // Ci % 8 == 0: eight channels of one tap (one 16-byte load) per row group and voxel
+  __device__ bool fill(bf16* As, int64_t row0, int64_t rows, int64_t m0, int64_t r_end) const {
+    if (!vec) return false;
+    fill_transposed(As, kBM / 8, [&](int g, int mc, uint4& v) {
+      const int64_t k = row0 + g * 8, m = m0 + mc;
+      if (k >= rows) return false;
+      v = make_uint4(0u, 0u, 0u, 0u);
+      if (m >= r_end) return true;
+      if (k == s.Kp) {
+        v.x = 0x3F80u;  // row Kp: one; rows Kp+1.. are past ``rows``
+      } else if (k < s.K) {
+        const int64_t o = tap_offset(s, m, (int)(k / s.Ci));
+        if (o >= 0) v = *(const uint4*)(x + o + k % s.Ci);
+      }
+      return true;
+    });
+    return true;
+  }
 };
 struct DpreB {  // dP[m, n]
   const bf16* dp;
   int Co;
+  bool vec;  // dp 16-byte aligned (Co is a multiple of 8): eight channels per load
+  __device__ DpreB at(int, int) const { return *this; }
   __device__ bf16 operator()(int64_t m, int n) const { return dp[m * Co + n]; }
   __device__ bool load8(int64_t, int, uint4&) const { return false; }
+  __device__ bool fill(bf16* Bs, int bn, int64_t m0, int64_t r_end) const {
+    if (!vec) return false;
+    fill_transposed(Bs, bn / 8, [&](int g, int mc, uint4& v) {
+      const int64_t m = m0 + mc;
+      v = make_uint4(0u, 0u, 0u, 0u);
+      if (m < r_end) v = *(const uint4*)(dp + m * Co + g * 8);
+      return true;
+    });
+    return true;
+  }
 };
-struct WgradEp {  // partial[split][k][n]
+struct WgradEp {  // partial[split][k][n] (16-byte aligned workspace rows)
   float* part;
-  int64_t stride;  // Kp * Co
+  int64_t stride;  // (Kp + 1) * Co
   int Co;
-  __device__ void operator()(int64_t k, int n, int split, float v) const {
-    part[split * stride + k * Co + n] = v;
+  __device__ WgradEp at(int, int) const { return *this; }
+  __device__ void put16(int64_t k, int c, int split, const float (&v)[16]) const {
+    float* r = part + split * stride + k * Co + c;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      *(float4*)(r + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
   }
 };
 
-__global__ void k_sum_splits(const float* __restrict__ part, int splits, int64_t n,
-                             float* __restrict__ out) {
+// Fixed-order sum of the split partials [split][Kp + 1][Co]: rows < Kp into dw,
+// row Kp (the ones row) into db.
+__global__ void k_sum_splits(const float* __restrict__ part, int splits, int64_t nw, int Co,
+                             float* __restrict__ dw, float* __restrict__ db) {
+  const int64_t n = nw + Co;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     float s = 0.f;
     for (int k = 0; k < splits; ++k) s += part[k * n + i];
-    out[i] = s;
+    if (i < nw)
+      dw[i] = s;
+    else
+      db[i - nw] = s;
   }
-}
-
-// db[n] = sum_m dP[m, n]: one block per n, fixed-order tree.
-__global__ void k_bias_grad(const bf16* __restrict__ dp, int64_t M, int Co, float* __restrict__ db) {
-  __shared__ float sh[256];
-  const int n = blockIdx.x;
-  float s = 0.f;
-  for (int64_t m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(dp[m * Co + n]);
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) db[n] = sh[0];
 }
 
 // dgrad for the input voxels of one stride-parity class (pd, ph, pw): per axis an
 // even coordinate d takes tap 1 (od = d/2), an odd one taps 0 and 2
-// (od = (d+1)/2, (d-1)/2).
+// (od = (d+1)/2, (d-1)/2).  The eight classes run in one launch, blockIdx.z = class.
 struct Cls {
-  int p[3];     // parity per axis
-  int n[3];     // class extent per axis
-  int nt[3];    // taps per axis (1 or 2)
-  int T;        // taps in the class
+  int p[3];      // parity per axis
+  int n[3];      // class extent per axis
+  int nt[3];     // taps per axis (1 or 2)
+  int T;         // taps in the class
+  int64_t rows;  // B * n0 * n1 * n2 (0: empty class)
+  int64_t red;   // T * Co rounded up to kBK
 };
+struct ClsSet {
+  Cls c[8];
+};
+
+// Class z of a set held in kernel parameters (constant indices: no local copy).
+__device__ __forceinline__ Cls pick_cls(const ClsSet& set, int z) {
+  switch (z) {
+    case 0: return set.c[0];
+    case 1: return set.c[1];
+    case 2: return set.c[2];
+    case 3: return set.c[3];
+    case 4: return set.c[4];
+    case 5: return set.c[5];
+    case 6: return set.c[6];
+    default: return set.c[7];
+  }
+}
 
 __device__ __forceinline__ void cls_tap(const Cls& c, int t, int kk[3]) {
   const int tw = t % c.nt[2], th = (t / c.nt[2]) % c.nt[1], td = t / (c.nt[2] * c.nt[1]);
@@ -373,21 +514,37 @@ __device__ __forceinline__ void cls_tap(const Cls& c, int t, int kk[3]) {
   for (int a = 0; a < 3; ++a) kk[a] = c.p[a] == 0 ? 1 : (tt[a] == 0 ? 0 : 2);
 }
 
+// Input voxel of class row q: (b, d, h, w).
+__device__ __forceinline__ void cls_voxel(const Cls& c, int64_t q, int& b, int& d, int& h,
+                                          int& w) {
+  uint32_t u = (uint32_t)q;
+  const int iw = (int)(u % (uint32_t)c.n[2]); u /= (uint32_t)c.n[2];
+  const int ih = (int)(u % (uint32_t)c.n[1]); u /= (uint32_t)c.n[1];
+  const int id = (int)(u % (uint32_t)c.n[0]);
+  b = (int)(u / (uint32_t)c.n[0]);
+  d = 2 * id + c.p[0];
+  h = 2 * ih + c.p[1];
+  w = 2 * iw + c.p[2];
+}
+
 struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the tap
   const bf16* dp;
   ConvShape s;
+  ClsSet set;  // the eight classes (kernel parameter)
   Cls c;
   bool vec;  // dp 16-byte aligned (Co is a multiple of 8): eight channels per load
+  __device__ DgradA at(int z) const {
+    DgradA a = *this;
+    a.c = pick_cls(set, z);
+    return a;
+  }
+  __device__ int64_t rows_at(int64_t) const { return c.rows; }
+  __device__ int64_t red_at(int64_t) const { return c.red; }
   // Offset of dP[voxel reached from input voxel q through tap t, 0], or -1 outside.
   __device__ int64_t offset(int64_t q, int t) const {
-    int kk[3];
+    int kk[3], b, d, h, w;
     cls_tap(c, t, kk);
-    int64_t u = q;
-    const int iw = (int)(u % c.n[2]); u /= c.n[2];
-    const int ih = (int)(u % c.n[1]); u /= c.n[1];
-    const int id = (int)(u % c.n[0]);
-    const int b = (int)(u / c.n[0]);
-    const int d = 2 * id + c.p[0], h = 2 * ih + c.p[1], w = 2 * iw + c.p[2];
+    cls_voxel(c, q, b, d, h, w);
     const int od = (d + 1 - kk[0]) >> 1, oh = (h + 1 - kk[1]) >> 1, ow = (w + 1 - kk[2]) >> 1;
     if (od < 0 || od >= s.Do || oh < 0 || oh >= s.Ho || ow < 0 || ow >= s.Wo) return -1;
     return ((((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow) * s.Co;
@@ -407,12 +564,19 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
     if (o >= 0) v = *(const uint4*)(dp + o + r % s.Co);
     return true;
   }
+  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t) const { return false; }
 };
 struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
   const bf16* w;
   ConvShape s;
+  ClsSet set;
   Cls c;
   bool vec;  // w 16-byte aligned (Co is a multiple of 8): eight co per load
+  __device__ DgradB at(int z, int) const {
+    DgradB b = *this;
+    b.c = pick_cls(set, z);
+    return b;
+  }
   __device__ int64_t offset(int t, int ci) const {
     int kk[3];
     cls_tap(c, t, kk);
@@ -432,20 +596,34 @@ struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
     v = *(const uint4*)(w + offset(t, ci) + r % s.Co);
     return true;
   }
+  __device__ bool fill(bf16*, int, int64_t, int64_t) const { return false; }
 };
 struct DgradEp {
   float* dx;
   ConvShape s;
+  ClsSet set;
   Cls c;
-  __device__ void operator()(int64_t q, int ci, int, float v) const {
-    if (ci >= s.Ci) return;
-    int64_t u = q;
-    const int iw = (int)(u % c.n[2]); u /= c.n[2];
-    const int ih = (int)(u % c.n[1]); u /= c.n[1];
-    const int id = (int)(u % c.n[0]);
-    const int b = (int)(u / c.n[0]);
-    const int d = 2 * id + c.p[0], h = 2 * ih + c.p[1], w = 2 * iw + c.p[2];
-    dx[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + ci] = v;
+  bool vec;  // dx 16-byte aligned and Ci a multiple of 16
+  __device__ DgradEp at(int z, int) const {
+    DgradEp e = *this;
+    e.c = pick_cls(set, z);
+    return e;
+  }
+  __device__ void put16(int64_t q, int c0, int, const float (&v)[16]) const {
+    if (c0 >= s.Ci) return;
+    int b, d, h, w;
+    cls_voxel(c, q, b, d, h, w);
+    float* r = dx + ((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + c0;
+    if (vec) {
+#pragma unroll
+      for (int q4 = 0; q4 < 4; ++q4)
+        *(float4*)(r + 4 * q4) =
+            make_float4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (c0 + j < s.Ci) r[j] = v[j];
+    }
   }
 };
 
@@ -464,22 +642,23 @@ static int* conv_status_ptr() {
   return p;
 }
 
+// rows: the largest sub-problem's rows (grid x); nz sub-problems or column tiles.
 template <int BN, class LA, class LB, class EP>
 static void umma_launch(LA la, LB lb, EP ep, int64_t rows, int64_t red, int64_t red_split,
-                        int splits, cudaStream_t st) {
-  const dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)splits);
+                        int splits, int nz, cudaStream_t st) {
+  const dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)splits, (unsigned)nz);
   k_conv_umma<BN><<<grid, kConvThreads, UmmaTile<BN>::kSmem, st>>>(la, lb, ep, rows, red,
                                                                     red_split, conv_status_ptr());
 }
 
 template <class LA, class LB, class EP>
 static void gemm_launch(int bn, LA la, LB lb, EP ep, int64_t rows, int64_t red, int64_t red_split,
-                        int splits, cudaStream_t st) {
+                        int splits, int nz, cudaStream_t st) {
   switch (bn) {
-    case 16: umma_launch<16>(la, lb, ep, rows, red, red_split, splits, st); break;
-    case 32: umma_launch<32>(la, lb, ep, rows, red, red_split, splits, st); break;
-    case 64: umma_launch<64>(la, lb, ep, rows, red, red_split, splits, st); break;
-    default: umma_launch<128>(la, lb, ep, rows, red, red_split, splits, st); break;
+    case 16: umma_launch<16>(la, lb, ep, rows, red, red_split, splits, nz, st); break;
+    case 32: umma_launch<32>(la, lb, ep, rows, red, red_split, splits, nz, st); break;
+    case 64: umma_launch<64>(la, lb, ep, rows, red, red_split, splits, nz, st); break;
+    default: umma_launch<128>(la, lb, ep, rows, red, red_split, splits, nz, st); break;
   }
   count_launches(1);
 }
@@ -492,6 +671,8 @@ bool conv_shape(int B, int D, int H, int W, int Ci, int Co, ConvShape& s) {
   if (B <= 0 || D <= 0 || H <= 0 || W <= 0 || Ci <= 0 || Co <= 0 || Co > 128 || Ci > 128)
     return false;
   if (Co != 16 && Co != 32 && Co != 64 && Co != 128) return false;
+  // every tensor below 2^31 elements (32-bit voxel arithmetic in the kernels)
+  if ((int64_t)B * D * H * W * std::max(Ci, Co) >= ((int64_t)1 << 31)) return false;
   s.B = B; s.D = D; s.H = H; s.W = W; s.Ci = Ci; s.Co = Co;
   s.Do = (D + 1) / 2; s.Ho = (H + 1) / 2; s.Wo = (W + 1) / 2;
   s.K = 27 * Ci;
@@ -501,22 +682,34 @@ bool conv_shape(int B, int D, int H, int W, int Ci, int Co, ConvShape& s) {
 }
 
 static int wgrad_splits(const ConvShape& s) {
-  const int64_t row_tiles = (s.Kp + kBM - 1) / kBM;
+  const int64_t row_tiles = (s.Kp + 1 + kBM - 1) / kBM;
   int64_t sp = std::max<int64_t>(1, (int64_t)148 * 4 / row_tiles);
   sp = std::min<int64_t>(sp, std::max<int64_t>(1, s.M / (4 * kBK)));
   return (int)sp;
 }
 
+// Workspace: dP (BF16) | split partials (FP32).
 size_t conv_ws_bytes(const ConvShape& s) {
   const size_t dp = ((size_t)s.M * s.Co * sizeof(bf16) + 255) / 256 * 256;
-  const size_t part = (size_t)wgrad_splits(s) * s.Kp * s.Co * sizeof(float);
+  const size_t part = (size_t)wgrad_splits(s) * (s.Kp + 1) * s.Co * sizeof(float);
   return dp + part + 256;
+}
+
+// Column tile of the forward: all Co columns, or fewer (>= 16) when the row tiles
+// alone would leave SMs idle (two blocks per SM wanted).
+static int fwd_cols(const ConvShape& s) {
+  const int64_t tiles = (s.M + kBM - 1) / kBM;
+  int bn = s.Co;
+  while (bn > 16 && tiles * (s.Co / bn) < 2 * 148) bn /= 2;
+  return bn;
 }
 
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st) {
-  gemm_launch(s.Co, FwdA{x, s, s.Ci % 8 == 0 && aligned16(x)}, WeightB{w, s.Co},
-              FwdEp{bias, pre, act, s.Co}, s.M, s.Kp, s.Kp, 1, st);
+  const int bn = fwd_cols(s);
+  gemm_launch(bn, FwdA{x, s, s.Ci % 8 == 0 && aligned16(x)}, WeightB{w, s.Co, 0},
+              FwdEp{bias, pre, act, s.Co, 0, aligned16(pre) && aligned16(act)}, s.M, s.Kp, s.Kp,
+              1, s.Co / bn, st);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -530,22 +723,25 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   k_gelu_back<<<(unsigned)std::min<int64_t>((nout + 255) / 256, 148 * 16), 256, 0, st>>>(
       pre, dact, dp, nout);
   count_launches(1);
-  // weight gradient: rows = Kp, reduction over m split across blockIdx.y
+  // weight and bias gradients: rows = Kp + 1 (the last row of A^T is ones), the
+  // reduction over m split across blockIdx.y
   const int splits = wgrad_splits(s);
   const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
   const int used = (int)((s.M + per - 1) / per);
-  gemm_launch(s.Co, WgradA{x, s}, DpreB{dp, s.Co}, WgradEp{part, (int64_t)s.Kp * s.Co, s.Co},
-              (int64_t)s.Kp, s.M, per, used, st);
+  gemm_launch(s.Co, WgradA{x, s, s.Ci % 8 == 0 && aligned16(x)}, DpreB{dp, s.Co, aligned16(dp)},
+              WgradEp{part, (int64_t)(s.Kp + 1) * s.Co, s.Co}, (int64_t)s.Kp + 1, s.M, per, used,
+              1, st);
   const int64_t nw = (int64_t)s.Kp * s.Co;
-  k_sum_splits<<<(unsigned)std::min<int64_t>((nw + 255) / 256, 148 * 4), 256, 0, st>>>(part, used,
-                                                                                       nw, dw);
-  k_bias_grad<<<s.Co, 256, 0, st>>>(dp, s.M, s.Co, db);
-  count_launches(2);
-  // data gradient: one GEMM per parity class of the input voxels
+  k_sum_splits<<<(unsigned)std::min<int64_t>((nw + s.Co + 255) / 256, 148 * 4), 256, 0, st>>>(
+      part, used, nw, s.Co, dw, db);
+  count_launches(1);
+  // data gradient: the eight parity classes of the input voxels in one launch
   if (dx) {
+    ClsSet set;
+    int64_t max_rows = 0, max_red = 0;
+    const int dims[3] = {s.D, s.H, s.W};
     for (int cls = 0; cls < 8; ++cls) {
-      Cls c;
-      const int dims[3] = {s.D, s.H, s.W};
+      Cls& c = set.c[cls];
       c.T = 1;
       bool empty = false;
       for (int a = 0; a < 3; ++a) {
@@ -555,12 +751,15 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
         c.T *= c.nt[a];
         if (c.n[a] <= 0) empty = true;
       }
-      if (empty) continue;
-      const int64_t rows = (int64_t)s.B * c.n[0] * c.n[1] * c.n[2];
-      const int64_t red = ((int64_t)c.T * s.Co + kBK - 1) / kBK * kBK;
-      gemm_launch(pad_cols(s.Ci), DgradA{dp, s, c, aligned16(dp)}, DgradB{w, s, c, aligned16(w)},
-                  DgradEp{dx, s, c}, rows, red, red, 1, st);
+      c.rows = empty ? 0 : (int64_t)s.B * c.n[0] * c.n[1] * c.n[2];
+      c.red = ((int64_t)c.T * s.Co + kBK - 1) / kBK * kBK;
+      max_rows = std::max(max_rows, c.rows);
+      max_red = std::max(max_red, c.red);
     }
+    const bool dvec = aligned16(dx) && s.Ci % 16 == 0;
+    gemm_launch(pad_cols(s.Ci), DgradA{dp, s, set, Cls{}, aligned16(dp)},
+                DgradB{w, s, set, Cls{}, aligned16(w)}, DgradEp{dx, s, set, Cls{}, dvec},
+                max_rows, max_red, max_red, 1, 8, st);
   }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }

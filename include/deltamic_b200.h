@@ -399,7 +399,7 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
  * initialiser's encoder (no counterpart in the reference).  Channels-last BF16
  * tensors (uint16 storage): x[B,D,H,W,Ci], w[Kp,Co] with row k = ((kd*3+kh)*3+kw)*Ci
  * + ci and Kp = 27*Ci rounded up to 32 (padding rows zero); Co in {16,32,64,128},
- * Ci <= 128; output (D+1)/2 x (H+1)/2 x (W+1)/2.  Implicit GEMMs on the fifth-
+ * Ci <= 128, B*D*H*W*max(Ci, Co) < 2^31; output (D+1)/2 x (H+1)/2 x (W+1)/2.  Implicit GEMMs on the fifth-
  * generation tensor cores (tcgen05 MMAs, FP32 accumulators in tensor memory).
  * Forward writes pre[.., Co] (FP32 pre-activation) and act = GELU(pre) (BF16).
  * Backward takes dact = dL/dact (FP32) and writes dw[Kp,Co], db[Co] and, if
