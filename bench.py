@@ -80,7 +80,7 @@ def parse():
     p.add_argument("--mask-grid", type=int, default=64,
                    help="masks64: grid points per axis of the masks (64: the workload's grid)")
     p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned",
-                                           "volume200", "psf200", "masks64"],
+                                           "volume200", "psf200", "masks64", "conv64"],
                    default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
                         "cells of mixed sizes per step; volume200: forward + adjoint of "
@@ -799,6 +799,157 @@ def run_learned(args, rank, world, local):
     print(json.dumps(out), flush=True)
 
 
+def _bf16_peak_tflops():
+    """Dense BF16 peak for the tensor roofline: the pool's measured cuBLAS figure
+    (MEASURED_PEAKS.json beside this file) if present, else the recipe's fallback."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        for key in ("bf16_tflops", "bf16_dense_tflops"):
+            if key in d and d[key]:
+                return float(d[key]), f"measured ({key}, MEASURED_PEAKS.json)"
+    except (OSError, ValueError):
+        pass
+    return 1590.0, "fallback (1.59 PFLOP/s dense BF16, earlier measurement on this pool)"
+
+
+def run_conv(args, rank, world, local):
+    """conv64: one training step of the learned initialiser's encoder convolutions
+    (no reference counterpart): the four 3x3x3 stride-2 convolutions 1 -> 16 -> 32 ->
+    64 -> 128 on a batch of 64 images of 64^3, forward (bias + GELU epilogue) then
+    weight, bias and data gradients (no data gradient for the image), BF16 operands
+    on the tcgen05 tensor cores with FP32 accumulators in tensor memory, called
+    through the C ABI.  value = algorithmic FLOPs (2 * M * 27 Ci * Co per product) /
+    device time."""
+    import torch
+    from deltamic_b200 import _native as N
+    from deltamic_b200.learned import CHANNELS, IMAGE, _kp, conv3d_s2
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.lib()
+    st = N.stream_ptr(dev)
+    B = 64
+    g = torch.Generator(device=dev).manual_seed(5 + rank)
+    n = IMAGE
+    x = torch.rand(B, n, n, n, 1, device=dev, generator=g).to(torch.bfloat16)
+    layers, flops = [], 0
+    for ci, co in zip(CHANNELS[:-1], CHANNELS[1:]):
+        no = (n + 1) // 2
+        w = torch.zeros(_kp(ci), co, device=dev)
+        w[:27 * ci] = torch.randn(27 * ci, co, device=dev, generator=g) * (2.0 / (27 * ci)) ** 0.5
+        L = dict(ci=ci, co=co, n=n, x=x, w=w.to(torch.bfloat16), w32=w,
+                 b=torch.randn(co, device=dev, generator=g) * 0.1,
+                 pre=torch.empty(B, no, no, no, co, device=dev),
+                 act=torch.empty(B, no, no, no, co, device=dev, dtype=torch.bfloat16),
+                 dact=torch.randn(B, no, no, no, co, device=dev, generator=g),
+                 dx=torch.empty(x.shape, device=dev) if ci > 1 else None,
+                 dw=torch.empty(_kp(ci), co, device=dev), db=torch.empty(co, device=dev))
+        L["wsb"] = lib.dm_conv3d_s2_workspace_size(B, n, n, n, ci, co)
+        L["ws"] = torch.empty(L["wsb"], dtype=torch.uint8, device=dev)
+        flops += 2 * B * no ** 3 * 27 * ci * co * (3 if ci > 1 else 2)
+        layers.append(L)
+        x, n = L["act"], no
+
+    def step():
+        for L in layers:
+            N.check(lib.dm_conv3d_s2_forward(N.ptr(L["x"]), B, L["n"], L["n"], L["n"], L["ci"],
+                                             N.ptr(L["w"]), N.ptr(L["b"]), L["co"],
+                                             N.ptr(L["pre"]), N.ptr(L["act"]), st),
+                    "dm_conv3d_s2_forward")
+        for L in reversed(layers):
+            N.check(lib.dm_conv3d_s2_backward(N.ptr(L["x"]), B, L["n"], L["n"], L["n"], L["ci"],
+                                              N.ptr(L["w"]), L["co"], N.ptr(L["pre"]),
+                                              N.ptr(L["dact"]), N.ptr(L["dx"]), N.ptr(L["dw"]),
+                                              N.ptr(L["db"]), N.ptr(L["ws"]), L["wsb"], st),
+                    "dm_conv3d_s2_backward")
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    c0 = lib.dm_launch_count()
+    step()
+    launches = int(lib.dm_launch_count() - c0)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ms = max_over_ranks(_event_ms(step, args.steps, 1), dev)
+    clk = clocks.stop()
+    from deltamic_b200.learned import conv_status_check
+    conv_status_check(dev)
+
+    # end to end through the public autograd op: the image batch from pinned host
+    # memory, the encoder's convolutions forward and backward, the weight and bias
+    # gradients back to the host
+    host_img = torch.rand(B, IMAGE, IMAGE, IMAGE, generator=torch.Generator().manual_seed(7))
+    host_img = host_img.pin_memory()
+    params = [(L["w32"].clone().requires_grad_(True), L["b"].clone().requires_grad_(True))
+              for L in layers]
+    host_g = [torch.empty(p.shape, pin_memory=True) for wb in params for p in wb]
+    img_d = torch.empty(host_img.shape, device=dev)
+
+    def e2e_step():
+        img_d.copy_(host_img, non_blocking=True)
+        h = img_d.to(torch.bfloat16).unsqueeze(-1)
+        for w, b in params:
+            h = conv3d_s2(h, w, b)
+        h.float().sum().backward()
+        for hg, p in zip(host_g, [p for wb in params for p in wb]):
+            hg.copy_(p.grad, non_blocking=True)
+            p.grad = None
+
+    e2e_ms = max_over_ranks(_event_ms(e2e_step, args.steps, max(args.warmup, 3)), dev)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        import oracle.conv as oc
+        # 32 images of the batch through the float64 oracle: forward, then weight,
+        # bias and data gradients of every layer (single thread)
+        from threadpoolctl import threadpool_limits
+        nb = 32
+        xs = layers[0]["x"][:nb].float().cpu().numpy().astype(np.float64)
+        ws = [(L["w"].float().cpu().numpy().astype(np.float64),
+               L["b"].cpu().numpy().astype(np.float64)) for L in layers]
+        cflops = 0
+        with threadpool_limits(1):
+            t0 = time.perf_counter()
+            for L, (w64, b64) in zip(layers, ws):
+                pre, act = oc.conv_forward(xs, w64, b64)
+                oc.conv_backward(xs, w64, pre, np.ones_like(pre))
+                no = pre.shape[1]
+                cflops += 2 * nb * no ** 3 * 27 * L["ci"] * L["co"] * (3 if L["ci"] > 1 else 2)
+                xs = act
+            dt = time.perf_counter() - t0
+        cpu = {"value": cflops / dt / 1e12, "unit": "TFLOP/s", "cores": 1, "kind": "port",
+               "sample": f"{nb} of the 64 images, all four layers fwd+bwd ({dt:.1f} s)"}
+    if rank != 0:
+        return
+    peak, peak_src = _bf16_peak_tflops()
+    value = flops * world / (ms * 1e-3) / 1e12
+    out = {"metric": "encoder convolution TFLOP/s (learned initialiser training step: "
+                     "forward + weight, bias and data gradients, batch 64, 64^3)",
+           "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (FP32 accumulate)",
+           "data": "synthetic (uniform images, random weights and output gradients)",
+           "config": {"workload": "conv64: 4 layers 1-16-32-64-128, batch 64, 64^3",
+                      "parallelism": "replicas only", "flops_per_step": flops,
+                      "l2_flush": "no: the step streams > 126 MB (layer-1 pre-activations "
+                                  "alone are 134 MB)"},
+           "gpu_launches": launches * args.steps, "clocks": clk,
+           "e2e": {"value": flops * world / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                   "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(host_img.numel() * 4),
+                   "d2h_bytes_per_step": int(sum(h.numel() * 4 for h in host_g))},
+           "roofline": {"bound": "tensor", "kernel": "k_conv_umma (all products of the step)",
+                        "achieved": value, "peak": peak, "unit": "TFLOP/s",
+                        "frac": value / peak, "peak_source": peak_src, "traffic": None,
+                        "note": "implicit-GEMM gathers (im2col of 3^3 stride-2 taps, 1-128 "
+                                "channels) bound these products, not the tensor pipe"}}
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -965,6 +1116,8 @@ def main():
             run_psf(args, rank, world, local)
         elif args.workload == "masks64":
             run_masks(args, rank, world, local)
+        elif args.workload == "conv64":
+            run_conv(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

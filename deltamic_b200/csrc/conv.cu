@@ -81,10 +81,10 @@ __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
 // element by element.
 template <class LA>
 __device__ __forceinline__ uint4 gather8_a(const LA& la, int64_t row, int64_t rows, int64_t red0,
-                                           int64_t r_end) {
+                                           int64_t r_end, const int4& info) {
   uint4 v = make_uint4(0u, 0u, 0u, 0u);
   if (row >= rows || red0 >= r_end) return v;
-  if (red0 + 8 <= r_end && la.load8(row, red0, v)) return v;
+  if (red0 + 8 <= r_end && la.load8(row, red0, info, v)) return v;
   const bf16 z = __float2bfloat16(0.f);
   bf16 e[8];
 #pragma unroll
@@ -110,30 +110,34 @@ __device__ __forceinline__ uint4 gather8_b(const LB& lb, int col, int64_t red0, 
 // direction runs along the rows.  Each thread stores its eight rows in an order
 // rotated by its lane group (lane >> 3 == mc >> 3), so the four lane groups of a
 // warp write four different rows of their core matrices: distinct banks.
+__device__ __forceinline__ void store_rotated8(bf16* S, int g, int mc, const uint4& v) {
+  const int c = mc >> 3;
+  const uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
+  // rw[q] = w[(q + c) & 3]: element j of rw is element (j + 2c) & 7 of v
+  const uint32_t rw[4] = {c == 0 ? w0 : c == 1 ? w1 : c == 2 ? w2 : w3,
+                          c == 0 ? w1 : c == 1 ? w2 : c == 2 ? w3 : w0,
+                          c == 0 ? w2 : c == 1 ? w3 : c == 2 ? w0 : w1,
+                          c == 0 ? w3 : c == 1 ? w0 : c == 2 ? w1 : w2};
+  bf16* col = S + tc::kmaj32_off(g * 8, mc);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t word = rw[j >> 1];
+    col[((j + 2 * c) & 7) * 8] = __ushort_as_bfloat16((unsigned short)((j & 1) ? word >> 16 : word));
+  }
+}
+
 template <class F>
 __device__ __forceinline__ void fill_transposed(bf16* S, int ngroups, F unit) {
-  const int c = (threadIdx.x >> 3) & 3;
   for (int u = threadIdx.x; u < ngroups * 32; u += kConvThreads) {
     const int g = u >> 5, mc = u & 31;
     uint4 v;
-    if (!unit(g, mc, v)) continue;
-    const uint32_t w0 = v.x, w1 = v.y, w2 = v.z, w3 = v.w;
-    // rw[q] = w[(q + c) & 3]: element j of rw is element (j + 2c) & 7 of v
-    const uint32_t rw[4] = {c == 0 ? w0 : c == 1 ? w1 : c == 2 ? w2 : w3,
-                            c == 0 ? w1 : c == 1 ? w2 : c == 2 ? w3 : w0,
-                            c == 0 ? w2 : c == 1 ? w3 : c == 2 ? w0 : w1,
-                            c == 0 ? w3 : c == 1 ? w0 : c == 2 ? w1 : w2};
-    bf16* col = S + tc::kmaj32_off(g * 8, mc);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint32_t word = rw[j >> 1];
-      col[((j + 2 * c) & 7) * 8] = __ushort_as_bfloat16((unsigned short)((j & 1) ? word >> 16 : word));
-    }
+    if (unit(g, mc, v)) store_rotated8(S, g, mc, v);
   }
 }
 
 // Shared memory of one tile: two stages of A [128 x 32] and B [BN x 32] in the
-// K-major no-swizzle layout, two mbarriers and the TMEM address slot.  The size is
+// K-major no-swizzle layout, two mbarriers, the TMEM address slot and one int4 of
+// per-row information (the A loader's, computed once per tile).  The size is
 // padded so that the CTAs one SM can hold never ask for more than its 512 TMEM
 // columns together (228 KB of shared memory per SM; 16 CTAs of 128 threads at most).
 template <int BN>
@@ -144,7 +148,7 @@ struct UmmaTile {
   static constexpr int kStageBytes = (kStageA + kStageB) * 2;
   static constexpr int kMaxCtas = 512 / kCols;
   static constexpr int kMinSmem = kMaxCtas >= 16 ? 0 : 233472 / (kMaxCtas + 1) + 128;
-  static constexpr int kUsed = 2 * kStageBytes + 64;
+  static constexpr int kUsed = 2 * kStageBytes + 64 + kBM * 16;  // + per-row info (int4)
   static constexpr int kSmem = ((kUsed > kMinSmem ? kUsed : kMinSmem) + 127) / 128 * 128;
   static_assert(kSmem <= 48 * 1024, "tile shared memory above the default 48 KB");
   static_assert(kStageBytes % 16 == 0, "stage alignment");
@@ -157,15 +161,15 @@ struct UmmaTile {
 // are left as they are: they only feed accumulator rows that are never read.
 template <class LA>
 __device__ __forceinline__ void fill_a(const LA& la, bf16* As, int64_t row0, int64_t rows,
-                                       int64_t k0, int64_t r_end) {
-  if (la.fill(As, row0, rows, k0, r_end)) return;
+                                       int64_t k0, int64_t r_end, const int4* rinfo) {
+  if (la.fill(As, row0, rows, k0, r_end, rinfo)) return;
 #pragma unroll
   for (int i = 0; i < kBM * (kBK / 8) / kConvThreads; ++i) {
     const int e = threadIdx.x + i * kConvThreads;
     const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
     if (row0 + r < rows)
       *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) =
-          gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end);
+          gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end, rinfo[r]);
   }
 }
 
@@ -202,11 +206,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la0, LB lb0, EP e
   bf16* const Bs0 = (bf16*)(smem + T::kStageA * 2);
   uint64_t* const bar = (uint64_t*)(smem + 2 * T::kStageBytes);
   uint32_t* const slot = (uint32_t*)(bar + 2);
+  int4* const rinfo = (int4*)(bar + 4);  // 16-byte aligned: bar is
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t r_begin = (int64_t)blockIdx.y * red_split;
   const int64_t r_end = min(red_total, r_begin + red_split);
   const int nk = r_end > r_begin ? (int)((r_end - r_begin + kBK - 1) / kBK) : 0;
 
+  rinfo[threadIdx.x] = la.row_info(row0 + threadIdx.x, rows);
   if (warp == 0) tc::tmem_alloc(slot, T::kCols);
   if (threadIdx.x == 32) {
     mbar_init(&bar[0], 1);
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la0, LB lb0, EP e
     // the MMAs of stage t - 2 read this buffer: wait for their commit
     if (t >= 2) ok = mbar_wait_bounded(&bar[s], (uint32_t)(((t - 2) >> 1) & 1), err);
     const int64_t k0 = r_begin + (int64_t)t * kBK;
-    fill_a(la, As, row0, rows, k0, r_end);
+    fill_a(la, As, row0, rows, k0, r_end, rinfo);
     fill_b<BN>(lb, Bs, k0, r_end);
     fence_proxy_async();  // generic-proxy stores -> the MMA's async-proxy reads
     if (__syncthreads_or(!ok)) {
@@ -283,27 +289,40 @@ struct FwdA {
   __device__ int64_t rows_at(int64_t r) const { return r; }
   __device__ int64_t red_at(int64_t r) const { return r; }
   __device__ bf16 operator()(int64_t m, int64_t k) const { return im2col(x, s, m, (int)k); }
-  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t) const { return false; }
-  __device__ bool load8(int64_t m, int64_t k, uint4& v) const {
-    v = make_uint4(0u, 0u, 0u, 0u);
-    if (k >= s.K) return true;
-    if (vec) {
-      const int64_t o = tap_offset(s, m, (int)(k / s.Ci));
-      if (o >= 0) v = *(const uint4*)(x + o + k % s.Ci);
-      return true;
-    }
-    // chunk across taps (Ci < 8): the output voxel decomposed once
+  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t, const int4*) const {
+    return false;
+  }
+  // Row info of output voxel m: the input voxel index of its tap (0, 0, 0) and that
+  // tap's coordinates (d0, h0, w0) (possibly -1: the zero padding).
+  __device__ int4 row_info(int64_t m, int64_t rows) const {
+    if (m >= rows) return make_int4(0, 0, 0, 0);
     int b, od, oh, ow;
     out_voxel(s, m, b, od, oh, ow);
+    const int d0 = 2 * od - 1, h0 = 2 * oh - 1, w0 = 2 * ow - 1;
+    return make_int4(((b * s.D + d0) * s.H + h0) * s.W + w0, d0, h0, w0);
+  }
+  __device__ bool load8(int64_t, int64_t k64, const int4& ri, uint4& v) const {
+    v = make_uint4(0u, 0u, 0u, 0u);
+    const int k = (int)k64;
+    if (k >= s.K) return true;
+    if (vec) {  // one tap, eight channels
+      const int tap = k / s.Ci, ci = k - tap * s.Ci;
+      const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+      const int d = ri.y + kd, h = ri.z + kh, w = ri.w + kw;
+      if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+        v = *(const uint4*)(x + ((int64_t)ri.x + (kd * s.H + kh) * s.W + kw) * s.Ci + ci);
+      return true;
+    }
+    // Ci < 8: the chunk runs across taps
     const bf16 z = __float2bfloat16(0.f);
     bf16 e[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const int kj = (int)k + j, tap = kj / s.Ci;
+      const int kj = k + j, tap = kj / s.Ci;
       const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
-      const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
+      const int d = ri.y + kd, h = ri.z + kh, w = ri.w + kw;
       e[j] = (kj < s.K && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-                 ? x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + kj % s.Ci]
+                 ? x[((int64_t)ri.x + (kd * s.H + kh) * s.W + kw) * s.Ci + (kj - tap * s.Ci)]
                  : z;
     }
     v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
@@ -378,25 +397,30 @@ struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
   __device__ bf16 operator()(int64_t k, int64_t m) const {
     return k == s.Kp ? __float2bfloat16(1.f) : im2col(x, s, m, (int)k);
   }
+  // Row info of row k < K: (ci, kd, kh, kw).
+  __device__ int4 row_info(int64_t k64, int64_t) const {
+    const int k = (int)k64;
+    if (k >= s.K) return make_int4(0, 0, 0, 0);
+    const int tap = k / s.Ci;
+    return make_int4(k - tap * s.Ci, tap / 9, (tap / 3) % 3, tap % 3);
+  }
   // eight consecutive output voxels m.. at one (tap, ci): decomposed once, then stepped
-  __device__ bool load8(int64_t k, int64_t m, uint4& v) const {
+  __device__ bool load8(int64_t k, int64_t m, const int4& ri, uint4& v) const {
     if (k == s.Kp) {
       v = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);  // BF16 ones
       return true;
     }
     v = make_uint4(0u, 0u, 0u, 0u);
     if (k >= s.K) return true;
-    const int ci = (int)(k % s.Ci), tap = (int)(k / s.Ci);
-    const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
     int b, od, oh, ow;
     out_voxel(s, m, b, od, oh, ow);
     const bf16 z = __float2bfloat16(0.f);
     bf16 e[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const int d = 2 * od - 1 + kd, h = 2 * oh - 1 + kh, w = 2 * ow - 1 + kw;
+      const int d = 2 * od - 1 + ri.y, h = 2 * oh - 1 + ri.z, w = 2 * ow - 1 + ri.w;
       e[j] = (b < s.B && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-                 ? x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + ci]
+                 ? x[((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + ri.x]
                  : z;
       if (++ow == s.Wo) {
         ow = 0;
@@ -412,22 +436,37 @@ struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
     v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
     return true;
   }
-  // Ci % 8 == 0: eight channels of one tap (one 16-byte load) per row group and voxel
-  __device__ bool fill(bf16* As, int64_t row0, int64_t rows, int64_t m0, int64_t r_end) const {
+  // Ci % 8 == 0: lane = reduction column (its voxel decomposed once per stage); per
+  // row group of eight k (one tap, eight channels) one 16-byte load, stored transposed
+  __device__ bool fill(bf16* As, int64_t row0, int64_t rows, int64_t m0, int64_t r_end,
+                       const int4* rinfo) const {
     if (!vec) return false;
-    fill_transposed(As, kBM / 8, [&](int g, int mc, uint4& v) {
-      const int64_t k = row0 + g * 8, m = m0 + mc;
-      if (k >= rows) return false;
-      v = make_uint4(0u, 0u, 0u, 0u);
-      if (m >= r_end) return true;
-      if (k == s.Kp) {
-        v.x = 0x3F80u;  // row Kp: one; rows Kp+1.. are past ``rows``
-      } else if (k < s.K) {
-        const int64_t o = tap_offset(s, m, (int)(k / s.Ci));
-        if (o >= 0) v = *(const uint4*)(x + o + k % s.Ci);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t m = m0 + lane;
+    const bool mv = m < r_end;
+    int b = 0, od = 0, oh = 0, ow = 0;
+    if (mv) out_voxel(s, m, b, od, oh, ow);
+    const int d0 = 2 * od - 1, h0 = 2 * oh - 1, w0 = 2 * ow - 1;
+    const int vbase = ((b * s.D + d0) * s.H + h0) * s.W + w0;
+#pragma unroll
+    for (int i = 0; i < kBM / 8 / (kConvThreads / 32); ++i) {
+      const int g = warp + (kConvThreads / 32) * i;
+      const int64_t k = row0 + g * 8;
+      if (k >= rows) continue;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (mv) {
+        if (k == s.Kp) {
+          v.x = 0x3F80u;  // row Kp: one; rows Kp+1.. are past ``rows``
+        } else if (k < s.K) {
+          const int4 ri = rinfo[g * 8];
+          const int d = d0 + ri.y, h = h0 + ri.z, w = w0 + ri.w;
+          if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+            v = *(const uint4*)(x + ((int64_t)vbase + (ri.y * s.H + ri.z) * s.W + ri.w) * s.Ci +
+                                ri.x);
+        }
       }
-      return true;
-    });
+      store_rotated8(As, g, lane, v);
+    }
     return true;
   }
 };
@@ -555,16 +594,30 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
     const int64_t o = offset(q, t);
     return o < 0 ? __float2bfloat16(0.f) : dp[o + r % s.Co];
   }
-  __device__ bool load8(int64_t q, int64_t r, uint4& v) const {
+  // Row info of class row q: its input voxel (b, d, h, w).
+  __device__ int4 row_info(int64_t q, int64_t rows) const {
+    if (q >= rows) return make_int4(0, 0, 0, 0);
+    int b, d, h, w;
+    cls_voxel(c, q, b, d, h, w);
+    return make_int4(b, d, h, w);
+  }
+  __device__ bool load8(int64_t, int64_t r64, const int4& ri, uint4& v) const {
     if (!vec) return false;
     v = make_uint4(0u, 0u, 0u, 0u);
-    const int t = (int)(r / s.Co);
+    const int r = (int)r64, t = r / s.Co;
     if (t >= c.T) return true;
-    const int64_t o = offset(q, t);
-    if (o >= 0) v = *(const uint4*)(dp + o + r % s.Co);
+    int kk[3];
+    cls_tap(c, t, kk);
+    const int od = (ri.y + 1 - kk[0]) >> 1, oh = (ri.z + 1 - kk[1]) >> 1,
+              ow = (ri.w + 1 - kk[2]) >> 1;
+    if (od < 0 || od >= s.Do || oh < 0 || oh >= s.Ho || ow < 0 || ow >= s.Wo) return true;
+    v = *(const uint4*)(dp + ((((int64_t)ri.x * s.Do + od) * s.Ho + oh) * s.Wo + ow) * s.Co +
+                        (r - t * s.Co));
     return true;
   }
-  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t) const { return false; }
+  __device__ bool fill(bf16*, int64_t, int64_t, int64_t, int64_t, const int4*) const {
+    return false;
+  }
 };
 struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
   const bf16* w;
