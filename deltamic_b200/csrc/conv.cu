@@ -380,11 +380,25 @@ struct FwdEp {
 // ---------------------------------------------------------------------------
 // backward pieces
 
+// dP = dact * GELU'(pre) in BF16; four elements per thread (n is a multiple of 16,
+// pointers 16-byte aligned), else one.
+template <bool kVec>
 __global__ void k_gelu_back(const float* __restrict__ pre, const float* __restrict__ dact,
                             bf16* __restrict__ dpre, int64_t n) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    dpre[i] = __float2bfloat16(dact[i] * gelu_grad(pre[i]));
+  if (kVec) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 4;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      const float4 p = ((const float4*)pre)[i], g = ((const float4*)dact)[i];
+      ((uint2*)dpre)[i] = make_uint2(pack2(__float2bfloat16(g.x * gelu_grad(p.x)),
+                                           __float2bfloat16(g.y * gelu_grad(p.y))),
+                                     pack2(__float2bfloat16(g.z * gelu_grad(p.z)),
+                                           __float2bfloat16(g.w * gelu_grad(p.w))));
+    }
+  } else {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      dpre[i] = __float2bfloat16(dact[i] * gelu_grad(pre[i]));
+  }
 }
 
 struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
@@ -502,18 +516,28 @@ struct WgradEp {  // partial[split][k][n] (16-byte aligned workspace rows)
 };
 
 // Fixed-order sum of the split partials [split][Kp + 1][Co]: rows < Kp into dw,
-// row Kp (the ones row) into db.
-__global__ void k_sum_splits(const float* __restrict__ part, int splits, int64_t nw, int Co,
-                             float* __restrict__ dw, float* __restrict__ db) {
+// row Kp (the ones row) into db.  Block (32, 8): x runs along the outputs
+// (coalesced), y takes every eighth split; the eight partial sums are added in
+// order of y.
+__global__ void __launch_bounds__(256) k_sum_splits(const float* __restrict__ part, int splits,
+                                                    int64_t nw, int Co, float* __restrict__ dw,
+                                                    float* __restrict__ db) {
+  __shared__ float sh[8][33];
   const int64_t n = nw + Co;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int k = 0; k < splits; ++k) s += part[k * n + i];
+  const int64_t i = (int64_t)blockIdx.x * 32 + threadIdx.x;
+  float s = 0.f;
+  if (i < n)
+    for (int k = threadIdx.y; k < splits; k += 8) s += part[k * n + i];
+  sh[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && i < n) {
+    float t = sh[0][threadIdx.x];
+#pragma unroll
+    for (int y = 1; y < 8; ++y) t += sh[y][threadIdx.x];
     if (i < nw)
-      dw[i] = s;
+      dw[i] = t;
     else
-      db[i - nw] = s;
+      db[i - nw] = t;
   }
 }
 
@@ -773,8 +797,12 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   bf16* dp = (bf16*)base;
   float* part = (float*)(base + ((size_t)s.M * s.Co * sizeof(bf16) + 255) / 256 * 256);
   const int64_t nout = s.M * s.Co;
-  k_gelu_back<<<(unsigned)std::min<int64_t>((nout + 255) / 256, 148 * 16), 256, 0, st>>>(
-      pre, dact, dp, nout);
+  if (aligned16(pre) && aligned16(dact) && aligned16(dp))  // nout: a multiple of 16
+    k_gelu_back<true><<<(unsigned)std::min<int64_t>((nout / 4 + 255) / 256, 148 * 16), 256, 0,
+                        st>>>(pre, dact, dp, nout);
+  else
+    k_gelu_back<false><<<(unsigned)std::min<int64_t>((nout + 255) / 256, 148 * 16), 256, 0, st>>>(
+        pre, dact, dp, nout);
   count_launches(1);
   // weight and bias gradients: rows = Kp + 1 (the last row of A^T is ones), the
   // reduction over m split across blockIdx.y
@@ -785,8 +813,8 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
               WgradEp{part, (int64_t)(s.Kp + 1) * s.Co, s.Co}, (int64_t)s.Kp + 1, s.M, per, used,
               1, st);
   const int64_t nw = (int64_t)s.Kp * s.Co;
-  k_sum_splits<<<(unsigned)std::min<int64_t>((nw + s.Co + 255) / 256, 148 * 4), 256, 0, st>>>(
-      part, used, nw, s.Co, dw, db);
+  k_sum_splits<<<(unsigned)((nw + s.Co + 31) / 32), dim3(32, 8), 0, st>>>(part, used, nw, s.Co,
+                                                                          dw, db);
   count_launches(1);
   // data gradient: the eight parity classes of the input voxels in one launch
   if (dx) {
