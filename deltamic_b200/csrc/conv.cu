@@ -126,12 +126,21 @@ __device__ __forceinline__ void store_rotated8(bf16* S, int g, int mc, const uin
   }
 }
 
-template <class F>
+// Up to kMaxGroups / 4 units per thread, all loaded before any is stored.
+template <int kMaxGroups, class F>
 __device__ __forceinline__ void fill_transposed(bf16* S, int ngroups, F unit) {
-  for (int u = threadIdx.x; u < ngroups * 32; u += kConvThreads) {
-    const int g = u >> 5, mc = u & 31;
-    uint4 v;
-    if (unit(g, mc, v)) store_rotated8(S, g, mc, v);
+  constexpr int kPer = kMaxGroups * 32 / kConvThreads;
+  uint4 v[kPer];
+  bool use[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int u = threadIdx.x + i * kConvThreads;
+    use[i] = u < ngroups * 32 && unit(u >> 5, u & 31, v[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int u = threadIdx.x + i * kConvThreads;
+    if (use[i]) store_rotated8(S, u >> 5, u & 31, v[i]);
   }
 }
 
@@ -159,17 +168,26 @@ struct UmmaTile {
 // eight lanes store one 128-byte core-matrix column (no bank conflicts), and tiles
 // with at most 32 live rows still spread over every thread.  Rows past ``rows``
 // are left as they are: they only feed accumulator rows that are never read.
+// All of a thread's chunks are loaded before any is stored, so their global loads
+// are in flight together.
 template <class LA>
 __device__ __forceinline__ void fill_a(const LA& la, bf16* As, int64_t row0, int64_t rows,
                                        int64_t k0, int64_t r_end, const int4* rinfo) {
   if (la.fill(As, row0, rows, k0, r_end, rinfo)) return;
+  constexpr int kPer = kBM * (kBK / 8) / kConvThreads;
+  uint4 v[kPer];
 #pragma unroll
-  for (int i = 0; i < kBM * (kBK / 8) / kConvThreads; ++i) {
+  for (int i = 0; i < kPer; ++i) {
     const int e = threadIdx.x + i * kConvThreads;
     const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
-    if (row0 + r < rows)
-      *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) =
-          gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end, rinfo[r]);
+    v[i] = row0 + r < rows ? gather8_a(la, row0 + r, rows, k0 + kc * 8, r_end, rinfo[r])
+                           : make_uint4(0u, 0u, 0u, 0u);
+  }
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int e = threadIdx.x + i * kConvThreads;
+    const int r = (e & 7) + ((e >> 5) << 3), kc = (e >> 3) & 3;
+    *(uint4*)(As + tc::kmaj32_off(r, kc * 8)) = v[i];
   }
 }
 
@@ -177,9 +195,17 @@ __device__ __forceinline__ void fill_a(const LA& la, bf16* As, int64_t row0, int
 template <int BN, class LB>
 __device__ __forceinline__ void fill_b(const LB& lb, bf16* Bs, int64_t k0, int64_t r_end) {
   if (lb.fill(Bs, BN, k0, r_end)) return;
-  for (int e = threadIdx.x; e < BN * (kBK / 8); e += kConvThreads) {
-    const int n = e % BN, kc = e / BN;
-    *(uint4*)(Bs + tc::kmaj32_off(n, kc * 8)) = gather8_b(lb, n, k0 + kc * 8, r_end);
+  constexpr int kChunks = BN * (kBK / 8), kPer = (kChunks + kConvThreads - 1) / kConvThreads;
+  uint4 v[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int e = threadIdx.x + i * kConvThreads;
+    if (e < kChunks) v[i] = gather8_b(lb, e % BN, k0 + (e / BN) * 8, r_end);
+  }
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int e = threadIdx.x + i * kConvThreads;
+    if (e < kChunks) *(uint4*)(Bs + tc::kmaj32_off(e % BN, (e / BN) * 8)) = v[i];
   }
 }
 
@@ -313,17 +339,27 @@ struct FwdA {
         v = *(const uint4*)(x + ((int64_t)ri.x + (kd * s.H + kh) * s.W + kw) * s.Ci + ci);
       return true;
     }
-    // Ci < 8: the chunk runs across taps
+    // Ci < 8: the chunk runs across taps; (ci, kw, kh, kd) decomposed once, then stepped
+    const int tap = k / s.Ci;
+    int ci = k - tap * s.Ci, kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
     const bf16 z = __float2bfloat16(0.f);
     bf16 e[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const int kj = k + j, tap = kj / s.Ci;
-      const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
       const int d = ri.y + kd, h = ri.z + kh, w = ri.w + kw;
-      e[j] = (kj < s.K && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-                 ? x[((int64_t)ri.x + (kd * s.H + kh) * s.W + kw) * s.Ci + (kj - tap * s.Ci)]
+      e[j] = (k + j < s.K && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+                 ? x[((int64_t)ri.x + (kd * s.H + kh) * s.W + kw) * s.Ci + ci]
                  : z;
+      if (++ci == s.Ci) {
+        ci = 0;
+        if (++kw == 3) {
+          kw = 0;
+          if (++kh == 3) {
+            kh = 0;
+            ++kd;
+          }
+        }
+      }
     }
     v = make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
     return true;
@@ -462,24 +498,29 @@ struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
     if (mv) out_voxel(s, m, b, od, oh, ow);
     const int d0 = 2 * od - 1, h0 = 2 * oh - 1, w0 = 2 * ow - 1;
     const int vbase = ((b * s.D + d0) * s.H + h0) * s.W + w0;
+    constexpr int kPer = kBM / 8 / (kConvThreads / 32);
+    uint4 v[kPer];
 #pragma unroll
-    for (int i = 0; i < kBM / 8 / (kConvThreads / 32); ++i) {
+    for (int i = 0; i < kPer; ++i) {
       const int g = warp + (kConvThreads / 32) * i;
       const int64_t k = row0 + g * 8;
-      if (k >= rows) continue;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (mv) {
+      v[i] = make_uint4(0u, 0u, 0u, 0u);
+      if (mv && k < rows) {
         if (k == s.Kp) {
-          v.x = 0x3F80u;  // row Kp: one; rows Kp+1.. are past ``rows``
+          v[i].x = 0x3F80u;  // row Kp: one; rows Kp+1.. are past ``rows``
         } else if (k < s.K) {
           const int4 ri = rinfo[g * 8];
           const int d = d0 + ri.y, h = h0 + ri.z, w = w0 + ri.w;
           if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-            v = *(const uint4*)(x + ((int64_t)vbase + (ri.y * s.H + ri.z) * s.W + ri.w) * s.Ci +
-                                ri.x);
+            v[i] = *(const uint4*)(x + ((int64_t)vbase + (ri.y * s.H + ri.z) * s.W + ri.w) *
+                                           s.Ci + ri.x);
         }
       }
-      store_rotated8(As, g, lane, v);
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int g = warp + (kConvThreads / 32) * i;
+      if (row0 + g * 8 < rows) store_rotated8(As, g, lane, v[i]);
     }
     return true;
   }
@@ -493,7 +534,7 @@ struct DpreB {  // dP[m, n]
   __device__ bool load8(int64_t, int, uint4&) const { return false; }
   __device__ bool fill(bf16* Bs, int bn, int64_t m0, int64_t r_end) const {
     if (!vec) return false;
-    fill_transposed(Bs, bn / 8, [&](int g, int mc, uint4& v) {
+    fill_transposed<128 / 8>(Bs, bn / 8, [&](int g, int mc, uint4& v) {
       const int64_t m = m0 + mc;
       v = make_uint4(0u, 0u, 0u, 0u);
       if (m < r_end) v = *(const uint4*)(dp + m * Co + g * 8);
@@ -758,9 +799,13 @@ bool conv_shape(int B, int D, int H, int W, int Ci, int Co, ConvShape& s) {
   return true;
 }
 
+// Blocks per SM the tile kernel reaches: shared memory allows 8-10 up to BN = 64,
+// the 512 TMEM columns 4 at BN = 128.
+static int tile_blocks_per_sm(int bn) { return bn >= 128 ? 4 : 8; }
+
 static int wgrad_splits(const ConvShape& s) {
   const int64_t row_tiles = (s.Kp + 1 + kBM - 1) / kBM;
-  int64_t sp = std::max<int64_t>(1, (int64_t)148 * 4 / row_tiles);
+  int64_t sp = std::max<int64_t>(1, (int64_t)148 * tile_blocks_per_sm(s.Co) / row_tiles);
   sp = std::min<int64_t>(sp, std::max<int64_t>(1, s.M / (4 * kBK)));
   return (int)sp;
 }
