@@ -866,8 +866,11 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
     ClsSet set;
     int64_t max_rows = 0, max_red = 0;
     const int dims[3] = {s.D, s.H, s.W};
-    for (int cls = 0; cls < 8; ++cls) {
-      Cls& c = set.c[cls];
+    // z = 7 - parity bits: the class with the most taps (all odd) first, so the
+    // longest blocks are not the last to start
+    for (int z = 0; z < 8; ++z) {
+      const int cls = 7 - z;
+      Cls& c = set.c[z];
       c.T = 1;
       bool empty = false;
       for (int a = 0; a < 3; ++a) {
