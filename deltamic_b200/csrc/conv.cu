@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "../../include/deltamic_b200.h"
 #include "band_internal.h"
@@ -748,14 +749,22 @@ struct DgradEp {
 // ---------------------------------------------------------------------------
 // launchers
 
-// Status word of the convolution kernels (bounded waits that gave up).
+// Status word of the convolution kernels (bounded waits that gave up), one per
+// device; its device address is looked up per device (with that device current).
 __device__ int g_conv_status;
 
+constexpr int kConvMaxDevices = 64;
+static std::atomic<int*> g_conv_status_addr[kConvMaxDevices];
+
 static int* conv_status_ptr() {
-  static int* p = nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kConvMaxDevices) return nullptr;
+  int* p = g_conv_status_addr[dev].load();
   if (!p) {
     void* a = nullptr;
-    if (cudaGetSymbolAddress(&a, g_conv_status) == cudaSuccess) p = (int*)a;
+    if (cudaGetSymbolAddress(&a, g_conv_status) != cudaSuccess) return nullptr;
+    p = (int*)a;
+    g_conv_status_addr[dev].store(p);
   }
   return p;
 }
