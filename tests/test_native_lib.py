@@ -103,3 +103,26 @@ def test_bandbox_render_host_checks(lib):
     assert lib.dm_render_loss_bandbox(fake, fake, 1, ctypes.byref(box), narrow, None, 0, None,
                                       0.0, fake, None, None, fake, 1024,
                                       None) == N.DM_ERR_WORKSPACE
+
+
+def test_conv_host_checks(lib):
+    """Convolution entry points: shapes outside the kernels' limits (Co not in
+    {16, 32, 64, 128}, Ci > 128, tensors of 2^31 elements or more) are refused on the
+    host; the workspace holds dP (BF16) and the weight-gradient split partials with
+    the bias row."""
+    from deltamic_b200 import _native as N
+    assert lib.dm_conv3d_s2_workspace_size(2, 16, 16, 16, 1, 24) == 0
+    assert lib.dm_conv3d_s2_workspace_size(2, 16, 16, 16, 129, 32) == 0
+    assert lib.dm_conv3d_s2_workspace_size(1024, 128, 128, 128, 1, 16) == 0  # 2^31 * 16
+    ws = lib.dm_conv3d_s2_workspace_size(2, 16, 16, 16, 16, 32)
+    M, Kp = 2 * 8 ** 3, 448
+    assert ws >= M * 32 * 2 + (Kp + 1) * 32 * 4
+    assert lib.dm_conv3d_s2_forward(None, 2, 16, 16, 16, 16, None, None, 32, None, None,
+                                    None) == N.DM_ERR_INVALID_ARG
+    assert lib.dm_conv3d_s2_forward(ctypes.c_void_p(16), 2, 16, 16, 16, 16, ctypes.c_void_p(16),
+                                    None, 48, ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                    None) == N.DM_ERR_INVALID_ARG
+    p = ctypes.c_void_p(16)
+    assert lib.dm_conv3d_s2_backward(p, 2, 16, 16, 16, 16, p, 32, p, p, None, p, p, p, ws - 1,
+                                     None) == N.DM_ERR_WORKSPACE
+    assert lib.dm_conv3d_s2_device_error(None, None) == N.DM_ERR_INVALID_ARG
