@@ -168,9 +168,9 @@ struct UmmaTile {
 // the reduction.  Chunk e: row (e & 7) + 8 (e >> 5), reduction chunk (e >> 3) & 3 --
 // eight lanes store one 128-byte core-matrix column (no bank conflicts), and tiles
 // with at most 32 live rows still spread over every thread.  Rows past ``rows``
-// are left as they are: they only feed accumulator rows that are never read.
-// All of a thread's chunks are loaded before any is stored, so their global loads
-// are in flight together.
+// are stored as zeros (they only feed accumulator rows that are never read).  All
+// of a thread's chunks are loaded before any is stored, so their global loads are
+// in flight together.
 template <class LA>
 __device__ __forceinline__ void fill_a(const LA& la, bf16* As, int64_t row0, int64_t rows,
                                        int64_t k0, int64_t r_end, const int4* rinfo) {
@@ -212,10 +212,11 @@ __device__ __forceinline__ void fill_b(const LB& lb, bf16* Bs, int64_t k0, int64
 
 // Generic tile: C[rows x BN] over a reduction [r_begin, r_end) split by blockIdx.y,
 // C = sum_k A[row, k] B[k, col] with A = la(row, k), B = lb(k, col), then
-// ep.put16(row, col, split, C[row, col..col+15]).  Every thread gathers its share of a stage into shared memory;
-// one thread issues the stage's two tcgen05 MMAs into the TMEM accumulator and
-// commits them to the stage's mbarrier, so the next stage's gather overlaps them.
-// Each warp reads its 32 accumulator rows back from TMEM for the epilogue.
+// ep.put16(row, col, split, C[row, col..col+15]).  Every thread gathers its share
+// of a stage into shared memory; one thread issues the stage's two tcgen05 MMAs
+// into the TMEM accumulator and commits them to the stage's mbarrier, so the next
+// stage's gather overlaps them.  Each warp reads its 32 accumulator rows back from
+// TMEM for the epilogue.
 template <int BN, class LA, class LB, class EP>
 __global__ void __launch_bounds__(kConvThreads) k_conv_umma(LA la0, LB lb0, EP ep0, int64_t rows0,
                                                             int64_t red_total0, int64_t red_split,
