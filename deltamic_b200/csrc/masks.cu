@@ -223,7 +223,7 @@ __global__ void k_children(const double* __restrict__ verts, int64_t nv,
 // Uniform bucket grid over the query box (centroids outside it go to the border
 // buckets; every bucket's box is the tight box of its own centroids).
 struct Buckets {
-  double lo[3], inv[3];
+  double lo[3], inv[3], h[3];  // h = 1 / inv: the bucket edge
   int32_t n[3];
 };
 
@@ -311,76 +311,105 @@ __global__ void k_bucket_boxes(const int32_t* __restrict__ off, const int32_t* _
   rec[nz_off[b]] = r;
 }
 
-// One thread per grid point.  Pass 1: U = the smallest farthest-corner distance
-// over the non-empty buckets (some centroid lies within it).  Pass 2: the
-// centroids of every bucket whose nearest corner is within min(U, best), the
-// nearest by (distance, child index).  Then the label on the point's side.
-constexpr int kRecTile = 64;
+constexpr double kSlackLabel = 1.0 + 1e-12;  // rounding of the box and face distances
+
+__device__ __forceinline__ int bucket_axis(const Buckets& g, int d, double x) {
+  const double t = (x - g.lo[d]) * g.inv[d];
+  return isfinite(t) ? (int)fmin(fmax(floor(t), 0.0), (double)(g.n[d] - 1)) : 0;
+}
+
+// Bucket b: skip it if its tight box is farther than ``best``, else its centroids
+// against (best, bi) by (squared distance, child index).
+__device__ __forceinline__ void visit_bucket(int64_t b, double q0, double q1, double q2,
+                                             const double* __restrict__ cen,
+                                             const int32_t* __restrict__ slot,
+                                             const int32_t* __restrict__ off,
+                                             const int32_t* __restrict__ nzo,
+                                             const BucketRec* __restrict__ rec, double& best,
+                                             int64_t& bi) {
+  const int32_t s0 = off[b], s1 = off[b + 1];
+  if (s0 == s1) return;
+  const BucketRec& r = rec[nzo[b]];
+  const double e0 = fmax(fmax(r.lo[0] - q0, q0 - r.hi[0]), 0.0);
+  const double e1 = fmax(fmax(r.lo[1] - q1, q1 - r.hi[1]), 0.0);
+  const double e2 = fmax(fmax(r.lo[2] - q2, q2 - r.hi[2]), 0.0);
+  if (e0 * e0 + e1 * e1 + e2 * e2 > best * kSlackLabel) return;
+  for (int32_t s = s0; s < s1; ++s) {
+    const int64_t c = slot[s];
+    const double dx = cen[3 * c] - q0, dy = cen[3 * c + 1] - q1, dz = cen[3 * c + 2] - q2;
+    const double dd = dx * dx + dy * dy + dz * dz;
+    if (dd < best || (dd == best && c < bi)) {
+      best = dd;
+      bi = c;
+    }
+  }
+}
+
+// Distance from x to the faces of the visited cube (buckets c - r .. c + r on axis
+// d) that have buckets beyond them, less a rounding margin.
+__device__ __forceinline__ void face_bound(const Buckets& g, int d, int c, int r, double x,
+                                           double& bound, bool& covered) {
+  const double h = g.h[d];
+  if (c - r > 0) {
+    covered = false;
+    bound = fmin(bound, x - (g.lo[d] + (c - r) * h) - 1e-9 * h);
+  }
+  if (c + r < g.n[d] - 1) {
+    covered = false;
+    bound = fmin(bound, (g.lo[d] + (c + r + 1) * h) - x - 1e-9 * h);
+  }
+}
+
+// One thread per grid point: exact nearest child centroid by (distance, child
+// index) through the bucket grid, visiting shells of buckets (Chebyshev distance
+// r = 0, 1, 2, ... from the point's own bucket) and skipping a bucket whose tight
+// box is farther than the best distance so far.  After shell r every unvisited
+// centroid lies beyond a face of the cube of visited buckets (a centroid clamped
+// into a border bucket lies beyond the box, hence beyond that face too), so the
+// search stops once the nearest such face is farther than the best distance (or
+// the cube covers the grid).  Then the label on the point's side of the child.
 __global__ void __launch_bounds__(kThreads)
     k_nearest_label(const double* __restrict__ cen, const double* __restrict__ nrm,
                     const double* __restrict__ lab, const int32_t* __restrict__ slot,
-                    const BucketRec* __restrict__ rec, const int32_t* __restrict__ n_rec_p,
-                    Axes a, double* __restrict__ out) {
-  __shared__ BucketRec sr[kRecTile];
+                    const int32_t* __restrict__ off, const int32_t* __restrict__ nzo,
+                    const BucketRec* __restrict__ rec, Buckets g, Axes a,
+                    double* __restrict__ out) {
   const int64_t npts = (int64_t)a.n[0] * a.n[1] * a.n[2];
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = p < npts;
-  const int32_t n_rec = *n_rec_p;
-  double q[3] = {0.0, 0.0, 0.0};
-  if (live) {
-    const int64_t nyz = (int64_t)a.n[1] * a.n[2];
-    const int ix = (int)(p / nyz), iy = (int)((p / a.n[2]) % a.n[1]), iz = (int)(p % a.n[2]);
-    q[0] = grid_value(a, 0, ix);
-    q[1] = grid_value(a, 1, iy);
-    q[2] = grid_value(a, 2, iz);
-  }
-  constexpr double kSlack = 1.0 + 1e-12;  // rounding of the box distances
-  double U = INFINITY;
-  for (int t0 = 0; t0 < n_rec; t0 += kRecTile) {
-    const int cnt = min(kRecTile, n_rec - t0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sr[k] = rec[t0 + k];
-    __syncthreads();
-    for (int k = 0; k < cnt; ++k) {
-      double far2 = 0.0;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double f = fmax(fabs(q[d] - sr[k].lo[d]), fabs(q[d] - sr[k].hi[d]));
-        far2 += f * f;
-      }
-      U = fmin(U, far2);
-    }
-  }
+  if (p >= npts) return;
+  const int64_t nyz = (int64_t)a.n[1] * a.n[2];
+  const int ix = (int)(p / nyz), iy = (int)((p / a.n[2]) % a.n[1]), iz = (int)(p % a.n[2]);
+  const double q0 = grid_value(a, 0, ix), q1 = grid_value(a, 1, iy), q2 = grid_value(a, 2, iz);
+  // the point's bucket, as bucket_of assigns centroids
+  const int c0 = bucket_axis(g, 0, q0), c1 = bucket_axis(g, 1, q1), c2 = bucket_axis(g, 2, q2);
   double best = INFINITY;
   int64_t bi = 0;
-  for (int t0 = 0; t0 < n_rec; t0 += kRecTile) {
-    const int cnt = min(kRecTile, n_rec - t0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) sr[k] = rec[t0 + k];
-    __syncthreads();
-    if (!live) continue;
-    for (int k = 0; k < cnt; ++k) {
-      double near2 = 0.0;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double e = fmax(fmax(sr[k].lo[d] - q[d], q[d] - sr[k].hi[d]), 0.0);
-        near2 += e * e;
-      }
-      if (near2 > fmin(U, best) * kSlack) continue;
-      for (int32_t s = sr[k].first; s < sr[k].first + sr[k].count; ++s) {
-        const int64_t c = slot[s];
-        const double dx = cen[3 * c] - q[0], dy = cen[3 * c + 1] - q[1],
-                     dz = cen[3 * c + 2] - q[2];
-        const double dd = dx * dx + dy * dy + dz * dz;
-        if (dd < best || (dd == best && c < bi)) {
-          best = dd;
-          bi = c;
-        }
+  const int rmax = max(g.n[0], max(g.n[1], g.n[2]));
+  for (int r = 0; r <= rmax; ++r) {
+    for (int dx = -r; dx <= r; ++dx) {
+      const int x = c0 + dx;
+      if (x < 0 || x >= g.n[0]) continue;
+      const bool ex = dx == -r || dx == r;
+      for (int dy = -r; dy <= r; ++dy) {
+        const int y = c1 + dy;
+        if (y < 0 || y >= g.n[1]) continue;
+        const int64_t row = ((int64_t)x * g.n[1] + y) * g.n[2];
+        // on an x or y face of the shell the whole z range, else its two z faces
+        const int step = (ex || dy == -r || dy == r) ? 1 : 2 * r;
+        for (int z = c2 - r; z <= c2 + r; z += step)
+          if (z >= 0 && z < g.n[2])
+            visit_bucket(row + z, q0, q1, q2, cen, slot, off, nzo, rec, best, bi);
       }
     }
+    // nearest face of the visited cube that has unvisited buckets beyond it
+    double bound = INFINITY;
+    bool covered = true;
+    face_bound(g, 0, c0, r, q0, bound, covered);
+    face_bound(g, 1, c1, r, q1, bound, covered);
+    face_bound(g, 2, c2, r, q2, bound, covered);
+    if (covered || (bound > 0.0 && bound * bound > best * kSlackLabel)) break;
   }
-  if (!live) return;
-  const double vx = cen[3 * bi] - q[0], vy = cen[3 * bi + 1] - q[1], vz = cen[3 * bi + 2] - q[2];
+  const double vx = cen[3 * bi] - q0, vy = cen[3 * bi + 1] - q1, vz = cen[3 * bi + 2] - q2;
   const double dot = __dadd_rn(__dadd_rn(__dmul_rn(vx, nrm[3 * bi]), __dmul_rn(vy, nrm[3 * bi + 1])),
                                __dmul_rn(vz, nrm[3 * bi + 2]));
   out[p] = lab[2 * bi + (dot < 0.0 ? 1 : 0)] + 1.0;
@@ -400,6 +429,7 @@ Buckets bucket_grid(const dm_box* b, int64_t nc) {
     g.n[d] = (int32_t)std::max(1.0, std::min(128.0, ceil(L[d] / h)));
     g.lo[d] = b->lo[d];
     g.inv[d] = g.n[d] / L[d];
+    g.h[d] = L[d] / g.n[d];
   }
   return g;
 }
@@ -515,7 +545,7 @@ int dm_instance_mask(const double* verts, int64_t nv, const int64_t* faces, int6
   k_bucket_boxes<<<gb, kThreads, 0, st>>>(off, nzo, slot, cen, nb, rec);
   const int64_t npts = (int64_t)box->shape[0] * box->shape[1] * box->shape[2];
   k_nearest_label<<<(unsigned)cdiv(npts, kThreads), kThreads, 0, st>>>(
-      cen, nrm, lab, slot, rec, nzo + nb, make_axes(box), mask);
+      cen, nrm, lab, slot, off, nzo, rec, g, make_axes(box), mask);
   count_launches(7);
   return status();
 }
