@@ -318,35 +318,9 @@ __device__ __forceinline__ int bucket_axis(const Buckets& g, int d, double x) {
   return isfinite(t) ? (int)fmin(fmax(floor(t), 0.0), (double)(g.n[d] - 1)) : 0;
 }
 
-// Bucket b: skip it if its tight box is farther than ``best``, else its centroids
-// against (best, bi) by (squared distance, child index).
-__device__ __forceinline__ void visit_bucket(int64_t b, double q0, double q1, double q2,
-                                             const double* __restrict__ cen,
-                                             const int32_t* __restrict__ slot,
-                                             const int32_t* __restrict__ off,
-                                             const int32_t* __restrict__ nzo,
-                                             const BucketRec* __restrict__ rec, double& best,
-                                             int64_t& bi) {
-  const int32_t s0 = off[b], s1 = off[b + 1];
-  if (s0 == s1) return;
-  const BucketRec& r = rec[nzo[b]];
-  const double e0 = fmax(fmax(r.lo[0] - q0, q0 - r.hi[0]), 0.0);
-  const double e1 = fmax(fmax(r.lo[1] - q1, q1 - r.hi[1]), 0.0);
-  const double e2 = fmax(fmax(r.lo[2] - q2, q2 - r.hi[2]), 0.0);
-  if (e0 * e0 + e1 * e1 + e2 * e2 > best * kSlackLabel) return;
-  for (int32_t s = s0; s < s1; ++s) {
-    const int64_t c = slot[s];
-    const double dx = cen[3 * c] - q0, dy = cen[3 * c + 1] - q1, dz = cen[3 * c + 2] - q2;
-    const double dd = dx * dx + dy * dy + dz * dz;
-    if (dd < best || (dd == best && c < bi)) {
-      best = dd;
-      bi = c;
-    }
-  }
-}
-
 // Distance from x to the faces of the visited cube (buckets c - r .. c + r on axis
-// d) that have buckets beyond them, less a rounding margin.
+// d) that have buckets beyond them, less a rounding margin (negative while x lies
+// outside the cube).
 __device__ __forceinline__ void face_bound(const Buckets& g, int d, int c, int r, double x,
                                            double& bound, bool& covered) {
   const double h = g.h[d];
@@ -360,28 +334,40 @@ __device__ __forceinline__ void face_bound(const Buckets& g, int d, int c, int r
   }
 }
 
-// One thread per grid point: exact nearest child centroid by (distance, child
-// index) through the bucket grid, visiting shells of buckets (Chebyshev distance
-// r = 0, 1, 2, ... from the point's own bucket) and skipping a bucket whose tight
-// box is farther than the best distance so far.  After shell r every unvisited
-// centroid lies beyond a face of the cube of visited buckets (a centroid clamped
-// into a border bucket lies beyond the box, hence beyond that face too), so the
-// search stops once the nearest such face is farther than the best distance (or
-// the cube covers the grid).  Then the label on the point's side of the child.
+// Grid points by warp: a warp takes a 2 x 4 x 4 brick of grid points (x, y, z),
+// all of which usually fall in one bucket, and walks shells of buckets (Chebyshev
+// distance r = 0, 1, 2, ... from the bucket of the brick's first point) together:
+// a bucket is scanned when its tight box is within the best distance so far of
+// any lane, every lane then measuring every centroid of it (no divergence), and
+// the walk ends when every lane is done -- the nearest face of the visited cube
+// with buckets beyond it is farther than that lane's best distance (every
+// unvisited centroid lies beyond such a face: a centroid clamped into a border
+// bucket lies beyond the box, hence beyond that face too), or the cube covers the
+// grid.  The result per point is the exact nearest child centroid by (distance,
+// child index); then the label on the point's side of that child.
+constexpr int kBrickX = 2, kBrickY = 4, kBrickZ = 4;
 __global__ void __launch_bounds__(kThreads)
     k_nearest_label(const double* __restrict__ cen, const double* __restrict__ nrm,
                     const double* __restrict__ lab, const int32_t* __restrict__ slot,
                     const int32_t* __restrict__ off, const int32_t* __restrict__ nzo,
                     const BucketRec* __restrict__ rec, Buckets g, Axes a,
                     double* __restrict__ out) {
-  const int64_t npts = (int64_t)a.n[0] * a.n[1] * a.n[2];
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npts) return;
-  const int64_t nyz = (int64_t)a.n[1] * a.n[2];
-  const int ix = (int)(p / nyz), iy = (int)((p / a.n[2]) % a.n[1]), iz = (int)(p % a.n[2]);
-  const double q0 = grid_value(a, 0, ix), q1 = grid_value(a, 1, iy), q2 = grid_value(a, 2, iz);
-  // the point's bucket, as bucket_of assigns centroids
-  const int c0 = bucket_axis(g, 0, q0), c1 = bucket_axis(g, 1, q1), c2 = bucket_axis(g, 2, q2);
+  const int lane = threadIdx.x & 31;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nbx = (a.n[0] + kBrickX - 1) / kBrickX, nby = (a.n[1] + kBrickY - 1) / kBrickY,
+            nbz = (a.n[2] + kBrickZ - 1) / kBrickZ;
+  if (w >= (int64_t)nbx * nby * nbz) return;  // whole warp
+  const int bz = (int)(w % nbz), by = (int)((w / nbz) % nby), bx = (int)(w / ((int64_t)nbz * nby));
+  const int ix = bx * kBrickX + (lane >> 4), iy = by * kBrickY + ((lane >> 2) & 3),
+            iz = bz * kBrickZ + (lane & 3);
+  const bool live = ix < a.n[0] && iy < a.n[1] && iz < a.n[2];
+  // lanes past the grid measure the brick's first point and store nothing
+  const double q0 = grid_value(a, 0, live ? ix : bx * kBrickX);
+  const double q1 = grid_value(a, 1, live ? iy : by * kBrickY);
+  const double q2 = grid_value(a, 2, live ? iz : bz * kBrickZ);
+  const int c0 = __shfl_sync(0xffffffffu, bucket_axis(g, 0, q0), 0);
+  const int c1 = __shfl_sync(0xffffffffu, bucket_axis(g, 1, q1), 0);
+  const int c2 = __shfl_sync(0xffffffffu, bucket_axis(g, 2, q2), 0);
   double best = INFINITY;
   int64_t bi = 0;
   const int rmax = max(g.n[0], max(g.n[1], g.n[2]));
@@ -396,23 +382,42 @@ __global__ void __launch_bounds__(kThreads)
         const int64_t row = ((int64_t)x * g.n[1] + y) * g.n[2];
         // on an x or y face of the shell the whole z range, else its two z faces
         const int step = (ex || dy == -r || dy == r) ? 1 : 2 * r;
-        for (int z = c2 - r; z <= c2 + r; z += step)
-          if (z >= 0 && z < g.n[2])
-            visit_bucket(row + z, q0, q1, q2, cen, slot, off, nzo, rec, best, bi);
+        for (int z = c2 - r; z <= c2 + r; z += step) {
+          if (z < 0 || z >= g.n[2]) continue;
+          const int64_t b = row + z;
+          const int32_t s0 = off[b], s1 = off[b + 1];
+          if (s0 == s1) continue;
+          const BucketRec& rb = rec[nzo[b]];
+          const double e0 = fmax(fmax(rb.lo[0] - q0, q0 - rb.hi[0]), 0.0);
+          const double e1 = fmax(fmax(rb.lo[1] - q1, q1 - rb.hi[1]), 0.0);
+          const double e2 = fmax(fmax(rb.lo[2] - q2, q2 - rb.hi[2]), 0.0);
+          const bool need = live && !(e0 * e0 + e1 * e1 + e2 * e2 > best * kSlackLabel);
+          if (!__any_sync(0xffffffffu, need)) continue;
+          for (int32_t s = s0; s < s1; ++s) {
+            const int64_t c = slot[s];
+            const double ux = cen[3 * c] - q0, uy = cen[3 * c + 1] - q1, uz = cen[3 * c + 2] - q2;
+            const double dd = ux * ux + uy * uy + uz * uz;
+            if (dd < best || (dd == best && c < bi)) {
+              best = dd;
+              bi = c;
+            }
+          }
+        }
       }
     }
-    // nearest face of the visited cube that has unvisited buckets beyond it
     double bound = INFINITY;
     bool covered = true;
     face_bound(g, 0, c0, r, q0, bound, covered);
     face_bound(g, 1, c1, r, q1, bound, covered);
     face_bound(g, 2, c2, r, q2, bound, covered);
-    if (covered || (bound > 0.0 && bound * bound > best * kSlackLabel)) break;
+    const bool done = !live || covered || (bound > 0.0 && bound * bound > best * kSlackLabel);
+    if (__all_sync(0xffffffffu, done)) break;
   }
+  if (!live) return;
   const double vx = cen[3 * bi] - q0, vy = cen[3 * bi + 1] - q1, vz = cen[3 * bi + 2] - q2;
   const double dot = __dadd_rn(__dadd_rn(__dmul_rn(vx, nrm[3 * bi]), __dmul_rn(vy, nrm[3 * bi + 1])),
                                __dmul_rn(vz, nrm[3 * bi + 2]));
-  out[p] = lab[2 * bi + (dot < 0.0 ? 1 : 0)] + 1.0;
+  out[((int64_t)ix * a.n[1] + iy) * a.n[2] + iz] = lab[2 * bi + (dot < 0.0 ? 1 : 0)] + 1.0;
 }
 
 // Bucket grid of about nc / 16 buckets over the query box (at most 2^21).
@@ -544,7 +549,9 @@ int dm_instance_mask(const double* verts, int64_t nv, const int64_t* faces, int6
   k_bucket_fill<<<gc, kThreads, 0, st>>>(cen, nc, g, off, cur, slot);
   k_bucket_boxes<<<gb, kThreads, 0, st>>>(off, nzo, slot, cen, nb, rec);
   const int64_t npts = (int64_t)box->shape[0] * box->shape[1] * box->shape[2];
-  k_nearest_label<<<(unsigned)cdiv(npts, kThreads), kThreads, 0, st>>>(
+  const int64_t bricks = cdiv(box->shape[0], kBrickX) * cdiv(box->shape[1], kBrickY) *
+                         cdiv(box->shape[2], kBrickZ);
+  k_nearest_label<<<(unsigned)cdiv(bricks * 32, kThreads), kThreads, 0, st>>>(
       cen, nrm, lab, slot, off, nzo, rec, g, make_axes(box), mask);
   count_launches(7);
   return status();
