@@ -393,6 +393,7 @@ __global__ void __launch_bounds__(kThreads)
           const double e2 = fmax(fmax(rb.lo[2] - q2, q2 - rb.hi[2]), 0.0);
           const bool need = live && !(e0 * e0 + e1 * e1 + e2 * e2 > best * kSlackLabel);
           if (!__any_sync(0xffffffffu, need)) continue;
+#pragma unroll 4
           for (int32_t s = s0; s < s1; ++s) {
             const int64_t c = slot[s];
             const double ux = cen[3 * c] - q0, uy = cen[3 * c + 1] - q1, uz = cen[3 * c + 2] - q2;
