@@ -170,9 +170,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=2048, threads=None):
+def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=6144, threads=None):
     """Oracle (reference algorithm restated in numpy) forward+adjoint on a sample
-    (2,048 band frequencies x all faces: about 10-15 s on 16 host threads)."""
+    (6,144 band frequencies x all faces: about 10 s on 16 host threads), in chunks
+    of at most 2^19 pairs per task."""
     import oracle
     threads = threads or os.cpu_count() or 1
     rng = np.random.default_rng(0)
@@ -181,7 +182,7 @@ def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=2048, threads=None):
     vs = gt_v - box[:, 0]
     coeff = np.ones(len(faces))
     g = np.ones(len(xi), np.complex128)
-    chunk = max(len(faces), len(xi) * len(faces) // (4 * threads))
+    chunk = max(len(faces), min(len(xi) * len(faces) // (4 * threads), 1 << 19))
     t0 = time.perf_counter()
     ft = oracle.meshft_forward(vs, faces, coeff, xi, threads=threads, chunk_pairs=chunk)
     oracle.meshft_backward(vs, faces, coeff, xi, g, ft, threads=threads, chunk_pairs=chunk)
@@ -192,7 +193,7 @@ def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=2048, threads=None):
                       f"float64 numpy ({dt:.1f} s)"}
 
 
-def volume_cpu_baseline(gt_v, faces, band_xi, sample_xi=2048, threads=None, regint=0.5):
+def volume_cpu_baseline(gt_v, faces, band_xi, sample_xi=6144, threads=None, regint=0.5):
     """Oracle of the autofluorescence transform, forward + adjoint, on a sample of
     the band (frequency chunks on a thread pool)."""
     import oracle.volume as ov
@@ -201,7 +202,7 @@ def volume_cpu_baseline(gt_v, faces, band_xi, sample_xi=2048, threads=None, regi
     sub = np.sort(rng.choice(len(band_xi), min(sample_xi, len(band_xi)), replace=False))
     xi = band_xi[sub]
     g = np.ones(len(xi), np.complex128)
-    chunk = max(len(faces), len(xi) * len(faces) // (4 * threads))
+    chunk = max(len(faces), min(len(xi) * len(faces) // (4 * threads), 1 << 19))
     t0 = time.perf_counter()
     ov.volume_forward(gt_v, faces, regint, xi, chunk_pairs=chunk, threads=threads)
     ov.volume_backward(gt_v, faces, regint, xi, g, chunk_pairs=chunk, threads=threads)
@@ -227,7 +228,7 @@ def run_reference(args, rank, world):
     idx = oracle.band_indices(otf, THRESH)
     band_xi = oracle.xi_list_from_band(idx, axes)
     threads = os.cpu_count() or 1
-    per_step = 48
+    per_step = 512  # band frequencies per step: chunks large enough for the thread pool
     vals = []
     for k in range(args.warmup + args.steps):
         r = cpu_baseline(gt_v, faces, box, band_xi[k * per_step % len(band_xi):], per_step,
@@ -310,7 +311,7 @@ def run_reference_volume(args):
     otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
     idx = oracle.band_indices(otf, THRESH)
     band_xi = oracle.xi_list_from_band(idx, axes)
-    per_step = 48
+    per_step = 512  # band frequencies per step: chunks large enough for the thread pool
     threads = os.cpu_count() or 1
     vals = []
     for k in range(args.warmup + args.steps):
