@@ -25,7 +25,7 @@ from .render import (Fourier3dMesh, center_verts_in_box, compute_box_size,
 from .pipeline import MeshRenderer
 from . import masks, mesh_io
 from .masks import create_instance_segmentation_mask, create_semantic_segmentation_mask
-from .mesh_io import read_obj, read_rec, write_obj, write_rec
+from .mesh_io import create_initial_mesh_from_points_mm, read_obj, read_rec, write_obj, write_rec
 
 __all__ = [
     "Fourier3dMesh", "generate_gaussian_psf", "generate_gaussian_psf_from_sigma",
@@ -35,5 +35,6 @@ __all__ = [
     "Anisotropic_gaussian_psf", "Gibson_Lanni_psf", "Hanser_psf", "zernike", "noll2degrees",
     "get_internal_triangle_and_mesh_areas", "get_internal_triangle_and_mesh_areas_and_normals",
     "compute_volume_manifold", "create_semantic_segmentation_mask",
-    "create_instance_segmentation_mask", "read_obj", "write_obj", "read_rec", "write_rec",
+    "create_instance_segmentation_mask", "create_initial_mesh_from_points_mm", "read_obj",
+    "write_obj", "read_rec", "write_rec",
 ]

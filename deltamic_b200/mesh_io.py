@@ -13,6 +13,8 @@ assembly helpers.
   vertex indices and the material labels on either side (the reference reads it
   with an external package's ``open_mesh_multitracker``,
   ``Examples/.ipynb_checkpoints/Example_multimaterial-checkpoint.ipynb``).
+* ``create_initial_mesh_from_points_mm`` (``deltamic/mesh_utilities.py:28-48``): one
+  subdivided sphere per point, merged with region labels.
 * ``combine_all_verts_faces`` / ``combine_all_verts_faces_mm``
   (``deltamic/mesh_utilities.py:8-25``): concatenation of several meshes with the
   face indices offset.
@@ -25,7 +27,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = ["read_obj", "write_obj", "read_rec", "write_rec", "combine_all_verts_faces",
-           "combine_all_verts_faces_mm"]
+           "combine_all_verts_faces_mm", "create_initial_mesh_from_points_mm"]
 
 
 def _obj_index(tok: str, nv: int) -> int:
@@ -125,3 +127,33 @@ def combine_all_verts_faces_mm(All_verts, All_faces):
         total += len(All_verts[i - 1])
         All_faces[i][:, :3] += total
     return np.vstack(All_verts), np.vstack(All_faces).astype(np.int32)
+
+
+def create_initial_mesh_from_points_mm(points, n_subdivisions=3, threshold_dist=0.9):
+    """One sphere per point, merged into a labelled mesh (mesh_utilities.py:28-48).
+
+    Every sphere has radius ``threshold_dist`` x (smallest nonzero distance between
+    the points) / 2 and is an icosahedron subdivided ``n_subdivisions`` times with
+    its vertices pushed to the sphere; sphere ``i`` gets face labels (0, i + 1).
+    Returns ``(verts[nv, 3] float64, faces[nt, 5] int32)`` as
+    ``combine_all_verts_faces_mm`` assembles them.  The reference takes trimesh's
+    primitive sphere, the same construction; this library's icosphere lists the
+    vertices and faces in its own order (the same points, faces outward).  Fewer
+    than two distinct points raise ``ValueError`` (the smallest distance is
+    undefined), as in the reference.
+    """
+    from scipy.spatial.distance import cdist
+
+    from .mesh import icosphere
+
+    points = np.asarray(points, dtype=np.float64)
+    d = cdist(points, points)
+    min_dist = np.amin(d[d != 0]) * threshold_dist
+    all_verts, all_faces = [], []
+    for i in range(len(points)):
+        v, f = icosphere(int(n_subdivisions), radius=min_dist / 2, center=points[i])
+        labels = np.stack([np.zeros(len(f)), np.full(len(f), float(i + 1))], axis=1)
+        all_verts.append(v)
+        all_faces.append(np.concatenate([f.astype(np.float64), labels], axis=1))
+    return combine_all_verts_faces_mm(all_verts, all_faces)
+

@@ -50,3 +50,32 @@ def test_reference_data_files_read():
     v, f = read_rec(os.path.join(REF_DATA, "Sample01_007.rec"))
     assert v.shape == (1996, 3) and f.shape == (4055, 5)
     assert set(np.unique(f[:, 3:]).tolist()) == {0, 1, 2, 3}
+
+
+def test_create_initial_mesh_from_points_mm():
+    """mesh_utilities.py:28-48: radius = threshold * (smallest pairwise distance) / 2,
+    one sphere of 10*4^n + 2 vertices / 20*4^n faces per point, labels (0, i + 1),
+    faces offset per sphere, int32; every face outward and every vertex on its
+    sphere."""
+    from scipy.spatial.distance import cdist
+
+    from deltamic_b200 import create_initial_mesh_from_points_mm
+    pts = np.array([[0.0, 0.0, 0.0], [1.0, 0.2, 0.0], [0.3, 1.5, -0.4]])
+    n = 2
+    V, F = create_initial_mesh_from_points_mm(pts, n_subdivisions=n, threshold_dist=0.9)
+    nv1, nf1 = 10 * 4 ** n + 2, 20 * 4 ** n
+    assert V.shape == (3 * nv1, 3) and V.dtype == np.float64
+    assert F.shape == (3 * nf1, 5) and F.dtype == np.int32
+    d = cdist(pts, pts)
+    radius = d[d != 0].min() * 0.9 / 2
+    for i in range(3):
+        vi = V[i * nv1:(i + 1) * nv1]
+        fi = F[i * nf1:(i + 1) * nf1]
+        assert np.allclose(np.linalg.norm(vi - pts[i], axis=1), radius, rtol=1e-12)
+        assert (fi[:, 3] == 0).all() and (fi[:, 4] == i + 1).all()
+        assert fi[:, :3].min() == i * nv1 and fi[:, :3].max() == (i + 1) * nv1 - 1
+        t = V[fi[:, :3]]
+        nrm = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+        assert (np.einsum("ij,ij->i", nrm, t.mean(axis=1) - pts[i]) > 0).all()
+    with pytest.raises(ValueError):
+        create_initial_mesh_from_points_mm(pts[:1])
