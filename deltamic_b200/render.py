@@ -159,6 +159,13 @@ def _heron(Verts, Faces):
     return pos, (hp * (hp - ls[:, 0]) * (hp - ls[:, 1]) * (hp - ls[:, 2])) ** 0.5
 
 
+def get_internal_triangle_and_mesh_areas_with_coeff(Verts, Faces, Faces_coeff):
+    """Heron areas times the face coefficients and their sum (render.py:21-33)."""
+    _, a = _heron(Verts, Faces)
+    trisar = Faces_coeff * a
+    return trisar, torch.sum(trisar)
+
+
 def get_internal_triangle_and_mesh_areas(Verts, Faces):
     """Heron areas of the faces and their sum (render.py:184-199)."""
     _, trisar = _heron(Verts, Faces)
