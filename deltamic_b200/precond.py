@@ -16,7 +16,6 @@ optimiser step is ``dm_vector_adam_step``.
 """
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 from . import _native as N
