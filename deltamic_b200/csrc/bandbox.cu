@@ -29,6 +29,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "band_internal.h"
 #include "dm_common.cuh"
@@ -958,13 +959,13 @@ void gemm(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X
 // Raises a kernel's dynamic shared-memory limit to kSmemLimit, once per device
 // (a host-side attribute, set on the first call, before any stream capture).
 template <typename Kern>
-cudaError_t smem_limit_once(Kern k, bool* done) {
+cudaError_t smem_limit_once(Kern k, std::atomic<bool>* done) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  if (dev >= 0 && dev < 64 && done[dev].load()) return cudaSuccess;
   e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit);
-  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true);
   return e;
 }
 
@@ -975,7 +976,7 @@ template <int C>
 cudaError_t zlines(const BBShape& s, const BBWs& w, float inv_n, float* image, cudaStream_t st) {
   const size_t smem = sizeof(float2) * ((size_t)s.ext[2] * 32 * C + 2 * (size_t)kLines * s.ext[2]);
   auto k = k_bb_zlines<C>;
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   cudaError_t e = smem_limit_once(k, done);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)line_ctas((s.nlines + kLines - 1) / kLines), s.ldw2 / (32 * C));
@@ -988,7 +989,7 @@ cudaError_t gradlines(const BBShape& s, const BBWs& w, int kind, const float* ta
                       float contrast, float* loss, cudaStream_t st) {
   const size_t smem = gradlines_smem(s.n[2], s.ldj);
   auto k = k_bb_gradlines<JC>;
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   cudaError_t e = smem_limit_once(k, done);
   if (e != cudaSuccess) return e;
   const unsigned nb = (unsigned)line_ctas((s.nlines + kLines - 1) / kLines);

@@ -460,16 +460,16 @@ __global__ void k_csr_sort(int64_t nv_total, const int32_t* __restrict__ off,
 // Host side: launch plans and launchers.
 
 int num_sms() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!cached[dev]) {
-    int v = 0;
+  int v = cached[dev].load();
+  if (v <= 0) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
       v = 148;
-    cached[dev] = v;
+    cached[dev].store(v);
   }
-  return cached[dev];
+  return v;
 }
 
 static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
