@@ -1,0 +1,49 @@
+"""The reference-named entry points on the host: CPU tensors are refused loudly
+(there is no CPU path), and the preconditioner matrix -- set-up linear algebra, as
+the reference's ``torch.inverse`` -- matches the oracle's operator."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import rel_l2
+from deltamic_b200.cuda_class import MeshFTCUDA
+from deltamic_b200.mesh import icosphere
+from deltamic_b200.optimize import VectorAdam, compute_precondition_matrix
+from deltamic_b200.render import compute_spatial_frequency_grid
+
+
+def test_meshftcuda_refuses_cpu_tensors():
+    v, f = icosphere(1, 0.3)
+    xi = compute_spatial_frequency_grid((8, 8, 8), [1.0, 1.0, 1.0])
+    otf = torch.ones(8, 8, 8)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        MeshFTCUDA.apply(torch.tensor(v, dtype=torch.float32), torch.tensor(f),
+                         torch.ones(len(f)), *xi, otf, 0.5)
+    with pytest.raises(TypeError):
+        MeshFTCUDA.apply(torch.tensor(v, dtype=torch.float16), torch.tensor(f),
+                         torch.ones(len(f)), *xi, otf, 0.5)
+
+
+def test_meshftcuda_rejects_axes_off_the_centred_grid():
+    v, f = icosphere(1, 0.3)
+    xi = list(compute_spatial_frequency_grid((8, 8, 8), [1.0, 1.0, 1.0]))
+    xi[1] = xi[1] ** 2  # not (2k - (n-1)) pi / L
+    with pytest.raises(ValueError, match="centred"):
+        MeshFTCUDA.apply(torch.tensor(v, dtype=torch.float32), torch.tensor(f),
+                         torch.ones(len(f)), *xi, torch.ones(8, 8, 8), 0.5)
+
+
+def test_vector_adam_refuses_cpu_parameters():
+    p = torch.nn.Parameter(torch.zeros(4, 3))
+    p.grad = torch.ones(4, 3)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        VectorAdam([p], lr=1e-2).step()
+
+
+def test_compute_precondition_matrix_matches_oracle():
+    v, f = icosphere(1, 0.3)
+    V = torch.tensor(v, dtype=torch.float64)
+    P = compute_precondition_matrix(V, torch.tensor(f), 5.0)
+    assert P.dtype == torch.float64
+    assert rel_l2(P.numpy(), oracle.fit.precondition_matrix(f, len(v), 5.0)) < 1e-12
