@@ -126,3 +126,25 @@ def test_conv_host_checks(lib):
     assert lib.dm_conv3d_s2_backward(p, 2, 16, 16, 16, 16, p, 32, p, p, None, p, p, p, ws - 1,
                                      None) == N.DM_ERR_WORKSPACE
     assert lib.dm_conv3d_s2_device_error(None, None) == N.DM_ERR_INVALID_ARG
+
+
+def test_header_and_library_from_plain_c(lib, tmp_path):
+    """A C99 program (tests/abi_host_check.c) compiles against the public header
+    with -Wall -Wextra -pedantic -Werror, links the shared library and runs its
+    host-side calls: the boundary is usable from C, not only through ctypes."""
+    import shutil
+    import subprocess
+    from deltamic_b200 import _native
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    libdir = os.path.dirname(_native.LIB_PATH)
+    exe = str(tmp_path / "abi_host_check")
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "abi_host_check.c"),
+                    "-L", libdir, "-ldeltamic_b200", f"-Wl,-rpath,{libdir}", "-o", exe],
+                   check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "ok"
