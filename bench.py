@@ -83,8 +83,12 @@ def parse():
                                            "volume200", "psf200", "masks64", "conv64"],
                    default="fit200",
                    help="fit200: the 200^3 single-mesh fit step (default); batch64: 64 "
-                        "cells of mixed sizes per step; volume200: forward + adjoint of "
-                        "the autofluorescence transform on the fit200 mesh and band")
+                        "cells of mixed sizes per step; fit300: 300-step fits (plain and "
+                        "preconditioned); learned: learned initialiser vs sphere start; "
+                        "volume200: forward + adjoint of the autofluorescence transform on "
+                        "the fit200 mesh and band; psf200: the spatial PSF models at 200^3; "
+                        "masks64: membrane and label masks; conv64: the encoder's "
+                        "convolution training step")
     return p.parse_args()
 
 
