@@ -15,8 +15,11 @@ roofline figures count the evaluated pairs.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0).  ``--impl reference`` times the reference
-algorithm's CPU path (the float64 numpy restatement in oracle/) on this host.
+Prints one JSON line (rank 0).  ``--impl reference`` times the reference's own CPU
+path on this host: ``deltamic.render.MeshFTPy`` (float32, torch autograd for the
+vertex gradient, all host threads) from the unmodified install in baseline/_ref
+(baseline/install_reference.py), on a sample of the band per step; without that
+install, the float64 numpy restatement in oracle/ (labelled kind "port").
 """
 from __future__ import annotations
 
@@ -44,8 +47,8 @@ LR = 1e-3
 FWD_FP32, FWD_MUFU = 32, 7
 BWD_FP32, BWD_MUFU = 80, 9
 # DRAM bytes (read + write) per launch of the adjoint kernel in this workload, from
-# one ncu capture of the fit step (dram__bytes_read.sum + dram__bytes_write.sum,
-# profiles/k_meshft_fit200.md): the kernel streams face records and frequency
+# one ncu capture of the fit step (dram__bytes_read.sum + dram__bytes_write.sum):
+# the kernel streams face records and frequency
 # tiles, far below its compute time at HBM speed.
 NCU_TRAFFIC_BWD = 3061248 + 577024
 # Surface + enclosed-volume transform (render.py:228-318): the complex weight
@@ -120,21 +123,47 @@ def make_workload(rank, small=False):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples every 200 ms while running."""
+    """SM clocks and clock-event reasons while running: NVML polled every 2 ms (a
+    timed region of a few tens of ms still gets a dozen samples) plus the
+    nvidia-smi line every 200 ms.  Both only read the GPU's state."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, pci_bus_id=None):
         self.gpu = gpu_index
+        self.pci = pci_bus_id
         self.proc = None
         self.lines = []
+        self.nvml = []          # (sm MHz, max MHz, reason bits)
+        self._stop = threading.Event()
+        self._nv_thread = None
+
+    def _nvml_loop(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            try:
+                h = (nv.nvmlDeviceGetHandleByPciBusId_v2(self.pci) if self.pci
+                     else nv.nvmlDeviceGetHandleByIndex(self.gpu))
+                smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                while not self._stop.is_set():
+                    self.nvml.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
+                                      nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    time.sleep(0.002)
+            finally:
+                nv.nvmlShutdown()
+        except Exception:  # no NVML: the nvidia-smi samples remain
+            pass
 
     def start(self):
+        self._nv_thread = threading.Thread(target=self._nvml_loop, daemon=True)
+        self._nv_thread.start()
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", f"--id={self.pci or self.gpu}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -147,16 +176,18 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.t.join(timeout=2)
+        self._stop.set()
+        if self._nv_thread is not None:
+            self._nv_thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+        n_smi = 0
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
@@ -166,35 +197,106 @@ class ClockSampler:
                 smax.append(float(parts[2]))
             except ValueError:
                 continue
-            for nm, val in zip(names, parts[5:9]):
+            n_smi += 1
+            for nm, val in zip(self.NAMES, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": float(max(smax)) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        bits = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+                "sw_power_cap": 0x4}
+        for mhz, mx, r in self.nvml:
+            sm.append(float(mhz))
+            smax.append(float(mx))
+            for nm, b in bits.items():
+                if r & b:
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm), "nvml_samples": len(self.nvml),
+                "smi_samples": n_smi}
 
 
-def cpu_baseline(gt_v, faces, box, band_xi, sample_xi=6144, threads=None):
-    """Oracle (reference algorithm restated in numpy) forward+adjoint on a sample
-    (6,144 band frequencies x all faces: about 10 s on 16 host threads), in chunks
-    of at most 2^19 pairs per task."""
+def pci_bus_id(dev):
+    """PCI bus id of a torch CUDA device in NVML's form, or None."""
+    import torch
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        return None
+
+
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def reference_meshftpy():
+    """The reference's own CPU meshFT, ``deltamic.render.MeshFTPy``
+    (render.py:36-109), from the unmodified install under baseline/_ref
+    (baseline/install_reference.py), or None when it is not installed."""
+    if not os.path.isdir(os.path.join(REF_DIR, "deltamic")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.append(REF_DIR)
+    try:
+        from deltamic.render import MeshFTPy
+    except Exception:
+        return None
+    return MeshFTPy
+
+
+def ref_sample_seconds(meshftpy, verts_shift, faces, axes, shape, idx, threads):
+    """Seconds of one reference CPU forward + vertex backward (torch autograd
+    through MeshFTPy, float32, ``threads`` torch threads) on the band frequencies
+    ``idx``: the OTF argument is 1 on those voxels and 0 elsewhere with threshold
+    0.5, so MeshFTPy evaluates exactly them (the xi-chunking of the full band by
+    masking the OTF; the chunks' spectra add up to the full one)."""
+    import torch
+    torch.set_num_threads(threads)
+    xi = [torch.tensor(a, dtype=torch.float32) for a in axes]
+    mask = torch.zeros(tuple(shape))
+    mask.view(-1)[torch.as_tensor(np.asarray(idx, np.int64))] = 1.0
+    V = torch.tensor(verts_shift, dtype=torch.float32, requires_grad=True)
+    F = torch.as_tensor(np.asarray(faces, np.int64))
+    C = torch.ones(len(faces))
+    t0 = time.perf_counter()
+    ft = meshftpy(V, F, C, *xi, mask, 0.5)
+    ft.backward(torch.ones_like(ft))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(gt_v, faces, box, shape, band_idx, sample_xi=2048, chunk=512, threads=None):
+    """The reference's CPU path (MeshFTPy, float32, all host threads) forward +
+    vertex backward on a sample of the band (``sample_xi`` frequencies in chunks of
+    ``chunk``: about 10-20 s), on the same vertices as the GPU step.  Without the
+    reference install, the float64 numpy restatement in oracle/ (kind "port")."""
     import oracle
     threads = threads or os.cpu_count() or 1
     rng = np.random.default_rng(0)
-    sub = np.sort(rng.choice(len(band_xi), min(sample_xi, len(band_xi)), replace=False))
-    xi = band_xi[sub]
+    idx = np.sort(rng.choice(np.asarray(band_idx), min(sample_xi, len(band_idx)), replace=False))
+    axes = oracle.frequency_axes(box, shape)
+    meshftpy = reference_meshftpy()
+    if meshftpy is not None:
+        dt = sum(ref_sample_seconds(meshftpy, gt_v - box[:, 0], faces, axes, shape,
+                                    idx[k:k + chunk], threads)
+                 for k in range(0, len(idx), chunk))
+        pairs = len(idx) * len(faces)
+        return {"value": pairs / dt, "unit": "pairs/s", "cores": threads, "kind": "reference",
+                "sample": f"{len(idx)} band frequencies x {len(faces)} faces in chunks of "
+                          f"{chunk}, forward + vertex backward of the reference's MeshFTPy "
+                          f"(float32, torch autograd, {dt:.1f} s)"}
+    xi = oracle.xi_list_from_band(idx, axes)
     vs = gt_v - box[:, 0]
     coeff = np.ones(len(faces))
     g = np.ones(len(xi), np.complex128)
-    chunk = max(len(faces), min(len(xi) * len(faces) // (4 * threads), 1 << 19))
+    ck = max(len(faces), min(len(xi) * len(faces) // (4 * threads), 1 << 19))
     t0 = time.perf_counter()
-    ft = oracle.meshft_forward(vs, faces, coeff, xi, threads=threads, chunk_pairs=chunk)
-    oracle.meshft_backward(vs, faces, coeff, xi, g, ft, threads=threads, chunk_pairs=chunk)
+    ft = oracle.meshft_forward(vs, faces, coeff, xi, threads=threads, chunk_pairs=ck)
+    oracle.meshft_backward(vs, faces, coeff, xi, g, ft, threads=threads, chunk_pairs=ck)
     dt = time.perf_counter() - t0
     pairs = len(xi) * len(faces)
     return {"value": pairs / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
             "sample": f"{len(xi)} band frequencies x {len(faces)} faces, forward+adjoint, "
-                      f"float64 numpy ({dt:.1f} s)"}
+                      f"float64 numpy restatement ({dt:.1f} s; reference not installed)"}
 
 
 def volume_cpu_baseline(gt_v, faces, band_xi, sample_xi=6144, threads=None, regint=0.5):
@@ -227,31 +329,49 @@ def run_reference(args, rank, world):
     if args.workload in ("psf200", "masks64"):
         return run_reference_host(args)
     gt_v, init_v, faces, box = make_workload(0, args.small)
-    axes = oracle.frequency_axes(box, SHAPE)
+    shape = (64, 64, 64) if args.small else SHAPE
+    axes = oracle.frequency_axes(box, shape)
     otf = oracle.gaussian_otf(np.diag(SIGMA), *axes)
     idx = oracle.band_indices(otf, THRESH)
-    band_xi = oracle.xi_list_from_band(idx, axes)
     threads = os.cpu_count() or 1
-    per_step = 512  # band frequencies per step: chunks large enough for the thread pool
-    vals = []
+    per_step = 384  # band frequencies per step: a bounded sample of the step's work
+    meshftpy = reference_meshftpy()
+    secs = []
     for k in range(args.warmup + args.steps):
-        r = cpu_baseline(gt_v, faces, box, band_xi[k * per_step % len(band_xi):], per_step,
-                         threads)
+        o = k * per_step % len(idx)
+        sub = np.concatenate([idx[o:], idx[:o]])[:per_step]
+        if meshftpy is not None:
+            dt = ref_sample_seconds(meshftpy, gt_v - box[:, 0], faces, axes, shape, sub, threads)
+        else:
+            r = cpu_baseline(gt_v, faces, box, shape, sub, len(sub), len(sub), threads)
+            dt = len(sub) * len(faces) / r["value"]
         if k >= args.warmup:
-            vals.append(r["value"])
-    value = float(np.mean(vals))
+            secs.append(dt)
+    sample_pairs = per_step * len(faces)
+    value = sample_pairs / float(np.mean(secs))
     full_pairs = len(idx) * len(faces)
+    kind = "reference" if meshftpy is not None else "port"
+    what = ("the reference's MeshFTPy (render.py:36-109, float32) forward + vertex backward "
+            "by torch autograd" if meshftpy is not None else
+            "the float64 numpy restatement in oracle/ (reference not installed)")
+    sample = (f"{per_step} band frequencies x {len(faces)} faces per step "
+              f"({sample_pairs} pairs), {what}, {threads} torch threads")
     out = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": full_pairs / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "ms_per_step": float(np.mean(secs)) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if meshftpy is not None else "f64", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": "fit200: level-5 SH mesh, 200^3, OTF>1e-5 band",
+                   "mesh_state": "the ground-truth SH shape (the GPU arm's timed state)",
                    "n_faces": int(len(faces)), "n_band": int(len(idx)),
-                   "pairs_per_step": int(full_pairs), "parallelism": "replicas only"},
-        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
-                         "sample": f"{per_step} band frequencies x {len(faces)} faces per step"},
+                   "pairs_per_sample_step": int(sample_pairs),
+                   "pairs_per_full_step": int(full_pairs), "parallelism": "replicas only"},
+        "extrapolated": {"full_step_ms": full_pairs / value * 1e3,
+                         "note": "a full-band step's time at the sampled rate (not measured)"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -508,7 +628,7 @@ def run_volume(args, rank, world, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, pci_bus_id(dev))
     clocks.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -642,11 +762,15 @@ def setup_fit200(args, rank, dev):
     gen = torch.Generator(device=dev).manual_seed(99 + rank)
     img = r.render(torch.tensor(gt_v, dtype=torch.float32, device=dev), F, C)
     target = noisy_target(img, gen, img.numel(), dev)
-    V = torch.tensor(init_v, dtype=torch.float32, device=dev)
+    # every timed step works on one mesh state, the ground-truth shape the fit
+    # converges to (restored before each step), so the step time does not depend
+    # on how many steps are timed; the reference arm and the CPU baseline
+    # evaluate the same vertices
+    V = torch.tensor(gt_v, dtype=torch.float32, device=dev)
     pairs = len(faces_np) * r.n_band
 
     def make_step(graph):
-        return FitStep(r, V.clone(), F, C, target, "mse", 0.0, LR, graph=graph)
+        return FitStep(r, V.clone(), F, C, target, "mse", 0.0, LR, graph=graph, restore=V)
 
     def e2e_call(Vd):
         loss = r.loss(Vd, F, C, "mse", target)
@@ -654,13 +778,15 @@ def setup_fit200(args, rank, dev):
         return loss
 
     info = {"workload": ("fit64-small: level-5 meshes at 64^3" if args.small else
-                         "fit200: Adam step fitting a level-5 sphere to a level-5 SH shape, "
-                         "200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5"),
+                         "fit200: Adam step of the fit of a level-5 mesh to a level-5 SH "
+                         "shape's noisy render, 200^3, sigma diag(1e-3,1e-3,4e-3), OTF>1e-5"),
             "n_verts": int(len(init_v)), "n_faces": int(len(faces_np)),
             "n_band": int(r.n_band), "box_shape": list(shape),
-            "eval_pairs_per_step": int(len(faces_np) * r.n_eval)}
+            "eval_pairs_per_step": int(len(faces_np) * r.n_eval),
+            "mesh_state": "the ground-truth SH shape, restored before every step (same "
+                          "vertices in the step, e2e, the CPU baseline and the reference arm)"}
     cpu = dict(gt_v=gt_v, faces=faces_np, box=box, shape=shape, band=r.band)
-    return make_step, e2e_call, init_v, pairs, info, cpu
+    return make_step, e2e_call, gt_v, pairs, info, cpu
 
 
 def setup_batch64(args, rank, dev):
@@ -876,7 +1002,7 @@ def run_conv(args, rank, world, local):
     c0 = lib.dm_launch_count()
     step()
     launches = int(lib.dm_launch_count() - c0)
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, pci_bus_id(dev))
     clocks.start()
     time.sleep(0.3)
     ms = max_over_ranks(_event_ms(step, args.steps, 1), dev)
@@ -974,7 +1100,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, pci_bus_id(dev))
     clocks.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1048,9 +1174,8 @@ def run_ours(args, rank, world, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline and cpu_case is not None:
-        axes = oracle.frequency_axes(cpu_case["box"], cpu_case["shape"])
-        band_xi = oracle.xi_list_from_band(cpu_case["band"].cpu().numpy().astype(np.int64), axes)
-        cpu = cpu_baseline(cpu_case["gt_v"], cpu_case["faces"], cpu_case["box"], band_xi)
+        cpu = cpu_baseline(cpu_case["gt_v"], cpu_case["faces"], cpu_case["box"],
+                           cpu_case["shape"], cpu_case["band"].cpu().numpy().astype(np.int64))
 
     if rank != 0:
         return

@@ -73,6 +73,7 @@ SIGNATURES = {
                                  _P]),
     "dm_meshft_forward_noalloc": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P,
                                          _P]),
+    "dm_meshft_forward_noalloc_device_error": (_INT, [ctypes.POINTER(_INT), _P]),
     "dm_meshft_volume_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_volume_forward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P,
                                         _P, _P, _SZ, _P]),

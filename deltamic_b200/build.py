@@ -58,14 +58,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(LIBDIR, "_obj")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj])
         objs.append(obj)
+    if verbose:
+        for cmd in cmds:
+            print(" ".join(cmd))
+    # one nvcc per source file, several at once
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=not verbose), cmds)):
+            if r.returncode != 0:
+                if r.stderr:
+                    sys.stderr.write(r.stderr.decode(errors="replace"))
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = lib_path() + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:

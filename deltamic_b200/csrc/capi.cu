@@ -13,6 +13,26 @@
 
 using namespace dm;
 
+namespace dm {
+
+bool box_ok(const dm_box* b) {
+  if (!b) return false;
+  if (b->band_flags & ~DM_BAND_HERMITIAN) return false;
+  for (int d = 0; d < 3; ++d) {
+    if (b->shape[d] <= 0) return false;
+    if (!(b->hi[d] > b->lo[d])) return false;
+  }
+  const int64_t n = (int64_t)b->shape[0] * b->shape[1] * b->shape[2];
+  return n <= (int64_t)INT32_MAX;
+}
+
+bool sizes_ok(int64_t nv, int64_t nt, int64_t nband) {
+  return nv >= 0 && nt >= 0 && nband >= 0 && nv < (int64_t)INT32_MAX / 3 &&
+         nt < (int64_t)INT32_MAX / 9 && nband < (int64_t)INT32_MAX;
+}
+
+}  // namespace dm
+
 namespace {
 
 constexpr size_t kAlign = 256;
@@ -30,17 +50,6 @@ struct Carve {
     return p;
   }
 };
-
-bool box_ok(const dm_box* b) {
-  if (!b) return false;
-  if (b->band_flags & ~DM_BAND_HERMITIAN) return false;
-  for (int d = 0; d < 3; ++d) {
-    if (b->shape[d] <= 0) return false;
-    if (!(b->hi[d] > b->lo[d])) return false;
-  }
-  const int64_t n = (int64_t)b->shape[0] * b->shape[1] * b->shape[2];
-  return n <= (int64_t)INT32_MAX;
-}
 
 CellDesc single_cell(const dm_box* b, int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
   CellDesc d;
@@ -83,11 +92,6 @@ Cells one_cell(const CellDesc& d) {
   c.n = 1;
   c.one = d;
   return c;
-}
-
-bool sizes_ok(int64_t nv, int64_t nt, int64_t nband) {
-  return nv >= 0 && nt >= 0 && nband >= 0 && nv < (int64_t)INT32_MAX / 3 &&
-         nt < (int64_t)INT32_MAX / 9 && nband < (int64_t)INT32_MAX;
 }
 
 // Forward workspace layout.

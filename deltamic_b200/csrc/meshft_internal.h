@@ -35,6 +35,12 @@ struct PlanTotals {
 
 int num_sms();
 
+// Host-side argument checks shared by the C-ABI entry points (capi.cu): a box
+// with positive extents and shapes of at most INT32_MAX voxels and only known
+// band flags; mesh and band sizes the kernels can index in int32.
+bool box_ok(const dm_box* b);
+bool sizes_ok(int64_t nv, int64_t nt, int64_t nband);
+
 // Instrumentation: launches counted per process; optional CUDA events around the
 // main forward / backward kernels (kind 0 / 1).
 void count_launches(int n);

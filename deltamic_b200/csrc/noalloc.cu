@@ -20,13 +20,17 @@
 //  * every call on a device shares the one array and it keeps the previous
 //    call's contents: the status word at its start is cleared by each call, all
 //    other scratch is fully rewritten before it is read; two calls whose work
-//    overlaps on the GPU (different streams without ordering) race on it.
+//    overlaps on the GPU (different streams without ordering) race on it;
+//  * faults the kernels detect (a face index out of range) set bits in that
+//    status word; dm_meshft_forward_noalloc_device_error reads and clears it.
+//    Every host-side argument check runs before anything is enqueued.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <atomic>
 
 #include "../../include/deltamic_b200.h"
+#include "meshft_internal.h"
 
 namespace {
 
@@ -62,6 +66,11 @@ extern "C" int dm_meshft_forward_noalloc(const float* verts, int64_t nv, const i
   const size_t need = dm_meshft_forward_workspace_size(nv, nt, n_band);
   if (need == 0) return DM_ERR_SIZE;              // sizes the kernels cannot index
   if (need > kNoAllocScratchBytes) return DM_ERR_SIZE;  // beyond the fixed scratch
+  // the argument checks of dm_meshft_forward, repeated here so that a refused
+  // call enqueues nothing (not even the status-word clear below)
+  if (!dm::box_ok(box)) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (n_band > 0 && (!band_index || !ft_list)) return DM_ERR_INVALID_ARG;
   void* scratch = nullptr;
   const int s = scratch_for_current_device(&scratch);
   if (s != DM_OK) return s;
@@ -69,4 +78,13 @@ extern "C" int dm_meshft_forward_noalloc(const float* verts, int64_t nv, const i
   if (cudaMemsetAsync(scratch, 0, 256, (cudaStream_t)stream) != cudaSuccess) return DM_ERR_CUDA;
   return dm_meshft_forward(verts, nv, faces, nt, faces_coeff, box, band_index, n_band, otf,
                            ft_list, grid, scratch, kNoAllocScratchBytes, stream);
+}
+
+extern "C" int dm_meshft_forward_noalloc_device_error(int* out_flags, dm_stream_t stream) {
+  if (!out_flags) return DM_ERR_INVALID_ARG;
+  void* scratch = nullptr;
+  const int s = scratch_for_current_device(&scratch);
+  if (s != DM_OK) return s;
+  // the status word is the first int of the scratch (the forward's workspace layout)
+  return dm_device_error(scratch, out_flags, stream);
 }

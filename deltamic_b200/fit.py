@@ -21,12 +21,20 @@ class FitStep:
     ``verts`` is updated in place (it is the optimised parameter).  The loss of the
     step (evaluated before the update, like ``loss.backward(); opt.step()``) is
     left in ``self.loss`` on the device.
+
+    ``restore`` (optional, [nv, 3] float32 on the device): copied into ``verts`` at
+    the start of every step, so every step renders the same mesh and does the same
+    work (a step timed at one mesh state; the update is still computed and applied).
     """
 
     def __init__(self, renderer: MeshRenderer, verts, faces, coeff, target=None, kind="mse",
                  contrast=0.0, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True,
-                 precond=None, optimizer="adam"):
+                 precond=None, optimizer="adam", restore=None):
         ops._check_mesh(verts, faces, coeff)
+        if restore is not None and (restore.shape != verts.shape or restore.dtype != verts.dtype
+                                    or restore.device != verts.device):
+            raise ValueError("restore must match verts in shape, dtype and device")
+        self.restore = restore
         if renderer.band is None:
             raise RuntimeError("set the renderer's OTF first")
         self.r = renderer
@@ -56,6 +64,8 @@ class FitStep:
 
     def _body(self):
         r = self.r
+        if self.restore is not None:
+            self.V.copy_(self.restore)
         if r.use_bandbox:
             ft = ops.meshft_list(self.V, self.F, self.C, r.grid, r.band)
             loss, G = r.render_loss(ft, self.kind, self.target, self.contrast)

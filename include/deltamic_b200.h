@@ -126,6 +126,14 @@ int dm_meshft_forward_noalloc(const float* verts, int64_t nv, const int64_t* fac
                               const int32_t* band_index, int64_t n_band, const float* otf,
                               float* ft_list, float* grid, dm_stream_t stream);
 
+/* Synchronous: the device status word of dm_meshft_forward_noalloc on the current
+ * device (DM_ERR_* bits set by its kernels, e.g. DM_ERR_BAD_INDEX for a face
+ * index out of range), then cleared; the counterpart of dm_device_error for the
+ * library's fixed scratch, whose address callers never see.  Each
+ * dm_meshft_forward_noalloc call clears the word before its kernels run, so read
+ * it after the call whose faults are wanted and before the next one. */
+int dm_meshft_forward_noalloc_device_error(int* out_flags, dm_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * meshFT backward.  Replaces backward_fourier3d_cpp
  * (deltamic/cpp/fourier3d_cuda.cpp:44-65, :114; kernels .cu:314-416, host prep

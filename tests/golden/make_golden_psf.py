@@ -1,10 +1,10 @@
 """Generate golden vectors for the spatial PSF models by running the reference's
 own modules (``deltamic/psf.py``) on the CPU.
 
-Run once in a container that has the reference source checked out (read-only) at
-``$DELTAMIC_REF`` (default ``/root/reference``):
+Run once in a container that has the reference source checked out (read-only),
+with ``$DELTAMIC_REF`` naming its root directory:
 
-    python tests/golden/make_golden_psf.py
+    DELTAMIC_REF=<reference checkout> python tests/golden/make_golden_psf.py
 
 Cases: ``Gaussian_psf_logsigma`` (psf.py:590-626), ``Anisotropic_gaussian_psf``
 (psf.py:628-665), ``Gibson_Lanni_psf`` (psf.py:23-154, two parameter sets),
@@ -23,10 +23,12 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("DELTAMIC_REF", "/root/reference")
+REF = os.environ.get("DELTAMIC_REF", "")
 
 
 def _import_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "deltamic")):
+        raise SystemExit("set $DELTAMIC_REF to the root of a deltaMic checkout")
     sys.path.insert(0, REF)
     import deltamic.psf as psf  # noqa: E402
     return psf

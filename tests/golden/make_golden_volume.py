@@ -1,10 +1,10 @@
 """Generate golden vectors for the autofluorescence (surface + enclosed volume)
 transform by running the reference's own function.
 
-Run once in a container that has the reference source checked out (read-only) at
-``$DELTAMIC_REF`` (default ``/root/reference``):
+Run once in a container that has the reference source checked out (read-only),
+with ``$DELTAMIC_REF`` naming its root directory:
 
-    python tests/golden/make_golden_volume.py
+    DELTAMIC_REF=<reference checkout> python tests/golden/make_golden_volume.py
 
 For every case it builds a small closed mesh and runs the reference's
 ``fourier_from_mesh_narrowband_autofluorescence`` (``deltamic/render.py:228-318``)
@@ -30,10 +30,12 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from deltamic_b200.mesh import icosphere, jitter, sh_perturb  # noqa: E402
 
-REF = os.environ.get("DELTAMIC_REF", "/root/reference")
+REF = os.environ.get("DELTAMIC_REF", "")
 
 
 def _import_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "deltamic")):
+        raise SystemExit("set $DELTAMIC_REF to the root of a deltaMic checkout")
     sys.path.insert(0, REF)
     import deltamic.psf as psf  # noqa: E402
     import deltamic.render as render  # noqa: E402

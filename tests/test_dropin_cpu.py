@@ -47,3 +47,30 @@ def test_compute_precondition_matrix_matches_oracle():
     P = compute_precondition_matrix(V, torch.tensor(f), 5.0)
     assert P.dtype == torch.float64
     assert rel_l2(P.numpy(), oracle.fit.precondition_matrix(f, len(v), 5.0)) < 1e-12
+
+
+def test_vector_adam_adopts_a_reference_layout_state():
+    """A state saved by the reference VectorAdam (optimize.py:225-257: ``step`` a
+    Python int, ``g2`` the per-vertex moment repeated over [nv, 3]) loads into this
+    optimiser and is brought into its layout; a state of another shape raises."""
+    from deltamic_b200.optimize import _adopt_state
+    p = torch.nn.Parameter(torch.zeros(5, 3))
+    opt = VectorAdam([p], lr=1e-2)
+    g1 = torch.arange(15, dtype=torch.float32).reshape(5, 3)
+    g2v = torch.arange(5, dtype=torch.float32) + 0.5
+    ref_state = {"state": {0: {"step": 7, "g1": g1.clone(),
+                               "g2": g2v[:, None].repeat_interleave(3, dim=1)}},
+                 "param_groups": [dict(opt.param_groups[0], params=[0])]}
+    opt.load_state_dict(ref_state)
+    st = opt.state[p]
+    _adopt_state(st, p, vector=True)
+    assert st["step"].dtype == torch.int64 and st["step"].tolist() == [7]
+    assert torch.equal(st["g1"], g1)
+    assert st["g2"].shape == (5,) and torch.equal(st["g2"], g2v)
+    _adopt_state(st, p, vector=True)  # already in this layout: unchanged
+    assert torch.equal(st["g2"], g2v) and st["step"].tolist() == [7]
+    bad = {"step": 1, "g1": g1.clone(), "g2": torch.zeros(4)}
+    with pytest.raises(ValueError, match="g2"):
+        _adopt_state(bad, p, vector=True)
+    with pytest.raises(ValueError, match="keys"):
+        _adopt_state({"step": 1}, p, vector=True)

@@ -9,7 +9,8 @@ from deltamic_b200.mesh import icosphere
 from deltamic_b200.mesh_io import (combine_all_verts_faces, combine_all_verts_faces_mm, read_obj,
                                    read_rec, write_obj, write_rec)
 
-REF_DATA = "/root/reference/data/mesh"
+# mesh files shipped with the reference (data/mesh), when $DELTAMIC_REF names a checkout
+REF_DATA = os.path.join(os.environ.get("DELTAMIC_REF", ""), "data", "mesh")
 
 
 def test_obj_round_trip_and_face_forms(tmp_path):
@@ -42,7 +43,7 @@ def test_rec_round_trip(tmp_path):
     assert np.array_equal(Fc[len(f1):], f2 + len(v1))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference data not present")
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="$DELTAMIC_REF not set to a reference checkout")
 def test_reference_data_files_read():
     for name, nv, nt in (("cow.obj", 2930, 5856), ("fish.obj", 7106, 14208)):
         v, f = read_obj(os.path.join(REF_DATA, name))
