@@ -23,6 +23,7 @@ DM_ERR_WORKSPACE = 8
 DM_ERR_CUDA = 16
 DM_ERR_TIMEOUT = 32
 DM_ERR_UNSUPPORTED = 64
+DM_ERR_NONFINITE = 128
 
 ABI_VERSION = 2
 
@@ -65,6 +66,7 @@ SIGNATURES = {
     "dm_device_error": (_INT, [_P, ctypes.POINTER(_INT), _P]),
     "dm_narrowband_workspace_size": (_SZ, [_I64]),
     "dm_narrowband_compact": (_INT, [_P, _I64, _F, _P, _P, _P, _SZ, _P]),
+    "dm_narrowband_compact64": (_INT, [_P, _I64, ctypes.c_double, _P, _P, _P, _SZ, _P]),
     "dm_narrowband_hermitian": (_INT, [_P, _I64, _I64, _P, _P]),
     "dm_topology_size": (_SZ, [_I64, _I64]),
     "dm_topology_build": (_INT, [_P, _I64, _I64, _P, _SZ, _P]),
@@ -74,6 +76,17 @@ SIGNATURES = {
     "dm_meshft_forward_noalloc": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P,
                                          _P]),
     "dm_meshft_forward_noalloc_device_error": (_INT, [ctypes.POINTER(_INT), _P]),
+    "dm_meshft_forward_xi_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft_forward_xi": (_INT, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _SZ, _P]),
+    "dm_meshft_backward_xi_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft_backward_xi": (_INT, [_P, _I64, _P, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, _P,
+                                     _SZ, _P]),
+    "dm_meshft64_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft64_forward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _P, _I64, _P, _P, _P, _P,
+                                   _SZ, _P]),
+    "dm_meshft64_backward_workspace_size": (_SZ, [_I64, _I64, _I64]),
+    "dm_meshft64_backward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _P, _I64, _P, _P, _P,
+                                    ctypes.c_double, _P, _P, _P, _P, _P, _SZ, _P]),
     "dm_meshft_volume_forward_workspace_size": (_SZ, [_I64, _I64, _I64]),
     "dm_meshft_volume_forward": (_INT, [_P, _I64, _P, _I64, _P, _BOXP, _P, _I64, _P, _P, _P,
                                         _P, _P, _SZ, _P]),
@@ -115,6 +128,10 @@ SIGNATURES = {
     "dm_batched_image_loss": (_INT, [_BATCHP, _P, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     "dm_gaussian_otf": (_INT, [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
                                _P, _P]),
+    "dm_gaussian_otf64": (_INT, [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
+                                 _P, _P]),
+    "dm_gaussian_otf64_sigma_grad": (_INT, [_P, _P, _I64, _P, _P, ctypes.c_int32, _P,
+                                            ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),
     "dm_gaussian_otf_grad_workspace_size": (_SZ, [_I64]),
     "dm_gaussian_otf_sigma_grad": (_INT, [_P, _P, _I64, _P, _P, ctypes.c_int32, _P,
                                           ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),

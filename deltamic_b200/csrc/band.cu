@@ -18,8 +18,9 @@ constexpr int kBandThreads = 256;
 constexpr int kBandPerThread = 16;
 constexpr int kBandTile = kBandThreads * kBandPerThread;  // voxels per block
 
-// Per-block count of otf > thresh over contiguous tiles.
-__global__ void k_band_count(const float* __restrict__ otf, int64_t n, float thresh,
+// Per-block count of otf > thresh over contiguous tiles (float or double OTF).
+template <typename T>
+__global__ void k_band_count(const T* __restrict__ otf, int64_t n, T thresh,
                              int32_t* __restrict__ blk_count) {
   __shared__ int32_t sh[kBandThreads / 32];
   const int64_t base = (int64_t)blockIdx.x * kBandTile;
@@ -67,7 +68,8 @@ __global__ void k_band_scan(const int32_t* __restrict__ blk_count, int32_t* __re
 
 // Write the indices in ascending order: within a block, tile k of the block is
 // handled in order and each warp-level ballot gives the rank inside the tile.
-__global__ void k_band_write(const float* __restrict__ otf, int64_t n, float thresh,
+template <typename T>
+__global__ void k_band_write(const T* __restrict__ otf, int64_t n, T thresh,
                              const int32_t* __restrict__ blk_off, int32_t* __restrict__ out) {
   __shared__ int32_t wsum[kBandThreads / 32];
   __shared__ int32_t run;
@@ -96,16 +98,28 @@ __global__ void k_band_write(const float* __restrict__ otf, int64_t n, float thr
 
 int64_t band_blocks(int64_t n) { return (n + kBandTile - 1) / kBandTile; }
 
-int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, int64_t* count,
-                      int32_t* blk_count, int32_t* blk_off, cudaStream_t st) {
+template <typename T>
+static int launch_narrowband_t(const T* otf, int64_t n, T thresh, int32_t* out, int64_t* count,
+                               int32_t* blk_count, int32_t* blk_off, cudaStream_t st) {
   const int64_t nb = band_blocks(n);
   if (nb > 0) {
-    k_band_count<<<(unsigned)nb, kBandThreads, 0, st>>>(otf, n, thresh, blk_count);
+    k_band_count<T><<<(unsigned)nb, kBandThreads, 0, st>>>(otf, n, thresh, blk_count);
   }
   k_band_scan<<<1, 1024, 0, st>>>(blk_count, blk_off, nb, count);
-  if (nb > 0) k_band_write<<<(unsigned)nb, kBandThreads, 0, st>>>(otf, n, thresh, blk_off, out);
+  if (nb > 0)
+    k_band_write<T><<<(unsigned)nb, kBandThreads, 0, st>>>(otf, n, thresh, blk_off, out);
   count_launches(1 + (nb > 0 ? 2 : 0));
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, int64_t* count,
+                      int32_t* blk_count, int32_t* blk_off, cudaStream_t st) {
+  return launch_narrowband_t<float>(otf, n, thresh, out, count, blk_count, blk_off, st);
+}
+
+int launch_narrowband64(const double* otf, int64_t n, double thresh, int32_t* out,
+                        int64_t* count, int32_t* blk_count, int32_t* blk_off, cudaStream_t st) {
+  return launch_narrowband_t<double>(otf, n, thresh, out, count, blk_count, blk_off, st);
 }
 
 // Mirror test of a band (DM_BAND_HERMITIAN): one block, fixed result.
@@ -130,12 +144,14 @@ int launch_band_mirror(const int32_t* band, int64_t nb, int64_t nvox, int32_t* f
 // outer grid of three frequency axes, with the float32 operation order of the
 // reference expression (no contraction into FMAs).
 
-struct Axes {
-  const float* x[3];
+template <typename T>
+struct AxesT {
+  const T* x[3];
   int32_t n[3];
 };
 
-__device__ __forceinline__ void grid_xi(int64_t i, const Axes& a, float x[3]) {
+template <typename T>
+__device__ __forceinline__ void grid_xi(int64_t i, const AxesT<T>& a, T x[3]) {
   const int64_t n12 = (int64_t)a.n[1] * a.n[2];
   const int32_t k0 = (int32_t)(i / n12);
   const int64_t rem = i - (int64_t)k0 * n12;
@@ -146,35 +162,46 @@ __device__ __forceinline__ void grid_xi(int64_t i, const Axes& a, float x[3]) {
   x[2] = a.x[2][k2];
 }
 
-__device__ __forceinline__ float quad_form(const float S[9], const float x[3]) {
-  float q = 0.f;
+// Rounded products and sums in the reference expression's order (no FMA).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float expT(float x) { return expf(x); }
+__device__ __forceinline__ double expT(double x) { return exp(x); }
+
+template <typename T>
+__device__ __forceinline__ T quad_form(const T S[9], const T x[3]) {
+  T q = 0;
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    float t = __fadd_rn(__fmul_rn(S[3 * r + 0], x[0]), __fmul_rn(S[3 * r + 1], x[1]));
-    t = __fadd_rn(t, __fmul_rn(S[3 * r + 2], x[2]));
-    const float p = __fmul_rn(x[r], t);
-    q = r == 0 ? p : __fadd_rn(q, p);
+    T t = radd(rmul(S[3 * r + 0], x[0]), rmul(S[3 * r + 1], x[1]));
+    t = radd(t, rmul(S[3 * r + 2], x[2]));
+    const T p = rmul(x[r], t);
+    q = r == 0 ? p : radd(q, p);
   }
   return q;
 }
 
-__global__ void k_gaussian_otf(const float* __restrict__ sigma, Axes a, int64_t n,
-                               float* __restrict__ otf) {
-  float S[9];
+template <typename T>
+__global__ void k_gaussian_otf(const T* __restrict__ sigma, AxesT<T> a, int64_t n,
+                               T* __restrict__ otf) {
+  T S[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) S[k] = sigma[k];
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    float x[3];
+    T x[3];
     grid_xi(i, a, x);
-    otf[i] = expf(-quad_form(S, x) / 2.0f);
+    otf[i] = expT(-quad_form(S, x) / (T)2);
   }
 }
 
 // Partial sums of grad_otf * otf * (-x_i x_j / 2) for the 6 distinct (i <= j).
-__global__ void k_otf_sigma_grad_part(const float* __restrict__ gotf,
+template <typename T>
+__global__ void k_otf_sigma_grad_part(const T* __restrict__ gotf,
                                       const int32_t* __restrict__ band, int64_t n,
-                                      const float* __restrict__ otf, Axes a,
+                                      const T* __restrict__ otf, AxesT<T> a,
                                       double* __restrict__ part) {
   const int64_t nvox = (int64_t)a.n[0] * a.n[1] * a.n[2];
   __shared__ double sh[6][kBandThreads / 32];
@@ -183,8 +210,9 @@ __global__ void k_otf_sigma_grad_part(const float* __restrict__ gotf,
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t v = band ? (int64_t)band[i] : i;
     if (v < 0 || v >= nvox) continue;  // indices outside the grid contribute nothing
-    float x[3];
-    grid_xi(v, a, x);
+    T xt[3];
+    grid_xi(v, a, xt);
+    const double x[3] = {(double)xt[0], (double)xt[1], (double)xt[2]};
     const double w = -0.5 * (double)gotf[i] * (double)otf[v];
     acc[0] += w * x[0] * x[0];
     acc[1] += w * x[0] * x[1];
@@ -207,19 +235,21 @@ __global__ void k_otf_sigma_grad_part(const float* __restrict__ gotf,
   }
 }
 
+template <typename T>
 __global__ void k_otf_sigma_grad_final(const double* __restrict__ part, int nblk,
-                                       float* __restrict__ grad_sigma) {
+                                       T* __restrict__ grad_sigma) {
   if (threadIdx.x >= 6) return;
   double s = 0.0;
   for (int b = 0; b < nblk; ++b) s += part[6 * b + threadIdx.x];
   const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
   const int i = ij[threadIdx.x][0], j = ij[threadIdx.x][1];
-  grad_sigma[3 * i + j] = (float)s;
-  grad_sigma[3 * j + i] = (float)s;
+  grad_sigma[3 * i + j] = (T)s;
+  grad_sigma[3 * j + i] = (T)s;
 }
 
-static Axes make_axes(const float* const xi[3], const int32_t n[3]) {
-  Axes a;
+template <typename T>
+static AxesT<T> make_axes(const T* const xi[3], const int32_t n[3]) {
+  AxesT<T> a;
   for (int d = 0; d < 3; ++d) {
     a.x[d] = xi[d];
     a.n[d] = n[d];
@@ -227,15 +257,26 @@ static Axes make_axes(const float* const xi[3], const int32_t n[3]) {
   return a;
 }
 
-int launch_gaussian_otf(const float* sigma, const float* const xi[3], const int32_t n[3],
-                        float* otf, cudaStream_t st) {
+template <typename T>
+static int launch_gaussian_otf_t(const T* sigma, const T* const xi[3], const int32_t n[3],
+                                 T* otf, cudaStream_t st) {
   const int64_t nv = (int64_t)n[0] * n[1] * n[2];
   const int64_t blocks = std::min<int64_t>((nv + 255) / 256, 148 * 32);
   if (nv > 0) {
-    k_gaussian_otf<<<(unsigned)blocks, 256, 0, st>>>(sigma, make_axes(xi, n), nv, otf);
+    k_gaussian_otf<T><<<(unsigned)blocks, 256, 0, st>>>(sigma, make_axes<T>(xi, n), nv, otf);
     count_launches(1);
   }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int launch_gaussian_otf(const float* sigma, const float* const xi[3], const int32_t n[3],
+                        float* otf, cudaStream_t st) {
+  return launch_gaussian_otf_t<float>(sigma, xi, n, otf, st);
+}
+
+int launch_gaussian_otf64(const double* sigma, const double* const xi[3], const int32_t n[3],
+                          double* otf, cudaStream_t st) {
+  return launch_gaussian_otf_t<double>(sigma, xi, n, otf, st);
 }
 
 int otf_grad_blocks(int64_t n) {
@@ -243,15 +284,28 @@ int otf_grad_blocks(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
 }
 
+template <typename T>
+static int launch_otf_sigma_grad_t(const T* gotf, const int32_t* band, int64_t n, const T* otf,
+                                   const T* const xi[3], const int32_t nax[3], T* grad_sigma,
+                                   double* part, cudaStream_t st) {
+  const int nblk = otf_grad_blocks(n);
+  k_otf_sigma_grad_part<T><<<nblk, kBandThreads, 0, st>>>(gotf, band, n, otf,
+                                                          make_axes<T>(xi, nax), part);
+  k_otf_sigma_grad_final<T><<<1, 32, 0, st>>>(part, nblk, grad_sigma);
+  count_launches(2);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
 int launch_otf_sigma_grad(const float* gotf, const int32_t* band, int64_t n, const float* otf,
                           const float* const xi[3], const int32_t nax[3], float* grad_sigma,
                           double* part, cudaStream_t st) {
-  const int nblk = otf_grad_blocks(n);
-  k_otf_sigma_grad_part<<<nblk, kBandThreads, 0, st>>>(gotf, band, n, otf, make_axes(xi, nax),
-                                                       part);
-  k_otf_sigma_grad_final<<<1, 32, 0, st>>>(part, nblk, grad_sigma);
-  count_launches(2);
-  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  return launch_otf_sigma_grad_t<float>(gotf, band, n, otf, xi, nax, grad_sigma, part, st);
+}
+
+int launch_otf_sigma_grad64(const double* gotf, const int32_t* band, int64_t n,
+                            const double* otf, const double* const xi[3], const int32_t nax[3],
+                            double* grad_sigma, double* part, cudaStream_t st) {
+  return launch_otf_sigma_grad_t<double>(gotf, band, n, otf, xi, nax, grad_sigma, part, st);
 }
 
 }  // namespace dm

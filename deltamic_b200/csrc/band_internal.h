@@ -13,11 +13,18 @@ void count_launches(int n);
 int64_t band_blocks(int64_t n);
 int launch_narrowband(const float* otf, int64_t n, float thresh, int32_t* out, int64_t* count,
                       int32_t* blk_count, int32_t* blk_off, cudaStream_t st);
+int launch_narrowband64(const double* otf, int64_t n, double thresh, int32_t* out,
+                        int64_t* count, int32_t* blk_count, int32_t* blk_off, cudaStream_t st);
 int launch_band_mirror(const int32_t* band, int64_t nb, int64_t nvox, int32_t* flag,
                        cudaStream_t st);
 int launch_gaussian_otf(const float* sigma, const float* const xi[3], const int32_t n[3],
                         float* otf, cudaStream_t st);
+int launch_gaussian_otf64(const double* sigma, const double* const xi[3], const int32_t n[3],
+                          double* otf, cudaStream_t st);
 int otf_grad_blocks(int64_t n);
+int launch_otf_sigma_grad64(const double* gotf, const int32_t* band, int64_t n,
+                            const double* otf, const double* const xi[3], const int32_t nax[3],
+                            double* grad_sigma, double* part, cudaStream_t st);
 int launch_otf_sigma_grad(const float* gotf, const int32_t* band, int64_t n, const float* otf,
                           const float* const xi[3], const int32_t nax[3], float* grad_sigma,
                           double* part, cudaStream_t st);

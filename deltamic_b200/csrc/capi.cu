@@ -31,25 +31,21 @@ bool sizes_ok(int64_t nv, int64_t nt, int64_t nband) {
          nt < (int64_t)INT32_MAX / 9 && nband < (int64_t)INT32_MAX;
 }
 
+size_t topo_layout(void* p, int64_t nv, int64_t nt, TopoWs* out) {
+  Carve c(p);
+  TopoWs w;
+  w.err = c.take<int>(4);
+  w.off = c.take<int32_t>(nv + 1);
+  w.ent = c.take<int32_t>(3 * nt);
+  w.count = c.take<int32_t>(nv + 1);
+  w.cursor = c.take<int32_t>(nv + 1);
+  if (out) *out = w;
+  return c.off;
+}
+
 }  // namespace dm
 
 namespace {
-
-constexpr size_t kAlign = 256;
-size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
-
-// Sequential carving of a workspace into aligned pieces.
-struct Carve {
-  char* base;
-  size_t off;
-  explicit Carve(void* p) : base((char*)p), off(0) {}
-  template <typename T>
-  T* take(size_t count) {
-    T* p = base ? (T*)(base + off) : nullptr;
-    off += up(sizeof(T) * std::max<size_t>(count, 1));
-    return p;
-  }
-};
 
 CellDesc single_cell(const dm_box* b, int64_t nv, int64_t nt, int64_t nband, PlanTotals& t) {
   CellDesc d;
@@ -108,26 +104,6 @@ size_t fwd_layout(void* ws, const PlanTotals& t, FwdWs* out) {
   w.area_part = c.take<double>(t.face_blks);
   w.recs = c.take<FaceRec>(t.nt);
   w.fpart = c.take<float2>(t.fpart);
-  if (out) *out = w;
-  return c.off;
-}
-
-// Topology layout: off[nv+1], ent[3nt], count[nv+1], cursor[nv+1].
-struct TopoWs {
-  int* err;
-  int32_t* off;
-  int32_t* ent;
-  int32_t* count;
-  int32_t* cursor;
-};
-size_t topo_layout(void* p, int64_t nv, int64_t nt, TopoWs* out) {
-  Carve c(p);
-  TopoWs w;
-  w.err = c.take<int>(4);
-  w.off = c.take<int32_t>(nv + 1);
-  w.ent = c.take<int32_t>(3 * nt);
-  w.count = c.take<int32_t>(nv + 1);
-  w.cursor = c.take<int32_t>(nv + 1);
   if (out) *out = w;
   return c.off;
 }
@@ -346,6 +322,7 @@ const char* dm_status_string(int status) {
   if (status & DM_ERR_CUDA) return "CUDA error";
   if (status & DM_ERR_TIMEOUT) return "bounded device wait timed out";
   if (status & DM_ERR_UNSUPPORTED) return "unsupported";
+  if (status & DM_ERR_NONFINITE) return "vertex coordinate not finite";
   return "unknown status";
 }
 
@@ -382,6 +359,22 @@ int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh, int3
   int32_t* bo = c.take<int32_t>(nb);
   return launch_narrowband(otf, n_voxels, thresh, band_index, band_count, bc, bo,
                            (cudaStream_t)stream);
+}
+
+int dm_narrowband_compact64(const double* otf, int64_t n_voxels, double thresh,
+                            int32_t* band_index, int64_t* band_count, void* workspace,
+                            size_t ws_bytes, dm_stream_t stream) {
+  if (n_voxels < 0 || !band_count || !workspace || (n_voxels > 0 && (!otf || !band_index)))
+    return DM_ERR_INVALID_ARG;
+  if (n_voxels > (int64_t)INT32_MAX) return DM_ERR_SIZE;
+  if (ws_bytes < dm_narrowband_workspace_size(n_voxels)) return DM_ERR_WORKSPACE;
+  const int64_t nb = std::max<int64_t>(band_blocks(n_voxels), 1);
+  Carve c(workspace);
+  c.take<int>(4);
+  int32_t* bc = c.take<int32_t>(nb);
+  int32_t* bo = c.take<int32_t>(nb);
+  return launch_narrowband64(otf, n_voxels, thresh, band_index, band_count, bc, bo,
+                             (cudaStream_t)stream);
 }
 
 int dm_narrowband_hermitian(const int32_t* band_index, int64_t n_band, int64_t n_voxels,
@@ -646,6 +639,244 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
 }
 
 // ---------------------------------------------------------------------------
+// Explicit float32 frequency lists.
+
+namespace {
+
+struct XiWs {
+  int* err;
+  CellDesc* desc;
+  double* area_part;
+  double* s_part;
+  FaceRec* recs;
+  XiRecOff* xr;
+  float2* fpart;
+  float* bpart;
+  float* contrib;
+  int32_t* key_hist;
+  int32_t* key_first;
+  int32_t* face_order;
+  int32_t* face_slot;
+  void* topo;
+};
+
+size_t xi_layout(void* ws, const PlanTotals& t, bool backward, XiWs* out) {
+  Carve c(ws);
+  XiWs w;
+  memset(&w, 0, sizeof(w));
+  w.err = c.take<int>(4);
+  w.desc = c.take<CellDesc>(1);
+  w.area_part = c.take<double>(t.face_blks);
+  w.recs = c.take<FaceRec>(t.nt);
+  w.xr = c.take<XiRecOff>(t.nband);
+  if (!backward) {
+    w.fpart = c.take<float2>(t.fpart);
+  } else {
+    w.s_part = c.take<double>(t.band_blks);
+    w.bpart = c.take<float>(t.bpart);
+    w.contrib = c.take<float>(9 * t.nt);
+    w.key_hist = c.take<int32_t>(256 * t.face_blks);
+    w.key_first = c.take<int32_t>(256 * t.face_blks);
+    w.face_order = c.take<int32_t>(t.nt);
+    w.face_slot = c.take<int32_t>(t.nt);
+    w.topo = c.base ? (void*)(c.base + c.off) : nullptr;
+    c.off += topo_layout(nullptr, t.nv, t.nt, nullptr);
+  }
+  if (out) *out = w;
+  return c.off;
+}
+
+}  // namespace
+
+size_t dm_meshft_forward_xi_workspace_size(int64_t nv, int64_t nt, int64_t n_xi) {
+  if (!sizes_ok(nv, nt, n_xi)) return 0;
+  PlanTotals t;
+  plan_xi_cell(nv, nt, n_xi, t);
+  return xi_layout(nullptr, t, false, nullptr);
+}
+
+int dm_meshft_forward_xi(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                         const float* faces_coeff, const float* xi_list, int64_t n_xi,
+                         float* ft_list, void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_xi)) return DM_ERR_SIZE;
+  if (!workspace) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (n_xi > 0 && (!xi_list || !ft_list)) return DM_ERR_INVALID_ARG;
+  if (nv > 0 && !verts) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_forward_xi_workspace_size(nv, nt, n_xi)) return DM_ERR_WORKSPACE;
+  PlanTotals t;
+  const CellDesc d = plan_xi_cell(nv, nt, n_xi, t);
+  XiWs w;
+  xi_layout(workspace, t, false, &w);
+  return launch_xi_forward(d, t, verts, faces, faces_coeff, xi_list, w.desc, w.recs,
+                           w.area_part, w.xr, w.fpart, (float2*)ft_list, w.err,
+                           (cudaStream_t)stream);
+}
+
+size_t dm_meshft_backward_xi_workspace_size(int64_t nv, int64_t nt, int64_t n_xi) {
+  if (!sizes_ok(nv, nt, n_xi)) return 0;
+  PlanTotals t;
+  plan_xi_cell(nv, nt, n_xi, t);
+  return xi_layout(nullptr, t, true, nullptr);
+}
+
+int dm_meshft_backward_xi(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                          const float* faces_coeff, const float* grad_output_list,
+                          const float* ftmesh_list, const float* xi_list, int64_t n_xi,
+                          const void* topology, float* grad_verts, float* grad_coeff,
+                          void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_xi)) return DM_ERR_SIZE;
+  if (!workspace) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (nv > 0 && (!grad_verts || !verts)) return DM_ERR_INVALID_ARG;
+  if (n_xi > 0 && (!xi_list || !grad_output_list || !ftmesh_list)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft_backward_xi_workspace_size(nv, nt, n_xi)) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PlanTotals t;
+  const CellDesc d = plan_xi_cell(nv, nt, n_xi, t);
+  XiWs w;
+  xi_layout(workspace, t, true, &w);
+  const void* topo = topology;
+  if (!topo && nt > 0) {
+    PlanTotals tt;
+    CellDesc dd = single_cell(nullptr, nv, nt, 0, tt);
+    TopoWs tw;
+    topo_layout(w.topo, nv, nt, &tw);
+    const int s = launch_topology(one_cell(dd), tt, faces, tw.count, tw.off, tw.cursor, tw.ent,
+                                  w.err, st);
+    if (s) return s;
+    topo = w.topo;
+  }
+  TopoWs tw;
+  memset(&tw, 0, sizeof(tw));
+  if (topo) topo_layout(const_cast<void*>(topo), nv, nt, &tw);
+  if (grad_coeff && nt > 0 && n_xi == 0)
+    cudaMemsetAsync(grad_coeff, 0, sizeof(float) * (size_t)nt, st);
+  return launch_xi_backward(d, t, verts, faces, faces_coeff, xi_list,
+                            (const float2*)grad_output_list, 1.0f, (const float2*)ftmesh_list,
+                            tw.off, tw.ent, w.desc, w.recs, w.area_part, w.xr, w.s_part,
+                            w.bpart, w.contrib, grad_verts, grad_coeff, w.key_hist,
+                            w.key_first, w.face_order, w.face_slot, w.err, st);
+}
+
+// ---------------------------------------------------------------------------
+// Float64 meshFT (meshft64.cu).
+
+namespace {
+
+struct Ws64 {
+  int* err;
+  double* area_part;
+  void* recs;
+  void* xrec;
+  double* fpart;
+  double* s_part;
+  double* bpart;
+  double* contrib;
+  void* topo;
+};
+
+size_t ws64_layout(void* ws, const Plan64& p, bool backward, Ws64* out) {
+  Carve c(ws);
+  Ws64 w;
+  memset(&w, 0, sizeof(w));
+  w.err = c.take<int>(4);
+  w.area_part = c.take<double>(p.face_blks);
+  w.recs = c.take<char>(face64_bytes() * (size_t)std::max<int64_t>(p.d.nt, 1));
+  w.xrec = c.take<char>(xi64_bytes() * (size_t)std::max<int64_t>(p.d.nband, 1));
+  if (!backward) {
+    w.fpart = c.take<double>(2 * (size_t)std::max<int64_t>(p.fpart, 1));
+  } else {
+    w.s_part = c.take<double>(p.band_blks);
+    w.bpart = c.take<double>(p.bpart);
+    w.contrib = c.take<double>(9 * (size_t)p.d.nt);
+    w.topo = c.base ? (void*)(c.base + c.off) : nullptr;
+    c.off += topo_layout(nullptr, p.d.nv, p.d.nt, nullptr);
+  }
+  if (out) *out = w;
+  return c.off;
+}
+
+// Exactly one frequency source: grid band (box + band_index) or list (xi_list,
+// no box); none needed without frequencies.
+bool source64_ok(const dm_box* box, const int32_t* band_index, const double* xi_list,
+                 int64_t n_freq) {
+  if (band_index && xi_list) return false;
+  if (band_index) return box_ok(box);
+  if (xi_list) return box == nullptr;
+  return n_freq == 0 && (box == nullptr || box_ok(box));
+}
+
+}  // namespace
+
+size_t dm_meshft64_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_freq) {
+  if (!sizes_ok(nv, nt, n_freq)) return 0;
+  return ws64_layout(nullptr, plan64(nv, nt, n_freq, nullptr), false, nullptr);
+}
+
+int dm_meshft64_forward(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                        const double* faces_coeff, const dm_box* box, const int32_t* band_index,
+                        const double* xi_list, int64_t n_freq, const double* otf,
+                        double* ft_list, double* grid, void* workspace, size_t ws_bytes,
+                        dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_freq)) return DM_ERR_SIZE;
+  if (!workspace || !source64_ok(box, band_index, xi_list, n_freq)) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (n_freq > 0 && !ft_list) return DM_ERR_INVALID_ARG;
+  if (grid && !band_index) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft64_forward_workspace_size(nv, nt, n_freq)) return DM_ERR_WORKSPACE;
+  const Plan64 p = plan64(nv, nt, n_freq, band_index ? box : nullptr);
+  Ws64 w;
+  ws64_layout(workspace, p, false, &w);
+  return launch64_forward(p, verts, faces, faces_coeff, band_index, xi_list, otf, w.recs,
+                          w.area_part, w.xrec, w.fpart, ft_list, grid, w.err,
+                          (cudaStream_t)stream);
+}
+
+size_t dm_meshft64_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_freq) {
+  if (!sizes_ok(nv, nt, n_freq)) return 0;
+  return ws64_layout(nullptr, plan64(nv, nt, n_freq, nullptr), true, nullptr);
+}
+
+int dm_meshft64_backward(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                         const double* faces_coeff, const dm_box* box,
+                         const int32_t* band_index, const double* xi_list, int64_t n_freq,
+                         const double* grad_list, const double* grad_grid, const double* otf,
+                         double grad_scale, const double* ft_list, const void* topology,
+                         double* grad_verts, double* grad_coeff, void* workspace,
+                         size_t ws_bytes, dm_stream_t stream) {
+  if (!sizes_ok(nv, nt, n_freq)) return DM_ERR_SIZE;
+  if (!workspace || !source64_ok(box, band_index, xi_list, n_freq)) return DM_ERR_INVALID_ARG;
+  if (nt > 0 && (!verts || !faces || !faces_coeff)) return DM_ERR_INVALID_ARG;
+  if (nv > 0 && !grad_verts) return DM_ERR_INVALID_ARG;
+  if (n_freq > 0 && (!ft_list || (!grad_list && !grad_grid))) return DM_ERR_INVALID_ARG;
+  if (grad_grid && !band_index) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_meshft64_backward_workspace_size(nv, nt, n_freq)) return DM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const Plan64 p = plan64(nv, nt, n_freq, band_index ? box : nullptr);
+  Ws64 w;
+  ws64_layout(workspace, p, true, &w);
+  const void* topo = topology;
+  if (!topo && nt > 0) {
+    PlanTotals t;
+    CellDesc d = single_cell(nullptr, nv, nt, 0, t);
+    TopoWs tw;
+    topo_layout(w.topo, nv, nt, &tw);
+    const int s = launch_topology(one_cell(d), t, faces, tw.count, tw.off, tw.cursor, tw.ent,
+                                  w.err, st);
+    if (s) return s;
+    topo = w.topo;
+  }
+  TopoWs tw;
+  memset(&tw, 0, sizeof(tw));
+  if (topo) topo_layout(const_cast<void*>(topo), nv, nt, &tw);
+  return launch64_backward(p, verts, faces, faces_coeff, band_index, xi_list, grad_list,
+                           grad_grid, otf, grad_scale, ft_list, tw.off, tw.ent, w.recs,
+                           w.area_part, w.xrec, w.s_part, w.bpart, w.contrib, grad_verts,
+                           grad_coeff, w.err, st);
+}
+
+// ---------------------------------------------------------------------------
 // Surface + enclosed-volume transform (volume.cu).
 
 size_t dm_meshft_volume_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_band) {
@@ -727,6 +958,11 @@ static bool axes_ok(const float* x0, int32_t n0, const float* x1, int32_t n1, co
          (int64_t)n0 * n1 * n2 <= (int64_t)INT32_MAX;
 }
 
+static bool axes_ok64(const double* x0, int32_t n0, const double* x1, int32_t n1,
+                      const double* x2, int32_t n2) {
+  return axes_ok((const float*)x0, n0, (const float*)x1, n1, (const float*)x2, n2);
+}
+
 int dm_gaussian_otf(const float* sigma, const float* xi0, int32_t n0, const float* xi1,
                     int32_t n1, const float* xi2, int32_t n2, float* otf, dm_stream_t stream) {
   if (!sigma || !otf || !axes_ok(xi0, n0, xi1, n1, xi2, n2)) return DM_ERR_INVALID_ARG;
@@ -757,6 +993,35 @@ int dm_gaussian_otf_sigma_grad(const float* grad_otf, const int32_t* band_index,
   const int32_t nax[3] = {n0, n1, n2};
   return launch_otf_sigma_grad(grad_otf, band_index, n, otf, xi, nax, grad_sigma, part,
                                (cudaStream_t)stream);
+}
+
+int dm_gaussian_otf64(const double* sigma, const double* xi0, int32_t n0, const double* xi1,
+                      int32_t n1, const double* xi2, int32_t n2, double* otf,
+                      dm_stream_t stream) {
+  if (!sigma || !otf || !axes_ok64(xi0, n0, xi1, n1, xi2, n2)) return DM_ERR_INVALID_ARG;
+  const double* xi[3] = {xi0, xi1, xi2};
+  const int32_t n[3] = {n0, n1, n2};
+  return launch_gaussian_otf64(sigma, xi, n, otf, (cudaStream_t)stream);
+}
+
+int dm_gaussian_otf64_sigma_grad(const double* grad_otf, const int32_t* band_index,
+                                 int64_t n_band, const double* otf, const double* xi0, int32_t n0,
+                                 const double* xi1, int32_t n1, const double* xi2, int32_t n2,
+                                 double* grad_sigma, void* workspace, size_t ws_bytes,
+                                 dm_stream_t stream) {
+  if (!otf || !grad_sigma || !workspace || !axes_ok64(xi0, n0, xi1, n1, xi2, n2))
+    return DM_ERR_INVALID_ARG;
+  const int64_t nvox = (int64_t)n0 * n1 * n2;
+  const int64_t n = band_index ? n_band : nvox;
+  if (n < 0 || (n > 0 && !grad_otf)) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm_gaussian_otf_grad_workspace_size(n)) return DM_ERR_WORKSPACE;
+  Carve c(workspace);
+  c.take<int>(4);
+  double* part = c.take<double>(6 * (size_t)otf_grad_blocks(n));
+  const double* xi[3] = {xi0, xi1, xi2};
+  const int32_t nax[3] = {n0, n1, n2};
+  return launch_otf_sigma_grad64(grad_otf, band_index, n, otf, xi, nax, grad_sigma, part,
+                                 (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -29,6 +29,19 @@ struct alignas(16) XiRec {
 };
 static_assert(sizeof(XiRec) == 32, "XiRec layout");
 
+// A frequency off the grid (explicit xi list), 48 bytes: the XiRec fields with
+// the real m_d = xi_d L_d / pi in mf, its nearest integer in mi and the
+// remainder m_d - mi_d in fr (split phase, pair_math.cuh).
+struct alignas(16) XiRecOff {
+  int32_t mi[3];
+  float g_re;
+  float mf[3];
+  float g_im;
+  float fr[3];
+  float pad;
+};
+static_assert(sizeof(XiRecOff) == 48, "XiRecOff layout");
+
 // Per-cell description of a batched launch.  A single mesh is a batch of one.
 struct CellDesc {
   double lo[3];       // box lower corner (box_size[:,0])

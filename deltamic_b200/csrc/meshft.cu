@@ -8,6 +8,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <string.h>
+
 #include <algorithm>
 #include <atomic>
 
@@ -46,10 +48,18 @@ __global__ void k_face_prep(Cells cells, const float* __restrict__ verts,
     }
     if (!ok) set_error(err, DM_ERR_BAD_INDEX);
     double p[3][3];
+    bool fin = true;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) p[k][j] = (double)verts[3 * (d.v_off + iv[k]) + j];
+      for (int j = 0; j < 3; ++j) {
+        p[k][j] = (double)verts[3 * (d.v_off + iv[k]) + j];
+        if (!isfinite(p[k][j])) {  // reported; the face is evaluated at lo instead
+          fin = false;
+          p[k][j] = d.lo[j];
+        }
+      }
+    if (!fin) set_error(err, DM_ERR_NONFINITE);
     FaceRec r;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
@@ -560,12 +570,12 @@ int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
     profile_begin(0, st);
     const unsigned g = (unsigned)t.fwd_items;
     switch (fwd_variant()) {
-      case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
-      case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
-      case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
-      case 4: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
-      case 5: k_meshft_fwd<2, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
-      default: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, fpart, err); break;
+      case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
+      case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
+      case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
+      case 4: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
+      case 5: k_meshft_fwd<2, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
+      default: k_meshft_fwd<4, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
     }
     profile_end(0, st);
     count_launches(1);
@@ -654,6 +664,219 @@ int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, i
   if (t.nv > 0) k_csr_sort<<<(unsigned)cdiv(t.nv, kBlk), kBlk, 0, st>>>(t.nv, off, ent);
   count_launches(2 + (t.nt > 0 ? 2 : 0) + (t.nv > 0 ? 1 : 0));
   return launch_status();
+}
+
+// ---------------------------------------------------------------------------
+// Explicit frequency lists (forward_fourier3d_cpp / backward_fourier3d_cpp,
+// fourier3d_cuda.cpp:27-65): frequencies off any grid, vertex coordinates as
+// given.  The cell has lower corner 0 and per-axis length L_d = 2.5 max|v_d|
+// (computed on the device, so |v_d| < L_d / 2 and the fixed-point positions fit
+// in int32); each frequency becomes m_d = xi_d L_d / pi, split into its nearest
+// integer and a remainder (split phase, pair_math.cuh).  The same main kernels
+// run with the off-grid records; every frequency is evaluated.
+
+constexpr FwdVariant kXiFwd{2, 256, 16};
+constexpr BwdVariant kXiBwd{1, 128, 16};
+
+// One block: L_d from the vertices, written with the host plan into *out.
+__global__ void k_xi_cell(CellDesc base, const float* __restrict__ verts, int64_t nv,
+                          CellDesc* __restrict__ out, int* err) {
+  __shared__ float sh[3][32];
+  float m[3] = {0.f, 0.f, 0.f};
+  bool fin = true;
+  for (int64_t i = threadIdx.x; i < nv; i += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float a = fabsf(verts[3 * i + j]);
+      if (isfinite(a)) m[j] = fmaxf(m[j], a); else fin = false;
+    }
+  if (!fin) set_error(err, DM_ERR_NONFINITE);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    for (int o = 16; o > 0; o >>= 1) m[j] = fmaxf(m[j], __shfl_down_sync(0xffffffffu, m[j], o));
+    if ((threadIdx.x & 31) == 0) sh[j][threadIdx.x >> 5] = m[j];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CellDesc d = base;
+    for (int j = 0; j < 3; ++j) {
+      float v = 0.f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmaxf(v, sh[j][w]);
+      d.lo[j] = 0.0;
+      d.len[j] = v > 0.f ? 2.5 * (double)v : 1.0;
+    }
+    *out = d;
+  }
+}
+
+// Off-grid frequency records (and, with a cotangent, g and per-block sums of
+// s = Re(conj(g) ft)).
+__global__ void k_xi_prep(const CellDesc* __restrict__ dp, const float* __restrict__ xi_list,
+                          const float2* __restrict__ grad_list, float grad_scale,
+                          const float2* __restrict__ ft_list, XiRecOff* __restrict__ xr,
+                          double* __restrict__ s_part, int* err) {
+  __shared__ double sh[40];
+  const CellDesc d = *dp;
+  const int m = blockIdx.x * kBlk + threadIdx.x;
+  double s = 0.0;
+  if (m < d.nband) {
+    XiRecOff r;
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double mm = (double)xi_list[3 * (int64_t)m + j] * d.len[j] * 0.3183098861837907;
+      if (!(fabs(mm) < 1073741824.0)) {  // |m| < 2^30 (NaN fails too)
+        ok = false;
+        r.mi[j] = 0;
+        r.mf[j] = 0.f;
+        r.fr[j] = 0.f;
+        continue;
+      }
+      const double mi = rint(mm);
+      r.mi[j] = (int32_t)mi;
+      r.mf[j] = (float)mm;
+      r.fr[j] = (float)(mm - mi);
+    }
+    if (!ok) set_error(err, DM_ERR_SIZE);
+    r.g_re = r.g_im = r.pad = 0.f;
+    if (grad_list) {
+      const float2 g = grad_list[m];
+      r.g_re = grad_scale * g.x;
+      r.g_im = grad_scale * g.y;
+      const float2 ft = ft_list[m];
+      s = (double)r.g_re * ft.x + (double)r.g_im * ft.y;
+    }
+    xr[m] = r;
+  }
+  if (s_part) {
+    const double t = block_sum_d(s, sh);
+    if (threadIdx.x == 0) s_part[blockIdx.x] = t;
+  }
+}
+
+// ft_list = (2/M) sum over splits, fixed order.
+__global__ void k_xi_fwd_epi(const CellDesc* __restrict__ dp, const float2* __restrict__ fpart,
+                             const double* __restrict__ area_part, int n_area,
+                             float2* __restrict__ ft_list) {
+  __shared__ double sh[40];
+  const CellDesc d = *dp;
+  const double M = block_sum_list(area_part, n_area, sh);
+  const int m = blockIdx.x * kBlk + threadIdx.x;
+  if (m >= d.nband) return;
+  double sx = 0.0, sy = 0.0;
+  for (int s = 0; s < d.fsplit; ++s) {
+    const float2 v = fpart[(int64_t)s * d.nband + m];
+    sx += v.x;
+    sy += v.y;
+  }
+  const double sc = d.nt > 0 ? 2.0 / M : 0.0;
+  ft_list[m] = make_float2((float)(sx * sc), (float)(sy * sc));
+}
+
+CellDesc plan_xi_cell(int64_t nv, int64_t nt, int64_t n_xi, PlanTotals& t) {
+  CellDesc d;
+  memset(&d, 0, sizeof(d));
+  for (int k = 0; k < 3; ++k) {
+    d.len[k] = 1.0;
+    d.n[k] = 1;
+  }
+  d.nv = (int32_t)nv;
+  d.nt = (int32_t)nt;
+  d.nband = (int32_t)n_xi;
+  set_band_half(d, false);
+  plan_cell_tiles_for(d, kXiFwd, kXiBwd);
+  t = PlanTotals{};
+  t.nv = nv;
+  t.nt = nt;
+  t.nband = n_xi;
+  t.fpart = (int64_t)d.fsplit * d.ne;
+  t.bpart = (int64_t)d.bchunks * 10 * d.nt;
+  t.face_blks = std::max<int64_t>(1, cdiv(nt, kBlk));
+  t.band_blks = std::max<int64_t>(1, cdiv(n_xi, kBlk));
+  t.fwd_items = (int64_t)d.xtiles * d.fsplit;
+  t.bwd_items = (int64_t)d.fblocks * d.bchunks;
+  return d;
+}
+
+int launch_xi_forward(const CellDesc& plan, const PlanTotals& t, const float* verts,
+                      const int64_t* faces, const float* coeff, const float* xi_list,
+                      CellDesc* dev_desc, FaceRec* recs, double* area_part, XiRecOff* xr,
+                      float2* fpart, float2* ft_list, int* err, cudaStream_t st) {
+  k_xi_cell<<<1, 1024, 0, st>>>(plan, verts, t.nv, dev_desc, err);
+  Cells c;
+  memset(&c, 0, sizeof(c));
+  c.p = dev_desc;
+  c.n = 1;
+  count_launches(1);
+  if (t.nt > 0) {
+    k_face_prep<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, recs, area_part,
+                                                       err);
+    count_launches(1);
+  }
+  if (t.nband <= 0) return launch_status();
+  k_xi_prep<<<(unsigned)t.band_blks, kBlk, 0, st>>>(dev_desc, xi_list, nullptr, 0.f, nullptr,
+                                                   xr, nullptr, err);
+  count_launches(1);
+  if (t.nt > 0) {
+    k_meshft_fwd<kXiFwd.R, kXiFwd.NT, kFwdTF, kStages, false, true>
+        <<<(unsigned)t.fwd_items, kXiFwd.NT, 0, st>>>(c, recs, nullptr, nullptr, xr, fpart, err);
+    count_launches(1);
+  } else {
+    cudaMemsetAsync(fpart, 0, sizeof(float2) * (size_t)std::max<int64_t>(t.fpart, 1), st);
+    cudaMemsetAsync(area_part, 0, sizeof(double), st);
+  }
+  k_xi_fwd_epi<<<(unsigned)t.band_blks, kBlk, 0, st>>>(dev_desc, fpart, area_part,
+                                                      (int)(t.nt > 0 ? t.face_blks : 1), ft_list);
+  count_launches(1);
+  return launch_status();
+}
+
+int launch_xi_backward(const CellDesc& plan, const PlanTotals& t, const float* verts,
+                       const int64_t* faces, const float* coeff, const float* xi_list,
+                       const float2* grad_list, float grad_scale, const float2* ft_list,
+                       const int32_t* csr_off, const int32_t* csr_ent, CellDesc* dev_desc,
+                       FaceRec* recs, double* area_part, XiRecOff* xr, double* s_part,
+                       float* bpart, float* contrib, float* grad_verts, float* grad_coeff,
+                       int32_t* key_hist, int32_t* key_first, int32_t* face_order,
+                       int32_t* face_slot, int* err, cudaStream_t st) {
+  if (t.nt <= 0) {
+    if (t.nv > 0) cudaMemsetAsync(grad_verts, 0, sizeof(float) * 3 * (size_t)t.nv, st);
+    return launch_status();
+  }
+  k_xi_cell<<<1, 1024, 0, st>>>(plan, verts, t.nv, dev_desc, err);
+  Cells c;
+  memset(&c, 0, sizeof(c));
+  c.p = dev_desc;
+  c.n = 1;
+  k_face_prep<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, recs, area_part,
+                                                     err);
+  count_launches(2);
+  const bool sort = t.nt >= kSortMinFaces;
+  if (sort) {
+    k_face_key_hist<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, recs, key_hist);
+    k_face_key_scan<<<1, kKeyBins, 0, st>>>(c, key_hist, key_first);
+    k_face_key_scatter<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, recs, key_first, face_order,
+                                                               face_slot);
+    count_launches(3);
+  }
+  if (t.nband > 0) {
+    k_xi_prep<<<(unsigned)t.band_blks, kBlk, 0, st>>>(dev_desc, xi_list, grad_list, grad_scale,
+                                                     ft_list, xr, s_part, err);
+    cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
+    k_meshft_bwd<kXiBwd.F, kXiBwd.NT, kBwdTX, kStages, false, XiRecOff>
+        <<<(unsigned)t.bwd_items, kXiBwd.NT, 0, st>>>(c, recs, nullptr, xr, nullptr,
+                                                      sort ? face_order : nullptr, bpart, err);
+    count_launches(2);
+  } else {
+    cudaMemsetAsync(s_part, 0, sizeof(double), st);
+    cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
+  }
+  k_bwd_face_epi<<<(unsigned)t.face_blks, kBlk, 0, st>>>(c, verts, faces, coeff, area_part,
+                                                        s_part, bpart,
+                                                        sort ? face_slot : nullptr, contrib,
+                                                        grad_coeff);
+  count_launches(1);
+  return launch_vertex_gather(t.nv, csr_off, csr_ent, contrib, grad_verts, st);
 }
 
 }  // namespace dm

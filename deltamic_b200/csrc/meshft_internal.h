@@ -41,6 +41,33 @@ int num_sms();
 bool box_ok(const dm_box* b);
 bool sizes_ok(int64_t nv, int64_t nt, int64_t nband);
 
+// Sequential carving of a caller's workspace into 256-byte aligned pieces (a
+// null base only measures: take() returns null and advances the offset).
+constexpr size_t kAlign = 256;
+inline size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+struct Carve {
+  char* base;
+  size_t off;
+  explicit Carve(void* p) : base((char*)p), off(0) {}
+  template <typename T>
+  T* take(size_t count) {
+    T* p = base ? (T*)(base + off) : nullptr;
+    off += up(sizeof(T) * (count > 0 ? count : 1));
+    return p;
+  }
+};
+
+// Topology (vertex <- face CSR) layout: status word, off[nv+1], ent[3nt],
+// count[nv+1], cursor[nv+1]; returns its size in bytes.
+struct TopoWs {
+  int* err;
+  int32_t* off;
+  int32_t* ent;
+  int32_t* count;
+  int32_t* cursor;
+};
+size_t topo_layout(void* p, int64_t nv, int64_t nt, TopoWs* out);
+
 // Instrumentation: launches counted per process; optional CUDA events around the
 // main forward / backward kernels (kind 0 / 1).
 void count_launches(int n);
@@ -84,6 +111,45 @@ int launch_volume_backward(const CellDesc& d, const PlanTotals& t, const float* 
                            float4* vrec, float4* fw, XiRec* xrec, float4* xg, float* bpart,
                            float* contrib, const int32_t* csr_off, const int32_t* csr_ent,
                            float* grad_verts, float* grad_regint, int* err, cudaStream_t st);
+// Explicit float32 frequency lists (meshft.cu): one mesh, vertex coordinates as
+// given, the cell (lower corner 0, lengths from the vertices) computed on the
+// device into dev_desc; plan_xi_cell sizes the launches (t.nband = n_xi).
+CellDesc plan_xi_cell(int64_t nv, int64_t nt, int64_t n_xi, PlanTotals& t);
+int launch_xi_forward(const CellDesc& plan, const PlanTotals& t, const float* verts,
+                      const int64_t* faces, const float* coeff, const float* xi_list,
+                      CellDesc* dev_desc, FaceRec* recs, double* area_part, XiRecOff* xr,
+                      float2* fpart, float2* ft_list, int* err, cudaStream_t st);
+int launch_xi_backward(const CellDesc& plan, const PlanTotals& t, const float* verts,
+                       const int64_t* faces, const float* coeff, const float* xi_list,
+                       const float2* grad_list, float grad_scale, const float2* ft_list,
+                       const int32_t* csr_off, const int32_t* csr_ent, CellDesc* dev_desc,
+                       FaceRec* recs, double* area_part, XiRecOff* xr, double* s_part,
+                       float* bpart, float* contrib, float* grad_verts, float* grad_coeff,
+                       int32_t* key_hist, int32_t* key_first, int32_t* face_order,
+                       int32_t* face_slot, int* err, cudaStream_t st);
+
+// Float64 meshFT (meshft64.cu): one mesh, the frequencies of a grid band
+// (band_index with the box) or of an explicit xi list (box NULL, vertices as
+// given); every frequency evaluated.
+struct Plan64 {
+  CellDesc d;
+  int64_t face_blks, band_blks, fpart, bpart, fwd_items, bwd_items;
+};
+Plan64 plan64(int64_t nv, int64_t nt, int64_t nfreq, const dm_box* box);
+size_t face64_bytes();
+size_t xi64_bytes();
+int launch64_forward(const Plan64& p, const double* verts, const int64_t* faces,
+                     const double* coeff, const int32_t* band_index, const double* xi_list,
+                     const double* otf, void* recs, double* area_part, void* xrec, double* fpart,
+                     double* ft_list, double* grid, int* err, cudaStream_t st);
+int launch64_backward(const Plan64& p, const double* verts, const int64_t* faces,
+                      const double* coeff, const int32_t* band_index, const double* xi_list,
+                      const double* grad_list, const double* grad_grid, const double* otf,
+                      double grad_scale, const double* ft_list, const int32_t* csr_off,
+                      const int32_t* csr_ent, void* recs, double* area_part, void* xrec,
+                      double* s_part, double* bpart, double* contrib, double* grad_verts,
+                      double* grad_coeff, int* err, cudaStream_t st);
+
 int launch_topology(const Cells& c, const PlanTotals& t, const int64_t* faces, int32_t* count,
                     int32_t* off, int32_t* cursor, int32_t* ent, int* err, cudaStream_t st);
 

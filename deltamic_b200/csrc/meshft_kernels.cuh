@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "dm_common.cuh"
 #include "pair_math.cuh"
 
@@ -124,9 +126,9 @@ __device__ __forceinline__ void stage_tile(Rec* dst, float4* xdst, const Rec* sr
 // Forward main kernel.
 
 // acc += ac F and, with kVol, vac += (m . nv) F for every frequency of the thread.
-template <int R, bool kVol>
+template <int R, bool kVol, class XV>
 __device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const float4& nv,
-                                         const XiVal (&xv)[R], float2 (&acc)[R],
+                                         const XV (&xv)[R], float2 (&acc)[R],
                                          float2 (&vac)[R]) {
   uint32_t spm = 0;
 #pragma unroll
@@ -161,13 +163,28 @@ __device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const floa
   }
 }
 
+// Frequency of an XiRecOff (off-grid xi list).
+__device__ __forceinline__ XiValOff xi_off(const XiRecOff& r) {
+  XiValOff x;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    x.mi[k] = r.mi[k];
+    x.mf[k] = r.mf[k];
+    x.fr[k] = r.fr[k];
+  }
+  return x;
+}
+
 // fpart[split][m] = sum over the split's faces of area_coeff F; with kVol also
-// fpart[fsplit + split][m] = sum of (m . nor') F, nor' = vrec[f].xyz.
-template <int R, int NT, int TF, int NS, bool kVol = false>
+// fpart[fsplit + split][m] = sum of (m . nor') F, nor' = vrec[f].xyz.  With kOff
+// the frequencies are the off-grid records xoff (split phase), else band voxels.
+template <int R, int NT, int TF, int NS, bool kVol = false, bool kOff = false>
 __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* __restrict__ recs,
                                                   const float4* __restrict__ vrec,
                                                   const int32_t* __restrict__ band_index,
+                                                  const XiRecOff* __restrict__ xoff,
                                                   float2* __restrict__ fpart, int* err) {
+  using XV = typename std::conditional<kOff, XiValOff, XiVal>::type;
   __shared__ __align__(128) FaceRec sf[NS][TF];
   __shared__ __align__(16) float4 sv[kVol ? NS : 1][kVol ? TF : 1];
   __shared__ __align__(8) uint64_t bar[NS];
@@ -191,7 +208,7 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
     return;
   }
 
-  XiVal xv[R];
+  XV xv[R];
   int mloc[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
@@ -200,9 +217,13 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
     // lanes past the band evaluate a real frequency so every lane takes the
     // same branches; their sums are never stored
     const int mm = min(m, d.ne - 1);
-    band_to_m(band_index[d.b_off + mm], d, xv[r].mi);
+    if constexpr (kOff) {
+      xv[r] = xi_off(xoff[d.b_off + mm]);
+    } else {
+      band_to_m(band_index[d.b_off + mm], d, xv[r].mi);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) xv[r].mf[k] = (float)xv[r].mi[k];
+      for (int k = 0; k < 3; ++k) xv[r].mf[k] = (float)xv[r].mi[k];
+    }
   }
 
   const int ntiles = (nf + TF - 1) / TF;
@@ -294,16 +315,47 @@ __device__ __forceinline__ void bwd_accumulate(BwdAccT<kVol>& a, const float z[3
 // bpart[chunk][i][f] = q[i] of face slot f over the chunk's frequencies.  With
 // kVol, fw[face] = {a, beta nor'} and xg[m] = {Re, Im} of g / |xi|^2 (0 at xi = 0);
 // the pair's cotangent for z is g conj(W) = a g - i (beta m.nor') g/|xi|^2.
-template <int F, int NT, int TX, int NS, bool kVol = false>
+// Frequency and cotangent of a staged record (grid or off-grid).
+__device__ __forceinline__ void load_xi(const XiRec& r, XiVal& xv, float& gre, float& gim) {
+  const uint4* q = reinterpret_cast<const uint4*>(&r);
+  const uint4 w0 = q[0], w1 = q[1];
+  xv.mi[0] = (int32_t)w0.x;
+  xv.mi[1] = (int32_t)w0.y;
+  xv.mi[2] = (int32_t)w0.z;
+  gre = __uint_as_float(w0.w);
+  xv.mf[0] = __uint_as_float(w1.x);
+  xv.mf[1] = __uint_as_float(w1.y);
+  xv.mf[2] = __uint_as_float(w1.z);
+  gim = __uint_as_float(w1.w);
+}
+__device__ __forceinline__ void load_xi(const XiRecOff& r, XiValOff& xv, float& gre,
+                                        float& gim) {
+  const uint4* q = reinterpret_cast<const uint4*>(&r);
+  const uint4 w0 = q[0], w1 = q[1], w2 = q[2];
+  xv.mi[0] = (int32_t)w0.x;
+  xv.mi[1] = (int32_t)w0.y;
+  xv.mi[2] = (int32_t)w0.z;
+  gre = __uint_as_float(w0.w);
+  xv.mf[0] = __uint_as_float(w1.x);
+  xv.mf[1] = __uint_as_float(w1.y);
+  xv.mf[2] = __uint_as_float(w1.z);
+  gim = __uint_as_float(w1.w);
+  xv.fr[0] = __uint_as_float(w2.x);
+  xv.fr[1] = __uint_as_float(w2.y);
+  xv.fr[2] = __uint_as_float(w2.z);
+}
+
+template <int F, int NT, int TX, int NS, bool kVol = false, class XR = XiRec>
 __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
                                                   const float4* __restrict__ fw,
-                                                  const XiRec* __restrict__ xrec,
+                                                  const XR* __restrict__ xrec,
                                                   const float4* __restrict__ xg,
                                                   const int32_t* __restrict__ order,
                                                   float* __restrict__ bpart, int* err) {
   using Acc = BwdAccT<kVol>;
+  using XV = typename std::conditional<std::is_same<XR, XiRecOff>::value, XiValOff, XiVal>::type;
   constexpr int NQ = Acc::N;
-  __shared__ __align__(128) XiRec sx[NS][TX];
+  __shared__ __align__(128) XR sx[NS][TX];
   __shared__ __align__(16) float4 sg[kVol ? NS : 1][kVol ? TX : 1];
   __shared__ __align__(8) uint64_t bar[NS];
   const int item = blockIdx.x;
@@ -332,7 +384,7 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
   }
 
   const int ntiles = (nx + TX - 1) / TX;
-  const XiRec* src0 = xrec + d.b_off + x0;
+  const XR* src0 = xrec + d.b_off + x0;
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
@@ -361,17 +413,9 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
 #pragma unroll
       for (int i = 0; i < NQ; ++i) tacc[k].q[i] = 0.f;
     for (int j = 0; j < nxt; ++j) {
-      const uint4* q = reinterpret_cast<const uint4*>(&sx[s][j]);
-      const uint4 w0 = q[0], w1 = q[1];
-      XiVal xv;
-      xv.mi[0] = (int32_t)w0.x;
-      xv.mi[1] = (int32_t)w0.y;
-      xv.mi[2] = (int32_t)w0.z;
-      const float gre = __uint_as_float(w0.w);
-      xv.mf[0] = __uint_as_float(w1.x);
-      xv.mf[1] = __uint_as_float(w1.y);
-      xv.mf[2] = __uint_as_float(w1.z);
-      const float gim = __uint_as_float(w1.w);
+      XV xv;
+      float gre, gim;
+      load_xi(sx[s][j], xv, gre, gim);
       float2 gv = make_float2(0.f, 0.f);
       if (kVol) {
         const float4 g4 = sg[s][j];

@@ -127,8 +127,40 @@ struct XiVal {
   float mf[3];
 };
 
+// A frequency off the grid (an explicit xi list): m_d = xi_d L_d / pi is real,
+// split into its nearest integer mi_d and the remainder fr_d (|fr_d| <= 1/2);
+// mf_d = m_d as a float (for the phase differences).
+struct XiValOff {
+  int32_t mi[3];
+  float mf[3];
+  float fr[3];
+};
+
 DM_HD uint32_t fixed_phase(const int32_t mi[3], uint32_t U0, uint32_t U1, uint32_t U2) {
   return (uint32_t)mi[0] * U0 + (uint32_t)mi[1] * U1 + (uint32_t)mi[2] * U2;
+}
+
+DM_HD int32_t round_to_int(float x) {
+#if defined(__CUDA_ARCH__)
+  return __float2int_rn(x);
+#else
+  return (int32_t)lrintf(x);
+#endif
+}
+
+// Vertex phase as an angle in [-pi, pi).  On the grid the phase in turns is
+// sum_d mi_d U_d / 2^32 (mod 1), exact in uint32.  Off the grid (split phase)
+// the remainder adds sum_d fr_d U_d / 2^32 turns, with U_d read as signed (the
+// off-grid cell has lower corner 0 and |v_d| < L_d / 2, so |U_d| < 2^30): that
+// term is below 3/8 of a turn and is formed in float, rounded back to 2^-32-turn
+// units and added in uint32 before the turns become an angle.
+DM_HD float vertex_angle(const XiVal& xv, uint32_t U0, uint32_t U1, uint32_t U2) {
+  return turns_to_angle(fixed_phase(xv.mi, U0, U1, U2));
+}
+DM_HD float vertex_angle(const XiValOff& xv, uint32_t U0, uint32_t U1, uint32_t U2) {
+  const float c = xv.fr[0] * (float)(int32_t)U0 + xv.fr[1] * (float)(int32_t)U1 +
+                  xv.fr[2] * (float)(int32_t)U2;
+  return turns_to_angle(fixed_phase(xv.mi, U0, U1, U2) + (uint32_t)round_to_int(c));
 }
 
 // G(U, W) and (optionally) dG/dU, dG/dW via S, for |W - U| >= 1.
@@ -266,8 +298,8 @@ DM_HD c32 expmi(float angle) {
 // Centroid path.  Vertex phases x'_v = x_v + off[v] with half differences
 // (hab, hbc, hca) of the x'.  Outputs E = exp(-i x'_g), H and, if kGrad, the
 // centroid deviations d[3] and the partials Hp2, Hp3; F = E H.
-template <bool kGrad, bool kLo = false>
-DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca, float off_a,
+template <bool kGrad, bool kLo = false, class XV>
+DM_HD void eval_series(const XV& xv, const FaceGeom& g, float hab, float hca, float off_a,
                        c32& E, c32& H, c32& Hp2, c32& Hp3, float d[3], float& p2) {
   const float ab = 2.0f * hab, ca = 2.0f * hca;
   const float da = (ca - ab) * (1.0f / 3.0f);
@@ -275,7 +307,7 @@ DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca,
   const float dc = da - ca;
   p2 = da * da + db * db + dc * dc;
   const float p3 = 3.0f * da * db * dc;  // sum d^3 when sum d = 0
-  E = expmi(turns_to_angle(fixed_phase(xv.mi, g.Ua[0], g.Ua[1], g.Ua[2])) + (off_a - da));
+  E = expmi(vertex_angle(xv, g.Ua[0], g.Ua[1], g.Ua[2]) + (off_a - da));
   centroid_H<kGrad, kLo>(p2, p3, H, Hp2, Hp3);
   d[0] = da;
   d[1] = db;
@@ -284,8 +316,8 @@ DM_HD void eval_series(const XiVal& xv, const FaceGeom& g, float hab, float hca,
 
 // Pivot path (largest difference >= 3.5).  Outputs E = exp(-i x'_p), G and, if
 // kGrad, dG/dU and dG/dW; F = E G; piv = 0/1/2 for pivot a/b/c.
-template <bool kGrad>
-DM_HD void eval_pivot(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+template <bool kGrad, class XV>
+DM_HD void eval_pivot(const XV& xv, const FaceGeom& g, float hab, float hbc, float hca,
                       const float off[3], c32& E, c32& G, c32& Gu, c32& Gw, int& piv) {
   const float aab = fabsf(hab), abc = fabsf(hbc), aca = fabsf(hca);
   const bool pa = (abc >= aca) && (abc >= aab);
@@ -297,13 +329,13 @@ DM_HD void eval_pivot(const XiVal& xv, const FaceGeom& g, float hab, float hbc, 
   const uint32_t P1 = pa ? g.Ua[1] : (pb ? g.Ub[1] : g.Uc[1]);
   const uint32_t P2 = pa ? g.Ua[2] : (pb ? g.Ub[2] : g.Uc[2]);
   const float o = pa ? off[0] : (pb ? off[1] : off[2]);
-  E = expmi(turns_to_angle(fixed_phase(xv.mi, P0, P1, P2)) + o);
+  E = expmi(vertex_angle(xv, P0, P1, P2) + o);
   g_sinc<kGrad>(hu, hw, G, Gu, Gw);
 }
 
 // F and dF/dx_{a,b,c} for vertex phases x_v + off[v] (no degenerate branch).
-template <bool kGrad>
-DM_HD void eval_any(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+template <bool kGrad, class XV>
+DM_HD void eval_any(const XV& xv, const FaceGeom& g, float hab, float hbc, float hca,
                     const float off[3], c32& F, c32* dF) {
   const float amax = fmaxf(fabsf(hab), fmaxf(fabsf(hbc), fabsf(hca)));
   if (amax < kSeriesHalf) {
@@ -339,8 +371,8 @@ DM_HD void eval_any(const XiVal& xv, const FaceGeom& g, float hab, float hbc, fl
 // R1 collapses the three phases to their centroid, R2/R3/R4 merge the close pair
 // at its midpoint (fourier3d_cuda_kernel.cu:250-271, render.py:77-102); the
 // merged vertices share the derivative of the merged phase equally.
-template <bool kGrad>
-DM_HD void pair_degenerate(const XiVal& xv, const FaceGeom& g, float hab, float hbc, float hca,
+template <bool kGrad, class XV>
+DM_HD void pair_degenerate(const XV& xv, const FaceGeom& g, float hab, float hbc, float hca,
                            c32& F, c32* dF) {
   const bool sab = fabsf(hab) <= kSepsHalf, sbc = fabsf(hbc) <= kSepsHalf,
              sca = fabsf(hca) <= kSepsHalf;
@@ -404,8 +436,8 @@ DM_HD int pair_class(float hab, float hbc, float hca) {
 }
 
 // Any pair: F and (if kGrad) dF/dx_{a,b,c}.
-template <bool kGrad>
-DM_HD void pair_general(const XiVal& xv, const FaceGeom& g, c32& F, c32* dF) {
+template <bool kGrad, class XV>
+DM_HD void pair_general(const XV& xv, const FaceGeom& g, c32& F, c32* dF) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
   if (pair_class(hab, hbc, hca) == 2) {
@@ -434,7 +466,8 @@ DM_HD bool series_short(float hab, float hbc, float hca) {
 
 // Forward: F on the series / pivot paths; returns false for a degenerate pair
 // (F then undefined: the caller runs pair_degenerate for it).
-DM_HD bool pair_forward(const XiVal& xv, const FaceGeom& g, c32& F) {
+template <class XV>
+DM_HD bool pair_forward(const XV& xv, const FaceGeom& g, c32& F) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
   const int cls = pair_class(hab, hbc, hca);
@@ -459,8 +492,8 @@ DM_HD bool pair_forward(const XiVal& xv, const FaceGeom& g, c32& F) {
 
 // Adjoint: z_v = Re(conj(g) dF/dx_v) and r = Re(conj(g) F) for cotangent g, and
 // F itself if kF; returns false for a degenerate pair (outputs undefined).
-template <bool kF>
-DM_HD bool pair_adjoint_t(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
+template <bool kF, class XV>
+DM_HD bool pair_adjoint_t(const XV& xv, const FaceGeom& g, float gre, float gim, float z[3],
                           float& r, c32& Fo) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
@@ -503,14 +536,16 @@ DM_HD bool pair_adjoint_t(const XiVal& xv, const FaceGeom& g, float gre, float g
   return true;
 }
 
-DM_HD bool pair_adjoint(const XiVal& xv, const FaceGeom& g, float gre, float gim, float z[3],
+template <class XV>
+DM_HD bool pair_adjoint(const XV& xv, const FaceGeom& g, float gre, float gim, float z[3],
                         float& r) {
   c32 unused;
   return pair_adjoint_t<false>(xv, g, gre, gim, z, r, unused);
 }
 
 // Adjoint of a degenerate pair (F returned as well).
-DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre, float gim,
+template <class XV>
+DM_HD void pair_adjoint_degenerate(const XV& xv, const FaceGeom& g, float gre, float gim,
                                    float z[3], float& r, c32& F) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
@@ -519,14 +554,16 @@ DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre
   r = gre * F.x + gim * F.y;
   for (int v = 0; v < 3; ++v) z[v] = gre * dF[v].x + gim * dF[v].y;
 }
-DM_HD void pair_adjoint_degenerate(const XiVal& xv, const FaceGeom& g, float gre, float gim,
+template <class XV>
+DM_HD void pair_adjoint_degenerate(const XV& xv, const FaceGeom& g, float gre, float gim,
                                    float z[3], float& r) {
   c32 F;
   pair_adjoint_degenerate(xv, g, gre, gim, z, r, F);
 }
 
 // Forward of a degenerate pair.
-DM_HD c32 pair_forward_degenerate(const XiVal& xv, const FaceGeom& g) {
+template <class XV>
+DM_HD c32 pair_forward_degenerate(const XV& xv, const FaceGeom& g) {
   float hab, hbc, hca;
   half_diffs(xv.mf, g, hab, hbc, hca);
   c32 F;

@@ -391,7 +391,7 @@ int launch_volume_forward(const CellDesc& d, const PlanTotals& t, const float* v
   if (t.fwd_items > 0) {
     profile_begin(0, st);
     k_meshft_fwd<kVolR, kVolFwdNT, kFwdTF, kStages, true>
-        <<<(unsigned)t.fwd_items, kVolFwdNT, 0, st>>>(c, recs, vrec, band_index, fpart, err);
+        <<<(unsigned)t.fwd_items, kVolFwdNT, 0, st>>>(c, recs, vrec, band_index, nullptr, fpart, err);
     profile_end(0, st);
     count_launches(1);
     if (status()) return DM_ERR_CUDA;

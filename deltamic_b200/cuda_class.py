@@ -3,13 +3,15 @@ its signature, on this library's kernels.
 
 ``MeshFTCUDA.apply(Verts, Faces, Faces_coeff, xi0, xi1, xi2, Filter,
 narrowband_thresh)`` returns the dense complex spectrum on the grid of the three
-centred frequency axes, zero outside ``Filter > narrowband_thresh``, for the vertex
+frequency axes, zero outside ``Filter > narrowband_thresh``, for the vertex
 coordinates as given (the phase of every vertex is ``xi . v``).  As in the
-reference, only ``Verts`` receives a gradient.  The axes must be the centred grids
-``(2k - (n - 1)) pi / L`` that ``compute_spatial_frequency_grid`` makes (the
-kernels evaluate the phases in exact fixed point on that grid); other axes raise
-``ValueError``.  A float64 ``Verts`` is evaluated in float32 and returns complex128,
-as ``Fourier3dMesh(dtype=float64)`` does.
+reference, only ``Verts`` receives a gradient.  On the centred grids
+``(2k - (n - 1)) pi / L`` that ``compute_spatial_frequency_grid`` makes, the
+grid kernels run (exact fixed-point phases, a mirror-symmetric band evaluated
+half); on any other axes the explicit-list kernels of ``forward_fourier3d_cpp``
+run on the band's frequency list (split phase), as the reference itself does.
+A float64 ``Verts`` runs the float64 kernels (the reference's double dispatch)
+and returns complex128.
 """
 from __future__ import annotations
 
@@ -35,18 +37,44 @@ class MeshFTCUDA:
         if tuple(Filter.shape) != shape:
             raise ValueError(f"Filter shape {tuple(Filter.shape)} does not match the axes "
                              f"{shape}")
-        L = [_axis_length(x) for x in (xi0, xi1, xi2)]
+        try:
+            L = [_axis_length(x) for x in (xi0, xi1, xi2)]
+        except ValueError:
+            return _off_grid(Verts, Faces, Faces_coeff, xi0, xi1, xi2, Filter,
+                             narrowband_thresh)
         grid = ops.FreqGrid(np.array([[0.0, L[0]], [0.0, L[1]], [0.0, L[2]]]), shape)
         thr = float(narrowband_thresh)
         key = (Filter.data_ptr(), Filter._version, shape, thr)
         hit = _BANDS.get(id(Filter))
+        f64 = Verts.dtype == torch.float64
+        key = key + (f64,)
         if hit is not None and hit[0] == key:
             band = hit[1]
         else:
-            band = ops.narrowband(Filter.detach().float().contiguous(), thr)
+            flt = Filter.detach()
+            band = ops.narrowband((flt.double() if f64 else flt.float()).contiguous(), thr)
             _BANDS.clear()
             _BANDS[id(Filter)] = (key, band)
-        f64 = Verts.dtype == torch.float64
-        coeff = Faces_coeff.detach().float()  # the reference returns no coefficient gradient
-        out = ops.meshft(Verts.float() if f64 else Verts, Faces, coeff, grid, band)
-        return out.to(torch.complex128) if f64 else out
+        # the reference returns no coefficient gradient
+        if f64:
+            return ops.meshft64(Verts, Faces, Faces_coeff.detach().double(), grid, band)
+        return ops.meshft(Verts, Faces, Faces_coeff.detach().float(), grid, band)
+
+
+def _off_grid(Verts, Faces, Faces_coeff, xi0, xi1, xi2, Filter, narrowband_thresh):
+    """Axes that are not centred grids: the band's frequency list (the meshgrid
+    gather of cuda_class.py:21-24) through the explicit-list kernels, scattered
+    into the dense spectrum."""
+    f64 = Verts.dtype == torch.float64
+    rt = torch.float64 if f64 else torch.float32
+    flt = Filter.detach()
+    band = ops.narrowband((flt.double() if f64 else flt.float()).contiguous(),
+                          float(narrowband_thresh)).long()
+    shape = tuple(Filter.shape)
+    n12 = shape[1] * shape[2]
+    axes = [x.detach().to(rt) for x in (xi0, xi1, xi2)]
+    xi_list = torch.stack([axes[0][band // n12], axes[1][(band // shape[2]) % shape[1]],
+                           axes[2][band % shape[2]]], dim=1).contiguous()
+    ft = ops.meshft_xi(Verts, Faces, Faces_coeff.detach().to(rt), xi_list)
+    out = torch.zeros(Filter.numel(), dtype=ft.dtype, device=ft.device)
+    return out.index_put((band,), ft).reshape(shape)

@@ -14,7 +14,8 @@ import torch
 from . import _native as N
 
 __all__ = ["FreqGrid", "narrowband", "band_is_hermitian", "band_eval_count", "band_box",
-           "topology", "meshft", "meshft_list",
+           "topology", "meshft", "meshft_list", "meshft64", "meshft64_list",
+           "meshft64_backward_list", "meshft_xi", "meshft_xi_list", "meshft_xi_backward_list",
            "meshft_backward_list", "volume_list", "volume_backward_list", "volume_ft",
            "gaussian_otf", "image_loss", "adam_step"]
 
@@ -53,18 +54,26 @@ class FreqGrid:
 # narrow band
 
 def narrowband(otf: torch.Tensor, thresh: float) -> torch.Tensor:
-    """Flat C-order indices (int32) of ``otf > thresh``; synchronises to learn the count."""
+    """Flat C-order indices (int32) of ``otf > thresh``, compared in the OTF's own
+    precision (float32 or float64); synchronises to learn the count."""
     otf = otf.detach()
-    N.require_cuda(otf, "OTF", torch.float32)
+    N.require_cuda(otf, "OTF")
+    if otf.dtype not in (torch.float32, torch.float64):
+        raise TypeError(f"OTF must be float32 or float64, not {otf.dtype}")
     otf = otf.contiguous()
     n = otf.numel()
     lib = N.lib()
     idx = torch.empty(max(n, 1), dtype=torch.int32, device=otf.device)
     cnt = torch.zeros(1, dtype=torch.int64, device=otf.device)
     ws = N.WORKSPACES.get("band", lib.dm_narrowband_workspace_size(n), otf.device)
-    N.check(lib.dm_narrowband_compact(N.ptr(otf), n, float(thresh), N.ptr(idx), N.ptr(cnt),
-                                      N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
-            "dm_narrowband_compact")
+    if otf.dtype == torch.float64:
+        N.check(lib.dm_narrowband_compact64(N.ptr(otf), n, float(thresh), N.ptr(idx),
+                                            N.ptr(cnt), N.ptr(ws), ws.numel(),
+                                            N.stream_ptr(otf.device)), "dm_narrowband_compact64")
+    else:
+        N.check(lib.dm_narrowband_compact(N.ptr(otf), n, float(thresh), N.ptr(idx), N.ptr(cnt),
+                                          N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
+                "dm_narrowband_compact")
     c = int(cnt.item())
     band = idx[:c].clone()
     flag = torch.zeros(1, dtype=torch.int32, device=otf.device)
@@ -223,6 +232,170 @@ def meshft(verts, faces, coeff, grid: FreqGrid, band) -> torch.Tensor:
 
 
 # ---------------------------------------------------------------------------
+# float32 meshFT on an explicit frequency list (split phase; any frequencies)
+
+def meshft_xi_list(verts, faces, coeff, xi_list):
+    """ft_list[n] (complex64) of the mesh (vertex coordinates as given) at the rows
+    of ``xi_list`` [n, 3] float32."""
+    _check_mesh(verts, faces, coeff)
+    N.require_cuda(xi_list, "xi_list", torch.float32)
+    lib = N.lib()
+    nv, nt, n = verts.shape[0], faces.shape[0], xi_list.shape[0]
+    ft = torch.empty(n, dtype=torch.complex64, device=verts.device)
+    ws = N.WORKSPACES.get("fwd_xi", lib.dm_meshft_forward_xi_workspace_size(nv, nt, n),
+                          verts.device)
+    N.check(lib.dm_meshft_forward_xi(N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff),
+                                     N.ptr(xi_list.contiguous()), n, N.ptr(ft), N.ptr(ws),
+                                     ws.numel(), N.stream_ptr(verts.device)),
+            "dm_meshft_forward_xi")
+    return ft
+
+
+def meshft_xi_backward_list(verts, faces, coeff, xi_list, grad_list, ft, want_coeff=True):
+    """(grad_verts, grad_coeff | None) of :func:`meshft_xi_list` for the cotangent
+    ``grad_list`` (complex64 on the list)."""
+    lib = N.lib()
+    nv, nt, n = verts.shape[0], faces.shape[0], xi_list.shape[0]
+    gv = torch.empty_like(verts)
+    gc = torch.empty_like(coeff) if want_coeff else None
+    topo = topology(faces, nv)
+    ws = N.WORKSPACES.get("bwd_xi", lib.dm_meshft_backward_xi_workspace_size(nv, nt, n),
+                          verts.device)
+    N.check(lib.dm_meshft_backward_xi(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), N.ptr(grad_list.contiguous()),
+        N.ptr(ft.contiguous()), N.ptr(xi_list.contiguous()), n, N.ptr(topo), N.ptr(gv),
+        N.ptr(gc), N.ptr(ws), ws.numel(), N.stream_ptr(verts.device)), "dm_meshft_backward_xi")
+    return gv, gc
+
+
+class _MeshFTXi(torch.autograd.Function):
+    """ft_list on an explicit frequency list (float32 or float64 by the inputs);
+    gradients for verts and coeff."""
+
+    @staticmethod
+    def forward(ctx, verts, coeff, faces, xi_list):
+        if verts.dtype == torch.float64:
+            ft = meshft64_list(verts, faces, coeff, xi_list=xi_list)
+        else:
+            ft = meshft_xi_list(verts, faces, coeff, xi_list)
+        ctx.save_for_backward(verts, coeff, faces, xi_list, ft)
+        return ft
+
+    @staticmethod
+    def backward(ctx, g):
+        verts, coeff, faces, xi_list, ft = ctx.saved_tensors
+        g = g.contiguous().to(ft.dtype)
+        want_c = ctx.needs_input_grad[1]
+        if verts.dtype == torch.float64:
+            gv, gc = meshft64_backward_list(verts, faces, coeff, ft, xi_list=xi_list,
+                                            grad_list=g, want_coeff=want_c)
+        else:
+            gv, gc = meshft_xi_backward_list(verts, faces, coeff, xi_list, g, ft,
+                                             want_coeff=want_c)
+        return gv, gc, None, None
+
+
+def meshft_xi(verts, faces, coeff, xi_list) -> torch.Tensor:
+    """Differentiable ft_list at explicit frequencies (vertex coordinates as
+    given): float32 inputs -> complex64 (split-phase kernels), float64 inputs ->
+    complex128 (float64 kernels)."""
+    if verts.dtype == torch.float64:
+        _check_mesh64(verts, faces, coeff)
+        N.require_cuda(xi_list, "xi_list", torch.float64)
+    else:
+        _check_mesh(verts, faces, coeff)
+        N.require_cuda(xi_list, "xi_list", torch.float32)
+    return _MeshFTXi.apply(verts.contiguous(), coeff.contiguous(), faces.contiguous(),
+                           xi_list.contiguous())
+
+
+# ---------------------------------------------------------------------------
+# float64 meshFT (the reference's double dispatch, fourier3d_cuda_kernel.cu:238-416)
+
+def _check_mesh64(verts, faces, coeff):
+    N.require_cuda(verts, "Verts", torch.float64)
+    N.require_cuda(faces, "Faces", torch.int64)
+    N.require_cuda(coeff, "Faces_coeff", torch.float64)
+    if verts.dim() != 2 or verts.shape[1] != 3:
+        raise ValueError("Verts must have shape [nv, 3]")
+    if faces.dim() != 2 or faces.shape[1] != 3:
+        raise ValueError("Faces must have shape [nt, 3]")
+    if coeff.shape != (faces.shape[0],):
+        raise ValueError("Faces_coeff must have shape [nt]")
+
+
+def meshft64_list(verts, faces, coeff, grid: FreqGrid = None, band=None, xi_list=None,
+                  otf=None, spectrum=None):
+    """Float64 forward: ft_list (complex128) on a grid band (``grid`` + ``band``) or
+    on an explicit ``xi_list`` [n, 3] float64 (vertex coordinates as given);
+    optionally scatters ft*otf into the complex128 ``spectrum`` (grid band only)."""
+    lib = N.lib()
+    nv, nt = verts.shape[0], faces.shape[0]
+    n = band.numel() if band is not None else xi_list.shape[0]
+    ft = torch.empty(n, dtype=torch.complex128, device=verts.device)
+    ws = N.WORKSPACES.get("fwd64", lib.dm_meshft64_forward_workspace_size(nv, nt, n),
+                          verts.device)
+    box = ctypes.byref(grid.cbox) if band is not None else None
+    N.check(lib.dm_meshft64_forward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), box, N.ptr(band), N.ptr(xi_list), n,
+        N.ptr(otf), N.ptr(ft), N.ptr(spectrum), N.ptr(ws), ws.numel(),
+        N.stream_ptr(verts.device)), "dm_meshft64_forward")
+    return ft
+
+
+def meshft64_backward_list(verts, faces, coeff, ft, grid: FreqGrid = None, band=None,
+                           xi_list=None, grad_list=None, grad_grid=None, otf=None, scale=1.0,
+                           want_coeff=True):
+    """Float64 backward: (grad_verts, grad_coeff | None) for the cotangent of
+    :func:`meshft64_list`'s result (``grad_list`` complex128 on the frequencies, or
+    ``grad_grid`` on the grid band)."""
+    lib = N.lib()
+    nv, nt = verts.shape[0], faces.shape[0]
+    n = band.numel() if band is not None else xi_list.shape[0]
+    gv = torch.empty_like(verts)
+    gc = torch.empty_like(coeff) if want_coeff else None
+    topo = topology(faces, nv)
+    ws = N.WORKSPACES.get("bwd64", lib.dm_meshft64_backward_workspace_size(nv, nt, n),
+                          verts.device)
+    box = ctypes.byref(grid.cbox) if band is not None else None
+    N.check(lib.dm_meshft64_backward(
+        N.ptr(verts), nv, N.ptr(faces), nt, N.ptr(coeff), box, N.ptr(band), N.ptr(xi_list), n,
+        N.ptr(grad_list), N.ptr(grad_grid), N.ptr(otf), float(scale), N.ptr(ft), N.ptr(topo),
+        N.ptr(gv), N.ptr(gc), N.ptr(ws), ws.numel(), N.stream_ptr(verts.device)),
+        "dm_meshft64_backward")
+    return gv, gc
+
+
+class _MeshFT64(torch.autograd.Function):
+    """Dense float64 meshFT: complex128 grid, ft on the band and 0 elsewhere."""
+
+    @staticmethod
+    def forward(ctx, verts, faces, coeff, grid, band):
+        out = torch.zeros(grid.shape, dtype=torch.complex128, device=verts.device)
+        ft = meshft64_list(verts, faces, coeff, grid, band, spectrum=out)
+        ctx.save_for_backward(verts, faces, coeff, band, ft)
+        ctx.grid = grid
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        verts, faces, coeff, band, ft = ctx.saved_tensors
+        g = g.contiguous()
+        if g.dtype != torch.complex128:
+            g = g.to(torch.complex128)
+        gv, gc = meshft64_backward_list(verts, faces, coeff, ft, ctx.grid, band, grad_grid=g,
+                                        want_coeff=ctx.needs_input_grad[2])
+        return gv, None, gc, None, None
+
+
+def meshft64(verts, faces, coeff, grid: FreqGrid, band) -> torch.Tensor:
+    """Differentiable dense float64 meshFT (gradients for verts and coeff)."""
+    _check_mesh64(verts, faces, coeff)
+    return _MeshFT64.apply(verts.contiguous(), faces.contiguous(), coeff.contiguous(), grid,
+                           band)
+
+
+# ---------------------------------------------------------------------------
 # surface + enclosed-volume transform (render.py:228-318)
 
 def volume_list(verts, faces, regint, grid: FreqGrid, band, otf=None, spectrum=None):
@@ -311,10 +484,10 @@ class _GaussianOTF(torch.autograd.Function):
     def forward(ctx, sigma, x0, x1, x2):
         lib = N.lib()
         n = (x0.numel(), x1.numel(), x2.numel())
-        otf = torch.empty(n, dtype=torch.float32, device=sigma.device)
-        N.check(lib.dm_gaussian_otf(N.ptr(sigma), N.ptr(x0), n[0], N.ptr(x1), n[1], N.ptr(x2),
-                                    n[2], N.ptr(otf), N.stream_ptr(sigma.device)),
-                "dm_gaussian_otf")
+        otf = torch.empty(n, dtype=sigma.dtype, device=sigma.device)
+        f = lib.dm_gaussian_otf64 if sigma.dtype == torch.float64 else lib.dm_gaussian_otf
+        N.check(f(N.ptr(sigma), N.ptr(x0), n[0], N.ptr(x1), n[1], N.ptr(x2), n[2], N.ptr(otf),
+                  N.stream_ptr(sigma.device)), "dm_gaussian_otf")
         ctx.save_for_backward(otf, x0, x1, x2)
         return otf
 
@@ -323,31 +496,37 @@ class _GaussianOTF(torch.autograd.Function):
         otf, x0, x1, x2 = ctx.saved_tensors
         if not ctx.needs_input_grad[0]:
             return None, None, None, None
-        return sigma_grad_dense(g.contiguous().float(), otf, x0, x1, x2), None, None, None
+        return sigma_grad_dense(g.contiguous().to(otf.dtype), otf, x0, x1, x2), None, None, None
 
 
 def sigma_grad_dense(gotf, otf, x0, x1, x2, band=None):
-    """d loss/d sigma from an OTF gradient (dense, or on ``band`` indices)."""
+    """d loss/d sigma from an OTF gradient (dense, or on ``band`` indices); in the
+    OTF's precision (float32 or float64)."""
     lib = N.lib()
     n = band.numel() if band is not None else otf.numel()
-    gs = torch.empty(3, 3, dtype=torch.float32, device=otf.device)
+    gs = torch.empty(3, 3, dtype=otf.dtype, device=otf.device)
     ws = N.WORKSPACES.get("otfgrad", lib.dm_gaussian_otf_grad_workspace_size(n), otf.device)
-    N.check(lib.dm_gaussian_otf_sigma_grad(
-        N.ptr(gotf), N.ptr(band), n, N.ptr(otf), N.ptr(x0), x0.numel(), N.ptr(x1), x1.numel(),
-        N.ptr(x2), x2.numel(), N.ptr(gs), N.ptr(ws), ws.numel(), N.stream_ptr(otf.device)),
-        "dm_gaussian_otf_sigma_grad")
+    f = (lib.dm_gaussian_otf64_sigma_grad if otf.dtype == torch.float64
+         else lib.dm_gaussian_otf_sigma_grad)
+    N.check(f(N.ptr(gotf), N.ptr(band), n, N.ptr(otf), N.ptr(x0), x0.numel(), N.ptr(x1),
+              x1.numel(), N.ptr(x2), x2.numel(), N.ptr(gs), N.ptr(ws), ws.numel(),
+              N.stream_ptr(otf.device)), "dm_gaussian_otf_sigma_grad")
     return gs
 
 
 def gaussian_otf(sigma, xi0, xi1, xi2) -> torch.Tensor:
+    """exp(-(xi^T sigma xi)/2) on the grid of the axes, differentiable in sigma;
+    float64 when sigma or the axes are float64 (the float64 kernel), else float32."""
     N.require_cuda(sigma, "sigma")
-    sigma = sigma.float().contiguous()
+    f64 = sigma.dtype == torch.float64 or xi0.dtype == torch.float64
+    rt = torch.float64 if f64 else torch.float32
+    sigma = sigma.to(rt).contiguous()
     if sigma.shape != (3, 3):
         raise ValueError("sigma must be a 3x3 matrix")
     axes = []
     for name, x in (("xi0", xi0), ("xi1", xi1), ("xi2", xi2)):
         N.require_cuda(x, name)
-        axes.append(x.detach().float().contiguous())
+        axes.append(x.detach().to(rt).contiguous())
     return _GaussianOTF.apply(sigma, *axes)
 
 

@@ -41,10 +41,8 @@ __all__ = ["generate_gaussian_psf", "generate_gaussian_psf_from_sigma", "Gaussia
 
 
 def generate_gaussian_psf(sigma, xi0, xi1, xi2):
-    """exp(-(xi^T sigma xi)/2) on the grid of the axes (float32 kernel; a float64
-    sigma or float64 axes give a float64 result with gradients to sigma)."""
-    if sigma.dtype == torch.float64 or xi0.dtype == torch.float64:
-        return ops.gaussian_otf(sigma.float(), xi0, xi1, xi2).double()
+    """exp(-(xi^T sigma xi)/2) on the grid of the axes with gradients to sigma: the
+    float64 kernel for a float64 sigma or float64 axes, else the float32 one."""
     return ops.gaussian_otf(sigma, xi0, xi1, xi2)
 
 
@@ -64,15 +62,13 @@ class Gaussian_psf(nn.Module):
         self.with_grad = with_grad
         self.dtype = dtype
         self.device = device
-        L = np.asarray(torch.as_tensor(box_size).detach().cpu().double().numpy(), np.float64)
-        self.axes = tuple(torch.linspace(-L[d] / 2, L[d] / 2, int(box_shape[d]),
-                                         dtype=torch.float32, device=device) for d in range(3))
+        self.axes = _linspace_axes(box_shape, box_size, device, _real(dtype))
         self.sigma = nn.Parameter(torch.tensor(np.identity(3) * sigma, dtype=dtype,
                                                device=device), requires_grad=with_grad)
 
     def forward(self):
-        out = ops.gaussian_otf(self.sigma.float(), *self.axes)
-        return out.to(self.dtype) if self.dtype != torch.float32 else out
+        # float64 parameters run the float64 kernel, anything else the float32 one
+        return ops.gaussian_otf(self.sigma.to(_real(self.dtype)), *self.axes)
 
 
 class _OTFfromPSF(torch.autograd.Function):
@@ -111,9 +107,13 @@ def _cuda_only(device, name):
         raise RuntimeError(f"deltamic_b200.{name} runs on CUDA devices only")
 
 
-def _linspace_axes(box_shape, box_size, device):
+def _real(dtype):
+    return torch.float64 if dtype == torch.float64 else torch.float32
+
+
+def _linspace_axes(box_shape, box_size, device, dtype=torch.float32):
     L = np.asarray(torch.as_tensor(box_size).detach().cpu().double().numpy(), np.float64)
-    return tuple(torch.linspace(-L[d] / 2, L[d] / 2, int(box_shape[d]), dtype=torch.float32,
+    return tuple(torch.linspace(-L[d] / 2, L[d] / 2, int(box_shape[d]), dtype=dtype,
                                 device=device) for d in range(3))
 
 
@@ -129,14 +129,13 @@ class Gaussian_psf_logsigma(nn.Module):
         self.with_grad = with_grad
         self.dtype = dtype
         self.device = device
-        self.axes = _linspace_axes(box_shape, box_size, device)
+        self.axes = _linspace_axes(box_shape, box_size, device, _real(dtype))
         self.logsigma = nn.Parameter(torch.tensor(np.identity(3) * np.log(sigma), dtype=dtype,
                                                   device=device), requires_grad=with_grad)
 
     def forward(self):
         self.sigma = torch.exp(self.logsigma)
-        out = ops.gaussian_otf(self.sigma.float(), *self.axes)
-        return out.to(self.dtype) if self.dtype != torch.float32 else out
+        return ops.gaussian_otf(self.sigma.to(_real(self.dtype)), *self.axes)
 
 
 class _AnisoPSF(torch.autograd.Function):

@@ -18,11 +18,11 @@ Same names, arguments and results as the reference:
   reference.
 
 Differences, all deliberate: the module runs on CUDA only (``device='cpu'``
-raises -- there is no CPU fallback); the kernels compute in float32 (with the
-fixed-point phases their error against a float64 evaluation is ~1e-6), so a
-``dtype=torch.float64`` module casts its inputs to float32 and returns a
-complex128 spectrum whose gradients flow back to the float64 inputs; the box
-used for the phases is kept in float64.  In the autofluorescence transform the
+raises -- there is no CPU fallback).  ``dtype=torch.float32`` runs the float32
+kernels (fixed-point phases; error against a float64 evaluation ~1e-6);
+``dtype=torch.float64`` runs the float64 kernels (the reference's double
+arithmetic, Seps = sqrt(DBL_EPSILON), band selected on the float64 OTF) and
+returns complex128.  In the autofluorescence transform the
 reference's value at xi = 0 (grids with every axis odd) is 0/0 = NaN; here it is
 the limit of its volume term, ``1 - regint`` in all.
 """
@@ -138,14 +138,16 @@ class Fourier3dMesh(nn.Module):
         if key != self._band_key or self._band is None:
             if tuple(otf.shape) != tuple(self.box_shape):
                 raise ValueError("OTF must have shape box_shape")
-            self._band = ops.narrowband(otf.detach().float().contiguous(), thr)
+            o = otf.detach()
+            o = o.double() if self.dtype == torch.float64 else o.float()
+            self._band = ops.narrowband(o.contiguous(), thr)
             self._band_key = key
         return self._band
 
     def forward(self, Verts, Faces, Faces_coeff):
         if self.dtype == torch.float64:
-            ft = ops.meshft(Verts.float(), Faces, Faces_coeff.float(), self.grid, self.band())
-            return ft.to(torch.complex128)
+            return ops.meshft64(Verts.double(), Faces, Faces_coeff.double(), self.grid,
+                                self.band())
         return ops.meshft(Verts, Faces, Faces_coeff, self.grid, self.band())
 
 
@@ -215,8 +217,9 @@ def fourier_from_mesh_narrowband_autofluorescence(OTF, narrowband_thresh, regint
     ``sum_k F_k (2 A_k / sum A + i (regint / regvol) xi . nor_k / |xi|^2)``.
 
     Vertex coordinates enter as given.  Gradients flow to ``Verts`` and to
-    ``regint`` when it is a tensor.  A float64 ``Verts`` is evaluated in float32
-    and returns complex128, as ``Fourier3dMesh(dtype=float64)`` does."""
+    ``regint`` when it is a tensor.  The transform runs on the float32 kernels
+    only: a float64 ``Verts`` raises ``TypeError`` (no silent change of
+    precision)."""
     shape = (int(xi0.numel()), int(xi1.numel()), int(xi2.numel()))
     if tuple(OTF.shape) != shape:
         raise ValueError(f"OTF shape {tuple(OTF.shape)} does not match the axes {shape}")
@@ -231,6 +234,7 @@ def fourier_from_mesh_narrowband_autofluorescence(OTF, narrowband_thresh, regint
         band = ops.narrowband(OTF.detach().float().contiguous(), thr)
         _AUTO_BANDS.clear()
         _AUTO_BANDS[id(OTF)] = (key, band)
-    f64 = Verts.dtype == torch.float64
-    out = ops.volume_ft(Verts.float() if f64 else Verts, Faces, regint, grid, band)
-    return out.to(torch.complex128) if f64 else out
+    if Verts.dtype != torch.float32:
+        raise TypeError("fourier_from_mesh_narrowband_autofluorescence runs in float32 "
+                        f"(got Verts of {Verts.dtype})")
+    return ops.volume_ft(Verts, Faces, regint, grid, band)

@@ -39,6 +39,7 @@ typedef struct CUstream_st* dm_stream_t; /* == cudaStream_t */
 #define DM_ERR_CUDA 16         /* a CUDA launch or copy failed */
 #define DM_ERR_TIMEOUT 32      /* a bounded device wait gave up */
 #define DM_ERR_UNSUPPORTED 64  /* valid request this build does not serve */
+#define DM_ERR_NONFINITE 128   /* a vertex coordinate is NaN or infinite (device status word) */
 
 /* Box of a meshFT grid: box_size (render.py:116-123) and box_shape, plus the
  * properties of the narrow band passed with it. */
@@ -81,6 +82,12 @@ size_t dm_narrowband_workspace_size(int64_t n_voxels);
 int dm_narrowband_compact(const float* otf, int64_t n_voxels, float thresh,
                           int32_t* band_index, int64_t* band_count, void* workspace,
                           size_t ws_bytes, dm_stream_t stream);
+
+/* The same selection on a float64 OTF (Fourier3dMesh(dtype=torch.float64)): the
+ * comparison otf > thresh in double; workspace from dm_narrowband_workspace_size. */
+int dm_narrowband_compact64(const double* otf, int64_t n_voxels, double thresh,
+                            int32_t* band_index, int64_t* band_count, void* workspace,
+                            size_t ws_bytes, dm_stream_t stream);
 
 /* Asynchronous: *is_hermitian (DEVICE int32) = 1 if band_index[0..n_band) (of a
  * grid of n_voxels) is closed under xi -> -xi in the sense of DM_BAND_HERMITIAN,
@@ -154,6 +161,69 @@ int dm_meshft_backward(const float* verts, int64_t nv, const int64_t* faces, int
                        const void* topology, float* grad_verts, float* grad_coeff,
                        float* grad_otf_band, void* workspace, size_t ws_bytes,
                        dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * meshFT on an explicit frequency list, float32: the reference FFI itself,
+ * forward_fourier3d_cpp(Verts, Faces, Faces_coeff, xi_list) and
+ * backward_fourier3d_cpp(Verts, Faces, Faces_coeff, grad_output_list,
+ * ftmesh_list, xi_list) for scalar_t = float (deltamic/cpp/fourier3d_cuda.cpp:
+ * 27-65, :112-115; kernels .cu:281-416).
+ *   verts[nv,3] as given (no box shift: the caller passes Verts - box_size[:,0]
+ *   as MeshFTCUDA does), faces[nt,3] int64, faces_coeff[nt], xi_list[n_xi,3] float32
+ *   (any frequencies, on a grid or not).
+ * forward writes ftmesh_list[n_xi] (complex64) = (2/M) sum_k A_k c_k F_k(xi).
+ * backward takes grad_output_list[n_xi] (complex64, PyTorch convention) and the
+ * forward's ftmesh_list, and writes grad_verts[nv,3] and, if not NULL,
+ * grad_coeff[nt] (the reference returns only the vertex gradient).  topology
+ * from dm_topology_build or NULL (built in the workspace).
+ * Phases: the cell has lower corner 0 and length 2.5 max|v_d| per axis (found on
+ * the device); each xi_d becomes m_d = xi_d L_d / pi, whose nearest integer
+ * enters the exact 32-bit fixed-point phase and whose remainder a float term
+ * below 3/8 of a turn (split phase).  A frequency with |m_d| >= 2^30 sets
+ * DM_ERR_SIZE and a non-finite vertex DM_ERR_NONFINITE in the status word. */
+size_t dm_meshft_forward_xi_workspace_size(int64_t nv, int64_t nt, int64_t n_xi);
+int dm_meshft_forward_xi(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                         const float* faces_coeff, const float* xi_list, int64_t n_xi,
+                         float* ftmesh_list, void* workspace, size_t ws_bytes,
+                         dm_stream_t stream);
+size_t dm_meshft_backward_xi_workspace_size(int64_t nv, int64_t nt, int64_t n_xi);
+int dm_meshft_backward_xi(const float* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                          const float* faces_coeff, const float* grad_output_list,
+                          const float* ftmesh_list, const float* xi_list, int64_t n_xi,
+                          const void* topology, float* grad_verts, float* grad_coeff,
+                          void* workspace, size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * meshFT in float64: the double-precision dispatch of forward_fourier3d_cpp /
+ * backward_fourier3d_cpp (deltamic/cpp/fourier3d_cuda.cpp:27-65; kernels
+ * .cu:238-416 for scalar_t = double, Seps = sqrt(DBL_EPSILON), .cu:454, :522),
+ * i.e. Fourier3dMesh(dtype=torch.float64) on CUDA.  Same arithmetic as the
+ * reference (phases xi . v in double, its R1..R5 branches), every frequency
+ * evaluated (band_flags ignored).  Frequencies come from exactly one source:
+ *   - a grid band: box and band_index[n_freq] as for dm_meshft_forward (vertices
+ *     shifted by box.lo inside, as Fourier3dMesh.forward does); or
+ *   - a list: xi_list[n_freq,3] float64 with box NULL (vertices as given, as
+ *     forward_fourier3d_cpp takes them).
+ * verts[nv,3], faces_coeff[nt] float64; ft_list[n_freq] complex128 (interleaved
+ * doubles); grid (grid band only, optional) receives ft * otf at the band's voxels.
+ * The backward's cotangent is g[m] = grad_scale * G[m] * (otf ? otf[idx] : 1)
+ * with G from grad_list[n_freq] (complex128) or grad_grid (grid band only); it
+ * writes grad_verts[nv,3] and, if not NULL, grad_coeff[nt] (float64); topology
+ * from dm_topology_build or NULL. */
+size_t dm_meshft64_forward_workspace_size(int64_t nv, int64_t nt, int64_t n_freq);
+int dm_meshft64_forward(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                        const double* faces_coeff, const dm_box* box, const int32_t* band_index,
+                        const double* xi_list, int64_t n_freq, const double* otf,
+                        double* ft_list, double* grid, void* workspace, size_t ws_bytes,
+                        dm_stream_t stream);
+size_t dm_meshft64_backward_workspace_size(int64_t nv, int64_t nt, int64_t n_freq);
+int dm_meshft64_backward(const double* verts, int64_t nv, const int64_t* faces, int64_t nt,
+                         const double* faces_coeff, const dm_box* box,
+                         const int32_t* band_index, const double* xi_list, int64_t n_freq,
+                         const double* grad_list, const double* grad_grid, const double* otf,
+                         double grad_scale, const double* ft_list, const void* topology,
+                         double* grad_verts, double* grad_coeff, void* workspace,
+                         size_t ws_bytes, dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Surface + enclosed-volume ("autofluorescence") transform.  Replaces
@@ -356,6 +426,18 @@ int dm_gaussian_otf_sigma_grad(const float* grad_otf, const int32_t* band_index,
                                const float* otf, const float* xi0, int32_t n0, const float* xi1,
                                int32_t n1, const float* xi2, int32_t n2, float* grad_sigma,
                                void* workspace, size_t ws_bytes, dm_stream_t stream);
+
+/* The same two calls in float64 (generate_gaussian_psf on float64 sigma and axes,
+ * Fourier3dMesh(dtype=torch.float64)): the reference expression's operation
+ * order in double; workspace from dm_gaussian_otf_grad_workspace_size. */
+int dm_gaussian_otf64(const double* sigma, const double* xi0, int32_t n0, const double* xi1,
+                      int32_t n1, const double* xi2, int32_t n2, double* otf,
+                      dm_stream_t stream);
+int dm_gaussian_otf64_sigma_grad(const double* grad_otf, const int32_t* band_index,
+                                 int64_t n_band, const double* otf, const double* xi0, int32_t n0,
+                                 const double* xi1, int32_t n1, const double* xi2, int32_t n2,
+                                 double* grad_sigma, void* workspace, size_t ws_bytes,
+                                 dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Fused image stage on the inverse FFT z = ifftn(ftmesh * OTF) (complex64[n]):

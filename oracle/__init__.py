@@ -16,7 +16,7 @@ from .meshft import (SEPS_F32, SEPS_F64, face_areas, pair_F, pair_F_and_grads,
                      meshft_forward, meshft_backward)
 from .render import (frequency_axes, gaussian_otf, band_indices, xi_list_from_band,
                      render_from_band, normalize, image_loss, image_loss_backward,
-                     pipeline, chain_floor, compute_box_size)
+                     pipeline, chain_floor, compute_box_size, smooth_target)
 from . import fit
 
 __all__ = [
@@ -24,4 +24,5 @@ __all__ = [
     "meshft_forward", "meshft_backward", "frequency_axes", "gaussian_otf",
     "band_indices", "xi_list_from_band", "render_from_band", "normalize",
     "image_loss", "image_loss_backward", "pipeline", "chain_floor", "compute_box_size", "fit",
+    "smooth_target",
 ]

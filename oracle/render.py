@@ -175,3 +175,14 @@ def chain_floor(verts, faces, coeff, box_size, box_shape, sigma, thresh, loss="s
                                    rl(o["grad_coeff"], base["grad_coeff"]),
                                    rl(o["grad_sigma"], base["grad_sigma"])])
     return dict(verts=float(worst[0]), coeff=float(worst[1]), sigma=float(worst[2]))
+
+
+def smooth_target(box_shape, seed, width=0.15, noise=0.05):
+    """Deterministic target image for image-L2 losses: a Gaussian blob at the box
+    centre (width relative to the box) plus N(0, noise^2) voxel noise from
+    numpy's PCG64 with ``seed``; float64, the same array on every machine."""
+    u = [np.arange(n, dtype=np.float64) / max(n - 1, 1) - 0.5 for n in box_shape]
+    r2 = u[0][:, None, None] ** 2 + u[1][None, :, None] ** 2 + u[2][None, None, :] ** 2
+    t = np.exp(-r2 / (2.0 * width * width))
+    rng = np.random.default_rng(seed)
+    return t + noise * rng.standard_normal(tuple(box_shape))

@@ -18,13 +18,13 @@ def pytest_configure(config):
 
 
 def golden_cases(prefix=""):
-    """Fixture names under tests/golden: the surface-transform cases (no prefix:
-    every file not starting with ``volume_`` or ``psf_``) or those starting with
-    ``prefix``."""
+    """Fixture names under tests/golden: the small surface-transform cases (no
+    prefix: every file not starting with ``volume_``, ``psf_`` or ``cfg``, the
+    benchmark-configuration cases) or those starting with ``prefix``."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
     if prefix:
         return [n for n in names if n.startswith(prefix)]
-    return [n for n in names if not n.startswith(("volume_", "psf_"))]
+    return [n for n in names if not n.startswith(("volume_", "psf_", "cfg"))]
 
 
 def load_golden(name):

@@ -62,4 +62,41 @@ void dm_host_pairs(const double* verts, const int64_t* faces, int64_t nt, const 
   }
 }
 
+// The same outputs for frequencies off the grid (explicit xi list): the cell has
+// lower corner 0 and lengths len[3] (the device takes 2.5 max|v_d|), each xi
+// becomes m = xi L / pi split into its nearest integer and the remainder, as the
+// list kernels' record builder does.  xi[nxi*3] double.
+void dm_host_pairs_off(const double* verts, const int64_t* faces, int64_t nt, const double* xi,
+                       int64_t nxi, const float* gc, const double* len, float* F, float* z,
+                       float* r, uint8_t* cls) {
+  const double lo[3] = {0.0, 0.0, 0.0};
+  for (int64_t k = 0; k < nt; ++k) {
+    const FaceGeom g = make_geom(verts + 3 * faces[3 * k], verts + 3 * faces[3 * k + 1],
+                                 verts + 3 * faces[3 * k + 2], lo, len);
+    for (int64_t i = 0; i < nxi; ++i) {
+      XiValOff xv;
+      for (int d = 0; d < 3; ++d) {
+        const double m = xi[3 * i + d] * len[d] / M_PI;
+        const double mi = std::rint(m);
+        xv.mi[d] = (int32_t)mi;
+        xv.mf[d] = (float)m;
+        xv.fr[d] = (float)(m - mi);
+      }
+      const int64_t o = i * nt + k;
+      float hab, hbc, hca;
+      half_diffs(xv.mf, g, hab, hbc, hca);
+      cls[o] = (uint8_t)pair_class(hab, hbc, hca);
+      c32 Fv;
+      if (!pair_forward(xv, g, Fv)) Fv = pair_forward_degenerate(xv, g);
+      F[2 * o] = Fv.x;
+      F[2 * o + 1] = Fv.y;
+      float zz[3], rr;
+      if (!pair_adjoint(xv, g, gc[2 * i], gc[2 * i + 1], zz, rr))
+        pair_adjoint_degenerate(xv, g, gc[2 * i], gc[2 * i + 1], zz, rr);
+      for (int v = 0; v < 3; ++v) z[3 * o + v] = zz[v];
+      r[o] = rr;
+    }
+  }
+}
+
 }  // extern "C"

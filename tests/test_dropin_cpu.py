@@ -25,13 +25,27 @@ def test_meshftcuda_refuses_cpu_tensors():
                          torch.ones(len(f)), *xi, otf, 0.5)
 
 
-def test_meshftcuda_rejects_axes_off_the_centred_grid():
+def test_meshftcuda_off_grid_axes_refuse_cpu_tensors():
+    """Axes that are not centred grids take the explicit-list path; on CPU tensors
+    it refuses as loudly as the grid path (there is no CPU path)."""
     v, f = icosphere(1, 0.3)
     xi = list(compute_spatial_frequency_grid((8, 8, 8), [1.0, 1.0, 1.0]))
     xi[1] = xi[1] ** 2  # not (2k - (n-1)) pi / L
-    with pytest.raises(ValueError, match="centred"):
+    with pytest.raises(RuntimeError, match="CUDA"):
         MeshFTCUDA.apply(torch.tensor(v, dtype=torch.float32), torch.tensor(f),
                          torch.ones(len(f)), *xi, torch.ones(8, 8, 8), 0.5)
+
+
+def test_fourier3d_cpp_shims_refuse_cpu_tensors():
+    from deltamic_b200.fourier3d_cpp import backward_fourier3d_cpp, forward_fourier3d_cpp
+    v, f = icosphere(1, 0.3)
+    V, F = torch.tensor(v, dtype=torch.float32), torch.tensor(f)
+    C, X = torch.ones(len(f)), torch.zeros(4, 3)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        forward_fourier3d_cpp(V, F, C, X)
+    g = torch.zeros(4, dtype=torch.complex64)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        backward_fourier3d_cpp(V, F, C, g, g, X)
 
 
 def test_vector_adam_refuses_cpu_parameters():

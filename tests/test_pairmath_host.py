@@ -92,3 +92,39 @@ def test_pair_math_degenerate_branches(hostlib):
     m = (2 * k - (np.array(shape) - 1)).astype(np.int32)
     cls = _check(hostlib, d["verts"], d["faces"], m, box, shape, 1e-6, 2e-6)
     assert (cls == 2).mean() > 0.01
+
+
+@pytest.mark.parametrize("scale,shift", [(30.0, (0.0, 0.0, 0.0)), (150.0, (0.9, -0.4, 2.0)),
+                                         (600.0, (-3.0, 1.0, 0.5))])
+def test_split_phase_off_grid_matches_oracle(hostlib, scale, shift):
+    """Off-grid frequencies (explicit xi list): nearest-integer fixed-point phase
+    plus the float remainder term, on raw vertex coordinates (lower corner 0,
+    length 2.5 max|v|), against the oracle's phases xi . v."""
+    rng = np.random.default_rng(3)
+    v, f = icosphere(3, 0.3)
+    v, _ = sh_perturb(v, 4, 0.08, rng, radius=0.3)
+    v = v + np.asarray(shift)
+    f = f[rng.choice(len(f), 256, replace=False)]
+    xi = rng.normal(size=(500, 3)) * scale
+    L = 2.5 * np.abs(v).max(axis=0)
+    g = rng.normal(size=len(xi)) + 1j * rng.normal(size=len(xi))
+    n, nt = len(xi), len(f)
+    F = np.zeros((n, nt, 2), np.float32)
+    z = np.zeros((n, nt, 3), np.float32)
+    r = np.zeros((n, nt), np.float32)
+    cls = np.zeros((n, nt), np.uint8)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    vv, ff = np.ascontiguousarray(v, np.float64), np.ascontiguousarray(f, np.int64)
+    xx = np.ascontiguousarray(xi, np.float64)
+    gg = np.ascontiguousarray(np.stack([g.real, g.imag], 1), np.float32)
+    LL = np.ascontiguousarray(L, np.float64)
+    hostlib.dm_host_pairs_off(P(vv), P(ff), ctypes.c_int64(nt), P(xx), ctypes.c_int64(n), P(gg),
+                              P(LL), P(F), P(z), P(r), P(cls))
+    Fc = F[..., 0] + 1j * F[..., 1]
+    xiv = xi @ v.T
+    F0, dF = oracle.pair_F_and_grads(xiv[:, f[:, 0]], xiv[:, f[:, 1]], xiv[:, f[:, 2]])
+    cg = np.conj(g)[:, None]
+    z0 = np.stack([np.real(cg * d) for d in dF], axis=2)
+    eF = np.linalg.norm(Fc - F0) / np.linalg.norm(F0)
+    ez = np.linalg.norm(z - z0) / np.linalg.norm(z0)
+    assert eF < 2e-6 and ez < 4e-6, (eF, ez)
