@@ -158,6 +158,7 @@ SIGNATURES = {
     "dm_set_variants": (_INT, [_INT, _INT]),
     "dm_get_variants": (_INT, [ctypes.POINTER(_INT)] * 4),
     "dm_peak_probe": (_INT, [_INT, _INT, ctypes.POINTER(ctypes.c_double), _P]),
+    "dm_selftest_bounded_wait": (_INT, [_INT, ctypes.c_uint32, _P, _P]),
     "dm_profile_enable": (_INT, [_INT]),
     "dm_profile_read": (_INT, [_INT, ctypes.POINTER(_INT), ctypes.POINTER(_F)]),
 }

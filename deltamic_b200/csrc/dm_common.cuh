@@ -165,16 +165,18 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t pari
 constexpr uint32_t kSleepTries = 1u << 16;
 constexpr uint32_t kSleepNs = 20000;
 __device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t* bar, uint32_t parity,
-                                                        int* err) {
-  for (uint32_t i = 0; i < kSleepTries; ++i)
+                                                        int* err,
+                                                        uint32_t tries = kSleepTries) {
+  for (uint32_t i = 0; i < tries; ++i)
     if (mbar_try_wait_sleep(bar, parity, kSleepNs)) return true;
   set_error(err, DM_ERR_TIMEOUT);
   return false;
 }
 
 constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err,
+                                                  uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   set_error(err, DM_ERR_TIMEOUT);
   return false;

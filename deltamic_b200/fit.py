@@ -3,6 +3,14 @@
 
 ``FitStep`` runs one iteration -- fused render + loss (``MeshRenderer``), adjoint,
 Adam -- entirely on the GPU and, by default, replays it as one captured CUDA graph.
+
+Checkpoints: ``FitStep.state_dict()`` / ``load_state_dict()`` hold the fit state
+(vertices, Adam moments, step count, learning rate and betas), and
+``save_fit_state`` / ``load_fit_state`` write and read it with ``torch.save``
+together with the Faces_coeff and PSF sigma of the run (the reference notebook
+saves the mesh with ``np.savez`` every 100 iterations,
+Examples/Gradient_Descent.ipynb cell 2).  Loading copies into the step's own
+tensors, so a captured graph keeps working.
 """
 from __future__ import annotations
 
@@ -12,7 +20,63 @@ from . import _native as N
 from . import ops
 from .pipeline import MeshRenderer
 
-__all__ = ["FitStep", "fit_mesh", "run_fit", "mesh_iou"]
+__all__ = ["FitStep", "fit_mesh", "run_fit", "mesh_iou", "fit_state_dict",
+           "load_fit_state_dict", "save_fit_state", "load_fit_state"]
+
+_STATE_TENSORS = (("verts", "V"), ("adam_m", "m"), ("adam_v", "v"), ("step", "t"))
+
+
+def fit_state_dict(step) -> dict:
+    """CPU copies of a fit step's state: ``verts``, ``adam_m``, ``adam_v`` (per
+    vertex for VectorAdam), ``step`` and the optimiser settings."""
+    out = {k: getattr(step, a).detach().cpu().clone() for k, a in _STATE_TENSORS}
+    out.update(lr=float(step.lr), betas=tuple(float(b) for b in step.betas), eps=float(step.eps),
+               optimizer=str(step.optimizer))
+    return out
+
+
+def load_fit_state_dict(step, state: dict) -> None:
+    """Copy a state from :func:`fit_state_dict` into the step's tensors in place
+    (shapes must match; a graph captured on those tensors replays the loaded
+    state)."""
+    if str(state.get("optimizer", step.optimizer)) != str(step.optimizer):
+        raise ValueError(f"state is for optimizer {state['optimizer']!r}, step uses "
+                         f"{step.optimizer!r}")
+    for k, a in _STATE_TENSORS:
+        dst, src = getattr(step, a), state[k]
+        if tuple(src.shape) != tuple(dst.shape):
+            raise ValueError(f"{k}: state has shape {tuple(src.shape)}, step {tuple(dst.shape)}")
+    settings = (float(state.get("lr", step.lr)), tuple(float(b) for b in
+                state.get("betas", step.betas)), float(state.get("eps", step.eps)))
+    if getattr(step, "graph", None) is not None and settings != (
+            float(step.lr), tuple(float(b) for b in step.betas), float(step.eps)):
+        # the captured graph holds the optimiser settings as launch arguments
+        raise ValueError("the state's lr/betas/eps differ from this captured step's; "
+                         "build the FitStep with the saved settings, then load")
+    for k, a in _STATE_TENSORS:
+        dst = getattr(step, a)
+        dst.copy_(state[k].to(device=dst.device, dtype=dst.dtype))
+    step.lr, step.betas, step.eps = settings
+
+
+def save_fit_state(path, step, faces_coeff=None, sigma=None, **extra) -> None:
+    """torch.save of the fit state, the run's Faces_coeff and sigma, and ``extra``."""
+    state = fit_state_dict(step)
+    if faces_coeff is not None:
+        state["faces_coeff"] = faces_coeff.detach().cpu().clone()
+    if sigma is not None:
+        state["sigma"] = torch.as_tensor(sigma).detach().cpu().clone()
+    state["extra"] = dict(extra)
+    torch.save(state, path)
+
+
+def load_fit_state(path, step=None) -> dict:
+    """Read a file of :func:`save_fit_state`; with ``step``, load it into the step.
+    Returns the saved dict (faces_coeff, sigma and extra included)."""
+    state = torch.load(path, map_location="cpu", weights_only=False)
+    if step is not None:
+        load_fit_state_dict(step, state)
+    return state
 
 
 class FitStep:
@@ -108,6 +172,12 @@ class FitStep:
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             self._body()
+
+    def state_dict(self) -> dict:
+        return fit_state_dict(self)
+
+    def load_state_dict(self, state: dict) -> None:
+        load_fit_state_dict(self, state)
 
     def __call__(self):
         if self.graph is not None:

@@ -24,7 +24,7 @@ from .batch import BatchRenderer
 from .mesh import icosphere, real_sph_harm
 
 __all__ = ["LearnedInit", "conv3d_s2", "conv_status_check", "ShapeSampler", "render_batch",
-           "train_learned_init"]
+           "train_learned_init", "save_checkpoint", "load_checkpoint"]
 
 CHANNELS = (1, 16, 32, 64, 128)
 IMAGE = 64
@@ -298,3 +298,33 @@ def evaluate_learned_init(model, sampler, n_eval=256, steps=300, lr=1e-3, seed=1
     res.update(ms_step_per_shape=ms_step, ms_infer_per_shape=ms_infer,
                time_ratio=t_learned / t_plain, steps=steps)
     return res
+
+
+def save_checkpoint(path, model: LearnedInit, optimizer=None, scheduler=None, **extra) -> None:
+    """torch.save of the network (weights, n_verts), the optimiser and scheduler
+    states when given, and ``extra`` (epoch, losses, ...)."""
+    state = {"model": model.state_dict(), "n_verts": int(model.n_verts),
+             "hidden": int(model.fc1.out_features), "extra": dict(extra)}
+    if optimizer is not None:
+        state["optimizer"] = optimizer.state_dict()
+    if scheduler is not None:
+        state["scheduler"] = scheduler.state_dict()
+    torch.save(state, path)
+
+
+def load_checkpoint(path, model: LearnedInit = None, optimizer=None, scheduler=None,
+                    device=None):
+    """Read a file of :func:`save_checkpoint` into ``model`` (a new LearnedInit of
+    the saved size when None, on ``device``) and the optimiser / scheduler when
+    given; returns ``(model, extra)``."""
+    state = torch.load(path, map_location="cpu", weights_only=False)
+    if model is None:
+        model = LearnedInit(n_verts=state["n_verts"], hidden=state["hidden"])
+    model.load_state_dict(state["model"])
+    if device is not None:
+        model = model.to(device)
+    if optimizer is not None and "optimizer" in state:
+        optimizer.load_state_dict(state["optimizer"])
+    if scheduler is not None and "scheduler" in state:
+        scheduler.load_state_dict(state["scheduler"])
+    return model, state["extra"]

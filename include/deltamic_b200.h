@@ -572,10 +572,20 @@ long long dm_launch_count(void);
 int dm_set_variants(int fwd, int bwd);
 int dm_get_variants(int* fwd, int* bwd, int* n_fwd, int* n_bwd);
 
+/* Self-test of the library's bounded device waits (no counterpart in the
+ * reference): one block waits on an mbarrier that nothing completes -- with the
+ * spinning wait (mode 0, at most limit <= 2^22 polls) or the sleeping wait of the
+ * persistent kernels (mode 1, at most limit <= 2^16 tries of 20 us) -- gives up,
+ * ORs DM_ERR_TIMEOUT into *status (DEVICE int, caller-zeroed) and returns, leaving
+ * the context usable.  Shows that a wait that never completes ends the kernel
+ * with a status instead of hanging it. */
+int dm_selftest_bounded_wait(int mode, uint32_t limit, int* status, dm_stream_t stream);
+
 /* Throughput probe (no counterpart in the reference): times ``iters`` rounds of
- * 8 independent FP32 FMA chains (kind 0) or MUFU sin.approx chains (kind 1) per
- * thread over the whole GPU and returns instructions per second.  Synchronous;
- * these are the roofline denominators for the FP32/MUFU-bound meshFT kernels. */
+ * 8 independent FP32 FMA chains (kind 0), MUFU sin.approx chains (kind 1) or
+ * paired FP32 FMA chains (kind 2, sm_100 FFMA2) per thread over the whole GPU and
+ * returns FMAs (kinds 0, 2) or sines (kind 1) per second.  Synchronous; these
+ * are the roofline denominators for the FP32/MUFU-bound meshFT kernels. */
 int dm_peak_probe(int kind, int iters, double* ops_per_s, dm_stream_t stream);
 int dm_profile_enable(int enable);
 int dm_profile_read(int kernel, int* count, float* total_ms);

@@ -81,12 +81,20 @@ def test_network_gradients_match_float32_reference():
         assert rel_l2(m.b[i].grad.cpu().numpy(), bs[i].grad.cpu().numpy()) < 5e-2, i
 
 
-def test_trained_network_beats_sphere_initialisation():
+@pytest.fixture(scope="module")
+def trained():
+    """A network trained briefly on 8,192 renderer-generated pairs (12 epochs)."""
+    from deltamic_b200.learned import train_learned_init
+    model, sampler, hist = train_learned_init(n_train=8192, epochs=12, batch=64, lr=2e-3,
+                                              seed=1, device=DEV)
+    return model, sampler, hist
+
+
+def test_trained_network_beats_sphere_initialisation(trained):
     """A briefly trained network predicts held-out shapes far better than the
     template sphere the plain fit starts from."""
-    from deltamic_b200.learned import render_batch, train_learned_init
-    model, sampler, hist = train_learned_init(n_train=2048, epochs=12, batch=64, lr=2e-3, seed=1,
-                                              device=DEV)
+    from deltamic_b200.learned import render_batch
+    model, sampler, hist = trained
     assert hist[-1] < 0.5 * hist[0]
     rng = np.random.default_rng(999)
     v, sig = sampler.sample(32, rng)
@@ -99,3 +107,22 @@ def test_trained_network_beats_sphere_initialisation():
     err_sphere = float(torch.sqrt(torch.mean((tmpl - gt) ** 2)))
     print(f"vertex RMSE: learned {err_learned:.4f} sphere {err_sphere:.4f}")
     assert err_learned < 0.7 * err_sphere
+
+
+def test_learned_init_time_to_fit_and_iou(trained):
+    """Held-out shapes: learned init + GD reaches the plain sphere-init fit's final
+    image L2 (within 1%) in under a quarter of the plain fit's time (network
+    inference included), with a volumetric IoU against the generating mesh of at
+    least 0.95 at that point (medians over 32 shapes)."""
+    from deltamic_b200.learned import evaluate_learned_init
+    model, sampler, _ = trained
+    res = evaluate_learned_init(model, sampler, n_eval=32, steps=300, lr=1e-3, seed=4321,
+                                device=DEV, chunk=32)
+    ratio = float(np.median(res["time_ratio"]))
+    iou_t = float(np.median(res["iou_learned_at_target"]))
+    print(f"learned init: median time ratio {ratio:.3f} (p90 "
+          f"{np.percentile(res['time_ratio'], 90):.3f}), reached {res['reached'].mean():.2f}, "
+          f"median IoU at target {iou_t:.3f}, plain final IoU {np.median(res['iou_plain']):.3f}")
+    assert res["reached"].mean() >= 0.9
+    assert ratio < 0.25
+    assert iou_t >= 0.95
