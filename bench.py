@@ -138,6 +138,7 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.nvml = []          # (sm MHz, max MHz, reason bits)
+        self.nvml_error = None
         self._stop = threading.Event()
         self._nv_thread = None
 
@@ -146,17 +147,28 @@ class ClockSampler:
             import pynvml as nv
             nv.nvmlInit()
             try:
-                h = (nv.nvmlDeviceGetHandleByPciBusId_v2(self.pci) if self.pci
-                     else nv.nvmlDeviceGetHandleByIndex(self.gpu))
+                h = None
+                if self.pci:
+                    try:
+                        h = nv.nvmlDeviceGetHandleByPciBusId_v2(self.pci)
+                    except Exception as e:  # fall back to the index below
+                        self.nvml_error = f"by PCI bus id {self.pci}: {e}"
+                if h is None:
+                    h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
                 smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                try:
+                    reasons = nv.nvmlDeviceGetCurrentClocksEventReasons
+                    reasons(h)
+                except Exception:
+                    reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons
                 while not self._stop.is_set():
                     self.nvml.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
-                                      nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                                      reasons(h)))
                     time.sleep(0.002)
             finally:
                 nv.nvmlShutdown()
-        except Exception:  # no NVML: the nvidia-smi samples remain
-            pass
+        except Exception as e:  # no NVML: the nvidia-smi samples remain
+            self.nvml_error = f"{type(e).__name__}: {e}"
 
     def start(self):
         self._nv_thread = threading.Thread(target=self._nvml_loop, daemon=True)
@@ -211,9 +223,12 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
-                "reasons": sorted(reasons), "samples": len(sm), "nvml_samples": len(self.nvml),
-                "smi_samples": n_smi}
+        out = {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+               "reasons": sorted(reasons), "samples": len(sm), "nvml_samples": len(self.nvml),
+               "smi_samples": n_smi}
+        if self.nvml_error:
+            out["nvml_error"] = self.nvml_error[:200]
+        return out
 
 
 def pci_bus_id(dev):

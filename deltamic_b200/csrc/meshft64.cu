@@ -1,7 +1,8 @@
 // Float64 meshFT: forward and adjoint in double precision with the reference's
-// float64 arithmetic (deltamic/cpp/fourier3d_cuda_kernel.cu:238-311 forward,
-// :73-233 partials, :314-416 adjoint, dispatched there by AT_DISPATCH for double
-// with Seps = sqrt(DBL_EPSILON), .cu:454, :522).
+// float64 CPU arithmetic (MeshFTPy, deltamic/render.py:36-109, whose Seps is
+// sqrt(1.19209e-07) for both dtypes, render.py:64-65, with a strict comparison in
+// R1 and <= in R2-R4, :77-82), and the partials of the CUDA path
+// (deltamic/cpp/fourier3d_cuda_kernel.cu:73-233, adjoint :314-416).
 //
 // Per (face, frequency) pair with vertex phases x_v = xi . v (double):
 //   F = e_a w_a + e_b w_b + e_c w_c,  e_v = exp(-i x_v),
@@ -11,6 +12,13 @@
 // e^{-i mean}/2, R2/R3/R4 the close pair merged at its midpoint d:
 // F = (i e_d + (e_d - e_o)/D)/D, D = d - x_o.  The partials are the derivatives of
 // those same expressions (merged vertices share dF/dd / 2; R1 gives -iF/3 each).
+//
+// Why the CPU path's Seps and not the CUDA double dispatch's sqrt(DBL_EPSILON)
+// (.cu:454, :522): the general formula cancels ~1/D^2 (F) and ~1/D^3 (partials)
+// terms, so with differences D between 1.5e-8 and ~1e-5 it loses the partials to
+// rounding (measured here: 2e-4 rel-L2 on a level-4 vertex gradient against the
+// CPU float64 reference, and 3e-4 on the spectrum at |xi| ~ 1e-5).  Above
+// 3.45e-4 the rounding error of the partials stays below ~3e-6 of their size.
 //
 // Layout and work split follow the float32 kernels: face records (80 B) and
 // frequency records (48 B) staged in shared memory by bulk copies into a ring of
@@ -36,7 +44,7 @@ namespace dm {
 
 namespace {
 
-constexpr double kSeps64 = 1.4901161193847656e-08;  // sqrt(DBL_EPSILON)
+constexpr double kSeps64 = 3.4526656368666803e-04;  // sqrt(1.19209e-07), render.py:64-65
 constexpr int kBlk64 = 256;  // element-wise kernels
 constexpr int kNT64 = 128;   // threads of the main kernels
 constexpr int kTF64 = 64;    // faces per staged tile (forward), = kFwdTF
@@ -76,8 +84,9 @@ __device__ __forceinline__ cd mul_mi(cd a) { return cd{a.y, -a.x}; }     // -i a
 
 // Branch of a pair: 0 = R5 (general), 1 = R1, 2/3/4 = R2/R3/R4.
 __device__ __forceinline__ int branch64(double ab, double bc, double ca) {
+  const bool tab = fabs(ab) < kSeps64, tbc = fabs(bc) < kSeps64, tca = fabs(ca) < kSeps64;
+  if ((tab && tbc) || (tbc && tca) || (tca && tab)) return 1;
   const bool sab = fabs(ab) <= kSeps64, sbc = fabs(bc) <= kSeps64, sca = fabs(ca) <= kSeps64;
-  if ((sab && sbc) || (sbc && sca) || (sca && sab)) return 1;
   if (sab) return 2;
   if (sbc) return 3;
   if (sca) return 4;

@@ -163,6 +163,39 @@ __device__ __forceinline__ void fwd_face(const FaceGeom& g, float ac, const floa
   }
 }
 
+// Two frequencies of one thread against one face with paired FP32 on the series
+// path (both pairs series with one coefficient set), scalar otherwise; lane x/y
+// of accx/accy accumulates frequency 0/1.  mf2[d] = {mf_d(xi0), mf_d(xi1)}.
+template <class XV>
+__device__ __forceinline__ void fwd_face2(const FaceGeom& g, float ac, const XV (&xv)[2],
+                                          const v2 (&mf2)[3], v2& accx, v2& accy) {
+  const v2 hab = fma2(mf2[0], B2(g.hab[0]), fma2(mf2[1], B2(g.hab[1]), mul2(mf2[2], B2(g.hab[2]))));
+  const v2 hbc = fma2(mf2[0], B2(g.hbc[0]), fma2(mf2[1], B2(g.hbc[1]), mul2(mf2[2], B2(g.hbc[2]))));
+  const v2 hca = neg2(add2(hab, hbc));
+  if (series_pair2(hab, hbc, hca)) {
+    v2 Fx, Fy;
+    if (series_short2(hab, hbc, hca))
+      forward_series2<true>(xv[0], xv[1], g.Ua, hab, hca, Fx, Fy);
+    else
+      forward_series2<false>(xv[0], xv[1], g.Ua, hab, hca, Fx, Fy);
+    accx = fma2(B2(ac), Fx, accx);
+    accy = fma2(B2(ac), Fy, accy);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    c32 F;
+    if (!pair_forward(xv[r], g, F)) F = pair_forward_degenerate(xv[r], g);
+    if (r == 0) {
+      accx.x += ac * F.x;
+      accy.x += ac * F.y;
+    } else {
+      accx.y += ac * F.x;
+      accy.y += ac * F.y;
+    }
+  }
+}
+
 // Frequency of an XiRecOff (off-grid xi list).
 __device__ __forceinline__ XiValOff xi_off(const XiRecOff& r) {
   XiValOff x;
@@ -251,11 +284,25 @@ __global__ void __launch_bounds__(NT) k_meshft_fwd(Cells cells, const FaceRec* _
     float2 tacc[R], tvac[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) tacc[r] = tvac[r] = make_float2(0.f, 0.f);
-    for (int j = 0; j < nft; ++j) {
-      FaceRec fr;
-      load_rec_shared(&sf[s][j], fr);
-      const float4 nv = kVol ? sv[s][j] : make_float4(0.f, 0.f, 0.f, 0.f);
-      fwd_face<R, kVol>(geom_from_rec(fr), fr.area_coeff, nv, xv, tacc, tvac);
+    if constexpr (R == 2 && !kVol) {
+      // paired FP32: both frequencies of the thread per face
+      v2 mf2[3], ax = B2(0.f), ay = B2(0.f);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) mf2[k] = v2{xv[0].mf[k], xv[1].mf[k]};
+      for (int j = 0; j < nft; ++j) {
+        FaceRec fr;
+        load_rec_shared(&sf[s][j], fr);
+        fwd_face2(geom_from_rec(fr), fr.area_coeff, xv, mf2, ax, ay);
+      }
+      tacc[0] = make_float2(ax.x, ay.x);
+      tacc[1] = make_float2(ax.y, ay.y);
+    } else {
+      for (int j = 0; j < nft; ++j) {
+        FaceRec fr;
+        load_rec_shared(&sf[s][j], fr);
+        const float4 nv = kVol ? sv[s][j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        fwd_face<R, kVol>(geom_from_rec(fr), fr.area_coeff, nv, xv, tacc, tvac);
+      }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -382,6 +429,13 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
     geom[k] = geom_from_rec(recs[gf]);
     wt[k] = kVol ? fw[gf] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
+  // edge vectors of the thread's first and last face as lane pairs (paired FP32)
+  v2 hab2[3], hbc2[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    hab2[c] = v2{geom[0].hab[c], geom[F - 1].hab[c]};
+    hbc2[c] = v2{geom[0].hbc[c], geom[F - 1].hbc[c]};
+  }
 
   const int ntiles = (nx + TX - 1) / TX;
   const XR* src0 = xrec + d.b_off + x0;
@@ -412,52 +466,103 @@ __global__ void __launch_bounds__(NT) k_meshft_bwd(Cells cells, const FaceRec* _
     for (int k = 0; k < F; ++k)
 #pragma unroll
       for (int i = 0; i < NQ; ++i) tacc[k].q[i] = 0.f;
-    for (int j = 0; j < nxt; ++j) {
-      XV xv;
-      float gre, gim;
-      load_xi(sx[s][j], xv, gre, gim);
-      float2 gv = make_float2(0.f, 0.f);
-      if (kVol) {
-        const float4 g4 = sg[s][j];
-        gv = make_float2(g4.x, g4.y);
-      }
-      uint32_t spm = 0;
+    if constexpr (F == 2 && !kVol) {
+      // paired FP32: both faces of the thread per frequency; lane x/y = face 0/1
+      v2 q2[10];
 #pragma unroll
-      for (int k = 0; k < F; ++k) {
-        float z[3], r;
-        if constexpr (kVol) {
-          const float tp = xv.mf[0] * wt[k].y + xv.mf[1] * wt[k].z + xv.mf[2] * wt[k].w;
-          const float ure = wt[k].x * gre + tp * gv.y;
-          const float uim = wt[k].x * gim - tp * gv.x;
-          c32 Fv;
-          if (pair_adjoint_t<true>(xv, geom[k], ure, uim, z, r, Fv))
-            bwd_accumulate<true>(tacc[k], z, gre * Fv.x + gim * Fv.y, xv.mf,
-                                 gv.y * Fv.x - gv.x * Fv.y);
+      for (int i = 0; i < 10; ++i) q2[i] = B2(0.f);
+      for (int j = 0; j < nxt; ++j) {
+        XV xv;
+        float gre, gim;
+        load_xi(sx[s][j], xv, gre, gim);
+        const v2 m0 = B2(xv.mf[0]), m1 = B2(xv.mf[1]), m2 = B2(xv.mf[2]);
+        const v2 hab = fma2(m0, hab2[0], fma2(m1, hab2[1], mul2(m2, hab2[2])));
+        const v2 hbc = fma2(m0, hbc2[0], fma2(m1, hbc2[1], mul2(m2, hbc2[2])));
+        const v2 hca = neg2(add2(hab, hbc));
+        if (series_pair2(hab, hbc, hca)) {
+          v2 z[3], r;
+          if (series_short2(hab, hbc, hca))
+            adjoint_series2<true>(xv, geom[0].Ua, geom[1].Ua, hab, hca, gre, gim, z, r);
           else
-            spm |= 1u << k;
-        } else {
-          if (pair_adjoint(xv, geom[k], gre, gim, z, r))
-            bwd_accumulate<false>(tacc[k], z, r, xv.mf, 0.f);
-          else
-            spm |= 1u << k;
+            adjoint_series2<false>(xv, geom[0].Ua, geom[1].Ua, hab, hca, gre, gim, z, r);
+#pragma unroll
+          for (int v = 0; v < 3; ++v) {
+            q2[3 * v + 0] = fma2(z[v], m0, q2[3 * v + 0]);
+            q2[3 * v + 1] = fma2(z[v], m1, q2[3 * v + 1]);
+            q2[3 * v + 2] = fma2(z[v], m2, q2[3 * v + 2]);
+          }
+          q2[9] = add2(q2[9], r);
+          continue;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          float z[3], r;
+          if (!pair_adjoint(xv, geom[k], gre, gim, z, r))
+            pair_adjoint_degenerate(xv, geom[k], gre, gim, z, r);
+#pragma unroll
+          for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              float& a = k == 0 ? q2[3 * v + c].x : q2[3 * v + c].y;
+              a += z[v] * xv.mf[c];
+            }
+          float& a9 = k == 0 ? q2[9].x : q2[9].y;
+          a9 += r;
         }
       }
-      if (spm) {
 #pragma unroll
+      for (int i = 0; i < 10; ++i) {
+        tacc[0].q[i] = q2[i].x;
+        tacc[F - 1].q[i] = q2[i].y;
+      }
+    } else {
+      for (int j = 0; j < nxt; ++j) {
+        XV xv;
+        float gre, gim;
+        load_xi(sx[s][j], xv, gre, gim);
+        float2 gv = make_float2(0.f, 0.f);
+        if (kVol) {
+          const float4 g4 = sg[s][j];
+          gv = make_float2(g4.x, g4.y);
+        }
+        uint32_t spm = 0;
+  #pragma unroll
         for (int k = 0; k < F; ++k) {
-          if ((spm >> k) & 1u) {
-            float z[3], r;
-            if constexpr (kVol) {
-              const float tp = xv.mf[0] * wt[k].y + xv.mf[1] * wt[k].z + xv.mf[2] * wt[k].w;
-              const float ure = wt[k].x * gre + tp * gv.y;
-              const float uim = wt[k].x * gim - tp * gv.x;
-              c32 Fv;
-              pair_adjoint_degenerate(xv, geom[k], ure, uim, z, r, Fv);
+          float z[3], r;
+          if constexpr (kVol) {
+            const float tp = xv.mf[0] * wt[k].y + xv.mf[1] * wt[k].z + xv.mf[2] * wt[k].w;
+            const float ure = wt[k].x * gre + tp * gv.y;
+            const float uim = wt[k].x * gim - tp * gv.x;
+            c32 Fv;
+            if (pair_adjoint_t<true>(xv, geom[k], ure, uim, z, r, Fv))
               bwd_accumulate<true>(tacc[k], z, gre * Fv.x + gim * Fv.y, xv.mf,
                                    gv.y * Fv.x - gv.x * Fv.y);
-            } else {
-              pair_adjoint_degenerate(xv, geom[k], gre, gim, z, r);
+            else
+              spm |= 1u << k;
+          } else {
+            if (pair_adjoint(xv, geom[k], gre, gim, z, r))
               bwd_accumulate<false>(tacc[k], z, r, xv.mf, 0.f);
+            else
+              spm |= 1u << k;
+          }
+        }
+        if (spm) {
+  #pragma unroll
+          for (int k = 0; k < F; ++k) {
+            if ((spm >> k) & 1u) {
+              float z[3], r;
+              if constexpr (kVol) {
+                const float tp = xv.mf[0] * wt[k].y + xv.mf[1] * wt[k].z + xv.mf[2] * wt[k].w;
+                const float ure = wt[k].x * gre + tp * gv.y;
+                const float uim = wt[k].x * gim - tp * gv.x;
+                c32 Fv;
+                pair_adjoint_degenerate(xv, geom[k], ure, uim, z, r, Fv);
+                bwd_accumulate<true>(tacc[k], z, gre * Fv.x + gim * Fv.y, xv.mf,
+                                     gv.y * Fv.x - gv.x * Fv.y);
+              } else {
+                pair_adjoint_degenerate(xv, geom[k], gre, gim, z, r);
+                bwd_accumulate<false>(tacc[k], z, r, xv.mf, 0.f);
+              }
             }
           }
         }

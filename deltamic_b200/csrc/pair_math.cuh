@@ -571,4 +571,189 @@ DM_HD c32 pair_forward_degenerate(const XV& xv, const FaceGeom& g) {
   return F;
 }
 
+// ---------------------------------------------------------------------------
+// Two pairs per instruction on the centroid-series path.
+//
+// sm_100 issues paired FP32 instructions (FFMA2 / FMUL2 / FADD2: two lanes' FP32
+// operations, one per half of a 64-bit register pair, per instruction).  The
+// meshFT kernels are issue-bound, so two pairs that take the series path with the
+// same coefficient set -- two faces at one frequency (adjoint), or one face at two
+// frequencies (forward) -- run their FP32 arithmetic packed: per component the
+// same operations in the same order as the scalar functions above, with the
+// integer phase and the MUFU sine / cosine still per pair.
+
+struct v2 {
+  float x, y;
+};
+
+DM_HD v2 B2(float s) { return v2{s, s}; }
+DM_HD v2 neg2(v2 a) { return v2{-a.x, -a.y}; }
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+DM_HD v2 fma2(v2 a, v2 b, v2 c) {
+  const float2 r = __ffma2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y), make_float2(c.x, c.y));
+  return v2{r.x, r.y};
+}
+DM_HD v2 mul2(v2 a, v2 b) {
+  const float2 r = __fmul2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return v2{r.x, r.y};
+}
+DM_HD v2 add2(v2 a, v2 b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return v2{r.x, r.y};
+}
+#else
+DM_HD v2 fma2(v2 a, v2 b, v2 c) { return v2{fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y)}; }
+DM_HD v2 mul2(v2 a, v2 b) { return v2{a.x * b.x, a.y * b.y}; }
+DM_HD v2 add2(v2 a, v2 b) { return v2{a.x + b.x, a.y + b.y}; }
+#endif
+DM_HD v2 sub2(v2 a, v2 b) { return add2(a, neg2(b)); }
+
+template <int N>
+DM_HD void horner2(const float* c, v2 x, v2& v, v2& dv) {
+  if constexpr (N == 0) {
+    v = B2(0.f);
+    dv = B2(0.f);
+  } else {
+    v = B2(c[N - 1]);
+    dv = B2(0.f);
+#pragma unroll
+    for (int k = N - 2; k >= 0; --k) {
+      dv = fma2(dv, x, v);
+      v = fma2(v, x, B2(c[k]));
+    }
+  }
+}
+
+// centroid_H_set for two pairs: H = (Hx, Hy) and, if kGrad, its partials.
+template <bool kGrad, int N0, int N2, int N4, int M1, int M3>
+DM_HD void centroid_H_set2(const float* P0, const float* P2, const float* P4, const float* Q1,
+                           const float* Q3, v2 p2, v2 p3, v2& Hx, v2& Hy, v2& Hp2x, v2& Hp2y,
+                           v2& Hp3x, v2& Hp3y) {
+  v2 a0, a0d, a2, a2d, a4, a4d, b1, b1d, b3, b3d;
+  horner2<N0>(P0, p2, a0, a0d);
+  horner2<N2>(P2, p2, a2, a2d);
+  horner2<N4>(P4, p2, a4, a4d);
+  horner2<M1>(Q1, p2, b1, b1d);
+  horner2<M3>(Q3, p2, b3, b3d);
+  const v2 q = mul2(p3, p3);
+  if constexpr (N4 > 0) {
+    Hx = fma2(q, fma2(q, a4, a2), a0);
+  } else {
+    Hx = fma2(q, a2, a0);
+  }
+  if constexpr (M3 > 0) {
+    Hy = mul2(p3, fma2(q, b3, b1));
+  } else {
+    Hy = mul2(p3, b1);
+  }
+  if (kGrad) {
+    if constexpr (N4 > 0) {
+      Hp2x = fma2(q, fma2(q, a4d, a2d), a0d);
+      Hp3x = mul2(p3, fma2(mul2(B2(4.0f), q), a4, mul2(B2(2.0f), a2)));
+    } else {
+      Hp2x = fma2(q, a2d, a0d);
+      Hp3x = mul2(p3, mul2(B2(2.0f), a2));
+    }
+    if constexpr (M3 > 0) {
+      Hp2y = mul2(p3, fma2(q, b3d, b1d));
+      Hp3y = fma2(mul2(B2(3.0f), q), b3, b1);
+    } else {
+      Hp2y = mul2(p3, b1d);
+      Hp3y = b1;
+    }
+  }
+}
+
+template <bool kGrad, bool kLo>
+DM_HD void centroid_H2(v2 p2, v2 p3, v2& Hx, v2& Hy, v2& Hp2x, v2& Hp2y, v2& Hp3x, v2& Hp3y) {
+  if constexpr (kLo) {
+    constexpr float P0[] = DM_SERIES_LO_P0;
+    constexpr float P2[] = DM_SERIES_LO_P2;
+    constexpr float P4[] = DM_SERIES_LO_P4;
+    constexpr float Q1[] = DM_SERIES_LO_Q1;
+    constexpr float Q3[] = DM_SERIES_LO_Q3;
+    centroid_H_set2<kGrad, DM_SERIES_LO_P0_N, DM_SERIES_LO_P2_N, DM_SERIES_LO_P4_N,
+                    DM_SERIES_LO_Q1_N, DM_SERIES_LO_Q3_N>(P0, P2, P4, Q1, Q3, p2, p3, Hx, Hy,
+                                                          Hp2x, Hp2y, Hp3x, Hp3y);
+  } else {
+    constexpr float P0[] = DM_SERIES_P0;
+    constexpr float P2[] = DM_SERIES_P2;
+    constexpr float P4[] = DM_SERIES_P4;
+    constexpr float Q1[] = DM_SERIES_Q1;
+    constexpr float Q3[] = DM_SERIES_Q3;
+    centroid_H_set2<kGrad, DM_SERIES_P0_N, DM_SERIES_P2_N, DM_SERIES_P4_N, DM_SERIES_Q1_N,
+                    DM_SERIES_Q3_N>(P0, P2, P4, Q1, Q3, p2, p3, Hx, Hy, Hp2x, Hp2y, Hp3x,
+                                    Hp3y);
+  }
+}
+
+// Centroid deviations d_v, p2 and p3 of two pairs from their half differences.
+DM_HD void series_dev2(v2 hab, v2 hca, v2 d[3], v2& p2, v2& p3) {
+  const v2 ab = add2(hab, hab), ca = add2(hca, hca);
+  d[0] = mul2(sub2(ca, ab), B2(1.0f / 3.0f));
+  d[1] = add2(d[0], ab);
+  d[2] = sub2(d[0], ca);
+  p2 = fma2(d[2], d[2], fma2(d[1], d[1], mul2(d[0], d[0])));
+  p3 = mul2(mul2(B2(3.0f), d[0]), mul2(d[1], d[2]));
+}
+
+// Both pairs in the series domain (no degenerate difference, largest below 3.5)?
+DM_HD bool series_pair2(v2 hab, v2 hbc, v2 hca) {
+  return pair_class(hab.x, hbc.x, hca.x) == 0 && pair_class(hab.y, hbc.y, hca.y) == 0;
+}
+
+// Short coefficient set for both pairs (and, on the GPU, every converged lane).
+DM_HD bool series_short2(v2 hab, v2 hbc, v2 hca) {
+  const float m0 = fmaxf(fabsf(hab.x), fmaxf(fabsf(hbc.x), fabsf(hca.x)));
+  const float m1 = fmaxf(fabsf(hab.y), fmaxf(fabsf(hbc.y), fabsf(hca.y)));
+  const bool lo = fmaxf(m0, m1) <= kSeriesLoHalf;
+#if defined(__CUDA_ARCH__)
+  return __all_sync(__activemask(), lo);
+#else
+  return lo;
+#endif
+}
+
+// Adjoint of two faces (vertex-a positions Ua0, Ua1) at one frequency on the
+// series path: z_v = Re(conj(g) dF/dx_v) and r = Re(conj(g) F), lane x for the
+// first face, y for the second (pair_adjoint_t's series branch).
+template <bool kLo, class XV>
+DM_HD void adjoint_series2(const XV& xv, const uint32_t Ua0[3], const uint32_t Ua1[3], v2 hab,
+                           v2 hca, float gre, float gim, v2 z[3], v2& r) {
+  v2 d[3], p2, p3;
+  series_dev2(hab, hca, d, p2, p3);
+  float s0, c0, s1, c1;
+  sincos_fast(vertex_angle(xv, Ua0[0], Ua0[1], Ua0[2]) - d[0].x, &s0, &c0);
+  sincos_fast(vertex_angle(xv, Ua1[0], Ua1[1], Ua1[2]) - d[0].y, &s1, &c1);
+  const v2 Ex{c0, c1}, Ey{-s0, -s1};
+  v2 Hx, Hy, Hp2x, Hp2y, Hp3x, Hp3y;
+  centroid_H2<true, kLo>(p2, p3, Hx, Hy, Hp2x, Hp2y, Hp3x, Hp3y);
+  const v2 hx = fma2(B2(gre), Ex, mul2(B2(gim), Ey));        // h = conj(g) E
+  const v2 hy = fma2(B2(gre), Ey, mul2(B2(-gim), Ex));
+  r = fma2(hx, Hx, mul2(neg2(hy), Hy));
+  const v2 zt = mul2(fma2(hx, Hy, mul2(hy, Hx)), B2(1.0f / 3.0f));
+  const v2 r1 = mul2(B2(2.0f), fma2(hx, Hp2x, mul2(neg2(hy), Hp2y)));
+  const v2 r2 = fma2(hx, Hp3x, mul2(neg2(hy), Hp3y));
+#pragma unroll
+  for (int v = 0; v < 3; ++v)
+    z[v] = fma2(r2, fma2(mul2(B2(3.0f), d[v]), d[v], neg2(p2)), fma2(r1, d[v], zt));
+}
+
+// Forward of one face (vertex-a position Ua) at two frequencies on the series
+// path: F = (Fx, Fy) per lane (pair_forward's series branch).
+template <bool kLo, class XV>
+DM_HD void forward_series2(const XV& x0, const XV& x1, const uint32_t Ua[3], v2 hab, v2 hca,
+                           v2& Fx, v2& Fy) {
+  v2 d[3], p2, p3;
+  series_dev2(hab, hca, d, p2, p3);
+  float s0, c0, s1, c1;
+  sincos_fast(vertex_angle(x0, Ua[0], Ua[1], Ua[2]) - d[0].x, &s0, &c0);
+  sincos_fast(vertex_angle(x1, Ua[0], Ua[1], Ua[2]) - d[0].y, &s1, &c1);
+  const v2 Ex{c0, c1}, Ey{-s0, -s1};
+  v2 Hx, Hy, u0, u1, u2, u3;
+  centroid_H2<false, kLo>(p2, p3, Hx, Hy, u0, u1, u2, u3);
+  Fx = fma2(Ex, Hx, mul2(neg2(Ey), Hy));
+  Fy = fma2(Ex, Hy, mul2(Ey, Hx));
+}
+
 }  // namespace dm

@@ -196,10 +196,12 @@ int dm_meshft_backward_xi(const float* verts, int64_t nv, const int64_t* faces, 
 /* ---------------------------------------------------------------------------
  * meshFT in float64: the double-precision dispatch of forward_fourier3d_cpp /
  * backward_fourier3d_cpp (deltamic/cpp/fourier3d_cuda.cpp:27-65; kernels
- * .cu:238-416 for scalar_t = double, Seps = sqrt(DBL_EPSILON), .cu:454, :522),
- * i.e. Fourier3dMesh(dtype=torch.float64) on CUDA.  Same arithmetic as the
- * reference (phases xi . v in double, its R1..R5 branches), every frequency
- * evaluated (band_flags ignored).  Frequencies come from exactly one source:
+ * .cu:238-416 for scalar_t = double), i.e. Fourier3dMesh(dtype=torch.float64).
+ * Phases xi . v in double and the R1..R5 branches with the reference CPU path's
+ * Seps = sqrt(1.19209e-07) (render.py:64-65, strict in R1) -- its CUDA double
+ * dispatch uses sqrt(DBL_EPSILON), where the general formula loses the partials
+ * to cancellation for phase differences below ~1e-5; every frequency evaluated
+ * (band_flags ignored).  Frequencies come from exactly one source:
  *   - a grid band: box and band_index[n_freq] as for dm_meshft_forward (vertices
  *     shifted by box.lo inside, as Fourier3dMesh.forward does); or
  *   - a list: xi_list[n_freq,3] float64 with box NULL (vertices as given, as

@@ -99,4 +99,71 @@ void dm_host_pairs_off(const double* verts, const int64_t* faces, int64_t nt, co
   }
 }
 
+// Packed two-pair series path against the scalar one: for faces (2j, 2j+1) at
+// each grid frequency (adjoint_series2) and for frequencies (2i, 2i+1) at each
+// face (forward_series2), where both pairs are series pairs; other entries are
+// left untouched (the caller fills them with the scalar results).
+void dm_host_series2(const double* verts, const int64_t* faces, int64_t nt, const int32_t* m,
+                     int64_t nxi, const float* gc, const double* lo, const double* len, float* z,
+                     float* r, float* F) {
+  for (int64_t i = 0; i < nxi; ++i) {
+    XiVal xv;
+    for (int d = 0; d < 3; ++d) {
+      xv.mi[d] = m[3 * i + d];
+      xv.mf[d] = (float)m[3 * i + d];
+    }
+    for (int64_t k = 0; k + 1 < nt; k += 2) {
+      const FaceGeom g0 = make_geom(verts + 3 * faces[3 * k], verts + 3 * faces[3 * k + 1],
+                                    verts + 3 * faces[3 * k + 2], lo, len);
+      const FaceGeom g1 = make_geom(verts + 3 * faces[3 * k + 3], verts + 3 * faces[3 * k + 4],
+                                    verts + 3 * faces[3 * k + 5], lo, len);
+      float a0, b0, c0, a1, b1, c1;
+      half_diffs(xv.mf, g0, a0, b0, c0);
+      half_diffs(xv.mf, g1, a1, b1, c1);
+      const v2 hab{a0, a1}, hbc{b0, b1}, hca{c0, c1};
+      if (!series_pair2(hab, hbc, hca)) continue;
+      v2 zz[3], rr;
+      if (series_short2(hab, hbc, hca))
+        adjoint_series2<true>(xv, g0.Ua, g1.Ua, hab, hca, gc[2 * i], gc[2 * i + 1], zz, rr);
+      else
+        adjoint_series2<false>(xv, g0.Ua, g1.Ua, hab, hca, gc[2 * i], gc[2 * i + 1], zz, rr);
+      const int64_t o0 = i * nt + k, o1 = o0 + 1;
+      for (int v = 0; v < 3; ++v) {
+        z[3 * o0 + v] = zz[v].x;
+        z[3 * o1 + v] = zz[v].y;
+      }
+      r[o0] = rr.x;
+      r[o1] = rr.y;
+    }
+  }
+  for (int64_t k = 0; k < nt; ++k) {
+    const FaceGeom g = make_geom(verts + 3 * faces[3 * k], verts + 3 * faces[3 * k + 1],
+                                 verts + 3 * faces[3 * k + 2], lo, len);
+    for (int64_t i = 0; i + 1 < nxi; i += 2) {
+      XiVal x0, x1;
+      for (int d = 0; d < 3; ++d) {
+        x0.mi[d] = m[3 * i + d];
+        x0.mf[d] = (float)m[3 * i + d];
+        x1.mi[d] = m[3 * i + 3 + d];
+        x1.mf[d] = (float)m[3 * i + 3 + d];
+      }
+      float a0, b0, c0, a1, b1, c1;
+      half_diffs(x0.mf, g, a0, b0, c0);
+      half_diffs(x1.mf, g, a1, b1, c1);
+      const v2 hab{a0, a1}, hbc{b0, b1}, hca{c0, c1};
+      if (!series_pair2(hab, hbc, hca)) continue;
+      v2 Fx, Fy;
+      if (series_short2(hab, hbc, hca))
+        forward_series2<true>(x0, x1, g.Ua, hab, hca, Fx, Fy);
+      else
+        forward_series2<false>(x0, x1, g.Ua, hab, hca, Fx, Fy);
+      const int64_t o0 = i * nt + k, o1 = (i + 1) * nt + k;
+      F[2 * o0] = Fx.x;
+      F[2 * o0 + 1] = Fy.x;
+      F[2 * o1] = Fx.y;
+      F[2 * o1 + 1] = Fy.y;
+    }
+  }
+}
+
 }  // extern "C"

@@ -273,7 +273,7 @@ def test_float64_module_runs_float64_kernels():
         assert ft.dtype == (torch.complex64 if dt == torch.float32 else torch.complex128)
     idx = out[1][2].astype(np.int64)
     xil = oracle.xi_list_from_band(idx, oracle.frequency_axes(box, shape))
-    ref = oracle.meshft_forward(v - box[:, 0], f, c, xil, seps=oracle.SEPS_F64)
+    ref = oracle.meshft_forward(v - box[:, 0], f, c, xil, seps=oracle.SEPS_F32)
     assert rel_l2(out[1][0].reshape(-1)[idx], ref) < 1e-11
     assert rel_l2(out[0][0].reshape(-1)[idx], ref) < TOL_FT
     assert rel_l2(out[1][1], out[0][1]) < 1e-5
@@ -347,3 +347,36 @@ def test_symmetry_flag_on_asymmetric_band_is_reported():
     flags = N._INT()
     assert lib.dm_device_error(N.ptr(ws), ctypes.byref(flags), N.stream_ptr(DEV)) == N.DM_OK
     assert flags.value & N.DM_ERR_BAD_INDEX
+
+
+def test_every_tile_variant_matches_oracle():
+    """Each forward and adjoint tile-shape variant (the autotuner's candidates,
+    including the paired-FP32 two-frequency forward and two-face adjoint) against
+    the oracle, on a mesh whose pairs take the series, pivot and degenerate paths."""
+    import ctypes
+    from deltamic_b200 import _native as N
+    lib = N.lib()
+    v, f, c, box, shape, sigma, thresh = _case(3, (41, 37, 33), seed=6)
+    grid, xi, otf, band = _setup(v, f, c, box, shape, sigma, thresh)
+    V, F, C = _t(v), _t(f, torch.int64), _t(c)
+    xil = _oracle_xi(grid, band)
+    ft64 = oracle.meshft_forward(v - box[:, 0], f, c, xil)
+    rng = np.random.default_rng(3)
+    g = (rng.normal(size=band.numel()) + 1j * rng.normal(size=band.numel())).astype(np.complex64)
+    rv, rc = oracle.meshft_backward(v - box[:, 0], f, c, xil, g, ft64)
+    fwd, bwd, nf, nb = N._INT(), N._INT(), N._INT(), N._INT()
+    N.check(lib.dm_get_variants(ctypes.byref(fwd), ctypes.byref(bwd), ctypes.byref(nf),
+                                ctypes.byref(nb)), "dm_get_variants")
+    try:
+        for k in range(max(nf.value, nb.value)):
+            N.check(lib.dm_set_variants(min(k, nf.value - 1), min(k, nb.value - 1)),
+                    "dm_set_variants")
+            ft = ops.meshft_list(V, F, C, grid, band)
+            gv, gc, _ = ops.meshft_backward_list(V, F, C, grid, band, ft,
+                                                 grad_list=_t(g, torch.complex64))
+            e = (rel_l2(ft.cpu().numpy(), ft64), rel_l2(gv.cpu().numpy(), rv),
+                 rel_l2(gc.cpu().numpy(), rc))
+            print(f"variant {k}: ft {e[0]:.2e} verts {e[1]:.2e} coeff {e[2]:.2e}")
+            assert e[0] < TOL_FT and e[1] < TOL_GV and e[2] < TOL_GC, k
+    finally:
+        lib.dm_set_variants(fwd.value, bwd.value)

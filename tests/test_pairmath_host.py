@@ -128,3 +128,33 @@ def test_split_phase_off_grid_matches_oracle(hostlib, scale, shift):
     eF = np.linalg.norm(Fc - F0) / np.linalg.norm(F0)
     ez = np.linalg.norm(z - z0) / np.linalg.norm(z0)
     assert eF < 2e-6 and ez < 4e-6, (eF, ez)
+
+
+def test_packed_two_pair_series_matches_scalar(hostlib):
+    """The paired-FP32 series path (two faces at one frequency in the adjoint, one
+    face at two frequencies in the forward) gives the scalar path's results."""
+    rng = np.random.default_rng(5)
+    v, f = icosphere(4, 0.3)
+    v, _ = sh_perturb(v, 4, 0.08, rng, radius=0.3)
+    box = oracle.compute_box_size(v, 0.2)
+    shape = (96, 96, 96)
+    f = f[rng.choice(len(f), 400, replace=False)]
+    k = np.stack([rng.integers(20, 76, 300) for _ in range(3)], 1)
+    m = (2 * k - (np.array(shape) - 1)).astype(np.int32)
+    g = rng.normal(size=len(m)) + 1j * rng.normal(size=len(m))
+    F, z, r, cls = _run(hostlib, v, f, m, g, box[:, 0], box[:, 1] - box[:, 0])
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    F2 = np.stack([F.real, F.imag], -1).astype(np.float32).copy()
+    z2, r2 = z.copy(), r.copy()
+    vv, ff = np.ascontiguousarray(v, np.float64), np.ascontiguousarray(f, np.int64)
+    mm = np.ascontiguousarray(m, np.int32)
+    gg = np.ascontiguousarray(np.stack([g.real, g.imag], 1), np.float32)
+    lo = np.ascontiguousarray(box[:, 0], np.float64)
+    L = np.ascontiguousarray(box[:, 1] - box[:, 0], np.float64)
+    hostlib.dm_host_series2(P(vv), P(ff), ctypes.c_int64(len(f)), P(mm), ctypes.c_int64(len(m)),
+                            P(gg), P(lo), P(L), P(z2), P(r2), P(F2))
+    Fp = F2[..., 0] + 1j * F2[..., 1]
+    assert (cls == 0).mean() > 0.25
+    assert np.linalg.norm(Fp - F) / np.linalg.norm(F) < 1e-6
+    assert np.linalg.norm(z2 - z) / np.linalg.norm(z) < 1e-6
+    assert np.linalg.norm(r2 - r) / np.linalg.norm(r) < 1e-6
