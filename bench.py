@@ -150,7 +150,7 @@ class ClockSampler:
                 h = None
                 if self.pci:
                     try:
-                        h = nv.nvmlDeviceGetHandleByPciBusId_v2(self.pci)
+                        h = nv.nvmlDeviceGetHandleByPciBusId(self.pci)
                     except Exception as e:  # fall back to the index below
                         self.nvml_error = f"by PCI bus id {self.pci}: {e}"
                 if h is None:

@@ -793,6 +793,166 @@ static void gemm_launch(int bn, LA la, LB lb, EP ep, int64_t rows, int64_t red, 
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
+// ---------------------------------------------------------------------------
+// Single-channel input (the encoder's first layer, Ci = 1): the reduction is only
+// 27 taps long, so an implicit GEMM spends its time gathering 2-byte elements.
+// These direct kernels stage each tile's input footprint once in shared memory
+// instead -- a tile is (b, od, 8 output rows, 32 output columns); its input is 3
+// planes x 17 rows x 65 columns -- and stream the outputs (HBM-bound: 2 B read and
+// 6 Co B written per output voxel in the forward).  Products and sums in FP32 on
+// the same BF16 inputs.
+
+constexpr int kC1TH = 8, kC1TW = 32;                       // output tile rows x columns
+constexpr int kC1IH = 2 * kC1TH + 1, kC1IW = 2 * kC1TW + 1;  // input footprint
+
+struct C1Tile {
+  int b, od, oh0, ow0;
+};
+
+__device__ __forceinline__ C1Tile c1_tile(const ConvShape& s, int64_t t) {
+  const int nw = (s.Wo + kC1TW - 1) / kC1TW, nh = (s.Ho + kC1TH - 1) / kC1TH;
+  C1Tile r;
+  r.ow0 = (int)(t % nw) * kC1TW;
+  t /= nw;
+  r.oh0 = (int)(t % nh) * kC1TH;
+  t /= nh;
+  r.od = (int)(t % s.Do);
+  r.b = (int)(t / s.Do);
+  return r;
+}
+
+__device__ __forceinline__ int64_t c1_tiles(const ConvShape& s) {
+  return (int64_t)s.B * s.Do * ((s.Ho + kC1TH - 1) / kC1TH) * ((s.Wo + kC1TW - 1) / kC1TW);
+}
+
+// Input footprint of a tile into xs[3][17][65] (zero outside the volume).
+__device__ __forceinline__ void c1_load(const bf16* __restrict__ x, const ConvShape& s,
+                                        const C1Tile& tl, float* xs) {
+  for (int i = threadIdx.x; i < 3 * kC1IH * kC1IW; i += blockDim.x) {
+    const int c = i % kC1IW, r = (i / kC1IW) % kC1IH, pz = i / (kC1IW * kC1IH);
+    const int d = 2 * tl.od - 1 + pz, h = 2 * tl.oh0 - 1 + r, w = 2 * tl.ow0 - 1 + c;
+    float v = 0.f;
+    if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+      v = __bfloat162float(x[(((int64_t)tl.b * s.D + d) * s.H + h) * s.W + w]);
+    xs[i] = v;
+  }
+}
+
+// pre = x * W + bias, act = GELU(pre) for one output voxel per thread.
+template <int CO>
+__global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, ConvShape s,
+                                                   const bf16* __restrict__ w,
+                                                   const float* __restrict__ bias,
+                                                   float* __restrict__ pre,
+                                                   bf16* __restrict__ act) {
+  __shared__ float xs[3 * kC1IH * kC1IW];
+  __shared__ float ws[27][CO];
+  __shared__ float bs[CO];
+  for (int i = threadIdx.x; i < 27 * CO; i += blockDim.x)
+    ws[i / CO][i % CO] = __bfloat162float(w[i]);  // rows 0..26 of W[Kp][Co]
+  if (threadIdx.x < CO) bs[threadIdx.x] = bias ? bias[threadIdx.x] : 0.f;
+  const C1Tile tl = c1_tile(s, blockIdx.x);
+  c1_load(x, s, tl, xs);
+  __syncthreads();
+  const int ty = threadIdx.x / kC1TW, tx = threadIdx.x % kC1TW;
+  const int oh = tl.oh0 + ty, ow = tl.ow0 + tx;
+  if (oh >= s.Ho || ow >= s.Wo) return;
+  float acc[CO];
+#pragma unroll
+  for (int c = 0; c < CO; ++c) acc[c] = bs[c];
+#pragma unroll
+  for (int kd = 0; kd < 3; ++kd)
+#pragma unroll
+    for (int kh = 0; kh < 3; ++kh)
+#pragma unroll
+      for (int kw = 0; kw < 3; ++kw) {
+        const float xv = xs[(kd * kC1IH + 2 * ty + kh) * kC1IW + 2 * tx + kw];
+        const int tap = (kd * 3 + kh) * 3 + kw;
+#pragma unroll
+        for (int c = 0; c < CO; ++c) acc[c] = fmaf(xv, ws[tap][c], acc[c]);
+      }
+  const int64_t m = (((int64_t)tl.b * s.Do + tl.od) * s.Ho + oh) * s.Wo + ow;
+  float4* pp = reinterpret_cast<float4*>(pre + m * CO);
+  uint4* ap = reinterpret_cast<uint4*>(act + m * CO);
+#pragma unroll
+  for (int q = 0; q < CO / 4; ++q) pp[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2],
+                                                       acc[4 * q + 3]);
+#pragma unroll
+  for (int q = 0; q < CO / 8; ++q) {
+    uint32_t u[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      u[j] = pack2(__float2bfloat16(gelu(acc[8 * q + 2 * j])),
+                   __float2bfloat16(gelu(acc[8 * q + 2 * j + 1])));
+    ap[q] = make_uint4(u[0], u[1], u[2], u[3]);
+  }
+}
+
+// Weight and bias gradient partials: block g sums its tiles (g, g + G, ...) into
+// part[g][(Kp + 1) * CO] (rows 0..26 taps, 27..Kp-1 zero, row Kp the bias);
+// k_sum_splits adds the blocks in order.  dP is the BF16 dL/dpre of k_gelu_back.
+template <int CO>
+__global__ void __launch_bounds__(256) k_conv1_wgrad(const bf16* __restrict__ x, ConvShape s,
+                                                     const bf16* __restrict__ dp,
+                                                     float* __restrict__ part) {
+  __shared__ float xs[3 * kC1IH * kC1IW];
+  __shared__ float ds[kC1TH * kC1TW][CO + 1];
+  constexpr int NO = 27 * CO + CO;  // tap x channel outputs, then the bias
+  constexpr int PER = (NO + 255) / 256;
+  float acc[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) acc[j] = 0.f;
+  const int64_t ntl = c1_tiles(s);
+  for (int64_t t = blockIdx.x; t < ntl; t += gridDim.x) {
+    const C1Tile tl = c1_tile(s, t);
+    __syncthreads();  // the previous tile's reads are done
+    c1_load(x, s, tl, xs);
+    for (int i = threadIdx.x; i < kC1TH * kC1TW * CO; i += blockDim.x) {
+      const int v = i / CO, c = i % CO;
+      const int oh = tl.oh0 + v / kC1TW, ow = tl.ow0 + v % kC1TW;
+      float g = 0.f;
+      if (oh < s.Ho && ow < s.Wo)
+        g = __bfloat162float(
+            dp[((((int64_t)tl.b * s.Do + tl.od) * s.Ho + oh) * s.Wo + ow) * CO + c]);
+      ds[v][c] = g;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int o = threadIdx.x + 256 * j;
+      if (o >= NO) continue;
+      float a = 0.f;
+      if (o < 27 * CO) {
+        const int tap = o / CO, c = o % CO;
+        const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+        for (int ty = 0; ty < kC1TH; ++ty) {
+          const float* xr = xs + (kd * kC1IH + 2 * ty + kh) * kC1IW + kw;
+#pragma unroll 8
+          for (int tx = 0; tx < kC1TW; ++tx) a = fmaf(xr[2 * tx], ds[ty * kC1TW + tx][c], a);
+        }
+      } else {
+        const int c = o - 27 * CO;
+        for (int v = 0; v < kC1TH * kC1TW; ++v) a += ds[v][c];
+      }
+      acc[j] += a;
+    }
+  }
+  float* out = part + (int64_t)blockIdx.x * (s.Kp + 1) * CO;
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int o = threadIdx.x + 256 * j;
+    if (o < 27 * CO) out[o] = acc[j];
+    else if (o < NO) out[(int64_t)s.Kp * CO + (o - 27 * CO)] = acc[j];
+  }
+  for (int o = 27 * CO + threadIdx.x; o < s.Kp * CO; o += blockDim.x) out[o] = 0.f;
+}
+
+static bool conv1_direct(const ConvShape& s) { return s.Ci == 1 && (s.Co == 16 || s.Co == 32); }
+
+static int64_t conv1_tiles_host(const ConvShape& s) {
+  return (int64_t)s.B * s.Do * ((s.Ho + kC1TH - 1) / kC1TH) * ((s.Wo + kC1TW - 1) / kC1TW);
+}
+
 static int pad_cols(int c) { return c <= 16 ? 16 : (c <= 32 ? 32 : (c <= 64 ? 64 : 128)); }
 
 bool conv_shape(int B, int D, int H, int W, int Ci, int Co, ConvShape& s) {
@@ -838,6 +998,15 @@ static int fwd_cols(const ConvShape& s) {
 
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st) {
+  if (conv1_direct(s) && aligned16(pre) && aligned16(act)) {
+    const unsigned g = (unsigned)conv1_tiles_host(s);
+    if (s.Co == 16)
+      k_conv1_fwd<16><<<g, 256, 0, st>>>(x, s, w, bias, pre, act);
+    else
+      k_conv1_fwd<32><<<g, 256, 0, st>>>(x, s, w, bias, pre, act);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  }
   const int bn = fwd_cols(s);
   gemm_launch(bn, FwdA{x, s, s.Ci % 8 == 0 && aligned16(x)}, WeightB{w, s.Co, 0},
               FwdEp{bias, pre, act, s.Co, 0, aligned16(pre) && aligned16(act)}, s.M, s.Kp, s.Kp,
@@ -862,11 +1031,22 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   // weight and bias gradients: rows = Kp + 1 (the last row of A^T is ones), the
   // reduction over m split across blockIdx.y
   const int splits = wgrad_splits(s);
-  const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
-  const int used = (int)((s.M + per - 1) / per);
-  gemm_launch(s.Co, WgradA{x, s, s.Ci % 8 == 0 && aligned16(x)}, DpreB{dp, s.Co, aligned16(dp)},
-              WgradEp{part, (int64_t)(s.Kp + 1) * s.Co, s.Co}, (int64_t)s.Kp + 1, s.M, per, used,
-              1, st);
+  int used;
+  if (conv1_direct(s)) {
+    used = (int)std::max<int64_t>(1, std::min<int64_t>(splits, conv1_tiles_host(s)));
+    if (s.Co == 16)
+      k_conv1_wgrad<16><<<used, 256, 0, st>>>(x, s, dp, part);
+    else
+      k_conv1_wgrad<32><<<used, 256, 0, st>>>(x, s, dp, part);
+    count_launches(1);
+  } else {
+    const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
+    used = (int)((s.M + per - 1) / per);
+    gemm_launch(s.Co, WgradA{x, s, s.Ci % 8 == 0 && aligned16(x)},
+                DpreB{dp, s.Co, aligned16(dp)},
+                WgradEp{part, (int64_t)(s.Kp + 1) * s.Co, s.Co}, (int64_t)s.Kp + 1, s.M, per,
+                used, 1, st);
+  }
   const int64_t nw = (int64_t)s.Kp * s.Co;
   k_sum_splits<<<(unsigned)((nw + s.Co + 31) / 32), dim3(32, 8), 0, st>>>(part, used, nw, s.Co,
                                                                           dw, db);
