@@ -1110,6 +1110,8 @@ def run_ours(args, rank, world, local):
     make_step, e2e_call, init_v, pairs, info, cpu_case = setup(args, rank, dev)
 
     step = make_step(not args.no_graph)
+    from deltamic_b200 import autotune
+    tuned = autotune.current()[:2]  # the tile-shape variants the step runs
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -1199,6 +1201,11 @@ def run_ours(args, rank, world, local):
         "pairs_per_step": int(pairs), "cuda_graph": not args.no_graph,
         "parallelism": "replicas only (one workload per GPU)",
         "l2_flush": "no: the step streams >256 MB of complex grids (> 126 MB L2)",
+        "tile_variants": {"forward": int(tuned[0]), "adjoint": int(tuned[1]),
+                          "table": "forward (frequencies/thread, threads): 0 (4,128) 1 (2,128) "
+                                   "2 (4,256) 3 (8,64) 4 (4,128) 5 (2,256); adjoint "
+                                   "(faces/thread, threads): 0 (2,128) 1 (1,128) 2 (2,64) "
+                                   "3 (1,256) 4 (2,128) 5 (1,128); 2 per thread = paired FP32"},
         "loss_last_step": loss_end})
     out = {
         "metric": METRIC if args.workload == "fit200" else METRIC_BATCH,
