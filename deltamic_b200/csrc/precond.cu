@@ -6,8 +6,9 @@
 // and its optimize.py:207-212 forms the same operator densely as
 // inv(M) @ inv(M).  Here the dense operator P (nv x nv, float32, rows padded to a
 // multiple of 4) is built once per topology and applied every step by an
-// HBM-bound product: each warp streams four rows of P with 16-byte loads and
-// multiplies them with the matching 4 x 3 block of g, read through L1.
+// HBM-bound product: each warp streams eight rows of P with 16-byte loads (sixteen
+// in flight per lane) and multiplies them with the matching 4 x 3 block of g, read
+// through L1 as three 16-byte loads.
 // The optimizer is VectorAdam of optimize.py:215-258 (axis -1): the second
 // moment of each vertex is the squared norm of its 3-vector gradient.
 #include <cuda_runtime.h>
@@ -22,14 +23,14 @@
 namespace dm {
 namespace {
 
-constexpr int kRowsPerWarp = 4;
-constexpr int kGemvThreads = 256;
+constexpr int kRowsPerWarp = 8;
+constexpr int kGemvThreads = 128;
 
 // out[r][d] = sum_c P[r][c] g[c][d] for d < 3; P row stride ldp (multiple of 4),
 // g and out [nv][3] (g read through the read-only cache).
 __global__ void __launch_bounds__(kGemvThreads)
     k_precond_gemv(const float* __restrict__ P, int64_t nv, int64_t ldp,
-                   const float* __restrict__ g, float* __restrict__ out) {
+                   const float* __restrict__ g, float* __restrict__ out, bool g16) {
   const int64_t warp = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t r0 = warp * kRowsPerWarp;
@@ -55,12 +56,21 @@ __global__ void __launch_bounds__(kGemvThreads)
     for (int u = 0; u < 2; ++u) {
       const int64_t c = 4 * (q0 + 32 * u);
       float gv[12];
+      if (c + 4 <= nv && g16) {
+        // g[c..c+3][0..2]: twelve floats at a 48c-byte offset, three 16-byte loads
+        const float4* g4 = reinterpret_cast<const float4*>(g + 3 * c);
+        const float4 a = __ldg(g4), b = __ldg(g4 + 1), e = __ldg(g4 + 2);
+        gv[0] = a.x; gv[1] = a.y; gv[2] = a.z; gv[3] = a.w;
+        gv[4] = b.x; gv[5] = b.y; gv[6] = b.z; gv[7] = b.w;
+        gv[8] = e.x; gv[9] = e.y; gv[10] = e.z; gv[11] = e.w;
+      } else {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const bool live = c + k < nv;
-        gv[3 * k + 0] = live ? __ldg(g + 3 * (c + k) + 0) : 0.f;
-        gv[3 * k + 1] = live ? __ldg(g + 3 * (c + k) + 1) : 0.f;
-        gv[3 * k + 2] = live ? __ldg(g + 3 * (c + k) + 2) : 0.f;
+        for (int k = 0; k < 4; ++k) {
+          const bool live = c + k < nv;
+          gv[3 * k + 0] = live ? __ldg(g + 3 * (c + k) + 0) : 0.f;
+          gv[3 * k + 1] = live ? __ldg(g + 3 * (c + k) + 1) : 0.f;
+          gv[3 * k + 2] = live ? __ldg(g + 3 * (c + k) + 2) : 0.f;
+        }
       }
 #pragma unroll
       for (int i = 0; i < kRowsPerWarp; ++i) {
@@ -79,7 +89,7 @@ __global__ void __launch_bounds__(kGemvThreads)
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       for (int o = 16; o > 0; o >>= 1) acc[i][d] += __shfl_xor_sync(0xffffffffu, acc[i][d], o);
-  if (lane < kRowsPerWarp * 3) {
+  if (lane < kRowsPerWarp * 3) {  // 24 lanes write the 8 x 3 outputs
     const int i = lane / 3, d = lane % 3;
     if (r0 + i < nv) {
       float v = 0.f;
@@ -139,8 +149,8 @@ int dm_precond_apply(const float* P, int64_t nv, int64_t ldp, const float* grad,
   const int64_t warps = (nv + kRowsPerWarp - 1) / kRowsPerWarp;
   const int64_t blocks = (warps * 32 + kGemvThreads - 1) / kGemvThreads;
   if (blocks > INT32_MAX) return DM_ERR_SIZE;
-  k_precond_gemv<<<(unsigned)blocks, kGemvThreads, 0, (cudaStream_t)stream>>>(P, nv, ldp, grad,
-                                                                             out);
+  k_precond_gemv<<<(unsigned)blocks, kGemvThreads, 0, (cudaStream_t)stream>>>(
+      P, nv, ldp, grad, out, ((uintptr_t)grad & 15) == 0);
   count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
