@@ -137,6 +137,11 @@ SIGNATURES = {
                                           ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _SZ, _P]),
     "dm_image_loss_workspace_size": (_SZ, [_I64]),
     "dm_image_loss": (_INT, [_P, _I64, _INT, _P, _F, _P, _P, _P, _P, _SZ, _P]),
+    "dm_normalize_workspace_size": (_SZ, [_I64]),
+    "dm_normalize": (_INT, [_P, _I64, ctypes.c_double, _P, _P, _P, _SZ, _P]),
+    "dm_normalize_backward": (_INT, [_P, _P, _I64, ctypes.c_double, _P, _P, _P, _SZ, _P]),
+    "dm_normalize64": (_INT, [_P, _I64, ctypes.c_double, _P, _P, _P, _SZ, _P]),
+    "dm_normalize64_backward": (_INT, [_P, _P, _I64, ctypes.c_double, _P, _P, _P, _SZ, _P]),
     "dm_band_bounds": (_INT, [_P, _I64, _BOXP, _P, _P]),
     "dm_render_loss_bandbox_supported": (_INT, [_BOXP, ctypes.POINTER(ctypes.c_int32)]),
     "dm_render_loss_bandbox_workspace_size": (_SZ, [_BOXP, ctypes.POINTER(ctypes.c_int32)]),

@@ -598,14 +598,18 @@ __global__ void __launch_bounds__(kLineThreads)
           if (kind == 0) {
             L += nv;
             gn = 1.0f;
-          } else {
+          } else if (kind == 1) {
             const float dlt = nv - tv[u];
             L += (double)dlt * dlt;
             gn = 2.0f * dlt * nseg_inv;
+          } else {
+            gn = tv[u];  // kind 2: dL/d|z| given, no normalisation
           }
-          dmn += (double)gn * (-(1.0 - (double)uu));
-          dmx += (double)gn * (-(double)uu);
-          const float gg = gn * inv;
+          if (kind != 2) {
+            dmn += (double)gn * (-(1.0 - (double)uu));
+            dmx += (double)gn * (-(double)uu);
+          }
+          const float gg = kind == 2 ? gn : gn * inv;
           const float sc = a > 0.f ? __fdividef(gg, a) : 0.f;
           g = make_float2(sc * zi.x, sc * zi.y);
         }
@@ -722,7 +726,7 @@ __global__ void __launch_bounds__(kLineThreads)
     hdr->fin[2] = f2;
     hdr->add_mn = hdr->cmn > 0 ? (float)(f1 / (double)hdr->cmn) : 0.f;
     hdr->add_mx = hdr->cmx > 0 ? (float)(f2 / (double)hdr->cmx) : 0.f;
-    hdr->ties_full = (hdr->cmn >= 2 || hdr->cmx >= 2) ? 1 : 0;
+    hdr->ties_full = (kind != 2 && (hdr->cmn >= 2 || hdr->cmx >= 2)) ? 1 : 0;
     if (loss) loss[0] = (float)f0;
   }
 }
@@ -1054,7 +1058,8 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
                            dm_stream_t stream) {
   if (!box || !bounds || !workspace || !loss || n_band <= 0 || !band_index || !ft_list)
     return DM_ERR_INVALID_ARG;
-  if ((kind != 0 && kind != 1) || (kind == 1 && !target)) return DM_ERR_INVALID_ARG;
+  if (kind < 0 || kind > 2 || (kind == 1 && !target) || (kind == 2 && grad_list && !target))
+    return DM_ERR_INVALID_ARG;
   if (!dm_render_loss_bandbox_supported(box, bounds)) return DM_ERR_UNSUPPORTED;
   if (n_band > (int64_t)INT32_MAX) return DM_ERR_SIZE;
   const size_t need = dm_render_loss_bandbox_workspace_size(box, bounds);
@@ -1105,6 +1110,11 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
     default: e = zlines<8>(s, w, inv_n, image, st); break;
   }
   if (e != cudaSuccess) return DM_ERR_CUDA;
+  if (kind == 2 && !grad_list) {  // the image alone
+    if (cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess) return DM_ERR_CUDA;
+    count_launches(launches + 1);
+    return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  }
   switch (s.ldj / 8) {
     case 1: e = gradlines<1>(s, w, kind, target, contrast, loss, st); break;
     case 2: e = gradlines<2>(s, w, kind, target, contrast, loss, st); break;

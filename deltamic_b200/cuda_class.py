@@ -58,7 +58,9 @@ class MeshFTCUDA:
         # the reference returns no coefficient gradient
         if f64:
             return ops.meshft64(Verts, Faces, Faces_coeff.detach().double(), grid, band)
-        return ops.meshft(Verts, Faces, Faces_coeff.detach().float(), grid, band)
+        out = ops.meshft(Verts, Faces, Faces_coeff.detach().float(), grid, band)
+        out._dm_band = (band, grid, out._version)  # zero off this band (band-box render)
+        return out
 
 
 def _off_grid(Verts, Faces, Faces_coeff, xi0, xi1, xi2, Filter, narrowband_thresh):

@@ -616,6 +616,101 @@ def render_loss_bandbox(ft, band, plan: BandBox, otf, kind="sum", target=None, c
     return loss, img, G
 
 
+def render_bandbox_image(ft, band, plan: BandBox, otf):
+    """|ifftn(S)| over the box for S = ft * otf on the band and 0 elsewhere
+    (render_image_from_ftmesh of a band-limited spectrum), by the band-box DFTs."""
+    lib = N.lib()
+    if not plan.supported:
+        raise N.DeltaMicError(N.DM_ERR_UNSUPPORTED, "render_bandbox_image")
+    N.require_cuda(ft, "ft", torch.complex64)
+    N.require_cuda(otf, "OTF", torch.float32)
+    dev = ft.device
+    loss = torch.empty(1, dtype=torch.float32, device=dev)
+    img = torch.empty(plan.grid.shape, dtype=torch.float32, device=dev)
+    ws = N.WORKSPACES.get("bandbox", plan.ws_bytes, dev)
+    N.check(lib.dm_render_loss_bandbox(
+        N.ptr(ft), N.ptr(band), band.numel(), ctypes.byref(plan.box), plan.bounds, N.ptr(otf), 2,
+        None, 0.0, N.ptr(loss), None, N.ptr(img), N.ptr(ws), ws.numel(), N.stream_ptr(dev)),
+        "dm_render_loss_bandbox")
+    return img
+
+
+def render_bandbox_adjoint(ft, band, plan: BandBox, otf, grad_image):
+    """G = fftn(dL/dz) on the band for the cotangent ``grad_image`` = dL/d|z| of
+    :func:`render_bandbox_image`; dL/dS on the band is G / numel."""
+    lib = N.lib()
+    if not plan.supported:
+        raise N.DeltaMicError(N.DM_ERR_UNSUPPORTED, "render_bandbox_adjoint")
+    N.require_cuda(ft, "ft", torch.complex64)
+    N.require_cuda(otf, "OTF", torch.float32)
+    N.require_cuda(grad_image, "grad_image", torch.float32)
+    if grad_image.numel() != plan.grid.numel:
+        raise ValueError("grad_image must have the image's shape")
+    dev = ft.device
+    loss = torch.empty(1, dtype=torch.float32, device=dev)
+    G = torch.empty_like(ft)
+    ws = N.WORKSPACES.get("bandbox", plan.ws_bytes, dev)
+    N.check(lib.dm_render_loss_bandbox(
+        N.ptr(ft), N.ptr(band), band.numel(), ctypes.byref(plan.box), plan.bounds, N.ptr(otf), 2,
+        N.ptr(grad_image), 0.0, N.ptr(loss), N.ptr(G), None, N.ptr(ws), ws.numel(),
+        N.stream_ptr(dev)), "dm_render_loss_bandbox")
+    return G
+
+
+# ---------------------------------------------------------------------------
+# normalize_tensor (render.py:5-6)
+
+def normalize_stats(t, contrast=0.0, want_out=True):
+    """(out | None, stats[2] = (min, max)) of normalize_tensor for a contiguous
+    float32 / float64 CUDA tensor ``t``."""
+    if t.dtype not in (torch.float32, torch.float64):
+        raise TypeError(f"normalize runs on float32 / float64 tensors, not {t.dtype}")
+    N.require_cuda(t, "t", t.dtype)
+    if t.numel() == 0:
+        raise RuntimeError("normalize_tensor of an empty tensor (min() has no value)")
+    lib = N.lib()
+    f = lib.dm_normalize64 if t.dtype == torch.float64 else lib.dm_normalize
+    stats = torch.empty(2, dtype=t.dtype, device=t.device)
+    out = torch.empty_like(t) if want_out else None
+    ws = N.WORKSPACES.get("normalize", lib.dm_normalize_workspace_size(t.numel()), t.device)
+    N.check(f(N.ptr(t), t.numel(), float(contrast), N.ptr(out), N.ptr(stats), N.ptr(ws),
+              ws.numel(), N.stream_ptr(t.device)), "dm_normalize")
+    return out, stats
+
+
+def normalize_backward(t, grad_out, stats, contrast=0.0):
+    """dL/dt of normalize_tensor for the cotangent ``grad_out``."""
+    lib = N.lib()
+    f = lib.dm_normalize64_backward if t.dtype == torch.float64 else lib.dm_normalize_backward
+    g = grad_out.contiguous()
+    if g.dtype != t.dtype:
+        g = g.to(t.dtype)
+    out = torch.empty_like(t)
+    ws = N.WORKSPACES.get("normalize", lib.dm_normalize_workspace_size(t.numel()), t.device)
+    N.check(f(N.ptr(t), N.ptr(g), t.numel(), float(contrast), N.ptr(stats), N.ptr(out),
+              N.ptr(ws), ws.numel(), N.stream_ptr(t.device)), "dm_normalize_backward")
+    return out
+
+
+class _Normalize(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, t, contrast):
+        out, stats = normalize_stats(t, contrast)
+        ctx.save_for_backward(t, stats)
+        ctx.contrast = contrast
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        t, stats = ctx.saved_tensors
+        return normalize_backward(t, g, stats, ctx.contrast), None
+
+
+def normalize(t, contrast=0.0):
+    """Differentiable normalize_tensor on the device kernels (gradient to ``t``)."""
+    return _Normalize.apply(t.contiguous(), float(contrast))
+
+
 def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
     lib = N.lib()
     N.check(lib.dm_adam_step(N.ptr(param), N.ptr(grad), N.ptr(exp_avg), N.ptr(exp_avg_sq),

@@ -20,9 +20,13 @@ Same names, arguments and results as the reference:
 Differences, all deliberate: the module runs on CUDA only (``device='cpu'``
 raises -- there is no CPU fallback).  ``dtype=torch.float32`` runs the float32
 kernels (fixed-point phases; error against a float64 evaluation ~1e-6);
-``dtype=torch.float64`` runs the float64 kernels (the reference's double
-arithmetic, Seps = sqrt(DBL_EPSILON), band selected on the float64 OTF) and
-returns complex128.  In the autofluorescence transform the
+``dtype=torch.float64`` runs the float64 kernels (the double arithmetic of the
+reference's CPU path, Seps = sqrt(1.19209e-07), band selected on the float64 OTF)
+and returns complex128.  ``render_image_from_ftmesh`` of a float32 spectrum that
+``Fourier3dMesh`` returned (unmodified) runs the band-box DFTs of bandbox.cu,
+which touch only the band's bounding box; other spectra take
+``abs(ifftn(ftmesh * OTF))`` on cuFFT.  ``normalize_tensor`` of a CUDA float32 /
+float64 tensor runs the kernels of normalize.cu.  In the autofluorescence transform the
 reference's value at xi = 0 (grids with every axis odd) is 0/0 = NaN; here it is
 the limit of its volume term, ``1 - regint`` in all.
 """
@@ -42,9 +46,17 @@ __all__ = ["Fourier3dMesh", "render_image_from_ftmesh", "normalize_tensor",
 
 
 def normalize_tensor(t, contrast_variable=0):
-    """Min-max normalisation ``((t - min)/(max - min) + c)/(1 + c)``."""
+    """Min-max normalisation ``((t - min)/(max - min) + c)/(1 + c)`` (render.py:5-6).
+
+    A non-empty float32 / float64 CUDA tensor with a constant ``c`` runs the
+    device kernels (two launches forward, two backward; gradient to ``t``).  A
+    ``c`` that requires grad, or a host tensor, takes the eager expression."""
+    c = contrast_variable
+    if (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype in (torch.float32, torch.float64)
+            and t.numel() > 0 and not (isinstance(c, torch.Tensor) and c.requires_grad)):
+        return ops.normalize(t, float(c))
     lo, hi = t.min(), t.max()
-    return ((t - lo) / (hi - lo) + contrast_variable) / (1 + contrast_variable)
+    return ((t - lo) / (hi - lo) + c) / (1 + c)
 
 
 def compute_box_size(verts, offset=0.1):
@@ -83,8 +95,85 @@ def center_verts_in_box(verts, box_size, offset=0.4):
     return verts
 
 
+_BB_PLANS: dict = {}
+
+
+def _bandbox_plan(grid, band):
+    """Cached (band-box plan, int64 band) of ``band`` on ``grid``: one host sync per
+    new band.  The entry holds the band tensor itself, so its memory cannot be
+    reused by another band while the entry lives."""
+    key = (tuple(grid.box_size.ravel().tolist()), grid.shape, id(band), band._version)
+    hit = _BB_PLANS.get(key)
+    if hit is not None and hit[0] is band:
+        return hit[1], hit[2]
+    if len(_BB_PLANS) >= 8:
+        _BB_PLANS.pop(next(iter(_BB_PLANS)))
+    plan = ops.BandBox(grid, band)
+    band64 = band.long()
+    _BB_PLANS[key] = (band, plan, band64)
+    return plan, band64
+
+
+class _BandImage(torch.autograd.Function):
+    """``|ifftn(ftmesh * OTF)|`` of a spectrum that is zero outside ``band``, by the
+    band-box DFTs; backward gives the dense dL/dftmesh (zero off the band) and,
+    for a real OTF, dL/dOTF = Re(conj(ftmesh) dL/dS)."""
+
+    @staticmethod
+    def forward(ctx, ftmesh, OTF, band, plan, band64):
+        ft = ftmesh.reshape(-1).index_select(0, band64)
+        otf = OTF.contiguous()
+        img = ops.render_bandbox_image(ft, band, plan, otf)
+        ctx.save_for_backward(ft, otf, band, band64)
+        ctx.plan = plan
+        ctx.shape = tuple(ftmesh.shape)
+        return img
+
+    @staticmethod
+    def backward(ctx, g):
+        ft, otf, band, band64 = ctx.saved_tensors
+        plan = ctx.plan
+        G = ops.render_bandbox_adjoint(ft, band, plan, otf, g.contiguous().float())
+        gS = G * (1.0 / plan.grid.numel)  # dL/dS on the band
+        g_ft = g_otf = None
+        if ctx.needs_input_grad[0]:
+            g_ft = torch.zeros(ctx.shape, dtype=torch.complex64, device=ft.device)
+            g_ft.view(-1).index_copy_(0, band64, gS * otf.view(-1).index_select(0, band64))
+        if ctx.needs_input_grad[1]:
+            g_otf = torch.zeros(ctx.shape, dtype=torch.float32, device=ft.device)
+            g_otf.view(-1).index_copy_(0, band64, (gS * ft.conj()).real)
+        return g_ft, g_otf, None, None, None
+
+
+def _band_route(ftmesh, OTF, box_shape):
+    info = getattr(ftmesh, "_dm_band", None)
+    if info is None or info[2] != ftmesh._version or ftmesh.dtype != torch.complex64:
+        return None
+    if not (isinstance(OTF, torch.Tensor) and OTF.is_cuda and OTF.dtype == torch.float32
+            and OTF.device == ftmesh.device and tuple(OTF.shape) == tuple(ftmesh.shape)):
+        return None
+    try:
+        if [int(b) for b in box_shape] != list(ftmesh.shape):
+            return None
+    except (TypeError, ValueError):
+        return None
+    band, grid = info[0], info[1]
+    if band.numel() == 0:
+        return None
+    plan, band64 = _bandbox_plan(grid, band)
+    return (band, plan, band64) if plan.supported else None
+
+
 def render_image_from_ftmesh(ftmesh, OTF, box_shape):
-    """``|ifftn(ftmesh * OTF)|`` over ``box_shape`` (cuFFT through torch.fft)."""
+    """``|ifftn(ftmesh * OTF)|`` over ``box_shape`` (render.py:177-180).
+
+    For a float32 spectrum straight from :class:`Fourier3dMesh` (zero off its
+    narrow band; no in-place change since) with a real float32 OTF of the same
+    shape, the image comes from the band-box DFTs; otherwise from cuFFT."""
+    route = _band_route(ftmesh, OTF, box_shape)
+    if route is not None:
+        band, plan, band64 = route
+        return _BandImage.apply(ftmesh, OTF, band, plan, band64)
     return torch.abs(torch.fft.ifftn(ftmesh * OTF, list(box_shape)))
 
 
@@ -148,7 +237,10 @@ class Fourier3dMesh(nn.Module):
         if self.dtype == torch.float64:
             return ops.meshft64(Verts.double(), Faces, Faces_coeff.double(), self.grid,
                                 self.band())
-        return ops.meshft(Verts, Faces, Faces_coeff, self.grid, self.band())
+        band = self.band()
+        out = ops.meshft(Verts, Faces, Faces_coeff, self.grid, band)
+        out._dm_band = (band, self.grid, out._version)  # zero off this band
+        return out
 
 
 # ---------------------------------------------------------------------------

@@ -456,6 +456,27 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
                   dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * normalize_tensor (render.py:5-6) of a real array t[n] (any shape, contiguous):
+ *   out = ((t - min t) / (max t - min t) + c) / (1 + c),   c = contrast
+ * in the operation order of the eager expression on a CUDA tensor (the scalar
+ * division as a product with its reciprocal).  min / max propagate NaN.
+ * dm_normalize writes stats[2] = (min, max) (DEVICE) and, if out is not NULL,
+ * out[n].  dm_normalize_backward takes those stats and dL/dout and writes dL/dt,
+ * the min / max terms shared evenly by tied elements (torch's rule for full
+ * min() / max() reductions).  Deterministic; 2 launches each. */
+size_t dm_normalize_workspace_size(int64_t n);
+int dm_normalize(const float* t, int64_t n, double contrast, float* out, float* stats,
+                 void* workspace, size_t ws_bytes, dm_stream_t stream);
+int dm_normalize_backward(const float* t, const float* grad_out, int64_t n, double contrast,
+                          const float* stats, float* grad_t, void* workspace, size_t ws_bytes,
+                          dm_stream_t stream);
+int dm_normalize64(const double* t, int64_t n, double contrast, double* out, double* stats,
+                   void* workspace, size_t ws_bytes, dm_stream_t stream);
+int dm_normalize64_backward(const double* t, const double* grad_out, int64_t n, double contrast,
+                            const double* stats, double* grad_t, void* workspace,
+                            size_t ws_bytes, dm_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Band-box render: the chain render_image_from_ftmesh -> normalize_tensor ->
  * loss of the reference fitting loop (render.py:177-180, render.py:5-6,
  * Examples/Gradient_Descent.ipynb cell 2) and its backward to the spectrum,
@@ -475,7 +496,13 @@ int dm_image_loss(const float* z, int64_t n, int kind, const float* target, floa
  * contrast and min / max tie rule).  Writes *loss (DEVICE float), optionally
  * image[n] = |z|, and, if grad_list is not NULL, grad_list[n_band] = fftn(dL/dz)
  * at the band voxels (complex64): the cotangent dm_meshft_backward takes as
- * grad_list with otf and grad_scale = 1/n.  Deterministic. */
+ * grad_list with otf and grad_scale = 1/n.  Deterministic.
+ * kind 2 renders without a loss: ``target`` then holds a cotangent dL/dimage[n]
+ * of the image |z| itself (no normalisation; *loss is written as 0), and
+ * grad_list receives fftn(dL/dz) at the band voxels for it -- the adjoint of
+ * render_image_from_ftmesh (render.py:177-180) for a band-limited spectrum.
+ * With kind 2 and grad_list NULL the call only renders (image, *loss = 0) and
+ * target may be NULL. */
 int dm_band_bounds(const int32_t* band_index, int64_t n_band, const dm_box* box,
                    int32_t* bounds, dm_stream_t stream);
 int dm_render_loss_bandbox_supported(const dm_box* box, const int32_t bounds[6]);
