@@ -624,6 +624,9 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
       case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 4: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 5: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 6: k_meshft_bwd<2, 128, kBwdTX, kStages, false, XiRec, 5><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 7: k_meshft_bwd<2, 128, kBwdTX, kStages, false, XiRec, 6><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
+      case 8: k_meshft_bwd<1, 128, kBwdTX, kStages, false, XiRec, 8><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
     }
     profile_end(1, st);

@@ -75,3 +75,34 @@ def test_batch_fit_step_graph_equals_eager():
         la, lb = float(a()[0]), float(b()[0])
         assert abs(la - lb) <= 1e-6 * abs(lb)
     assert torch.equal(a.V, b.V)
+
+
+def test_batch_cells_match_oracle_pipeline():
+    """Every cell of a batch against the float64 oracle chain (meshFT -> render ->
+    normalise -> mse -> gradients), with the float32 chain's noise floor."""
+    cells = _cells(4, seed=7)
+    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV)
+    br.set_sigmas([c[5] for c in cells])
+    br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
+    V = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV,
+                     requires_grad=True)
+    C = torch.tensor(np.concatenate([c[2] for c in cells]), dtype=torch.float32, device=DEV,
+                     requires_grad=True)
+    rng = np.random.default_rng(8)
+    target = torch.tensor(rng.uniform(0, 1, br.grid_elems), dtype=torch.float32, device=DEV)
+    loss = br.loss(V, C, "mse", target)
+    loss.backward()
+    vo = np.cumsum([0] + [len(c[0]) for c in cells])
+    fo = np.cumsum([0] + [len(c[1]) for c in cells])
+    total = 0.0
+    for i, (v, f, c, box, shape, sig) in enumerate(cells):
+        t64 = br.cell_view(target, i).cpu().double().numpy()
+        o = oracle.pipeline(v, f, c, box, shape, sig, 1e-5, loss="mse", target=t64)
+        fl = oracle.chain_floor(v, f, c, box, shape, sig, 1e-5, "mse", t64)
+        total += o["loss"]
+        ev = rel_l2(V.grad[vo[i]:vo[i + 1]].cpu().numpy(), o["grad_verts"])
+        ec = rel_l2(C.grad[fo[i]:fo[i + 1]].cpu().numpy(), o["grad_coeff"])
+        print(f"cell {i} {shape}: verts {ev:.2e} coeff {ec:.2e} floor {fl}")
+        assert ev < max(2e-4, 2 * fl["verts"])
+        assert ec < max(1e-4, 2 * fl["coeff"])
+    assert abs(float(loss) - total) < 1e-4 * abs(total)
