@@ -152,6 +152,8 @@ SIGNATURES = {
     "dm_conv3d_s2_device_error": (_INT, [ctypes.POINTER(_INT), _P]),
     "dm_conv3d_s2_backward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P, _P, _P,
                                      _P, _P, _SZ, _P]),
+    "dm_conv3d_s2_backward_bf16": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P,
+                                          _P, _P, _P, _P, _SZ, _P]),
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
     "dm_precond_apply": (_INT, [_P, _I64, _I64, _P, _P, _P]),

@@ -420,13 +420,27 @@ struct FwdEp {
 
 // dP = dact * GELU'(pre) in BF16; four elements per thread (n is a multiple of 16,
 // pointers 16-byte aligned), else one.
-template <bool kVec>
-__global__ void k_gelu_back(const float* __restrict__ pre, const float* __restrict__ dact,
+__device__ __forceinline__ float ld_grad(const float* g, int64_t i) { return g[i]; }
+__device__ __forceinline__ float ld_grad(const bf16* g, int64_t i) {
+  return __bfloat162float(g[i]);
+}
+__device__ __forceinline__ float4 ld_grad4(const float* g, int64_t i) {
+  return reinterpret_cast<const float4*>(g)[i];
+}
+__device__ __forceinline__ float4 ld_grad4(const bf16* g, int64_t i) {
+  const uint2 u = reinterpret_cast<const uint2*>(g)[i];
+  return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+                     __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+}
+
+// dL/dpre = dL/dact * GELU'(pre) in BF16; dL/dact in FP32 or BF16 (TG).
+template <bool kVec, class TG>
+__global__ void k_gelu_back(const float* __restrict__ pre, const TG* __restrict__ dact,
                             bf16* __restrict__ dpre, int64_t n) {
   if (kVec) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 4;
          i += (int64_t)gridDim.x * blockDim.x) {
-      const float4 p = ((const float4*)pre)[i], g = ((const float4*)dact)[i];
+      const float4 p = ((const float4*)pre)[i], g = ld_grad4(dact, i);
       ((uint2*)dpre)[i] = make_uint2(pack2(__float2bfloat16(g.x * gelu_grad(p.x)),
                                            __float2bfloat16(g.y * gelu_grad(p.y))),
                                      pack2(__float2bfloat16(g.z * gelu_grad(p.z)),
@@ -435,7 +449,7 @@ __global__ void k_gelu_back(const float* __restrict__ pre, const float* __restri
   } else {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-      dpre[i] = __float2bfloat16(dact[i] * gelu_grad(pre[i]));
+      dpre[i] = __float2bfloat16(ld_grad(dact, i) * gelu_grad(pre[i]));
   }
 }
 
@@ -720,6 +734,7 @@ struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
 };
 struct DgradEp {
   float* dx;
+  bf16* dxb;  // BF16 output instead of dx when not NULL
   ConvShape s;
   ClsSet set;
   Cls c;
@@ -733,7 +748,27 @@ struct DgradEp {
     if (c0 >= s.Ci) return;
     int b, d, h, w;
     cls_voxel(c, q, b, d, h, w);
-    float* r = dx + ((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + c0;
+    const int64_t at = ((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * s.Ci + c0;
+    if (dxb) {
+      bf16* r = dxb + at;
+      if (vec) {
+#pragma unroll
+        for (int q8 = 0; q8 < 2; ++q8) {
+          uint32_t u[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            u[j] = pack2(__float2bfloat16(v[8 * q8 + 2 * j]),
+                         __float2bfloat16(v[8 * q8 + 2 * j + 1]));
+          *(uint4*)(r + 8 * q8) = make_uint4(u[0], u[1], u[2], u[3]);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (c0 + j < s.Ci) r[j] = __float2bfloat16(v[j]);
+      }
+      return;
+    }
+    float* r = dx + at;
     if (vec) {
 #pragma unroll
       for (int q4 = 0; q4 < 4; ++q4)
@@ -825,16 +860,37 @@ __device__ __forceinline__ int64_t c1_tiles(const ConvShape& s) {
   return (int64_t)s.B * s.Do * ((s.Ho + kC1TH - 1) / kC1TH) * ((s.Wo + kC1TW - 1) / kC1TW);
 }
 
-// Input footprint of a tile into xs[3][17][65] (zero outside the volume).
+// Input footprint of a tile in shared memory, columns de-interleaved: row r of
+// plane p holds the even columns 0, 2, .., 64 at [0, 33) and the odd columns
+// 1, 3, .., 63 at [34, 66), rows kC1RS apart, planes kC1PS apart (zero outside the
+// volume).  Output column tx, tap kw then reads offset kC1Col[kw] + tx: consecutive
+// across the lanes of a forward warp (one voxel per lane), and, with the strides
+// = 3 and 9 (mod 32) banks, 27 distinct banks across the lanes of a weight-gradient
+// warp (one tap per lane).
+constexpr int kC1RS = 67, kC1PS = 1161, kC1XS = 3 * kC1PS;
+constexpr int kC1Load = (3 * kC1IH * kC1IW + 255) / 256;  // footprint loads per thread
+
+__device__ __forceinline__ int c1_col(int kw) { return kw == 0 ? 0 : (kw == 1 ? 34 : 1); }
+
 __device__ __forceinline__ void c1_load(const bf16* __restrict__ x, const ConvShape& s,
                                         const C1Tile& tl, float* xs) {
-  for (int i = threadIdx.x; i < 3 * kC1IH * kC1IW; i += blockDim.x) {
+  bf16 v[kC1Load];
+  // all loads first (independent), then the shared-memory stores
+#pragma unroll
+  for (int u = 0; u < kC1Load; ++u) {
+    const int i = threadIdx.x + 256 * u;
     const int c = i % kC1IW, r = (i / kC1IW) % kC1IH, pz = i / (kC1IW * kC1IH);
     const int d = 2 * tl.od - 1 + pz, h = 2 * tl.oh0 - 1 + r, w = 2 * tl.ow0 - 1 + c;
-    float v = 0.f;
-    if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-      v = __bfloat162float(x[(((int64_t)tl.b * s.D + d) * s.H + h) * s.W + w]);
-    xs[i] = v;
+    v[u] = __float2bfloat16(0.f);
+    if (i < 3 * kC1IH * kC1IW && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
+      v[u] = x[(((int64_t)tl.b * s.D + d) * s.H + h) * s.W + w];
+  }
+#pragma unroll
+  for (int u = 0; u < kC1Load; ++u) {
+    const int i = threadIdx.x + 256 * u;
+    if (i >= 3 * kC1IH * kC1IW) continue;
+    const int c = i % kC1IW, r = (i / kC1IW) % kC1IH, pz = i / (kC1IW * kC1IH);
+    xs[pz * kC1PS + r * kC1RS + ((c & 1) ? 34 + (c >> 1) : (c >> 1))] = __bfloat162float(v[u]);
   }
 }
 
@@ -845,9 +901,9 @@ __global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, C
                                                    const float* __restrict__ bias,
                                                    float* __restrict__ pre,
                                                    bf16* __restrict__ act) {
-  __shared__ float xs[3 * kC1IH * kC1IW];
-  __shared__ float ws[27][CO];
-  __shared__ float bs[CO];
+  __shared__ float xs[kC1XS];
+  __shared__ __align__(16) float ws[27][CO];
+  __shared__ __align__(16) float bs[CO];
   for (int i = threadIdx.x; i < 27 * CO; i += blockDim.x)
     ws[i / CO][i % CO] = __bfloat162float(w[i]);  // rows 0..26 of W[Kp][Co]
   if (threadIdx.x < CO) bs[threadIdx.x] = bias ? bias[threadIdx.x] : 0.f;
@@ -866,7 +922,7 @@ __global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, C
     for (int kh = 0; kh < 3; ++kh)
 #pragma unroll
       for (int kw = 0; kw < 3; ++kw) {
-        const float xv = xs[(kd * kC1IH + 2 * ty + kh) * kC1IW + 2 * tx + kw];
+        const float xv = xs[kd * kC1PS + (2 * ty + kh) * kC1RS + c1_col(kw) + tx];
         const int tap = (kd * 3 + kh) * 3 + kw;
 #pragma unroll
         for (int c = 0; c < CO; ++c) acc[c] = fmaf(xv, ws[tap][c], acc[c]);
@@ -891,58 +947,84 @@ __global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, C
 // Weight and bias gradient partials: block g sums its tiles (g, g + G, ...) into
 // part[g][(Kp + 1) * CO] (rows 0..26 taps, 27..Kp-1 zero, row Kp the bias);
 // k_sum_splits adds the blocks in order.  dP is the BF16 dL/dpre of k_gelu_back.
+// Lane l of every warp owns tap l (l = 27: the bias, input 1; lanes 28..31 idle)
+// and all CO channels; warp w takes the tile's voxels w, w + 8, ..: per voxel one
+// shared-memory read of the input (27 banks) and CO / 4 broadcast 16-byte reads of
+// the voxel's dP row.  The eight warps' sums are added in warp order at the end.
 template <int CO>
 __global__ void __launch_bounds__(256) k_conv1_wgrad(const bf16* __restrict__ x, ConvShape s,
                                                      const bf16* __restrict__ dp,
                                                      float* __restrict__ part) {
-  __shared__ float xs[3 * kC1IH * kC1IW];
-  __shared__ float ds[kC1TH * kC1TW][CO + 1];
-  constexpr int NO = 27 * CO + CO;  // tap x channel outputs, then the bias
-  constexpr int PER = (NO + 255) / 256;
-  float acc[PER];
+  constexpr int NV = kC1TH * kC1TW;
+  // dP rows, then the footprint; after the last tile the warps' sums reuse the space
+  __shared__ __align__(16) float sm[NV * CO + kC1XS];
+  static_assert(8 * 28 * CO <= NV * CO + kC1XS, "reduction area");
+  float* ds = sm;
+  float* xs = sm + NV * CO;
+  float* red = sm;  // [8][28 * CO], after the loop
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tap = min(lane, 27);
+  const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+  const int xoff = kd * kC1PS + kh * kC1RS + c1_col(kw);
+  float acc[CO];
 #pragma unroll
-  for (int j = 0; j < PER; ++j) acc[j] = 0.f;
+  for (int c = 0; c < CO; ++c) acc[c] = 0.f;
   const int64_t ntl = c1_tiles(s);
   for (int64_t t = blockIdx.x; t < ntl; t += gridDim.x) {
     const C1Tile tl = c1_tile(s, t);
     __syncthreads();  // the previous tile's reads are done
     c1_load(x, s, tl, xs);
-    for (int i = threadIdx.x; i < kC1TH * kC1TW * CO; i += blockDim.x) {
-      const int v = i / CO, c = i % CO;
+    // dP rows of the tile's voxels, 16-byte loads (8 channels each)
+    constexpr int NQ = NV * CO / 8;
+#pragma unroll
+    for (int u = 0; u < (NQ + 255) / 256; ++u) {
+      const int q = threadIdx.x + 256 * u;
+      if (q >= NQ) continue;
+      const int v = q / (CO / 8), c0 = (q % (CO / 8)) * 8;
       const int oh = tl.oh0 + v / kC1TW, ow = tl.ow0 + v % kC1TW;
-      float g = 0.f;
+      uint4 g = make_uint4(0u, 0u, 0u, 0u);
       if (oh < s.Ho && ow < s.Wo)
-        g = __bfloat162float(
-            dp[((((int64_t)tl.b * s.Do + tl.od) * s.Ho + oh) * s.Wo + ow) * CO + c]);
-      ds[v][c] = g;
+        g = *reinterpret_cast<const uint4*>(
+            dp + ((((int64_t)tl.b * s.Do + tl.od) * s.Ho + oh) * s.Wo + ow) * CO + c0);
+      const uint32_t gw[4] = {g.x, g.y, g.z, g.w};
+      float4* d4 = reinterpret_cast<float4*>(ds + v * CO + c0);
+      float f[8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        f[2 * j] = __uint_as_float(gw[j] << 16);
+        f[2 * j + 1] = __uint_as_float(gw[j] & 0xffff0000u);
+      }
+      d4[0] = make_float4(f[0], f[1], f[2], f[3]);
+      d4[1] = make_float4(f[4], f[5], f[6], f[7]);
     }
     __syncthreads();
+    for (int v = warp; v < NV; v += 8) {
+      const int ty = v / kC1TW, tx = v % kC1TW;
+      const float xv = lane < 27 ? xs[xoff + 2 * ty * kC1RS + tx] : (lane == 27 ? 1.f : 0.f);
+      const float4* d4 = reinterpret_cast<const float4*>(ds + v * CO);
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-      const int o = threadIdx.x + 256 * j;
-      if (o >= NO) continue;
-      float a = 0.f;
-      if (o < 27 * CO) {
-        const int tap = o / CO, c = o % CO;
-        const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
-        for (int ty = 0; ty < kC1TH; ++ty) {
-          const float* xr = xs + (kd * kC1IH + 2 * ty + kh) * kC1IW + kw;
-#pragma unroll 8
-          for (int tx = 0; tx < kC1TW; ++tx) a = fmaf(xr[2 * tx], ds[ty * kC1TW + tx][c], a);
-        }
-      } else {
-        const int c = o - 27 * CO;
-        for (int v = 0; v < kC1TH * kC1TW; ++v) a += ds[v][c];
+      for (int q = 0; q < CO / 4; ++q) {
+        const float4 g = d4[q];
+        acc[4 * q] = fmaf(xv, g.x, acc[4 * q]);
+        acc[4 * q + 1] = fmaf(xv, g.y, acc[4 * q + 1]);
+        acc[4 * q + 2] = fmaf(xv, g.z, acc[4 * q + 2]);
+        acc[4 * q + 3] = fmaf(xv, g.w, acc[4 * q + 3]);
       }
-      acc[j] += a;
     }
   }
-  float* out = part + (int64_t)blockIdx.x * (s.Kp + 1) * CO;
+  __syncthreads();  // every warp is done with ds / xs
+  if (lane < 28) {
 #pragma unroll
-  for (int j = 0; j < PER; ++j) {
-    const int o = threadIdx.x + 256 * j;
-    if (o < 27 * CO) out[o] = acc[j];
-    else if (o < NO) out[(int64_t)s.Kp * CO + (o - 27 * CO)] = acc[j];
+    for (int c = 0; c < CO; ++c) red[warp * 28 * CO + lane * CO + c] = acc[c];
+  }
+  __syncthreads();
+  float* out = part + (int64_t)blockIdx.x * (s.Kp + 1) * CO;
+  for (int o = threadIdx.x; o < 28 * CO; o += blockDim.x) {
+    float a = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a += red[k * 28 * CO + o];
+    if (o < 27 * CO) out[o] = a;
+    else out[(int64_t)s.Kp * CO + (o - 27 * CO)] = a;
   }
   for (int o = 27 * CO + threadIdx.x; o < s.Kp * CO; o += blockDim.x) out[o] = 0.f;
 }
@@ -1014,19 +1096,27 @@ int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const 
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
+template <class TG>
+static void gelu_back(const float* pre, const TG* dact, bf16* dp, int64_t nout, cudaStream_t st) {
+  if (aligned16(pre) && aligned16(dact) && aligned16(dp))  // nout: a multiple of 16
+    k_gelu_back<true, TG><<<(unsigned)std::min<int64_t>((nout / 4 + 255) / 256, 148 * 16), 256,
+                            0, st>>>(pre, dact, dp, nout);
+  else
+    k_gelu_back<false, TG><<<(unsigned)std::min<int64_t>((nout + 255) / 256, 148 * 16), 256, 0,
+                             st>>>(pre, dact, dp, nout);
+}
+
 int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const float* pre,
-                         const float* dact, float* dx, float* dw, float* db, void* ws,
-                         cudaStream_t st) {
+                         const float* dact, const bf16* dact_b, float* dx, bf16* dx_b, float* dw,
+                         float* db, void* ws, cudaStream_t st) {
   char* base = (char*)ws;
   bf16* dp = (bf16*)base;
   float* part = (float*)(base + ((size_t)s.M * s.Co * sizeof(bf16) + 255) / 256 * 256);
   const int64_t nout = s.M * s.Co;
-  if (aligned16(pre) && aligned16(dact) && aligned16(dp))  // nout: a multiple of 16
-    k_gelu_back<true><<<(unsigned)std::min<int64_t>((nout / 4 + 255) / 256, 148 * 16), 256, 0,
-                        st>>>(pre, dact, dp, nout);
+  if (dact_b)
+    gelu_back(pre, dact_b, dp, nout, st);
   else
-    k_gelu_back<false><<<(unsigned)std::min<int64_t>((nout + 255) / 256, 148 * 16), 256, 0, st>>>(
-        pre, dact, dp, nout);
+    gelu_back(pre, dact, dp, nout, st);
   count_launches(1);
   // weight and bias gradients: rows = Kp + 1 (the last row of A^T is ones), the
   // reduction over m split across blockIdx.y
@@ -1052,7 +1142,7 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
                                                                           dw, db);
   count_launches(1);
   // data gradient: the eight parity classes of the input voxels in one launch
-  if (dx) {
+  if (dx || dx_b) {
     ClsSet set;
     int64_t max_rows = 0, max_red = 0;
     const int dims[3] = {s.D, s.H, s.W};
@@ -1075,9 +1165,10 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
       max_rows = std::max(max_rows, c.rows);
       max_red = std::max(max_red, c.red);
     }
-    const bool dvec = aligned16(dx) && s.Ci % 16 == 0;
+    const bool dvec = (dx_b ? aligned16(dx_b) : aligned16(dx)) && s.Ci % 16 == 0;
     gemm_launch(pad_cols(s.Ci), DgradA{dp, s, set, Cls{}, aligned16(dp)},
-                DgradB{w, s, set, Cls{}, aligned16(w)}, DgradEp{dx, s, set, Cls{}, dvec},
+                DgradB{w, s, set, Cls{}, aligned16(w)},
+                DgradEp{dx_b ? nullptr : dx, dx_b, s, set, Cls{}, dvec},
                 max_rows, max_red, max_red, 1, 8, st);
   }
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
@@ -1126,7 +1217,20 @@ int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,
   if (!dm::conv_shape(B, D, H, W, Ci, Co, s)) return DM_ERR_INVALID_ARG;
   if (!x || !w || !pre || !dact || !dw || !db || !workspace) return DM_ERR_INVALID_ARG;
   if (ws_bytes < dm::conv_ws_bytes(s)) return DM_ERR_WORKSPACE;
-  return dm::launch_conv_backward(s, (const dm::bf16*)x, (const dm::bf16*)w, pre, dact, dx, dw, db,
+  return dm::launch_conv_backward(s, (const dm::bf16*)x, (const dm::bf16*)w, pre, dact, nullptr,
+                                  dx, nullptr, dw, db, workspace, (cudaStream_t)stream);
+}
+
+int dm_conv3d_s2_backward_bf16(const uint16_t* x, int B, int D, int H, int W, int Ci,
+                               const uint16_t* w, int Co, const float* pre, const uint16_t* dact,
+                               uint16_t* dx, float* dw, float* db, void* workspace,
+                               size_t ws_bytes, dm_stream_t stream) {
+  dm::ConvShape s;
+  if (!dm::conv_shape(B, D, H, W, Ci, Co, s)) return DM_ERR_INVALID_ARG;
+  if (!x || !w || !pre || !dact || !dw || !db || !workspace) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm::conv_ws_bytes(s)) return DM_ERR_WORKSPACE;
+  return dm::launch_conv_backward(s, (const dm::bf16*)x, (const dm::bf16*)w, pre, nullptr,
+                                  (const dm::bf16*)dact, nullptr, (dm::bf16*)dx, dw, db,
                                   workspace, (cudaStream_t)stream);
 }
 

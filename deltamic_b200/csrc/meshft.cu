@@ -335,24 +335,27 @@ __global__ void k_face_key_hist(Cells cells, const FaceRec* __restrict__ recs,
 // One CTA per cell (thread = bin): first slot of every (block, bin).
 __global__ void k_face_key_scan(Cells cells, const int32_t* __restrict__ hist,
                                 int32_t* __restrict__ first) {
-  __shared__ int32_t tot[kKeyBins];
+  __shared__ int32_t wsum[kKeyBins / 32];
   const CellDesc d = cell_get(cells, blockIdx.x);
   const int nblk = (d.nt + kBlk - 1) / kBlk;
-  const int k = threadIdx.x;
+  const int k = threadIdx.x, lane = k & 31, warp = k >> 5;
   int32_t sum = 0;
+#pragma unroll 8
   for (int b = 0; b < nblk; ++b) sum += hist[(int64_t)(d.face_blk0 + b) * kKeyBins + k];
-  tot[k] = sum;
-  __syncthreads();
-  if (k == 0) {  // exclusive scan over the bins, in order
-    int32_t run = 0;
-    for (int i = 0; i < kKeyBins; ++i) {
-      const int32_t v = tot[i];
-      tot[i] = run;
-      run += v;
-    }
+  // exclusive scan over the bins (one bin per thread): warp scans, then the warp totals
+  int32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t n = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += n;
   }
+  if (lane == 31) wsum[warp] = inc;
   __syncthreads();
-  int32_t run = (int32_t)d.f_off + tot[k];
+  int32_t before = 0;
+#pragma unroll
+  for (int w = 0; w < kKeyBins / 32; ++w) before += w < warp ? wsum[w] : 0;
+  int32_t run = (int32_t)d.f_off + before + inc - sum;
+#pragma unroll 8
   for (int b = 0; b < nblk; ++b) {
     const int64_t o = (int64_t)(d.face_blk0 + b) * kKeyBins + k;
     first[o] = run;

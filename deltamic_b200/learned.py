@@ -58,18 +58,19 @@ class _ConvS2(torch.autograd.Function):
         x, wb, pre = ctx.saved_tensors
         B, D, H, W, Ci = x.shape
         Kp, Co = wb.shape
-        dact = dact.float().contiguous()
-        dx = torch.empty(x.shape, dtype=torch.float32, device=x.device) \
+        dact = dact.to(torch.bfloat16).contiguous()
+        dx = torch.empty(x.shape, dtype=torch.bfloat16, device=x.device) \
             if ctx.needs_input_grad[0] else None
         dw = torch.empty(Kp, Co, dtype=torch.float32, device=x.device)
         db = torch.empty(Co, dtype=torch.float32, device=x.device)
         ws = N.WORKSPACES.get(("conv", Ci, Co),
                               lib.dm_conv3d_s2_workspace_size(B, D, H, W, Ci, Co), x.device)
-        N.check(lib.dm_conv3d_s2_backward(N.ptr(x), B, D, H, W, Ci, N.ptr(wb), Co, N.ptr(pre),
-                                          N.ptr(dact), N.ptr(dx), N.ptr(dw), N.ptr(db),
-                                          N.ptr(ws), ws.numel(), N.stream_ptr(x.device)),
-                "dm_conv3d_s2_backward")
-        return (dx.to(x.dtype) if dx is not None else None), dw, db
+        N.check(lib.dm_conv3d_s2_backward_bf16(N.ptr(x), B, D, H, W, Ci, N.ptr(wb), Co,
+                                               N.ptr(pre), N.ptr(dact), N.ptr(dx), N.ptr(dw),
+                                               N.ptr(db), N.ptr(ws), ws.numel(),
+                                               N.stream_ptr(x.device)),
+                "dm_conv3d_s2_backward_bf16")
+        return dx, dw, db
 
 
 def conv_status_check(device):

@@ -534,6 +534,12 @@ int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,
                           const uint16_t* w, int Co, const float* pre, const float* dact,
                           float* dx, float* dw, float* db, void* workspace, size_t ws_bytes,
                           dm_stream_t stream);
+/* The same with dact and dx in BF16 (the dtype of the activations they belong
+ * to), as an autograd chain of these layers passes them: no FP32 round trip. */
+int dm_conv3d_s2_backward_bf16(const uint16_t* x, int B, int D, int H, int W, int Ci,
+                               const uint16_t* w, int Co, const float* pre, const uint16_t* dact,
+                               uint16_t* dx, float* dw, float* db, void* workspace,
+                               size_t ws_bytes, dm_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Occupancy of a closed mesh (for the volumetric IoU of a fit; no counterpart in

@@ -46,8 +46,11 @@ def test_batch_matches_single_cells():
     fo = np.cumsum([0] + [len(c[1]) for c in cells])
     total = 0.0
     for i, (v, f, c, box, shape, sig) in enumerate(cells):
-        # the batch renders through cuFFT: compare with the single cell's dense path
-        r = MeshRenderer(box, shape, 1e-5, DEV, render_path="dense")
+        # the batch renders through cuFFT: compare with the single cell's dense path,
+        # on the tile variants the batch was planned with (a different variant sums
+        # in another order, and the normalised loss's gradient amplifies rounding at
+        # the image minimum, where |z| is near zero)
+        r = MeshRenderer(box, shape, 1e-5, DEV, render_path="dense", autotune=False)
         r.set_sigma(torch.tensor(sig, dtype=torch.float32, device=DEV))
         assert r.n_band == br.band_sizes[i]
         Vi = torch.tensor(v, dtype=torch.float32, device=DEV, requires_grad=True)
