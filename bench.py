@@ -847,6 +847,8 @@ def setup_batch64(args, rank, dev):
     info = {"workload": f"batch{ncells}: {ncells} cells, levels 2-5, 64/96/128^3, sigma diag "
                         "U[5e-4,4e-3], Faces_coeff U[0.5,1.5], summed per-cell image L2",
             "n_cells": ncells, "n_verts": int(V.shape[0]), "n_faces": int(sum(br.nt)),
+            "render": ("band-box DFTs of all cells, one launch per stage" if br.use_bandbox
+                       else "batched cuFFT per grid shape + batched image-loss kernels"),
             "n_band": int(br.band.numel()), "eval_pairs_per_step": int(br.eval_pairs)}
     return make_step, e2e_call, np.concatenate(inits), br.pairs, info, None
 

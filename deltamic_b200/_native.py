@@ -60,6 +60,15 @@ class DmBatch(ctypes.Structure):
 
 _BATCHP = ctypes.POINTER(DmBatch)
 
+
+class DmBandboxBatch(ctypes.Structure):
+    _fields_ = [("ncells", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("workspace_bytes", ctypes.c_int64), ("plan", ctypes.c_int64 * 128),
+                ("cells", ctypes.c_void_p), ("workspace", ctypes.c_void_p)]
+
+
+_BBBP = ctypes.POINTER(DmBandboxBatch)
+
 SIGNATURES = {
     "dm_abi_version": (_INT, []),
     "dm_status_string": (ctypes.c_char_p, [_INT]),
@@ -121,6 +130,13 @@ SIGNATURES = {
     "dm_instance_mask": (_INT, [_P, _I64, _P, _I64, _BOXP, _I32, _P, _P, _SZ, _P]),
     "dm_batch_desc_size": (_SZ, [_INT]),
     "dm_batch_plan": (_INT, [ctypes.POINTER(DmCell), _INT, _P, _SZ, _BATCHP, _P]),
+    "dm_bandbox_batch_desc_size": (_SZ, [_INT]),
+    "dm_bandbox_batch_workspace_size": (_INT, [ctypes.POINTER(DmCell), _P, _INT,
+                                               ctypes.POINTER(ctypes.c_size_t)]),
+    "dm_bandbox_batch_plan": (_INT, [ctypes.POINTER(DmCell), _P, _INT, _P, _SZ, _P, _SZ, _BBBP,
+                                     _P]),
+    "dm_bandbox_batch_render_loss": (_INT, [_BBBP, _P, _P, _P, _INT, _P, _F, _P, _P, _P, _P]),
+    "dm_bandbox_batch_device_error": (_INT, [_BBBP, ctypes.POINTER(_INT), _P]),
     "dm_batched_topology_build": (_INT, [_BATCHP, _P, _P, _SZ, _P]),
     "dm_batched_meshft_forward": (_INT, [_BATCHP, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "dm_batched_meshft_backward": (_INT, [_BATCHP, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P, _P,

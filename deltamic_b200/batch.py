@@ -2,9 +2,12 @@
 
 Each stage runs once for the whole batch: one meshFT forward launch over the
 flattened (cell, frequency tile, face split) items, one adjoint launch over
-(cell, face block, frequency chunk) items, one image-loss launch set over all cell
-images, and one batched cuFFT per distinct grid shape.  Per-cell results are those
-of ``MeshRenderer`` on each cell alone.
+(cell, face block, frequency chunk) items, and the render + normalise + loss
+with its adjoint as the band-box DFTs of every cell, one launch per stage
+(``dm_bandbox_batch_render_loss``).  ``render_path="dense"`` (or a cell whose
+band box the line kernels do not serve, under ``"auto"``) renders with one
+batched cuFFT per distinct grid shape and the batched image-loss kernels
+instead.  Per-cell results are those of ``MeshRenderer`` on each cell alone.
 """
 from __future__ import annotations
 
@@ -23,10 +26,15 @@ __all__ = ["BatchRenderer", "BatchFitStep"]
 class BatchRenderer:
     """Cells ``i`` with ``boxes[i]`` ([3,2]) and ``shapes[i]`` (3 ints)."""
 
-    def __init__(self, boxes, shapes, narrowband_thresh=1e-5, device="cuda"):
+    def __init__(self, boxes, shapes, narrowband_thresh=1e-5, device="cuda",
+                 render_path="auto"):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("BatchRenderer runs on CUDA devices only")
+        if render_path not in ("auto", "bandbox", "dense"):
+            raise ValueError("render_path must be 'auto', 'bandbox' or 'dense'")
+        self.render_path = render_path
+        self.bb = None
         self.grids = [ops.FreqGrid(b, s) for b, s in zip(boxes, shapes)]
         self.ncells = len(self.grids)
         self.thresh = float(narrowband_thresh)
@@ -82,6 +90,45 @@ class BatchRenderer:
         self.band = torch.cat(bands).contiguous()
         self.spec.zero_()
         self.batch = None
+        self._plan_bandbox(bands)
+
+    def _plan_bandbox(self, bands):
+        """Band-box plan of every cell (one host sync per cell for its bounds)."""
+        self.bb = None
+        if self.render_path == "dense":
+            return
+        lib = N.lib()
+        n = self.ncells
+        cells = (N.DmCell * n)()
+        flat = []
+        ok = all(b.numel() > 0 for b in bands)
+        for i, b in enumerate(bands):
+            cells[i].n_band = self.band_sizes[i]
+            cells[i].grid_offset = self.grid_offset[i]
+            cells[i].box = ops.band_box(self.grids[i], self.band_herm[i])
+            flat.extend(ops.band_bounds(b, self.grids[i]) if b.numel() else (0,) * 6)
+        bounds = (ctypes.c_int32 * (6 * n))(*flat)
+        size = ctypes.c_size_t(0)
+        st = lib.dm_bandbox_batch_workspace_size(cells, bounds, n, ctypes.byref(size)) if ok \
+            else N.DM_ERR_UNSUPPORTED
+        if st != 0:
+            if self.render_path == "bandbox":
+                N.check(st, "dm_bandbox_batch_workspace_size")
+            return
+        self._bb_ws = torch.empty(max(int(size.value), 256), dtype=torch.uint8,
+                                  device=self.device)
+        self._bb_desc = torch.empty(lib.dm_bandbox_batch_desc_size(n), dtype=torch.uint8,
+                                    device=self.device)
+        plan = N.DmBandboxBatch()
+        N.check(lib.dm_bandbox_batch_plan(cells, bounds, n, N.ptr(self._bb_desc),
+                                          self._bb_desc.numel(), N.ptr(self._bb_ws),
+                                          self._bb_ws.numel(), ctypes.byref(plan),
+                                          N.stream_ptr(self.device)), "dm_bandbox_batch_plan")
+        self.bb = plan
+
+    @property
+    def use_bandbox(self) -> bool:
+        return self.bb is not None
 
     # -- meshes -----------------------------------------------------------------
     def set_meshes(self, verts_list, faces_list):
@@ -126,15 +173,46 @@ class BatchRenderer:
         return faces
 
     # -- stages -----------------------------------------------------------------
-    def forward_spectrum(self, verts, coeff):
+    def forward_spectrum(self, verts, coeff, dense=True):
+        """ft on the concatenated bands (complex64); with ``dense`` also ft * OTF
+        scattered into the concatenated grids (the cuFFT path's input)."""
         lib = N.lib()
         ft = torch.empty(self.band.numel(), dtype=torch.complex64, device=self.device)
         w = self._ws["fwd_workspace"]
         N.check(lib.dm_batched_meshft_forward(
             ctypes.byref(self.batch), N.ptr(verts), N.ptr(self.faces), N.ptr(coeff),
-            N.ptr(self.band), N.ptr(self.otf), N.ptr(ft), N.ptr(self.spec), N.ptr(w), w.numel(),
-            N.stream_ptr(self.device)), "dm_batched_meshft_forward")
+            N.ptr(self.band), N.ptr(self.otf), N.ptr(ft), N.ptr(self.spec) if dense else None,
+            N.ptr(w), w.numel(), N.stream_ptr(self.device)), "dm_batched_meshft_forward")
         return ft
+
+    def render_loss_bandbox(self, ft, kind, target, contrast=0.0, want_grad=True,
+                            want_image=False):
+        """(losses[ncells], dL/dS on the concatenated bands | None, image | None) by
+        the band-box DFTs of every cell."""
+        lib = N.lib()
+        losses = torch.empty(self.ncells, dtype=torch.float32, device=self.device)
+        G = torch.empty_like(ft) if want_grad else None
+        img = torch.empty(self.grid_elems, device=self.device) if want_image else None
+        if kind == "mse":
+            N.require_cuda(target, "target", torch.float32)
+            if target.numel() != self.grid_elems:
+                raise ValueError("target must hold every cell's grid")
+        N.check(lib.dm_bandbox_batch_render_loss(
+            ctypes.byref(self.bb), N.ptr(ft), N.ptr(self.band), N.ptr(self.otf),
+            ops.LOSS_KINDS[kind], N.ptr(target) if kind == "mse" else None, float(contrast),
+            N.ptr(losses), N.ptr(G), N.ptr(img), N.stream_ptr(self.device)),
+            "dm_bandbox_batch_render_loss")
+        return losses, G, img
+
+    def device_error(self) -> int:
+        """Status words of the band-box plan's cells (read and cleared; synchronous)."""
+        flags = N._INT(0)
+        if self.bb is not None:
+            N.check(N.lib().dm_bandbox_batch_device_error(ctypes.byref(self.bb),
+                                                          ctypes.byref(flags),
+                                                          N.stream_ptr(self.device)),
+                    "dm_bandbox_batch_device_error")
+        return flags.value
 
     def inverse_fft(self):
         for gi in range(len(self.groups)):
@@ -159,21 +237,26 @@ class BatchRenderer:
             N.stream_ptr(self.device)), "dm_batched_image_loss")
         return losses, img, gz
 
-    def backward(self, verts, coeff, ft, want_coeff=True):
+    def backward(self, verts, coeff, ft, want_coeff=True, grad_list=None):
+        """(grad_verts, grad_coeff | None) for the cotangent dL/dS: ``grad_list`` on
+        the concatenated bands, or (default) the dense grids in ``self.G``."""
         lib = N.lib()
         gv = torch.empty_like(verts)
         gc = torch.empty_like(coeff) if want_coeff else None
         w = self._ws["bwd_workspace"]
         N.check(lib.dm_batched_meshft_backward(
             ctypes.byref(self.batch), N.ptr(verts), N.ptr(self.faces), N.ptr(coeff),
-            N.ptr(self.band), None, N.ptr(self.G), N.ptr(self.otf), 1.0, N.ptr(ft),
-            N.ptr(self._topo), N.ptr(gv), N.ptr(gc), None, N.ptr(w), w.numel(),
-            N.stream_ptr(self.device)), "dm_batched_meshft_backward")
+            N.ptr(self.band), N.ptr(grad_list), None if grad_list is not None else N.ptr(self.G),
+            N.ptr(self.otf), 1.0, N.ptr(ft), N.ptr(self._topo), N.ptr(gv), N.ptr(gc), None,
+            N.ptr(w), w.numel(), N.stream_ptr(self.device)), "dm_batched_meshft_backward")
         return gv, gc
 
     @torch.no_grad()
     def render(self, verts, coeff):
         """|ifftn(meshFT * OTF)| of every cell, concatenated (float32)."""
+        if self.use_bandbox:
+            ft = self.forward_spectrum(verts, coeff, dense=False)
+            return self.render_loss_bandbox(ft, "sum", None, want_grad=False, want_image=True)[2]
         self.forward_spectrum(verts, coeff)
         self.inverse_fft()
         return self.z.abs()
@@ -187,19 +270,29 @@ class BatchRenderer:
 class _BatchLoss(torch.autograd.Function):
     @staticmethod
     def forward(ctx, verts, coeff, r: BatchRenderer, kind, target, contrast):
-        ft = r.forward_spectrum(verts, coeff)
-        r.inverse_fft()
-        losses, _, gz = r.image_loss(kind, target, contrast)
-        ctx.save_for_backward(verts, coeff, ft, gz)
+        if r.use_bandbox:
+            ft = r.forward_spectrum(verts, coeff, dense=False)
+            losses, G, _ = r.render_loss_bandbox(ft, kind, target, contrast)
+            ctx.save_for_backward(verts, coeff, ft, G)
+        else:
+            ft = r.forward_spectrum(verts, coeff)
+            r.inverse_fft()
+            losses, _, gz = r.image_loss(kind, target, contrast)
+            ctx.save_for_backward(verts, coeff, ft, gz)
+        ctx.bandbox = r.use_bandbox
         ctx.r = r
         return losses.sum()
 
     @staticmethod
     def backward(ctx, gl):
-        verts, coeff, ft, gz = ctx.saved_tensors
+        verts, coeff, ft, g = ctx.saved_tensors
         r = ctx.r
-        r.adjoint_fft(gz)
-        gv, gc = r.backward(verts, coeff, ft, want_coeff=ctx.needs_input_grad[1])
+        if ctx.bandbox:
+            gv, gc = r.backward(verts, coeff, ft, want_coeff=ctx.needs_input_grad[1],
+                                grad_list=g)
+        else:
+            r.adjoint_fft(g)
+            gv, gc = r.backward(verts, coeff, ft, want_coeff=ctx.needs_input_grad[1])
         gv = gv * gl
         if gc is not None:
             gc = gc * gl
@@ -226,13 +319,20 @@ class BatchFitStep:
 
     def _body(self):
         r = self.r
-        ft = r.forward_spectrum(self.V, self.C)
-        r.inverse_fft()
-        losses, _, gz = r.image_loss(self.kind, self.target, self.contrast)
-        self.cell_losses.copy_(losses)
-        torch.sum(losses, dim=0, keepdim=True, out=self.loss)
-        r.adjoint_fft(gz)
-        gv, _ = r.backward(self.V, self.C, ft, want_coeff=False)
+        if r.use_bandbox:
+            ft = r.forward_spectrum(self.V, self.C, dense=False)
+            losses, G, _ = r.render_loss_bandbox(ft, self.kind, self.target, self.contrast)
+            self.cell_losses.copy_(losses)
+            torch.sum(losses, dim=0, keepdim=True, out=self.loss)
+            gv, _ = r.backward(self.V, self.C, ft, want_coeff=False, grad_list=G)
+        else:
+            ft = r.forward_spectrum(self.V, self.C)
+            r.inverse_fft()
+            losses, _, gz = r.image_loss(self.kind, self.target, self.contrast)
+            self.cell_losses.copy_(losses)
+            torch.sum(losses, dim=0, keepdim=True, out=self.loss)
+            r.adjoint_fft(gz)
+            gv, _ = r.backward(self.V, self.C, ft, want_coeff=False)
         ops.adam_step(self.V, gv, self.m, self.v, self.t, self.lr, self.betas[0], self.betas[1],
                       self.eps)
 

@@ -30,6 +30,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <vector>
 
 #include "band_internal.h"
 #include "dm_common.cuh"
@@ -1103,6 +1105,166 @@ cudaError_t gradlines(const BBShape& s, const BBWs& w, int kind, const float* ta
   return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------
+// Many boxes per launch (the cells of a batch).  Each stage is one launch over
+// all cells (the z and gradient passes: one per distinct template parameter),
+// blockIdx.z (or the flat element index) selecting the cell; CTAs past a cell's
+// own grid return at once.  Per cell the work and every sum are those of the
+// single-box call.
+
+struct BBCell {
+  BBShape s;
+  BBWs w;
+  int64_t band_off, nband, grid_off;
+  int32_t zctas, zcb, gctas, e12;
+  float inv_n, gscale;
+};
+
+// Largest c in [0, n) with pref[c] <= x (pref ascending, pref[0] = 0).
+template <typename T>
+__device__ __forceinline__ int find_cell(const T* __restrict__ pref, int n, T x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pref[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_bbb_scatter(const BBCell* __restrict__ cells, const int64_t* __restrict__ bpref,
+                              int ncells, int64_t total, const int32_t* __restrict__ band,
+                              const float2* __restrict__ ft, const float* __restrict__ otf) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= total) return;
+  const int c = find_cell(bpref, ncells, m);
+  const BBCell& cc = cells[c];
+  bb_scatter(cc.s, band + cc.band_off, m - cc.band_off, ft + cc.band_off,
+             otf ? otf + cc.grid_off : nullptr, cc.w.t0, &cc.w.hdr->err);
+}
+
+template <bool kInv>
+__global__ void __launch_bounds__(kGemmThreads)
+    k_bbb_gemm(const GemmP* __restrict__ ps, const int32_t* __restrict__ zp, int ncells) {
+  const int c = find_cell(zp, ncells, (int32_t)blockIdx.z);
+  const GemmP p = ps[c];
+  if ((int)blockIdx.x * 32 >= p.N || (int)blockIdx.y * 64 >= p.M) return;
+  bb_gemm_tile<kInv>(p, blockIdx.x, blockIdx.y, (int)blockIdx.z - zp[c]);
+}
+
+template <int C>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bbb_zlines(const BBCell* __restrict__ cells, const int32_t* __restrict__ order,
+                 float* __restrict__ image) {
+  const BBCell& cc = cells[order[blockIdx.z]];
+  if ((int)blockIdx.x >= cc.zctas || (int)blockIdx.y >= cc.zcb) return;
+  bb_zlines<C>(cc.s, cc.w.t2, cc.w.w2, cc.inv_n, cc.w.z, image ? image + cc.grid_off : nullptr,
+               cc.w.mm, cc.w.hdr, blockIdx.x, blockIdx.y, cc.zctas, cc.zcb);
+}
+
+template <int JC>
+__global__ void __launch_bounds__(kLineThreads)
+    k_bbb_gradlines(const BBCell* __restrict__ cells, const int32_t* __restrict__ order, int kind,
+                    const float* __restrict__ target, float contrast, float* __restrict__ loss) {
+  const int ci = order[blockIdx.z];
+  const BBCell& cc = cells[ci];
+  if ((int)blockIdx.x >= cc.gctas) return;
+  bb_gradlines<JC>(cc.s, cc.w.z, target ? target + cc.grid_off : nullptr, kind, contrast,
+                   cc.w.hdr, cc.w.w2t, cc.w.t2, cc.w.lp, loss ? loss + ci : nullptr, blockIdx.x,
+                   cc.gctas);
+}
+
+__global__ void k_bbb_ties(const BBCell* __restrict__ cells) {
+  const BBCell& cc = cells[blockIdx.z];
+  bb_ties(cc.s, cc.w.z, cc.w.hdr, cc.w.w2t, cc.w.t2,
+          (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void __launch_bounds__(kColThreads) k_bbb_columns(const BBCell* __restrict__ cells) {
+  const BBCell& cc = cells[blockIdx.z];
+  if ((int)blockIdx.x >= cc.e12) return;
+  bb_columns(cc.s, cc.w.q1p, cc.w.w0, cc.w.g0, blockIdx.x);
+}
+
+__global__ void k_bbb_gather(const BBCell* __restrict__ cells, const int64_t* __restrict__ bpref,
+                             int ncells, int64_t total, const int32_t* __restrict__ band,
+                             float2* __restrict__ grad_list) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= total) return;
+  const int c = find_cell(bpref, ncells, m);
+  const BBCell& cc = cells[c];
+  const float2 g = bb_gather(cc.s, band + cc.band_off, m - cc.band_off, cc.w.g0, cc.w.w0,
+                             cc.w.w1, cc.w.w2, cc.w.z, cc.w.hdr);
+  grad_list[m] = make_float2(g.x * cc.gscale, g.y * cc.gscale);
+}
+
+// OR of the cells' status words into *out; the words are cleared.
+__global__ void k_bbb_errors(const BBCell* __restrict__ cells, int ncells, int* out) {
+  for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+    int* e = &cells[c].w.hdr->err;
+    const int v = *e;
+    if (v) atomicOr(out, v);
+    *e = 0;
+  }
+}
+
+// Host plan of a batch, kept in dm_bandbox_batch::plan (int64 slots).
+constexpr int kBBBMaxZ = 8, kBBBMaxJ = 4;
+struct BBBPlan {
+  int64_t ncells, total_band;
+  int64_t gx[3], gy[3], gz[3];
+  int64_t ties_x, col_x, col_smem;
+  int64_t nz, zC[kBBBMaxZ], zfirst[kBBBMaxZ], zcount[kBBBMaxZ], zx[kBBBMaxZ], zy[kBBBMaxZ],
+      zsmem[kBBBMaxZ];
+  int64_t nj, jJC[kBBBMaxJ], jfirst[kBBBMaxJ], jcount[kBBBMaxJ], jx[kBBBMaxJ], jsmem[kBBBMaxJ];
+  int64_t off_cells, off_gemm, off_zp, off_zord, off_gord, off_bpref, off_err;
+};
+
+// Device-buffer layout of a batch plan for ncells cells.
+size_t bbb_desc_layout(int ncells, BBBPlan* p) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += up256(bytes);
+    return (int64_t)o;
+  };
+  const int64_t oc = take(sizeof(BBCell) * ncells);
+  const int64_t og = take(sizeof(GemmP) * 3 * (size_t)ncells);
+  const int64_t oz = take(sizeof(int32_t) * 3 * (size_t)(ncells + 1));
+  const int64_t o1 = take(sizeof(int32_t) * ncells);
+  const int64_t o2 = take(sizeof(int32_t) * ncells);
+  const int64_t ob = take(sizeof(int64_t) * (size_t)(ncells + 1));
+  const int64_t oe = take(sizeof(int));
+  if (p) {
+    p->off_cells = oc; p->off_gemm = og; p->off_zp = oz; p->off_zord = o1;
+    p->off_gord = o2; p->off_bpref = ob; p->off_err = oe;
+  }
+  return off;
+}
+
+template <int C>
+cudaError_t zlines_cells(const BBCell* cells, const int32_t* order, unsigned gx, unsigned gy,
+                         unsigned gz, size_t smem, float* image, cudaStream_t st) {
+  auto k = k_bbb_zlines<C>;
+  static std::atomic<bool> done[64];
+  cudaError_t e = smem_limit_once(k, done);
+  if (e != cudaSuccess) return e;
+  k<<<dim3(gx, gy, gz), kLineThreads, smem, st>>>(cells, order, image);
+  return cudaGetLastError();
+}
+
+template <int JC>
+cudaError_t gradlines_cells(const BBCell* cells, const int32_t* order, unsigned gx, unsigned gz,
+                            size_t smem, int kind, const float* target, float contrast,
+                            float* loss, cudaStream_t st) {
+  auto k = k_bbb_gradlines<JC>;
+  static std::atomic<bool> done[64];
+  cudaError_t e = smem_limit_once(k, done);
+  if (e != cudaSuccess) return e;
+  k<<<dim3(gx, 1, gz), kLineThreads, smem, st>>>(cells, order, kind, target, contrast, loss);
+  return cudaGetLastError();
+}
+
 }  // namespace
 }  // namespace dm
 
@@ -1240,6 +1402,264 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
   }
   count_launches(launches);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batches of boxes (one plan, one workspace; see the header).
+
+size_t dm_bandbox_batch_desc_size(int ncells) {
+  return ncells > 0 ? bbb_desc_layout(ncells, nullptr) : 0;
+}
+
+static int bbb_shapes(const dm_cell* cells, const int32_t* bounds, int ncells,
+                      std::vector<BBShape>& shapes, size_t* ws_total) {
+  if (!cells || !bounds || ncells <= 0) return DM_ERR_INVALID_ARG;
+  shapes.resize(ncells);
+  size_t tot = 0;
+  for (int i = 0; i < ncells; ++i) {
+    if (cells[i].n_band <= 0) return DM_ERR_INVALID_ARG;
+    if (!dm_render_loss_bandbox_supported(&cells[i].box, bounds + 6 * i)) return DM_ERR_UNSUPPORTED;
+    int32_t lo[3], ext[3];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = bounds[6 * i + d];
+      ext[d] = bounds[6 * i + 3 + d] - bounds[6 * i + d] + 1;
+    }
+    if (!make_shape(cells[i].box.shape, lo, ext, shapes[i])) return DM_ERR_UNSUPPORTED;
+    tot += bb_layout(shapes[i], nullptr, nullptr);
+  }
+  *ws_total = tot;
+  return DM_OK;
+}
+
+int dm_bandbox_batch_workspace_size(const dm_cell* cells, const int32_t* bounds, int ncells,
+                                    size_t* bytes) {
+  if (!bytes) return DM_ERR_INVALID_ARG;
+  std::vector<BBShape> shapes;
+  size_t tot = 0;
+  const int r = bbb_shapes(cells, bounds, ncells, shapes, &tot);
+  *bytes = r == DM_OK ? tot : 0;
+  return r;
+}
+
+int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncells, void* desc,
+                          size_t desc_bytes, void* workspace, size_t ws_bytes,
+                          dm_bandbox_batch* out, dm_stream_t stream) {
+  static_assert(sizeof(BBBPlan) <= sizeof(((dm_bandbox_batch*)nullptr)->plan), "plan slots");
+  if (!desc || !workspace || !out) return DM_ERR_INVALID_ARG;
+  std::vector<BBShape> sh;
+  size_t need = 0;
+  int r = bbb_shapes(cells, bounds, ncells, sh, &need);
+  if (r != DM_OK) return r;
+  if (ws_bytes < need) return DM_ERR_WORKSPACE;
+  BBBPlan P;
+  memset(&P, 0, sizeof(P));
+  const size_t dbytes = bbb_desc_layout(ncells, &P);
+  if (desc_bytes < dbytes) return DM_ERR_WORKSPACE;
+  std::vector<char> host(dbytes, 0);
+  BBCell* hc = (BBCell*)(host.data() + P.off_cells);
+  GemmP* hg = (GemmP*)(host.data() + P.off_gemm);
+  int32_t* hz = (int32_t*)(host.data() + P.off_zp);
+  int32_t* zord = (int32_t*)(host.data() + P.off_zord);
+  int32_t* gord = (int32_t*)(host.data() + P.off_gord);
+  int64_t* bpref = (int64_t*)(host.data() + P.off_bpref);
+  const int sms = num_sms();
+  double wtot = 0.0;
+  for (int i = 0; i < ncells; ++i) wtot += (double)sh[i].nvox * sh[i].ext[2];
+  size_t off = 0;
+  bpref[0] = 0;
+  for (int k = 0; k < 3; ++k) hz[k * (ncells + 1)] = 0;
+  P.ncells = ncells;
+  for (int i = 0; i < ncells; ++i) {
+    const BBShape& s = sh[i];
+    BBCell& c = hc[i];
+    c.s = s;
+    off += bb_layout(s, (char*)workspace + off, &c.w);
+    c.band_off = bpref[i];
+    c.nband = cells[i].n_band;
+    bpref[i + 1] = bpref[i] + c.nband;
+    c.grid_off = cells[i].grid_offset;
+    c.inv_n = (float)(1.0 / (double)s.nvox);
+    c.gscale = c.inv_n;
+    const int64_t tiles = (s.nlines + kLines - 1) / kLines;
+    const double share = 2.0 * sms * ((double)s.nvox * s.ext[2]) / wtot;
+    const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)(share + 0.5)));
+    c.zctas = (int32_t)ctas;
+    c.zcb = (int32_t)(s.ldw2 / (32 * s.zc));
+    c.gctas = (int32_t)ctas;
+    c.e12 = s.ext[1] * s.ext[2];
+    const int64_t e12 = c.e12;
+    GemmP g[3];
+    g[0] = gemm_p(c.w.w0, s.n[0], s.n[0], (int)e12, s.ext[0], s.ext[0], c.w.t0, 0, e12, 1, 0,
+                  c.w.t1, 0, e12, 1, 0, 1);
+    g[1] = gemm_p(c.w.w1, s.n[1], s.n[1], s.ext[2], s.ext[1], s.ext[1], c.w.t1, e12, s.ext[2], 1,
+                  0, c.w.t2, (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, s.n[0]);
+    g[2] = gemm_p(c.w.w1, s.n[1], s.ext[1], s.ext[2], s.n[1], s.q1chunk, c.w.t2,
+                  (int64_t)s.n[1] * s.ext[2], s.ext[2], 1, 0, c.w.q1p, 1,
+                  (int64_t)s.ext[2] * s.n[0], s.n[0], e12 * s.n[0], s.n[0]);
+    for (int k = 0; k < 3; ++k) {
+      hg[k * ncells + i] = g[k];
+      const dim3 gd = gemm_grid(g[k]);
+      P.gx[k] = std::max<int64_t>(P.gx[k], gd.x);
+      P.gy[k] = std::max<int64_t>(P.gy[k], gd.y);
+      hz[k * (ncells + 1) + i + 1] = hz[k * (ncells + 1) + i] + (int32_t)gd.z;
+    }
+    P.ties_x = std::max<int64_t>(P.ties_x, (s.nlines + 127) / 128);
+    P.col_x = std::max<int64_t>(P.col_x, e12);
+    P.col_smem = std::max<int64_t>(P.col_smem, (int64_t)sizeof(float2) * s.n[0]);
+  }
+  P.total_band = bpref[ncells];
+  for (int k = 0; k < 3; ++k) {
+    P.gz[k] = hz[k * (ncells + 1) + ncells];
+    if (P.gz[k] > 65535 || P.gy[k] > 65535) return DM_ERR_SIZE;
+  }
+  if (P.ties_x > INT32_MAX || P.col_x > INT32_MAX) return DM_ERR_SIZE;
+  // z pass groups (by columns per thread), gradient pass groups (by offset groups)
+  std::vector<int> idx(ncells);
+  for (int i = 0; i < ncells; ++i) idx[i] = i;
+  auto jc_of = [&](int i) { return std::min(4, sh[i].ldj / 8); };
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return sh[a].zc < sh[b].zc; });
+  for (int k = 0; k < ncells;) {
+    const int C = sh[idx[k]].zc;
+    const int g = (int)P.nz++;
+    if (g >= kBBBMaxZ) return DM_ERR_SIZE;
+    P.zC[g] = C;
+    P.zfirst[g] = k;
+    for (; k < ncells && sh[idx[k]].zc == C; ++k) {
+      zord[k] = idx[k];
+      P.zcount[g] += 1;
+      P.zx[g] = std::max<int64_t>(P.zx[g], hc[idx[k]].zctas);
+      P.zy[g] = std::max<int64_t>(P.zy[g], hc[idx[k]].zcb);
+      P.zsmem[g] = std::max<int64_t>(P.zsmem[g], (int64_t)zlines_smem(sh[idx[k]]));
+    }
+  }
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return jc_of(a) < jc_of(b); });
+  for (int k = 0; k < ncells;) {
+    const int J = jc_of(idx[k]);
+    const int g = (int)P.nj++;
+    if (g >= kBBBMaxJ) return DM_ERR_SIZE;
+    P.jJC[g] = J;
+    P.jfirst[g] = k;
+    for (; k < ncells && jc_of(idx[k]) == J; ++k) {
+      gord[k] = idx[k];
+      P.jcount[g] += 1;
+      P.jx[g] = std::max<int64_t>(P.jx[g], hc[idx[k]].gctas);
+      P.jsmem[g] = std::max<int64_t>(
+          P.jsmem[g], (int64_t)gradlines_smem(sh[idx[k]].n[2], sh[idx[k]].ldj));
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(desc, host.data(), dbytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return DM_ERR_CUDA;
+  // zero band boxes (only the band voxels are ever written), counters and status
+  // words, then the root tables of every cell
+  if (cudaMemsetAsync(workspace, 0, need, st) != cudaSuccess) return DM_ERR_CUDA;
+  for (int i = 0; i < ncells; ++i) {
+    const BBShape& s = sh[i];
+    const BBWs& w = hc[i].w;
+    const int64_t tot = (int64_t)s.ext[0] * s.n[0] + (int64_t)s.ext[1] * s.n[1] +
+                        (int64_t)s.ext[2] * s.ldw2 + (int64_t)s.n[2] * s.ldj;
+    const unsigned nb = (unsigned)std::min<int64_t>((tot + 255) / 256, 1024);
+    k_bb_tables<<<nb, 256, 0, st>>>(s, w.w0, w.w1, w.w2, w.w2t, w.hdr);
+  }
+  count_launches(ncells);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return DM_ERR_CUDA;
+  memset(out, 0, sizeof(*out));
+  out->ncells = ncells;
+  out->workspace_bytes = (int64_t)need;
+  memcpy(out->plan, &P, sizeof(P));
+  out->cells = desc;
+  out->workspace = workspace;
+  return DM_OK;
+}
+
+int dm_bandbox_batch_render_loss(const dm_bandbox_batch* bb, const float* ft_list,
+                                 const int32_t* band_index, const float* otf, int kind,
+                                 const float* target, float contrast, float* loss,
+                                 float* grad_list, float* image, dm_stream_t stream) {
+  if (!bb || !bb->cells || !ft_list || !band_index || !loss) return DM_ERR_INVALID_ARG;
+  if ((kind != 0 && kind != 1) || (kind == 1 && !target)) return DM_ERR_INVALID_ARG;
+  BBBPlan P;
+  memcpy(&P, bb->plan, sizeof(P));
+  const int n = (int)P.ncells;
+  if (n <= 0 || n != bb->ncells) return DM_ERR_INVALID_ARG;
+  const char* d = (const char*)bb->cells;
+  const BBCell* cells = (const BBCell*)(d + P.off_cells);
+  const GemmP* gp = (const GemmP*)(d + P.off_gemm);
+  const int32_t* zp = (const int32_t*)(d + P.off_zp);
+  const int32_t* zord = (const int32_t*)(d + P.off_zord);
+  const int32_t* gord = (const int32_t*)(d + P.off_gord);
+  const int64_t* bpref = (const int64_t*)(d + P.off_bpref);
+  cudaStream_t st = (cudaStream_t)stream;
+  int launches = 0;
+  const unsigned nbb = (unsigned)((P.total_band + 255) / 256);
+  k_bbb_scatter<<<nbb, 256, 0, st>>>(cells, bpref, n, P.total_band, band_index,
+                                      (const float2*)ft_list, otf);
+  k_bbb_gemm<true><<<dim3((unsigned)P.gx[0], (unsigned)P.gy[0], (unsigned)P.gz[0]),
+                     kGemmThreads, 0, st>>>(gp, zp, n);
+  k_bbb_gemm<true><<<dim3((unsigned)P.gx[1], (unsigned)P.gy[1], (unsigned)P.gz[1]),
+                     kGemmThreads, 0, st>>>(gp + n, zp + (n + 1), n);
+  launches += 3;
+  cudaError_t e = cudaSuccess;
+  for (int g = 0; g < P.nz && e == cudaSuccess; ++g) {
+    const int32_t* ord = zord + P.zfirst[g];
+    const unsigned gx = (unsigned)P.zx[g], gy = (unsigned)P.zy[g], gz = (unsigned)P.zcount[g];
+    const size_t sm = (size_t)P.zsmem[g];
+    switch (P.zC[g]) {
+      case 1: e = zlines_cells<1>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 2: e = zlines_cells<2>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 3: e = zlines_cells<3>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 4: e = zlines_cells<4>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 5: e = zlines_cells<5>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 6: e = zlines_cells<6>(cells, ord, gx, gy, gz, sm, image, st); break;
+      case 7: e = zlines_cells<7>(cells, ord, gx, gy, gz, sm, image, st); break;
+      default: e = zlines_cells<8>(cells, ord, gx, gy, gz, sm, image, st); break;
+    }
+    ++launches;
+  }
+  for (int g = 0; g < P.nj && e == cudaSuccess; ++g) {
+    const int32_t* ord = gord + P.jfirst[g];
+    const unsigned gx = (unsigned)P.jx[g], gz = (unsigned)P.jcount[g];
+    const size_t sm = (size_t)P.jsmem[g];
+    switch (P.jJC[g]) {
+      case 1: e = gradlines_cells<1>(cells, ord, gx, gz, sm, kind, target, contrast, loss, st); break;
+      case 2: e = gradlines_cells<2>(cells, ord, gx, gz, sm, kind, target, contrast, loss, st); break;
+      case 3: e = gradlines_cells<3>(cells, ord, gx, gz, sm, kind, target, contrast, loss, st); break;
+      default: e = gradlines_cells<4>(cells, ord, gx, gz, sm, kind, target, contrast, loss, st); break;
+    }
+    ++launches;
+  }
+  if (e != cudaSuccess) return DM_ERR_CUDA;
+  if (grad_list) {
+    k_bbb_ties<<<dim3((unsigned)P.ties_x, 1, (unsigned)n), 128, 0, st>>>(cells);
+    k_bbb_gemm<false><<<dim3((unsigned)P.gx[2], (unsigned)P.gy[2], (unsigned)P.gz[2]),
+                        kGemmThreads, 0, st>>>(gp + 2 * n, zp + 2 * (n + 1), n);
+    k_bbb_columns<<<dim3((unsigned)P.col_x, 1, (unsigned)n), kColThreads, (size_t)P.col_smem,
+                    st>>>(cells);
+    k_bbb_gather<<<nbb, 256, 0, st>>>(cells, bpref, n, P.total_band, band_index,
+                                       (float2*)grad_list);
+    launches += 4;
+  }
+  count_launches(launches);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int dm_bandbox_batch_device_error(const dm_bandbox_batch* bb, int* out_flags, dm_stream_t stream) {
+  if (!bb || !bb->cells || !out_flags) return DM_ERR_INVALID_ARG;
+  BBBPlan P;
+  memcpy(&P, bb->plan, sizeof(P));
+  int* slot = (int*)((char*)bb->cells + P.off_err);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(slot, 0, sizeof(int), st) != cudaSuccess) return DM_ERR_CUDA;
+  k_bbb_errors<<<1, 256, 0, st>>>((const BBCell*)((const char*)bb->cells + P.off_cells),
+                                  (int)P.ncells, slot);
+  count_launches(1);
+  int v = 0;
+  if (cudaMemcpyAsync(&v, slot, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return DM_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return DM_ERR_CUDA;
+  *out_flags = v;
+  return DM_OK;
 }
 
 }  // extern "C"

@@ -513,6 +513,43 @@ int dm_render_loss_bandbox(const float* ft_list, const int32_t* band_index, int6
                            float* grad_list, float* image, void* workspace, size_t ws_bytes,
                            dm_stream_t stream);
 
+/* Band-box render + loss for the cells of a batch (each cell's box, band and
+ * loss as dm_render_loss_bandbox alone; kinds 0 and 1).  The plan (host,
+ * synchronous, outside stream capture) takes the cells (box, n_band,
+ * grid_offset of dm_cell) and their band bounds (HOST int32 [ncells][6], as
+ * dm_band_bounds writes them); it owns ``workspace`` (its size from
+ * dm_bandbox_batch_workspace_size, DM_ERR_UNSUPPORTED if a cell's box is not
+ * served) and uploads its tables into ``desc`` (dm_bandbox_batch_desc_size).
+ * dm_bandbox_batch_render_loss takes the concatenated band lists (ft_list,
+ * band_index with cell-local voxel indices) and concatenated grids (otf, target,
+ * image at each cell's grid_offset), writes loss[ncells] (DEVICE) and, if
+ * grad_list is not NULL, grad_list = fftn(dL/dz) / n_cell at each cell's band
+ * voxels: dL/dS, the cotangent dm_batched_meshft_backward takes with otf and
+ * grad_scale 1.  One launch per stage for all cells (the two line passes: one
+ * per distinct line-tile shape).  dm_bandbox_batch_device_error reads and clears
+ * the cells' status words (synchronous). */
+typedef struct dm_bandbox_batch {
+  int32_t ncells;
+  int32_t reserved;
+  int64_t workspace_bytes;
+  int64_t plan[128]; /* launch sizes (opaque) */
+  const void* cells; /* device copy of the plan */
+  void* workspace;
+} dm_bandbox_batch;
+
+size_t dm_bandbox_batch_desc_size(int ncells);
+int dm_bandbox_batch_workspace_size(const dm_cell* cells, const int32_t* bounds, int ncells,
+                                    size_t* bytes);
+int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncells, void* desc,
+                          size_t desc_bytes, void* workspace, size_t ws_bytes,
+                          dm_bandbox_batch* out, dm_stream_t stream);
+int dm_bandbox_batch_render_loss(const dm_bandbox_batch* bb, const float* ft_list,
+                                 const int32_t* band_index, const float* otf, int kind,
+                                 const float* target, float contrast, float* loss,
+                                 float* grad_list, float* image, dm_stream_t stream);
+int dm_bandbox_batch_device_error(const dm_bandbox_batch* bb, int* out_flags,
+                                  dm_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * 3x3x3 stride-2 padding-1 3D convolution with bias and GELU, for the learned
  * initialiser's encoder (no counterpart in the reference).  Channels-last BF16

@@ -1,5 +1,6 @@
 """Batched cells (uneven meshes, grid shapes and PSFs in one launch per stage)
-against the single-cell path, cell by cell."""
+against the single-cell path and against the float64 oracle chain, cell by cell,
+on both render paths (band-box DFTs of all cells per launch; batched cuFFT)."""
 import numpy as np
 import pytest
 import torch
@@ -28,9 +29,11 @@ def _cells(n=5, seed=0):
     return out
 
 
-def test_batch_matches_single_cells():
+@pytest.mark.parametrize("path", ["dense", "bandbox"])
+def test_batch_matches_single_cells(path):
     cells = _cells()
-    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV)
+    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV,
+                       render_path=path)
     br.set_sigmas([c[5] for c in cells])
     br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
     V = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV,
@@ -50,9 +53,10 @@ def test_batch_matches_single_cells():
         # on the tile variants the batch was planned with (a different variant sums
         # in another order, and the normalised loss's gradient amplifies rounding at
         # the image minimum, where |z| is near zero)
-        r = MeshRenderer(box, shape, 1e-5, DEV, render_path="dense", autotune=False)
+        r = MeshRenderer(box, shape, 1e-5, DEV, render_path=path, autotune=False)
         r.set_sigma(torch.tensor(sig, dtype=torch.float32, device=DEV))
         assert r.n_band == br.band_sizes[i]
+        assert r.use_bandbox == (path == "bandbox") and br.use_bandbox == (path == "bandbox")
         Vi = torch.tensor(v, dtype=torch.float32, device=DEV, requires_grad=True)
         Ci = torch.tensor(c, dtype=torch.float32, device=DEV, requires_grad=True)
         Ti = br.cell_view(target, i).contiguous()
@@ -62,11 +66,14 @@ def test_batch_matches_single_cells():
         assert rel_l2(V.grad[vo[i]:vo[i + 1]].cpu().numpy(), Vi.grad.cpu().numpy()) < 1e-5
         assert rel_l2(C.grad[fo[i]:fo[i + 1]].cpu().numpy(), Ci.grad.cpu().numpy()) < 1e-5
     assert abs(float(loss) - total) < 1e-5 * abs(total)
+    assert br.device_error() == 0
 
 
-def test_batch_fit_step_graph_equals_eager():
+@pytest.mark.parametrize("path", ["dense", "bandbox"])
+def test_batch_fit_step_graph_equals_eager(path):
     cells = _cells(4, seed=3)
-    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV)
+    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV,
+                       render_path=path)
     br.set_sigmas([c[5] for c in cells])
     br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
     V0 = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV)
@@ -80,11 +87,14 @@ def test_batch_fit_step_graph_equals_eager():
     assert torch.equal(a.V, b.V)
 
 
-def test_batch_cells_match_oracle_pipeline():
+@pytest.mark.parametrize("path", ["dense", "bandbox"])
+def test_batch_cells_match_oracle_pipeline(path):
     """Every cell of a batch against the float64 oracle chain (meshFT -> render ->
     normalise -> mse -> gradients), with the float32 chain's noise floor."""
     cells = _cells(4, seed=7)
-    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV)
+    br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV,
+                       render_path=path)
+    assert br.use_bandbox == (path == "bandbox")
     br.set_sigmas([c[5] for c in cells])
     br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
     V = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV,
@@ -109,3 +119,65 @@ def test_batch_cells_match_oracle_pipeline():
         assert ev < max(2e-4, 2 * fl["verts"])
         assert ec < max(1e-4, 2 * fl["coeff"])
     assert abs(float(loss) - total) < 1e-4 * abs(total)
+
+
+def test_batch_bandbox_wide_bands_and_image():
+    """Cells whose band extent along the line axis needs the two-chunk gradient
+    pass (above 32), mixed with narrow ones and three grid shapes: image, per-cell
+    loss and dL/dS of the batched band-box DFTs against the batched cuFFT chain on
+    the same spectra.  One dominant frequency per cell keeps |z| away from zero,
+    so the normalised loss's gradient at the image minimum is well determined."""
+    rng = np.random.default_rng(11)
+    cells = []
+    for i, (shape, sz) in enumerate([((40, 36, 80), 5e-4), ((32, 32, 32), 2e-3),
+                                     ((48, 40, 64), 6e-4)]):
+        v, f = random_sh_shape(2, 0.3, 4, 0.08, seed=200 + i)
+        box = oracle.compute_box_size(v, 0.2)
+        cells.append((v, f, rng.uniform(0.5, 1.5, len(f)), box, shape,
+                      np.diag([2e-3, 2e-3, sz])))
+    rs = {}
+    for path in ("dense", "bandbox"):
+        br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV,
+                           render_path=path)
+        br.set_sigmas([c[5] for c in cells])
+        br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
+        assert br.use_bandbox == (path == "bandbox")
+        rs[path] = br
+    bb, dn = rs["bandbox"], rs["dense"]
+    V = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV)
+    C = torch.tensor(np.concatenate([c[2] for c in cells]), dtype=torch.float32, device=DEV)
+    ft = bb.forward_spectrum(V, C, dense=False)
+    offs = np.concatenate([[0], np.cumsum(bb.band_sizes)])
+    band = bb.band.long()
+    gidx = torch.cat([band[offs[i]:offs[i + 1]] + bb.grid_offset[i] for i in range(len(cells))])
+    otf_b = bb.otf[gidx]
+    for i in range(len(cells)):  # one dominant frequency per cell
+        sl = slice(int(offs[i]), int(offs[i + 1]))
+        o = otf_b[sl]
+        k = int(torch.argmax(o))
+        ft[sl] = 0.3 * ft[sl] / float((ft[sl].abs() * o).sum())
+        ft[sl][k] += 1.0 / float(o[k])
+    # the cuFFT chain on the same spectra
+    dn.spec.zero_()
+    dn.spec[gidx] = ft * otf_b
+    dn.inverse_fft()
+    _, img0, _ = dn.image_loss("sum", None, want_grad=False, want_image=True)
+    target = torch.empty_like(img0)
+    for i in range(len(cells)):
+        x = dn.cell_view(img0, i)
+        nx = (x - x.min()) / (x.max() - x.min())
+        noise = torch.tensor(rng.normal(size=x.shape), dtype=torch.float32, device=DEV)
+        dn.cell_view(target, i).copy_(nx + 0.05 * noise)
+    ld, imgd, gz = dn.image_loss("mse", target, want_grad=True, want_image=True)
+    dn.adjoint_fft(gz)
+    Gd = dn.G[gidx]
+    lb, Gb, imgb = bb.render_loss_bandbox(ft, "mse", target, want_grad=True, want_image=True)
+    torch.cuda.synchronize()
+    assert bb.device_error() == 0
+    for i in range(len(cells)):
+        sl = slice(int(offs[i]), int(offs[i + 1]))
+        e_img = rel_l2(bb.cell_view(imgb, i).cpu().numpy(), dn.cell_view(imgd, i).cpu().numpy())
+        e_l = abs(float(lb[i]) - float(ld[i])) / abs(float(ld[i]))
+        e_g = rel_l2(Gb[sl].cpu().numpy(), Gd[sl].cpu().numpy())
+        print(f"cell {i} {cells[i][4]}: image {e_img:.2e} loss {e_l:.2e} dL/dS {e_g:.2e}")
+        assert e_img < 2e-6 and e_l < 5e-5 and e_g < 1e-4, i
