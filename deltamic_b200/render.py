@@ -24,8 +24,8 @@ kernels (fixed-point phases; error against a float64 evaluation ~1e-6);
 reference's CPU path, Seps = sqrt(1.19209e-07), band selected on the float64 OTF)
 and returns complex128.  ``render_image_from_ftmesh`` of a float32 spectrum that
 ``Fourier3dMesh`` returned (unmodified) runs the band-box DFTs of bandbox.cu,
-which touch only the band's bounding box; other spectra take
-``abs(ifftn(ftmesh * OTF))`` on cuFFT.  ``normalize_tensor`` of a CUDA float32 /
+which touch only the band's bounding box, for boxes of 64^3 voxels or more; other
+spectra take ``abs(ifftn(ftmesh * OTF))`` on cuFFT.  ``normalize_tensor`` of a CUDA float32 /
 float64 tensor runs the kernels of normalize.cu.  In the autofluorescence transform the
 reference's value at xi = 0 (grids with every axis odd) is 0/0 = NaN; here it is
 the limit of its volume term, ``1 - regint`` in all.
@@ -145,9 +145,16 @@ class _BandImage(torch.autograd.Function):
         return g_ft, g_otf, None, None, None
 
 
+# Below this many voxels the two cuFFT transforms of the dense route cost less than
+# the band-box route's launches (and its backward recomputes z).
+_BAND_ROUTE_MIN_VOXELS = 1 << 18
+
+
 def _band_route(ftmesh, OTF, box_shape):
     info = getattr(ftmesh, "_dm_band", None)
     if info is None or info[2] != ftmesh._version or ftmesh.dtype != torch.complex64:
+        return None
+    if ftmesh.numel() < _BAND_ROUTE_MIN_VOXELS:
         return None
     if not (isinstance(OTF, torch.Tensor) and OTF.is_cuda and OTF.dtype == torch.float32
             and OTF.device == ftmesh.device and tuple(OTF.shape) == tuple(ftmesh.shape)):
@@ -169,7 +176,8 @@ def render_image_from_ftmesh(ftmesh, OTF, box_shape):
 
     For a float32 spectrum straight from :class:`Fourier3dMesh` (zero off its
     narrow band; no in-place change since) with a real float32 OTF of the same
-    shape, the image comes from the band-box DFTs; otherwise from cuFFT."""
+    shape and at least 64^3 voxels, the image comes from the band-box DFTs;
+    otherwise from cuFFT."""
     route = _band_route(ftmesh, OTF, box_shape)
     if route is not None:
         band, plan, band64 = route

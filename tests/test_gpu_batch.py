@@ -7,7 +7,7 @@ import torch
 
 import oracle
 from conftest import rel_l2
-from deltamic_b200 import MeshRenderer
+from deltamic_b200 import MeshRenderer, ops
 from deltamic_b200.batch import BatchFitStep, BatchRenderer
 from deltamic_b200.mesh import random_sh_shape
 
@@ -94,9 +94,9 @@ def test_batch_cells_match_oracle_pipeline(path):
     cells = _cells(4, seed=7)
     br = BatchRenderer([c[3] for c in cells], [c[4] for c in cells], 1e-5, DEV,
                        render_path=path)
-    assert br.use_bandbox == (path == "bandbox")
     br.set_sigmas([c[5] for c in cells])
     br.set_meshes([c[0] for c in cells], [c[1] for c in cells])
+    assert br.use_bandbox == (path == "bandbox")
     V = torch.tensor(np.concatenate([c[0] for c in cells]), dtype=torch.float32, device=DEV,
                      requires_grad=True)
     C = torch.tensor(np.concatenate([c[2] for c in cells]), dtype=torch.float32, device=DEV,
@@ -174,10 +174,22 @@ def test_batch_bandbox_wide_bands_and_image():
     lb, Gb, imgb = bb.render_loss_bandbox(ft, "mse", target, want_grad=True, want_image=True)
     torch.cuda.synchronize()
     assert bb.device_error() == 0
+    errs = []
     for i in range(len(cells)):
         sl = slice(int(offs[i]), int(offs[i + 1]))
         e_img = rel_l2(bb.cell_view(imgb, i).cpu().numpy(), dn.cell_view(imgd, i).cpu().numpy())
         e_l = abs(float(lb[i]) - float(ld[i])) / abs(float(ld[i]))
         e_g = rel_l2(Gb[sl].cpu().numpy(), Gd[sl].cpu().numpy())
-        print(f"cell {i} {cells[i][4]}: image {e_img:.2e} loss {e_l:.2e} dL/dS {e_g:.2e}")
+        # the same cell through the single-box call
+        band_i = bb.band[sl].contiguous()
+        plan = ops.BandBox(bb.grids[i], band_i)
+        l1, _, G1 = ops.render_loss_bandbox(ft[sl].contiguous(), band_i, plan,
+                                            bb.cell_view(bb.otf, i).contiguous(), "mse",
+                                            bb.cell_view(target, i).contiguous())
+        e_1 = rel_l2((G1 / bb.grids[i].numel).cpu().numpy(), Gd[sl].cpu().numpy())
+        e_b1 = rel_l2(Gb[sl].cpu().numpy(), (G1 / bb.grids[i].numel).cpu().numpy())
+        print(f"cell {i} {cells[i][4]} extent {plan.extent}: image {e_img:.2e} loss {e_l:.2e} "
+              f"dL/dS {e_g:.2e}; single box vs cuFFT {e_1:.2e}, batch vs single box {e_b1:.2e}")
+        errs.append((e_img, e_l, e_g))
+    for i, (e_img, e_l, e_g) in enumerate(errs):
         assert e_img < 2e-6 and e_l < 5e-5 and e_g < 1e-4, i

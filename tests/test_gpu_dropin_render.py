@@ -86,7 +86,7 @@ def _dense_image64(ft, otf, shape):
                                      list(shape)))
 
 
-@pytest.mark.parametrize("shape", [(64, 64, 64), (72, 60, 48), (200, 200, 200)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (80, 72, 60), (200, 200, 200)])
 def test_render_bandbox_route_matches_dense(shape):
     fm, otf, v, f, c = _scene(shape, level=3 if shape[0] < 200 else 5)
     V = torch.tensor(v, dtype=torch.float32, device=DEV, requires_grad=True)
@@ -167,3 +167,8 @@ def test_render_route_falls_back_after_in_place_change():
     assert rel_l2(img.cpu().numpy(), _dense_image64(ft, otf, shape).cpu().numpy()) < 1e-5
     # a padded box_shape is not the band box's grid either
     assert render._band_route(ft, otf, (70, 64, 64)) is None
+    # below 64^3 voxels the dense route is the cheaper one
+    fs, os_, vs, f_s, cs = _scene((40, 40, 40))
+    fts = fs(torch.tensor(vs, dtype=torch.float32, device=DEV), torch.tensor(f_s, device=DEV),
+             torch.tensor(cs, dtype=torch.float32, device=DEV))
+    assert render._band_route(fts, os_, (40, 40, 40)) is None

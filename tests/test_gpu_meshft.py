@@ -109,6 +109,22 @@ def test_drop_in_chain_matches_reference_golden(golden):
     img_fft = torch.abs(torch.fft.ifftn(ft.detach() * 1 * otf.detach(), list(shape)))
     print(name, "image vs reference float64: %.2e (cuFFT of the same spectrum %.2e)" % (
         e_img, rel_l2(img_fft.cpu().numpy(), d["image"])))
+    # the vertex gradient through each combination of render route and normalize
+    for route in ("bandbox", "cufft"):
+        for nrm in ("kernels", "eager"):
+            Vx = _t(d["verts"]).requires_grad_(True)
+            ftx = mft(Vx, F, C.detach())
+            if route == "cufft":
+                ftx = ftx * 1
+            ix = dm.render_image_from_ftmesh(ftx, otf.detach(), shape)
+            if nrm == "kernels":
+                nx = dm.normalize_tensor(ix)
+            else:
+                nx = (ix - ix.min()) / (ix.max() - ix.min())
+            lx = nx.sum() if str(d["loss_kind"]) == "sum" else \
+                torch.mean((nx - _t(d["target"])) ** 2)
+            lx.backward()
+            print(name, route, nrm, "verts %.2e" % rel_l2(Vx.grad.cpu().numpy(), d["grad_verts"]))
     assert e_ft < TOL_FT, name
     assert e_img < TOL_FT, name
     ev = rel_l2(V.grad.cpu().numpy(), d["grad_verts"])
