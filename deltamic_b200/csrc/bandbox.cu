@@ -245,31 +245,35 @@ struct GemmP {
   int64_t scb, scm, scn, scp;
 };
 
-// One 64 x 32 output tile (bx, by) of split / batch entry bz.
-template <bool kInv>
+// One (16 RM) x 32 output tile (bx, by) of split / batch entry bz; each thread
+// owns RM x 2 outputs (RM = 4: 64-row tiles; RM = 2: 32-row tiles, for products
+// with few rows).
+template <bool kInv, int RM = 4>
 __device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int bz) {
+  constexpr int TM = 16 * RM;   // tile rows
+  constexpr int RA = TM / 16;   // A elements per thread and k step
   const float2* __restrict__ W = p.W;
   const float2* __restrict__ X = p.X;
   const int ldw = p.ldw, M = p.M, N = p.N, K = p.K, batch = p.batch, kc = p.kc;
   const int xparts = p.xparts;
   const int64_t sxb = p.sxb, sxk = p.sxk, sxp = p.sxp;
   // rows padded by 16 bytes: the forward pass stores A with k across the lanes
-  __shared__ __align__(16) float2 As[16][66];
+  __shared__ __align__(16) float2 As[16][TM + 2];
   __shared__ __align__(16) float2 Bs[16][32];
   const int t = threadIdx.x;
   const int tm = t >> 4, tn = t & 15;
-  const int m0 = by * 64, n0 = bx * 32;
+  const int m0 = by * TM, n0 = bx * 32;
   const int64_t b = bz % batch;
   const int kp = bz / batch;
   const int kb = kp * kc, ke = min(K, kb + kc);
   const float2* Xb = X + b * sxb;
-  float2 ra[4], rb[2];
+  float2 ra[RA], rb[2];
   auto fetch = [&](int k0) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < RA; ++r) {
       const int e = t + kGemmThreads * r;
-      const int m = kInv ? (e & 63) : (e >> 4);
-      const int k = kInv ? (e >> 6) : (e & 15);
+      const int m = kInv ? (e % TM) : (e >> 4);
+      const int k = kInv ? (e / TM) : (e & 15);
       float2 v = make_float2(0.f, 0.f);
       if (m0 + m < M && k0 + k < ke) {
         if (kInv) {
@@ -298,16 +302,16 @@ __device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int
       rb[r] = v;
     }
   };
-  float2 acc[4][2];
+  float2 acc[RM][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+  for (int i = 0; i < RM; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
   if (kb < ke) fetch(kb);
   for (int k0 = kb; k0 < ke; k0 += 16) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < RA; ++r) {
       const int e = t + kGemmThreads * r;
-      const int m = kInv ? (e & 63) : (e >> 4);
-      const int k = kInv ? (e >> 6) : (e & 15);
+      const int m = kInv ? (e % TM) : (e >> 4);
+      const int k = kInv ? (e / TM) : (e & 15);
       As[k][m] = ra[r];
     }
 #pragma unroll
@@ -319,14 +323,17 @@ __device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int
     if (k0 + 16 < ke) fetch(k0 + 16);
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
-      const float4 a01 = *reinterpret_cast<const float4*>(&As[kk][tm * 4]);
-      const float4 a23 = *reinterpret_cast<const float4*>(&As[kk][tm * 4 + 2]);
+      float2 a[RM];
+#pragma unroll
+      for (int q = 0; q < RM / 2; ++q) {
+        const float4 v = *reinterpret_cast<const float4*>(&As[kk][tm * RM + 2 * q]);
+        a[2 * q] = make_float2(v.x, v.y);
+        a[2 * q + 1] = make_float2(v.z, v.w);
+      }
       const float4 bb = *reinterpret_cast<const float4*>(&Bs[kk][tn * 2]);
-      const float2 a[4] = {make_float2(a01.x, a01.y), make_float2(a01.z, a01.w),
-                           make_float2(a23.x, a23.y), make_float2(a23.z, a23.w)};
       const float2 bv[2] = {make_float2(bb.x, bb.y), make_float2(bb.z, bb.w)};
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < RM; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j] = cmac(acc[i][j], a[i], bv[j]);
     }
@@ -334,8 +341,8 @@ __device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int
   }
   float2* Cb = p.C + kp * p.scp + b * p.scb;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int m = m0 + tm * 4 + i;
+  for (int i = 0; i < RM; ++i) {
+    const int m = m0 + tm * RM + i;
     if (m >= M) continue;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -345,9 +352,9 @@ __device__ __forceinline__ void bb_gemm_tile(const GemmP& p, int bx, int by, int
   }
 }
 
-template <bool kInv>
+template <bool kInv, int RM>
 __global__ void __launch_bounds__(kGemmThreads) k_bb_gemm(GemmP p) {
-  bb_gemm_tile<kInv>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+  bb_gemm_tile<kInv, RM>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -1043,19 +1050,23 @@ GemmP gemm_p(const float2* W, int ldw, int M, int N, int K, int kc, const float2
   return p;
 }
 
-// grid of one product: N tiles, M tiles, batch x K splits
-dim3 gemm_grid(const GemmP& p) {
+// grid of one product: N tiles, M tiles (of 16 rm rows), batch x K splits
+dim3 gemm_grid(const GemmP& p, int rm = 4) {
   const int splits = (p.K + p.kc - 1) / p.kc;
-  return dim3((p.N + 31) / 32, (p.M + 63) / 64, p.batch * splits);
+  return dim3((p.N + 31) / 32, (p.M + 16 * rm - 1) / (16 * rm), p.batch * splits);
 }
 
+// The axis-1 forward contraction has few rows (band offsets j1): 32-row tiles.
 template <bool kInv>
 void gemm(const float2* W, int ldw, int M, int N, int K, int kc, const float2* X, int64_t sxb,
           int64_t sxk, int xparts, int64_t sxp, float2* C, int64_t scb, int64_t scm,
           int64_t scn, int64_t scp, int batch, cudaStream_t st) {
   const GemmP p = gemm_p(W, ldw, M, N, K, kc, X, sxb, sxk, xparts, sxp, C, scb, scm, scn, scp,
                          batch);
-  k_bb_gemm<kInv><<<gemm_grid(p), kGemmThreads, 0, st>>>(p);
+  if (kInv)
+    k_bb_gemm<kInv, 4><<<gemm_grid(p, 4), kGemmThreads, 0, st>>>(p);
+  else
+    k_bb_gemm<kInv, 2><<<gemm_grid(p, 2), kGemmThreads, 0, st>>>(p);
 }
 
 
@@ -1146,10 +1157,11 @@ __global__ void k_bbb_scatter(const BBCell* __restrict__ cells, const int64_t* _
 template <bool kInv>
 __global__ void __launch_bounds__(kGemmThreads)
     k_bbb_gemm(const GemmP* __restrict__ ps, const int32_t* __restrict__ zp, int ncells) {
+  constexpr int RM = kInv ? 4 : 2;
   const int c = find_cell(zp, ncells, (int32_t)blockIdx.z);
   const GemmP p = ps[c];
-  if ((int)blockIdx.x * 32 >= p.N || (int)blockIdx.y * 64 >= p.M) return;
-  bb_gemm_tile<kInv>(p, blockIdx.x, blockIdx.y, (int)blockIdx.z - zp[c]);
+  if ((int)blockIdx.x * 32 >= p.N || (int)blockIdx.y * 16 * RM >= p.M) return;
+  bb_gemm_tile<kInv, RM>(p, blockIdx.x, blockIdx.y, (int)blockIdx.z - zp[c]);
 }
 
 template <int C>
@@ -1464,8 +1476,6 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
   int32_t* gord = (int32_t*)(host.data() + P.off_gord);
   int64_t* bpref = (int64_t*)(host.data() + P.off_bpref);
   const int sms = num_sms();
-  double wtot = 0.0;
-  for (int i = 0; i < ncells; ++i) wtot += (double)sh[i].nvox * sh[i].ext[2];
   size_t off = 0;
   bpref[0] = 0;
   for (int k = 0; k < 3; ++k) hz[k * (ncells + 1)] = 0;
@@ -1481,12 +1491,7 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
     c.grid_off = cells[i].grid_offset;
     c.inv_n = (float)(1.0 / (double)s.nvox);
     c.gscale = c.inv_n;
-    const int64_t tiles = (s.nlines + kLines - 1) / kLines;
-    const double share = 2.0 * sms * ((double)s.nvox * s.ext[2]) / wtot;
-    const int64_t ctas = std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)(share + 0.5)));
-    c.zctas = (int32_t)ctas;
     c.zcb = (int32_t)(s.ldw2 / (32 * s.zc));
-    c.gctas = (int32_t)ctas;
     c.e12 = s.ext[1] * s.ext[2];
     const int64_t e12 = c.e12;
     GemmP g[3];
@@ -1499,7 +1504,7 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
                   (int64_t)s.ext[2] * s.n[0], s.n[0], e12 * s.n[0], s.n[0]);
     for (int k = 0; k < 3; ++k) {
       hg[k * ncells + i] = g[k];
-      const dim3 gd = gemm_grid(g[k]);
+      const dim3 gd = gemm_grid(g[k], k == 2 ? 2 : 4);
       P.gx[k] = std::max<int64_t>(P.gx[k], gd.x);
       P.gy[k] = std::max<int64_t>(P.gy[k], gd.y);
       hz[k * (ncells + 1) + i + 1] = hz[k * (ncells + 1) + i] + (int32_t)gd.z;
@@ -1518,7 +1523,29 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
   std::vector<int> idx(ncells);
   for (int i = 0; i < ncells; ++i) idx[i] = i;
   auto jc_of = [&](int i) { return std::min(4, sh[i].ldj / 8); };
+  // CTAs of a line-pass launch: about two per SM (per column block), shared by the
+  // launch's cells in proportion to their work (voxels x band extent), at least one
+  // and at most one per line tile
+  auto share = [&](int first, int count, const std::vector<int>& ord, bool z) {
+    double wsum = 0.0;
+    for (int k = first; k < first + count; ++k)
+      wsum += (double)sh[ord[k]].nvox * sh[ord[k]].ext[2];
+    for (int k = first; k < first + count; ++k) {
+      const BBShape& s = sh[ord[k]];
+      const int64_t tiles = (s.nlines + kLines - 1) / kLines;
+      const double w = 2.0 * sms * ((double)s.nvox * s.ext[2]) / wsum;
+      const int32_t ctas =
+          (int32_t)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)(w + 0.5)));
+      if (z) hc[ord[k]].zctas = ctas; else hc[ord[k]].gctas = ctas;
+    }
+  };
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return sh[a].zc < sh[b].zc; });
+  for (int k0 = 0; k0 < ncells;) {
+    int k1 = k0;
+    while (k1 < ncells && sh[idx[k1]].zc == sh[idx[k0]].zc) ++k1;
+    share(k0, k1 - k0, idx, true);
+    k0 = k1;
+  }
   for (int k = 0; k < ncells;) {
     const int C = sh[idx[k]].zc;
     const int g = (int)P.nz++;
@@ -1534,6 +1561,12 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
     }
   }
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return jc_of(a) < jc_of(b); });
+  for (int k0 = 0; k0 < ncells;) {
+    int k1 = k0;
+    while (k1 < ncells && jc_of(idx[k1]) == jc_of(idx[k0])) ++k1;
+    share(k0, k1 - k0, idx, false);
+    k0 = k1;
+  }
   for (int k = 0; k < ncells;) {
     const int J = jc_of(idx[k]);
     const int g = (int)P.nj++;
