@@ -73,6 +73,9 @@ def parse():
                    help="the level-5 meshes at 64^3 instead of 200^3: the same meshFT kernel "
                         "work with small grids (for profiler captures)")
     p.add_argument("--skip-cpu-baseline", action="store_true")
+    p.add_argument("--variants", default=None,
+                   help="fit200: 'F,B' pins the forward / adjoint tile variants instead of "
+                        "autotuning them (a fixed launch sequence, for profiler captures)")
     p.add_argument("--train", type=int, default=50000, help="learned: training pairs")
     p.add_argument("--epochs", type=int, default=8, help="learned: training epochs")
     p.add_argument("--eval", type=int, default=256, help="learned: held-out shapes")
@@ -770,7 +773,10 @@ def setup_fit200(args, rank, dev):
     from deltamic_b200.fit import FitStep
     gt_v, init_v, faces_np, box = make_workload(rank, False)
     shape = (64, 64, 64) if args.small else SHAPE
-    r = MeshRenderer(box, shape, THRESH, dev)
+    r = MeshRenderer(box, shape, THRESH, dev, autotune=args.variants is None)
+    if args.variants is not None:
+        from deltamic_b200 import autotune
+        autotune.apply(tuple(int(v) for v in args.variants.split(",")))
     r.set_sigma(torch.diag(torch.tensor(SIGMA, device=dev)))
     F = torch.tensor(faces_np, device=dev)
     C = torch.ones(len(faces_np), device=dev)

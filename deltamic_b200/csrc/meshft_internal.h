@@ -16,7 +16,7 @@ struct FwdVariant {
 };
 struct BwdVariant {
   int F, NT, waves;
-  int minb = 1;  // CTAs per SM the register allocation must allow (launch bounds)
+  int minb = 0;  // CTAs per SM the register allocation must allow (0: no cap)
 };
 constexpr int kFwdTF = 64, kBwdTX = 128, kStages = 3;
 constexpr int kNumFwdVariants = 6;

@@ -392,7 +392,8 @@ __device__ __forceinline__ void load_xi(const XiRecOff& r, XiValOff& xv, float& 
   xv.fr[2] = __uint_as_float(w2.z);
 }
 
-template <int F, int NT, int TX, int NS, bool kVol = false, class XR = XiRec, int MINB = 1>
+// MINB > 0 caps the registers for MINB CTAs per SM; 0 leaves the choice to ptxas.
+template <int F, int NT, int TX, int NS, bool kVol = false, class XR = XiRec, int MINB = 0>
 __global__ void __launch_bounds__(NT, MINB) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
                                                   const float4* __restrict__ fw,
                                                   const XR* __restrict__ xrec,

@@ -301,10 +301,11 @@ DM_HD c32 expmi(float angle) {
 template <bool kGrad, bool kLo = false, class XV>
 DM_HD void eval_series(const XV& xv, const FaceGeom& g, float hab, float hca, float off_a,
                        c32& E, c32& H, c32& Hp2, c32& Hp3, float d[3], float& p2) {
-  const float ab = 2.0f * hab, ca = 2.0f * hca;
-  const float da = (ca - ab) * (1.0f / 3.0f);
-  const float db = da + ab;
-  const float dc = da - ca;
+  // d_a = (ca - ab) / 3, d_b = d_a + ab, d_c = d_a - ca for the full differences
+  // ab = 2 hab, ca = 2 hca (the doubling is exact, so these are the same floats)
+  const float da = (hca - hab) * (2.0f / 3.0f);
+  const float db = fmaf(2.0f, hab, da);
+  const float dc = fmaf(-2.0f, hca, da);
   p2 = da * da + db * db + dc * dc;
   const float p3 = 3.0f * da * db * dc;  // sum d^3 when sum d = 0
   E = expmi(vertex_angle(xv, g.Ua[0], g.Ua[1], g.Ua[2]) + (off_a - da));
@@ -510,12 +511,13 @@ DM_HD bool pair_adjoint_t(const XV& xv, const FaceGeom& g, float gre, float gim,
     const float hy = gre * E.y - gim * E.x;
     r = hx * H.x - hy * H.y;
     if (kF) Fo = cmul(E, H);
-    const float zt = (hx * H.y + hy * H.x) * (1.0f / 3.0f);
+    const float zt3 = hx * H.y + hy * H.x;  // z_a + z_b + z_c (sum d = 0)
+    const float zt = zt3 * (1.0f / 3.0f);
     const float r1 = 2.0f * (hx * Hp2.x - hy * Hp2.y);
     const float r2 = hx * Hp3.x - hy * Hp3.y;
     z[0] = zt + r1 * d[0] + r2 * (3.0f * d[0] * d[0] - p2);
     z[1] = zt + r1 * d[1] + r2 * (3.0f * d[1] * d[1] - p2);
-    z[2] = zt + r1 * d[2] + r2 * (3.0f * d[2] * d[2] - p2);
+    z[2] = (zt3 - z[0]) - z[1];
   } else {
     const float off[3] = {0.f, 0.f, 0.f};
     c32 E, G, Gu, Gw;
@@ -689,10 +691,9 @@ DM_HD void centroid_H2(v2 p2, v2 p3, v2& Hx, v2& Hy, v2& Hp2x, v2& Hp2y, v2& Hp3
 
 // Centroid deviations d_v, p2 and p3 of two pairs from their half differences.
 DM_HD void series_dev2(v2 hab, v2 hca, v2 d[3], v2& p2, v2& p3) {
-  const v2 ab = add2(hab, hab), ca = add2(hca, hca);
-  d[0] = mul2(sub2(ca, ab), B2(1.0f / 3.0f));
-  d[1] = add2(d[0], ab);
-  d[2] = sub2(d[0], ca);
+  d[0] = mul2(sub2(hca, hab), B2(2.0f / 3.0f));
+  d[1] = fma2(B2(2.0f), hab, d[0]);
+  d[2] = fma2(B2(-2.0f), hca, d[0]);
   p2 = fma2(d[2], d[2], fma2(d[1], d[1], mul2(d[0], d[0])));
   p3 = mul2(mul2(B2(3.0f), d[0]), mul2(d[1], d[2]));
 }
@@ -731,12 +732,14 @@ DM_HD void adjoint_series2(const XV& xv, const uint32_t Ua0[3], const uint32_t U
   const v2 hx = fma2(B2(gre), Ex, mul2(B2(gim), Ey));        // h = conj(g) E
   const v2 hy = fma2(B2(gre), Ey, mul2(B2(-gim), Ex));
   r = fma2(hx, Hx, mul2(neg2(hy), Hy));
-  const v2 zt = mul2(fma2(hx, Hy, mul2(hy, Hx)), B2(1.0f / 3.0f));
+  const v2 zt3 = fma2(hx, Hy, mul2(hy, Hx));  // z_a + z_b + z_c
+  const v2 zt = mul2(zt3, B2(1.0f / 3.0f));
   const v2 r1 = mul2(B2(2.0f), fma2(hx, Hp2x, mul2(neg2(hy), Hp2y)));
   const v2 r2 = fma2(hx, Hp3x, mul2(neg2(hy), Hp3y));
 #pragma unroll
-  for (int v = 0; v < 3; ++v)
+  for (int v = 0; v < 2; ++v)
     z[v] = fma2(r2, fma2(mul2(B2(3.0f), d[v]), d[v], neg2(p2)), fma2(r1, d[v], zt));
+  z[2] = sub2(sub2(zt3, z[0]), z[1]);
 }
 
 // Forward of one face (vertex-a position Ua) at two frequencies on the series
