@@ -83,6 +83,8 @@ def parse():
                    help="fit300: precondition the vertex gradient with (M M)^-1, M = I + lambda L, "
                         "and step with VectorAdam (0: plain Adam, the configured fit)")
     p.add_argument("--precond-lr", type=float, default=5e-3)
+    p.add_argument("--precond-method", choices=["auto", "dense", "chebyshev"], default="auto",
+                   help="fit300: the formed (M M)^-1 or two sparse Chebyshev solves with M")
     p.add_argument("--mask-grid", type=int, default=64,
                    help="masks64: grid points per axis of the masks (64: the workload's grid)")
     p.add_argument("--workload", choices=["fit200", "batch64", "fit300", "learned",
@@ -882,7 +884,8 @@ def run_fit300(args, rank, world, local):
     if args.precond_lambda > 0:
         from deltamic_b200.precond import LargeStepsPreconditioner
         t0 = time.perf_counter()
-        pc = LargeStepsPreconditioner(F, len(init_v), args.precond_lambda, dev)
+        pc = LargeStepsPreconditioner(F, len(init_v), args.precond_lambda, dev,
+                                      method=args.precond_method)
         torch.cuda.synchronize()
         t_setup = time.perf_counter() - t0
         kw = dict(lr=args.precond_lr, precond=pc, optimizer="vector_adam")
@@ -906,6 +909,9 @@ def run_fit300(args, rank, world, local):
                       "iou_init": iou0, "iou_final": iou1}}
     if args.precond_lambda > 0:
         out["config"]["precond_setup_s"] = t_setup
+        out["config"]["precond_method"] = pc.method
+        if pc.method == "chebyshev":
+            out["config"]["chebyshev_iterations_per_solve"] = pc.iters
     print(json.dumps(out), flush=True)
 
 

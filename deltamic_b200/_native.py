@@ -173,6 +173,8 @@ SIGNATURES = {
     "dm_voxelize": (_INT, [_P, _I64, _P, _I64, _BOXP, _P, _P, _P]),
     "dm_adam_step": (_INT, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _P, _P]),
     "dm_precond_apply": (_INT, [_P, _I64, _I64, _P, _P, _P]),
+    "dm_precond_chebyshev": (_INT, [_P, _P, _I64, _F, ctypes.c_double, ctypes.c_double, _INT,
+                                    _P, _P, _P, _P]),
     "dm_otf_from_spectrum": (_INT, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P]),
     "dm_otf_from_spectrum_backward": (_INT, [_P, _P, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, _P, _P]),

@@ -9,6 +9,8 @@
 // HBM-bound product: each warp streams eight rows of P with 16-byte loads (sixteen
 // in flight per lane) and multiplies them with the matching 4 x 3 block of g, read
 // through L1 as three 16-byte loads.
+// For meshes whose dense operator would not fit (or stream) well, the sparse form
+// below applies the same operator without forming it.
 // The optimizer is VectorAdam of optimize.py:215-258 (axis -1): the second
 // moment of each vertex is the squared norm of its 3-vector gradient.
 #include <cuda_runtime.h>
@@ -133,6 +135,59 @@ __global__ void k_vector_adam(float* __restrict__ p, const float* __restrict__ g
 
 __global__ void k_step_bump(int64_t* step) { *step += 1; }
 
+// Sparse form: (M M)^-1 g as two solves with M = I + lambda L, each a Chebyshev
+// iteration for the eigenvalue interval [theta - delta, theta + delta] of M (Saad,
+// Iterative Methods for Sparse Linear Systems, Alg. 12.1):
+//   x0 = 0, r0 = b, d0 = r0 / theta, rho0 = delta / theta;
+//   x_{k+1} = x_k + d_k,  r_{k+1} = r_k - M d_k,
+//   d_{k+1} = rho_{k+1} rho_k d_k + (2 rho_{k+1} / delta) r_{k+1},
+//   rho_{k+1} = 1 / (2 theta / delta - rho_k).
+// L is held as CSR neighbour lists (row i: the vertices sharing an edge with i), so
+// (M d)_i = (1 + lambda deg_i) d_i - lambda sum_j d_j.  One launch per iteration
+// (no device-side waits); the rho sequence is fixed by the interval, so the
+// launches carry their coefficients and replay in a CUDA graph.
+
+__global__ void k_cheb_init(const float* __restrict__ b, int64_t n3, float inv_theta,
+                            float* __restrict__ x, float* __restrict__ r,
+                            float* __restrict__ d) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float v = b[i];
+    x[i] = 0.f;
+    r[i] = v;
+    d[i] = v * inv_theta;
+  }
+}
+
+__global__ void k_cheb_iter(const int32_t* __restrict__ rowp, const int32_t* __restrict__ col,
+                            int64_t nv, float lam, float a, float c,
+                            const float* __restrict__ dc, float* __restrict__ dn,
+                            float* __restrict__ r, float* __restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t b = rowp[i], e = rowp[i + 1];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int32_t k = b; k < e; ++k) {
+      const int64_t j = 3 * (int64_t)col[k];
+      s0 += dc[j];
+      s1 += dc[j + 1];
+      s2 += dc[j + 2];
+    }
+    const float w = fmaf(lam, (float)(e - b), 1.0f);
+    const float s[3] = {s0, s1, s2};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int64_t o = 3 * i + q;
+      const float di = dc[o];
+      const float md = fmaf(w, di, -lam * s[q]);
+      x[o] += di;
+      const float ri = r[o] - md;
+      r[o] = ri;
+      dn[o] = fmaf(a, di, c * ri);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace dm
 
@@ -152,6 +207,49 @@ int dm_precond_apply(const float* P, int64_t nv, int64_t ldp, const float* grad,
   k_precond_gemv<<<(unsigned)blocks, kGemvThreads, 0, (cudaStream_t)stream>>>(
       P, nv, ldp, grad, out, ((uintptr_t)grad & 15) == 0);
   count_launches(1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+int dm_precond_chebyshev(const int32_t* rowp, const int32_t* col, int64_t nv, float lambda,
+                         double lo, double hi, int iters, const float* grad, float* out,
+                         float* work, dm_stream_t stream) {
+  if (nv < 0 || iters < 1 || iters > 4096 || !(lambda >= 0.f) || !(lo > 0.0) || !(hi >= lo))
+    return DM_ERR_INVALID_ARG;
+  if (nv == 0) return DM_OK;
+  if (!rowp || !col || !grad || !out || !work || grad == out) return DM_ERR_INVALID_ARG;
+  if (3 * nv > (int64_t)INT32_MAX * 64) return DM_ERR_SIZE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n3 = 3 * nv;
+  float* y = work;          // the first solve's result
+  float* r = work + n3;
+  float* d0 = work + 2 * n3;
+  float* d1 = work + 3 * n3;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+  const unsigned nb3 = (unsigned)std::min<int64_t>((n3 + 255) / 256, 148 * 8);
+  const unsigned nbv = (unsigned)std::min<int64_t>((nv + 127) / 128, 148 * 8);
+  int launches = 0;
+  for (int solve = 0; solve < 2; ++solve) {
+    const float* b = solve == 0 ? grad : y;
+    float* x = solve == 0 ? y : out;
+    k_cheb_init<<<nb3, 256, 0, st>>>(b, n3, (float)(1.0 / theta), x, r, d0);
+    ++launches;
+    double rho = delta > 0.0 ? delta / theta : 0.0;
+    float* dc = d0;
+    float* dn = d1;
+    for (int k = 0; k < iters; ++k) {
+      double a = 0.0, c = 0.0;
+      if (delta > 0.0) {
+        const double rho1 = 1.0 / (2.0 * theta / delta - rho);
+        a = rho1 * rho;
+        c = 2.0 * rho1 / delta;
+        rho = rho1;
+      }
+      k_cheb_iter<<<nbv, 128, 0, st>>>(rowp, col, nv, lambda, (float)a, (float)c, dc, dn, r, x);
+      ++launches;
+      std::swap(dc, dn);
+    }
+  }
+  count_launches(launches);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 

@@ -621,6 +621,14 @@ int dm_otf_from_spectrum_backward(const float* spectrum, const float* grad_otf, 
  * DEVICE int64 counter that the call increments. */
 int dm_precond_apply(const float* P, int64_t nv, int64_t ldp, const float* grad, float* out,
                      dm_stream_t stream);
+/* (M M)^-1 grad without forming the operator: two Chebyshev solves with
+ * M = I + lambda L for the eigenvalue interval [lo, hi] of M (lo > 0), ``iters``
+ * iterations each (one launch per iteration).  L from CSR neighbour lists rowp[nv+1],
+ * col[] (DEVICE int32: row i lists the vertices sharing an edge with i, so L = D - A
+ * of the uniform Laplacian); grad, out [nv][3]; work: 12 nv floats (DEVICE). */
+int dm_precond_chebyshev(const int32_t* rowp, const int32_t* col, int64_t nv, float lambda,
+                         double lo, double hi, int iters, const float* grad, float* out,
+                         float* work, dm_stream_t stream);
 int dm_vector_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_norm_sq,
                         int64_t nv, float lr, float beta1, float beta2, float eps, int64_t* step,
                         dm_stream_t stream);

@@ -106,3 +106,38 @@ def test_preconditioned_fit_converges_with_regular_edges():
     assert iou_pre >= 0.97
     assert float(pre["losses"][-1]) < 0.2 * float(pre["losses"][0])
     assert sp_pre < 1.5 * sp0
+
+
+@pytest.mark.parametrize("level,lam", [(3, 20.0), (5, 50.0)])
+def test_chebyshev_form_matches_oracle_operator(level, lam):
+    """The sparse form (two Chebyshev solves with M, no formed operator) against the
+    oracle's (M M)^-1 and against the dense form, and under a CUDA graph."""
+    v, f = icosphere(level, 0.3)
+    F = torch.tensor(f, device=DEV)
+    pc = LargeStepsPreconditioner(F, len(v), lam, DEV, method="chebyshev")
+    assert pc.method == "chebyshev" and pc.P is None
+    rng = np.random.default_rng(level)
+    g = rng.normal(size=(len(v), 3))
+    G = torch.tensor(g, dtype=torch.float32, device=DEV)
+    out = pc.apply(G)
+    dense = LargeStepsPreconditioner(F, len(v), lam, DEV, method="dense").apply(G)
+    if level <= 3:
+        P64 = oracle.fit.precondition_matrix(f, len(v), lam)
+        assert rel_l2(out.cpu().numpy(), P64 @ g) < 1e-5
+    assert rel_l2(out.cpu().numpy(), dense.cpu().numpy()) < 1e-5
+    print(f"level {level} lambda {lam}: {pc.iters} iterations per solve, interval "
+          f"[{pc.lo}, {pc.hi}]")
+    # graph replay gives the eager result
+    o2 = torch.empty_like(G)
+    side = torch.cuda.Stream(device=DEV)
+    side.wait_stream(torch.cuda.current_stream(DEV))
+    with torch.cuda.stream(side):
+        pc.apply(G, o2)
+    torch.cuda.current_stream(DEV).wait_stream(side)
+    gr = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gr):
+        pc.apply(G, o2)
+    o2.zero_()
+    gr.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(o2, out)
