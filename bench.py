@@ -47,10 +47,10 @@ LR = 1e-3
 FWD_FP32, FWD_MUFU = 32, 7
 BWD_FP32, BWD_MUFU = 80, 9
 # DRAM bytes (read + write) per launch of the adjoint kernel in this workload, from
-# one ncu capture of the fit step (dram__bytes_read.sum + dram__bytes_write.sum):
-# the kernel streams face records and frequency
-# tiles, far below its compute time at HBM speed.
-NCU_TRAFFIC_BWD = 3061248 + 577024
+# one ncu capture of the fit step's adjoint launch (dram__bytes_read.sum +
+# dram__bytes_write.sum, paired-FP32 two-face variant): the kernel streams face
+# records and frequency tiles, far below its compute time at HBM speed.
+NCU_TRAFFIC_BWD = 1919488 + 150784
 # Surface + enclosed-volume transform (render.py:228-318): the complex weight
 # a_k + i beta xi.nor_k/|xi|^2 adds 5 FP32 ops per pair to the forward (the
 # normal's dot product and a second complex accumulate) and 18 to the adjoint
@@ -1136,11 +1136,15 @@ def run_ours(args, rank, world, local):
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    # an NVTX range around the timed steps: ncu --nvtx --nvtx-include "timed/" lists
+    # exactly these launches
+    torch.cuda.nvtx.range_push("timed")
     e0.record()
     for _ in range(args.steps):
         step()
     e1.record()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()

@@ -1192,10 +1192,13 @@ __global__ void k_bbb_ties(const BBCell* __restrict__ cells) {
           (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// CTA bx takes the cell's columns bx, bx + gridDim.x, ...
 __global__ void __launch_bounds__(kColThreads) k_bbb_columns(const BBCell* __restrict__ cells) {
   const BBCell& cc = cells[blockIdx.z];
-  if ((int)blockIdx.x >= cc.e12) return;
-  bb_columns(cc.s, cc.w.q1p, cc.w.w0, cc.w.g0, blockIdx.x);
+  for (int64_t c = blockIdx.x; c < cc.e12; c += gridDim.x) {
+    bb_columns(cc.s, cc.w.q1p, cc.w.w0, cc.w.g0, c);
+    __syncthreads();  // the column's staged values are read; the next one overwrites them
+  }
 }
 
 __global__ void k_bbb_gather(const BBCell* __restrict__ cells, const int64_t* __restrict__ bpref,
@@ -1510,7 +1513,7 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
       hz[k * (ncells + 1) + i + 1] = hz[k * (ncells + 1) + i] + (int32_t)gd.z;
     }
     P.ties_x = std::max<int64_t>(P.ties_x, (s.nlines + 127) / 128);
-    P.col_x = std::max<int64_t>(P.col_x, e12);
+    P.col_x = std::max<int64_t>(P.col_x, (e12 + 7) / 8);  // eight columns per CTA
     P.col_smem = std::max<int64_t>(P.col_smem, (int64_t)sizeof(float2) * s.n[0]);
   }
   P.total_band = bpref[ncells];
@@ -1526,14 +1529,22 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
   // CTAs of a line-pass launch: about two per SM (per column block), shared by the
   // launch's cells in proportion to their work (voxels x band extent), at least one
   // and at most one per line tile
+  // (as many as shared memory lets reside, up to four, when the launch's tiles are
+  // small)
   auto share = [&](int first, int count, const std::vector<int>& ord, bool z) {
     double wsum = 0.0;
-    for (int k = first; k < first + count; ++k)
-      wsum += (double)sh[ord[k]].nvox * sh[ord[k]].ext[2];
+    size_t smem = 0;
+    for (int k = first; k < first + count; ++k) {
+      const BBShape& s = sh[ord[k]];
+      wsum += (double)s.nvox * s.ext[2];
+      smem = std::max(smem, z ? zlines_smem(s) : gradlines_smem(s.n[2], s.ldj));
+    }
+    const int per_sm = (int)std::max<size_t>(
+        2, std::min<size_t>(4, (size_t)kSmemLimit / std::max<size_t>(smem + 8192, 1)));
     for (int k = first; k < first + count; ++k) {
       const BBShape& s = sh[ord[k]];
       const int64_t tiles = (s.nlines + kLines - 1) / kLines;
-      const double w = 2.0 * sms * ((double)s.nvox * s.ext[2]) / wsum;
+      const double w = (double)per_sm * sms * ((double)s.nvox * s.ext[2]) / wsum;
       const int32_t ctas =
           (int32_t)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)(w + 0.5)));
       if (z) hc[ord[k]].zctas = ctas; else hc[ord[k]].gctas = ctas;
