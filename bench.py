@@ -1125,7 +1125,8 @@ def run_ours(args, rank, world, local):
 
     step = make_step(not args.no_graph)
     from deltamic_b200 import autotune
-    tuned = autotune.current()[:2]  # the tile-shape variants the step runs
+    # the tile-shape variants the step runs (a batch keeps its own, planned for them)
+    tuned = getattr(getattr(step, "r", None), "variants", None) or autotune.current()[:2]
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

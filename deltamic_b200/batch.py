@@ -27,13 +27,15 @@ class BatchRenderer:
     """Cells ``i`` with ``boxes[i]`` ([3,2]) and ``shapes[i]`` (3 ints)."""
 
     def __init__(self, boxes, shapes, narrowband_thresh=1e-5, device="cuda",
-                 render_path="auto"):
+                 render_path="auto", autotune=True):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("BatchRenderer runs on CUDA devices only")
         if render_path not in ("auto", "bandbox", "dense"):
             raise ValueError("render_path must be 'auto', 'bandbox' or 'dense'")
         self.render_path = render_path
+        self.autotune = autotune
+        self.variants = None
         self.bb = None
         self.grids = [ops.FreqGrid(b, s) for b, s in zip(boxes, shapes)]
         self.ncells = len(self.grids)
@@ -148,29 +150,61 @@ class BatchRenderer:
             cells[i].nv, cells[i].nt, cells[i].n_band = nvs[i], nts[i], self.band_sizes[i]
             cells[i].grid_offset = self.grid_offset[i]
             cells[i].box = ops.band_box(self.grids[i], self.band_herm[i])
-        lib = N.lib()
-        self._desc = torch.empty(lib.dm_batch_desc_size(self.ncells), dtype=torch.uint8,
-                                 device=self.device)
-        self.batch = N.DmBatch()
-        N.check(lib.dm_batch_plan(cells, self.ncells, N.ptr(self._desc), self._desc.numel(),
-                                  ctypes.byref(self.batch), N.stream_ptr(self.device)),
-                "dm_batch_plan")
-        self._topo = torch.zeros(max(self.batch.topology_bytes, 256), dtype=torch.uint8,
-                                 device=self.device)
-        N.check(lib.dm_batched_topology_build(ctypes.byref(self.batch), N.ptr(faces),
-                                              N.ptr(self._topo), self._topo.numel(),
-                                              N.stream_ptr(self.device)),
-                "dm_batched_topology_build")
+        self._cells = cells
         self.faces = faces
         self.nv, self.nt = nvs, nts
+        self._plan()
         self.pairs = sum(nt * nb for nt, nb in zip(nts, self.band_sizes))
         # face*xi pairs the kernels evaluate (half of each mirror-symmetric band)
         self.eval_pairs = sum(nt * ((nb + 1) // 2 if h else nb)
                               for nt, nb, h in zip(nts, self.band_sizes, self.band_herm))
+        return faces
+
+    def _plan(self):
+        """Plan the meshFT launches for the current tile variants (the launches use
+        the variants the plan was made for), topology and workspaces."""
+        lib = N.lib()
+        self._desc = torch.empty(lib.dm_batch_desc_size(self.ncells), dtype=torch.uint8,
+                                 device=self.device)
+        self.batch = N.DmBatch()
+        N.check(lib.dm_batch_plan(self._cells, self.ncells, N.ptr(self._desc),
+                                  self._desc.numel(), ctypes.byref(self.batch),
+                                  N.stream_ptr(self.device)), "dm_batch_plan")
+        self._topo = torch.zeros(max(self.batch.topology_bytes, 256), dtype=torch.uint8,
+                                 device=self.device)
+        N.check(lib.dm_batched_topology_build(ctypes.byref(self.batch), N.ptr(self.faces),
+                                              N.ptr(self._topo), self._topo.numel(),
+                                              N.stream_ptr(self.device)),
+                "dm_batched_topology_build")
         self._ws = {k: torch.zeros(max(int(getattr(self.batch, k)), 256), dtype=torch.uint8,
                                    device=self.device)
                     for k in ("fwd_workspace", "bwd_workspace", "image_workspace")}
-        return faces
+
+    def tune(self, verts, coeff):
+        """Time every forward and adjoint tile variant on this batch (a plan per
+        variant) and keep the fastest; the batch is re-planned for them."""
+        from . import autotune
+        f0, b0, nf, nb = autotune.current()
+        g = torch.ones(self.band.numel(), dtype=torch.complex64, device=self.device)
+
+        def with_variant(v):
+            autotune.apply(v)
+            self._plan()
+
+        def fwd():
+            return self.forward_spectrum(verts, coeff, dense=False)
+
+        ft = fwd()
+
+        def bwd():
+            return self.backward(verts, coeff, ft, want_coeff=False, grad_list=g)
+
+        best_f = autotune._pick(nf, lambda v: with_variant((v, b0)), fwd, 2, trials=2)
+        best_b = autotune._pick(nb, lambda v: with_variant((best_f, v)), bwd, 2, trials=2)
+        self.variants = (best_f, best_b)
+        with_variant(self.variants)
+        autotune.apply((f0, b0))
+        return self.variants
 
     # -- stages -----------------------------------------------------------------
     def forward_spectrum(self, verts, coeff, dense=True):
@@ -314,6 +348,8 @@ class BatchFitStep:
         self.cell_losses = torch.zeros(r.ncells, dtype=torch.float32, device=verts.device)
         self.graph = None
         self.launches_per_step = None
+        if r.autotune and r.variants is None:
+            r.tune(verts.detach().contiguous(), self.C)  # before any capture: it re-plans
         if graph:
             self._capture()
 

@@ -1192,13 +1192,10 @@ __global__ void k_bbb_ties(const BBCell* __restrict__ cells) {
           (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// CTA bx takes the cell's columns bx, bx + gridDim.x, ...
 __global__ void __launch_bounds__(kColThreads) k_bbb_columns(const BBCell* __restrict__ cells) {
   const BBCell& cc = cells[blockIdx.z];
-  for (int64_t c = blockIdx.x; c < cc.e12; c += gridDim.x) {
-    bb_columns(cc.s, cc.w.q1p, cc.w.w0, cc.w.g0, c);
-    __syncthreads();  // the column's staged values are read; the next one overwrites them
-  }
+  if ((int)blockIdx.x >= cc.e12) return;
+  bb_columns(cc.s, cc.w.q1p, cc.w.w0, cc.w.g0, blockIdx.x);
 }
 
 __global__ void k_bbb_gather(const BBCell* __restrict__ cells, const int64_t* __restrict__ bpref,
@@ -1513,7 +1510,7 @@ int dm_bandbox_batch_plan(const dm_cell* cells, const int32_t* bounds, int ncell
       hz[k * (ncells + 1) + i + 1] = hz[k * (ncells + 1) + i] + (int32_t)gd.z;
     }
     P.ties_x = std::max<int64_t>(P.ties_x, (s.nlines + 127) / 128);
-    P.col_x = std::max<int64_t>(P.col_x, (e12 + 7) / 8);  // eight columns per CTA
+    P.col_x = std::max<int64_t>(P.col_x, e12);
     P.col_smem = std::max<int64_t>(P.col_smem, (int64_t)sizeof(float2) * s.n[0]);
   }
   P.total_band = bpref[ncells];

@@ -446,6 +446,8 @@ static PlanTotals totals_of(const dm_batch* b) {
   t.band_blks = b->plan[6];
   t.fwd_items = b->plan[7];
   t.bwd_items = b->plan[8];
+  t.fwd_var = (int32_t)b->plan[10];
+  t.bwd_var = (int32_t)b->plan[11];
   return t;
 }
 
@@ -518,6 +520,8 @@ int dm_batch_plan(const dm_cell* cells, int ncells, void* desc, size_t desc_byte
                         t.face_blks, t.band_blks, t.fwd_items, t.bwd_items};
   for (int k = 0; k < 9; ++k) out->plan[k] = p[k];
   out->plan[9] = max_grid;
+  out->plan[10] = t.fwd_var;  // launches use the variants the tiles were planned for
+  out->plan[11] = t.bwd_var;
   out->cells = desc;
   return DM_OK;
 }

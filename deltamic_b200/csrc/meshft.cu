@@ -530,6 +530,8 @@ void plan_cell_tiles_for(CellDesc& d, const FwdVariant& fv, const BwdVariant& bv
 
 void plan_offsets(CellDesc* cells, int ncells, PlanTotals& t) {
   t = PlanTotals{};
+  t.fwd_var = fwd_variant();
+  t.bwd_var = bwd_variant();
   for (int i = 0; i < ncells; ++i) {
     CellDesc& d = cells[i];
     plan_cell_tiles(d);
@@ -572,7 +574,7 @@ int launch_forward(const Cells& c, const PlanTotals& t, const FaceRec* recs,
   if (t.fwd_items > 0 && t.nband > 0) {
     profile_begin(0, st);
     const unsigned g = (unsigned)t.fwd_items;
-    switch (fwd_variant()) {
+    switch (t.fwd_var) {  // the variant the tiles were planned for
       case 1: k_meshft_fwd<2, 128, kFwdTF, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
       case 2: k_meshft_fwd<4, 256, kFwdTF, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
       case 3: k_meshft_fwd<8, 64, kFwdTF, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, band_index, nullptr, fpart, err); break;
@@ -621,7 +623,7 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
     cudaMemsetAsync(bpart, 0, sizeof(float) * (size_t)std::max<int64_t>(t.bpart, 1), st);
     profile_begin(1, st);
     const unsigned g = (unsigned)t.bwd_items;
-    switch (bwd_variant()) {
+    switch (t.bwd_var) {  // the variant the tiles were planned for
       case 1: k_meshft_bwd<1, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 2: k_meshft_bwd<2, 64, kBwdTX, kStages><<<g, 64, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 3: k_meshft_bwd<1, 256, kBwdTX, kStages><<<g, 256, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;

@@ -33,6 +33,7 @@ void set_variants(int fwd, int bwd);
 // Totals of a batched plan (sums over cells).
 struct PlanTotals {
   int64_t nv, nt, nband, fpart, bpart, face_blks, band_blks, fwd_items, bwd_items;
+  int32_t fwd_var = 0, bwd_var = 0;  // the tile variants the plan was made for
 };
 
 int num_sms();
