@@ -479,18 +479,21 @@ def run_reference_volume(args):
                 "d2h_bytes_per_step": 0}}), flush=True)
 
 
-def _event_ms(fn, steps, warmup):
-    """Device time per call of ``fn`` (CUDA events, after ``warmup`` calls)."""
+def _event_ms(fn, steps, warmup, nvtx="timed"):
+    """Device time per call of ``fn`` (CUDA events, after ``warmup`` calls), the
+    timed calls inside an NVTX range named ``nvtx``."""
     import torch
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push(nvtx)
     e0.record()
     for _ in range(steps):
         fn()
     e1.record()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     return e0.elapsed_time(e1) / steps
 
 
@@ -1059,7 +1062,7 @@ def run_conv(args, rank, world, local):
             hg.copy_(p.grad, non_blocking=True)
             p.grad = None
 
-    e2e_ms = max_over_ranks(_event_ms(e2e_step, args.steps, max(args.warmup, 3)), dev)
+    e2e_ms = max_over_ranks(_event_ms(e2e_step, args.steps, max(args.warmup, 3), "e2e"), dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
@@ -1225,8 +1228,9 @@ def run_ours(args, rank, world, local):
                                    "2 (4,256) 3 (8,64) 4 (4,128) 5 (2,256); adjoint "
                                    "(faces/thread, threads): 0 (2,128) 1 (1,128) 2 (2,64) "
                                    "3 (1,256) 4 (2,128) 5 (1,128) 6 (2,128; >=5 CTAs/SM) "
-                                   "7 (2,128; >=6 CTAs/SM) 8 (1,128; >=8 CTAs/SM); 2 per "
-                                   "thread = paired FP32"},
+                                   "7 (2,128; >=6 CTAs/SM) 8 (1,128; >=8 CTAs/SM) 9, 10 "
+                                   "(2,128; two frequencies per iteration); 2 per thread = "
+                                   "paired FP32"},
         "loss_last_step": loss_end})
     out = {
         "metric": METRIC if args.workload == "fit200" else METRIC_BATCH,
