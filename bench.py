@@ -1228,9 +1228,8 @@ def run_ours(args, rank, world, local):
                                    "2 (4,256) 3 (8,64) 4 (4,128) 5 (2,256); adjoint "
                                    "(faces/thread, threads): 0 (2,128) 1 (1,128) 2 (2,64) "
                                    "3 (1,256) 4 (2,128) 5 (1,128) 6 (2,128; >=5 CTAs/SM) "
-                                   "7 (2,128; >=6 CTAs/SM) 8 (1,128; >=8 CTAs/SM) 9, 10 "
-                                   "(2,128; two frequencies per iteration); 2 per thread = "
-                                   "paired FP32"},
+                                   "7 (2,128; >=6 CTAs/SM) 8 (1,128; >=8 CTAs/SM); 2 per "
+                                   "thread = paired FP32"},
         "loss_last_step": loss_end})
     out = {
         "metric": METRIC if args.workload == "fit200" else METRIC_BATCH,

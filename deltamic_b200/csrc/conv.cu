@@ -35,7 +35,15 @@ struct ConvShape {
   int Do, Ho, Wo, Co;      // output
   int K, Kp;               // 27*Ci and its padding to kBK
   int64_t M;               // B*Do*Ho*Wo
+  int ci_sh, co_sh;        // log2 of Ci / Co when a power of two, else -1
 };
+
+// x / n and x % n for the channel counts: shifts when n is a power of two (the
+// loaders' index decomposition runs per gathered element).
+__device__ __forceinline__ int ch_div(int x, int n, int sh) { return sh >= 0 ? x >> sh : x / n; }
+__device__ __forceinline__ int64_t ch_div(int64_t x, int n, int sh) {
+  return sh >= 0 ? x >> sh : x / n;
+}
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -69,8 +77,9 @@ __device__ __forceinline__ int64_t tap_offset(const ConvShape& s, int64_t m, int
 __device__ __forceinline__ bf16 im2col(const bf16* __restrict__ x, const ConvShape& s, int64_t m,
                                        int k) {
   if (k >= s.K) return __float2bfloat16(0.f);
-  const int64_t o = tap_offset(s, m, k / s.Ci);
-  return o < 0 ? __float2bfloat16(0.f) : x[o + k % s.Ci];
+  const int64_t tap = ch_div(k, s.Ci, s.ci_sh);
+  const int64_t o = tap_offset(s, m, tap);
+  return o < 0 ? __float2bfloat16(0.f) : x[o + k - tap * s.Ci];
 }
 
 __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
@@ -334,7 +343,7 @@ struct FwdA {
     const int k = (int)k64;
     if (k >= s.K) return true;
     if (vec) {  // one tap, eight channels
-      const int tap = k / s.Ci, ci = k - tap * s.Ci;
+      const int tap = ch_div(k, s.Ci, s.ci_sh), ci = k - tap * s.Ci;
       const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
       const int d = ri.y + kd, h = ri.z + kh, w = ri.w + kw;
       if (d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
@@ -342,7 +351,7 @@ struct FwdA {
       return true;
     }
     // Ci < 8: the chunk runs across taps; (ci, kw, kh, kd) decomposed once, then stepped
-    const int tap = k / s.Ci;
+    const int tap = ch_div(k, s.Ci, s.ci_sh);
     int ci = k - tap * s.Ci, kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
     const bf16 z = __float2bfloat16(0.f);
     bf16 e[8];
@@ -467,7 +476,7 @@ struct WgradA {  // A^T[k, m]; row Kp is all ones, so its product row is db
   __device__ int4 row_info(int64_t k64, int64_t) const {
     const int k = (int)k64;
     if (k >= s.K) return make_int4(0, 0, 0, 0);
-    const int tap = k / s.Ci;
+    const int tap = ch_div(k, s.Ci, s.ci_sh);
     return make_int4(k - tap * s.Ci, tap / 9, (tap / 3) % 3, tap % 3);
   }
   // eight consecutive output voxels m.. at one (tap, ci): decomposed once, then stepped
@@ -628,7 +637,9 @@ __device__ __forceinline__ Cls pick_cls(const ClsSet& set, int z) {
 }
 
 __device__ __forceinline__ void cls_tap(const Cls& c, int t, int kk[3]) {
-  const int tw = t % c.nt[2], th = (t / c.nt[2]) % c.nt[1], td = t / (c.nt[2] * c.nt[1]);
+  // taps per axis are 1 or 2: shifts and masks
+  const int s2 = c.nt[2] - 1, s1 = c.nt[1] - 1;
+  const int tw = t & s2, th = (t >> s2) & s1, td = t >> (s2 + s1);
   const int tt[3] = {td, th, tw};
 #pragma unroll
   for (int a = 0; a < 3; ++a) kk[a] = c.p[a] == 0 ? 1 : (tt[a] == 0 ? 0 : 2);
@@ -670,10 +681,10 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
     return ((((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow) * s.Co;
   }
   __device__ bf16 operator()(int64_t q, int64_t r) const {
-    const int t = (int)(r / s.Co);
+    const int t = (int)ch_div(r, s.Co, s.co_sh);
     if (t >= c.T) return __float2bfloat16(0.f);
     const int64_t o = offset(q, t);
-    return o < 0 ? __float2bfloat16(0.f) : dp[o + r % s.Co];
+    return o < 0 ? __float2bfloat16(0.f) : dp[o + r - (int64_t)t * s.Co];
   }
   // Row info of class row q: its input voxel (b, d, h, w).
   __device__ int4 row_info(int64_t q, int64_t rows) const {
@@ -685,7 +696,7 @@ struct DgradA {  // A[q, (tap, co)] = dP at the output voxel reached through the
   __device__ bool load8(int64_t, int64_t r64, const int4& ri, uint4& v) const {
     if (!vec) return false;
     v = make_uint4(0u, 0u, 0u, 0u);
-    const int r = (int)r64, t = r / s.Co;
+    const int r = (int)r64, t = ch_div(r, s.Co, s.co_sh);
     if (t >= c.T) return true;
     int kk[3];
     cls_tap(c, t, kk);
@@ -718,16 +729,16 @@ struct DgradB {  // B[(tap, co), ci] = W[(k(tap), ci), co]
     return ((int64_t)tap * s.Ci + ci) * s.Co;
   }
   __device__ bf16 operator()(int64_t r, int ci) const {
-    const int t = (int)(r / s.Co);
+    const int t = (int)ch_div(r, s.Co, s.co_sh);
     if (t >= c.T || ci >= s.Ci) return __float2bfloat16(0.f);
-    return w[offset(t, ci) + r % s.Co];
+    return w[offset(t, ci) + r - (int64_t)t * s.Co];
   }
   __device__ bool load8(int64_t r, int ci, uint4& v) const {
     if (!vec) return false;
     v = make_uint4(0u, 0u, 0u, 0u);
-    const int t = (int)(r / s.Co);
+    const int t = (int)ch_div(r, s.Co, s.co_sh);
     if (t >= c.T || ci >= s.Ci) return true;
-    v = *(const uint4*)(w + offset(t, ci) + r % s.Co);
+    v = *(const uint4*)(w + offset(t, ci) + r - (int64_t)t * s.Co);
     return true;
   }
   __device__ bool fill(bf16*, int, int64_t, int64_t) const { return false; }
@@ -1048,6 +1059,9 @@ bool conv_shape(int B, int D, int H, int W, int Ci, int Co, ConvShape& s) {
   s.K = 27 * Ci;
   s.Kp = (s.K + kBK - 1) / kBK * kBK;
   s.M = (int64_t)B * s.Do * s.Ho * s.Wo;
+  auto lg = [](int n) { return (n & (n - 1)) == 0 ? __builtin_ctz((unsigned)n) : -1; };
+  s.ci_sh = lg(Ci);
+  s.co_sh = lg(Co);
   return true;
 }
 

@@ -632,8 +632,6 @@ int launch_backward(const Cells& c, const PlanTotals& t, const float* verts, con
       case 6: k_meshft_bwd<2, 128, kBwdTX, kStages, false, XiRec, 5><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 7: k_meshft_bwd<2, 128, kBwdTX, kStages, false, XiRec, 6><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       case 8: k_meshft_bwd<1, 128, kBwdTX, kStages, false, XiRec, 8><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
-      case 9:
-      case 10: k_meshft_bwd<2, 128, kBwdTX, kStages, false, XiRec, 0, 2><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
       default: k_meshft_bwd<2, 128, kBwdTX, kStages><<<g, 128, 0, st>>>(c, recs, nullptr, xrec, nullptr, order, bpart, err); break;
     }
     profile_end(1, st);

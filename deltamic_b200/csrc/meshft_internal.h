@@ -17,17 +17,15 @@ struct FwdVariant {
 struct BwdVariant {
   int F, NT, waves;
   int minb = 0;  // CTAs per SM the register allocation must allow (0: no cap)
-  int ju = 1;    // frequencies per inner iteration (2: two per packed chain pair)
 };
 constexpr int kFwdTF = 64, kBwdTX = 128, kStages = 3;
 constexpr int kNumFwdVariants = 6;
-constexpr int kNumBwdVariants = 11;
+constexpr int kNumBwdVariants = 9;
 constexpr FwdVariant kFwdVariants[kNumFwdVariants] = {
     {4, 128, 8}, {2, 128, 8}, {4, 256, 8}, {8, 64, 8}, {4, 128, 16}, {2, 256, 16}};
 constexpr BwdVariant kBwdVariants[kNumBwdVariants] = {
     {2, 128, 8},    {1, 128, 8},    {2, 64, 8},     {1, 256, 8},   {2, 128, 16},
-    {1, 128, 16},   {2, 128, 8, 5}, {2, 128, 16, 6}, {1, 128, 16, 8}, {2, 128, 8, 0, 2},
-    {2, 128, 16, 0, 2}};
+    {1, 128, 16},   {2, 128, 8, 5}, {2, 128, 16, 6}, {1, 128, 16, 8}};
 int fwd_variant();
 int bwd_variant();
 void set_variants(int fwd, int bwd);

@@ -393,9 +393,7 @@ __device__ __forceinline__ void load_xi(const XiRecOff& r, XiValOff& xv, float& 
 }
 
 // MINB > 0 caps the registers for MINB CTAs per SM; 0 leaves the choice to ptxas.
-// JU = 2 (two faces per thread only): two frequencies per inner iteration.
-template <int F, int NT, int TX, int NS, bool kVol = false, class XR = XiRec, int MINB = 0,
-          int JU = 1>
+template <int F, int NT, int TX, int NS, bool kVol = false, class XR = XiRec, int MINB = 0>
 __global__ void __launch_bounds__(NT, MINB) k_meshft_bwd(Cells cells, const FaceRec* __restrict__ recs,
                                                   const float4* __restrict__ fw,
                                                   const XR* __restrict__ xrec,
@@ -517,41 +515,7 @@ __global__ void __launch_bounds__(NT, MINB) k_meshft_bwd(Cells cells, const Face
           a9 += r;
         }
       };
-      int j = 0;
-      if constexpr (JU == 2) {
-        // two frequencies per iteration: two independent packed chains
-        for (; j + 1 < nxt; j += 2) {
-          XV xa, xb;
-          float gra, gia, grb, gib;
-          load_xi(sx[s][j], xa, gra, gia);
-          load_xi(sx[s][j + 1], xb, grb, gib);
-          const v2 ma0 = B2(xa.mf[0]), ma1 = B2(xa.mf[1]), ma2 = B2(xa.mf[2]);
-          const v2 mb0 = B2(xb.mf[0]), mb1 = B2(xb.mf[1]), mb2 = B2(xb.mf[2]);
-          const v2 haba = fma2(ma0, hab2[0], fma2(ma1, hab2[1], mul2(ma2, hab2[2])));
-          const v2 hbca = fma2(ma0, hbc2[0], fma2(ma1, hbc2[1], mul2(ma2, hbc2[2])));
-          const v2 hcaa = neg2(add2(haba, hbca));
-          const v2 habb = fma2(mb0, hab2[0], fma2(mb1, hab2[1], mul2(mb2, hab2[2])));
-          const v2 hbcb = fma2(mb0, hbc2[0], fma2(mb1, hbc2[1], mul2(mb2, hbc2[2])));
-          const v2 hcab = neg2(add2(habb, hbcb));
-          if (series_pair2(haba, hbca, hcaa) && series_pair2(habb, hbcb, hcab)) {
-            v2 za[3], ra, zb[3], rb;
-            // one warp-uniform set for both frequencies (each vote over the same lanes)
-            if (series_short2(haba, hbca, hcaa) && series_short2(habb, hbcb, hcab)) {
-              adjoint_series2<true>(xa, geom[0].Ua, geom[1].Ua, haba, hcaa, gra, gia, za, ra);
-              adjoint_series2<true>(xb, geom[0].Ua, geom[1].Ua, habb, hcab, grb, gib, zb, rb);
-            } else {
-              adjoint_series2<false>(xa, geom[0].Ua, geom[1].Ua, haba, hcaa, gra, gia, za, ra);
-              adjoint_series2<false>(xb, geom[0].Ua, geom[1].Ua, habb, hcab, grb, gib, zb, rb);
-            }
-            accum2(za, ra, ma0, ma1, ma2);
-            accum2(zb, rb, mb0, mb1, mb2);
-          } else {
-            one(j);
-            one(j + 1);
-          }
-        }
-      }
-      for (; j < nxt; ++j) one(j);
+      for (int j = 0; j < nxt; ++j) one(j);
 #pragma unroll
       for (int i = 0; i < 10; ++i) {
         tacc[0].q[i] = q2[i].x;
