@@ -845,10 +845,12 @@ def setup_batch64(args, rank, dev):
     target = torch.empty_like(img)
     for i in range(ncells):
         br.cell_view(target, i).copy_(noisy_target(br.cell_view(img, i), gen, 0, dev))
-    V = torch.tensor(np.concatenate(inits), dtype=torch.float32, device=dev)
+    # every timed step works on one mesh state, the cells' ground-truth shapes the
+    # fits converge to (restored before every step, as in fit200)
+    V = torch.tensor(np.concatenate(gts), dtype=torch.float32, device=dev)
 
     def make_step(graph):
-        return BatchFitStep(br, V.clone(), C, target, "mse", 0.0, LR, graph=graph)
+        return BatchFitStep(br, V.clone(), C, target, "mse", 0.0, LR, graph=graph, restore=V)
 
     def e2e_call(Vd):
         loss = br.loss(Vd, C, "mse", target)
@@ -860,8 +862,10 @@ def setup_batch64(args, rank, dev):
             "n_cells": ncells, "n_verts": int(V.shape[0]), "n_faces": int(sum(br.nt)),
             "render": ("band-box DFTs of all cells, one launch per stage" if br.use_bandbox
                        else "batched cuFFT per grid shape + batched image-loss kernels"),
-            "n_band": int(br.band.numel()), "eval_pairs_per_step": int(br.eval_pairs)}
-    return make_step, e2e_call, np.concatenate(inits), br.pairs, info, None
+            "n_band": int(br.band.numel()), "eval_pairs_per_step": int(br.eval_pairs),
+            "mesh_state": "the cells' ground-truth SH shapes, restored before every step "
+                          "(the same vertices in the step and e2e)"}
+    return make_step, e2e_call, np.concatenate(gts), br.pairs, info, None
 
 
 def run_fit300(args, rank, world, local):

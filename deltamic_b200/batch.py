@@ -334,10 +334,17 @@ class _BatchLoss(torch.autograd.Function):
 
 
 class BatchFitStep:
-    """One Adam step on all cells' vertices (concatenated), replayed as a CUDA graph."""
+    """One Adam step on all cells' vertices (concatenated), replayed as a CUDA graph.
+
+    ``restore`` (optional, like ``fit.FitStep``'s): copied into the vertices at the
+    start of every step, so every step works on the same mesh state."""
 
     def __init__(self, r: BatchRenderer, verts, coeff, target, kind="mse", contrast=0.0,
-                 lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True):
+                 lr=1e-3, betas=(0.9, 0.999), eps=1e-8, graph=True, restore=None):
+        if restore is not None and (restore.shape != verts.shape or restore.dtype != verts.dtype
+                                    or restore.device != verts.device):
+            raise ValueError("restore must match verts in shape, dtype and device")
+        self.restore = restore
         self.r, self.V, self.C, self.target = r, verts, coeff.contiguous(), target
         self.kind, self.contrast = kind, float(contrast)
         self.lr, self.betas, self.eps = float(lr), betas, float(eps)
@@ -355,6 +362,8 @@ class BatchFitStep:
 
     def _body(self):
         r = self.r
+        if self.restore is not None:
+            self.V.copy_(self.restore)
         if r.use_bandbox:
             ft = r.forward_spectrum(self.V, self.C, dense=False)
             losses, G, _ = r.render_loss_bandbox(ft, self.kind, self.target, self.contrast)
