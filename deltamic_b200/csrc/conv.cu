@@ -879,29 +879,40 @@ __device__ __forceinline__ int64_t c1_tiles(const ConvShape& s) {
 // = 3 and 9 (mod 32) banks, 27 distinct banks across the lanes of a weight-gradient
 // warp (one tap per lane).
 constexpr int kC1RS = 67, kC1PS = 1161, kC1XS = 3 * kC1PS;
-constexpr int kC1Load = (3 * kC1IH * kC1IW + 255) / 256;  // footprint loads per thread
 
 __device__ __forceinline__ int c1_col(int kw) { return kw == 0 ? 0 : (kw == 1 ? 34 : 1); }
 
 __device__ __forceinline__ void c1_load(const bf16* __restrict__ x, const ConvShape& s,
                                         const C1Tile& tl, float* xs) {
-  bf16 v[kC1Load];
-  // all loads first (independent), then the shared-memory stores
-#pragma unroll
-  for (int u = 0; u < kC1Load; ++u) {
-    const int i = threadIdx.x + 256 * u;
-    const int c = i % kC1IW, r = (i / kC1IW) % kC1IH, pz = i / (kC1IW * kC1IH);
-    const int d = 2 * tl.od - 1 + pz, h = 2 * tl.oh0 - 1 + r, w = 2 * tl.ow0 - 1 + c;
-    v[u] = __float2bfloat16(0.f);
-    if (i < 3 * kC1IH * kC1IW && d >= 0 && d < s.D && h >= 0 && h < s.H && w >= 0 && w < s.W)
-      v[u] = x[(((int64_t)tl.b * s.D + d) * s.H + h) * s.W + w];
-  }
-#pragma unroll
-  for (int u = 0; u < kC1Load; ++u) {
-    const int i = threadIdx.x + 256 * u;
-    if (i >= 3 * kC1IH * kC1IW) continue;
-    const int c = i % kC1IW, r = (i / kC1IW) % kC1IH, pz = i / (kC1IW * kC1IH);
-    xs[pz * kC1PS + r * kC1RS + ((c & 1) ? 34 + (c >> 1) : (c >> 1))] = __bfloat162float(v[u]);
+  // warp w takes footprint rows w, w + 8, ...; lane l the columns 2l + 1, 2l + 2 (one
+  // aligned pair of input columns, w = 2 ow0 + 2l) and lane 0 also column 0
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kRows = 3 * kC1IH;
+  for (int row = warp; row < kRows; row += 8) {
+    const int pz = row / kC1IH, r = row - pz * kC1IH;
+    const int d = 2 * tl.od - 1 + pz, h = 2 * tl.oh0 - 1 + r;
+    float* xr = xs + pz * kC1PS + r * kC1RS;
+    const bool in_dh = d >= 0 && d < s.D && h >= 0 && h < s.H;
+    const bf16* src = x + (((int64_t)tl.b * s.D + (in_dh ? d : 0)) * s.H + (in_dh ? h : 0)) * s.W;
+    const int w0 = 2 * tl.ow0 + 2 * lane;  // columns 2l + 1 and 2l + 2 of the footprint
+    float odd = 0.f, even = 0.f;
+    if (in_dh) {
+      // one 4-byte load when the pair is 4-byte aligned (even rows, aligned base)
+      if (w0 + 1 < s.W && (s.W & 1) == 0 && ((uintptr_t)x & 3) == 0) {
+        const uint32_t u = *reinterpret_cast<const uint32_t*>(src + w0);
+        odd = __uint_as_float(u << 16);
+        even = __uint_as_float(u & 0xffff0000u);
+      } else {
+        if (w0 < s.W) odd = __bfloat162float(src[w0]);
+        if (w0 + 1 < s.W) even = __bfloat162float(src[w0 + 1]);
+      }
+    }
+    xr[34 + lane] = odd;       // footprint column 2l + 1
+    xr[lane + 1] = even;       // footprint column 2l + 2
+    if (lane == 0) {           // footprint column 0: input column 2 ow0 - 1
+      const int wl = 2 * tl.ow0 - 1;
+      xr[0] = (in_dh && wl >= 0) ? __bfloat162float(src[wl]) : 0.f;
+    }
   }
 }
 
@@ -924,9 +935,10 @@ __global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, C
   const int ty = threadIdx.x / kC1TW, tx = threadIdx.x % kC1TW;
   const int oh = tl.oh0 + ty, ow = tl.ow0 + tx;
   if (oh >= s.Ho || ow >= s.Wo) return;
-  float acc[CO];
+  // channel pairs on the paired FP32 path (two FMAs per instruction)
+  float2 acc2[CO / 2];
 #pragma unroll
-  for (int c = 0; c < CO; ++c) acc[c] = bs[c];
+  for (int c = 0; c < CO / 2; ++c) acc2[c] = make_float2(bs[2 * c], bs[2 * c + 1]);
 #pragma unroll
   for (int kd = 0; kd < 3; ++kd)
 #pragma unroll
@@ -934,10 +946,22 @@ __global__ void __launch_bounds__(256) k_conv1_fwd(const bf16* __restrict__ x, C
 #pragma unroll
       for (int kw = 0; kw < 3; ++kw) {
         const float xv = xs[kd * kC1PS + (2 * ty + kh) * kC1RS + c1_col(kw) + tx];
+        const float2 x2 = make_float2(xv, xv);
         const int tap = (kd * 3 + kh) * 3 + kw;
+        const float4* w4 = reinterpret_cast<const float4*>(&ws[tap][0]);
 #pragma unroll
-        for (int c = 0; c < CO; ++c) acc[c] = fmaf(xv, ws[tap][c], acc[c]);
+        for (int q = 0; q < CO / 4; ++q) {
+          const float4 wv = w4[q];
+          acc2[2 * q] = __ffma2_rn(x2, make_float2(wv.x, wv.y), acc2[2 * q]);
+          acc2[2 * q + 1] = __ffma2_rn(x2, make_float2(wv.z, wv.w), acc2[2 * q + 1]);
+        }
       }
+  float acc[CO];
+#pragma unroll
+  for (int c = 0; c < CO / 2; ++c) {
+    acc[2 * c] = acc2[c].x;
+    acc[2 * c + 1] = acc2[c].y;
+  }
   const int64_t m = (((int64_t)tl.b * s.Do + tl.od) * s.Ho + oh) * s.Wo + ow;
   float4* pp = reinterpret_cast<float4*>(pre + m * CO);
   uint4* ap = reinterpret_cast<uint4*>(act + m * CO);
@@ -977,9 +1001,9 @@ __global__ void __launch_bounds__(256) k_conv1_wgrad(const bf16* __restrict__ x,
   const int tap = min(lane, 27);
   const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
   const int xoff = kd * kC1PS + kh * kC1RS + c1_col(kw);
-  float acc[CO];
+  float2 acc2[CO / 2];  // channel pairs on the paired FP32 path
 #pragma unroll
-  for (int c = 0; c < CO; ++c) acc[c] = 0.f;
+  for (int c = 0; c < CO / 2; ++c) acc2[c] = make_float2(0.f, 0.f);
   const int64_t ntl = c1_tiles(s);
   for (int64_t t = blockIdx.x; t < ntl; t += gridDim.x) {
     const C1Tile tl = c1_tile(s, t);
@@ -1012,16 +1036,21 @@ __global__ void __launch_bounds__(256) k_conv1_wgrad(const bf16* __restrict__ x,
     for (int v = warp; v < NV; v += 8) {
       const int ty = v / kC1TW, tx = v % kC1TW;
       const float xv = lane < 27 ? xs[xoff + 2 * ty * kC1RS + tx] : (lane == 27 ? 1.f : 0.f);
+      const float2 x2 = make_float2(xv, xv);
       const float4* d4 = reinterpret_cast<const float4*>(ds + v * CO);
 #pragma unroll
       for (int q = 0; q < CO / 4; ++q) {
         const float4 g = d4[q];
-        acc[4 * q] = fmaf(xv, g.x, acc[4 * q]);
-        acc[4 * q + 1] = fmaf(xv, g.y, acc[4 * q + 1]);
-        acc[4 * q + 2] = fmaf(xv, g.z, acc[4 * q + 2]);
-        acc[4 * q + 3] = fmaf(xv, g.w, acc[4 * q + 3]);
+        acc2[2 * q] = __ffma2_rn(x2, make_float2(g.x, g.y), acc2[2 * q]);
+        acc2[2 * q + 1] = __ffma2_rn(x2, make_float2(g.z, g.w), acc2[2 * q + 1]);
       }
     }
+  }
+  float acc[CO];
+#pragma unroll
+  for (int c = 0; c < CO / 2; ++c) {
+    acc[2 * c] = acc2[c].x;
+    acc[2 * c + 1] = acc2[c].y;
   }
   __syncthreads();  // every warp is done with ds / xs
   if (lane < 28) {
