@@ -1015,16 +1015,18 @@ def run_conv(args, rank, world, local):
                  dw=torch.empty(_kp(ci), co, device=dev), db=torch.empty(co, device=dev))
         L["wsb"] = lib.dm_conv3d_s2_workspace_size(B, n, n, n, ci, co)
         L["ws"] = torch.empty(L["wsb"], dtype=torch.uint8, device=dev)
+        L["fwsb"] = lib.dm_conv3d_s2_forward_workspace_size(B, n, n, n, ci, co)
+        L["fws"] = torch.empty(L["fwsb"], dtype=torch.uint8, device=dev)
         flops += 2 * B * no ** 3 * 27 * ci * co * (3 if ci > 1 else 2)
         layers.append(L)
         x, n = L["act"], no
 
     def step():
         for L in layers:
-            N.check(lib.dm_conv3d_s2_forward(N.ptr(L["x"]), B, L["n"], L["n"], L["n"], L["ci"],
-                                             N.ptr(L["w"]), N.ptr(L["b"]), L["co"],
-                                             N.ptr(L["pre"]), N.ptr(L["act"]), st),
-                    "dm_conv3d_s2_forward")
+            N.check(lib.dm_conv3d_s2_forward_ws(N.ptr(L["x"]), B, L["n"], L["n"], L["n"],
+                                                L["ci"], N.ptr(L["w"]), N.ptr(L["b"]), L["co"],
+                                                N.ptr(L["pre"]), N.ptr(L["act"]), N.ptr(L["fws"]),
+                                                L["fwsb"], st), "dm_conv3d_s2_forward_ws")
         for L in reversed(layers):
             N.check(lib.dm_conv3d_s2_backward(N.ptr(L["x"]), B, L["n"], L["n"], L["n"], L["ci"],
                                               N.ptr(L["w"]), L["co"], N.ptr(L["pre"]),

@@ -166,6 +166,9 @@ SIGNATURES = {
     "dm_conv3d_s2_workspace_size": (_SZ, [_INT] * 6),
     "dm_conv3d_s2_forward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _P, _INT, _P, _P, _P]),
     "dm_conv3d_s2_device_error": (_INT, [ctypes.POINTER(_INT), _P]),
+    "dm_conv3d_s2_forward_workspace_size": (_SZ, [_INT] * 6),
+    "dm_conv3d_s2_forward_ws": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _P, _INT, _P, _P,
+                                       _P, _SZ, _P]),
     "dm_conv3d_s2_backward": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P, _P, _P,
                                      _P, _P, _SZ, _P]),
     "dm_conv3d_s2_backward_bf16": (_INT, [_P, _INT, _INT, _INT, _INT, _INT, _P, _INT, _P, _P,

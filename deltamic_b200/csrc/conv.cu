@@ -424,6 +424,56 @@ struct FwdEp {
   }
 };
 
+// Forward with the reduction split over blockIdx.y (few row tiles): each split
+// writes its FP32 partial product part[split][m][n]; k_fwd_reduce adds them in
+// split order and applies the bias and GELU.
+struct FwdSplitEp {
+  float* part;
+  int64_t stride;  // M * Co
+  int Co;
+  int col0;
+  __device__ FwdSplitEp at(int z, int bn) const {
+    FwdSplitEp e = *this;
+    e.col0 = z * bn;
+    return e;
+  }
+  __device__ void put16(int64_t m, int c, int split, const float (&v)[16]) const {
+    float* r = part + split * stride + m * Co + col0 + c;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      *(float4*)(r + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
+};
+
+__global__ void __launch_bounds__(256) k_fwd_reduce(const float* __restrict__ part, int splits,
+                                                    int64_t n, int Co,
+                                                    const float* __restrict__ bias,
+                                                    float* __restrict__ pre,
+                                                    bf16* __restrict__ act) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float4 v = reinterpret_cast<const float4*>(part)[i];
+    for (int k = 1; k < splits; ++k) {
+      const float4 q = reinterpret_cast<const float4*>(part + (int64_t)k * n)[i];
+      v.x += q.x;
+      v.y += q.y;
+      v.z += q.z;
+      v.w += q.w;
+    }
+    const int c = (int)((4 * i) % Co);
+    if (bias) {
+      v.x += bias[c];
+      v.y += bias[c + 1];
+      v.z += bias[c + 2];
+      v.w += bias[c + 3];
+    }
+    reinterpret_cast<float4*>(pre)[i] = v;
+    reinterpret_cast<uint2*>(act)[i] =
+        make_uint2(pack2(__float2bfloat16(gelu(v.x)), __float2bfloat16(gelu(v.y))),
+                   pack2(__float2bfloat16(gelu(v.z)), __float2bfloat16(gelu(v.w))));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // backward pieces
 
@@ -1121,8 +1171,42 @@ static int fwd_cols(const ConvShape& s) {
   return bn;
 }
 
+// Reduction splits of the forward: when the row tiles alone cannot fill the SMs
+// (two blocks per SM wanted), all Co columns per block and the reduction split so
+// the input is gathered once; at least four 32-element stages per split.
+static int fwd_splits(const ConvShape& s) {
+  if (conv1_direct(s)) return 1;
+  const int64_t tiles = (s.M + kBM - 1) / kBM;
+  if (tiles >= 148) return 1;
+  const int64_t stages = s.Kp / kBK;
+  int64_t sp = std::min<int64_t>((2 * 148 + tiles - 1) / tiles, stages / 4);
+  if (sp < 2) return 1;
+  const int64_t per = (stages + sp - 1) / sp;
+  return (int)((stages + per - 1) / per);
+}
+
+size_t conv_fwd_ws_bytes(const ConvShape& s) {
+  const int sp = fwd_splits(s);
+  return sp > 1 ? (size_t)sp * s.M * s.Co * sizeof(float) + 256 : 256;
+}
+
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
-                        float* pre, bf16* act, cudaStream_t st) {
+                        float* pre, bf16* act, cudaStream_t st, void* ws = nullptr,
+                        size_t ws_bytes = 0) {
+  const int sp = fwd_splits(s);
+  if (sp > 1 && ws && ws_bytes >= conv_fwd_ws_bytes(s) && aligned16(ws) && aligned16(pre) &&
+      aligned16(act) && s.Co % 16 == 0) {
+    const int64_t stages = s.Kp / kBK;
+    const int64_t per = (stages + sp - 1) / sp * kBK;
+    float* part = (float*)ws;
+    gemm_launch(s.Co, FwdA{x, s, s.Ci % 8 == 0 && aligned16(x)}, WeightB{w, s.Co, 0},
+                FwdSplitEp{part, s.M * s.Co, s.Co, 0}, s.M, s.Kp, per, sp, 1, st);
+    const int64_t n = s.M * s.Co;
+    k_fwd_reduce<<<(unsigned)std::min<int64_t>((n / 4 + 255) / 256, 148 * 16), 256, 0, st>>>(
+        part, sp, n, s.Co, bias, pre, act);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  }
   if (conv1_direct(s) && aligned16(pre) && aligned16(act)) {
     const unsigned g = (unsigned)conv1_tiles_host(s);
     if (s.Co == 16)
@@ -1236,6 +1320,23 @@ int dm_conv3d_s2_forward(const uint16_t* x, int B, int D, int H, int W, int Ci, 
   if (!x || !w || !pre || !act) return DM_ERR_INVALID_ARG;
   return dm::launch_conv_forward(s, (const dm::bf16*)x, (const dm::bf16*)w, bias, pre,
                                  (dm::bf16*)act, (cudaStream_t)stream);
+}
+
+size_t dm_conv3d_s2_forward_workspace_size(int B, int D, int H, int W, int Ci, int Co) {
+  dm::ConvShape s;
+  if (!dm::conv_shape(B, D, H, W, Ci, Co, s)) return 0;
+  return dm::conv_fwd_ws_bytes(s);
+}
+
+int dm_conv3d_s2_forward_ws(const uint16_t* x, int B, int D, int H, int W, int Ci,
+                            const uint16_t* w, const float* bias, int Co, float* pre,
+                            uint16_t* act, void* workspace, size_t ws_bytes, dm_stream_t stream) {
+  dm::ConvShape s;
+  if (!dm::conv_shape(B, D, H, W, Ci, Co, s)) return DM_ERR_INVALID_ARG;
+  if (!x || !w || !pre || !act || !workspace) return DM_ERR_INVALID_ARG;
+  if (ws_bytes < dm::conv_fwd_ws_bytes(s)) return DM_ERR_WORKSPACE;
+  return dm::launch_conv_forward(s, (const dm::bf16*)x, (const dm::bf16*)w, bias, pre,
+                                 (dm::bf16*)act, (cudaStream_t)stream, workspace, ws_bytes);
 }
 
 int dm_conv3d_s2_device_error(int* out_flags, dm_stream_t stream) {

@@ -46,9 +46,12 @@ class _ConvS2(torch.autograd.Function):
         Do, Ho, Wo = (D + 1) // 2, (H + 1) // 2, (W + 1) // 2
         pre = torch.empty(B, Do, Ho, Wo, Co, dtype=torch.float32, device=x.device)
         act = torch.empty(B, Do, Ho, Wo, Co, dtype=torch.bfloat16, device=x.device)
-        N.check(lib.dm_conv3d_s2_forward(N.ptr(x), B, D, H, W, Ci, N.ptr(wb), N.ptr(b32), Co,
-                                         N.ptr(pre), N.ptr(act), N.stream_ptr(x.device)),
-                "dm_conv3d_s2_forward")
+        ws = N.WORKSPACES.get(("conv_fwd", Ci, Co),
+                              lib.dm_conv3d_s2_forward_workspace_size(B, D, H, W, Ci, Co),
+                              x.device)
+        N.check(lib.dm_conv3d_s2_forward_ws(N.ptr(x), B, D, H, W, Ci, N.ptr(wb), N.ptr(b32), Co,
+                                            N.ptr(pre), N.ptr(act), N.ptr(ws), ws.numel(),
+                                            N.stream_ptr(x.device)), "dm_conv3d_s2_forward_ws")
         ctx.save_for_backward(x, wb, pre)
         return act
 

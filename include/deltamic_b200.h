@@ -566,6 +566,13 @@ size_t dm_conv3d_s2_workspace_size(int B, int D, int H, int W, int Ci, int Co);
 int dm_conv3d_s2_forward(const uint16_t* x, int B, int D, int H, int W, int Ci, const uint16_t* w,
                          const float* bias, int Co, float* pre, uint16_t* act,
                          dm_stream_t stream);
+/* The forward with a workspace (its size from the query): when the row tiles alone
+ * would leave SMs idle (small layers), the reduction is split across blocks and the
+ * FP32 partials are added in split order before the bias and GELU (deterministic). */
+size_t dm_conv3d_s2_forward_workspace_size(int B, int D, int H, int W, int Ci, int Co);
+int dm_conv3d_s2_forward_ws(const uint16_t* x, int B, int D, int H, int W, int Ci,
+                            const uint16_t* w, const float* bias, int Co, float* pre,
+                            uint16_t* act, void* workspace, size_t ws_bytes, dm_stream_t stream);
 int dm_conv3d_s2_device_error(int* out_flags, dm_stream_t stream);
 int dm_conv3d_s2_backward(const uint16_t* x, int B, int D, int H, int W, int Ci,
                           const uint16_t* w, int Co, const float* pre, const float* dact,
