@@ -1438,6 +1438,10 @@ static int bbb_shapes(const dm_cell* cells, const int32_t* bounds, int ncells,
       ext[d] = bounds[6 * i + 3 + d] - bounds[6 * i + d] + 1;
     }
     if (!make_shape(cells[i].box.shape, lo, ext, shapes[i])) return DM_ERR_UNSUPPORTED;
+    // the batch's (cell x position) entries already fill the GPU: the axis-1 forward
+    // contraction runs over all positions in one block instead of K splits
+    shapes[i].q1split = 1;
+    shapes[i].q1chunk = (shapes[i].n[1] + 15) / 16 * 16;
     tot += bb_layout(shapes[i], nullptr, nullptr);
   }
   *ws_total = tot;
