@@ -20,6 +20,7 @@
 
 #include "../../include/deltamic_b200.h"
 #include "band_internal.h"
+#include "meshft_internal.h"
 #include "tcgen05.cuh"
 
 namespace dm {
@@ -843,6 +844,12 @@ struct DgradEp {
   }
 };
 
+}  // namespace dm
+
+#include "conv_fp.cuh"
+
+namespace dm {
+
 // ---------------------------------------------------------------------------
 // launchers
 
@@ -1190,9 +1197,132 @@ size_t conv_fwd_ws_bytes(const ConvShape& s) {
   return sp > 1 ? (size_t)sp * s.M * s.Co * sizeof(float) + 256 : 256;
 }
 
+// Footprint kernels (conv_fp.cuh): the layer shapes they are instantiated for.
+static bool fp_layer(const ConvShape& s) {
+  return (s.Ci == 16 && s.Co == 32) || (s.Ci == 32 && s.Co == 64);
+}
+
+// Raises a footprint kernel's dynamic shared-memory limit to its size, once per
+// device (a host-side attribute: the first call on a device should come before any
+// stream capture).
+template <typename Kern>
+static cudaError_t fp_smem_once(Kern k, int bytes, std::atomic<bool>* done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kConvMaxDevices && done[dev].load()) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && dev >= 0 && dev < kConvMaxDevices) done[dev].store(true);
+  return e;
+}
+
+// Persistent grid of a footprint kernel: as many blocks as the SMs hold at once
+// (shared memory bound), never more than the tiles.
+static unsigned fp_grid(int64_t tiles, int smem) {
+  const int per_sm = std::max(1, 232448 / (smem + 1024));
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)num_sms() * per_sm));
+}
+
+template <int CI, int CO, int HR>
+static cudaError_t fp_fwd_launch(const ConvShape& s, const bf16* x, const bf16* w, FwdEp ep,
+                                 cudaStream_t st) {
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_fp_fwd<CI, CO, HR>;
+  const int smem = FpFwd<CI, CO, HR>::kSmem;
+  cudaError_t e = fp_smem_once(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(x, s, w, ep, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// Forward on the footprint kernels: (Ci, Co) = (16, 32) at any size, (32, 64) with
+// at most 8 output rows (the 33-row footprint of a 64-channel weight image would not
+// fit in shared memory); 16-byte aligned tensors.  Returns false when not taken.
+static bool fp_forward(const ConvShape& s, const bf16* x, const bf16* w, const FwdEp& ep,
+                       cudaStream_t st, int& rc) {
+  if (!fp_layer(s) || !ep.vec || !aligned16(x) || !aligned16(w)) return false;
+  cudaError_t e;
+  if (s.Ci == 16)
+    e = s.Ho > 8 ? fp_fwd_launch<16, 32, 33>(s, x, w, ep, st)
+                 : fp_fwd_launch<16, 32, 17>(s, x, w, ep, st);
+  else if (s.Ho <= 8)
+    e = fp_fwd_launch<32, 64, 17>(s, x, w, ep, st);
+  else
+    return false;
+  rc = e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  return true;
+}
+
+template <int CI, int CO>
+static cudaError_t fp_dgrad_launch(const ConvShape& s, const bf16* dp, const bf16* w, float* dx,
+                                   bf16* dxb, cudaStream_t st) {
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_fp_dgrad<CI, CO>;
+  const int smem = FpDgrad<CI, CO>::kSmem;
+  cudaError_t e = fp_smem_once(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const int nd = (s.D + 1) / 2, nh = (s.H + 1) / 2, nw = (s.W + 1) / 2;
+  const int64_t tiles = (int64_t)s.B * nd * ((nh + 15) / 16) * ((nw + 7) / 8);
+  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(dp, s, w, dx, dxb, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// Data gradient on the footprint kernel (all eight parity classes per tile).
+static bool fp_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* dx, bf16* dxb,
+                     cudaStream_t st, int& rc) {
+  if (!fp_layer(s) || !aligned16(dp) || !aligned16(w) || !aligned16(dxb ? (void*)dxb : (void*)dx))
+    return false;
+  const cudaError_t e = s.Ci == 16 ? fp_dgrad_launch<16, 32>(s, dp, w, dx, dxb, st)
+                                   : fp_dgrad_launch<32, 64>(s, dp, w, dx, dxb, st);
+  rc = e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  return true;
+}
+
+template <int CI, int CO>
+static cudaError_t fp_wgrad_launch(const ConvShape& s, const bf16* x, const bf16* dp, float* part,
+                                   int splits, int& used, cudaStream_t st) {
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_fp_wgrad<CI, CO>;
+  const int smem = FpWgrad<CI, CO>::kSmem;
+  cudaError_t e = fp_smem_once(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+  const int64_t per = (tiles + splits - 1) / splits;
+  used = (int)((tiles + per - 1) / per);
+  k<<<dim3((unsigned)used, 3), kFpThreads, smem, st>>>(x, s, dp, (int)per, part,
+                                                       conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// Weight + bias gradient partials on the footprint kernel: blocks (split, kd), at most
+// as many splits as the workspace holds, about one wave of blocks (three per SM for
+// Ci = 16, two for Ci = 32) and at least eight forward tiles per split.
+static bool fp_wgrad(const ConvShape& s, const bf16* x, const bf16* dp, float* part, int& used,
+                     cudaStream_t st, int& rc) {
+  if (!fp_layer(s) || !aligned16(x) || !aligned16(dp) || !aligned16(part)) return false;
+  const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+  const int64_t wave = (int64_t)148 * (s.Ci == 16 ? 3 : 2) / 3;
+  const int splits = (int)std::max<int64_t>(
+      1, std::min<int64_t>({wave, tiles / 8, (int64_t)wgrad_splits(s)}));
+  const cudaError_t e = s.Ci == 16 ? fp_wgrad_launch<16, 32>(s, x, dp, part, splits, used, st)
+                                   : fp_wgrad_launch<32, 64>(s, x, dp, part, splits, used, st);
+  rc = e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  return true;
+}
+
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st, void* ws = nullptr,
                         size_t ws_bytes = 0) {
+  {
+    int rc = DM_OK;
+    if (fp_forward(s, x, w, FwdEp{bias, pre, act, s.Co, 0, aligned16(pre) && aligned16(act)}, st,
+                   rc))
+      return rc;
+  }
   const int sp = fwd_splits(s);
   if (sp > 1 && ws && ws_bytes >= conv_fwd_ws_bytes(s) && aligned16(ws) && aligned16(pre) &&
       aligned16(act) && s.Co % 16 == 0) {
@@ -1256,6 +1386,8 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
     else
       k_conv1_wgrad<32><<<used, 256, 0, st>>>(x, s, dp, part);
     count_launches(1);
+  } else if (int rc = DM_OK; fp_wgrad(s, x, dp, part, used, st, rc)) {
+    if (rc != DM_OK) return rc;
   } else {
     const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
     used = (int)((s.M + per - 1) / per);
@@ -1270,6 +1402,8 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   count_launches(1);
   // data gradient: the eight parity classes of the input voxels in one launch
   if (dx || dx_b) {
+    int rc = DM_OK;
+    if (fp_dgrad(s, dp, w, dx, dx_b, st, rc)) return rc;
     ClsSet set;
     int64_t max_rows = 0, max_red = 0;
     const int dims[3] = {s.D, s.H, s.W};
