@@ -847,6 +847,7 @@ struct DgradEp {
 }  // namespace dm
 
 #include "conv_fp.cuh"
+#include "conv_s2d.cuh"
 
 namespace dm {
 
@@ -1314,9 +1315,57 @@ static bool fp_wgrad(const ConvShape& s, const bf16* x, const bf16* dp, float* p
   return true;
 }
 
+// Single-channel layer on the space-to-depth kernels (conv_s2d.cuh): W even (each
+// block's column pairs are 4-byte words), x 4-byte aligned, outputs 16-byte aligned.
+static bool s2d_layer(const ConvShape& s, const bf16* x) {
+  return conv1_direct(s) && (s.W & 1) == 0 && ((uintptr_t)x & 3u) == 0;
+}
+
+template <int CO>
+static cudaError_t s2d_fwd_launch(const ConvShape& s, const bf16* x, const bf16* w,
+                                  const float* bias, float* pre, bf16* act, cudaStream_t st) {
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_s2d_fwd<CO>;
+  const int smem = S2dFwd<CO>::kSmem;
+  cudaError_t e = fp_smem_once(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+  // one wave: the blocks of 256 threads the SMs' registers hold at once
+  cudaFuncAttributes fa;
+  int per_sm = 4;
+  if (cudaFuncGetAttributes(&fa, k) == cudaSuccess && fa.numRegs > 0)
+    per_sm = std::max(1, std::min(8, 65536 / (256 * ((fa.numRegs + 7) / 8 * 8))));
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)per_sm * num_sms()));
+  k<<<grid, 256, smem, st>>>(x, s, w, bias, pre, act, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+template <int CO>
+static cudaError_t s2d_wgrad_launch(const ConvShape& s, const bf16* x, const bf16* dp,
+                                    float* part, int splits, int& used, cudaStream_t st) {
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_s2d_wgrad<CO>;
+  const int smem = S2dWgrad<CO>::kSmem;
+  cudaError_t e = fp_smem_once(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+  const int64_t per = (tiles + splits - 1) / splits;
+  used = (int)((tiles + per - 1) / per);
+  k<<<(unsigned)used, 256, smem, st>>>(x, s, dp, (int)per, part, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st, void* ws = nullptr,
                         size_t ws_bytes = 0) {
+  if (s2d_layer(s, x) && s.W % 8 == 0 && aligned16(x) && aligned16(pre) && aligned16(act)) {
+    const cudaError_t e = s.Co == 16 ? s2d_fwd_launch<16>(s, x, w, bias, pre, act, st)
+                                     : s2d_fwd_launch<32>(s, x, w, bias, pre, act, st);
+    return e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+  }
   {
     int rc = DM_OK;
     if (fp_forward(s, x, w, FwdEp{bias, pre, act, s.Co, 0, aligned16(pre) && aligned16(act)}, st,
@@ -1379,7 +1428,15 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   // reduction over m split across blockIdx.y
   const int splits = wgrad_splits(s);
   int used;
-  if (conv1_direct(s)) {
+  if (s2d_layer(s, x) && aligned16(dp) && aligned16(part)) {
+    // one wave of blocks (three per SM), at least eight tiles per block
+    const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
+    const int sp = (int)std::max<int64_t>(
+        1, std::min<int64_t>({(int64_t)3 * num_sms(), tiles / 8, (int64_t)splits}));
+    const cudaError_t e = s.Co == 16 ? s2d_wgrad_launch<16>(s, x, dp, part, sp, used, st)
+                                     : s2d_wgrad_launch<32>(s, x, dp, part, sp, used, st);
+    if (e != cudaSuccess) return DM_ERR_CUDA;
+  } else if (conv1_direct(s)) {
     used = (int)std::max<int64_t>(1, std::min<int64_t>(splits, conv1_tiles_host(s)));
     if (s.Co == 16)
       k_conv1_wgrad<16><<<used, 256, 0, st>>>(x, s, dp, part);

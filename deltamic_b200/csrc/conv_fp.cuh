@@ -55,6 +55,17 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Waits for an MMA commit with only thread 0 sleeping on the barrier (every
+// thread polling it spends issue slots the other blocks on the SM need); after the
+// block barrier each other thread confirms the completed phase with one test.
+__device__ __forceinline__ bool mbar_wait_block(uint64_t* bar, uint32_t parity, int* err) {
+  int ok = 1;
+  if (threadIdx.x == 0) ok = mbar_wait_sleep_bounded(bar, parity, err) ? 1 : 0;
+  ok = __syncthreads_and(ok);
+  if (ok && threadIdx.x != 0) ok = mbar_wait_bounded(bar, parity, err) ? 1 : 0;
+  return __syncthreads_and(ok) != 0;  // the same answer in every thread
+}
+
 // Shared-memory matrix descriptor with explicit leading / stride byte offsets (bytes,
 // multiples of 16), no swizzle, descriptor version 1.
 __device__ __forceinline__ uint64_t fp_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -175,7 +186,7 @@ __global__ void __launch_bounds__(kFpThreads) k_conv_fp_fwd(const bf16* __restri
       }
       tc::commit(bar);
     }
-    ok = mbar_wait_sleep_bounded(bar, (uint32_t)(it & 1), err) && ok;
+    ok = mbar_wait_block(bar, (uint32_t)(it & 1), err) && ok;
     tc::fence_after_sync();
     const int cb = b, cod = od, coh0 = oh0, cow0 = ow0;
     t += gridDim.x;
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(kFpThreads) k_conv_fp_dgrad(const bf16* __rest
       }
       tc::commit(bar);
     }
-    ok = mbar_wait_sleep_bounded(bar, (uint32_t)(it & 1), err) && ok;
+    ok = mbar_wait_block(bar, (uint32_t)(it & 1), err) && ok;
     tc::fence_after_sync();
     const int cb = b, cjd = jd, cjh0 = jh0, cjw0 = jw0;
     t += gridDim.x;
