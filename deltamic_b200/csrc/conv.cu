@@ -11,6 +11,8 @@
 //                                                   class of the input voxel)
 // with m = (b, od, oh, ow), k = ((kd*3 + kh)*3 + kw)*Ci + ci (rows past 27*Ci are
 // zero padding up to a multiple of 32), P = pre-activation, dP = dL/dP.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -1246,18 +1248,62 @@ static unsigned fp_grid(int64_t tiles, int smem) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)num_sms() * per_sm));
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static std::atomic<void*> fn{nullptr};
+  void* f = fn.load();
+  if (!f) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return nullptr;
+    fn.store(f);
+  }
+  return (PFN_cuTensorMapEncodeTiled_v12000)f;
+}
+
+// Tensor map of a dense BF16 array of ``rank`` dimensions (innermost first, in
+// elements), boxes ``box`` with traversal strides ``estr``, out-of-range elements
+// read as zero.  False when the driver refuses it (the caller takes another path).
+static bool bf16_tmap(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
+                      const cuuint32_t* box, const cuuint32_t* estr) {
+  auto enc = tmap_encoder();
+  if (!enc) return false;
+  cuuint64_t strides[4];
+  cuuint64_t st = 2;
+  for (int i = 0; i < rank - 1; ++i) {
+    st *= dims[i];
+    strides[i] = st;
+  }
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(base), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// W [27 CI rows][CO] as [tap][ci][co], boxes {8 co, CI, 27}.
+static bool weight_tmap(CUtensorMap* m, const ConvShape& s, const bf16* w) {
+  const cuuint64_t dims[3] = {(cuuint64_t)s.Co, (cuuint64_t)s.Ci, 27};
+  const cuuint32_t box[3] = {8, (cuuint32_t)s.Ci, 27}, estr[3] = {1, 1, 1};
+  return bf16_tmap(m, w, 3, dims, box, estr);
+}
+
 template <int CI, int CO, int HR>
-static cudaError_t fp_fwd_launch(const ConvShape& s, const bf16* x, const bf16* w, FwdEp ep,
-                                 cudaStream_t st) {
+static int fp_fwd_launch(const ConvShape& s, const bf16* x, const bf16* w, FwdEp ep,
+                         cudaStream_t st) {
+  CUtensorMap xmap, wmap;
+  const cuuint64_t dims[5] = {(cuuint64_t)CI, (cuuint64_t)s.W, (cuuint64_t)s.H, (cuuint64_t)s.D,
+                              (cuuint64_t)s.B};
+  const cuuint32_t box[5] = {8, 18, HR, 3, 1}, estr[5] = {1, 2, 1, 1, 1};
+  if (!bf16_tmap(&xmap, x, 5, dims, box, estr) || !weight_tmap(&wmap, s, w)) return -1;
   static std::atomic<bool> done[kConvMaxDevices];
   auto k = k_conv_fp_fwd<CI, CO, HR>;
   const int smem = FpFwd<CI, CO, HR>::kSmem;
-  cudaError_t e = fp_smem_once(k, smem, done);
-  if (e != cudaSuccess) return e;
+  if (fp_smem_once(k, smem, done) != cudaSuccess) return DM_ERR_CUDA;
   const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
-  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(x, s, w, ep, conv_status_ptr());
+  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(xmap, wmap, s, ep, conv_status_ptr());
   count_launches(1);
-  return cudaGetLastError();
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
 // Forward on the footprint kernels: (Ci, Co) = (16, 32) at any size, (32, 64) with
@@ -1266,31 +1312,33 @@ static cudaError_t fp_fwd_launch(const ConvShape& s, const bf16* x, const bf16* 
 static bool fp_forward(const ConvShape& s, const bf16* x, const bf16* w, const FwdEp& ep,
                        cudaStream_t st, int& rc) {
   if (!fp_layer(s) || !ep.vec || !aligned16(x) || !aligned16(w)) return false;
-  cudaError_t e;
   if (s.Ci == 16)
-    e = s.Ho > 8 ? fp_fwd_launch<16, 32, 33>(s, x, w, ep, st)
-                 : fp_fwd_launch<16, 32, 17>(s, x, w, ep, st);
+    rc = s.Ho > 8 ? fp_fwd_launch<16, 32, 33>(s, x, w, ep, st)
+                  : fp_fwd_launch<16, 32, 17>(s, x, w, ep, st);
   else if (s.Ho <= 8)
-    e = fp_fwd_launch<32, 64, 17>(s, x, w, ep, st);
+    rc = fp_fwd_launch<32, 64, 17>(s, x, w, ep, st);
   else
     return false;
-  rc = e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
-  return true;
+  return rc != -1;  // -1: no tensor map, nothing launched
 }
 
 template <int CI, int CO>
-static cudaError_t fp_dgrad_launch(const ConvShape& s, const bf16* dp, const bf16* w, float* dx,
-                                   bf16* dxb, cudaStream_t st) {
+static int fp_dgrad_launch(const ConvShape& s, const bf16* dp, const bf16* w, float* dx,
+                           bf16* dxb, cudaStream_t st) {
+  CUtensorMap dmap, wmap;
+  const cuuint64_t dims[5] = {(cuuint64_t)CO, (cuuint64_t)s.Wo, (cuuint64_t)s.Ho,
+                              (cuuint64_t)s.Do, (cuuint64_t)s.B};
+  const cuuint32_t box[5] = {8, 9, 17, 2, 1}, estr[5] = {1, 1, 1, 1, 1};
+  if (!bf16_tmap(&dmap, dp, 5, dims, box, estr) || !weight_tmap(&wmap, s, w)) return -1;
   static std::atomic<bool> done[kConvMaxDevices];
   auto k = k_conv_fp_dgrad<CI, CO>;
   const int smem = FpDgrad<CI, CO>::kSmem;
-  cudaError_t e = fp_smem_once(k, smem, done);
-  if (e != cudaSuccess) return e;
+  if (fp_smem_once(k, smem, done) != cudaSuccess) return DM_ERR_CUDA;
   const int nd = (s.D + 1) / 2, nh = (s.H + 1) / 2, nw = (s.W + 1) / 2;
   const int64_t tiles = (int64_t)s.B * nd * ((nh + 15) / 16) * ((nw + 7) / 8);
-  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(dp, s, w, dx, dxb, conv_status_ptr());
+  k<<<fp_grid(tiles, smem), kFpThreads, smem, st>>>(dmap, wmap, s, dx, dxb, conv_status_ptr());
   count_launches(1);
-  return cudaGetLastError();
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
 // Data gradient on the footprint kernel (all eight parity classes per tile).
@@ -1298,10 +1346,9 @@ static bool fp_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* d
                      cudaStream_t st, int& rc) {
   if (!fp_layer(s) || !aligned16(dp) || !aligned16(w) || !aligned16(dxb ? (void*)dxb : (void*)dx))
     return false;
-  const cudaError_t e = s.Ci == 16 ? fp_dgrad_launch<16, 32>(s, dp, w, dx, dxb, st)
-                                   : fp_dgrad_launch<32, 64>(s, dp, w, dx, dxb, st);
-  rc = e == cudaSuccess ? DM_OK : DM_ERR_CUDA;
-  return true;
+  rc = s.Ci == 16 ? fp_dgrad_launch<16, 32>(s, dp, w, dx, dxb, st)
+                  : fp_dgrad_launch<32, 64>(s, dp, w, dx, dxb, st);
+  return rc != -1;
 }
 
 template <int CI, int CO>

@@ -58,12 +58,35 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // Waits for an MMA commit with only thread 0 sleeping on the barrier (every
 // thread polling it spends issue slots the other blocks on the SM need); after the
 // block barrier each other thread confirms the completed phase with one test.
-__device__ __forceinline__ bool mbar_wait_block(uint64_t* bar, uint32_t parity, int* err) {
-  int ok = 1;
-  if (threadIdx.x == 0) ok = mbar_wait_sleep_bounded(bar, parity, err) ? 1 : 0;
+// ``mine`` folds a thread's own failure into the (block-uniform) answer.
+__device__ __forceinline__ bool mbar_wait_block(uint64_t* bar, uint32_t parity, int* err,
+                                                bool mine = true) {
+  int ok = mine ? 1 : 0;
+  if (threadIdx.x == 0) ok = (mbar_wait_sleep_bounded(bar, parity, err) && mine) ? 1 : 0;
   ok = __syncthreads_and(ok);
   if (ok && threadIdx.x != 0) ok = mbar_wait_bounded(bar, parity, err) ? 1 : 0;
   return __syncthreads_and(ok) != 0;  // the same answer in every thread
+}
+
+// Tensor-map (TMA) box loads from this GPU's global memory into shared memory,
+// completing on an mbarrier (no multicast).  Coordinates innermost first; the
+// innermost one (a channel) is a multiple of 8 BF16 (16 bytes); the others may be
+// negative or past the extent (those elements read zero).
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, int c3, int c4, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
 }
 
 // Shared-memory matrix descriptor with explicit leading / stride byte offsets (bytes,
@@ -73,125 +96,167 @@ __device__ __forceinline__ uint64_t fp_desc(uint32_t saddr, uint32_t lbo, uint32
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Weight image: chunk (tap, co8, ci) <- w[(tap * CI + ci) * CO + 8 co8 .. + 7].
-template <int CI, int CO>
-__device__ __forceinline__ void fp_load_weights(uint8_t* wimg, const bf16* __restrict__ w) {
-  constexpr int kChunks = 27 * (CO / 8) * CI;
-  // lanes take consecutive 16-byte chunks of W (full sectors, coalesced)
-  for (int e = threadIdx.x; e < kChunks; e += blockDim.x) {
-    const int co8 = e % (CO / 8), k = e / (CO / 8);
-    const int ci = k % CI, tap = k / CI;
-    cp_async16(wimg + ((tap * (CO / 8) + co8) * CI + ci) * 16, w + (size_t)e * 8, 16);
-  }
-}
-
-template <int CI, int CO, int HR>
-struct FpFwd {
-  static constexpr int kC8 = CI / 8;
-  static constexpr int kFpChunks = kC8 * 3 * HR * 18;
-  static constexpr int kPadChunks = (33 - HR) * 18;  // lines 8..15 of a 17-row footprint
-  static constexpr int kWBytes = 27 * (CO / 8) * CI * 16;
-  static constexpr int kFpBytes = (kFpChunks + kPadChunks) * 16;
-  static constexpr int kSmem = kWBytes + kFpBytes + 64;
-  static constexpr uint32_t kLbo = 3 * HR * 18 * 16;  // channel group -> next
-  static constexpr uint32_t kSbo = 36 * 16;           // line -> next (two input rows)
-  static_assert(kSmem <= 227 * 1024, "footprint tile above the shared-memory limit");
-};
-
 // Threads of a footprint block: eight warps; warp w reads accumulator lanes
 // 32 (w % 4) .. + 31 (its TMEM lane quarter) and the column half w / 4.
 constexpr int kFpThreads = 256;
 
-// Footprint of forward tile t (see the layout above), issued as cp.async copies.
+// Weight image, loaded by TMA as CO / 8 boxes {8 co, CI ci, 27 taps} of W viewed as
+// [tap][ci][co]: chunk (co8, tap, ci) = W[tap * CI + ci, 8 co8 .. 8 co8 + 7] at
+// (co8 * 27 + tap) * CI + ci.  It is the forward's MN-major B (N = co: groups of 8
+// co 27 CI chunks apart, K = ci: rows 16 bytes apart, groups of 8 ci 128 bytes
+// apart) and the data gradient's K-major B (N = ci rows, K = co: groups 27 CI
+// chunks apart).
+template <int CI, int CO>
+struct FpWeights {
+  static constexpr int kBoxBytes = 8 * CI * 27 * 2;
+  static constexpr int kBytes = (CO / 8) * kBoxBytes;
+  static_assert(kBoxBytes % 128 == 0, "weight boxes 128-byte aligned");
+};
+
+template <int CI, int CO>
+__device__ __forceinline__ void fp_tma_weights(uint8_t* wimg, const CUtensorMap* wmap,
+                                               uint64_t* bar) {
+#pragma unroll
+  for (int co8 = 0; co8 < CO / 8; ++co8)
+    tma_load_3d(wimg + co8 * FpWeights<CI, CO>::kBoxBytes, wmap, co8 * 8, 0, 0, bar);
+}
+
+// Forward footprint (TMA): box (c8, par) = x[b, 2 od - 1 + kd, 2 oh0 - 1 + r,
+// 2 ow0 - 1 + par + 2 j, 8 c8 .. + 7], kd < 3, r < HR, j < 9 (a W traversal stride
+// of 2 de-interleaves the parities), chunk ((kd * HR + r) * 9 + j) of the box; boxes
+// (c8 * 2 + par) are kBlk chunks apart (128-byte aligned).  Tap (kd, kh, kw) of
+// output line l, voxel i reads box par(kw) = (kw == 1), chunk (kd HR + 2 l + kh) 9 +
+// i + (kw == 2): lines 18 chunks apart, channel groups 2 kBlk chunks apart.
+template <int CI, int CO, int HR>
+struct FpFwd {
+  static constexpr int kC8 = CI / 8;
+  static constexpr int kBlk = (3 * HR * 9 + 7) / 8 * 8;
+  // HR = 17: lines 8..15 read past the loaded rows (garbage accumulator rows, never
+  // stored); the last box's reads end (2 HR + 32) 9 + 9 chunks into it
+  static constexpr int kTail = (2 * HR + 32) * 9 + 9 > kBlk ? (2 * HR + 32) * 9 + 9 - kBlk : 0;
+  static constexpr int kFpBytes = (2 * kC8 * kBlk + (kTail + 7) / 8 * 8) * 16;
+  static constexpr int kBoxBytes = 8 * 9 * HR * 3 * 2;  // bytes one box writes
+  static constexpr int kWBytes = FpWeights<CI, CO>::kBytes;
+  static constexpr int kSmem = 128 + kWBytes + kFpBytes + 64;  // + base alignment
+  static constexpr uint32_t kLbo = 2 * kBlk * 16;  // channel group -> next
+  static constexpr uint32_t kSbo = 18 * 16;        // line -> next (two input rows)
+  static_assert(kSmem <= 227 * 1024, "footprint tile above the shared-memory limit");
+};
+
 template <int CI, int HR>
-__device__ __forceinline__ void fp_fwd_tile(const bf16* __restrict__ x, const ConvShape& s, int t,
-                                            uint8_t* fp, int& b, int& od, int& oh0, int& ow0) {
+__device__ __forceinline__ void fp_fwd_tma(const CUtensorMap* xmap, const ConvShape& s, int t,
+                                           uint8_t* fp, uint64_t* bar, int& b, int& od,
+                                           int& oh0, int& ow0) {
+  constexpr int kBlk = (3 * HR * 9 + 7) / 8 * 8;
   const int nwb = (s.Wo + 7) >> 3, nhb = (s.Ho + 15) >> 4;
-  const int owb = t % nwb;
+  ow0 = (t % nwb) * 8;
   t /= nwb;
-  const int ohb = t % nhb;
+  oh0 = (t % nhb) * 16;
   t /= nhb;
   od = t % s.Do;
   b = t / s.Do;
-  ow0 = owb * 8;
-  oh0 = ohb * 16;
-  const int d0 = 2 * od - 1, h0 = 2 * oh0 - 1, w0 = 2 * ow0 - 1;
-  // lanes take consecutive chunks of an input row (18 voxels x CI channels, in
-  // global order: coalesced full sectors) and scatter them into the layout
-  constexpr int kC8 = CI / 8;
-  for (int e = threadIdx.x; e < kC8 * 3 * HR * 18; e += kFpThreads) {
-    const int c8 = e % kC8, q = e / kC8;
-    const int wl = q % 18, row = q / 18;
-    const int hr = row % HR, kd = row / HR;
-    const int d = d0 + kd, h = h0 + hr, ww = w0 + wl;
-    const bool ok = d >= 0 && d < s.D && h >= 0 && h < s.H && ww >= 0 && ww < s.W;
-    const bf16* src = ok ? x + ((((size_t)b * s.D + d) * s.H + h) * s.W + ww) * CI + c8 * 8 : x;
-    cp_async16(fp + ((((c8 * 3 + kd) * HR + hr) * 18) + (wl & 1) * 9 + (wl >> 1)) * 16, src,
-               ok ? 16u : 0u);
-  }
+#pragma unroll
+  for (int c8 = 0; c8 < CI / 8; ++c8)
+#pragma unroll
+    for (int par = 0; par < 2; ++par)
+      tma_load_5d(fp + (c8 * 2 + par) * kBlk * 16, xmap, c8 * 8, 2 * ow0 - 1 + par,
+                  2 * oh0 - 1, 2 * od - 1, b, bar);
 }
 
 // Forward: pre = conv(x, w) + bias (FP32), act = GELU(pre) (BF16).  Persistent
-// blocks: the weight image is staged once, then tiles blockIdx.x, + gridDim.x, ...
-// Per tile: wait for its footprint, thread 0 issues the 27 taps' MMAs, and once
-// they are done the next tile's footprint copies are issued before the epilogue
-// reads this tile's accumulator, so their latency hides behind it.
+// blocks: thread 0 loads the weight image once and each tile's footprint with TMA
+// (bar[0]), issues the 27 taps' MMAs (bar[1]), and once they are done the next
+// tile's footprint is requested before the epilogue reads this tile's accumulator.
 template <int CI, int CO, int HR>
-__global__ void __launch_bounds__(kFpThreads) k_conv_fp_fwd(const bf16* __restrict__ x,
-                                                            ConvShape s,
-                                                            const bf16* __restrict__ w, FwdEp ep,
-                                                            int* err) {
+__global__ void __launch_bounds__(kFpThreads) k_conv_fp_fwd(const __grid_constant__ CUtensorMap xmap,
+                                                            const __grid_constant__ CUtensorMap wmap,
+                                                            ConvShape s, FwdEp ep, int* err) {
   using F = FpFwd<CI, CO, HR>;
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint8_t* const wimg = smem;
   uint8_t* const fp = smem + F::kWBytes;
-  uint64_t* const bar = (uint64_t*)(fp + F::kFpBytes);
-  uint32_t* const slot = (uint32_t*)(bar + 1);
+  uint64_t* const bar = (uint64_t*)(fp + F::kFpBytes);  // [0] loads, [1] MMAs
+  uint32_t* const slot = (uint32_t*)(bar + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = s.B * s.Do * ((s.Ho + 15) >> 4) * ((s.Wo + 7) >> 3);
 
-  fp_load_weights<CI, CO>(wimg, w);
   int b = 0, od = 0, oh0 = 0, ow0 = 0;
   int t = blockIdx.x;
-  if (t < ntiles) fp_fwd_tile<CI, HR>(x, s, t, fp, b, od, oh0, ow0);
-  if (warp == 0) tc::tmem_alloc(slot, tc::tmem_cols<CO>());
-  if (threadIdx.x == 32) {
-    mbar_init(bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_mbar_init();
+    if (t < ntiles) {
+      mbar_expect_tx(&bar[0], F::kWBytes + 2 * F::kC8 * F::kBoxBytes);
+      fp_tma_weights<CI, CO>(wimg, &wmap, &bar[0]);
+      fp_fwd_tma<CI, HR>(&xmap, s, t, fp, &bar[0], b, od, oh0, ow0);
+    }
   }
+  if (threadIdx.x != 0 && t < ntiles) {  // the tile coordinates, without issuing
+    const int nwb = (s.Wo + 7) >> 3, nhb = (s.Ho + 15) >> 4;
+    int u = t;
+    ow0 = (u % nwb) * 8;
+    u /= nwb;
+    oh0 = (u % nhb) * 16;
+    u /= nhb;
+    od = u % s.Do;
+    b = u / s.Do;
+  }
+  if (warp == 0) tc::tmem_alloc(slot, tc::tmem_cols<CO>());
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
   bool ok = true;
+  int lost = -1;  // thread 0: a load wait that gave up (its copies may still land)
   for (int it = 0; t < ntiles; ++it) {
-    cp_async_wait_all();
-    fence_proxy_async();  // the copies -> the MMA's async-proxy reads
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *slot;
+    bool lok = true;
     if (threadIdx.x == 0) {
-      const uint32_t wb = smem_u32(wimg), fb = smem_u32(fp);
-      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>() | (1u << 16);  // B MN-major
-      int n = 0;
+      // the tile's footprint (and, first, the weights) have landed
+      lok = mbar_wait_sleep_bounded(&bar[0], (uint32_t)(it & 1), err);
+      if (!lok) lost = it;
+      if (lok) {
+        tc::fence_after_sync();
+        const uint32_t wb = smem_u32(wimg), fb = smem_u32(fp);
+        constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>() | (1u << 16);  // B MN-major
+        int n = 0;
 #pragma unroll 1
-      for (int tap = 0; tap < 27; ++tap) {
-        const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
-        const int aoff = (kd * HR + kh) * 18 + (kw == 1 ? 9 : 0) + (kw == 2 ? 1 : 0);
+        for (int tap = 0; tap < 27; ++tap) {
+          const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+          const int aoff = (kw == 1 ? F::kBlk : 0) + (kd * HR + kh) * 9 + (kw == 2 ? 1 : 0);
 #pragma unroll
-        for (int kk = 0; kk < CI / 16; ++kk) {
-          const uint32_t a = fb + (uint32_t)(aoff + 2 * kk * 3 * HR * 18) * 16;
-          const uint32_t bb = wb + (uint32_t)(tap * (CO / 8) * CI + 16 * kk) * 16;
-          // B MN-major: K groups (8 ci) 128 bytes apart, N groups (8 co) CI chunks apart
-          tc::mma_bf16(tmem, fp_desc(a, F::kLbo, F::kSbo), fp_desc(bb, 128, CI * 16), idesc,
-                       n++ > 0);
+          for (int kk = 0; kk < CI / 16; ++kk) {
+            const uint32_t a = fb + (uint32_t)(aoff + 2 * kk * 2 * F::kBlk) * 16;
+            const uint32_t bb = wb + (uint32_t)(tap * CI + 16 * kk) * 16;
+            // B MN-major: K groups (8 ci) 128 bytes apart, N groups (8 co) 27 CI chunks
+            tc::mma_bf16(tmem, fp_desc(a, F::kLbo, F::kSbo), fp_desc(bb, 128, 27 * CI * 16),
+                         idesc, n++ > 0);
+          }
         }
       }
-      tc::commit(bar);
+      tc::commit(&bar[1]);  // also without MMAs, so the phase completes
     }
-    ok = mbar_wait_block(bar, (uint32_t)(it & 1), err) && ok;
+    ok = mbar_wait_block(&bar[1], (uint32_t)(it & 1), err, lok) && ok;
     tc::fence_after_sync();
     const int cb = b, cod = od, coh0 = oh0, cow0 = ow0;
     t += gridDim.x;
     if (!ok) break;
-    if (t < ntiles) fp_fwd_tile<CI, HR>(x, s, t, fp, b, od, oh0, ow0);
+    if (t < ntiles) {  // the MMAs reading fp are done: request the next footprint
+      if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar[0], 2 * F::kC8 * F::kBoxBytes);
+        fp_fwd_tma<CI, HR>(&xmap, s, t, fp, &bar[0], b, od, oh0, ow0);
+      } else {
+        const int nwb = (s.Wo + 7) >> 3, nhb = (s.Ho + 15) >> 4;
+        int u = t;
+        ow0 = (u % nwb) * 8;
+        u /= nwb;
+        oh0 = (u % nhb) * 16;
+        u /= nhb;
+        od = u % s.Do;
+        b = u / s.Do;
+      }
+    }
     const int q = warp & 3, row = q * 32 + lane;
     const int oh = coh0 + (row >> 3), ow = cow0 + (row & 7);
     const bool live = oh < s.Ho && ow < s.Wo;
@@ -203,124 +268,136 @@ __global__ void __launch_bounds__(kFpThreads) k_conv_fp_fwd(const bf16* __restri
       if (live) ep.put16(m, c, 0, v);
     }
   }
-  cp_async_wait_all();  // copies of a tile the loop left early
+  // copies whose wait gave up: one more bounded wait, so none lands after the block
+  // has left
+  if (threadIdx.x == 0 && lost >= 0) mbar_wait_sleep_bounded(&bar[0], (uint32_t)(lost & 1), err);
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(*slot, tc::tmem_cols<CO>());
+    tc::tmem_dealloc(tmem, tc::tmem_cols<CO>());
   }
 }
 
+// Data-gradient footprint (TMA): box co8 = dP[b, jd + dd, jh0 + hh, jw0 + ww,
+// 8 co8 .. + 7], dd < 2, hh < 17, ww < 9, chunk (dd * 17 + hh) * 9 + ww, boxes 312
+// chunks apart (128-byte aligned).
 template <int CI, int CO>
 struct FpDgrad {
-  static constexpr int kFpChunks = (CO / 8) * 2 * 17 * 9;
-  static constexpr int kWBytes = 27 * (CO / 8) * CI * 16;
-  static constexpr int kFpBytes = kFpChunks * 16;
-  static constexpr int kSmem = kWBytes + kFpBytes + 64;
+  static constexpr int kBlk = 312;
+  static constexpr int kBoxBytes = 8 * 9 * 17 * 2 * 2;
+  static constexpr int kFpBytes = (CO / 8) * kBlk * 16;
+  static constexpr int kWBytes = FpWeights<CI, CO>::kBytes;
+  static constexpr int kSmem = 128 + kWBytes + kFpBytes + 64;
   static constexpr int kCols = 8 * CI;                // one accumulator per parity class
-  static constexpr uint32_t kLbo = 2 * 17 * 9 * 16;   // channel group -> next
+  static constexpr uint32_t kLbo = kBlk * 16;         // channel group -> next
   static constexpr uint32_t kSbo = 9 * 16;            // line -> next
   static_assert(kCols == 128 || kCols == 256 || kCols == 512, "TMEM allocation");
   static_assert(kSmem <= 227 * 1024, "footprint tile above the shared-memory limit");
 };
 
-// dP footprint of data-gradient tile t (see the layout above).
+// Tile t of the data gradient: (b, jd, jh0, jw0), and (thread 0) its dP boxes.
 template <int CO>
-__device__ __forceinline__ void fp_dgrad_tile(const bf16* __restrict__ dp, const ConvShape& s,
-                                              int t, uint8_t* fp, int& b, int& jd, int& jh0,
+__device__ __forceinline__ void fp_dgrad_tile(const CUtensorMap* dmap, const ConvShape& s, int t,
+                                              uint8_t* fp, uint64_t* bar, bool issue,
+                                              uint32_t extra_tx, int& b, int& jd, int& jh0,
                                               int& jw0) {
   const int nd = (s.D + 1) >> 1, nh = (s.H + 1) >> 1, nw = (s.W + 1) >> 1;
   const int nwb = (nw + 7) >> 3, nhb = (nh + 15) >> 4;
-  const int jwb = t % nwb;
+  jw0 = (t % nwb) * 8;
   t /= nwb;
-  const int jhb = t % nhb;
+  jh0 = (t % nhb) * 16;
   t /= nhb;
   jd = t % nd;
   b = t / nd;
-  jw0 = jwb * 8;
-  jh0 = jhb * 16;
-  for (int e = threadIdx.x; e < (CO / 8) * 2 * 17 * 9; e += kFpThreads) {  // global order
-    const int co8 = e % (CO / 8), q = e / (CO / 8);
-    const int ww = q % 9, row = q / 9;
-    const int hh = row % 17, dd = row / 17;
-    const int od = jd + dd, oh = jh0 + hh, ow = jw0 + ww;
-    const bool ok = od < s.Do && oh < s.Ho && ow < s.Wo;
-    const bf16* src =
-        ok ? dp + ((((size_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow) * CO + co8 * 8 : dp;
-    cp_async16(fp + (((co8 * 2 + dd) * 17 + hh) * 9 + ww) * 16, src, ok ? 16u : 0u);
-  }
+  if (!issue) return;
+  // one arrival per phase: the expected bytes of everything in flight on bar
+  mbar_expect_tx(bar, extra_tx + (CO / 8) * FpDgrad<16, CO>::kBoxBytes);
+#pragma unroll
+  for (int co8 = 0; co8 < CO / 8; ++co8)
+    tma_load_5d(fp + co8 * 312 * 16, dmap, co8 * 8, jw0, jh0, jd, b, bar);
 }
 
 // Data gradient of all eight parity classes of a tile of input voxels: dX[q, ci] =
 // sum over the class's taps of dP[output reached through the tap] W[tap, ci, :].
-// dx (FP32) or dxb (BF16) receives it.  Persistent blocks, as the forward.
+// dx (FP32) or dxb (BF16) receives it.  Persistent blocks, loads and MMAs as in the
+// forward.
 template <int CI, int CO>
-__global__ void __launch_bounds__(kFpThreads) k_conv_fp_dgrad(const bf16* __restrict__ dp,
-                                                              ConvShape s,
-                                                              const bf16* __restrict__ w,
-                                                              float* __restrict__ dx,
+__global__ void __launch_bounds__(kFpThreads) k_conv_fp_dgrad(const __grid_constant__ CUtensorMap dmap,
+                                                              const __grid_constant__ CUtensorMap wmap,
+                                                              ConvShape s, float* __restrict__ dx,
                                                               bf16* __restrict__ dxb, int* err) {
   using F = FpDgrad<CI, CO>;
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint8_t* const wimg = smem;
   uint8_t* const fp = smem + F::kWBytes;
-  uint64_t* const bar = (uint64_t*)(fp + F::kFpBytes);
-  uint32_t* const slot = (uint32_t*)(bar + 1);
+  uint64_t* const bar = (uint64_t*)(fp + F::kFpBytes);  // [0] loads, [1] MMAs
+  uint32_t* const slot = (uint32_t*)(bar + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nd = (s.D + 1) >> 1, nh = (s.H + 1) >> 1, nw = (s.W + 1) >> 1;
   const int ntiles = s.B * nd * ((nh + 15) >> 4) * ((nw + 7) >> 3);
 
-  fp_load_weights<CI, CO>(wimg, w);
   int b = 0, jd = 0, jh0 = 0, jw0 = 0;
   int t = blockIdx.x;
-  if (t < ntiles) fp_dgrad_tile<CO>(dp, s, t, fp, b, jd, jh0, jw0);
-  if (warp == 0) tc::tmem_alloc(slot, F::kCols);
-  if (threadIdx.x == 32) {
-    mbar_init(bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_mbar_init();
   }
+  if (t < ntiles) {
+    // the weights' bytes ride on the first footprint's expect_tx
+    fp_dgrad_tile<CO>(&dmap, s, t, fp, &bar[0], threadIdx.x == 0, F::kWBytes, b, jd, jh0, jw0);
+    if (threadIdx.x == 0) fp_tma_weights<CI, CO>(wimg, &wmap, &bar[0]);
+  }
+  if (warp == 0) tc::tmem_alloc(slot, F::kCols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
   bool ok = true;
+  int lost = -1;
   for (int it = 0; t < ntiles; ++it) {
-    cp_async_wait_all();
-    fence_proxy_async();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *slot;
+    bool lok = true;
     if (threadIdx.x == 0) {
-      const uint32_t wb = smem_u32(wimg), fb = smem_u32(fp);
-      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CI>();  // both K-major
+      lok = mbar_wait_sleep_bounded(&bar[0], (uint32_t)(it & 1), err);
+      if (!lok) lost = it;
+      if (lok) {
+        tc::fence_after_sync();
+        const uint32_t wb = smem_u32(wimg), fb = smem_u32(fp);
+        constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CI>();  // both K-major
 #pragma unroll 1
-      for (int tap = 0; tap < 27; ++tap) {
-        const int k[3] = {tap / 9, (tap / 3) % 3, tap % 3};
-        // parity of the input voxels this tap reaches (k = 1: even; 0, 2: odd) and
-        // the output offset (k = 0: j + 1, else j)
-        int cls = 0, dl[3];
+        for (int tap = 0; tap < 27; ++tap) {
+          const int k[3] = {tap / 9, (tap / 3) % 3, tap % 3};
+          // parity of the input voxels this tap reaches (k = 1: even; 0, 2: odd) and
+          // the output offset (k = 0: j + 1, else j)
+          int cls = 0, dl[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          cls = cls * 2 + (k[a] == 1 ? 0 : 1);
-          dl[a] = k[a] == 0 ? 1 : 0;
-        }
-        const int first = (k[0] != 2) && (k[1] != 2) && (k[2] != 2);  // first tap of its class
-        const int aoff = (dl[0] * 17 + dl[1]) * 9 + dl[2];
+          for (int a = 0; a < 3; ++a) {
+            cls = cls * 2 + (k[a] == 1 ? 0 : 1);
+            dl[a] = k[a] == 0 ? 1 : 0;
+          }
+          const int first = (k[0] != 2) && (k[1] != 2) && (k[2] != 2);  // first tap of its class
+          const int aoff = (dl[0] * 17 + dl[1]) * 9 + dl[2];
 #pragma unroll
-        for (int kk = 0; kk < CO / 16; ++kk) {
-          const uint32_t a = fb + (uint32_t)(aoff + 2 * kk * 2 * 17 * 9) * 16;
-          const uint32_t bb = wb + (uint32_t)((tap * (CO / 8) + 2 * kk) * CI) * 16;
-          // B K-major: K groups (8 co) CI chunks apart, N groups (8 ci) 128 bytes apart
-          tc::mma_bf16(tmem + (uint32_t)(cls * CI), fp_desc(a, F::kLbo, F::kSbo),
-                       fp_desc(bb, CI * 16, 128), idesc, !(first && kk == 0));
+          for (int kk = 0; kk < CO / 16; ++kk) {
+            const uint32_t a = fb + (uint32_t)(aoff + 2 * kk * F::kBlk) * 16;
+            const uint32_t bb = wb + (uint32_t)((2 * kk * 27 + tap) * CI) * 16;
+            // B K-major: K groups (8 co) 27 CI chunks apart, N groups (8 ci) 128 bytes
+            tc::mma_bf16(tmem + (uint32_t)(cls * CI), fp_desc(a, F::kLbo, F::kSbo),
+                         fp_desc(bb, 27 * CI * 16, 128), idesc, !(first && kk == 0));
+          }
         }
       }
-      tc::commit(bar);
+      tc::commit(&bar[1]);  // also without MMAs, so the phase completes
     }
-    ok = mbar_wait_block(bar, (uint32_t)(it & 1), err) && ok;
+    ok = mbar_wait_block(&bar[1], (uint32_t)(it & 1), err, lok) && ok;
     tc::fence_after_sync();
     const int cb = b, cjd = jd, cjh0 = jh0, cjw0 = jw0;
     t += gridDim.x;
     if (!ok) break;
-    if (t < ntiles) fp_dgrad_tile<CO>(dp, s, t, fp, b, jd, jh0, jw0);
+    if (t < ntiles)
+      fp_dgrad_tile<CO>(&dmap, s, t, fp, &bar[0], threadIdx.x == 0, 0u, b, jd, jh0, jw0);
     const int q = warp & 3, row = q * 32 + lane;
     const int jh = cjh0 + (row >> 3), jw = cjw0 + (row & 7);
 #pragma unroll 1
@@ -352,12 +429,12 @@ __global__ void __launch_bounds__(kFpThreads) k_conv_fp_dgrad(const bf16* __rest
       }
     }
   }
-  cp_async_wait_all();
+  if (threadIdx.x == 0 && lost >= 0) mbar_wait_sleep_bounded(&bar[0], (uint32_t)(lost & 1), err);
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(*slot, F::kCols);
+    tc::tmem_dealloc(tmem, F::kCols);
   }
 }
 
