@@ -1,35 +1,24 @@
-// Footprint convolution kernels (included by conv.cu): the forward and the data
-// gradient of the 3x3x3 stride-2 convolution for the encoder's middle layers
-// (Ci = 16 -> Co = 32 and Ci = 32 -> Co = 64), with the MMA operands read straight
-// from a tile's input footprint in shared memory -- no im2col copy.
+// Footprint convolution kernels (included by conv.cu): the forward, data gradient
+// and weight gradient of the 3x3x3 stride-2 convolution for the encoder's middle
+// layers (Ci = 16 -> Co = 32 and Ci = 32 -> Co = 64), with the MMA operands read
+// straight from a tile's input footprint in shared memory -- no im2col copy.
 //
 // A tile is 16 "lines" of 8 voxels along the fastest spatial axis (128 rows, the
-// MMA's M).  Its input footprint is staged once with 16-byte cp.async copies
-// (zero-filled outside the volume, which is the padding), channel groups of eight
-// (16 bytes) as the unit, laid out so that for every tap the 8 rows of a core
-// matrix are 8 consecutive 16-byte chunks and the 16 lines are a uniform stride
-// apart.  A tap is then only a start address: the shared-memory matrix descriptor
-// of tap t points into the footprint with the line stride as its stride byte offset
-// and the channel-group stride as its leading byte offset.  The weights are staged
-// once per tile as an image [tap][co/8][ci] of 16-byte chunks (8 output channels of
-// one (tap, ci) row of W), which is the MN-major B operand of the forward
-// (N = co) and the K-major B operand of the data gradient (N = ci, K = co).
+// MMA's M).  Its input footprint is staged once (zero outside the volume, which is
+// the padding), channel groups of eight (16 bytes) as the unit, laid out so that for
+// every tap the 8 rows of a core matrix are 8 consecutive 16-byte chunks and the 16
+// lines are a uniform stride apart.  A tap is then only a start address: the
+// shared-memory matrix descriptor of tap t points into the footprint with the line
+// stride as its stride byte offset and the channel-group stride as its leading byte
+// offset.  The forward and the data gradient stage the footprint and the weight
+// image with TMA boxes (layouts at FpWeights, FpFwd and FpDgrad below); the weight
+// gradient, whose layout interleaves rows and channel groups, with cp.async.
 //
-// Forward footprint, tile (b, od, oh0 + l, ow0 + i), l < 16, i < 8: chunk
-//   ((c8 * 3 + kd) * HR + r) * 18 + par * 9 + j
-// holds x[b, 2 od - 1 + kd, 2 oh0 - 1 + r, w, 8 c8 .. 8 c8 + 7] with w = 2 ow0 - 1 + 2 j
-// (par 0: taps kw = 0 (j = i) and kw = 2 (j = i + 1)) or w = 2 ow0 + 2 j (par 1:
-// kw = 1, j = i).  Row r of line l and tap kh is 2 l + kh, so lines are 36 chunks
-// apart.  HR = 33 rows when the output has more than 8 rows, else 17 (lines 8..15
-// then read past the loaded rows into a padded region: garbage rows of the
-// accumulator that are never stored).
-//
-// Data-gradient footprint, tile of input voxels (b, 2 jd + pd, 2 (jh0 + l) + ph,
-// 2 (jw0 + i) + pw) for all eight parity classes (pd, ph, pw): per axis, parity 0
-// takes tap 1 from output j and parity 1 taps 0 and 2 from outputs j + 1 and j, so
-// the tile needs dP at outputs (jd + dd, jh0 + hh, jw0 + ww), dd < 2, hh < 17,
-// ww < 9: chunk ((co8 * 2 + dd) * 17 + hh) * 9 + ww.  Each class accumulates in its
-// own TMEM columns (class * Ci), the 27 taps are each issued once.
+// Data gradient, tile of input voxels (b, 2 jd + pd, 2 (jh0 + l) + ph, 2 (jw0 + i) +
+// pw) for all eight parity classes (pd, ph, pw): per axis, parity 0 takes tap 1 from
+// output j and parity 1 taps 0 and 2 from outputs j + 1 and j, so the tile needs dP
+// at outputs (jd + dd, jh0 + hh, jw0 + ww), dd < 2, hh < 17, ww < 9.  Each class
+// accumulates in its own TMEM columns (class * Ci), the 27 taps are each issued once.
 //
 // Weight gradient, per block one input plane kd (blockIdx.y) and a run of forward
 // tiles (blockIdx.x): dW[(kd, kh, kw, ci), co] = sum_m x[m through the tap][ci]

@@ -10,9 +10,10 @@
 // channel non-zero ((dd, p) = (0, 0) reaches no tap).
 //
 // A tile is 16 output lines x 8 voxels (128 rows).  Its block footprint is
-// chunk ((dd * 17 + hh) * 9 + ww) for blocks (od - 1 + dd, oh0 - 1 + hh, ow0 - 1 + ww),
-// staged with 4-byte cp.async copies (one (pd, ph) pair of columns each, zero
-// outside the volume).  8 consecutive voxels of a line are 8 consecutive chunks, and
+// chunk ((dd * 17 + hh) * 9 + ww) for blocks (od - 1 + dd, oh0 - 1 + hh, ow0 - 1 + ww)
+// (zero outside the volume), each block's four (pd, ph) column pairs 4 bytes apart:
+// the forward stages it through registers from aligned 16-byte row pieces, the
+// weight gradient with 4-byte cp.async copies.  8 consecutive voxels of a line are 8 consecutive chunks, and
 // the block tap dw is one chunk further: the forward's A operand (K-major, K = (dw,
 // par)) is the footprint itself with a leading byte offset of 16 (the two core
 // matrices along K overlap by seven rows) and lines 9 chunks apart.  Four MMAs, one
@@ -129,8 +130,8 @@ struct S2dFwd {
 // Forward of the single-channel layer: pre = conv(x, w) + bias (FP32), act =
 // GELU(pre) (BF16).  Persistent blocks of 256 threads: the weight image is built
 // once; per tile four MMAs, then the next tile's footprint loads are issued, the
-// epilogue runs, and the loaded pieces are stored into the footprint.  Warp w reads accumulator lanes
-// 32 (w % 4) .. + 31, columns (w / 4) CO / 2 .. + CO / 2 - 1.
+// epilogue runs, and the loaded pieces are stored into the footprint.  Warp w reads
+// accumulator lanes 32 (w % 4) .. + 31, columns (w / 4) CO / 2 .. + CO / 2 - 1.
 template <int CO>
 __global__ void __launch_bounds__(256) k_conv_s2d_fwd(const bf16* __restrict__ x, ConvShape s,
                                                       const bf16* __restrict__ w,
