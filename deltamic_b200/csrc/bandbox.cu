@@ -84,11 +84,13 @@ struct BBHdr {
 
 __device__ __forceinline__ float cabs2(float2 z) { return sqrtf(fmaf(z.x, z.x, z.y * z.y)); }
 
+// acc += a b (complex) on the paired FP32 path: two FFMA2, each rounding once per
+// component in the order re: + a.x b.x, - a.y b.y; im: + a.x b.y, + a.y b.x (the
+// same results as four scalar FMAs in that order).  In unrolled register tiles the
+// broadcast pairs (a.x, a.x), (a.y, a.y) and the swapped (-b.y, b.x) are shared.
 __device__ __forceinline__ float2 cmac(float2 acc, float2 a, float2 b) {
-  acc.x = fmaf(a.x, b.x, acc.x);
-  acc.x = fmaf(-a.y, b.y, acc.x);
-  acc.y = fmaf(a.x, b.y, acc.y);
-  acc.y = fmaf(a.y, b.x, acc.y);
+  acc = __ffma2_rn(make_float2(a.x, a.x), b, acc);
+  acc = __ffma2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x), acc);
   return acc;
 }
 
