@@ -872,6 +872,7 @@ struct DgradEp {
 
 #include "conv_fp.cuh"
 #include "conv_s2d.cuh"
+#include "conv_tg.cuh"
 
 namespace dm {
 
@@ -1187,10 +1188,14 @@ static int wgrad_splits(const ConvShape& s) {
   return (int)sp;
 }
 
-// Workspace: dP (BF16) | split partials (FP32).
+static bool tg_layer(const ConvShape& s);
+
+// Workspace: dP (BF16) | split partials (FP32); a tap-GEMM layer's data gradient
+// reuses the partials' area (summed by then) for dcol [M][27 Ci] FP32.
 size_t conv_ws_bytes(const ConvShape& s) {
   const size_t dp = ((size_t)s.M * s.Co * sizeof(bf16) + 255) / 256 * 256;
-  const size_t part = (size_t)wgrad_splits(s) * (s.Kp + 1) * s.Co * sizeof(float);
+  size_t part = (size_t)wgrad_splits(s) * (s.Kp + 1) * s.Co * sizeof(float);
+  if (tg_layer(s)) part = std::max(part, (size_t)s.M * 27 * s.Ci * sizeof(float));
   return dp + part + 256;
 }
 
@@ -1217,9 +1222,33 @@ static int fwd_splits(const ConvShape& s) {
   return (int)((stages + per - 1) / per);
 }
 
+// Tap-GEMM forward (conv_tg.cuh): 64 -> 128 channels, whole images of at most 128
+// output voxels per tile (128 divisible by the voxels per image).
+static bool tg_layer(const ConvShape& s) {
+  const int per_img = s.Do * s.Ho * s.Wo;
+  return s.Ci == 64 && s.Co == 128 && per_img <= 128 && 128 % per_img == 0;
+}
+static int64_t tg_tiles(const ConvShape& s) {
+  const int nb = 128 / (s.Do * s.Ho * s.Wo);
+  return (s.B + nb - 1) / nb;
+}
+// Taps per split: about one block per SM over the m tiles and the splits.
+static int tg_tps(const ConvShape& s) {
+  const int64_t sp = std::max<int64_t>(1, std::min<int64_t>(27, 148 / tg_tiles(s)));
+  return (int)((27 + sp - 1) / sp);
+}
+static int tg_splits(const ConvShape& s) { return (27 + tg_tps(s) - 1) / tg_tps(s); }
+static size_t tg_wt_offset(const ConvShape& s) {
+  return ((size_t)tg_splits(s) * s.M * s.Co * sizeof(float) + 1023) / 1024 * 1024;
+}
+
 size_t conv_fwd_ws_bytes(const ConvShape& s) {
   const int sp = fwd_splits(s);
-  return sp > 1 ? (size_t)sp * s.M * s.Co * sizeof(float) + 256 : 256;
+  const size_t split = sp > 1 ? (size_t)sp * s.M * s.Co * sizeof(float) + 256 : 256;
+  // a tap-GEMM layer may still take the split path (no tensor map): room for both
+  if (tg_layer(s))
+    return std::max(split, tg_wt_offset(s) + (size_t)27 * s.Ci * s.Co * sizeof(bf16) + 256);
+  return split;
 }
 
 // Footprint kernels (conv_fp.cuh): the layer shapes they are instantiated for.
@@ -1267,7 +1296,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 // elements), boxes ``box`` with traversal strides ``estr``, out-of-range elements
 // read as zero.  False when the driver refuses it (the caller takes another path).
 static bool bf16_tmap(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
-                      const cuuint32_t* box, const cuuint32_t* estr) {
+                      const cuuint32_t* box, const cuuint32_t* estr,
+                      CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE) {
   auto enc = tmap_encoder();
   if (!enc) return false;
   cuuint64_t strides[4];
@@ -1277,7 +1307,7 @@ static bool bf16_tmap(CUtensorMap* m, const void* base, int rank, const cuuint64
     strides[i] = st;
   }
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(base), dims,
-             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -1427,9 +1457,71 @@ static cudaError_t s2d_wgrad_launch(const ConvShape& s, const bf16* x, const bf1
   return cudaGetLastError();
 }
 
+// Forward of a tap-GEMM layer: W^T into the workspace, the tap GEMM's partials, their
+// fixed-order sum with the bias and GELU.  -1: not taken (no tensor map).
+static int tg_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
+                      float* pre, bf16* act, void* ws, cudaStream_t st) {
+  float* part = (float*)ws;
+  bf16* wt = (bf16*)((char*)ws + tg_wt_offset(s));
+  const int K = 27 * s.Ci, nb = 128 / (s.Do * s.Ho * s.Wo);
+  CUtensorMap xmap, wtmap;
+  {
+    const cuuint64_t dims[5] = {(cuuint64_t)s.Ci, (cuuint64_t)s.W, (cuuint64_t)s.H,
+                                (cuuint64_t)s.D, (cuuint64_t)s.B};
+    const cuuint32_t box[5] = {64, (cuuint32_t)(2 * s.Wo), (cuuint32_t)(2 * s.Ho),
+                               (cuuint32_t)(2 * s.Do), (cuuint32_t)nb};
+    const cuuint32_t estr[5] = {1, 2, 2, 2, 1};
+    const cuuint64_t wdims[2] = {(cuuint64_t)K, (cuuint64_t)s.Co};
+    const cuuint32_t wbox[2] = {64, 128}, westr[2] = {1, 1};
+    if (!bf16_tmap(&xmap, x, 5, dims, box, estr, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !bf16_tmap(&wtmap, wt, 2, wdims, wbox, westr, CU_TENSOR_MAP_SWIZZLE_128B))
+      return -1;
+  }
+  k_conv_wt<<<dim3((unsigned)((K + 31) / 32), (unsigned)((s.Co + 31) / 32)), 256, 0, st>>>(
+      w, K, s.Co, wt);
+  static std::atomic<bool> done[kConvMaxDevices];
+  const int smem = 1024 + kTgStages * kTgStageBytes + 128;
+  if (fp_smem_once(k_conv_tg_fwd, smem, done) != cudaSuccess) return DM_ERR_CUDA;
+  const int tps = tg_tps(s), sp = tg_splits(s);
+  k_conv_tg_fwd<<<dim3((unsigned)tg_tiles(s), (unsigned)sp), 128, smem, st>>>(
+      xmap, wtmap, s, tps, part, conv_status_ptr());
+  const int64_t n = s.M * s.Co;
+  k_fwd_reduce<<<(unsigned)std::min<int64_t>((n / 4 + 255) / 256, 148 * 16), 256, 0, st>>>(
+      part, sp, n, s.Co, bias, pre, act);
+  count_launches(3);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+// Data gradient of a tap-GEMM layer: dcol = dP W^T per (m tile, 4 taps) into the
+// workspace, then the fixed-order col2im gather into dx.  -1: not taken.
+static int tg_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* dcol, float* dx,
+                    bf16* dxb, cudaStream_t st) {
+  CUtensorMap dmap, wmap;
+  const cuuint64_t ddims[2] = {(cuuint64_t)s.Co, (cuuint64_t)s.M};
+  const cuuint64_t wdims[2] = {(cuuint64_t)s.Co, (cuuint64_t)(27 * s.Ci)};
+  const cuuint32_t dbox[2] = {64, 128}, wbox[2] = {64, 256}, estr[2] = {1, 1};
+  if (!bf16_tmap(&dmap, dp, 2, ddims, dbox, estr, CU_TENSOR_MAP_SWIZZLE_128B) ||
+      !bf16_tmap(&wmap, w, 2, wdims, wbox, estr, CU_TENSOR_MAP_SWIZZLE_128B))
+    return -1;
+  static std::atomic<bool> done[kConvMaxDevices];
+  if (fp_smem_once(k_conv_tg_dgrad, kTgDgradSmem, done) != cudaSuccess) return DM_ERR_CUDA;
+  k_conv_tg_dgrad<<<dim3((unsigned)((s.M + 127) / 128), (27 * s.Ci + 255) / 256), 128,
+                    kTgDgradSmem, st>>>(dmap, wmap, s, dcol, conv_status_ptr());
+  const int64_t n = (int64_t)s.B * s.D * s.H * s.W * 16;
+  k_conv_col2im<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(
+      dcol, s, dx, dxb);
+  count_launches(2);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st, void* ws = nullptr,
                         size_t ws_bytes = 0) {
+  if (tg_layer(s) && ws && ws_bytes >= conv_fwd_ws_bytes(s) && aligned16(x) && aligned16(w) &&
+      aligned16(pre) && aligned16(act) && aligned16(ws)) {
+    const int rc = tg_forward(s, x, w, bias, pre, act, ws, st);
+    if (rc != -1) return rc;
+  }
   if (s2d_layer(s, x) && s.W % 8 == 0 && aligned16(x) && aligned16(pre) && aligned16(act)) {
     const cudaError_t e = s.Co == 16 ? s2d_fwd_launch<16>(s, x, w, bias, pre, act, st)
                                      : s2d_fwd_launch<32>(s, x, w, bias, pre, act, st);
@@ -1529,6 +1621,11 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
   // data gradient: the eight parity classes of the input voxels in one launch
   if (dx || dx_b) {
     int rc = DM_OK;
+    if (tg_layer(s) && aligned16(dp) && aligned16(w) && aligned16(part) &&
+        aligned16(dx_b ? (void*)dx_b : (void*)dx)) {
+      rc = tg_dgrad(s, dp, w, part, dx, dx_b, st);
+      if (rc != -1) return rc;
+    }
     if (fp_dgrad(s, dp, w, dx, dx_b, st, rc)) return rc;
     ClsSet set;
     int64_t max_rows = 0, max_red = 0;

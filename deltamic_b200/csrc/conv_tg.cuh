@@ -1,0 +1,261 @@
+// Tap-GEMM forward for layers with 64 input channels and few output voxels per
+// image (the encoder's last layer, 64 -> 128 at 4^3 outputs), included by conv.cu.
+//
+// A tap's 64 input channels are one 128-byte row, so for tap (kd, kh, kw) the A tile
+// of 128 output voxels (whole images: 128 / (Do Ho Wo) of them) is one TMA box of x
+// with a traversal stride of 2 along W, H and D, starting at input (kw - 1, kh - 1,
+// kd - 1): rows in output-voxel order, 64 channels each, written with the 128-byte
+// swizzle -- the canonical K-major SW128 operand (8-row groups 1024 bytes apart,
+// K = 16 steps 32 bytes further along the row).  The B tile is the tap's 64 rows of
+// W^T (128 output channels x 64, the same layout), from a transposed copy of W.  The
+// 27 taps are split over blockIdx.y; each block accumulates its taps in TMEM and
+// writes FP32 partials part[split][m][co], added in split order with the bias and
+// GELU by k_fwd_reduce.  No gathers: the TMA engine fetches the taps, one thread
+// issues copies and MMAs through a ring of stages.
+#pragma once
+
+namespace dm {
+
+constexpr int kTgStages = 3;
+constexpr int kTgStageBytes = 2 * 128 * 128;  // A and B tiles, 128 rows x 128 bytes each
+
+// SW128 K-major descriptor: start address, LBO 16 bytes (unused by this layout),
+// SBO 1024 bytes (8-row groups), version 1, layout type 2 (128-byte swizzle).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) |
+         ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// W[27 * 64 rows][Co] -> wt[Co][27 * 64] (rows of W^T 128-byte aligned).
+__global__ void __launch_bounds__(256) k_conv_wt(const bf16* __restrict__ w, int K, int Co,
+                                                 bf16* __restrict__ wt) {
+  __shared__ bf16 t[32][33];
+  const int k0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < 32; r += 8)
+    if (k0 + r < K && c0 + tx < Co) t[r][tx] = w[(size_t)(k0 + r) * Co + c0 + tx];
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8)
+    if (c0 + r < Co && k0 + tx < K) wt[(size_t)(c0 + r) * K + k0 + tx] = t[tx][r];
+}
+
+// Block (m tile, split): taps [split * tps, ..) of output rows [128 m, 128 m + 128).
+// 128 threads: thread 0 issues, then all four warps read their TMEM lane quarter.
+__global__ void __launch_bounds__(128) k_conv_tg_fwd(const __grid_constant__ CUtensorMap xmap,
+                                                     const __grid_constant__ CUtensorMap wtmap,
+                                                     ConvShape s, int tps, float* __restrict__ part,
+                                                     int* err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t* const full = (uint64_t*)(smem + kTgStages * kTgStageBytes);
+  uint64_t* const empty = full + kTgStages;
+  uint64_t* const done = empty + kTgStages;
+  uint32_t* const slot = (uint32_t*)(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int per_img = s.Do * s.Ho * s.Wo, nb = 128 / per_img;
+  const int b0 = blockIdx.x * nb;
+  const int t0 = blockIdx.y * tps, nt = min(27, t0 + tps) - t0;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTgStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(slot, 128);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+
+  int lost = 0;  // thread 0: a wait gave up (copies may be in flight)
+  if (threadIdx.x == 0) {
+    auto load = [&](int i) {
+      const int st = i % kTgStages, tap = t0 + i;
+      const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+      uint8_t* a = smem + st * kTgStageBytes;
+      mbar_expect_tx(&full[st], kTgStageBytes);
+      tma_load_5d(a, &xmap, 0, kw - 1, kh - 1, kd - 1, b0, &full[st]);
+      tma_load_2d(a + 128 * 128, &wtmap, tap * 64, 0, &full[st]);
+    };
+    for (int i = 0; i < nt && i < kTgStages; ++i) load(i);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 128>();  // both K-major
+    for (int i = 0; i < nt; ++i) {
+      const int st = i % kTgStages;
+      if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((i / kTgStages) & 1), err)) {
+        lost = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t a = smem_u32(smem + st * kTgStageBytes), b = a + 128 * 128;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)  // K = 64 channels: four K = 16 steps, 32 bytes apart
+        tc::mma_bf16(tmem, sw128_desc(a + 32 * kk), sw128_desc(b + 32 * kk), idesc,
+                     i > 0 || kk > 0);
+      tc::commit(&empty[st]);
+      if (i + kTgStages < nt) {  // refill this stage once its MMAs are done
+        if (!mbar_wait_sleep_bounded(&empty[st], (uint32_t)((i / kTgStages) & 1), err)) {
+          lost = 1;
+          break;
+        }
+        load(i + kTgStages);
+      }
+    }
+    tc::commit(done);  // every MMA issued so far
+  }
+  const bool ok = mbar_wait_block(done, 0u, err, lost == 0);
+  tc::fence_after_sync();
+  const int row = warp * 32 + lane;
+  const int64_t m = (int64_t)blockIdx.x * 128 + row;
+  const bool live = ok && m < s.M;
+  float* dst = part + ((int64_t)blockIdx.y * s.M + m) * 128;
+#pragma unroll 1
+  for (int c = 0; c < 128; c += 16) {
+    float v[16];
+    tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (!live) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      *(float4*)(dst + c + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
+  // a copy whose wait gave up: wait for every issued stage once more before leaving
+  if (threadIdx.x == 0 && lost)
+    for (int i = 0; i < kTgStages; ++i) mbar_wait_sleep_bounded(&full[i], 0u, err, 1u);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, 128);
+  }
+}
+
+// Data gradient of a tap-GEMM layer in two steps.  dcol[m][tap * 64 + ci] = sum_co
+// dP[m][co] W[tap * 64 + ci][co] as a GEMM per (m tile, group of four taps): A = the
+// dP tile (128 x 128 channels, two SW128 K halves), B = the group's 256 rows of W
+// (the same layout: W rows are K-major in co), N = 256, D in TMEM, FP32 out.  Then
+// k_conv_col2im gathers dX[voxel][ci] = the sum over the voxel's taps (fixed order)
+// of dcol at the output voxel each reaches.  Both operands K-major SW128.
+constexpr int kTgDgradSmem = 1024 + 2 * 128 * 128 + 2 * 256 * 128 + 64;
+
+__global__ void __launch_bounds__(128) k_conv_tg_dgrad(const __grid_constant__ CUtensorMap dmap,
+                                                       const __grid_constant__ CUtensorMap wmap,
+                                                       ConvShape s, float* __restrict__ dcol,
+                                                       int* err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint8_t* const A = smem;                       // [2 K halves][128 rows][128 B]
+  uint8_t* const Bt = smem + 2 * 128 * 128;      // [2 K halves][256 rows][128 B]
+  uint64_t* const bar = (uint64_t*)(Bt + 2 * 256 * 128);  // [0] loads, [1] MMAs
+  uint32_t* const slot = (uint32_t*)(bar + 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * 128, g0 = blockIdx.y * 256;
+  const int K = 27 * 64;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(slot, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+  bool lok = true;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar[0], 2 * 128 * 128 + 2 * 256 * 128);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      tma_load_2d(A + h * 128 * 128, &dmap, 64 * h, m0, &bar[0]);
+      tma_load_2d(Bt + h * 256 * 128, &wmap, 64 * h, g0, &bar[0]);
+    }
+    lok = mbar_wait_sleep_bounded(&bar[0], 0u, err);
+    if (lok) {
+      tc::fence_after_sync();
+      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 256>();  // both K-major
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+          tc::mma_bf16(tmem, sw128_desc(smem_u32(A + h * 128 * 128) + 32 * kk),
+                       sw128_desc(smem_u32(Bt + h * 256 * 128) + 32 * kk), idesc,
+                       h > 0 || kk > 0);
+    }
+    tc::commit(&bar[1]);  // also without MMAs, so the phase completes
+  }
+  const bool ok = mbar_wait_block(&bar[1], 0u, err, lok);
+  tc::fence_after_sync();
+  const int64_t m = (int64_t)m0 + warp * 32 + lane;
+  const bool live = ok && m < s.M;
+  const int ncol = min(256, K - g0);
+  float* dst = dcol + m * K + g0;
+#pragma unroll 1
+  for (int c = 0; c < 256; c += 16) {
+    float v[16];
+    tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (!live || c >= ncol) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      *(float4*)(dst + c + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
+  // a load wait that gave up: once more, so no copy lands after the block has left
+  if (threadIdx.x == 0 && !lok) mbar_wait_sleep_bounded(&bar[0], 0u, err);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, 256);
+  }
+}
+
+// dX[b, d, h, w, 4 c .. 4 c + 3] = sum over the taps reaching input (d, h, w) -- per
+// axis k = 1 from output d / 2 (d even) or k = 0, 2 from outputs (d + 1) / 2, (d - 1) / 2
+// (d odd), within the output extent -- of dcol[output][tap * 64 + ci], in tap order.
+__global__ void __launch_bounds__(256) k_conv_col2im(const float* __restrict__ dcol, ConvShape s,
+                                                     float* __restrict__ dx,
+                                                     bf16* __restrict__ dxb) {
+  const int64_t n = (int64_t)s.B * s.D * s.H * s.W * 16;  // (voxel, 4-channel group)
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int c4 = (int)(i & 15);
+    int64_t v = i >> 4;
+    const int w = (int)(v % s.W);
+    v /= s.W;
+    const int h = (int)(v % s.H);
+    v /= s.H;
+    const int d = (int)(v % s.D);
+    const int b = (int)(v / s.D);
+    const int pc[3] = {d, h, w}, no[3] = {s.Do, s.Ho, s.Wo};
+    int ks[3][2], os[3][2], nk[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      nk[a] = 0;
+      const int p = pc[a];
+      if ((p & 1) == 0) {
+        if (p / 2 < no[a]) { ks[a][0] = 1; os[a][0] = p / 2; nk[a] = 1; }
+      } else {
+        if ((p + 1) / 2 < no[a]) { ks[a][nk[a]] = 0; os[a][nk[a]] = (p + 1) / 2; ++nk[a]; }
+        ks[a][nk[a]] = 2; os[a][nk[a]] = (p - 1) / 2; ++nk[a];
+      }
+    }
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i0 = 0; i0 < nk[0]; ++i0)
+      for (int i1 = 0; i1 < nk[1]; ++i1)
+        for (int i2 = 0; i2 < nk[2]; ++i2) {
+          const int tap = (ks[0][i0] * 3 + ks[1][i1]) * 3 + ks[2][i2];
+          const int64_t mo = (((int64_t)b * s.Do + os[0][i0]) * s.Ho + os[1][i1]) * s.Wo + os[2][i2];
+          const float4 t = *(const float4*)(dcol + mo * (27 * 64) + tap * 64 + 4 * c4);
+          acc.x += t.x; acc.y += t.y; acc.z += t.z; acc.w += t.w;
+        }
+    const int64_t o = (((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * 64) + 4 * c4;
+    if (dxb) {
+      *(uint2*)(dxb + o) = make_uint2(pack2(__float2bfloat16(acc.x), __float2bfloat16(acc.y)),
+                                      pack2(__float2bfloat16(acc.z), __float2bfloat16(acc.w)));
+    } else {
+      *(float4*)(dx + o) = acc;
+    }
+  }
+}
+
+}  // namespace dm
