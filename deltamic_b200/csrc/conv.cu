@@ -1238,16 +1238,12 @@ static int tg_tps(const ConvShape& s) {
   return (int)((27 + sp - 1) / sp);
 }
 static int tg_splits(const ConvShape& s) { return (27 + tg_tps(s) - 1) / tg_tps(s); }
-static size_t tg_wt_offset(const ConvShape& s) {
-  return ((size_t)tg_splits(s) * s.M * s.Co * sizeof(float) + 1023) / 1024 * 1024;
-}
 
 size_t conv_fwd_ws_bytes(const ConvShape& s) {
   const int sp = fwd_splits(s);
   const size_t split = sp > 1 ? (size_t)sp * s.M * s.Co * sizeof(float) + 256 : 256;
   // a tap-GEMM layer may still take the split path (no tensor map): room for both
-  if (tg_layer(s))
-    return std::max(split, tg_wt_offset(s) + (size_t)27 * s.Ci * s.Co * sizeof(bf16) + 256);
+  if (tg_layer(s)) return std::max(split, (size_t)tg_splits(s) * s.M * s.Co * sizeof(float) + 256);
   return split;
 }
 
@@ -1457,38 +1453,63 @@ static cudaError_t s2d_wgrad_launch(const ConvShape& s, const bf16* x, const bf1
   return cudaGetLastError();
 }
 
-// Forward of a tap-GEMM layer: W^T into the workspace, the tap GEMM's partials, their
+// Forward of a tap-GEMM layer: the tap GEMM's partials into the workspace, their
 // fixed-order sum with the bias and GELU.  -1: not taken (no tensor map).
 static int tg_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                       float* pre, bf16* act, void* ws, cudaStream_t st) {
   float* part = (float*)ws;
-  bf16* wt = (bf16*)((char*)ws + tg_wt_offset(s));
   const int K = 27 * s.Ci, nb = 128 / (s.Do * s.Ho * s.Wo);
-  CUtensorMap xmap, wtmap;
+  CUtensorMap xmap, wmap;
   {
     const cuuint64_t dims[5] = {(cuuint64_t)s.Ci, (cuuint64_t)s.W, (cuuint64_t)s.H,
                                 (cuuint64_t)s.D, (cuuint64_t)s.B};
     const cuuint32_t box[5] = {64, (cuuint32_t)(2 * s.Wo), (cuuint32_t)(2 * s.Ho),
                                (cuuint32_t)(2 * s.Do), (cuuint32_t)nb};
     const cuuint32_t estr[5] = {1, 2, 2, 2, 1};
-    const cuuint64_t wdims[2] = {(cuuint64_t)K, (cuuint64_t)s.Co};
-    const cuuint32_t wbox[2] = {64, 128}, westr[2] = {1, 1};
+    const cuuint64_t wdims[2] = {(cuuint64_t)s.Co, (cuuint64_t)K};
+    const cuuint32_t wbox[2] = {64, 64}, westr[2] = {1, 1};
     if (!bf16_tmap(&xmap, x, 5, dims, box, estr, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !bf16_tmap(&wtmap, wt, 2, wdims, wbox, westr, CU_TENSOR_MAP_SWIZZLE_128B))
+        !bf16_tmap(&wmap, w, 2, wdims, wbox, westr, CU_TENSOR_MAP_SWIZZLE_128B))
       return -1;
   }
-  k_conv_wt<<<dim3((unsigned)((K + 31) / 32), (unsigned)((s.Co + 31) / 32)), 256, 0, st>>>(
-      w, K, s.Co, wt);
   static std::atomic<bool> done[kConvMaxDevices];
   const int smem = 1024 + kTgStages * kTgStageBytes + 128;
   if (fp_smem_once(k_conv_tg_fwd, smem, done) != cudaSuccess) return DM_ERR_CUDA;
   const int tps = tg_tps(s), sp = tg_splits(s);
   k_conv_tg_fwd<<<dim3((unsigned)tg_tiles(s), (unsigned)sp), 128, smem, st>>>(
-      xmap, wtmap, s, tps, part, conv_status_ptr());
+      xmap, wmap, s, tps, part, conv_status_ptr());
   const int64_t n = s.M * s.Co;
   k_fwd_reduce<<<(unsigned)std::min<int64_t>((n / 4 + 255) / 256, 148 * 16), 256, 0, st>>>(
       part, sp, n, s.Co, bias, pre, act);
-  count_launches(3);
+  count_launches(2);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+// Weight + bias gradient of a tap-GEMM layer: blocks (tap pair or bias, split over
+// m tiles), partials into part, ``used`` splits.  -1: not taken.
+static int tg_wgrad(const ConvShape& s, const bf16* x, const bf16* dp, float* part, int& used,
+                    cudaStream_t st) {
+  const int nb = 128 / (s.Do * s.Ho * s.Wo);
+  CUtensorMap xmap, dmap;
+  const cuuint64_t dims[5] = {(cuuint64_t)s.Ci, (cuuint64_t)s.W, (cuuint64_t)s.H,
+                              (cuuint64_t)s.D, (cuuint64_t)s.B};
+  const cuuint32_t box[5] = {64, (cuuint32_t)(2 * s.Wo), (cuuint32_t)(2 * s.Ho),
+                             (cuuint32_t)(2 * s.Do), (cuuint32_t)nb};
+  const cuuint32_t estr[5] = {1, 2, 2, 2, 1};
+  const cuuint64_t ddims[2] = {(cuuint64_t)s.Co, (cuuint64_t)s.M};
+  const cuuint32_t dbox[2] = {64, 128}, destr[2] = {1, 1};
+  if (!bf16_tmap(&xmap, x, 5, dims, box, estr, CU_TENSOR_MAP_SWIZZLE_128B) ||
+      !bf16_tmap(&dmap, dp, 2, ddims, dbox, destr, CU_TENSOR_MAP_SWIZZLE_128B))
+    return -1;
+  static std::atomic<bool> done[kConvMaxDevices];
+  if (fp_smem_once(k_conv_tg_wgrad, kTgWgradSmem, done) != cudaSuccess) return DM_ERR_CUDA;
+  const int64_t mtiles = (s.M + 127) / 128;
+  const int sp = (int)std::max<int64_t>(1, std::min<int64_t>({10, mtiles, (int64_t)wgrad_splits(s)}));
+  const int64_t per = (mtiles + sp - 1) / sp;
+  used = (int)((mtiles + per - 1) / per);
+  k_conv_tg_wgrad<<<dim3(15, (unsigned)used), 128, kTgWgradSmem, st>>>(xmap, dmap, s, (int)per,
+                                                                        part, conv_status_ptr());
+  count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
@@ -1606,6 +1627,11 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
     count_launches(1);
   } else if (int rc = DM_OK; fp_wgrad(s, x, dp, part, used, st, rc)) {
     if (rc != DM_OK) return rc;
+  } else if (int trc = tg_layer(s) && aligned16(x) && aligned16(dp) && aligned16(part)
+                           ? tg_wgrad(s, x, dp, part, used, st)
+                           : -1;
+             trc != -1) {
+    if (trc != DM_OK) return trc;
   } else {
     const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
     used = (int)((s.M + per - 1) / per);

@@ -7,7 +7,8 @@
 // kd - 1): rows in output-voxel order, 64 channels each, written with the 128-byte
 // swizzle -- the canonical K-major SW128 operand (8-row groups 1024 bytes apart,
 // K = 16 steps 32 bytes further along the row).  The B tile is the tap's 64 rows of
-// W^T (128 output channels x 64, the same layout), from a transposed copy of W.  The
+// W, read MN-major (two boxes of 64 output channels; 8-row K groups 1024 bytes
+// apart, a K = 16 step 2048 bytes).  The
 // 27 taps are split over blockIdx.y; each block accumulates its taps in TMEM and
 // writes FP32 partials part[split][m][co], added in split order with the bias and
 // GELU by k_fwd_reduce.  No gathers: the TMA engine fetches the taps, one thread
@@ -26,23 +27,17 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
          ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// W[27 * 64 rows][Co] -> wt[Co][27 * 64] (rows of W^T 128-byte aligned).
-__global__ void __launch_bounds__(256) k_conv_wt(const bf16* __restrict__ w, int K, int Co,
-                                                 bf16* __restrict__ wt) {
-  __shared__ bf16 t[32][33];
-  const int k0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int r = ty; r < 32; r += 8)
-    if (k0 + r < K && c0 + tx < Co) t[r][tx] = w[(size_t)(k0 + r) * Co + c0 + tx];
-  __syncthreads();
-  for (int r = ty; r < 32; r += 8)
-    if (c0 + r < Co && k0 + tx < K) wt[(size_t)(c0 + r) * K + k0 + tx] = t[tx][r];
+// MN-major SW128 descriptor: 64-element MN groups ``lbo`` bytes apart, 8-row K
+// groups 1024 bytes apart (a K = 16 step is 2048 bytes), layout type 2.
+__device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) | (2ull << 61);
 }
 
 // Block (m tile, split): taps [split * tps, ..) of output rows [128 m, 128 m + 128).
 // 128 threads: thread 0 issues, then all four warps read their TMEM lane quarter.
 __global__ void __launch_bounds__(128) k_conv_tg_fwd(const __grid_constant__ CUtensorMap xmap,
-                                                     const __grid_constant__ CUtensorMap wtmap,
+                                                     const __grid_constant__ CUtensorMap wmap,
                                                      ConvShape s, int tps, float* __restrict__ part,
                                                      int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -78,10 +73,12 @@ __global__ void __launch_bounds__(128) k_conv_tg_fwd(const __grid_constant__ CUt
       uint8_t* a = smem + st * kTgStageBytes;
       mbar_expect_tx(&full[st], kTgStageBytes);
       tma_load_5d(a, &xmap, 0, kw - 1, kh - 1, kd - 1, b0, &full[st]);
-      tma_load_2d(a + 128 * 128, &wtmap, tap * 64, 0, &full[st]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h)  // W rows of the tap, 64 output channels per box
+        tma_load_2d(a + 128 * 128 + h * 64 * 128, &wmap, 64 * h, tap * 64, &full[st]);
     };
     for (int i = 0; i < nt && i < kTgStages; ++i) load(i);
-    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 128>();  // both K-major
+    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 128>() | (1u << 16);  // B MN-major
     for (int i = 0; i < nt; ++i) {
       const int st = i % kTgStages;
       if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((i / kTgStages) & 1), err)) {
@@ -91,9 +88,9 @@ __global__ void __launch_bounds__(128) k_conv_tg_fwd(const __grid_constant__ CUt
       tc::fence_after_sync();
       const uint32_t a = smem_u32(smem + st * kTgStageBytes), b = a + 128 * 128;
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk)  // K = 64 channels: four K = 16 steps, 32 bytes apart
-        tc::mma_bf16(tmem, sw128_desc(a + 32 * kk), sw128_desc(b + 32 * kk), idesc,
-                     i > 0 || kk > 0);
+      for (int kk = 0; kk < 4; ++kk)  // K = 64 channels: four K = 16 steps
+        tc::mma_bf16(tmem, sw128_desc(a + 32 * kk), sw128_mn_desc(b + 2048 * kk, 64 * 128),
+                     idesc, i > 0 || kk > 0);
       tc::commit(&empty[st]);
       if (i + kTgStages < nt) {  // refill this stage once its MMAs are done
         if (!mbar_wait_sleep_bounded(&empty[st], (uint32_t)((i / kTgStages) & 1), err)) {
@@ -255,6 +252,129 @@ __global__ void __launch_bounds__(256) k_conv_col2im(const float* __restrict__ d
     } else {
       *(float4*)(dx + o) = acc;
     }
+  }
+}
+
+// Weight + bias gradient of a tap-GEMM layer: block (pair, split) accumulates
+// dW[(2 pair + t) * 64 + ci][co] = sum_m X_tap[m][ci] dP[m][co], t < 2, over the m
+// tiles [split * per, ..): A = the two taps' forward A tiles (the same TMA boxes of
+// x) read MN-major (M = channel, K = voxel), B = the dP tile (two 64-channel SW128
+// halves) MN-major, M = N = 128, eight K = 16 steps per tile, two stages.  Block
+// pair = 14 takes an all-ones A: its row 0 is db.  Partials part[split][k][co] with
+// row Kp = db, summed in split order by k_sum_splits.
+constexpr int kTgWgStage = 4 * 128 * 128;  // A0, A1, B (two halves)
+constexpr int kTgWgradSmem = 1024 + 2 * kTgWgStage + 64;
+
+__global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ CUtensorMap xmap,
+                                                       const __grid_constant__ CUtensorMap dmap,
+                                                       ConvShape s, int per,
+                                                       float* __restrict__ part, int* err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t* const full = (uint64_t*)(smem + 2 * kTgWgStage);
+  uint64_t* const empty = full + 2;
+  uint64_t* const done = empty + 2;
+  uint32_t* const slot = (uint32_t*)(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = blockIdx.x, bias = pair == 14;
+  const int tap0 = 2 * pair, two = !bias && tap0 + 1 < 27;
+  const int nb = 128 / (s.Do * s.Ho * s.Wo);
+  const int64_t mtiles = (s.M + 127) / 128;
+  const int64_t j0 = (int64_t)blockIdx.y * per;
+  const int nt = j0 >= mtiles ? 0 : (int)(mtiles - j0 < per ? mtiles - j0 : per);
+  if (bias)  // all-ones A in both stages (a constant tile reads the same swizzled or not)
+    for (int i = threadIdx.x; i < 2 * 128 * 128 * 2 / 4; i += 128) {
+      const int st = i / (128 * 128 * 2 / 4), o = i % (128 * 128 * 2 / 4);
+      ((uint32_t*)(smem + st * kTgWgStage))[o] = 0x3F803F80u;
+    }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  fence_proxy_async();  // the ones -> the MMA's async-proxy reads
+  if (warp == 0) tc::tmem_alloc(slot, 128);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+  int lost = 0;
+  if (threadIdx.x == 0 && nt > 0) {
+    auto load = [&](int i) {
+      const int st = i & 1;
+      const int64_t j = j0 + i;
+      uint8_t* const a0 = smem + st * kTgWgStage;
+      const uint32_t bytes = (bias ? 0u : (two ? 2u : 1u) * 128 * 128) + 2 * 128 * 128;
+      mbar_expect_tx(&full[st], bytes);
+      if (!bias)
+        for (int t = 0; t < 1 + two; ++t) {
+          const int tap = tap0 + t, kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+          tma_load_5d(a0 + t * 128 * 128, &xmap, 0, kw - 1, kh - 1, kd - 1, (int)(j * nb),
+                      &full[st]);
+        }
+      for (int h = 0; h < 2; ++h)
+        tma_load_2d(a0 + (2 + h) * 128 * 128, &dmap, 64 * h, (int)(j * 128), &full[st]);
+    };
+    load(0);
+    if (nt > 1) load(1);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 128>() | (1u << 15) | (1u << 16);
+    for (int i = 0; i < nt; ++i) {
+      const int st = i & 1;
+      if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((i >> 1) & 1), err)) {
+        lost = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t a = smem_u32(smem + st * kTgWgStage), b = a + 2 * 128 * 128;
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk)  // 128 voxels: eight K = 16 steps of 16 rows
+        tc::mma_bf16(tmem, sw128_mn_desc(a + 2048 * kk, 128 * 128),
+                     sw128_mn_desc(b + 2048 * kk, 128 * 128), idesc, i > 0 || kk > 0);
+      tc::commit(&empty[st]);
+      if (i + 2 < nt) {
+        if (!mbar_wait_sleep_bounded(&empty[st], (uint32_t)((i >> 1) & 1), err)) {
+          lost = 1;
+          break;
+        }
+        load(i + 2);
+      }
+    }
+  }
+  if (threadIdx.x == 0) tc::commit(done);
+  const bool ok = mbar_wait_block(done, 0u, err, lost == 0);
+  tc::fence_after_sync();
+  float* const pw = part + (int64_t)blockIdx.y * (s.Kp + 1) * 128;
+  const int row = warp * 32 + lane;
+  int k = -1;
+  if (bias)
+    k = row == 0 ? s.Kp : -1;
+  else if (row < 64 || two)
+    k = (tap0 + (row >> 6)) * 64 + (row & 63);
+  const bool live = ok && k >= 0;
+#pragma unroll 1
+  for (int c = 0; c < 128; c += 16) {
+    float v[16];
+    tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (!live) continue;
+    if (nt == 0) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      *(float4*)(pw + (int64_t)k * 128 + c + 4 * q) =
+          make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
+  if (threadIdx.x == 0 && lost)
+    for (int i = 0; i < 2; ++i) mbar_wait_sleep_bounded(&full[i], 0u, err, 1u);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, 128);
   }
 }
 
