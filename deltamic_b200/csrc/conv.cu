@@ -1535,9 +1535,70 @@ static int tg_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* dc
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
+// Tile geometry of the persistent tap GEMM (conv_tg.cuh): 128 output voxels as
+// Wt = Wo voxels x Ht rows x Dt planes x nbt images.  False when Wo does not divide
+// 128 or the rows / planes do not fill a tile exactly.
+static bool tgp_geom(const ConvShape& s, TgGeom& g) {
+  if (s.Wo > 128 || 128 % s.Wo) return false;
+  g.wt = s.Wo;
+  const int r = 128 / s.Wo;
+  g.ht = r; g.nh = (s.Ho + r - 1) / r; g.dt = 1; g.nd = s.Do; g.nbt = 1;
+  if (s.Ho < r) {
+    if (r % s.Ho) return false;
+    g.ht = s.Ho; g.nh = 1;
+    const int r2 = r / s.Ho;
+    g.dt = r2; g.nd = (s.Do + r2 - 1) / r2;
+    if (s.Do < r2) {
+      if (r2 % s.Do) return false;
+      g.dt = s.Do; g.nd = 1; g.nbt = r2 / s.Do;
+    }
+  }
+  g.nbk = (s.B + g.nbt - 1) / g.nbt;
+  return g.wt * g.ht * g.dt * g.nbt == 128;
+}
+
+template <int CI, int CO>
+static int tgp_fwd_launch(const ConvShape& s, const TgGeom& g, const bf16* x, const bf16* w,
+                          const FwdEp& ep, cudaStream_t st) {
+  CUtensorMap xmap, wmap;
+  const cuuint64_t dims[5] = {(cuuint64_t)CI, (cuuint64_t)s.W, (cuuint64_t)s.H, (cuuint64_t)s.D,
+                              (cuuint64_t)s.B};
+  const cuuint32_t box[5] = {CI, (cuuint32_t)(2 * g.wt), (cuuint32_t)(2 * g.ht),
+                             (cuuint32_t)(2 * g.dt), (cuuint32_t)g.nbt};
+  const cuuint32_t estr[5] = {1, 2, 2, 2, 1};
+  const cuuint64_t wdims[2] = {(cuuint64_t)CO, (cuuint64_t)(27 * CI)};
+  const cuuint32_t wbox[2] = {CO, CI}, westr[2] = {1, 1};
+  const CUtensorMapSwizzle xs = CI == 16 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B;
+  const CUtensorMapSwizzle wsz = CO == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+  if (!bf16_tmap(&xmap, x, 5, dims, box, estr, xs) || !bf16_tmap(&wmap, w, 2, wdims, wbox, westr, wsz))
+    return -1;
+  using F = TgpFwd<CI, CO>;
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_tgp_fwd<CI, CO>;
+  if (fp_smem_once(k, F::kSmem, done) != cudaSuccess) return DM_ERR_CUDA;
+  const int64_t tiles = (int64_t)g.nbk * g.nd * g.nh;
+  const int per_sm = std::max(1, std::min({232448 / (F::kSmem + 1024), 512 / F::kCols, 12}));
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)per_sm * num_sms()));
+  k<<<grid, 160, F::kSmem, st>>>(xmap, wmap, s, g, ep, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
 int launch_conv_forward(const ConvShape& s, const bf16* x, const bf16* w, const float* bias,
                         float* pre, bf16* act, cudaStream_t st, void* ws = nullptr,
                         size_t ws_bytes = 0) {
+  {
+    TgGeom g;
+    const FwdEp ep{bias, pre, act, s.Co, 0, aligned16(pre) && aligned16(act)};
+    // 32 -> 64 channels: a tap's 64-byte rows keep the boxes large enough for the TMA
+    // engine (the 16-channel layer's 32-byte rows made its 27 boxes per tile slower
+    // than the footprint kernel: 68 against 60 us at batch 64, 32^3 in)
+    if (s.Ci == 32 && s.Co == 64 && tgp_geom(s, g) && ep.vec && aligned16(x) && aligned16(w)) {
+      const int rc = tgp_fwd_launch<32, 64>(s, g, x, w, ep, st);
+      if (rc != -1) return rc;
+    }
+  }
   if (tg_layer(s) && ws && ws_bytes >= conv_fwd_ws_bytes(s) && aligned16(x) && aligned16(w) &&
       aligned16(pre) && aligned16(act) && aligned16(ws)) {
     const int rc = tg_forward(s, x, w, bias, pre, act, ws, st);

@@ -378,4 +378,183 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent tap-GEMM forward for the middle layers (16 -> 32, 32 -> 64 channels).
+// A tap's A tile is one TMA box of 128 output voxels (Wt x Ht x Dt x nbt, traversal
+// stride 2) whose rows are CI channels (32 or 64 bytes, written with the swizzle of
+// that width: the K-major SW32 / SW64 operand, 8-row groups 8 rows apart); B is the
+// tap's CI rows of W read MN-major (CO = 32: 64-byte rows, SW64; CO = 64: SW128).
+// Warp 4 issues the boxes and the MMAs through a ring over the block's flat (tile,
+// tap) sequence; warps 0-3 take a tile's accumulator (two in TMEM, alternating) for
+// the bias + GELU epilogue while the next tile's MMAs run.
+
+// Layout type of an R-byte row swizzle (R = 32, 64, 128).
+__host__ __device__ constexpr uint32_t swz_code(int row_bytes) {
+  return row_bytes == 32 ? 6u : (row_bytes == 64 ? 4u : 2u);
+}
+// Swizzled K-major descriptor for R-byte rows (8-row groups 8 R bytes apart).
+template <int R>
+__device__ __forceinline__ uint64_t swk_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) |
+         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
+}
+// Swizzled MN-major descriptor for R-byte rows: MN groups lbo bytes apart, 8-row K
+// groups 8 R bytes apart.
+template <int R>
+__device__ __forceinline__ uint64_t swmn_desc(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
+}
+
+// Tile geometry of the persistent tap GEMM: Wt = Wo, Ht, Dt, nbt with Wt Ht Dt nbt = 128.
+struct TgGeom {
+  int wt, ht, dt, nbt;   // tile extents (voxels, rows, planes, images)
+  int nh, nd, nbk;       // tiles along h, d and images
+};
+
+template <int CI, int CO>
+struct TgpFwd {
+  static constexpr int kA = 128 * CI * 2;        // A tile bytes
+  static constexpr int kB = CI * CO * 2;         // B tile bytes
+  static constexpr int kStage = (kA + kB + 1023) / 1024 * 1024;
+  static constexpr int kStages = 6;
+  static constexpr int kSmem = 1024 + kStages * kStage + 256;
+  static constexpr int kCols = 2 * CO <= 32 ? 32 : (2 * CO <= 64 ? 64 : 128);  // two accumulators
+  static_assert(kSmem <= 227 * 1024, "stages above the shared-memory limit");
+};
+
+__device__ __forceinline__ void mbar_arrive1(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int CI, int CO>
+__global__ void __launch_bounds__(160) k_conv_tgp_fwd(const __grid_constant__ CUtensorMap xmap,
+                                                      const __grid_constant__ CUtensorMap wmap,
+                                                      ConvShape s, TgGeom g, FwdEp ep, int* err) {
+  using F = TgpFwd<CI, CO>;
+  constexpr int S = F::kStages;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t* const full = (uint64_t*)(smem + S * F::kStage);
+  uint64_t* const empty = full + S;
+  uint64_t* const tfull = empty + S;   // [2] accumulator complete
+  uint64_t* const tempty = tfull + 2;  // [2] accumulator read back (one arrival per warp)
+  uint64_t* const done = tempty + 2;
+  uint32_t* const slot = (uint32_t*)(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntiles = g.nbk * g.nd * g.nh;
+  const int nloc = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto tile_of = [&](int lt, int& b0, int& od0, int& oh0) {
+    int t = (int)blockIdx.x + lt * (int)gridDim.x;
+    oh0 = (t % g.nh) * g.ht;
+    t /= g.nh;
+    od0 = (t % g.nd) * g.dt;
+    b0 = (t / g.nd) * g.nbt;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 4);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(slot, F::kCols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      const int n = nloc * 27;
+      auto load = [&](int i) {
+        const int st = i % S, tap = i % 27;
+        int b0, od0, oh0;
+        tile_of(i / 27, b0, od0, oh0);
+        const int kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+        uint8_t* const a = smem + st * F::kStage;
+        mbar_expect_tx(&full[st], F::kA + F::kB);
+        tma_load_5d(a, &xmap, 0, kw - 1, 2 * oh0 - 1 + kh, 2 * od0 - 1 + kd, b0, &full[st]);
+        tma_load_2d(a + F::kA, &wmap, 0, tap * CI, &full[st]);
+      };
+      int issued = 0;  // loads issued (items 0 .. issued - 1)
+      for (; issued < n && issued < S; ++issued) load(issued);
+      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>() | (1u << 16);  // B MN-major
+      bool good = true;
+      for (int i = 0; i < n; ++i) {
+        const int st = i % S, lt = i / 27, tap = i % 27, acc = lt & 1;
+        if (tap == 0 && lt >= 2 &&
+            !mbar_wait_sleep_bounded(&tempty[acc], (uint32_t)(((lt >> 1) - 1) & 1), err)) {
+          good = false;
+          break;
+        }
+        if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((i / S) & 1), err)) {
+          good = false;
+          break;
+        }
+        tc::fence_after_sync();
+        const uint32_t a = smem_u32(smem + st * F::kStage), b = a + F::kA;
+#pragma unroll
+        for (int kk = 0; kk < CI / 16; ++kk)
+          tc::mma_bf16(tmem + (uint32_t)(acc * CO), swk_desc<2 * CI>(a + 32 * kk),
+                       swmn_desc<2 * CO>(b + 32 * CO * kk, F::kB), idesc, tap > 0 || kk > 0);
+        tc::commit(&empty[st]);
+        if (tap == 26) tc::commit(&tfull[acc]);
+        // refill the stage of item i - 1 (its MMAs run ahead of item i's)
+        if (i >= 1 && issued < n) {
+          const int p = i - 1;
+          if (!mbar_wait_sleep_bounded(&empty[p % S], (uint32_t)((p / S) & 1), err)) {
+            good = false;
+            break;
+          }
+          load(issued++);
+        }
+      }
+      tc::commit(done);
+      mbar_wait_sleep_bounded(done, 0u, err);  // every MMA issued is complete
+      if (!good)  // copies whose consumer never came: let them land
+        for (int i = 0; i < S; ++i) mbar_wait_sleep_bounded(&full[i], 0u, err, 1u);
+    }
+  } else {  // warps 0..3: epilogue, TMEM lane quarter = warp
+    const int row = warp * 32 + lane;
+    const int wl = row % g.wt, hl = (row / g.wt) % g.ht, dl = (row / (g.wt * g.ht)) % g.dt;
+    const int bl = row / (g.wt * g.ht * g.dt);
+    for (int lt = 0; lt < nloc; ++lt) {
+      const int acc = lt & 1;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait_sleep_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      if (lane != 0) mbar_wait_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      tc::fence_after_sync();
+      int b0, od0, oh0;
+      tile_of(lt, b0, od0, oh0);
+      const int b = b0 + bl, od = od0 + dl, oh = oh0 + hl;
+      const bool live = b < s.B && od < s.Do && oh < s.Ho && wl < s.Wo;
+      const int64_t m = (((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + wl;
+#pragma unroll
+      for (int c = 0; c < CO; c += 16) {
+        float v[16];
+        tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * CO + c), v);
+        if (live) ep.put16(m, c, 0, v);
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&tempty[acc]);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, F::kCols);
+  }
+}
+
 }  // namespace dm
