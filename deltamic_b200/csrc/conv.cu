@@ -1437,11 +1437,11 @@ static cudaError_t s2d_fwd_launch(const ConvShape& s, const bf16* x, const bf16*
   return cudaGetLastError();
 }
 
-template <int CO>
+template <int CO, bool VEC>
 static cudaError_t s2d_wgrad_launch(const ConvShape& s, const bf16* x, const bf16* dp,
                                     float* part, int splits, int& used, cudaStream_t st) {
   static std::atomic<bool> done[kConvMaxDevices];
-  auto k = k_conv_s2d_wgrad<CO>;
+  auto k = k_conv_s2d_wgrad<CO, VEC>;
   const int smem = S2dWgrad<CO>::kSmem;
   cudaError_t e = fp_smem_once(k, smem, done);
   if (e != cudaSuccess) return e;
@@ -1676,8 +1676,12 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
     const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);
     const int sp = (int)std::max<int64_t>(
         1, std::min<int64_t>({(int64_t)3 * num_sms(), tiles / 8, (int64_t)splits}));
-    const cudaError_t e = s.Co == 16 ? s2d_wgrad_launch<16>(s, x, dp, part, sp, used, st)
-                                     : s2d_wgrad_launch<32>(s, x, dp, part, sp, used, st);
+    const bool vec = s.W % 8 == 0 && aligned16(x);
+    const cudaError_t e =
+        s.Co == 16 ? (vec ? s2d_wgrad_launch<16, true>(s, x, dp, part, sp, used, st)
+                          : s2d_wgrad_launch<16, false>(s, x, dp, part, sp, used, st))
+                   : (vec ? s2d_wgrad_launch<32, true>(s, x, dp, part, sp, used, st)
+                          : s2d_wgrad_launch<32, false>(s, x, dp, part, sp, used, st));
     if (e != cudaSuccess) return DM_ERR_CUDA;
   } else if (conv1_direct(s)) {
     used = (int)std::max<int64_t>(1, std::min<int64_t>(splits, conv1_tiles_host(s)));

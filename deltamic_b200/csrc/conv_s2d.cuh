@@ -252,7 +252,10 @@ struct S2dWgrad {
 // zero, row Kp = db).  Per tile: the block footprint and dP tile are copied one tile
 // ahead (two stages), the footprint is expanded into the eight block-tap groups, and
 // eight MMAs (M = 128: group x parity, N = CO, K = 16 voxels) accumulate in TMEM.
-template <int CO>
+// VEC (W a multiple of 8, x 16-byte aligned): the footprint through registers as in
+// the forward -- tile it + 1's pieces are loaded before tile it's expansion and
+// stored after its MMAs are issued; else 4-byte cp.async copies.
+template <int CO, bool VEC>
 __global__ void __launch_bounds__(256) k_conv_s2d_wgrad(const bf16* __restrict__ x, ConvShape s,
                                                         const bf16* __restrict__ dp, int per,
                                                         float* __restrict__ part, int* err) {
@@ -270,7 +273,9 @@ __global__ void __launch_bounds__(256) k_conv_s2d_wgrad(const bf16* __restrict__
   const int64_t left = ntiles - t0;
   const int nt = left <= 0 ? 0 : (int)(left < per ? left : per);
 
-  // tile it's copies into stage st: block footprint and dP [co8][voxel]
+  // tile it's copies into stage st: block footprint (or, VEC, its pieces into pf) and
+  // dP [co8][voxel]
+  S2dPrefetch pf;
   auto load = [&](int it, int st) {
     int64_t t = t0 + it;
     const int ow0 = (int)(t % nwb) * 8;
@@ -278,7 +283,10 @@ __global__ void __launch_bounds__(256) k_conv_s2d_wgrad(const bf16* __restrict__
     const int oh0 = (int)(t % nhb) * 16;
     t /= nhb;
     const int od = (int)(t % s.Do), b = (int)(t / s.Do);
-    s2d_footprint(x, s, b, od, oh0, ow0, fps + st * kS2dFpBytes, 256);
+    if (VEC)
+      s2d_prefetch(x, s, b, od, oh0, ow0, pf);
+    else
+      s2d_footprint(x, s, b, od, oh0, ow0, fps + st * kS2dFpBytes, 256);
     uint8_t* const d = dps + st * F::kDpBytes;
     for (int e = threadIdx.x; e < (CO / 8) * 128; e += 256) {
       const int co8 = e % (CO / 8), ml = e / (CO / 8);
@@ -295,7 +303,10 @@ __global__ void __launch_bounds__(256) k_conv_s2d_wgrad(const bf16* __restrict__
     const int st = e / (F::kGroupBytes / 4), o = e % (F::kGroupBytes / 4);
     ((uint32_t*)(areg + st * F::kABytes + 8 * F::kGroupBytes))[o] = 0x3F803F80u;
   }
-  if (nt > 0) load(0, 0);
+  if (nt > 0) {
+    load(0, 0);
+    if (VEC) s2d_store(fps, pf);
+  }
   if (warp == 0) tc::tmem_alloc(slot, 32);
   if (threadIdx.x == 32) {
     mbar_init(&bar[0], 1);
@@ -344,6 +355,8 @@ __global__ void __launch_bounds__(256) k_conv_s2d_wgrad(const bf16* __restrict__
       tc::commit(&bar[st]);
     }
     issued = it + 1;
+    // the next tile's pieces: its footprint stage was expanded an iteration ago
+    if (VEC && it + 1 < nt) s2d_store(fps + (st ^ 1) * kS2dFpBytes, pf);
   }
   cp_async_wait_all();
   for (int it = issued >= 2 ? issued - 2 : 0; it < issued; ++it)

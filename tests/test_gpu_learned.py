@@ -20,13 +20,14 @@ def _bf(a):
                                    (1, 8, 8, 8, 32, 64), (2, 6, 6, 6, 64, 128),
                                    (3, 17, 15, 19, 8, 32), (1, 9, 7, 5, 128, 16),
                                    (2, 17, 23, 70, 1, 32), (1, 9, 11, 13, 1, 16),
-                                   (3, 8, 8, 8, 64, 128)])
+                                   (3, 8, 8, 8, 64, 128), (1, 9, 7, 14, 32, 64)])
 def test_conv_kernels_match_oracle(shape):
     """Forward, weight, bias and data gradients of the tcgen05 implicit GEMMs (and
     of the direct single-channel kernels, Ci = 1) against the float64 oracle on the
     same BF16 inputs (odd extents: ragged row tiles and parity classes; Ci = 8 and
-    128: the vector and element gathers; 3 x 8^3 x 64 -> 128: the tap-GEMM forward with a
-    ragged last tile)."""
+    128: the vector and element gathers; 3 x 8^3 x 64 -> 128: the tap-GEMM kernels with a
+    ragged last tile; 1 x 8^3 x 32 -> 64 the persistent tap-GEMM forward and 9 x 7 x 14 x 32
+    -> 64 (7 output columns) the footprint forward)."""
     from deltamic_b200.learned import _kp, conv3d_s2, conv_status_check
     B, D, H, W, Ci, Co = shape
     rng = np.random.default_rng(Ci)
