@@ -1485,32 +1485,49 @@ static int tg_forward(const ConvShape& s, const bf16* x, const bf16* w, const fl
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
-// Weight + bias gradient of a tap-GEMM layer: blocks (tap pair or bias, split over
-// m tiles), partials into part, ``used`` splits.  -1: not taken.
-static int tg_wgrad(const ConvShape& s, const bf16* x, const bf16* dp, float* part, int& used,
-                    cudaStream_t st) {
-  const int nb = 128 / (s.Do * s.Ho * s.Wo);
+static bool tgp_geom(const ConvShape& s, TgGeom& g);
+
+// Weight + bias gradient on the tap-GEMM kernel: blocks (tap group or bias, split
+// over m tiles), partials into part, ``used`` splits.  -1: not taken.
+template <int CI, int CO>
+static int tg_wgrad_t(const ConvShape& s, const TgGeom& g, const bf16* x, const bf16* dp,
+                      float* part, int& used, cudaStream_t st) {
   CUtensorMap xmap, dmap;
-  const cuuint64_t dims[5] = {(cuuint64_t)s.Ci, (cuuint64_t)s.W, (cuuint64_t)s.H,
-                              (cuuint64_t)s.D, (cuuint64_t)s.B};
-  const cuuint32_t box[5] = {64, (cuuint32_t)(2 * s.Wo), (cuuint32_t)(2 * s.Ho),
-                             (cuuint32_t)(2 * s.Do), (cuuint32_t)nb};
+  const cuuint64_t dims[5] = {(cuuint64_t)CI, (cuuint64_t)s.W, (cuuint64_t)s.H, (cuuint64_t)s.D,
+                              (cuuint64_t)s.B};
+  const cuuint32_t box[5] = {CI, (cuuint32_t)(2 * g.wt), (cuuint32_t)(2 * g.ht),
+                             (cuuint32_t)(2 * g.dt), (cuuint32_t)g.nbt};
   const cuuint32_t estr[5] = {1, 2, 2, 2, 1};
-  const cuuint64_t ddims[2] = {(cuuint64_t)s.Co, (cuuint64_t)s.M};
+  const cuuint64_t ddims[2] = {(cuuint64_t)CO, (cuuint64_t)s.M};
   const cuuint32_t dbox[2] = {64, 128}, destr[2] = {1, 1};
-  if (!bf16_tmap(&xmap, x, 5, dims, box, estr, CU_TENSOR_MAP_SWIZZLE_128B) ||
+  const CUtensorMapSwizzle xs = CI == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+  if (!bf16_tmap(&xmap, x, 5, dims, box, estr, xs) ||
       !bf16_tmap(&dmap, dp, 2, ddims, dbox, destr, CU_TENSOR_MAP_SWIZZLE_128B))
     return -1;
+  using F = TgWgrad<CI, CO>;
   static std::atomic<bool> done[kConvMaxDevices];
-  if (fp_smem_once(k_conv_tg_wgrad, kTgWgradSmem, done) != cudaSuccess) return DM_ERR_CUDA;
-  const int64_t mtiles = (s.M + 127) / 128;
-  const int sp = (int)std::max<int64_t>(1, std::min<int64_t>({10, mtiles, (int64_t)wgrad_splits(s)}));
+  auto k = k_conv_tg_wgrad<CI, CO>;
+  if (fp_smem_once(k, F::kSmem, done) != cudaSuccess) return DM_ERR_CUDA;
+  const int64_t mtiles = (int64_t)g.nbk * g.nd * g.nh;
+  // about one wave: blocks per SM from shared memory, over the tap groups + bias
+  const int per_sm = std::max(1, 232448 / (F::kSmem + 1024));
+  const int64_t cap = std::max<int64_t>(1, (int64_t)num_sms() * per_sm / (F::kGroups + 1));
+  const int sp = (int)std::max<int64_t>(1, std::min<int64_t>({cap, mtiles, (int64_t)wgrad_splits(s)}));
   const int64_t per = (mtiles + sp - 1) / sp;
   used = (int)((mtiles + per - 1) / per);
-  k_conv_tg_wgrad<<<dim3(15, (unsigned)used), 128, kTgWgradSmem, st>>>(xmap, dmap, s, (int)per,
-                                                                        part, conv_status_ptr());
+  k<<<dim3(F::kGroups + 1, (unsigned)used), 128, F::kSmem, st>>>(xmap, dmap, s, g, (int)per, part,
+                                                                   conv_status_ptr());
   count_launches(1);
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
+static int tg_wgrad(const ConvShape& s, const bf16* x, const bf16* dp, float* part, int& used,
+                    cudaStream_t st) {
+  TgGeom g;
+  if (!tgp_geom(s, g) || !aligned16(x) || !aligned16(dp) || !aligned16(part)) return -1;
+  if (s.Ci == 64 && s.Co == 128) return tg_wgrad_t<64, 128>(s, g, x, dp, part, used, st);
+  if (s.Ci == 32 && s.Co == 64) return tg_wgrad_t<32, 64>(s, g, x, dp, part, used, st);
+  return -1;
 }
 
 // Data gradient of a tap-GEMM layer: dcol = dP W^T per (m tile, 4 taps) into the
@@ -1690,13 +1707,10 @@ int launch_conv_backward(const ConvShape& s, const bf16* x, const bf16* w, const
     else
       k_conv1_wgrad<32><<<used, 256, 0, st>>>(x, s, dp, part);
     count_launches(1);
+  } else if (int trc = tg_wgrad(s, x, dp, part, used, st); trc != -1) {
+    if (trc != DM_OK) return trc;
   } else if (int rc = DM_OK; fp_wgrad(s, x, dp, part, used, st, rc)) {
     if (rc != DM_OK) return rc;
-  } else if (int trc = tg_layer(s) && aligned16(x) && aligned16(dp) && aligned16(part)
-                           ? tg_wgrad(s, x, dp, part, used, st)
-                           : -1;
-             trc != -1) {
-    if (trc != DM_OK) return trc;
   } else {
     const int64_t per = ((s.M + splits - 1) / splits + kBK - 1) / kBK * kBK;
     used = (int)((s.M + per - 1) / per);

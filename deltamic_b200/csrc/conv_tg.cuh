@@ -34,6 +34,24 @@ __device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t saddr, uint32_t lbo) 
          ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) | (2ull << 61);
 }
 
+// Layout type of an R-byte row swizzle (R = 32, 64, 128).
+__host__ __device__ constexpr uint32_t swz_code(int row_bytes) {
+  return row_bytes == 32 ? 6u : (row_bytes == 64 ? 4u : 2u);
+}
+// Swizzled K-major descriptor for R-byte rows (8-row groups 8 R bytes apart).
+template <int R>
+__device__ __forceinline__ uint64_t swk_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) |
+         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
+}
+// Swizzled MN-major descriptor for R-byte rows: MN groups lbo bytes apart, 8-row K
+// groups 8 R bytes apart.
+template <int R>
+__device__ __forceinline__ uint64_t swmn_desc(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
+}
+
 // Block (m tile, split): taps [split * tps, ..) of output rows [128 m, 128 m + 128).
 // 128 threads: thread 0 issues, then all four warps read their TMEM lane quarter.
 __global__ void __launch_bounds__(128) k_conv_tg_fwd(const __grid_constant__ CUtensorMap xmap,
@@ -255,37 +273,54 @@ __global__ void __launch_bounds__(256) k_conv_col2im(const float* __restrict__ d
   }
 }
 
-// Weight + bias gradient of a tap-GEMM layer: block (pair, split) accumulates
-// dW[(2 pair + t) * 64 + ci][co] = sum_m X_tap[m][ci] dP[m][co], t < 2, over the m
-// tiles [split * per, ..): A = the two taps' forward A tiles (the same TMA boxes of
-// x) read MN-major (M = channel, K = voxel), B = the dP tile (two 64-channel SW128
-// halves) MN-major, M = N = 128, eight K = 16 steps per tile, two stages.  Block
-// pair = 14 takes an all-ones A: its row 0 is db.  Partials part[split][k][co] with
-// row Kp = db, summed in split order by k_sum_splits.
-constexpr int kTgWgStage = 4 * 128 * 128;  // A0, A1, B (two halves)
-constexpr int kTgWgradSmem = 1024 + 2 * kTgWgStage + 64;
+// Tile geometry of the persistent tap GEMM: Wt = Wo, Ht, Dt, nbt with Wt Ht Dt nbt = 128.
+struct TgGeom {
+  int wt, ht, dt, nbt;   // tile extents (voxels, rows, planes, images)
+  int nh, nd, nbk;       // tiles along h, d and images
+};
 
+// Weight + bias gradient of a tap-GEMM layer: block (group, split) accumulates
+// dW[(TPG group + t) * CI + ci][co] = sum_m X_tap[m][ci] dP[m][co], t < TPG = 128 / CI
+// taps, over the m tiles [split * per, ..) of the forward's tile geometry: A = the
+// TPG taps' forward A tiles (the same TMA boxes of x) read MN-major (M = tap x
+// channel, MN groups of CI channels one tile apart, K = voxel), B = the tile's dP
+// rows (the tile's voxels are consecutive in m), 64-channel SW128 boxes, MN-major;
+// eight K = 16 steps per tile, two stages.  The block past the last tap group takes
+// an all-ones A: its row 0 is db.  Partials part[split][k][co] with row Kp = db,
+// summed in split order by k_sum_splits.
+template <int CI, int CO>
+struct TgWgrad {
+  static constexpr int kTpg = 128 / CI;                   // taps per group
+  static constexpr int kGroups = (27 + kTpg - 1) / kTpg;  // + 1 bias block
+  static constexpr int kATile = 128 * CI * 2;
+  static constexpr int kBTile = 128 * 128;                // one 64-channel dP box
+  static constexpr int kStage = kTpg * kATile + (CO / 64) * kBTile;
+  static constexpr int kSmem = 1024 + 2 * kStage + 64;
+};
+
+template <int CI, int CO>
 __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ CUtensorMap xmap,
                                                        const __grid_constant__ CUtensorMap dmap,
-                                                       ConvShape s, int per,
+                                                       ConvShape s, TgGeom g, int per,
                                                        float* __restrict__ part, int* err) {
+  using F = TgWgrad<CI, CO>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  uint64_t* const full = (uint64_t*)(smem + 2 * kTgWgStage);
+  uint64_t* const full = (uint64_t*)(smem + 2 * F::kStage);
   uint64_t* const empty = full + 2;
   uint64_t* const done = empty + 2;
   uint32_t* const slot = (uint32_t*)(done + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int pair = blockIdx.x, bias = pair == 14;
-  const int tap0 = 2 * pair, two = !bias && tap0 + 1 < 27;
-  const int nb = 128 / (s.Do * s.Ho * s.Wo);
-  const int64_t mtiles = (s.M + 127) / 128;
+  const int grp = blockIdx.x, bias = grp == F::kGroups;
+  const int tap0 = grp * F::kTpg;
+  const int ntap = bias ? 0 : (27 - tap0 < F::kTpg ? 27 - tap0 : F::kTpg);
+  const int64_t mtiles = (int64_t)g.nbk * g.nd * g.nh;
   const int64_t j0 = (int64_t)blockIdx.y * per;
   const int nt = j0 >= mtiles ? 0 : (int)(mtiles - j0 < per ? mtiles - j0 : per);
   if (bias)  // all-ones A in both stages (a constant tile reads the same swizzled or not)
-    for (int i = threadIdx.x; i < 2 * 128 * 128 * 2 / 4; i += 128) {
-      const int st = i / (128 * 128 * 2 / 4), o = i % (128 * 128 * 2 / 4);
-      ((uint32_t*)(smem + st * kTgWgStage))[o] = 0x3F803F80u;
+    for (int i = threadIdx.x; i < 2 * F::kTpg * F::kATile / 4; i += 128) {
+      const int st = i / (F::kTpg * F::kATile / 4), o = i % (F::kTpg * F::kATile / 4);
+      ((uint32_t*)(smem + st * F::kStage))[o] = 0x3F803F80u;
     }
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2; ++i) {
@@ -296,7 +331,7 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
     fence_mbar_init();
   }
   fence_proxy_async();  // the ones -> the MMA's async-proxy reads
-  if (warp == 0) tc::tmem_alloc(slot, 128);
+  if (warp == 0) tc::tmem_alloc(slot, CO < 32 ? 32 : CO);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -305,22 +340,24 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
   if (threadIdx.x == 0 && nt > 0) {
     auto load = [&](int i) {
       const int st = i & 1;
-      const int64_t j = j0 + i;
-      uint8_t* const a0 = smem + st * kTgWgStage;
-      const uint32_t bytes = (bias ? 0u : (two ? 2u : 1u) * 128 * 128) + 2 * 128 * 128;
-      mbar_expect_tx(&full[st], bytes);
-      if (!bias)
-        for (int t = 0; t < 1 + two; ++t) {
-          const int tap = tap0 + t, kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
-          tma_load_5d(a0 + t * 128 * 128, &xmap, 0, kw - 1, kh - 1, kd - 1, (int)(j * nb),
-                      &full[st]);
-        }
-      for (int h = 0; h < 2; ++h)
-        tma_load_2d(a0 + (2 + h) * 128 * 128, &dmap, 64 * h, (int)(j * 128), &full[st]);
+      int t = (int)(j0 + i);
+      const int oh0 = (t % g.nh) * g.ht;
+      t /= g.nh;
+      const int od0 = (t % g.nd) * g.dt, b0 = (t / g.nd) * g.nbt;
+      const int64_t m0 = (((int64_t)b0 * s.Do + od0) * s.Ho + oh0) * s.Wo;
+      uint8_t* const a0 = smem + st * F::kStage;
+      mbar_expect_tx(&full[st], (uint32_t)(ntap * F::kATile + (CO / 64) * F::kBTile));
+      for (int u = 0; u < ntap; ++u) {
+        const int tap = tap0 + u, kd = tap / 9, kh = (tap / 3) % 3, kw = tap % 3;
+        tma_load_5d(a0 + u * F::kATile, &xmap, 0, kw - 1, 2 * oh0 - 1 + kh, 2 * od0 - 1 + kd, b0,
+                    &full[st]);
+      }
+      for (int h = 0; h < CO / 64; ++h)
+        tma_load_2d(a0 + F::kTpg * F::kATile + h * F::kBTile, &dmap, 64 * h, (int)m0, &full[st]);
     };
     load(0);
     if (nt > 1) load(1);
-    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 128>() | (1u << 15) | (1u << 16);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>() | (1u << 15) | (1u << 16);
     for (int i = 0; i < nt; ++i) {
       const int st = i & 1;
       if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((i >> 1) & 1), err)) {
@@ -328,11 +365,11 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
         break;
       }
       tc::fence_after_sync();
-      const uint32_t a = smem_u32(smem + st * kTgWgStage), b = a + 2 * 128 * 128;
+      const uint32_t a = smem_u32(smem + st * F::kStage), b = a + F::kTpg * F::kATile;
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk)  // 128 voxels: eight K = 16 steps of 16 rows
-        tc::mma_bf16(tmem, sw128_mn_desc(a + 2048 * kk, 128 * 128),
-                     sw128_mn_desc(b + 2048 * kk, 128 * 128), idesc, i > 0 || kk > 0);
+        tc::mma_bf16(tmem, swmn_desc<2 * CI>(a + 32 * CI * kk, F::kATile),
+                     swmn_desc<128>(b + 2048 * kk, F::kBTile), idesc, i > 0 || kk > 0);
       tc::commit(&empty[st]);
       if (i + 2 < nt) {
         if (!mbar_wait_sleep_bounded(&empty[st], (uint32_t)((i >> 1) & 1), err)) {
@@ -346,16 +383,16 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
   if (threadIdx.x == 0) tc::commit(done);
   const bool ok = mbar_wait_block(done, 0u, err, lost == 0);
   tc::fence_after_sync();
-  float* const pw = part + (int64_t)blockIdx.y * (s.Kp + 1) * 128;
+  float* const pw = part + (int64_t)blockIdx.y * (s.Kp + 1) * CO;
   const int row = warp * 32 + lane;
   int k = -1;
   if (bias)
     k = row == 0 ? s.Kp : -1;
-  else if (row < 64 || two)
-    k = (tap0 + (row >> 6)) * 64 + (row & 63);
+  else if (row / CI < ntap)
+    k = (tap0 + row / CI) * CI + row % CI;
   const bool live = ok && k >= 0;
 #pragma unroll 1
-  for (int c = 0; c < 128; c += 16) {
+  for (int c = 0; c < CO; c += 16) {
     float v[16];
     tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
     if (!live) continue;
@@ -365,7 +402,7 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-      *(float4*)(pw + (int64_t)k * 128 + c + 4 * q) =
+      *(float4*)(pw + (int64_t)k * CO + c + 4 * q) =
           make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
   }
   if (threadIdx.x == 0 && lost)
@@ -374,7 +411,7 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, 128);
+    tc::tmem_dealloc(tmem, CO < 32 ? 32 : CO);
   }
 }
 
@@ -388,29 +425,6 @@ __global__ void __launch_bounds__(128) k_conv_tg_wgrad(const __grid_constant__ C
 // tap) sequence; warps 0-3 take a tile's accumulator (two in TMEM, alternating) for
 // the bias + GELU epilogue while the next tile's MMAs run.
 
-// Layout type of an R-byte row swizzle (R = 32, 64, 128).
-__host__ __device__ constexpr uint32_t swz_code(int row_bytes) {
-  return row_bytes == 32 ? 6u : (row_bytes == 64 ? 4u : 2u);
-}
-// Swizzled K-major descriptor for R-byte rows (8-row groups 8 R bytes apart).
-template <int R>
-__device__ __forceinline__ uint64_t swk_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) |
-         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
-}
-// Swizzled MN-major descriptor for R-byte rows: MN groups lbo bytes apart, 8-row K
-// groups 8 R bytes apart.
-template <int R>
-__device__ __forceinline__ uint64_t swmn_desc(uint32_t saddr, uint32_t lbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((8 * R) >> 4) << 32) | (1ull << 46) | ((uint64_t)swz_code(R) << 61);
-}
-
-// Tile geometry of the persistent tap GEMM: Wt = Wo, Ht, Dt, nbt with Wt Ht Dt nbt = 128.
-struct TgGeom {
-  int wt, ht, dt, nbt;   // tile extents (voxels, rows, planes, images)
-  int nh, nd, nbk;       // tiles along h, d and images
-};
 
 template <int CI, int CO>
 struct TgpFwd {
