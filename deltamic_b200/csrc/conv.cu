@@ -1420,8 +1420,8 @@ template <int CO>
 static cudaError_t s2d_fwd_launch(const ConvShape& s, const bf16* x, const bf16* w,
                                   const float* bias, float* pre, bf16* act, cudaStream_t st) {
   static std::atomic<bool> done[kConvMaxDevices];
-  auto k = k_conv_s2d_fwd<CO>;
-  const int smem = S2dFwd<CO>::kSmem;
+  auto k = k_conv_s2d_fwd_ws<CO>;
+  const int smem = S2dFwdWs<CO>::kSmem;
   cudaError_t e = fp_smem_once(k, smem, done);
   if (e != cudaSuccess) return e;
   const int64_t tiles = (int64_t)s.B * s.Do * ((s.Ho + 15) / 16) * ((s.Wo + 7) / 8);

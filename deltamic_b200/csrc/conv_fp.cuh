@@ -57,6 +57,25 @@ __device__ __forceinline__ bool mbar_wait_block(uint64_t* bar, uint32_t parity, 
   return __syncthreads_and(ok) != 0;  // the same answer in every thread
 }
 
+__device__ __forceinline__ void mbar_arrive1(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Named barrier ``id`` over ``n`` threads that also ANDs a flag across them (every
+// participant leaves with the same answer).
+__device__ __forceinline__ bool named_bar_and(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
 // Tensor-map (TMA) box loads from this GPU's global memory into shared memory,
 // completing on an mbarrier (no multicast).  Coordinates innermost first; the
 // innermost one (a channel) is a multiple of 8 BF16 (16 bytes); the others may be

@@ -121,33 +121,92 @@ __device__ __forceinline__ void s2d_store(uint8_t* fp, const S2dPrefetch& p) {
   }
 }
 
-template <int CO>
-struct S2dFwd {
-  static constexpr int kWBytes = 8 * CO * 16;  // chunk (block tap, co): 8 parities
-  static constexpr int kSmem = kWBytes + kS2dFpBytes + 64;
+// The same for a group of 128 threads (t = its thread index): items t + 128 i, i < 4.
+struct S2dPrefetch4 {
+  uint4 v[4];
+  int16_t dst[4];
+  int8_t j[4];
 };
 
-// Forward of the single-channel layer: pre = conv(x, w) + bias (FP32), act =
-// GELU(pre) (BF16).  Persistent blocks of 256 threads: the weight image is built
-// once; per tile four MMAs, then the next tile's footprint loads are issued, the
-// epilogue runs, and the loaded pieces are stored into the footprint.  Warp w reads
-// accumulator lanes 32 (w % 4) .. + 31, columns (w / 4) CO / 2 .. + CO / 2 - 1.
+__device__ __forceinline__ void s2d_prefetch4(const bf16* __restrict__ x, const ConvShape& s,
+                                              int b, int od, int oh0, int ow0, int t,
+                                              S2dPrefetch4& p) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int e = t + 128 * i;
+    p.dst[i] = -1;
+    p.v[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (e >= 136 * 3) continue;
+    const int j = e % 3, rr = e / 3;
+    const int pp = rr & 3, r2 = rr >> 2;
+    const int hh = r2 % 17, dd = r2 / 17;
+    const int d = 2 * (od - 1 + dd) + (pp >> 1), h = 2 * (oh0 - 1 + hh) + (pp & 1);
+    const int c0 = 2 * ow0 - 8 + 8 * j;
+    p.dst[i] = (int16_t)(((dd * 17 + hh) * 9) * 4 + pp);
+    p.j[i] = (int8_t)j;
+    if (d < 0 || d >= s.D || h < 0 || h >= s.H) continue;
+    const bf16* row = x + (((size_t)b * s.D + d) * s.H + h) * s.W;
+    if (c0 >= 0 && c0 + 8 <= s.W) {
+      p.v[i] = __ldg((const uint4*)(row + c0));
+    } else {  // a piece at the volume's edge
+      uint16_t e8[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        e8[k] = (c0 + k >= 0 && c0 + k < s.W) ? __bfloat16_as_ushort(row[c0 + k]) : (uint16_t)0;
+      p.v[i] = make_uint4(e8[0] | (uint32_t)e8[1] << 16, e8[2] | (uint32_t)e8[3] << 16,
+                          e8[4] | (uint32_t)e8[5] << 16, e8[6] | (uint32_t)e8[7] << 16);
+    }
+  }
+}
+
+__device__ __forceinline__ void s2d_store4(uint8_t* fp, const S2dPrefetch4& p) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (p.dst[i] < 0) continue;
+    const int chunk4 = p.dst[i] >> 2, pp = p.dst[i] & 3, j = p.j[i];
+    const uint32_t w4[4] = {p.v[i].x, p.v[i].y, p.v[i].z, p.v[i].w};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int ww = 4 * j + t - 3;
+      if (ww >= 0 && ww < 9) *(uint32_t*)(fp + (chunk4 + ww) * 16 + pp * 4) = w4[t];
+    }
+  }
+}
+
+// Warp-specialized forward of the single-channel layer.  Warps 4-7 stage a tile's
+// block footprint (register loads of aligned row pieces, two footprint buffers) and
+// one of their threads issues its four MMAs into one of two TMEM accumulators;
+// warps 0-3 run the bias + GELU epilogue of the other accumulator meanwhile (one
+// output row per thread, all CO channels).  Barriers: mdone[buffer] (the MMAs that
+// read a footprint buffer are done), tfull / tempty[accumulator].
 template <int CO>
-__global__ void __launch_bounds__(256) k_conv_s2d_fwd(const bf16* __restrict__ x, ConvShape s,
-                                                      const bf16* __restrict__ w,
-                                                      const float* __restrict__ bias,
-                                                      float* __restrict__ pre,
-                                                      bf16* __restrict__ act, int* err) {
-  using F = S2dFwd<CO>;
+struct S2dFwdWs {
+  static constexpr int kWBytes = 8 * CO * 16;
+  static constexpr int kSmem = kWBytes + 2 * kS2dFpBytes + 128;
+  static constexpr int kCols = 2 * CO < 32 ? 32 : 2 * CO;
+};
+
+template <int CO>
+__global__ void __launch_bounds__(256) k_conv_s2d_fwd_ws(const bf16* __restrict__ x, ConvShape s,
+                                                         const bf16* __restrict__ w,
+                                                         const float* __restrict__ bias,
+                                                         float* __restrict__ pre,
+                                                         bf16* __restrict__ act, int* err) {
+  using F = S2dFwdWs<CO>;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const wimg = smem;
-  uint8_t* const fp = smem + F::kWBytes;
-  uint64_t* const bar = (uint64_t*)(fp + kS2dFpBytes);
-  uint32_t* const slot = (uint32_t*)(bar + 1);
+  uint8_t* const fps = smem + F::kWBytes;
+  uint64_t* const mdone = (uint64_t*)(fps + 2 * kS2dFpBytes);
+  uint64_t* const tfull = mdone + 2;
+  uint64_t* const tempty = tfull + 2;
+  uint64_t* const done = tempty + 2;
+  uint32_t* const slot = (uint32_t*)(done + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwb = (s.Wo + 7) >> 3, nhb = (s.Ho + 15) >> 4;
   const int ntiles = s.B * s.Do * nhb * nwb;
-  auto tile = [&](int t, int& b, int& od, int& oh0, int& ow0) {
+  const int nloc = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto tile = [&](int lt, int& b, int& od, int& oh0, int& ow0) {
+    int t = (int)blockIdx.x + lt * (int)gridDim.x;
     ow0 = (t % nwb) * 8;
     t /= nwb;
     oh0 = (t % nhb) * 16;
@@ -156,83 +215,120 @@ __global__ void __launch_bounds__(256) k_conv_s2d_fwd(const bf16* __restrict__ x
     b = t / s.Do;
   };
 
-  // weight image, K-major B: chunk (block tap, co) holds the eight parities
-  for (int e = threadIdx.x; e < 8 * CO * 8; e += 256) {
+  for (int e = threadIdx.x; e < 8 * CO * 8; e += 256) {  // weight image (K-major B)
     const int par = e & 7, co = (e >> 3) % CO, btap = (e >> 3) / CO;
     const int tap = s2d_tap(btap, par);
     ((bf16*)wimg)[e] = tap < 0 ? __float2bfloat16(0.f) : w[tap * CO + co];
   }
-  int b = 0, od = 0, oh0 = 0, ow0 = 0;
-  int t = blockIdx.x;
-  S2dPrefetch pf;
-  if (t < ntiles) {
-    tile(t, b, od, oh0, ow0);
-    s2d_prefetch(x, s, b, od, oh0, ow0, pf);
-    s2d_store(fp, pf);
-  }
-  if (warp == 0) tc::tmem_alloc(slot, 32);
-  if (threadIdx.x == 32) {
-    mbar_init(bar, 1);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&mdone[i], 1);
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 4);
+    }
+    mbar_init(done, 1);
     fence_mbar_init();
   }
-  const int q = warp & 3, row = q * 32 + lane, c0 = (warp >> 2) * (CO / 2);
-  float bv[CO / 2];
-#pragma unroll
-  for (int j = 0; j < CO / 2; ++j) bv[j] = bias ? bias[c0 + j] : 0.f;
-  bool ok = true;
-  for (int it = 0; t < ntiles; ++it) {
-    fence_proxy_async();  // footprint and weight-image stores -> the MMA's async-proxy reads
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *slot;
-    if (threadIdx.x == 0) {
-      const uint32_t wb = smem_u32(wimg), fb = smem_u32(fp);
-      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>();  // both K-major
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {  // (dd, dh); K = (dw, par)
-        const uint32_t a = fb + (uint32_t)(((g >> 1) * 17 + (g & 1)) * 9) * 16;
-        const uint32_t bb = wb + (uint32_t)(2 * g * CO) * 16;
-        tc::mma_bf16(tmem, fp_desc(a, 16, 9 * 16), fp_desc(bb, CO * 16, 128), idesc, g > 0);
+  if (warp == 0) tc::tmem_alloc(slot, F::kCols);
+  fence_proxy_async();  // weight image -> the MMA's async-proxy reads
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+
+  if (warp >= 4) {  // producer
+    const int t = threadIdx.x - 128;
+    bool good = true;
+    S2dPrefetch4 pf;  // the pieces of the tile about to be stored, loaded a tile ahead
+    if (nloc > 0) {
+      int b, od, oh0, ow0;
+      tile(0, b, od, oh0, ow0);
+      s2d_prefetch4(x, s, b, od, oh0, ow0, t, pf);
+    }
+    for (int lt = 0; lt < nloc && good; ++lt) {
+      const int fb = lt & 1, acc = lt & 1;
+      // the MMAs of tile lt - 2 read this footprint buffer
+      if (lt >= 2 && !mbar_wait_sleep_bounded(&mdone[fb], (uint32_t)(((lt - 2) >> 1) & 1), err))
+        good = false;
+      if (good) s2d_store4(fps + fb * kS2dFpBytes, pf);
+      fence_proxy_async();
+      good = named_bar_and(1, 128, good);  // the footprint is stored, by every producer
+      if (!good) break;
+      if (lt + 1 < nloc) {  // next tile's loads in flight while this tile's MMAs issue
+        int b, od, oh0, ow0;
+        tile(lt + 1, b, od, oh0, ow0);
+        s2d_prefetch4(x, s, b, od, oh0, ow0, t, pf);
       }
-      tc::commit(bar);
-    }
-    ok = mbar_wait_block(bar, (uint32_t)(it & 1), err) && ok;
-    tc::fence_after_sync();
-    const int cb = b, cod = od, coh0 = oh0, cow0 = ow0;
-    t += gridDim.x;
-    if (!ok) break;
-    const bool more = t < ntiles;
-    if (more) {
-      tile(t, b, od, oh0, ow0);
-      s2d_prefetch(x, s, b, od, oh0, ow0, pf);
-    }
-    const int oh = coh0 + (row >> 3), ow = cow0 + (row & 7);
-    const bool live = oh < s.Ho && ow < s.Wo;
-    const int64_t m = (((int64_t)cb * s.Do + cod) * s.Ho + oh) * s.Wo + ow;
+      if (t == 0) {
+        if (lt >= 2 &&
+            !mbar_wait_sleep_bounded(&tempty[acc], (uint32_t)(((lt >> 1) - 1) & 1), err)) {
+          good = false;
+        } else {
+          tc::fence_after_sync();
+          const uint32_t wb = smem_u32(wimg), fb0 = smem_u32(fps + fb * kS2dFpBytes);
+          constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CO>();  // both K-major
 #pragma unroll
-    for (int c = 0; c < CO / 2; c += 8) {
-      float v[8];
-      tc::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c0 + c), v);
-      if (!live) continue;
-      uint32_t u[4];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] += bv[c + j];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        u[j] = pack2(__float2bfloat16(gelu(v[2 * j])), __float2bfloat16(gelu(v[2 * j + 1])));
-      float4* pp = (float4*)(pre + m * CO + c0 + c);
-      pp[0] = make_float4(v[0], v[1], v[2], v[3]);
-      pp[1] = make_float4(v[4], v[5], v[6], v[7]);
-      *(uint4*)(act + m * CO + c0 + c) = make_uint4(u[0], u[1], u[2], u[3]);
+          for (int g = 0; g < 4; ++g) {  // (dd, dh); K = (dw, par)
+            const uint32_t a = fb0 + (uint32_t)(((g >> 1) * 17 + (g & 1)) * 9) * 16;
+            const uint32_t bb = wb + (uint32_t)(2 * g * CO) * 16;
+            tc::mma_bf16(tmem + (uint32_t)(acc * CO), fp_desc(a, 16, 9 * 16),
+                         fp_desc(bb, CO * 16, 128), idesc, g > 0);
+          }
+        }
+        tc::commit(&mdone[fb]);
+        tc::commit(&tfull[acc]);
+      }
+      good = named_bar_and(1, 128, good);  // thread 0's accumulator wait, shared
     }
-    if (more) s2d_store(fp, pf);  // the MMAs reading fp are done
+    if (t == 0) {  // every MMA issued is complete before the block leaves
+      tc::commit(done);
+      mbar_wait_sleep_bounded(done, 0u, err);
+    }
+  } else {  // epilogue: warp q reads TMEM lane quarter q
+    const int row = warp * 32 + lane;
+    float bv[CO];
+#pragma unroll
+    for (int j = 0; j < CO; ++j) bv[j] = bias ? bias[j] : 0.f;
+    for (int lt = 0; lt < nloc; ++lt) {
+      const int acc = lt & 1;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait_sleep_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      if (lane != 0) mbar_wait_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      tc::fence_after_sync();
+      int b, od, oh0, ow0;
+      tile(lt, b, od, oh0, ow0);
+      const int oh = oh0 + (row >> 3), ow = ow0 + (row & 7);
+      const bool live = oh < s.Ho && ow < s.Wo;
+      const int64_t m = (((int64_t)b * s.Do + od) * s.Ho + oh) * s.Wo + ow;
+#pragma unroll
+      for (int c = 0; c < CO; c += 16) {
+        float v[16];
+        tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * CO + c), v);
+        if (!live) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += bv[c + j];
+        float4* pp = (float4*)(pre + m * CO + c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) pp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        uint32_t u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          u[j] = pack2(__float2bfloat16(gelu(v[2 * j])), __float2bfloat16(gelu(v[2 * j + 1])));
+        *(uint4*)(act + m * CO + c) = make_uint4(u[0], u[1], u[2], u[3]);
+        *(uint4*)(act + m * CO + c + 8) = make_uint4(u[4], u[5], u[6], u[7]);
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&tempty[acc]);
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(*slot, 32);
+    tc::tmem_dealloc(tmem, F::kCols);
   }
 }
 

@@ -437,9 +437,6 @@ struct TgpFwd {
   static_assert(kSmem <= 227 * 1024, "stages above the shared-memory limit");
 };
 
-__device__ __forceinline__ void mbar_arrive1(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 template <int CI, int CO>
 __global__ void __launch_bounds__(160) k_conv_tgp_fwd(const __grid_constant__ CUtensorMap xmap,
