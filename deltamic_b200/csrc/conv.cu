@@ -1367,11 +1367,49 @@ static int fp_dgrad_launch(const ConvShape& s, const bf16* dp, const bf16* w, fl
   return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
 }
 
+static bool tgp_geom(const ConvShape& s, TgGeom& g);
+
+// Data gradient on the per-class tap-GEMM kernel (32 -> 64 channels, even input
+// extents).  -1: not taken.
+static int tgc_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* dx, bf16* dxb,
+                     cudaStream_t st) {
+  TgGeom g;
+  if (s.Ci != 32 || s.Co != 64 || (s.D & 1) || (s.H & 1) || (s.W & 1) || !tgp_geom(s, g) ||
+      !aligned16(dp) || !aligned16(w) || !aligned16(dxb ? (void*)dxb : (void*)dx))
+    return -1;
+  CUtensorMap dmap, wmap;
+  const cuuint64_t ddims[5] = {64, (cuuint64_t)s.Wo, (cuuint64_t)s.Ho, (cuuint64_t)s.Do,
+                               (cuuint64_t)s.B};
+  const cuuint32_t dbox[5] = {64, (cuuint32_t)g.wt, (cuuint32_t)g.ht, (cuuint32_t)g.dt,
+                              (cuuint32_t)g.nbt};
+  const cuuint32_t destr[5] = {1, 1, 1, 1, 1};
+  const cuuint64_t wdims[2] = {64, (cuuint64_t)(27 * 32)};
+  const cuuint32_t wbox[2] = {64, 32}, westr[2] = {1, 1};
+  if (!bf16_tmap(&dmap, dp, 5, ddims, dbox, destr, CU_TENSOR_MAP_SWIZZLE_128B) ||
+      !bf16_tmap(&wmap, w, 2, wdims, wbox, westr, CU_TENSOR_MAP_SWIZZLE_128B))
+    return -1;
+  using F = TgcDgrad<32, 64>;
+  static std::atomic<bool> done[kConvMaxDevices];
+  auto k = k_conv_tgc_dgrad<32, 64>;
+  if (fp_smem_once(k, F::kSmem, done) != cudaSuccess) return DM_ERR_CUDA;
+  const int64_t tiles = 8 * (int64_t)g.nbk * g.nd * g.nh;
+  const int per_sm = std::max(1, std::min(232448 / (F::kSmem + 1024), 512 / F::kCols));
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)per_sm * num_sms()));
+  k<<<grid, 160, F::kSmem, st>>>(dmap, wmap, s, g, dx, dxb, conv_status_ptr());
+  count_launches(1);
+  return cudaGetLastError() == cudaSuccess ? DM_OK : DM_ERR_CUDA;
+}
+
 // Data gradient on the footprint kernel (all eight parity classes per tile).
 static bool fp_dgrad(const ConvShape& s, const bf16* dp, const bf16* w, float* dx, bf16* dxb,
                      cudaStream_t st, int& rc) {
   if (!fp_layer(s) || !aligned16(dp) || !aligned16(w) || !aligned16(dxb ? (void*)dxb : (void*)dx))
     return false;
+  if (s.Ci == 32) {
+    rc = tgc_dgrad(s, dp, w, dx, dxb, st);
+    if (rc != -1) return true;
+  }
   rc = s.Ci == 16 ? fp_dgrad_launch<16, 32>(s, dp, w, dx, dxb, st)
                   : fp_dgrad_launch<32, 64>(s, dp, w, dx, dxb, st);
   return rc != -1;

@@ -568,4 +568,214 @@ __global__ void __launch_bounds__(160) k_conv_tgp_fwd(const __grid_constant__ CU
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-parity-class tap-GEMM data gradient (32 -> 64 channels, even input extents, so
+// every class has the output extents and the forward's tile geometry).  A class
+// tile is 128 input voxels (b, 2 j + p) of class p = (pd, ph, pw); each of the
+// class's taps (per axis k = 1 for p = 0, k = 0 and 2 for p = 1) reads dP at the
+// outputs j + delta (delta = 1 for k = 0, else 0): one stride-1 TMA box of dP (64
+// channels = 128-byte rows, K-major SW128; past the extent it reads zero), times the
+// tap's 32 rows of W (K-major SW128: N = ci, K = co).  Warp 4 issues through a
+// 4-stage ring over the block's flat (class tile, class tap) sequence; warps 0-3
+// write dx from one of two TMEM accumulators.
+template <int CI, int CO>
+struct TgcDgrad {
+  static constexpr int kA = 128 * CO * 2;
+  static constexpr int kB = CI * CO * 2;
+  static constexpr int kStage = (kA + kB + 1023) / 1024 * 1024;
+  static constexpr int kStages = 4;
+  static constexpr int kSmem = 1024 + kStages * kStage + 256;
+  static constexpr int kCols = 2 * CI < 32 ? 32 : 2 * CI;
+  static_assert(CO == 64, "dP rows of 128 bytes");
+};
+
+// Taps of class c (bits pd ph pw) in order: tap i of 2^(odd axes).
+__device__ __forceinline__ void tgc_tap(int c, int i, int& kd, int& kh, int& kw) {
+  int k[3];
+#pragma unroll
+  for (int a = 2; a >= 0; --a) {
+    if ((c >> (2 - a)) & 1) {  // odd axis: k = 0 or 2 by the next bit of i
+      k[a] = (i & 1) ? 2 : 0;
+      i >>= 1;
+    } else {
+      k[a] = 1;
+    }
+  }
+  kd = k[0];
+  kh = k[1];
+  kw = k[2];
+}
+
+template <int CI, int CO>
+__global__ void __launch_bounds__(160) k_conv_tgc_dgrad(const __grid_constant__ CUtensorMap dmap,
+                                                        const __grid_constant__ CUtensorMap wmap,
+                                                        ConvShape s, TgGeom g,
+                                                        float* __restrict__ dx,
+                                                        bf16* __restrict__ dxb, int* err) {
+  using F = TgcDgrad<CI, CO>;
+  constexpr int S = F::kStages;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* const smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t* const full = (uint64_t*)(smem + S * F::kStage);
+  uint64_t* const empty = full + S;
+  uint64_t* const tfull = empty + S;
+  uint64_t* const tempty = tfull + 2;
+  uint64_t* const done = tempty + 2;
+  uint32_t* const slot = (uint32_t*)(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntc = g.nbk * g.nd * g.nh;  // tiles per class
+  const int ntiles = 8 * ntc;
+  const int nloc = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  // class tile lt of this block: class c and the tile origin (b0, jd0, jh0)
+  auto tile_of = [&](int lt, int& c, int& b0, int& jd0, int& jh0) {
+    int t = (int)blockIdx.x + lt * (int)gridDim.x;
+    c = t / ntc;
+    t -= c * ntc;
+    jh0 = (t % g.nh) * g.ht;
+    t /= g.nh;
+    jd0 = (t % g.nd) * g.dt;
+    b0 = (t / g.nd) * g.nbt;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 4);
+    }
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(slot, F::kCols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      // flat items: (class tile lt, tap i < 2^popc(c)); the loader runs S items ahead
+      int llt = 0, li = 0, lc = 0, lb0 = 0, ljd0 = 0, ljh0 = 0, ln = 0;  // next item to load
+      if (nloc > 0) {
+        tile_of(0, lc, lb0, ljd0, ljh0);
+        ln = 1 << __popc(lc);
+      }
+      int issued = 0;
+      auto load_next = [&]() {  // the item (llt, li) into stage issued % S
+        const int st = issued % S;
+        int kd, kh, kw;
+        tgc_tap(lc, li, kd, kh, kw);
+        const int tap = (kd * 3 + kh) * 3 + kw;
+        uint8_t* const a = smem + st * F::kStage;
+        mbar_expect_tx(&full[st], F::kA + F::kB);
+        tma_load_5d(a, &dmap, 0, kw == 0 ? 1 : 0, ljh0 + (kh == 0 ? 1 : 0),
+                    ljd0 + (kd == 0 ? 1 : 0), lb0, &full[st]);
+        tma_load_2d(a + F::kA, &wmap, 0, tap * CI, &full[st]);
+        ++issued;
+        if (++li == ln) {  // next class tile
+          li = 0;
+          if (++llt < nloc) {
+            tile_of(llt, lc, lb0, ljd0, ljh0);
+            ln = 1 << __popc(lc);
+          }
+        }
+      };
+      auto more = [&]() { return llt < nloc; };
+      while (issued < S && more()) load_next();
+      constexpr uint32_t idesc = tc::idesc_bf16_f32<128, CI>();  // both K-major
+      bool good = true;
+      int item = 0;
+      for (int lt = 0; lt < nloc && good; ++lt) {
+        int c, b0, jd0, jh0;
+        tile_of(lt, c, b0, jd0, jh0);
+        const int nt = 1 << __popc(c), acc = lt & 1;
+        if (lt >= 2 &&
+            !mbar_wait_sleep_bounded(&tempty[acc], (uint32_t)(((lt >> 1) - 1) & 1), err)) {
+          good = false;
+          break;
+        }
+        for (int i = 0; i < nt; ++i, ++item) {
+          const int st = item % S;
+          if (!mbar_wait_sleep_bounded(&full[st], (uint32_t)((item / S) & 1), err)) {
+            good = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t a = smem_u32(smem + st * F::kStage), b = a + F::kA;
+#pragma unroll
+          for (int kk = 0; kk < CO / 16; ++kk)
+            tc::mma_bf16(tmem + (uint32_t)(acc * CI), swk_desc<128>(a + 32 * kk),
+                         swk_desc<128>(b + 32 * kk), idesc, i > 0 || kk > 0);
+          tc::commit(&empty[st]);
+          if (item >= 1 && more()) {  // refill the stage of the previous item
+            const int p = item - 1;
+            if (!mbar_wait_sleep_bounded(&empty[p % S], (uint32_t)((p / S) & 1), err)) {
+              good = false;
+              break;
+            }
+            load_next();
+          }
+        }
+        tc::commit(&tfull[acc]);
+      }
+      tc::commit(done);
+      mbar_wait_sleep_bounded(done, 0u, err);
+      if (!good)
+        for (int i = 0; i < S; ++i) mbar_wait_sleep_bounded(&full[i], 0u, err, 1u);
+    }
+  } else {  // warps 0..3: epilogue
+    const int row = warp * 32 + lane;
+    const int wl = row % g.wt, hl = (row / g.wt) % g.ht, dl = (row / (g.wt * g.ht)) % g.dt;
+    const int bl = row / (g.wt * g.ht * g.dt);
+    for (int lt = 0; lt < nloc; ++lt) {
+      const int acc = lt & 1;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait_sleep_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      if (lane != 0) mbar_wait_bounded(&tfull[acc], (uint32_t)((lt >> 1) & 1), err);
+      tc::fence_after_sync();
+      int c, b0, jd0, jh0;
+      tile_of(lt, c, b0, jd0, jh0);
+      const int b = b0 + bl, jd = jd0 + dl, jh = jh0 + hl;
+      const int d = 2 * jd + (c >> 2), h = 2 * jh + ((c >> 1) & 1), w = 2 * wl + (c & 1);
+      const bool live = b < s.B && jd < s.Do && jh < s.Ho && wl < s.Wo;
+      const int64_t at = ((((int64_t)b * s.D + d) * s.H + h) * s.W + w) * CI;
+#pragma unroll
+      for (int cc = 0; cc < CI; cc += 16) {
+        float v[16];
+        tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * CI + cc), v);
+        if (!live) continue;
+        if (dxb) {
+#pragma unroll
+          for (int q8 = 0; q8 < 2; ++q8) {
+            uint32_t u[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              u[j] = pack2(__float2bfloat16(v[8 * q8 + 2 * j]), __float2bfloat16(v[8 * q8 + 2 * j + 1]));
+            *(uint4*)(dxb + at + cc + 8 * q8) = make_uint4(u[0], u[1], u[2], u[3]);
+          }
+        } else {
+#pragma unroll
+          for (int q4 = 0; q4 < 4; ++q4)
+            *(float4*)(dx + at + cc + 4 * q4) =
+                make_float4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
+        }
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&tempty[acc]);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, F::kCols);
+  }
+}
+
 }  // namespace dm
