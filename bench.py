@@ -1110,13 +1110,14 @@ def run_conv(args, rank, world, local):
            "e2e": {"value": flops * world / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                    "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(host_img.numel() * 4),
                    "d2h_bytes_per_step": int(sum(h.numel() * 4 for h in host_g))},
-           "roofline": {"bound": "tensor", "kernel": "k_conv_s2d / k_conv_fp / k_conv_umma "
+           "roofline": {"bound": "tensor", "kernel": "k_conv_s2d / k_conv_fp / k_conv_tg "
                                                      "(all products of the step)",
                         "achieved": value, "peak": peak, "unit": "TFLOP/s",
                         "frac": value / peak, "peak_source": peak_src, "traffic": None,
-                        "note": "tensor fraction of the whole step; at about 49 FLOP per DRAM "
-                                "byte the step is memory bound, its tiles serial (TMA wait, "
-                                "MMAs, epilogue) and the space-to-depth kernels issue bound"}}
+                        "note": "tensor fraction of the whole step; at about 50 FLOP per DRAM "
+                                "byte the step is memory bound; the space-to-depth (layer 1) "
+                                "and footprint (layer 2) kernels bound it, the tap GEMMs "
+                                "(layers 3, 4) run from swizzled TMA tiles"}}
     if cpu is not None:
         out["cpu_baseline"] = cpu
     print(json.dumps(out), flush=True)
